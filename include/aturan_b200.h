@@ -1,0 +1,202 @@
+/*
+ * aturan_b200 — B200 (sm_100a) kernels for ATURAN's dynamical-core time step, behind a C ABI.
+ *
+ * The reference has no plugin or FFI layer for this path: its call sites are member and friend
+ * calls on one cUranusModel object. Each entry point below replaces one of those calls and says
+ * which. A maintainer binds them from the reference's driver (planet/cUranusModel.cpp:Run) with
+ * the glue shown in INTEGRATION.md, or from Python with ctypes (aturan_b200/_lib.py).
+ *
+ * Conventions
+ *   - Every function returns an int status: 0 = ATURAN_OK, negative = error (nothing was
+ *     changed on the device unless the function says otherwise), positive = completed but not
+ *     converged. aturan_last_error() returns a message for the last error on a context.
+ *   - Fields are exchanged as contiguous FP64 blocks in the reference's logical order x[i][j][k]
+ *     (i = radius 0..im-1, j = colatitude 0..jm-1, k = longitude 0..km-1, k fastest), i.e. the
+ *     jagged Array of lib/Array.cpp:58-67 flattened. On the device each row is padded to a
+ *     pitch of 32 elements; the padding never crosses this interface.
+ *   - State stays resident on the device between calls. A context owns one CUDA stream; calls on
+ *     one context are not thread-safe, separate contexts may be used from separate threads.
+ *   - There is no CPU fallback: without a usable CUDA device every call returns ATURAN_E_CUDA.
+ */
+#ifndef ATURAN_B200_H
+#define ATURAN_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATURAN_ABI_VERSION 1
+
+enum aturan_status {
+    ATURAN_OK              =  0,
+    ATURAN_NOT_CONVERGED   =  1,   /* iterative solve stopped at its cap above tolerance */
+    ATURAN_E_INVALID       = -1,   /* bad argument: null pointer, size, id, version */
+    ATURAN_E_UNSUPPORTED   = -2,   /* a parameter value this build does not implement */
+    ATURAN_E_CUDA          = -3,   /* CUDA runtime error (message in aturan_last_error) */
+    ATURAN_E_NOMEM         = -4,   /* device allocation failed */
+    ATURAN_E_NONFINITE     = -5    /* a NaN/Inf was found where the path forbids it */
+};
+
+enum aturan_precision {
+    ATURAN_FP64  = 0,   /* state, stencils and solves in FP64: the parity path */
+    ATURAN_MIXED = 1    /* FP32 state and stencils; FP64 Poisson refinement and SatAdj Newton */
+};
+
+/* Field ids. The first 19 are the prognostic fields in the order RHS_Uran_Turb.cpp assembles
+ * them; the next 19 their start-of-step copies (tn, un, ...; cUranusModel.h:1377-1393). */
+enum aturan_field {
+    ATURAN_T = 0, ATURAN_U, ATURAN_V, ATURAN_W,
+    ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE,
+    ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+    ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE,
+    ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+    ATURAN_NH4SH, ATURAN_TKE, ATURAN_DIS,                       /* 0..18 */
+    ATURAN_TN, ATURAN_UN, ATURAN_VN, ATURAN_WN,
+    ATURAN_CH4N, ATURAN_CH4_CLOUDN, ATURAN_CH4_ICEN,
+    ATURAN_H2ON, ATURAN_H2O_CLOUDN, ATURAN_H2O_ICEN,
+    ATURAN_H2SN, ATURAN_H2S_CLOUDN, ATURAN_H2S_ICEN,
+    ATURAN_NH3N, ATURAN_NH3_CLOUDN, ATURAN_NH3_ICEN,
+    ATURAN_NH4SHN, ATURAN_TKEN, ATURAN_DISN,                    /* 19..37 */
+    ATURAN_P_DYN, ATURAN_P_HYDRO, ATURAN_P_STAT,                /* 38..40 */
+    /* pointwise inputs of the RHS, held fixed through a step */
+    ATURAN_NUE, ATURAN_THERMALMASSFLUX, ATURAN_Q_PRECIP,
+    ATURAN_S_PRECIP_CH4, ATURAN_S_PRECIP_CH4_CLOUD, ATURAN_S_PRECIP_CH4_ICE,
+    ATURAN_S_PRECIP_H2O, ATURAN_S_PRECIP_H2O_CLOUD, ATURAN_S_PRECIP_H2O_ICE,
+    ATURAN_S_PRECIP_H2S, ATURAN_S_PRECIP_H2S_CLOUD, ATURAN_S_PRECIP_H2S_ICE,
+    ATURAN_S_PRECIP_NH3, ATURAN_S_PRECIP_NH3_CLOUD, ATURAN_S_PRECIP_NH3_ICE,
+    ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH,
+    ATURAN_RHO_MIX, ATURAN_TKE_SOURCE, ATURAN_DIS_SOURCE,       /* 41..62 */
+    /* hydrostatic split state (cUranusModel.h:1482-1495, flat [(i*jm + j)*km + k] there) */
+    ATURAN_P_BARO, ATURAN_P_B0, ATURAN_P_BFOLLOW,               /* 63..65 */
+    /* projection fields: last RK stage's tendencies and aux = rhs + grad p_dyn */
+    ATURAN_RHS_U, ATURAN_RHS_V, ATURAN_RHS_W,
+    ATURAN_AUX_U, ATURAN_AUX_V, ATURAN_AUX_W,                   /* 66..71 */
+    ATURAN_NFIELDS
+};
+
+#define ATURAN_NPROG 19
+
+/* One condensable's constants, exactly the arguments SaturationAdjustmentUran::run passes to the
+ * shared SaturationAdjustment<Planet>::run (SaturationAdjustmentUran.cpp:222-238). */
+typedef struct aturan_gas {
+    double t_0, t_00;                   /* [K] melting point, all-ice temperature */
+    double ep, lv, ls;                  /* gas-constant ratio, latent heats [J/kg] */
+    double C, L0, R, del_alf, del_bet;  /* liquid saturation-pressure set (ATPhys.h:49-53) */
+    double C_i, L0_i, del_alf_i, del_bet_i;   /* ice set */
+} aturan_gas;
+
+/* Everything the path reads besides the fields: the grid, the config scalars
+ * (UranusParams.h.inc), the mixture properties of the initialised model and the resolved knobs.
+ * aturan_params_default() fills the reference's defaults after its initialisation. */
+typedef struct aturan_params {
+    int32_t abi_version;         /* = ATURAN_ABI_VERSION */
+    int32_t im, jm, km;          /* stored grid; k = km-1 is the copy of k = 0 */
+    int32_t precision;           /* enum aturan_precision */
+    int32_t turb_active;         /* k*, omega* prognostic (cUranusModel::turb_active) */
+    int32_t coriolis_full;       /* ATURAN_CORIOLIS_FULL: scale L_atm in metres */
+    int32_t cp_h2_mode;          /* ATURAN_CP_H2: 0 constant, 1 normal, 2 equilibrium H2 */
+    int32_t cp_gas;              /* ATURAN_CP_GAS */
+    int32_t cp_dyn;              /* cp(T) in the RHS pressure-work term (CpH2::dyn_on) */
+    int32_t press_consistent;    /* ATURAN_PRESS_CONSISTENT (PressureSolverUran.h:68) */
+    int32_t press_incr;          /* ATURAN_PRESS_INCR of PressureSolverUran (:139) */
+    int32_t rigid_lid;           /* ATURAN_BC_RIGID_LID for the shared solver */
+    int32_t satadj_conserve, satadj_newton, satadj_evap, satadj_ice_entry;
+    int32_t satadj_bergeron, satadj_freeze, satadj_dry_exit, local_rho;
+    int32_t nh4sh_sync;          /* RK_SCALAR_SYNC also copies nh4sh (ATURAN_NH4SH_EQ) */
+    int32_t reserved_i[8];
+
+    double r0, dr, the0, dthe, phi0, dphi, dt;
+    double metric_R_km;          /* ATURAN_METRIC_RADIUS; <= 0 keeps the unshifted rad.z */
+    double sinthe_min;           /* polar metric floor (cUranusModel.h:675) */
+    double L_atm, u_0, t_ref, g, omega, re, pr;
+    double Coriolis, centrifugal, buoyancy, chemical_reaction, R_ref, p_ref;
+    double r_mix, R_mix, cp_mix, mue_mix;
+    double r_h2, r_he, r_ch4, cp_h2, cp_he, cp_ch4;
+    double sc_ch4, sc_h2o, sc_h2s, sc_nh3, sc_nh4sh;
+    double alpha_sponge, r_p_nh4sh, rho_cond_nh4sh;
+    double turb_coupling;        /* ATURAN_TURB_COUPLING */
+    double precip_coupling;      /* ATURAN_PRECIP_COUPLING */
+    double tmf_scale;            /* ATURAN_THERMAL_MASSFLUX */
+    double cent_mom;             /* ATURAN_CENTRIFUGAL_MOM (0 or 1) */
+    double pbaro_follow;         /* ATURAN_PBARO_FOLLOW tau [RK steps]; 0 = p_baro frozen */
+    double t_min_K, t_max_K;     /* integrator temperature guards */
+    double p_dyn_cap;            /* shared solver source clamp (PressureSolver.h:168) */
+    double reserved_d[8];
+    aturan_gas gas[4];           /* H2O, H2S, NH3, CH4: the loop's order */
+} aturan_params;
+
+enum aturan_pressure_kind {
+    ATURAN_PRESS_GS_LEX    = 0, /* PressureSolverUran::run, one lexicographic GS sweep (default) */
+    ATURAN_PRESS_RB_SHARED = 1, /* PressureSolver<cUranusModel>::run, max_sweeps red-black sweeps */
+    ATURAN_PRESS_RB_SOR    = 2  /* the shared solver's equation solved to a relative residual with
+                                   red-black SOR at omega (new behaviour, no reference oracle) */
+};
+
+typedef struct aturan_ctx aturan_ctx;
+
+/* Fill *p with the reference's resolved defaults on the 41 x 181 x 361 grid. */
+int aturan_params_default(aturan_params* p);
+
+/* Create a context: allocate the device state for p->im x p->jm x p->km, build the geometry and
+ * cp(T) tables on the host in FP64 and upload them. Replaces nothing in the reference (its state
+ * is allocated by cUranusModel::resetArrays, cUranusModel.cpp:1416). */
+int aturan_ctx_create(const aturan_params* p, aturan_ctx** out);
+int aturan_ctx_destroy(aturan_ctx* ctx);
+const char* aturan_last_error(const aturan_ctx* ctx);
+
+/* Copy one field between host memory (contiguous FP64 [i][j][k], im*jm*km values) and the
+ * device. Upload is asynchronous on the context's stream from pinned memory, synchronous from
+ * pageable memory; download returns when the data is on the host. */
+int aturan_upload(aturan_ctx* ctx, int field, const double* host);
+int aturan_download(aturan_ctx* ctx, int field, double* host);
+/* As upload/download for a field on a device pointer (contiguous [i][j][k] FP64). */
+int aturan_upload_device(aturan_ctx* ctx, int field, const double* dev);
+int aturan_download_device(aturan_ctx* ctx, int field, double* dev);
+/* buoy_ref_level[im] of the last RK4 step (cUranusModel.h:1431). */
+int aturan_download_buoy_ref(aturan_ctx* ctx, double* host_im);
+
+/* One RK4 step: computeBuoyancyRefLevel + computeHydrostaticPressure(true) + the four stages
+ * with their fused RHS evaluation and the final update.
+ * Replaces cUranusModel::RungeKuttaUran() (RungeKutta_Uran_Turb.cpp:179-404). */
+int aturan_rk4_step(aturan_ctx* ctx);
+
+/* The pressure solve.
+ *   GS_LEX:    replaces PressureSolverUran(m).run() (PressureSolverUran.h:33-250); omega,
+ *              max_sweeps and tol are ignored (exactly one sweep, as the reference).
+ *   RB_SHARED: replaces PressureSolver<cUranusModel>(m).run() (PressureSolver.h:145-766) with
+ *              ATURAN_PRESS_SWEEPS = max_sweeps; omega and tol ignored.
+ *   RB_SOR:    the shared solver's equation (its source, clamp and boundary folds) solved with
+ *              red-black SOR at omega until the relative L2 residual <= tol or max_sweeps.
+ * sweeps_done and resid (relative L2 residual at exit; RB_SOR only, else 0) may be NULL. */
+int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
+                    int* sweeps_done, double* resid);
+
+/* The saturation adjustment of every gas whose bit is set in gas_mask (bit 0 H2O, 1 H2S, 2 NH3,
+ * 3 CH4), in that order, fused per cell. Replaces the four
+ * SaturationAdjustmentUran(m).run(...) calls of cUranusModel.cpp:998-1027 (and each one alone).
+ * n_adjusted / n_noconv (may be NULL) receive the reference's per-call counters summed over
+ * the gases (SaturationAdjustment.h:592-593). */
+int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_noconv);
+
+/* The ATURAN_RK_SCALAR_SYNC=2 copy of the condensables and T (and NH4SH when nh4sh_sync) into
+ * their start-of-step copies, cUranusModel.cpp:1049-1073. */
+int aturan_sync_ncopies(aturan_ctx* ctx);
+
+/* The in-scope part of one even iteration of cUranusModel::Run (cUranusModel.cpp:967-1123):
+ * pressure (kind/omega/max_sweeps/tol as aturan_pressure), the four saturation adjustments,
+ * the n-copy sync and the RK4 step. */
+int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol);
+
+/* Wait for all work queued on the context's stream. */
+int aturan_sync(aturan_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work around it. */
+void* aturan_stream(aturan_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATURAN_B200_H */

@@ -1,0 +1,1111 @@
+/*
+ * CPU ORACLE for the aturan_b200 hot path — TEST INFRASTRUCTURE, NOT PART OF THE PRODUCT.
+ * See aturan_oracle.h for what it is, who may call it and how its parity is pinned.
+ *
+ * Each function restates one reference routine; the citation in front of it names the
+ * reference file and lines it follows, by the file's path within the reference project. The
+ * expressions keep the reference's operand order (including its association order) because the
+ * point of this file is bit equality with the compiled reference; the knobs are the resolved
+ * values carried in aturan_params instead of the reference's environment reads.
+ */
+#include "aturan_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define IDX(i, j, k) (((size_t)(i) * jm + (j)) * km + (k))
+#define NPROG ATURAN_NPROG
+
+static const double C43 = 4.0 / 3.0, C13 = 1.0 / 3.0;   /* cUranusModel.h:866 */
+
+/* std::max(a, b) of <algorithm>: (a < b) ? b : a, NaN handling included. */
+static double stdmax(double a, double b){ return (a < b) ? b : a; }
+
+void oracle_set_threads(int n){
+#ifdef _OPENMP
+    if(n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* lib/Array_1D.cpp:50-60 (Coordinates: a running sum, not i*dz) with the model's r0 = 1,
+ * dr = 0.025, the0 = 0, dthe = 1 deg (cUranusModel.cpp:336-372). */
+void oracle_coords(const aturan_params* p, double* rad_z, double* the_z){
+    rad_z[0] = p->r0;
+    for(int l = 1; l < p->im; l++) rad_z[l] = rad_z[l-1] + p->dr;
+    the_z[0] = p->the0;
+    for(int l = 1; l < p->jm; l++) the_z[l] = the_z[l-1] + p->dthe;
+}
+
+/* cUranusModel.h:641-647 */
+static double metric_radius(const aturan_params* p, double rm){
+    const double R_km = p->metric_R_km;
+    if(!(R_km > 0.0)) return rm;
+    return rm + (R_km / p->L_atm - 1.0);
+}
+
+/* ---- cp(T) of the gas, CpH2.h:43-134 ---- */
+#define CP_R_GAS 8.314462618
+#define CP_M_H2  2.01588e-3
+#define CP_TH_R  87.57
+#define CP_TH_V  6332.0
+#define CP_T_LO  5.0
+#define CP_T_HI  1500.0
+#define CP_DT    0.5
+
+/* CpH2.h:43-64 */
+static void cp_moments(double T, int J0, double wgt, double* Z, double* E1, double* E2){
+    for(int J = J0; J < 60; J += 2){
+        const double e = CP_TH_R * J * (J + 1.0), b = wgt * (2.0 * J + 1.0) * exp(-e / T);
+        *Z += b; *E1 += b * e; *E2 += b * e * e;
+    }
+}
+static double cp_crot(double T, double Z, double E1, double E2){
+    const double m1 = E1 / Z, m2 = E2 / Z;
+    return (m2 - m1 * m1) / (T * T);
+}
+static double cpR_exact(double T, int mode){
+    double c;
+    if(mode == 1){
+        double Zp = 0, Ep = 0, Fp = 0, Zo = 0, Eo = 0, Fo = 0;
+        cp_moments(T, 0, 1.0, &Zp, &Ep, &Fp); cp_moments(T, 1, 1.0, &Zo, &Eo, &Fo);
+        c = 0.25 * cp_crot(T, Zp, Ep, Fp) + 0.75 * cp_crot(T, Zo, Eo, Fo);
+    } else {
+        double Z = 0, E1 = 0, E2 = 0;
+        cp_moments(T, 0, 1.0, &Z, &E1, &E2); cp_moments(T, 1, 3.0, &Z, &E1, &E2);
+        c = cp_crot(T, Z, E1, E2);
+    }
+    const double x = CP_TH_V / T, cv = (x < 700.0) ? x * x * exp(x) / ((exp(x) - 1.0) * (exp(x) - 1.0)) : 0.0;
+    return 2.5 + c + cv;
+}
+
+static double* g_cp_table[3];   /* per mode, built once (CpH2.h:66-75) */
+static int g_cp_n;
+
+static const double* cp_table(int mode){
+    if(g_cp_table[mode]) return g_cp_table[mode];
+    const int n = (int)((CP_T_HI - CP_T_LO) / CP_DT) + 1;
+    double* t = (double*)malloc(sizeof(double) * n);
+    for(int i = 0; i < n; i++) t[i] = cpR_exact(CP_T_LO + i * CP_DT, mode) * CP_R_GAS / CP_M_H2;
+    g_cp_n = n;
+    g_cp_table[mode] = t;
+    return t;
+}
+
+/* CpH2.h:77-84 */
+static double cp_h2_of(const aturan_params* p, double T){
+    if(p->cp_h2_mode <= 0) return p->cp_h2;
+    const double* t = cp_table(p->cp_h2_mode);
+    const int n = g_cp_n;
+    const double Tc = T < CP_T_LO ? CP_T_LO : T;
+    const double x = ((Tc > CP_T_HI ? CP_T_HI : Tc) - CP_T_LO) / CP_DT;
+    int i = (int)x; if(i > n - 2) i = n - 2;
+    const double fr = x - i;
+    return t[i] + fr * (t[i+1] - t[i]);
+}
+
+/* CpH2.h:122-134 (Lapse::cp with dyn_on) */
+double oracle_cp_lapse(const aturan_params* p, double T){
+    if(!p->cp_dyn) return p->cp_mix;
+    const double ch = cp_h2_of(p, T);
+    if(p->cp_gas) return (p->r_h2 * ch + p->r_he * p->cp_he + p->r_ch4 * p->cp_ch4) / (p->r_h2 + p->r_he + p->r_ch4);
+    return p->cp_mix + (p->r_h2 / p->r_mix) * (ch - p->cp_h2);
+}
+
+/* ATPhys.h:135-139 with the periodic seam on (the only supported setting). */
+static int phi_wrap(int kk, int km){
+    const int n = km - 1;
+    return kk < 0 ? kk + n : (kk >= n ? kk - n : kk);
+}
+
+/* ATPhys.h:49-53 */
+static double svp(double T_K, double C, double L0, double R, double del_alf, double del_bet){
+    return exp(C + (-L0 / T_K + del_alf * log(T_K) + del_bet * T_K) / (1e-3 * R));
+}
+
+static double coriolis_scale(const aturan_params* p){   /* cUranusModel.h:1498 */
+    return (p->coriolis_full ? p->L_atm * 1.0e3 : p->L_atm) / p->u_0;
+}
+
+/* ---- RungeKutta_Uran_Turb.cpp:18-37, computeBuoyancyRefLevel ---- */
+int oracle_buoy_ref(const aturan_params* p, double* const* f, double* ref){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const double* t = f[ATURAN_T];
+    const double* ps = f[ATURAN_P_STAT];
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    #pragma omp parallel for schedule(static)
+    for(int i = 0; i < im; i++){
+        double sum = 0.0, wsum = 0.0;
+        for(int j = 0; j < jm; j++){
+            const double wgt = sin(the[j]);
+            for(int k = 0; k < km; k++){
+                if(!(t[IDX(i,j,k)] > 0.0)) continue;
+                const double b = p->g * ps[IDX(i,j,k)]
+                               / (p->r_mix * p->R_mix * t[IDX(i,j,k)] * p->t_ref);
+                if(!isfinite(b)) continue;
+                sum  += wgt * b;
+                wsum += wgt;
+            }
+        }
+        ref[i] = (wsum > 0.0) ? sum / wsum : 0.0;
+    }
+    free(rad); free(the);
+    return 0;
+}
+
+/* ---- RungeKutta_Uran_Turb.cpp:62-177, computeHydrostaticPressure, with the default knobs:
+ * ATURAN_HYDRO_SPLIT=1, METRIC_SPLIT=1, CORIOLIS_SPLIT=1, BUOY_RHO_LEVEL=1, HYDRO_REF=0,
+ * HYDRO_ND_KM=0, BUOY_SCALE=1; p_baro allocated (PDYN_GEO=2), p_b0 already captured. ---- */
+int oracle_hydro(const aturan_params* p, double* const* f, const double* ref, int advance){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const double* t = f[ATURAN_T]; const double* ps = f[ATURAN_P_STAT];
+    const double* v = f[ATURAN_V]; const double* w = f[ATURAN_W];
+    double* ph = f[ATURAN_P_HYDRO];
+    const double* pbaro = f[ATURAN_P_BARO]; const double* pb0 = f[ATURAN_P_B0];
+    double* pbf = f[ATURAN_P_BFOLLOW];
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    const double nd_rel = p->g * (p->L_atm * 1.0e3) / (p->u_0 * p->u_0);
+    const double buoy_scale_local = 1.0;
+    const double follow_tau = p->pbaro_follow;
+    const int follow_on = follow_tau > 0.0;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int j = 0; j < jm; j++){
+        for(int k = 0; k < km; k++){
+            const double cor_ = p->Coriolis * coriolis_scale(p) * 2.0 * p->omega * fabs(sin(the[j]));
+            #define BUOY(ii) ({ const double T_ = t[IDX(ii,j,k)]; double r_ = 0.0;                    \
+                if(T_ > 0.0){                                                                          \
+                    const double b_ = p->g * ps[IDX(ii,j,k)] / (p->r_mix * p->R_mix * T_ * p->t_ref)   \
+                                    - ref[ii];                                                         \
+                    const double f_ = -nd_rel * buoy_scale_local * p->buoyancy * b_ / ref[ii];          \
+                    r_ = isfinite(f_) ? f_ : 0.0; }                                                    \
+                r_; })
+            #define MET0(ii) ((v[IDX(ii,j,k)] * v[IDX(ii,j,k)] + w[IDX(ii,j,k)] * w[IDX(ii,j,k)])     \
+                              / metric_radius(p, rad[ii]) + cor_ * w[IDX(ii,j,k)])
+            if(follow_on){
+                double Pm = 0.0, Pb = 0.0;
+                for(int i = 0; i < im; i++){
+                    if(i > 0){
+                        Pm += 0.5 * (MET0(i-1) + MET0(i)) * p->dr;
+                        Pb += 0.5 * (BUOY(i-1) + BUOY(i)) * p->dr;
+                    }
+                    const size_t q = IDX(i,j,k);
+                    if(advance) pbf[q] += (Pb - pb0[q] - pbf[q]) / follow_tau;
+                    ph[q] = Pm + Pb + pbaro[q] - pbf[q];
+                }
+            } else {
+                ph[IDX(0,j,k)] = 0.0;
+                #define F_(ii) (BUOY(ii) + (v[IDX(ii,j,k)] * v[IDX(ii,j,k)] + w[IDX(ii,j,k)] * w[IDX(ii,j,k)]) \
+                                    / metric_radius(p, rad[ii]) + cor_ * w[IDX(ii,j,k)])
+                for(int i = 1; i < im; i++){
+                    const double fa = F_(i-1);
+                    const double fb = F_(i);
+                    ph[IDX(i,j,k)] = ph[IDX(i-1,j,k)] + 0.5 * (fa + fb) * p->dr;
+                }
+                for(int i = 0; i < im; i++) ph[IDX(i,j,k)] += pbaro[IDX(i,j,k)];
+                #undef F_
+            }
+            #undef BUOY
+            #undef MET0
+        }
+    }
+    free(rad); free(the);
+    return 0;
+}
+
+/* ---- cUranusModel.h:1212-1223 CellGeometry, filled as RungeKutta_Uran_Turb.cpp:192-283 ---- */
+typedef struct {
+    double rm, rm2, sinthe, sinthe2, costhe, cotanthe;
+    double inv_rm, inv_rm2, inv_rmsinthe, inv_rm2sinthe, inv_rm2sinthe2, costhe_inv_rm2sinthe;
+    double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
+} geo_t;
+
+static void geo_fill(const aturan_params* p, const double* rad, const double* the, int i, int j, geo_t* g){
+    const double s = fabs(sin(the[j]));
+    g->rm      = metric_radius(p, rad[i]);
+    g->rm2     = g->rm * g->rm;
+    g->sinthe  = stdmax(p->sinthe_min, s);
+    g->sinthe2 = g->sinthe * g->sinthe;
+    g->costhe  = cos(the[j]);
+    g->cotanthe             = g->costhe / g->sinthe;
+    g->inv_rm               = 1.0 / g->rm;
+    g->inv_rm2              = 1.0 / g->rm2;
+    g->inv_rmsinthe         = 1.0 / (g->rm * g->sinthe);
+    g->inv_rm2sinthe        = g->inv_rm2 / g->sinthe;
+    g->inv_rm2sinthe2       = g->inv_rm2 / g->sinthe2;
+    g->costhe_inv_rm2sinthe = g->costhe * g->inv_rm2sinthe;
+    g->inv_2dr   = 1.0 / (2.0 * p->dr);
+    g->inv_2dthe = 1.0 / (2.0 * p->dthe);
+    g->inv_2dphi = 1.0 / (2.0 * p->dphi);
+    g->inv_dr2   = 1.0 / (p->dr   * p->dr);
+    g->inv_dthe2 = 1.0 / (p->dthe * p->dthe);
+    g->inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+}
+
+/* Species of the RHS in enum order 4..16 with their Schmidt number, precipitation source and
+ * chemistry source (RHS_Uran_Turb.cpp:790-850). */
+static const int SP_SPRECIP[12] = {
+    ATURAN_S_PRECIP_CH4, ATURAN_S_PRECIP_CH4_CLOUD, ATURAN_S_PRECIP_CH4_ICE,
+    ATURAN_S_PRECIP_H2O, ATURAN_S_PRECIP_H2O_CLOUD, ATURAN_S_PRECIP_H2O_ICE,
+    ATURAN_S_PRECIP_H2S, ATURAN_S_PRECIP_H2S_CLOUD, ATURAN_S_PRECIP_H2S_ICE,
+    ATURAN_S_PRECIP_NH3, ATURAN_S_PRECIP_NH3_CLOUD, ATURAN_S_PRECIP_NH3_ICE };
+
+/* ---- RHS_Uran_Turb.cpp:20-1023, RHSUran(i,j,k,geo), default knobs. out[0..18] = rhs of the
+ * prognostic fields in enum order, out[19..21] = aux_u, aux_v, aux_w. ---- */
+static void rhs_cell(const aturan_params* p, double* const* f, int i, int j, int k,
+                     const geo_t* geo, double* out){
+    const int jm = p->jm, km = p->km;
+    const double inv_rm = geo->inv_rm, inv_rm2 = geo->inv_rm2, inv_rmsinthe = geo->inv_rmsinthe;
+    const double inv_rm2sinthe = geo->inv_rm2sinthe, inv_rm2sinthe2 = geo->inv_rm2sinthe2;
+    const double costhe_inv_rm2sinthe = geo->costhe_inv_rm2sinthe;
+    const double costhe = geo->costhe, cotanthe = geo->cotanthe, rm = geo->rm;
+    const double inv_2dr = geo->inv_2dr, inv_2dthe = geo->inv_2dthe, inv_2dphi = geo->inv_2dphi;
+    const double inv_dr2 = geo->inv_dr2, inv_dthe2 = geo->inv_dthe2, inv_dphi2 = geo->inv_dphi2;
+    const int kw = phi_wrap(k - 1, km), ke = phi_wrap(k + 1, km);
+    const size_t c = IDX(i,j,k);
+
+    /* first and second derivatives of the 19 prognostic fields (:92-176) */
+    double d1r[NPROG], d2r[NPROG], d1t[NPROG], d2t[NPROG], d1p[NPROG], d2p[NPROG];
+    for(int q = 0; q < NPROG; q++){
+        const double* F = f[q];
+        d1r[q] = (F[IDX(i+1,j,k)] - F[IDX(i-1,j,k)]) * inv_2dr;
+        d2r[q] = (F[IDX(i+1,j,k)] - 2.0*F[c] + F[IDX(i-1,j,k)]) * inv_dr2;
+        d1t[q] = (F[IDX(i,j+1,k)] - F[IDX(i,j-1,k)]) * inv_2dthe;
+        d2t[q] = (F[IDX(i,j+1,k)] - 2.0*F[c] + F[IDX(i,j-1,k)]) * inv_dthe2;
+        d1p[q] = (F[IDX(i,j,ke)] - F[IDX(i,j,kw)]) * inv_2dphi;
+        d2p[q] = (F[IDX(i,j,ke)] - 2.0*F[c] + F[IDX(i,j,kw)]) * inv_dphi2;
+    }
+    const double* P = f[ATURAN_P_DYN];
+    const double dpdr   = (P[IDX(i+1,j,k)] - P[IDX(i-1,j,k)]) * inv_2dr;
+    const double dpdthe = (P[IDX(i,j+1,k)] - P[IDX(i,j-1,k)]) * inv_2dthe;
+    const double dpdphi = (P[IDX(i,j,ke)] - P[IDX(i,j,kw)]) * inv_2dphi;
+
+    const double u_ijk = f[ATURAN_U][c], v_ijk = f[ATURAN_V][c], w_ijk = f[ATURAN_W][c];
+    const double omega = p->omega;
+
+    /* Coriolis and centrifugal (:208-278), CORIOLIS_TRUE_SINE=1, no legacy signs */
+    const double sinthe_bf = sqrt(stdmax(0.0, 1.0 - costhe * costhe));
+    const double Coriolis_rad = -2.0 * omega * sinthe_bf * w_ijk;
+    const double Coriolis_the = -2.0 * omega * costhe * w_ijk;
+    const double Coriolis_phi = +2.0 * omega * (1.0 * costhe * v_ijk + sinthe_bf * u_ijk);
+    const double cent_mom = p->cent_mom;
+    const double centrifugal_rad = omega * omega * rm * sinthe_bf * sinthe_bf;
+    const double centrifugal_the = omega * omega * rm * sinthe_bf * costhe;
+
+    const double coeff_energy_p = p->u_0 * p->u_0 / (p->cp_mix * p->t_ref);
+    const double scale_p   = 1.0e5 / (p->r_mix * p->u_0 * p->u_0);
+    const double scale_Cor = coriolis_scale(p);
+    const double scale_cen = p->L_atm * p->L_atm / (p->u_0 * p->u_0);
+
+    /* transport (:288-326) */
+    const double v_invrm = v_ijk * inv_rm;
+    const double w_invrs = w_ijk * inv_rmsinthe;
+    double pressure_t = coeff_energy_p * scale_p * (u_ijk * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
+    const double tc = f[ATURAN_T][c];
+    if(p->cp_dyn && tc > 0.0) pressure_t *= p->cp_mix / oracle_cp_lapse(p, tc * p->t_ref);
+    const double transport_t = u_ijk * d1r[ATURAN_T] + v_invrm * d1t[ATURAN_T] + w_invrs * d1p[ATURAN_T];
+    const double metric_on = 0.0, cor_rad_on = 0.0;   /* METRIC_SPLIT = CORIOLIS_SPLIT = 1 */
+    const double transport_u = u_ijk * d1r[ATURAN_U] + v_invrm * d1t[ATURAN_U] + w_invrs * d1p[ATURAN_U]
+        - metric_on * (v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
+    const double transport_v = u_ijk * d1r[ATURAN_V] + v_invrm * d1t[ATURAN_V] + w_invrs * d1p[ATURAN_V]
+        + (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
+    const double transport_w = u_ijk * d1r[ATURAN_W] + v_invrm * d1t[ATURAN_W] + w_invrs * d1p[ATURAN_W]
+        + (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
+
+    /* diffusion (:329-379) */
+    const double two_inv_rm = 2.0 * inv_rm;
+    const double v_metric   = (1.0 + costhe / geo->sinthe2) * inv_rm2;
+    const double diffusion_t = d2r[ATURAN_T] + d1r[ATURAN_T] * two_inv_rm + d2t[ATURAN_T] * inv_rm2
+        + d1t[ATURAN_T] * costhe_inv_rm2sinthe + d2p[ATURAN_T] * inv_rm2sinthe2;
+    const double diffusion_u = d2r[ATURAN_U] + 2.0 * u_ijk * inv_rm2 + d2t[ATURAN_U] * inv_rm2
+        + 4.0 * d1r[ATURAN_U] * inv_rm + d1t[ATURAN_U] * costhe_inv_rm2sinthe
+        + d2p[ATURAN_U] * inv_rm2sinthe2;
+    const double diffusion_v = d2r[ATURAN_V] + d1r[ATURAN_V] * two_inv_rm + d2t[ATURAN_V] * inv_rm2
+        + d1t[ATURAN_V] * costhe_inv_rm2sinthe - v_metric * v_ijk
+        + d2p[ATURAN_V] * inv_rm2sinthe2
+        + 2.0 * d1t[ATURAN_U] * inv_rm2
+        - d1p[ATURAN_W] * 2.0 * costhe * inv_rm2sinthe2;
+    const double diffusion_w = d2r[ATURAN_W] + d1r[ATURAN_W] * two_inv_rm + d2t[ATURAN_W] * inv_rm2
+        + d1t[ATURAN_W] * costhe_inv_rm2sinthe - v_metric * w_ijk
+        + d2p[ATURAN_W] * inv_rm2sinthe2
+        + 2.0 * d1p[ATURAN_U] * inv_rm2sinthe
+        + d1p[ATURAN_V] * 2.0 * costhe * inv_rm2sinthe2;
+
+    const double dpdr_term   = dpdr   * scale_p;
+    const double dpdthe_term = dpdthe * scale_p * inv_rm;
+    const double dpdphi_term = dpdphi * scale_p * inv_rmsinthe;
+
+    const double re = p->re;
+    const double re_eff = re / (1.0 + 2.5 * 0.0);          /* EINSTEIN_VISC = 0 */
+
+    const double nue_c = f[ATURAN_NUE][c];
+    const double nue_t = (p->turb_coupling != 0.0 && isfinite(nue_c))
+                       ? p->turb_coupling * stdmax(0.0, nue_c) : 0.0;
+    const double nue_t_s = nue_t / 0.9;
+
+    const double tmf = p->tmf_scale != 0.0 ? p->tmf_scale * p->chemical_reaction * f[ATURAN_THERMALMASSFLUX][c] : 0.0;
+    double precip_t = 0.0;
+    if(p->precip_coupling != 0.0 && p->r_mix > 0.0 && p->cp_mix > 0.0){
+        precip_t = p->precip_coupling * f[ATURAN_Q_PRECIP][c] * (p->L_atm * 1.0e3) / (p->r_mix * p->cp_mix * p->u_0 * p->t_ref);
+        if(!isfinite(precip_t)) precip_t = 0.0;
+        else if(precip_t >  0.5) precip_t =  0.5;
+        else if(precip_t < -0.5) precip_t = -0.5;
+    }
+    out[ATURAN_T] = + pressure_t - transport_t + diffusion_t / (re * p->pr) + diffusion_t * nue_t_s
+                    - tmf + 0.0 + precip_t;
+
+    /* sponge (:594-595) */
+    const int im = p->im;
+    double frac_sp = (double)(i - (im - 1) * 3 / 4) / (double)((im - 1) / 4);
+    if(frac_sp < 0.0) frac_sp = 0.0;
+    const double sponge = p->alpha_sponge * frac_sp * frac_sp;
+
+    /* hydrostatic split (:717-721) */
+    const double* PH = f[ATURAN_P_HYDRO];
+    const double dphdthe_term = (PH[IDX(i,j+1,k)] - PH[IDX(i,j-1,k)]) * inv_2dthe * inv_rm;
+    const double dphdphi_term = (PH[IDX(i,j,ke)] - PH[IDX(i,j,kw)]) * inv_2dphi * inv_rmsinthe;
+    const double buoyancy_u = 0.0;
+
+    out[ATURAN_U] = - dpdr_term + buoyancy_u - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
+                    - cor_rad_on * p->Coriolis * scale_Cor * Coriolis_rad
+                    + 1.0 * p->centrifugal * cent_mom * scale_cen * centrifugal_rad
+                    - sponge * u_ijk;
+    out[ATURAN_V] = - dpdthe_term - dphdthe_term - transport_v + diffusion_v / re_eff + diffusion_v * nue_t
+                    - p->Coriolis * scale_Cor * Coriolis_the
+                    + 1.0 * p->centrifugal * cent_mom * scale_cen * centrifugal_the;
+    out[ATURAN_W] = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
+                    - p->Coriolis * scale_Cor * Coriolis_phi;
+
+    /* the twelve condensable species (:790-850) */
+    static const int sc_of[12] = {0,0,0, 1,1,1, 2,2,2, 3,3,3};
+    const double scs[4] = { p->sc_ch4, p->sc_h2o, p->sc_h2s, p->sc_nh3 };
+    for(int s = 0; s < 12; s++){
+        const int q = ATURAN_CH4 + s;
+        const double transport = u_ijk * d1r[q] + v_invrm * d1t[q] + w_invrs * d1p[q];
+        const double diffusion = d2r[q] + d1r[q] * two_inv_rm + d2t[q] * inv_rm2
+            + d1t[q] * costhe_inv_rm2sinthe + d2p[q] * inv_rm2sinthe2;
+        const double sc = scs[sc_of[s]];
+        double r = - transport + diffusion / (sc * re) + diffusion * nue_t_s;
+        if(q == ATURAN_H2S) r = r + p->chemical_reaction * f[ATURAN_MASSFLUX_H2S][c];
+        if(q == ATURAN_NH3) r = r + p->chemical_reaction * f[ATURAN_MASSFLUX_NH3][c];
+        out[q] = r + p->precip_coupling * f[SP_SPRECIP[s]][c];
+    }
+
+    /* NH4SH with flux limiter and Stokes settling (:857-913) */
+    {
+        const int q = ATURAN_NH4SH;
+        const double transport = u_ijk * d1r[q] + v_invrm * d1t[q] + w_invrs * d1p[q];
+        const double diffusion = d2r[q] + d1r[q] * two_inv_rm + d2t[q] * inv_rm2
+            + d1t[q] * costhe_inv_rm2sinthe + d2p[q] * inv_rm2sinthe2;
+        const double v_stokes = (2.0 / 9.0) * p->r_p_nh4sh * p->r_p_nh4sh
+            * (p->rho_cond_nh4sh - f[ATURAN_RHO_MIX][c]) * p->g / p->mue_mix;
+        out[q] = - transport + f[ATURAN_FLUXLIM_NH4SH][c]
+                 + diffusion / (p->sc_nh4sh * re) + diffusion * nue_t_s
+                 + p->chemical_reaction * f[ATURAN_MASSFLUX_NH4SH][c]
+                 + (v_stokes / p->u_0) * d1r[q];
+    }
+
+    /* k* and dis* (:989-1018) */
+    if(p->turb_active){
+        const double sig_k = 0.85, sig_w = 0.5;
+        const double nue_here = nue_c;
+        const int qt = ATURAN_TKE, qd = ATURAN_DIS;
+        const double transport_tke = u_ijk * d1r[qt] + v_ijk * d1t[qt] * inv_rm + w_ijk * d1p[qt] * inv_rmsinthe;
+        const double transport_dis = u_ijk * d1r[qd] + v_ijk * d1t[qd] * inv_rm + w_ijk * d1p[qd] * inv_rmsinthe;
+        const double diffusion_tke = d2r[qt] + d1r[qt] * 2.0 * inv_rm + d2t[qt] * inv_rm2
+            + d1t[qt] * costhe_inv_rm2sinthe + d2p[qt] * inv_rm2sinthe2;
+        const double diffusion_dis = d2r[qd] + d1r[qd] * 2.0 * inv_rm + d2t[qd] * inv_rm2
+            + d1t[qd] * costhe_inv_rm2sinthe + d2p[qd] * inv_rm2sinthe2;
+        out[qt] = - transport_tke + diffusion_tke * (1.0 / re + nue_here / sig_k) + f[ATURAN_TKE_SOURCE][c];
+        out[qd] = - transport_dis + diffusion_dis * (1.0 / re + nue_here / sig_w) + f[ATURAN_DIS_SOURCE][c];
+    } else {
+        out[ATURAN_TKE] = 0.0;
+        out[ATURAN_DIS] = 0.0;
+    }
+
+    out[19] = out[ATURAN_U] + dpdr_term;   /* aux_u (:1020-1022) */
+    out[20] = out[ATURAN_V] + dpdthe_term;
+    out[21] = out[ATURAN_W] + dpdphi_term;
+}
+
+int oracle_rhs_cell(const aturan_params* p, double* const* f, int i, int j, int k, double* rhs22){
+    double rad[256], the[4096];
+    if(p->im > 256 || p->jm > 4096) return -1;
+    oracle_coords(p, rad, the);
+    geo_t g; geo_fill(p, rad, the, i, j, &g);
+    rhs_cell(p, f, i, j, k, &g, rhs22);
+    return 0;
+}
+
+static double clampd(double v, double lo, double hi){ return v < lo ? lo : (v > hi ? hi : v); }
+
+
+/* ---- RungeKutta_Uran_Turb.cpp:179-404, RungeKuttaUran ---- */
+int oracle_rk4(const aturan_params* p, double* const* f, double* ref_out){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const size_t N = (size_t)im * jm * km;
+    double ref[512];
+    if(im > 512) return -1;
+    oracle_buoy_ref(p, f, ref);
+    oracle_hydro(p, f, ref, 1);
+    if(ref_out) memcpy(ref_out, ref, sizeof(double) * im);
+
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    double* rhs = (double*)malloc(sizeof(double) * N * NPROG);
+    double* acc = (double*)malloc(sizeof(double) * N * NPROG);
+    if(!rhs || !acc){ free(rhs); free(acc); free(rad); free(the); return -1; }
+
+    const int turb = p->turb_active;
+    const double tke_max_nd = 1000.0 / (p->u_0 * p->u_0);
+    const double dis_min_nd = 1.0e-10;
+    const double t_min = p->t_min_K / p->t_ref, t_max = p->t_max_K / p->t_ref;
+    const double dt = p->dt;
+
+    for(int stage = 0; stage < 4; stage++){
+        const double c_in = (stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0);
+        const double wgt  = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+        /* pass A */
+        #pragma omp parallel for collapse(2) schedule(static)
+        for(int i = 1; i < im-1; i++){
+            for(int j = 1; j < jm-1; j++){
+                geo_t g; geo_fill(p, rad, the, i, j, &g);
+                double out[22];
+                for(int k = 0; k < km-1; k++){
+                    rhs_cell(p, f, i, j, k, &g, out);
+                    const size_t c = IDX(i,j,k);
+                    for(int q = 0; q < NPROG; q++) rhs[(size_t)q * N + c] = out[q];
+                    f[ATURAN_RHS_U][c] = out[ATURAN_U];
+                    f[ATURAN_RHS_V][c] = out[ATURAN_V];
+                    f[ATURAN_RHS_W][c] = out[ATURAN_W];
+                    f[ATURAN_AUX_U][c] = out[19];
+                    f[ATURAN_AUX_V][c] = out[20];
+                    f[ATURAN_AUX_W][c] = out[21];
+                }
+            }
+        }
+        /* pass B */
+        #pragma omp parallel for collapse(2) schedule(static)
+        for(int i = 1; i < im-1; i++){
+            for(int j = 1; j < jm-1; j++){
+                for(int k = 0; k < km-1; k++){
+                    const size_t c = IDX(i,j,k);
+                    const int nq = turb ? NPROG : NPROG - 2;
+                    for(int q = 0; q < nq; q++){
+                        double* A = acc + (size_t)q * N;
+                        const double r = rhs[(size_t)q * N + c];
+                        A[c] = (stage == 0) ? wgt * r : A[c] + wgt * r;
+                    }
+                    if(stage < 3){
+                        for(int q = 0; q < NPROG - 2; q++)
+                            f[q][c] = f[ATURAN_TN + q][c] + c_in * rhs[(size_t)q * N + c];
+                        if(turb){
+                            f[ATURAN_TKE][c] = clampd(f[ATURAN_TKEN][c] + c_in * rhs[(size_t)ATURAN_TKE * N + c],
+                                                      0.0, tke_max_nd);
+                            const double d_ = f[ATURAN_DISN][c] + c_in * rhs[(size_t)ATURAN_DIS * N + c];
+                            f[ATURAN_DIS][c] = stdmax(d_, dis_min_nd);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    /* the step (:371-403) */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            for(int k = 0; k < km-1; k++){
+                const size_t c = IDX(i,j,k);
+                f[ATURAN_T][c] = clampd(f[ATURAN_TN][c] + dt * acc[c] / 6.0, t_min, t_max);
+                for(int q = 1; q < NPROG - 2; q++)
+                    f[q][c] = f[ATURAN_TN + q][c] + dt * acc[(size_t)q * N + c] / 6.0;
+                if(turb){
+                    double x = f[ATURAN_TKEN][c] + dt * acc[(size_t)ATURAN_TKE * N + c] / 6.0;
+                    x = stdmax(x, 0.0);
+                    f[ATURAN_TKE][c] = clampd(x, 0.0, tke_max_nd);
+                    const double d_ = f[ATURAN_DISN][c] + dt * acc[(size_t)ATURAN_DIS * N + c] / 6.0;
+                    f[ATURAN_DIS][c] = stdmax(d_, dis_min_nd);
+                }
+            }
+        }
+    }
+    free(rhs); free(acc); free(rad); free(the);
+    return 0;
+}
+
+/* The sin table of both pressure solvers: sin(theta) floored at sinthe_min(), no fabs
+ * (PressureSolverUran.h:42-47; PressureSolver.h:156-162 adds the exact-zero guard). */
+static void press_sin_table(const aturan_params* p, const double* the, double* s, int shared){
+    for(int j = 0; j < p->jm; j++){
+        s[j] = sin(the[j]);
+        if(s[j] < p->sinthe_min) s[j] = p->sinthe_min;
+        if(shared && s[j] == 0.0) s[j] = 1.0e-5;
+    }
+}
+
+/* p_dyn boundary passes shared by both solvers: r, then theta, then the periodic phi copy
+ * (PressureSolverUran.h:213-244; PressureSolver.h:718-746). */
+static void p_dyn_bcs(const aturan_params* p, double* P){
+    const int im = p->im, jm = p->jm, km = p->km;
+    #pragma omp parallel for collapse(2)
+    for(int k = 0; k < km; k++) for(int j = 0; j < jm; j++){
+        P[IDX(0,j,k)]    = C43 * P[IDX(1,j,k)]    - C13 * P[IDX(2,j,k)];
+        P[IDX(im-1,j,k)] = C43 * P[IDX(im-2,j,k)] - C13 * P[IDX(im-3,j,k)];
+    }
+    #pragma omp parallel for collapse(2)
+    for(int k = 0; k < km; k++) for(int i = 0; i < im; i++){
+        P[IDX(i,0,k)]    = C43 * P[IDX(i,1,k)]    - C13 * P[IDX(i,2,k)];
+        P[IDX(i,jm-1,k)] = C43 * P[IDX(i,jm-2,k)] - C13 * P[IDX(i,jm-3,k)];
+    }
+    #pragma omp parallel for collapse(2)
+    for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++)
+        P[IDX(i,j,km-1)] = P[IDX(i,j,0)];
+}
+
+/* ---- PressureSolverUran.h:33-250, the default solver: one serial lexicographic sweep ---- */
+int oracle_pressure_gs(const aturan_params* p, double* const* f){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 0);
+    const int consistent = p->press_consistent;
+    const double src_scale = consistent ? (p->r_mix * p->u_0 * p->u_0) / 1.0e5 : 1.0;
+    double* au = f[ATURAN_AUX_U]; double* av = f[ATURAN_AUX_V]; double* aw = f[ATURAN_AUX_W];
+    double* P = f[ATURAN_P_DYN];
+
+    /* aux radial BC (:70-81) */
+    #pragma omp parallel for collapse(2)
+    for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++){
+        au[IDX(0,j,k)]    = C43 * au[IDX(1,j,k)]    - C13 * au[IDX(2,j,k)];
+        au[IDX(im-1,j,k)] = C43 * au[IDX(im-2,j,k)] - C13 * au[IDX(im-3,j,k)];
+        av[IDX(0,j,k)]    = C43 * av[IDX(1,j,k)]    - C13 * av[IDX(2,j,k)];
+        av[IDX(im-1,j,k)] = C43 * av[IDX(im-2,j,k)] - C13 * av[IDX(im-3,j,k)];
+        aw[IDX(0,j,k)]    = C43 * aw[IDX(1,j,k)]    - C13 * aw[IDX(2,j,k)];
+        aw[IDX(im-1,j,k)] = C43 * aw[IDX(im-2,j,k)] - C13 * aw[IDX(im-3,j,k)];
+    }
+    const double inv_2dr = 1.0 / (2.0 * p->dr), inv_2dthe = 1.0 / (2.0 * p->dthe), inv_2dphi = 1.0 / (2.0 * p->dphi);
+    const double inv_dr2 = 1.0 / (p->dr * p->dr), inv_dthe2 = 1.0 / (p->dthe * p->dthe), inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+
+    /* defect-correction source (:139-175) */
+    double* incr = NULL;
+    const size_t N = (size_t)im * jm * km;
+    if(p->press_incr){
+        incr = (double*)calloc(N, sizeof(double));
+        const double* ru_u = f[ATURAN_RHS_U]; const double* ru_v = f[ATURAN_RHS_V]; const double* ru_w = f[ATURAN_RHS_W];
+        #pragma omp parallel for collapse(2) schedule(static)
+        for(int i = 1; i < im-1; i++){
+            for(int j = 1; j < jm-1; j++){
+                const double rm = consistent ? metric_radius(p, rad[i]) : rad[i];
+                const double inv_rm = 1.0 / rm;
+                const double inv_rmsinthe = 1.0 / (rm * st[j]);
+                const double inv_rm2 = inv_rm * inv_rm;
+                const double inv_rm2sinthe2 = inv_rm2 / (st[j] * st[j]);
+                const double num1 = 1.0 / (p->dr * p->dr), num2 = inv_rm2 / (p->dthe * p->dthe),
+                             num3 = inv_rm2sinthe2 / (p->dphi * p->dphi);
+                const double denom = 2.0 * (num1 + num2 + num3);
+                for(int k = 0; k < km-1; k++){
+                    const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                    #define RU(A, ii, jj, kk) ((ii) == 0 ? C43 * A[IDX(1,jj,kk)] - C13 * A[IDX(2,jj,kk)] : \
+                        ((ii) == im-1 ? C43 * A[IDX(im-2,jj,kk)] - C13 * A[IDX(im-3,jj,kk)] : A[IDX(ii,jj,kk)]))
+                    const double div_rhs =
+                          (RU(ru_u, i+1, j, k) - RU(ru_u, i-1, j, k)) / (2.0 * p->dr)
+                        + (RU(ru_v, i, j+1, k) - RU(ru_v, i, j-1, k)) / (2.0 * p->dthe) * inv_rm
+                        + (RU(ru_w, i, j, ke)  - RU(ru_w, i, j, kw))  / (2.0 * p->dphi) * inv_rmsinthe;
+                    #undef RU
+                    const double lc_old =
+                          (P[IDX(i+1,j,k)] + P[IDX(i-1,j,k)]) * num1
+                        + (P[IDX(i,j+1,k)] + P[IDX(i,j-1,k)]) * num2
+                        + (P[IDX(i,j,ke)]  + P[IDX(i,j,kw)])  * num3
+                        - denom * P[IDX(i,j,k)];
+                    incr[IDX(i,j,k)] = src_scale * div_rhs + lc_old;
+                }
+            }
+        }
+    }
+
+    /* the serial sweep (:177-211) */
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            const double rm = consistent ? metric_radius(p, rad[i]) : rad[i];
+            const double rm2 = rm * rm;
+            const double sinthe = st[j];
+            const double inv_rm = 1.0 / rm;
+            const double inv_rm2 = 1.0 / rm2;
+            const double inv_rmsinthe = 1.0 / (rm * sinthe);
+            const double inv_rm2sinthe2 = inv_rm2 / (sinthe * sinthe);
+            const double denom = 2.0 * inv_dr2 + 2.0 * inv_rm2 * inv_dthe2 + 2.0 * inv_rm2sinthe2 * inv_dphi2;
+            const double inv_denom = 1.0 / denom;
+            const double num1 = inv_dr2, num2 = inv_rm2 * inv_dthe2, num3 = inv_rm2sinthe2 * inv_dphi2;
+            for(int k = 0; k < km-1; k++){
+                const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                double src;
+                if(incr) src = incr[IDX(i,j,k)];
+                else {
+                    const double du_dr   = (au[IDX(i+1,j,k)] - au[IDX(i-1,j,k)]) * inv_2dr;
+                    const double dv_dthe = (av[IDX(i,j+1,k)] - av[IDX(i,j-1,k)]) * inv_2dthe * inv_rm;
+                    const double dw_dphi = (aw[IDX(i,j,ke)] - aw[IDX(i,j,kw)]) * inv_2dphi * inv_rmsinthe;
+                    src = src_scale * (du_dr + dv_dthe + dw_dphi);
+                }
+                P[IDX(i,j,k)] =
+                    ((P[IDX(i+1,j,k)] + P[IDX(i-1,j,k)]) * num1
+                   + (P[IDX(i,j+1,k)] + P[IDX(i,j-1,k)]) * num2
+                   + (P[IDX(i,j,ke)] + P[IDX(i,j,kw)]) * num3
+                   - src) * inv_denom;
+            }
+        }
+    }
+    p_dyn_bcs(p, P);
+    free(incr); free(rad); free(the); free(st);
+    return 0;
+}
+
+/* ---- Pressure_Uran.cpp:30-146, prepareProjectionBoundaries, periodic phi ---- */
+static void prepare_projection_boundaries(const aturan_params* p, double* const* f){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* A[6] = { f[ATURAN_AUX_U], f[ATURAN_AUX_V], f[ATURAN_AUX_W],
+                     f[ATURAN_RHS_U], f[ATURAN_RHS_V], f[ATURAN_RHS_W] };
+    #define CUB0(X, jj, kk) (X[IDX(3,jj,kk)] - 3.0 * X[IDX(2,jj,kk)] + 3.0 * X[IDX(1,jj,kk)])
+    #define CUB1(X, jj, kk) (X[IDX(im-4,jj,kk)] - 3.0 * X[IDX(im-3,jj,kk)] + 3.0 * X[IDX(im-2,jj,kk)])
+    #pragma omp parallel for
+    for(int j = 1; j < jm-1; j++){
+        for(int k = 0; k < km-1; k++){
+            if(p->rigid_lid){ A[0][IDX(0,j,k)] = 0.0; A[0][IDX(im-1,j,k)] = 0.0; }
+            else { A[0][IDX(0,j,k)] = CUB0(A[0], j, k); A[0][IDX(im-1,j,k)] = CUB1(A[0], j, k); }
+            for(int q = 1; q < 6; q++){
+                A[q][IDX(0,j,k)]    = CUB0(A[q], j, k);
+                A[q][IDX(im-1,j,k)] = CUB1(A[q], j, k);
+            }
+        }
+    }
+    #undef CUB0
+    #undef CUB1
+    #define CUBJ0(X, ii, kk) (X[IDX(ii,3,kk)] - 3.0 * X[IDX(ii,2,kk)] + 3.0 * X[IDX(ii,1,kk)])
+    #define CUBJ1(X, ii, kk) (X[IDX(ii,jm-4,kk)] - 3.0 * X[IDX(ii,jm-3,kk)] + 3.0 * X[IDX(ii,jm-2,kk)])
+    #pragma omp parallel for
+    for(int k = 0; k < km-1; k++){
+        for(int i = 1; i < im-1; i++){
+            A[0][IDX(i,0,k)] = CUBJ0(A[0], i, k);
+            A[1][IDX(i,0,k)] = 0.0;
+            A[2][IDX(i,0,k)] = 0.0;
+            A[0][IDX(i,jm-1,k)] = CUBJ1(A[0], i, k);
+            A[1][IDX(i,jm-1,k)] = 0.0;
+            A[2][IDX(i,jm-1,k)] = 0.0;
+            A[3][IDX(i,0,k)] = CUBJ0(A[3], i, k);
+            A[4][IDX(i,0,k)] = 0.0;
+            A[5][IDX(i,0,k)] = 0.0;
+            A[3][IDX(i,jm-1,k)] = CUBJ1(A[3], i, k);
+            A[4][IDX(i,jm-1,k)] = 0.0;
+            A[5][IDX(i,jm-1,k)] = 0.0;
+        }
+    }
+    #undef CUBJ0
+    #undef CUBJ1
+    #pragma omp parallel for
+    for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++)
+        for(int q = 0; q < 6; q++) A[q][IDX(i,j,km-1)] = A[q][IDX(i,j,0)];
+}
+
+/* The shared solver's per-(i,j) weights (PressureSolver.h:326-353). */
+typedef struct { double num1, num2, num3, den, inv_rm, inv_rmsinthe; } pweights_t;
+static void press_weights(const aturan_params* p, const double* rad, const double* st, int i, int j, pweights_t* w){
+    const double rm = metric_radius(p, rad[i]);
+    const double rm2 = rm * rm;
+    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
+    const double sinthe2 = st[j] * st[j];
+    const double inv_rm2 = 1.0 / rm2;
+    const double inv_rm2sinthe2 = inv_rm2 / sinthe2;
+    const double inv_dr2 = 1.0 / (p->dr * p->dr), inv_dthe2 = 1.0 / (p->dthe * p->dthe), inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+    w->num1 = exp_2_rm * inv_dr2;
+    w->num2 = inv_rm2 * inv_dthe2;
+    w->num3 = inv_rm2sinthe2 * inv_dphi2;
+    w->den  = 2.0 * w->num1 + 2.0 * w->num2 + 2.0 * w->num3;
+    w->inv_rm = 1.0 / rm;
+    w->inv_rmsinthe = 1.0 / (rm * st[j]);
+}
+
+/* The shared solver's source: div(aux) with centred differences, the clamp at den*p_dyn_cap and
+ * the non-finite guard (PressureSolver.h:370-487, no obstacle, PRESS_SRC=1, PRESS_INCR=0).
+ * Runs prepare_projection_boundaries first, as run() does (:208). */
+int oracle_pressure_source(const aturan_params* p, double* const* f, double* src){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    prepare_projection_boundaries(p, f);
+    const double* au = f[ATURAN_AUX_U]; const double* av = f[ATURAN_AUX_V]; const double* aw = f[ATURAN_AUX_W];
+    const double inv_2dr = 1.0 / (2.0 * p->dr), inv_2dthe = 1.0 / (2.0 * p->dthe), inv_2dphi = 1.0 / (2.0 * p->dphi);
+    memset(src, 0, sizeof(double) * (size_t)im * jm * km);
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            pweights_t w; press_weights(p, rad, st, i, j, &w);
+            for(int k = 0; k < km-1; k++){
+                const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                const double du_dr   = (au[IDX(i+1,j,k)] - au[IDX(i-1,j,k)]) * inv_2dr;
+                const double dv_dthe = (av[IDX(i,j+1,k)] - av[IDX(i,j-1,k)]) * inv_2dthe;
+                const double dw_dphi = (aw[IDX(i,j,ke)] - aw[IDX(i,j,kw)]) * inv_2dphi;
+                double div_src = du_dr * 1.0 + dv_dthe * w.inv_rm + dw_dphi * w.inv_rmsinthe;
+                const double src_max = w.den * p->p_dyn_cap;
+                if      (!isfinite(div_src)) div_src = 0.0;
+                else if (div_src >  src_max) div_src =  src_max;
+                else if (div_src < -src_max) div_src = -src_max;
+                src[IDX(i,j,k)] = div_src;
+            }
+        }
+    }
+    free(rad); free(the); free(st);
+    return 0;
+}
+
+/* One red-black colour pass of PressureSolver.h:320-495 at relaxation factor omega (omega = 1
+ * is the reference's update p = (acc - src) / den exactly). */
+static void rb_colour(const aturan_params* p, const double* rad, const double* st, double* P,
+                      const double* src, int colour, double omega){
+    const int im = p->im, jm = p->jm, km = p->km;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            pweights_t w; press_weights(p, rad, st, i, j, &w);
+            for(int k = 0; k < km-1; k++){
+                if(((i + j + k) & 1) != colour) continue;
+                const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                const double acc = (P[IDX(i+1,j,k)] + P[IDX(i-1,j,k)]) * w.num1
+                                 + (P[IDX(i,j+1,k)] + P[IDX(i,j-1,k)]) * w.num2
+                                 + (P[IDX(i,j,ke)] + P[IDX(i,j,kw)]) * w.num3;
+                const double pn = (acc - src[IDX(i,j,k)]) / w.den;
+                if(omega == 1.0) P[IDX(i,j,k)] = pn;
+                else P[IDX(i,j,k)] = P[IDX(i,j,k)] + omega * (pn - P[IDX(i,j,k)]);
+            }
+        }
+    }
+}
+
+/* ---- PressureSolver.h:145-766 with ATURAN_PRESS_SWEEPS = sweeps (no line, no barotropic) ---- */
+int oracle_pressure_rb(const aturan_params* p, double* const* f, int sweeps){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    double* src = (double*)malloc(sizeof(double) * (size_t)im * jm * km);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    oracle_pressure_source(p, f, src);
+    if(sweeps < 1) sweeps = 1;
+    for(int s = 0; s < sweeps; s++){
+        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 0, 1.0);
+        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 1, 1.0);
+        p_dyn_bcs(p, f[ATURAN_P_DYN]);
+    }
+    free(rad); free(the); free(st); free(src);
+    return 0;
+}
+
+/* Relative L2 residual ||src - Lc p|| / ||src|| over the interior rows, with Lc the shared
+ * solver's compact operator on the current (boundary-folded) p_dyn. */
+double oracle_pressure_residual(const aturan_params* p, double* const* f, const double* src){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    const double* P = f[ATURAN_P_DYN];
+    double rr = 0.0, ss = 0.0;
+    #pragma omp parallel for collapse(2) reduction(+:rr,ss) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            pweights_t w; press_weights(p, rad, st, i, j, &w);
+            for(int k = 0; k < km-1; k++){
+                const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                const double lc = (P[IDX(i+1,j,k)] + P[IDX(i-1,j,k)]) * w.num1
+                                + (P[IDX(i,j+1,k)] + P[IDX(i,j-1,k)]) * w.num2
+                                + (P[IDX(i,j,ke)] + P[IDX(i,j,kw)]) * w.num3 - w.den * P[IDX(i,j,k)];
+                const double r = src[IDX(i,j,k)] - lc;
+                rr += r * r; ss += src[IDX(i,j,k)] * src[IDX(i,j,k)];
+            }
+        }
+    }
+    free(rad); free(the); free(st);
+    return ss > 0.0 ? sqrt(rr / ss) : sqrt(rr);
+}
+
+/* Red-black SOR on the shared solver's equation to a relative residual (no reference oracle:
+ * this is the restatement the GPU to-residual solver is checked against). The source is made
+ * compatible with the all-Neumann operator by removing its component along the left null vector
+ * y = a(i) b(j), a = b = (3/2, 1, ..., 1, 3/2) (PressureSolver.h:63-65 states it for theta; the
+ * radial fold has the same form), using a constant shift. */
+int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, int max_sweeps,
+                        double tol, int check_every, int* sweeps_done, double* resid){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    double* src = (double*)malloc(sizeof(double) * (size_t)im * jm * km);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    oracle_pressure_source(p, f, src);
+    double ys = 0.0, yy = 0.0;
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++){
+        const double yi = (i == 1 || i == im-2) ? 1.5 : 1.0, yj = (j == 1 || j == jm-2) ? 1.5 : 1.0;
+        for(int k = 0; k < km-1; k++){ ys += yi * yj * src[IDX(i,j,k)]; yy += yi * yj; }
+    }
+    const double shift = ys / yy;
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++)
+        src[IDX(i,j,k)] -= shift;
+    if(check_every < 1) check_every = 1;
+    int s = 0; double r = oracle_pressure_residual(p, f, src);
+    while(s < max_sweeps && !(r <= tol)){
+        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 0, omega);
+        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 1, omega);
+        p_dyn_bcs(p, f[ATURAN_P_DYN]);
+        s++;
+        if(s % check_every == 0 || s == max_sweeps) r = oracle_pressure_residual(p, f, src);
+    }
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    free(rad); free(the); free(st); free(src);
+    return r <= tol ? 0 : 1;
+}
+
+/* ---- SaturationAdjustment.h:255-746 for one gas, the non-diagnostic arithmetic ---- */
+int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adjusted, long* n_noconv){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const aturan_gas* G = &p->gas[gas];
+    static const int base[4] = { ATURAN_H2O, ATURAN_H2S, ATURAN_NH3, ATURAN_CH4 };
+    double* c = f[base[gas]]; double* cloud = f[base[gas] + 1]; double* ice = f[base[gas] + 2];
+    double* tt = f[ATURAN_T];
+    const double* ps = f[ATURAN_P_STAT];
+    const double* rho_mix = f[ATURAN_RHO_MIX];
+    const double t_0 = G->t_0, t_00 = G->t_00, ep = G->ep, lv = G->lv, ls = G->ls;
+    const double C = G->C, L0 = G->L0, R = G->R, del_alf = G->del_alf, del_bet = G->del_bet;
+    const double C_i = G->C_i, L0_i = G->L0_i, del_alf_i = G->del_alf_i, del_bet_i = G->del_bet_i;
+    const double t_range_inv = 1.0 / (t_0 - t_00);
+    const int conserve = p->satadj_conserve, newton = p->satadj_newton, evap = p->satadj_evap;
+    const int ice_entry = p->satadj_ice_entry, bergeron = p->satadj_bergeron;
+    const int freeze_on = p->satadj_freeze && conserve && t_00 > 0.0 && t_00 < t_0;
+    const int dry_exit = p->satadj_dry_exit;
+    const double Lf = ls - lv;
+    const double cp_mix = p->cp_mix, t_ref = p->t_ref;
+    const int iter_prec_end = 15;
+    const double q_diff_min = 1.0e-3;
+    long nadj = 0, nnc = 0;
+
+    #pragma omp parallel for collapse(2) schedule(static) reduction(+:nadj,nnc)
+    for(int k = 0; k < km; k++){
+        for(int j = 0; j < jm; j++){
+            for(int i = 0; i < im; i++){
+                const size_t q = IDX(i,j,k);
+                double t_u = tt[q] * t_ref;
+                const double p_u = ps[q];
+                if(!(t_u > 0.0) || !(p_u > 0.0)) continue;
+                /* rho_at (cUranusModel.h:526-531) */
+                double rho_c = p->r_mix;
+                if(p->local_rho){ const double r_ = rho_mix[q]; rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : p->r_mix; }
+
+                if(t_u > t_0){
+                    if(conserve){
+                        if(ice[q] > 0.0){
+                            double dm = ice[q];
+                            if(Lf > 0.0){
+                                const double hc  = cp_mix * rho_c;
+                                const double cap = hc * (t_u - t_0) / Lf;
+                                if(dm > cap) dm = cap;
+                                t_u -= Lf * dm / hc;
+                                tt[q] = t_u / t_ref;
+                            }
+                            ice[q]   -= dm;
+                            cloud[q] += dm;
+                        }
+                    } else {
+                        ice[q] = 0.0;
+                    }
+                }
+                if(freeze_on && t_u < t_00 && cloud[q] > 0.0){
+                    double dm = cloud[q];
+                    if(Lf > 0.0){
+                        const double hc  = cp_mix * rho_c;
+                        const double cap = hc * (t_00 - t_u) / Lf;
+                        if(dm > cap) dm = cap;
+                        t_u += Lf * dm / hc;
+                        tt[q] = t_u / t_ref;
+                    }
+                    cloud[q] -= dm;
+                    ice[q]   += dm;
+                }
+                if(c[q]     < 0.0) c[q]     = 0.0;
+                if(cloud[q] < 0.0) cloud[q] = 0.0;
+                if(ice[q]   < 0.0) ice[q]   = 0.0;
+
+                const double E_Rain_0 = svp(t_u, C, L0, R, del_alf, del_bet);
+                const double q_Rain_0 = rho_c * ep * E_Rain_0 / p_u;
+                if(q_Rain_0 <= 0.0) continue;
+                double q_entry = q_Rain_0;
+                if(ice_entry && cloud[q] <= 0.0 && ice[q] <= 0.0){
+                    const double cnd0 = t_u <= t_00 ? 0.0 : (t_u >= t_0 ? 1.0 : (t_u - t_00) * t_range_inv);
+                    if(cnd0 < 1.0)
+                        q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * rho_c * ep
+                                * svp(t_u, C_i, L0_i, R, del_alf_i, del_bet_i) / p_u;
+                }
+                if(bergeron >= 2 && cloud[q] <= 0.0 && ice[q] <= 0.0 && t_u < t_0)
+                    q_entry = rho_c * ep * svp(t_u, C_i, L0_i, R, del_alf_i, del_bet_i) / p_u;
+                if(c[q] <= q_entry){
+                    const double q_c0 = cloud[q], q_i0 = ice[q];
+                    if(!evap || !conserve || (q_c0 <= 0.0 && q_i0 <= 0.0)) continue;
+                    const double q_Ice_0 = rho_c * ep * svp(t_u, C_i, L0_i, R, del_alf_i, del_bet_i) / p_u;
+                    double q_t0;
+                    if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
+                    else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
+                    else                         q_t0 = q_Ice_0;
+                    if(fabs(c[q] - q_t0) <= q_diff_min * q_t0) continue;
+                }
+
+                double q_v_b = c[q], q_c_b = cloud[q], q_i_b = ice[q];
+                double T = t_u, q_v_hyp = q_v_b;
+                int cell_found = 0, cell_dry = 0;
+                double q_rain_now = q_Rain_0;
+                for(int itr = 1; itr <= iter_prec_end; itr++){
+                    double CND = (T - t_00) * t_range_inv;
+                    double DEP = (t_0 - T)  * t_range_inv;
+                    if(T <= t_00){ CND = 0.0; DEP = 1.0; }
+                    if(T >= t_0) { CND = 1.0; DEP = 0.0; }
+                    const int berg = bergeron != 0 && T < t_0 && q_v_b <= q_rain_now
+                                   && (q_i_b > 0.0 || (bergeron >= 2 && q_c_b <= 0.0));
+                    if(berg){
+                        CND = 0.0; DEP = 1.0;
+                        if(q_c_b > 0.0){
+                            T     -= lv * q_c_b / (cp_mix * rho_c);
+                            q_v_b += q_c_b;
+                            q_c_b  = 0.0;
+                        }
+                    }
+                    double d_q_v = q_v_hyp - q_v_b;
+                    double d_q_c = -d_q_v * CND;
+                    double d_q_i = -d_q_v * DEP;
+                    if(conserve){
+                        if(d_q_v < -q_v_b){ d_q_v = -q_v_b; d_q_c = -d_q_v * CND; d_q_i = -d_q_v * DEP; }
+                        if(q_c_b + d_q_c < 0.0){ const double ex = -(q_c_b + d_q_c); d_q_c = -q_c_b; d_q_i -= ex; }
+                        if(q_i_b + d_q_i < 0.0){ const double ex = -(q_i_b + d_q_i); d_q_i = -q_i_b; d_q_c -= ex;
+                                                 if(q_c_b + d_q_c < 0.0) d_q_c = -q_c_b; }
+                        d_q_v = -(d_q_c + d_q_i);
+                    }
+                    T     += (lv * d_q_c + ls * d_q_i) / (cp_mix * rho_c);
+                    q_v_b += d_q_v;
+                    q_c_b += d_q_c;
+                    q_i_b += d_q_i;
+                    if(q_v_b < 0.0) q_v_b = 0.0;
+                    if(q_c_b < 0.0) q_c_b = 0.0;
+                    if(q_i_b < 0.0) q_i_b = 0.0;
+
+                    const double E_Rain = svp(T, C,   L0,   R, del_alf,   del_bet);
+                    const double E_Ice  = svp(T, C_i, L0_i, R, del_alf_i, del_bet_i);
+                    const double q_Rain = rho_c * ep * E_Rain / p_u;
+                    const double q_Ice  = rho_c * ep * E_Ice  / p_u;
+                    q_rain_now = q_Rain;
+                    if(q_c_b > 0.0 && q_i_b > 0.0)
+                        q_v_hyp = (q_c_b * q_Rain + q_i_b * q_Ice) / (q_c_b + q_i_b);
+                    else if(bergeron >= 2 && q_c_b <= 0.0 && q_i_b <= 0.0 && T < t_0) q_v_hyp = q_Ice;
+                    else if(ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0){
+                        const double cn = T <= t_00 ? 0.0 : (T >= t_0 ? 1.0 : (T - t_00) * t_range_inv);
+                        q_v_hyp = cn * q_Rain + (1.0 - cn) * q_Ice; }
+                    else if(q_i_b == 0.0) q_v_hyp = q_Rain;
+                    else                  q_v_hyp = q_Ice;
+
+                    if(T >= t_0){
+                        if(conserve){
+                            if(q_i_b > 0.0){
+                                double dm = q_i_b;
+                                if(Lf > 0.0){
+                                    const double hc  = cp_mix * rho_c;
+                                    const double cap = hc * (T - t_0) / Lf;
+                                    if(dm > cap) dm = cap;
+                                    T -= Lf * dm / hc;
+                                }
+                                q_i_b -= dm;
+                                q_c_b += dm;
+                            }
+                        } else {
+                            q_i_b = 0.0;
+                        }
+                    }
+                    const double q_diff = fabs(q_v_b - q_v_hyp) / (q_v_hyp + 1e-20);
+                    if(q_diff <= q_diff_min){ cell_found = 1; break; }
+                    if(dry_exit && conserve && q_c_b <= 0.0 && q_i_b <= 0.0 && q_v_b < q_v_hyp){ cell_dry = 1; break; }
+                    if(newton){
+                        const double dT = 0.1;
+                        const double q_Rain_d = rho_c * ep * svp(T + dT, C,   L0,   R, del_alf,   del_bet)   / p_u;
+                        const double q_Ice_d  = rho_c * ep * svp(T + dT, C_i, L0_i, R, del_alf_i, del_bet_i) / p_u;
+                        double q_hyp_d;
+                        if(q_c_b > 0.0 && q_i_b > 0.0)
+                            q_hyp_d = (q_c_b * q_Rain_d + q_i_b * q_Ice_d) / (q_c_b + q_i_b);
+                        else if(bergeron >= 2 && q_c_b <= 0.0 && q_i_b <= 0.0 && T < t_0) q_hyp_d = q_Ice_d;
+                        else if(ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0){
+                            const double cn = T <= t_00 ? 0.0 : (T >= t_0 ? 1.0 : (T - t_00) * t_range_inv);
+                            q_hyp_d = cn * q_Rain_d + (1.0 - cn) * q_Ice_d; }
+                        else if(q_i_b == 0.0) q_hyp_d = q_Rain_d;
+                        else                  q_hyp_d = q_Ice_d;
+                        double CNDn = (T - t_00) * t_range_inv;
+                        if(T <= t_00) CNDn = 0.0;
+                        if(T >= t_0)  CNDn = 1.0;
+                        if(berg)      CNDn = 0.0;
+                        const double Gf = (lv * CNDn + ls * (1.0 - CNDn)) / (cp_mix * rho_c)
+                                        * (q_hyp_d - q_v_hyp) / dT;
+                        double wn = 1.0 / (1.0 + stdmax(Gf, 0.0));
+                        if(wn < 0.05) wn = 0.05;
+                        q_v_hyp = q_v_b + wn * (q_v_hyp - q_v_b);
+                    } else {
+                        q_v_hyp = 0.5 * (q_v_hyp + q_v_b);
+                    }
+                }
+                nadj++;
+                if(!cell_found && !cell_dry) nnc++;
+                c[q] = q_v_b; cloud[q] = q_c_b; ice[q] = q_i_b;
+                tt[q] = T / t_ref;
+            }
+        }
+    }
+    /* final clamp (:673-685) */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int k = 0; k < km; k++) for(int j = 0; j < jm; j++) for(int i = 0; i < im; i++){
+        const size_t q = IDX(i,j,k);
+        if(c[q]     <= 0.0) c[q]     = 0.0;
+        if(cloud[q] <= 0.0) cloud[q] = 0.0;
+        if(ice[q]   <= 0.0) ice[q]   = 0.0;
+    }
+    if(n_adjusted) *n_adjusted = nadj;
+    if(n_noconv) *n_noconv = nnc;
+    return 0;
+}
+
+/* cUranusModel.cpp:1049-1073, ATURAN_RK_SCALAR_SYNC=2 */
+int oracle_sync_ncopies(const aturan_params* p, double* const* f){
+    const size_t N = (size_t)p->im * p->jm * p->km;
+    for(int q = ATURAN_CH4; q <= ATURAN_NH3_ICE; q++) memcpy(f[ATURAN_TN + q], f[q], sizeof(double) * N);
+    memcpy(f[ATURAN_TN], f[ATURAN_T], sizeof(double) * N);
+    if(p->nh4sh_sync) memcpy(f[ATURAN_NH4SHN], f[ATURAN_NH4SH], sizeof(double) * N);
+    return 0;
+}
+
+/* cUranusModel.cpp:967-1123, the in-scope calls of one even iteration in their order. */
+int oracle_step(const aturan_params* p, double* const* f, int press_kind, double omega,
+                int max_sweeps, double tol, double* ref_out){
+    if(press_kind == ATURAN_PRESS_GS_LEX) oracle_pressure_gs(p, f);
+    else if(press_kind == ATURAN_PRESS_RB_SHARED) oracle_pressure_rb(p, f, max_sweeps);
+    else { int s; double r; oracle_pressure_sor(p, f, omega, max_sweeps, tol, 1, &s, &r); }
+    for(int g = 0; g < 4; g++) oracle_satadj(p, f, g, NULL, NULL);
+    oracle_sync_ncopies(p, f);
+    return oracle_rk4(p, f, ref_out);
+}

@@ -1,0 +1,47 @@
+/*
+ * CPU ORACLE for the aturan_b200 hot path — TEST INFRASTRUCTURE, NOT PART OF THE PRODUCT.
+ *
+ * A plain-C restatement of the reference's FP64 algorithm for the dynamical-core step, written
+ * from the reference's sources with the same expression order so that, compiled without FMA
+ * contraction, it reproduces the reference bit for bit. Only tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg may load it, and only as the checker.
+ *
+ * Parity pinned: tests/test_oracle_vs_ref.py runs every function below against the compiled
+ * reference (oracle/_ref, built from the reference's own sources by oracle/Makefile) on the
+ * reference's initialised state and on seeded perturbations of it, and requires bit equality;
+ * tests/golden/ holds fixtures made the same way for machines without the reference tree.
+ *
+ * Fields: f[id] for id in enum aturan_field, each a contiguous FP64 block [i][j][k] of
+ * im*jm*km values (NULL where a function does not read it). Grid sizes come from the params.
+ */
+#ifndef ATURAN_ORACLE_H
+#define ATURAN_ORACLE_H
+#include "aturan_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void   oracle_coords(const aturan_params* p, double* rad_z, double* the_z);
+double oracle_cp_lapse(const aturan_params* p, double T_K);
+
+int oracle_buoy_ref(const aturan_params* p, double* const* f, double* ref_level);
+int oracle_hydro(const aturan_params* p, double* const* f, const double* ref_level, int advance_follow);
+int oracle_rhs_cell(const aturan_params* p, double* const* f, int i, int j, int k, double* rhs22);
+int oracle_rk4(const aturan_params* p, double* const* f, double* ref_level_out);
+int oracle_pressure_gs(const aturan_params* p, double* const* f);
+int oracle_pressure_rb(const aturan_params* p, double* const* f, int sweeps);
+int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, int max_sweeps,
+                        double tol, int check_every, int* sweeps_done, double* resid);
+double oracle_pressure_residual(const aturan_params* p, double* const* f, const double* src);
+int oracle_pressure_source(const aturan_params* p, double* const* f, double* src);
+int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adjusted, long* n_noconv);
+int oracle_sync_ncopies(const aturan_params* p, double* const* f);
+int oracle_step(const aturan_params* p, double* const* f, int press_kind, double omega,
+                int max_sweeps, double tol, double* ref_level_out);
+void oracle_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+"""Generate tests/golden/golden.json from the COMPILED REFERENCE (oracle/_ref).
+
+Each case builds a seeded synthetic state (aturan_b200.state.synthetic_state, deterministic
+numpy), loads it into the reference model, runs the reference's own routine(s) and records, per
+output field, the SHA-256 of the FP64 bytes plus a seeded sample of cell values (hex). The
+oracle restatement must reproduce every digest bit for bit (tests/test_golden.py), which pins
+it on machines without the reference tree.
+
+    python tests/golden/make_golden.py          # needs oracle/_ref (make -C oracle ref)
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from aturan_b200 import fields as F, params as P, state as S  # noqa: E402
+
+CASES = {
+    "satadj4": dict(seed=101, outputs=["t"] + [n for g in F.GASES for n in F.GAS_FIELDS[g]]),
+    "rk4": dict(seed=102, outputs=F.PROGNOSTIC + ["p_hydro", "p_bfollow"] + F.PROJECTION + ["buoy_ref_level"]),
+    "pressure_gs": dict(seed=103, outputs=["p_dyn", "aux_u", "aux_v", "aux_w"]),
+    "pressure_rb3": dict(seed=104, outputs=["p_dyn"] + F.PROJECTION),
+    "step_gs": dict(seed=105, outputs=F.PROGNOSTIC + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION),
+}
+NSAMPLE = 32
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+def samples(a, seed):
+    rng = np.random.default_rng(seed)
+    flat = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    idx = rng.integers(0, flat.size, NSAMPLE)
+    return [[int(i), float.hex(float(flat[i]))] for i in idx]
+
+
+def run_case(name, runner):
+    """runner(state) -> dict of outputs; returns the golden record."""
+    c = CASES[name]
+    p = P.default_params()
+    st = S.synthetic_state(p, seed=c["seed"])
+    out = runner(name, p, st)
+    rec = {"seed": c["seed"], "fields": {}}
+    for n in c["outputs"]:
+        rec["fields"][n] = {"sha256": digest(out[n]), "samples": samples(out[n], c["seed"] + len(n))}
+    return rec
+
+
+def ref_runner(name, p, st):
+    from oracle.ref import Ref
+    ref = Ref.get_instance()
+    ref.load(st)
+    if name == "satadj4":
+        for g in range(4):
+            ref.satadj(g)
+    elif name == "rk4":
+        ref.rk4()
+    elif name == "pressure_gs":
+        ref.pressure_gs()
+    elif name == "pressure_rb3":
+        ref.pressure_rb(3)
+    elif name == "step_gs":
+        ref.pressure_gs()
+        for g in range(4):
+            ref.satadj(g)
+        ref.sync_ncopies()
+        ref.rk4()
+    out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
+    if "buoy_ref_level" in CASES[name]["outputs"]:
+        out["buoy_ref_level"] = ref.get("buoy_ref_level")
+    return out
+
+
+def main():
+    golden = {"note": "SHA-256 of FP64 outputs of the compiled reference on seeded synthetic states; "
+                      "made by tests/golden/make_golden.py",
+              "numpy": np.__version__, "cases": {}}
+    for name in CASES:
+        golden["cases"][name] = run_case(name, ref_runner)
+        print("done", name, flush=True)
+    with open(os.path.join(HERE, "golden.json"), "w") as fh:
+        json.dump(golden, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,108 @@
+"""The oracle restatement against the compiled reference (oracle/_ref), bit for bit.
+
+The reference is the unmodified C++ compiled from its own sources; its model is initialised
+once (Run() with nm = 0). Each test loads the same state into both, runs the reference routine
+and the oracle function, and requires every output FP64 value to be identical. Skipped where the
+reference has not been built (it needs the reference tree).
+"""
+import numpy as np
+import pytest
+
+from aturan_b200 import fields as F, params as P, state as S
+
+pytestmark = pytest.mark.slow
+
+
+@pytest.fixture(scope="module")
+def base_state(ref_model):
+    return ref_model.state()
+
+
+def assert_same(a, b, names):
+    for n in names:
+        x, y = a[n], b[n]
+        ne = np.count_nonzero(x != y)
+        assert ne == 0, f"{n}: {ne} cells differ, max |d| = {np.abs(x - y).max()}"
+
+
+def test_params_are_the_references(ref_model):
+    p, pr = P.default_params(), P.params_from_ref(ref_model)
+    for name, _ in P.Params._fields_:
+        if name in ("gas", "reserved_i", "reserved_d"):
+            continue
+        assert getattr(p, name) == getattr(pr, name), name
+    for n in range(4):
+        for name, _ in P.Gas._fields_:
+            assert getattr(p.gas[n], name) == getattr(pr.gas[n], name), (n, name)
+
+
+def test_coordinates(ref_model):
+    rad, the = ref_model.coords()
+    r2, t2 = S.coords(P.default_params())
+    assert np.array_equal(rad, r2) and np.array_equal(the, t2)
+
+
+def test_cp_lapse(ref_model, oracle_lib):
+    p = P.default_params()
+    for T in [1.0, 5.0, 5.25, 49.3, 76.4, 150.0, 233.7, 1499.75, 1500.0, 2500.0]:
+        assert ref_model.cp_lapse(T) == oracle_lib.cp_lapse(p, T), T
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_satadj_sequence(ref_model, oracle_lib, base_state, source):
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=11) if source == "reference_init" else S.synthetic_state(p, seed=12)
+    ref_model.load(st)
+    for g, gas in enumerate(F.GASES):
+        ref_model.satadj(g)
+        oracle_lib.satadj(p, st, g)
+        names = ["t"] + list(F.GAS_FIELDS[gas])
+        assert_same(ref_model.state(names), st, names)
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_rk4(ref_model, oracle_lib, base_state, source):
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=21) if source == "reference_init" else S.synthetic_state(p, seed=22)
+    ref_model.load(st)
+    ref_model.rk4()
+    lev = oracle_lib.rk4(p, st)
+    names = F.PROGNOSTIC + ["p_hydro", "p_bfollow"] + F.PROJECTION
+    assert_same(ref_model.state(names), st, names)
+    assert np.array_equal(ref_model.get("buoy_ref_level"), lev)
+
+
+def test_pressure_gs(ref_model, oracle_lib, base_state):
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=31)
+    ref_model.load(st)
+    ref_model.pressure_gs()
+    oracle_lib.pressure_gs(p, st)
+    names = ["p_dyn", "aux_u", "aux_v", "aux_w"]
+    assert_same(ref_model.state(names), st, names)
+
+
+@pytest.mark.parametrize("sweeps", [1, 4])
+def test_pressure_rb(ref_model, oracle_lib, base_state, sweeps):
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=40 + sweeps)
+    ref_model.load(st)
+    ref_model.pressure_rb(sweeps)
+    oracle_lib.pressure_rb(p, st, sweeps)
+    names = ["p_dyn"] + F.PROJECTION
+    assert_same(ref_model.state(names), st, names)
+
+
+def test_full_step(ref_model, oracle_lib, base_state):
+    """cUranusModel.cpp:967-1123, in-scope calls: GS pressure, SatAdj x4, n-copy sync, RK4."""
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=51)
+    ref_model.load(st)
+    ref_model.pressure_gs()
+    for g in range(4):
+        ref_model.satadj(g)
+    ref_model.sync_ncopies()
+    ref_model.rk4()
+    oracle_lib.step(p, st, P.PRESS_GS_LEX)
+    names = F.PROGNOSTIC + F.NCOPIES + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION
+    assert_same(ref_model.state(names), st, names)
