@@ -1,0 +1,196 @@
+"""Python face of the C ABI (include/aturan_b200.h) over ctypes.
+
+`Context` mirrors the reference's call sites on the hot path:
+
+    ctx.pressure(kind)      PressureSolverUran(m).run() / PressureSolver<cUranusModel>(m).run()
+    ctx.satadj(mask)        SaturationAdjustmentUran(m).run(gas, ...) x 4, in the loop's order
+    ctx.sync_ncopies()      the ATURAN_RK_SCALAR_SYNC=2 copy after the adjustments
+    ctx.rk4_step()          cUranusModel::RungeKuttaUran()
+    ctx.step(kind)          the in-scope calls of one even iteration of cUranusModel::Run
+
+State lives on the device; `upload`/`download` move whole fields as FP64 [i][j][k] arrays.
+There is no CPU fallback: without the built library or a CUDA device the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import fields as F
+from .params import Params, default_params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
+
+OK, NOT_CONVERGED = 0, 1
+E_INVALID, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_NONFINITE = -1, -2, -3, -4, -5
+_NAMES = {0: "ok", 1: "not converged", -1: "invalid argument", -2: "unsupported", -3: "CUDA error",
+          -4: "out of device memory", -5: "non-finite value"}
+
+# Every entry point the header declares, with its ctypes signature.
+SIGNATURES = {
+    "aturan_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_ctx_create": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "aturan_upload": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "aturan_download": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "aturan_upload_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "aturan_download_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "aturan_download_buoy_ref": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_rk4_step": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_pressure": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                         ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_satadj": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_sync_ncopies": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_step": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+    "aturan_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_stream": ([ctypes.c_void_p], ctypes.c_void_p),
+    "aturan_profile": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_profile_read": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+}
+
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy"]
+
+_LIB = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libaturan_b200.so (built in-tree by `make -C aturan_b200/csrc`)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `make -C aturan_b200/csrc` "
+                           "(there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+class AturanError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def library_default_params():
+    p = Params()
+    rc = load_library().aturan_params_default(ctypes.byref(p))
+    assert rc == 0
+    return p
+
+
+class Context:
+    """One device-resident model state and its stream (aturan_ctx)."""
+
+    def __init__(self, params=None):
+        self.L = load_library()
+        self.p = (params if params is not None else default_params()).copy()
+        h = ctypes.c_void_p()
+        rc = self.L.aturan_ctx_create(ctypes.byref(self.p), ctypes.byref(h))
+        if rc != 0:
+            raise AturanError(rc, "aturan_ctx_create failed")
+        self.h = h
+        self.shape = (self.p.im, self.p.jm, self.p.km)
+
+    def _check(self, rc, what):
+        if rc < 0:
+            msg = self.L.aturan_last_error(self.h)
+            raise AturanError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.aturan_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- fields ----
+    def upload(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.shape == self.shape, (name, a.shape)
+        self._check(self.L.aturan_upload(self.h, F.ID[name], a.ctypes.data), f"upload {name}")
+
+    def download(self, name, out=None):
+        a = out if out is not None else np.empty(self.shape)
+        self._check(self.L.aturan_download(self.h, F.ID[name], a.ctypes.data), f"download {name}")
+        return a
+
+    def upload_state(self, state):
+        for n, a in state.items():
+            if n in F.ID:
+                self.upload(n, a)
+
+    def download_state(self, names=F.NAMES):
+        return {n: self.download(n) for n in names}
+
+    def upload_device(self, name, ptr):
+        self._check(self.L.aturan_upload_device(self.h, F.ID[name], ctypes.c_void_p(ptr)), f"upload_device {name}")
+
+    def download_device(self, name, ptr):
+        self._check(self.L.aturan_download_device(self.h, F.ID[name], ctypes.c_void_p(ptr)), f"download_device {name}")
+
+    def buoy_ref_level(self):
+        a = np.empty(self.p.im)
+        self._check(self.L.aturan_download_buoy_ref(self.h, a.ctypes.data), "buoy_ref")
+        return a
+
+    # ---- the path ----
+    def rk4_step(self):
+        self._check(self.L.aturan_rk4_step(self.h), "rk4_step")
+
+    def pressure(self, kind=0, omega=1.0, max_sweeps=1, tol=0.0):
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        rc = self._check(self.L.aturan_pressure(self.h, int(kind), float(omega), int(max_sweeps), float(tol),
+                                                ctypes.byref(s), ctypes.byref(r)), "pressure")
+        return rc, s.value, r.value
+
+    def satadj(self, gas_mask=0xF, count=True):
+        na, nn = ctypes.c_long(), ctypes.c_long()
+        if count:
+            self._check(self.L.aturan_satadj(self.h, int(gas_mask), ctypes.byref(na), ctypes.byref(nn)), "satadj")
+            return na.value, nn.value
+        self._check(self.L.aturan_satadj(self.h, int(gas_mask), None, None), "satadj")
+        return None
+
+    def sync_ncopies(self):
+        self._check(self.L.aturan_sync_ncopies(self.h), "sync_ncopies")
+
+    def step(self, kind=0, omega=1.0, max_sweeps=1, tol=0.0):
+        return self._check(self.L.aturan_step(self.h, int(kind), float(omega), int(max_sweeps), float(tol)), "step")
+
+    def profile(self, timing=True):
+        """Reset the per-class launch counters (and event timing when timing=True)."""
+        self._check(self.L.aturan_profile(self.h, 1 if timing else 0), "profile")
+
+    def profile_read(self):
+        """{kind: (launches, ms)} since the last profile()."""
+        n = len(KERNEL_KINDS)
+        ms = (ctypes.c_double * n)()
+        la = (ctypes.c_long * n)()
+        self._check(self.L.aturan_profile_read(self.h, ms, la, n), "profile_read")
+        return {k: (la[q], ms[q]) for q, k in enumerate(KERNEL_KINDS)}
+
+    def synchronize(self):
+        self._check(self.L.aturan_sync(self.h), "sync")
+
+    @property
+    def stream(self):
+        return self.L.aturan_stream(self.h)

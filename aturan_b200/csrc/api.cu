@@ -1,0 +1,776 @@
+// The C ABI of include/aturan_b200.h: context, device layout, tables and the call sequences.
+//
+// Host logic only; the kernels live in fp64.cu / mixed.cu behind launch.h. Geometry, pressure
+// weights and the cp(T) table are built here in FP64 with the reference's expressions and
+// operand order (sources cited per table) and uploaded once, so the device reads the CPU's
+// values rather than recomputing them.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "aturan_b200.h"
+#include "common.cuh"
+#include "launch.h"
+#include "rk4.cuh"
+#include "satadj.cuh"
+#include "pressure.cuh"
+
+using namespace aturan;
+
+struct aturan_ctx {
+    aturan_params p;
+    Grid g;
+    int mixed;                 // 0: FP64 storage, 1: FP32 storage
+    size_t esz;                // bytes per stored element
+    int device;
+    cudaStream_t st;
+    char* mem;                 // one device allocation for everything below
+    size_t mem_bytes;
+    // storage-type groups (each field fstride elements)
+    void* state;               // 19 prognostic
+    void* ncopy;               // 19 start-of-step copies
+    void* ybuf[2];             // stage ping-pong, 19 each
+    void* acc;                 // 19
+    void* forc;                // 22 pointwise RHS inputs
+    void* proj;                // rhs_u, rhs_v, rhs_w, aux_u, aux_v, aux_w
+    void* pstat;               // p_stat
+    // FP64 always
+    double *pdyn, *phydro, *pbaro, *pb0, *pbf;
+    double* scratch;           // incr_src / clamped source
+    double* stage64;           // one padded FP64 field, for conversions
+    double* ref_level;         // im
+    double *part_sum, *part_w; // im * nblk
+    int nblk;
+    double *wsin, *rm_i, *cor_j, *cp_tab64;
+    void* geo;                 // GeoIJ<C>[im*jm]
+    void* cp_tab;              // C[CP_TABLE_N]
+    GSW* gsw;
+    RBW* rbw;
+    unsigned long long* counters;
+    // host-side constants
+    RhsConst<double> k64;
+    RhsConst<float> k32;
+    HydroConst hc;
+    SatConst sc;
+    PressConst pc;
+    cudaGraphExec_t gs_exec;
+    long gs_launches;          // kernels in the captured GS graph
+    // per-class launch counts and optional CUDA-event timing (aturan_profile)
+    int prof_timing;
+    long launches[ATURAN_K_NKINDS];
+    struct EvPair { int kind; cudaEvent_t a, b; };
+    std::vector<EvPair> evs;
+    size_t ev_used;
+    std::string err;
+};
+
+namespace {
+
+int fail(aturan_ctx* c, int code, const std::string& msg){
+    if(c) c->err = msg;
+    return code;
+}
+
+int cuda_check(aturan_ctx* c, cudaError_t e, const char* what){
+    if(e == cudaSuccess) return ATURAN_OK;
+    return fail(c, ATURAN_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call) do { int rc_ = cuda_check(ctx, (call), #call); if(rc_) return rc_; } while(0)
+#define CK_LAUNCH(what) do { int rc_ = cuda_check(ctx, cudaGetLastError(), what); if(rc_) return rc_; } while(0)
+
+size_t round_up(size_t x, size_t a){ return (x + a - 1) / a * a; }
+
+// lib/Array_1D.cpp:50-60
+void coords(const aturan_params& p, std::vector<double>& rad, std::vector<double>& the){
+    rad.resize(p.im); the.resize(p.jm);
+    rad[0] = p.r0;
+    for(int l = 1; l < p.im; l++) rad[l] = rad[l - 1] + p.dr;
+    the[0] = p.the0;
+    for(int l = 1; l < p.jm; l++) the[l] = the[l - 1] + p.dthe;
+}
+
+// cUranusModel.h:641-647
+double metric_radius(const aturan_params& p, double rm){
+    if(!(p.metric_R_km > 0.0)) return rm;
+    return rm + (p.metric_R_km / p.L_atm - 1.0);
+}
+
+double stdmax(double a, double b){ return (a < b) ? b : a; }
+
+// CpH2.h:43-75: the H2 heat capacity table, 0.5 K steps from 5 K to 1500 K.
+double cpR_exact(double T, int mode){
+    auto moments = [T](int J0, double wgt, double& Z, double& E1, double& E2){
+        for(int J = J0; J < 60; J += 2){
+            const double e = 87.57 * J * (J + 1.0), b = wgt * (2.0 * J + 1.0) * std::exp(-e / T);
+            Z += b; E1 += b * e; E2 += b * e * e;
+        }
+    };
+    auto crot = [T](double Z, double E1, double E2){ const double m1 = E1 / Z, m2 = E2 / Z; return (m2 - m1 * m1) / (T * T); };
+    double c;
+    if(mode == 1){
+        double Zp = 0, Ep = 0, Fp = 0, Zo = 0, Eo = 0, Fo = 0;
+        moments(0, 1.0, Zp, Ep, Fp); moments(1, 1.0, Zo, Eo, Fo);
+        c = 0.25 * crot(Zp, Ep, Fp) + 0.75 * crot(Zo, Eo, Fo);
+    } else {
+        double Z = 0, E1 = 0, E2 = 0;
+        moments(0, 1.0, Z, E1, E2); moments(1, 3.0, Z, E1, E2);
+        c = crot(Z, E1, E2);
+    }
+    const double x = 6332.0 / T, cv = (x < 700.0) ? x * x * std::exp(x) / ((std::exp(x) - 1.0) * (std::exp(x) - 1.0)) : 0.0;
+    return 2.5 + c + cv;
+}
+
+template <typename C>
+RhsConst<C> make_rhs_const(const aturan_params& p){
+    RhsConst<double> k{};
+    k.inv_2dr   = 1.0 / (2.0 * p.dr);
+    k.inv_2dthe = 1.0 / (2.0 * p.dthe);
+    k.inv_2dphi = 1.0 / (2.0 * p.dphi);
+    k.inv_dr2   = 1.0 / (p.dr * p.dr);
+    k.inv_dthe2 = 1.0 / (p.dthe * p.dthe);
+    k.inv_dphi2 = 1.0 / (p.dphi * p.dphi);
+    const double coeff_energy_p = p.u_0 * p.u_0 / (p.cp_mix * p.t_ref);          // RHS_Uran_Turb.cpp:280
+    const double scale_p   = 1.0e5 / (p.r_mix * p.u_0 * p.u_0);                    // :283
+    const double scale_Cor = (p.coriolis_full ? p.L_atm * 1.0e3 : p.L_atm) / p.u_0; // cUranusModel.h:1498
+    const double scale_cen = p.L_atm * p.L_atm / (p.u_0 * p.u_0);                 // :285
+    k.ce_sp = coeff_energy_p * scale_p;
+    k.scale_p = scale_p;
+    k.m2om = -2.0 * p.omega;
+    k.p2om = +2.0 * p.omega;
+    k.cor_sc = p.Coriolis * scale_Cor;
+    k.cor_rad_f = 0.0 * p.Coriolis * scale_Cor;                                    // CORIOLIS_SPLIT = 1
+    k.cen_f = 1.0 * p.centrifugal * p.cent_mom * scale_cen;
+    k.re = p.re;
+    k.re_pr = p.re * p.pr;
+    k.re_eff = p.re / (1.0 + 2.5 * 0.0);
+    k.inv_re = 1.0 / p.re;
+    k.turb_coupling = p.turb_coupling;
+    k.precip_coupling = p.precip_coupling;
+    k.chemical_reaction = p.chemical_reaction;
+    k.tmf = p.tmf_scale * p.chemical_reaction;
+    k.precip_L = p.L_atm * 1.0e3;
+    k.precip_den = p.r_mix * p.cp_mix * p.u_0 * p.t_ref;
+    k.sc_re[0] = p.sc_ch4 * p.re; k.sc_re[1] = p.sc_h2o * p.re; k.sc_re[2] = p.sc_h2s * p.re;
+    k.sc_re[3] = p.sc_nh3 * p.re; k.sc_re[4] = p.sc_nh4sh * p.re;
+    k.stokes_a = (2.0 / 9.0) * p.r_p_nh4sh * p.r_p_nh4sh;
+    k.rho_cond_nh4sh = p.rho_cond_nh4sh; k.g = p.g; k.mue_mix = p.mue_mix; k.u_0 = p.u_0;
+    k.cp_mix = p.cp_mix; k.t_ref = p.t_ref;
+    if(p.cp_gas){
+        k.cp_rh2 = p.r_h2;
+        k.cp_he_term = p.r_he * p.cp_he;
+        k.cp_ch4_term = p.r_ch4 * p.cp_ch4;
+        k.cp_rsum = p.r_h2 + p.r_he + p.r_ch4;
+    } else {
+        k.cp_rh2 = p.r_h2 / p.r_mix;
+    }
+    k.cp_h2_const = p.cp_h2;
+    k.tke_max = 1000.0 / (p.u_0 * p.u_0);
+    k.dis_min = 1.0e-10;
+    k.t_min = p.t_min_K / p.t_ref;
+    k.t_max = p.t_max_K / p.t_ref;
+    k.dt = p.dt;
+    k.cp_dyn = p.cp_dyn; k.cp_gas = p.cp_gas; k.cp_mode = p.cp_h2_mode; k.turb_active = p.turb_active;
+    RhsConst<C> out;
+    const double* src = reinterpret_cast<const double*>(&k);
+    C* dst = reinterpret_cast<C*>(&out);
+    const size_t nd = offsetof(RhsConst<double>, cp_dyn) / sizeof(double);
+    for(size_t n = 0; n < nd; n++) dst[n] = (C)src[n];
+    out.cp_dyn = k.cp_dyn; out.cp_gas = k.cp_gas; out.cp_mode = k.cp_mode; out.turb_active = k.turb_active;
+    return out;
+}
+
+int validate(const aturan_params* p, std::string& why){
+    if(p->abi_version != ATURAN_ABI_VERSION){ why = "abi_version mismatch"; return ATURAN_E_INVALID; }
+    if(p->im < 5 || p->jm < 5 || p->km < 5 || p->im > 512 || p->jm > 4096 || p->km > 8192){ why = "grid size out of range"; return ATURAN_E_INVALID; }
+    if((p->km - 1) % 2){ why = "km-1 must be even (the red-black colours must alternate across the seam)"; return ATURAN_E_UNSUPPORTED; }
+    if(p->precision != ATURAN_FP64 && p->precision != ATURAN_MIXED){ why = "unknown precision"; return ATURAN_E_INVALID; }
+    if(!(p->dt > 0.0) || !(p->dr > 0.0) || !(p->dthe > 0.0) || !(p->dphi > 0.0)){ why = "non-positive step"; return ATURAN_E_INVALID; }
+    if(p->cp_h2_mode < 0 || p->cp_h2_mode > 2){ why = "cp_h2_mode must be 0, 1 or 2"; return ATURAN_E_INVALID; }
+    if(p->pbaro_follow < 0.0){ why = "pbaro_follow must be >= 0"; return ATURAN_E_INVALID; }
+    return ATURAN_OK;
+}
+
+// Brackets the launches of one kernel class: counts them and, with timing on, records a pair of
+// CUDA events on the context's stream around them.
+struct Region {
+    aturan_ctx* c; int kind; long n; int slot;
+    Region(aturan_ctx* c_, int kind_, long n_) : c(c_), kind(kind_), n(n_), slot(-1){
+        if(!c->prof_timing) return;
+        if(c->ev_used == c->evs.size()){
+            aturan_ctx::EvPair e{kind, nullptr, nullptr};
+            if(cudaEventCreate(&e.a) != cudaSuccess || cudaEventCreate(&e.b) != cudaSuccess){ cudaGetLastError(); return; }
+            c->evs.push_back(e);
+        }
+        slot = (int)c->ev_used++;
+        c->evs[slot].kind = kind;
+        cudaEventRecord(c->evs[slot].a, c->st);
+    }
+    ~Region(){
+        c->launches[kind] += n;
+        if(slot >= 0) cudaEventRecord(c->evs[slot].b, c->st);
+    }
+};
+
+template <typename T>
+T* carve(char*& cur, size_t n){
+    T* r = reinterpret_cast<T*>(cur);
+    cur += round_up(n * sizeof(T), 256);
+    return r;
+}
+
+// field id -> (device pointer, is FP64)
+void* field_ptr(aturan_ctx* c, int id, bool* is64){
+    const size_t fs = c->g.fstride, e = c->esz;
+    *is64 = !c->mixed;
+    if(id >= 0 && id < ATURAN_NPROG) return (char*)c->state + (size_t)id * fs * e;
+    if(id >= ATURAN_TN && id < ATURAN_TN + ATURAN_NPROG) return (char*)c->ncopy + (size_t)(id - ATURAN_TN) * fs * e;
+    if(id >= ATURAN_NUE && id <= ATURAN_DIS_SOURCE) return (char*)c->forc + (size_t)(id - ATURAN_NUE) * fs * e;
+    if(id >= ATURAN_RHS_U && id <= ATURAN_AUX_W) return (char*)c->proj + (size_t)(id - ATURAN_RHS_U) * fs * e;
+    if(id == ATURAN_P_STAT) return c->pstat;
+    *is64 = true;
+    switch(id){
+    case ATURAN_P_DYN: return c->pdyn;
+    case ATURAN_P_HYDRO: return c->phydro;
+    case ATURAN_P_BARO: return c->pbaro;
+    case ATURAN_P_B0: return c->pb0;
+    case ATURAN_P_BFOLLOW: return c->pbf;
+    }
+    return nullptr;
+}
+
+template <typename S> S* grp(void* base, int q, size_t fs){ return reinterpret_cast<S*>(base) + (size_t)q * fs; }
+
+template <typename S, typename C>
+int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* state = reinterpret_cast<S*>(ctx->state);
+    {
+    Region reg(ctx, ATURAN_K_HYDRO, ctx->p.exact_reductions ? 2 : 3);
+    launch_buoy(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), ctx->wsin, ctx->hc,
+                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, ctx->p.exact_reductions, ctx->st);
+    CK_LAUNCH("buoyancy reference level");
+    launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
+                 grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
+                 ctx->phydro, ctx->hc, 1, ctx->st);
+    CK_LAUNCH("hydrostatic integral");
+    }
+    StageArgs<S, C> a;
+    a.g = g;
+    a.St = state;
+    a.Nc = reinterpret_cast<const S*>(ctx->ncopy);
+    a.acc = reinterpret_cast<S*>(ctx->acc);
+    a.pdyn = ctx->pdyn;
+    a.phydro = ctx->phydro;
+    a.forc = reinterpret_cast<const S*>(ctx->forc);
+    a.proj = reinterpret_cast<S*>(ctx->proj);
+    a.geo = reinterpret_cast<const GeoIJ<C>*>(ctx->geo);
+    a.cp_tab = reinterpret_cast<const C*>(ctx->cp_tab);
+    a.k = K;
+    S* y0 = reinterpret_cast<S*>(ctx->ybuf[0]);
+    S* y1 = reinterpret_cast<S*>(ctx->ybuf[1]);
+    const double dt = ctx->p.dt;
+    for(int stage = 0; stage < 4; stage++){   // RungeKutta_Uran_Turb.cpp:242-245
+        a.stage = stage;
+        a.c_in = (C)((stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0));
+        a.wgt  = (C)((stage == 0 || stage == 3) ? 1.0 : 2.0);
+        a.X = stage == 0 ? state : (stage == 1 ? y0 : (stage == 2 ? y1 : y0));
+        a.Y = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : state));
+        Region reg(ctx, ATURAN_K_RK_STAGE, 1);
+        launch_stage(a, ctx->st);
+        CK_LAUNCH("RK4 stage");
+    }
+    return ATURAN_OK;
+}
+
+template <typename S>
+int run_satadj(aturan_ctx* ctx, int mask, bool count){
+    const size_t fs = ctx->g.fstride;
+    S* state = reinterpret_cast<S*>(ctx->state);
+    SatArgs<S> a;
+    a.g = ctx->g;
+    a.t = grp<S>(state, ATURAN_T, fs);
+    a.ps = reinterpret_cast<const S*>(ctx->pstat);
+    a.rho_mix = grp<S>(ctx->forc, ATURAN_RHO_MIX - ATURAN_NUE, fs);
+    static const int base[4] = {ATURAN_H2O, ATURAN_H2S, ATURAN_NH3, ATURAN_CH4};
+    for(int gi = 0; gi < 4; gi++)
+        for(int n = 0; n < 3; n++) a.spec[gi][n] = grp<S>(state, base[gi] + n, fs);
+    a.k = ctx->sc;
+    a.gas_mask = mask;
+    a.counters = count ? ctx->counters : nullptr;
+    Region reg(ctx, ATURAN_K_SATADJ, 1);
+    launch_satadj(a, ctx->st);
+    CK_LAUNCH("saturation adjustment");
+    return ATURAN_OK;
+}
+
+template <typename S>
+int run_gs(aturan_ctx* ctx){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* proj = reinterpret_cast<S*>(ctx->proj);
+    if(!ctx->gs_exec){
+        // The hyperplane sweep is (im-2)+(jm-2)+(km-2)-1 dependent launches; capture the whole
+        // call once per context and replay it.
+        cudaStream_t cs;
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        launch_gs_pre(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
+                      grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->pdyn, ctx->gsw,
+                      ctx->pc, ctx->scratch, cs);
+        const int s_lo = 2, s_hi = (g.im - 2) + (g.jm - 2) + (g.km - 2);
+        ctx->gs_launches = 1 + (ctx->pc.press_incr ? 1 : 0) + (s_hi - s_lo + 1) + 3;
+        for(int s = s_lo; s <= s_hi; s++)
+            launch_gs_plane(g, ctx->pdyn, ctx->scratch, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs),
+                            grp<S>(proj, 5, fs), ctx->gsw, ctx->pc, s, cs);
+        launch_pdyn_bcs(g, ctx->pdyn, cs);
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+        if(e1 != cudaSuccess || e2 != cudaSuccess){
+            cudaStreamDestroy(cs);
+            return fail(ctx, ATURAN_E_CUDA, std::string("capturing the GS sweep: ") +
+                        cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&ctx->gs_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        CK(e3);
+    }
+    Region reg(ctx, ATURAN_K_GS, ctx->gs_launches);
+    CK(cudaGraphLaunch(ctx->gs_exec, ctx->st));
+    return ATURAN_OK;
+}
+
+template <typename S>
+int run_rb(aturan_ctx* ctx, int sweeps, double omega){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* proj = reinterpret_cast<S*>(ctx->proj);
+    if(sweeps < 1) sweeps = 1;                                  // PressureSolver.h:174-175
+    Region reg(ctx, ATURAN_K_RB, 3 + 5L * sweeps);
+    launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
+                   grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->p.rigid_lid,
+                   ctx->rbw, ctx->pc, ctx->scratch, ctx->st);
+    CK_LAUNCH("projection boundaries and source");
+    for(int s = 0; s < sweeps; s++){
+        launch_rb_colour(g, ctx->pdyn, ctx->scratch, ctx->rbw, 0, omega, ctx->st);
+        launch_rb_colour(g, ctx->pdyn, ctx->scratch, ctx->rbw, 1, omega, ctx->st);
+        launch_pdyn_bcs(g, ctx->pdyn, ctx->st);
+        CK_LAUNCH("red-black sweep");
+    }
+    return ATURAN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aturan_params_default(aturan_params* p){
+    if(!p) return ATURAN_E_INVALID;
+    std::memset(p, 0, sizeof(*p));
+    p->abi_version = ATURAN_ABI_VERSION;
+    p->im = 41; p->jm = 181; p->km = 361;
+    p->precision = ATURAN_FP64;
+    p->turb_active = 1; p->coriolis_full = 1; p->cp_h2_mode = 2; p->cp_gas = 1; p->cp_dyn = 1;
+    p->press_consistent = 1; p->press_incr = 1; p->rigid_lid = 1;
+    p->satadj_conserve = 1; p->satadj_newton = 1; p->satadj_evap = 1; p->satadj_ice_entry = 0;
+    p->satadj_bergeron = 2; p->satadj_freeze = 1; p->satadj_dry_exit = 1; p->local_rho = 1;
+    p->nh4sh_sync = 1; p->exact_reductions = 0;
+    const double pi180 = 180.0 / M_PI;                        // cUranusModel.cpp:340-351
+    p->r0 = 1.0; p->dr = 0.025; p->the0 = 0.0; p->dthe = 1.0 / pi180; p->phi0 = 0.0; p->dphi = 1.0 / pi180;
+    p->dt = 0.001; p->metric_R_km = 25362.0; p->sinthe_min = 0.4;
+    p->L_atm = 225.0; p->u_0 = 100.0; p->t_ref = 76.4; p->g = 8.69; p->omega = 0.000101;
+    p->re = 1000.0; p->pr = 0.69; p->Coriolis = 1.0; p->centrifugal = 1.0; p->buoyancy = 1.0;
+    p->chemical_reaction = 1.0; p->R_ref = 3.61491; p->p_ref = 1.0;
+    p->r_mix = 0x1.d296ea433d4a6p+1; p->R_mix = 0x1.31fad52a5899ap+11;
+    p->cp_mix = 0x1.0f59f37b7f291p+13; p->mue_mix = 0x1.5e6b31135aa58p-17;
+    p->r_h2 = 0x1.e0c778070069fp+0; p->r_he = 0x1.2eb67afaed4c3p-2; p->r_ch4 = 0x1.a6e858fcad66bp-2;
+    p->cp_h2 = 14.32e3; p->cp_he = 5.19e3; p->cp_ch4 = 2.232e3;
+    p->sc_ch4 = 0.99; p->sc_h2o = 0.61; p->sc_h2s = 0.94; p->sc_nh3 = 0.61; p->sc_nh4sh = 0.7;
+    p->alpha_sponge = 10.0; p->r_p_nh4sh = 1.0e-5; p->rho_cond_nh4sh = 1170.0;
+    p->turb_coupling = 1.0; p->precip_coupling = 1.0; p->tmf_scale = 0.0; p->cent_mom = 0.0;
+    p->pbaro_follow = 64.0; p->t_min_K = 7.5; p->t_max_K = 2000.0; p->p_dyn_cap = 0.2;
+    const double G[4][14] = {
+        {273.15, 210.15, 8.1253, 2.5009e6, 2.8339e6, 25.096, 3148.2, 461.52, 0.0, -8.7e-3, 28.418, 3567.3, 0.0, -8.7e-3},
+        {187.65, 140.0, 14.5192, 5.5e5, 7.45e5, 17.064, 747.0, 243.96, 0.0, -2.9e-3, 17.064, 747.0, 0.0, -2.9e-3},
+        {195.5, 140.0, 7.6752, 1.3720e6, 1.8320e6, 27.863, 2016.0, 488.21, -0.888, 0.0, 34.948, 2692.5, -0.888, 0.0},
+        {90.69, 67.36, 7.6752, 5.11e5, 5.11e5, 1.627, 553.1, 518.28, 1.002, -4.1e-3, 1.627, 553.1, 1.002, -4.1e-3}};
+    for(int n = 0; n < 4; n++) std::memcpy(&p->gas[n], G[n], sizeof(G[n]));
+    return ATURAN_OK;
+}
+
+const char* aturan_last_error(const aturan_ctx* ctx){
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
+    if(!p || !out) return ATURAN_E_INVALID;
+    *out = nullptr;
+    std::string why;
+    int rc = validate(p, why);
+    if(rc){ std::fprintf(stderr, "aturan_ctx_create: %s\n", why.c_str()); return rc; }
+    int ndev = 0;
+    if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0){
+        cudaGetLastError();
+        std::fprintf(stderr, "aturan_ctx_create: no CUDA device\n");
+        return ATURAN_E_CUDA;
+    }
+    aturan_ctx* ctx = new (std::nothrow) aturan_ctx();
+    if(!ctx) return ATURAN_E_NOMEM;
+    ctx->p = *p;
+    cudaGetDevice(&ctx->device);
+    ctx->mixed = p->precision == ATURAN_MIXED;
+    ctx->esz = ctx->mixed ? sizeof(float) : sizeof(double);
+    Grid& g = ctx->g;
+    g.im = p->im; g.jm = p->jm; g.km = p->km;
+    g.kp = (int)round_up(p->km, 32);
+    g.fstride = (size_t)g.im * g.jm * g.kp;
+    ctx->nblk = 32;
+    const size_t fs = g.fstride, e = ctx->esz;
+    const size_t nij = (size_t)g.im * g.jm;
+    const size_t sgeo = ctx->mixed ? sizeof(GeoIJ<float>) : sizeof(GeoIJ<double>);
+    size_t bytes = 0;
+    auto add = [&](size_t n){ bytes += round_up(n, 256); };
+    add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e);
+    add(22 * fs * e); add(6 * fs * e); add(fs * e);
+    for(int n = 0; n < 7; n++) add(fs * 8);                   // pdyn phydro pbaro pb0 pbf scratch stage64
+    add(g.im * 8); add(2 * (size_t)g.im * ctx->nblk * 8);
+    add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
+    add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
+    ctx->mem_bytes = bytes;
+    if(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess){
+        delete ctx; return ATURAN_E_CUDA;
+    }
+    if(cudaMalloc((void**)&ctx->mem, bytes) != cudaSuccess){
+        cudaGetLastError();
+        cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_NOMEM;
+    }
+    char* cur = ctx->mem;
+    ctx->state = carve<char>(cur, 19 * fs * e);
+    ctx->ncopy = carve<char>(cur, 19 * fs * e);
+    ctx->ybuf[0] = carve<char>(cur, 19 * fs * e);
+    ctx->ybuf[1] = carve<char>(cur, 19 * fs * e);
+    ctx->acc = carve<char>(cur, 19 * fs * e);
+    ctx->forc = carve<char>(cur, 22 * fs * e);
+    ctx->proj = carve<char>(cur, 6 * fs * e);
+    ctx->pstat = carve<char>(cur, fs * e);
+    ctx->pdyn = carve<double>(cur, fs); ctx->phydro = carve<double>(cur, fs);
+    ctx->pbaro = carve<double>(cur, fs); ctx->pb0 = carve<double>(cur, fs); ctx->pbf = carve<double>(cur, fs);
+    ctx->scratch = carve<double>(cur, fs); ctx->stage64 = carve<double>(cur, fs);
+    ctx->ref_level = carve<double>(cur, g.im);
+    ctx->part_sum = carve<double>(cur, 2 * (size_t)g.im * ctx->nblk);
+    ctx->part_w = ctx->part_sum + (size_t)g.im * ctx->nblk;
+    ctx->wsin = carve<double>(cur, g.jm); ctx->rm_i = carve<double>(cur, g.im); ctx->cor_j = carve<double>(cur, g.jm);
+    ctx->cp_tab64 = carve<double>(cur, CP_TABLE_N);
+    ctx->geo = carve<char>(cur, nij * sgeo);
+    ctx->cp_tab = carve<char>(cur, CP_TABLE_N * e);
+    ctx->gsw = carve<GSW>(cur, nij); ctx->rbw = carve<RBW>(cur, nij);
+    ctx->counters = carve<unsigned long long>(cur, 8);
+
+    // zero everything once: padding columns and unused planes read as 0, never as garbage
+    if(cudaMemsetAsync(ctx->mem, 0, bytes, ctx->st) != cudaSuccess){ aturan_ctx_destroy(ctx); return ATURAN_E_CUDA; }
+
+    // ---- host tables ----
+    std::vector<double> rad, the;
+    coords(*p, rad, the);
+    std::vector<double> wsin(g.jm), rm_i(g.im), cor_j(g.jm), cp64(CP_TABLE_N);
+    const double scale_Cor = (p->coriolis_full ? p->L_atm * 1.0e3 : p->L_atm) / p->u_0;
+    for(int j = 0; j < g.jm; j++){
+        wsin[j] = std::sin(the[j]);                                             // RungeKutta_Uran_Turb.cpp:25
+        cor_j[j] = p->Coriolis * scale_Cor * 2.0 * p->omega * std::abs(std::sin(the[j]));   // :132-133
+    }
+    for(int i = 0; i < g.im; i++) rm_i[i] = metric_radius(*p, rad[i]);
+    const int mode = p->cp_h2_mode > 0 ? p->cp_h2_mode : 2;
+    for(int n = 0; n < CP_TABLE_N; n++) cp64[n] = cpR_exact(5.0 + n * 0.5, mode) * 8.314462618 / 2.01588e-3;
+
+    std::vector<GeoIJ<double>> geo(nij);
+    std::vector<GSW> gsw(nij);
+    std::vector<RBW> rbw(nij);
+    const double inv_dr2 = 1.0 / (p->dr * p->dr), inv_dthe2 = 1.0 / (p->dthe * p->dthe), inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+    std::vector<double> st_uran(g.jm), st_shared(g.jm);
+    for(int j = 0; j < g.jm; j++){                     // PressureSolverUran.h:42-47, PressureSolver.h:156-162
+        st_uran[j] = std::sin(the[j]);
+        if(st_uran[j] < p->sinthe_min) st_uran[j] = p->sinthe_min;
+        st_shared[j] = st_uran[j];
+        if(st_shared[j] == 0.0) st_shared[j] = 1.0e-5;
+    }
+    const int im = g.im;
+    for(int i = 0; i < g.im; i++){
+        double frac_sp = (double)(i - (im - 1) * 3 / 4) / (double)((im - 1) / 4);   // RHS_Uran_Turb.cpp:594-595
+        frac_sp = stdmax(0.0, frac_sp);
+        const double sponge = p->alpha_sponge * frac_sp * frac_sp;
+        for(int j = 0; j < g.jm; j++){
+            GeoIJ<double>& G = geo[(size_t)i * g.jm + j];
+            // RungeKutta_Uran_Turb.cpp:192-197, 266-277
+            const double rm = metric_radius(*p, rad[i]);
+            const double rm2 = rm * rm;
+            const double sinthe = stdmax(p->sinthe_min, std::abs(std::sin(the[j])));
+            const double sinthe2 = sinthe * sinthe;
+            const double costhe = std::cos(the[j]);
+            G.cotanthe = costhe / sinthe;
+            G.inv_rm = 1.0 / rm;
+            G.inv_rm2 = 1.0 / rm2;
+            G.inv_rmsinthe = 1.0 / (rm * sinthe);
+            G.inv_rm2sinthe = G.inv_rm2 / sinthe;
+            G.inv_rm2sinthe2 = G.inv_rm2 / sinthe2;
+            G.costhe_inv_rm2sinthe = costhe * G.inv_rm2sinthe;
+            G.costhe = costhe;
+            G.v_metric = (1.0 + costhe / sinthe2) * G.inv_rm2;                         // RHS_Uran_Turb.cpp:331
+            G.two_inv_rm = 2.0 * G.inv_rm;                                              // :330
+            G.sinthe_bf = std::sqrt(stdmax(0.0, 1.0 - costhe * costhe));               // :224
+            G.cent_rad = p->omega * p->omega * rm * G.sinthe_bf * G.sinthe_bf;          // :276
+            G.cent_the = p->omega * p->omega * rm * G.sinthe_bf * costhe;               // :277
+            G.sponge = sponge;
+
+            // PressureSolverUran weights (:151-157, :180-190)
+            const double rmc = p->press_consistent ? rm : rad[i];
+            GSW& W = gsw[(size_t)i * g.jm + j];
+            {
+                const double s = st_uran[j];
+                const double inv_rm = 1.0 / rmc;
+                const double inv_rmsinthe = 1.0 / (rmc * s);
+                const double inv_rm2 = inv_rm * inv_rm;
+                const double inv_rm2sinthe2 = inv_rm2 / (s * s);
+                W.n1 = 1.0 / (p->dr * p->dr); W.n2 = inv_rm2 / (p->dthe * p->dthe);
+                W.n3 = inv_rm2sinthe2 / (p->dphi * p->dphi);
+                W.denom = 2.0 * (W.n1 + W.n2 + W.n3);
+                W.inv_rm = inv_rm; W.inv_rmsinthe = inv_rmsinthe;
+                const double rm2c = rmc * rmc;
+                const double inv_rm2b = 1.0 / rm2c;
+                const double inv_rm2sinthe2b = inv_rm2b / (s * s);
+                const double denom = 2.0 * inv_dr2 + 2.0 * inv_rm2b * inv_dthe2 + 2.0 * inv_rm2sinthe2b * inv_dphi2;
+                W.inv_denom = 1.0 / denom;
+                W.num1 = inv_dr2; W.num2 = inv_rm2b * inv_dthe2; W.num3 = inv_rm2sinthe2b * inv_dphi2;
+            }
+            // shared solver weights (PressureSolver.h:326-353, 484)
+            RBW& R = rbw[(size_t)i * g.jm + j];
+            {
+                const double s = st_shared[j];
+                const double inv_rm2 = 1.0 / rm2;
+                const double inv_rm2sinthe2 = inv_rm2 / (s * s);
+                const double exp_2_rm = 1.0 * 1.0;
+                R.num1 = exp_2_rm * inv_dr2; R.num2 = inv_rm2 * inv_dthe2; R.num3 = inv_rm2sinthe2 * inv_dphi2;
+                R.den = 2.0 * R.num1 + 2.0 * R.num2 + 2.0 * R.num3;
+                R.inv_rm = 1.0 / rm; R.inv_rmsinthe = 1.0 / (rm * s);
+                R.src_max = R.den * p->p_dyn_cap;
+            }
+        }
+    }
+    ctx->k64 = make_rhs_const<double>(*p);
+    ctx->k32 = make_rhs_const<float>(*p);
+    HydroConst& h = ctx->hc;                             // RungeKutta_Uran_Turb.cpp:76-99
+    h.g = p->g; h.rR = p->r_mix * p->R_mix; h.t_ref = p->t_ref;
+    const double nd_rel = p->g * (p->L_atm * 1.0e3) / (p->u_0 * p->u_0);
+    h.m_nd_rel_b = -nd_rel * 1.0 * p->buoyancy;
+    h.dr = p->dr; h.follow_tau = p->pbaro_follow; h.follow_on = p->pbaro_follow > 0.0;
+    SatConst& sc = ctx->sc;
+    for(int n = 0; n < 4; n++){
+        const aturan_gas& G = p->gas[n];
+        GasConst& K = sc.gas[n];
+        K.t_0 = G.t_0; K.t_00 = G.t_00; K.ep = G.ep; K.lv = G.lv; K.ls = G.ls;
+        K.C = G.C; K.L0 = G.L0; K.den = 1e-3 * G.R; K.del_alf = G.del_alf; K.del_bet = G.del_bet;
+        K.C_i = G.C_i; K.L0_i = G.L0_i; K.del_alf_i = G.del_alf_i; K.del_bet_i = G.del_bet_i;
+        K.t_range_inv = 1.0 / (G.t_0 - G.t_00);
+        K.Lf = G.ls - G.lv;
+        K.freeze_on = p->satadj_freeze && p->satadj_conserve && G.t_00 > 0.0 && G.t_00 < G.t_0;
+    }
+    sc.cp_mix = p->cp_mix; sc.t_ref = p->t_ref; sc.r_mix = p->r_mix;
+    sc.conserve = p->satadj_conserve; sc.newton = p->satadj_newton; sc.evap = p->satadj_evap;
+    sc.ice_entry = p->satadj_ice_entry; sc.bergeron = p->satadj_bergeron; sc.dry_exit = p->satadj_dry_exit;
+    sc.local_rho = p->local_rho;
+    PressConst& pc = ctx->pc;
+    pc.inv_2dr = 1.0 / (2.0 * p->dr); pc.inv_2dthe = 1.0 / (2.0 * p->dthe); pc.inv_2dphi = 1.0 / (2.0 * p->dphi);
+    pc.two_dr = 2.0 * p->dr; pc.two_dthe = 2.0 * p->dthe; pc.two_dphi = 2.0 * p->dphi;
+    pc.src_scale = p->press_consistent ? (p->r_mix * p->u_0 * p->u_0) / 1.0e5 : 1.0;
+    pc.press_incr = p->press_incr;
+
+    auto up = [&](void* dst, const void* src, size_t n) -> int {
+        return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, ctx->st) == cudaSuccess ? 0 : 1;
+    };
+    int bad = 0;
+    bad |= up(ctx->wsin, wsin.data(), g.jm * 8);
+    bad |= up(ctx->rm_i, rm_i.data(), g.im * 8);
+    bad |= up(ctx->cor_j, cor_j.data(), g.jm * 8);
+    bad |= up(ctx->cp_tab64, cp64.data(), CP_TABLE_N * 8);
+    bad |= up(ctx->gsw, gsw.data(), nij * sizeof(GSW));
+    bad |= up(ctx->rbw, rbw.data(), nij * sizeof(RBW));
+    std::vector<GeoIJ<float>> geo32;
+    std::vector<float> cp32;
+    if(ctx->mixed){
+        geo32.resize(nij);
+        for(size_t n = 0; n < nij; n++){
+            const double* s = reinterpret_cast<const double*>(&geo[n]);
+            float* d = reinterpret_cast<float*>(&geo32[n]);
+            for(size_t q = 0; q < sizeof(GeoIJ<double>) / sizeof(double); q++) d[q] = (float)s[q];
+        }
+        cp32.resize(CP_TABLE_N);
+        for(int n = 0; n < CP_TABLE_N; n++) cp32[n] = (float)cp64[n];
+        bad |= up(ctx->geo, geo32.data(), nij * sizeof(GeoIJ<float>));
+        bad |= up(ctx->cp_tab, cp32.data(), CP_TABLE_N * sizeof(float));
+    } else {
+        bad |= up(ctx->geo, geo.data(), nij * sizeof(GeoIJ<double>));
+        bad |= up(ctx->cp_tab, cp64.data(), CP_TABLE_N * 8);
+    }
+    if(bad || cudaStreamSynchronize(ctx->st) != cudaSuccess){
+        cudaGetLastError();
+        aturan_ctx_destroy(ctx);
+        return ATURAN_E_CUDA;
+    }
+    *out = ctx;
+    return ATURAN_OK;
+}
+
+int aturan_ctx_destroy(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    if(ctx->st) cudaStreamSynchronize(ctx->st);
+    if(ctx->gs_exec) cudaGraphExecDestroy(ctx->gs_exec);
+    for(auto& e : ctx->evs){ cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+    if(ctx->mem) cudaFree(ctx->mem);
+    if(ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+    return ATURAN_OK;
+}
+
+void* aturan_stream(aturan_ctx* ctx){ return ctx ? (void*)ctx->st : nullptr; }
+
+static int xfer(aturan_ctx* ctx, int field, void* other, bool up, bool other_is_device){
+    if(!ctx || !other) return ATURAN_E_INVALID;
+    if(field < 0 || field >= ATURAN_NFIELDS) return fail(ctx, ATURAN_E_INVALID, "field id out of range");
+    bool is64;
+    void* dev = field_ptr(ctx, field, &is64);
+    const Grid& g = ctx->g;
+    const size_t rows = (size_t)g.im * g.jm;
+    const cudaMemcpyKind kind = other_is_device ? cudaMemcpyDeviceToDevice : (up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost);
+    double* d64 = is64 ? reinterpret_cast<double*>(dev) : ctx->stage64;
+    if(up){
+        CK(cudaMemcpy2DAsync(d64, g.kp * 8, other, g.km * 8, g.km * 8, rows, kind, ctx->st));
+        if(!is64){ launch_f64_to_f32(ctx->stage64, reinterpret_cast<float*>(dev), g.fstride, ctx->st); CK_LAUNCH("f64->f32"); }
+        if(!other_is_device) CK(cudaStreamSynchronize(ctx->st));
+    } else {
+        if(!is64){ launch_f32_to_f64(reinterpret_cast<const float*>(dev), ctx->stage64, g.fstride, ctx->st); CK_LAUNCH("f32->f64"); }
+        CK(cudaMemcpy2DAsync(other, g.km * 8, d64, g.kp * 8, g.km * 8, rows, kind, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    return ATURAN_OK;
+}
+
+int aturan_upload(aturan_ctx* ctx, int field, const double* host){ return xfer(ctx, field, (void*)host, true, false); }
+int aturan_download(aturan_ctx* ctx, int field, double* host){ return xfer(ctx, field, host, false, false); }
+int aturan_upload_device(aturan_ctx* ctx, int field, const double* dev){ return xfer(ctx, field, (void*)dev, true, true); }
+int aturan_download_device(aturan_ctx* ctx, int field, double* dev){ return xfer(ctx, field, dev, false, true); }
+
+int aturan_download_buoy_ref(aturan_ctx* ctx, double* host){
+    if(!ctx || !host) return ATURAN_E_INVALID;
+    CK(cudaMemcpyAsync(host, ctx->ref_level, ctx->g.im * 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return ATURAN_OK;
+}
+
+int aturan_rk4_step(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    return ctx->mixed ? run_rk4<float, float>(ctx, ctx->k32) : run_rk4<double, double>(ctx, ctx->k64);
+}
+
+int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_noconv){
+    if(!ctx) return ATURAN_E_INVALID;
+    if(gas_mask & ~0xF) return fail(ctx, ATURAN_E_INVALID, "gas_mask has bits above 3");
+    const bool count = n_adjusted || n_noconv;
+    if(count) CK(cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), ctx->st));
+    int rc = ctx->mixed ? run_satadj<float>(ctx, gas_mask, count) : run_satadj<double>(ctx, gas_mask, count);
+    if(rc) return rc;
+    if(count){
+        unsigned long long h[2];
+        CK(cudaMemcpyAsync(h, ctx->counters, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if(n_adjusted) *n_adjusted = (long)h[0];
+        if(n_noconv) *n_noconv = (long)h[1];
+    }
+    return ATURAN_OK;
+}
+
+int aturan_sync_ncopies(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    const size_t fs = ctx->g.fstride, e = ctx->esz;
+    char* s = (char*)ctx->state; char* n = (char*)ctx->ncopy;
+    Region reg(ctx, ATURAN_K_COPY, 0);
+    CK(cudaMemcpyAsync(n + ATURAN_CH4 * fs * e, s + ATURAN_CH4 * fs * e, 12 * fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(n, s, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    if(ctx->p.nh4sh_sync)
+        CK(cudaMemcpyAsync(n + ATURAN_NH4SH * fs * e, s + ATURAN_NH4SH * fs * e, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    return ATURAN_OK;
+}
+
+int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
+                    int* sweeps_done, double* resid){
+    if(!ctx) return ATURAN_E_INVALID;
+    if(sweeps_done) *sweeps_done = 0;
+    if(resid) *resid = 0.0;
+    int rc;
+    switch(kind){
+    case ATURAN_PRESS_GS_LEX:
+        rc = ctx->mixed ? run_gs<float>(ctx) : run_gs<double>(ctx);
+        if(!rc && sweeps_done) *sweeps_done = 1;
+        return rc;
+    case ATURAN_PRESS_RB_SHARED:
+        rc = ctx->mixed ? run_rb<float>(ctx, max_sweeps, 1.0) : run_rb<double>(ctx, max_sweeps, 1.0);
+        if(!rc && sweeps_done) *sweeps_done = max_sweeps < 1 ? 1 : max_sweeps;
+        return rc;
+    case ATURAN_PRESS_RB_SOR:
+        (void)omega; (void)tol;
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "RB_SOR is not built yet");
+    }
+    return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
+}
+
+int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol){
+    if(!ctx) return ATURAN_E_INVALID;
+    int rc = aturan_pressure(ctx, press_kind, omega, max_sweeps, tol, nullptr, nullptr);
+    if(rc < 0) return rc;
+    int rc2 = aturan_satadj(ctx, 0xF, nullptr, nullptr);
+    if(rc2) return rc2;
+    rc2 = aturan_sync_ncopies(ctx);
+    if(rc2) return rc2;
+    rc2 = aturan_rk4_step(ctx);
+    if(rc2) return rc2;
+    return rc;
+}
+
+int aturan_profile(aturan_ctx* ctx, int enable){
+    if(!ctx) return ATURAN_E_INVALID;
+    CK(cudaStreamSynchronize(ctx->st));
+    for(long& l : ctx->launches) l = 0;
+    ctx->ev_used = 0;
+    ctx->prof_timing = enable ? 1 : 0;
+    return ATURAN_OK;
+}
+
+int aturan_profile_read(aturan_ctx* ctx, double* ms, long* launches, int nkinds){
+    if(!ctx || nkinds < 0) return ATURAN_E_INVALID;
+    CK(cudaStreamSynchronize(ctx->st));
+    const int n = nkinds < ATURAN_K_NKINDS ? nkinds : ATURAN_K_NKINDS;
+    if(launches) for(int q = 0; q < n; q++) launches[q] = ctx->launches[q];
+    if(ms){
+        for(int q = 0; q < n; q++) ms[q] = 0.0;
+        for(size_t u = 0; u < ctx->ev_used; u++){
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, ctx->evs[u].a, ctx->evs[u].b));
+            if(ctx->evs[u].kind < n) ms[ctx->evs[u].kind] += t;
+        }
+    }
+    return ATURAN_OK;
+}
+
+int aturan_sync(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    CK(cudaStreamSynchronize(ctx->st));
+    return ATURAN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,40 @@
+// Host-side launch wrappers. Each kernel family is instantiated in the translation unit whose
+// compiler flags it needs: fp64.cu (FP64 state, no FMA contraction: the parity path) and
+// mixed.cu (FP32 state with FMA). api.cu holds the host logic and calls these.
+#pragma once
+#include "common.cuh"
+
+namespace aturan {
+
+template <typename S, typename C> struct StageArgs;
+template <typename S> struct SatArgs;
+struct GSW; struct RBW; struct PressConst;
+
+#define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
+void launch_stage(const StageArgs<S, C>& a, cudaStream_t st);                                              \
+void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
+                 double* part_w, int nblk, double* ref, int exact, cudaStream_t st);                       \
+void launch_hydro(Grid g, const S* t, const S* ps, const S* v, const S* w, const double* ref,              \
+                  const double* rm_i, const double* cor_j, const double* pbaro, const double* pb0,         \
+                  double* pbf, double* ph, HydroConst h, int advance, cudaStream_t st);                    \
+void launch_satadj(const SatArgs<S>& a, cudaStream_t st);                                                  \
+void launch_gs_pre(Grid g, S* au, S* av, S* aw, const S* ru, const S* rv, const S* rw, const double* P,    \
+                   const GSW* w, PressConst c, double* incr, cudaStream_t st);                             \
+void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S* av, const S* aw,         \
+                     const GSW* w, PressConst c, int s, cudaStream_t st);                                   \
+void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
+                    const RBW* w, PressConst c, double* src, cudaStream_t st);
+
+ATURAN_DECLARE_LAUNCHERS(double, double)
+ATURAN_DECLARE_LAUNCHERS(float, float)
+#undef ATURAN_DECLARE_LAUNCHERS
+
+// FP64-only kernels (p_dyn is FP64 in both precisions).
+void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st);
+void launch_rb_colour(Grid g, double* P, const double* src, const RBW* w, int colour, double omega, cudaStream_t st);
+
+// Layout conversions for the mixed-precision context (FP64 exchange <-> FP32 storage).
+void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st);
+void launch_f32_to_f64(const float* in, double* out, size_t n, cudaStream_t st);
+
+}  // namespace aturan

@@ -1,0 +1,50 @@
+// Definitions of the launch wrappers declared in launch.h, instantiated per storage/compute type
+// by the translation unit that includes this file (fp64.cu, mixed.cu).
+#pragma once
+#include "rk4.cuh"
+#include "satadj.cuh"
+#include "pressure.cuh"
+
+#define ATURAN_DEFINE_LAUNCHERS(S, C)                                                                     \
+void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                                             \
+    const Grid& g = a.g;                                                                                  \
+    dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);                                        \
+    rk_stage_kernel<S, C><<<grid, dim3(32, 4), 0, st>>>(a);                                               \
+}                                                                                                         \
+void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
+                 double* part_w, int nblk, double* ref, int exact, cudaStream_t st){                       \
+    if(exact){ buoy_serial_kernel<S><<<(g.im + 31) / 32, 32, 0, st>>>(g, t, ps, wsin, h, ref); return; } \
+    buoy_partial_kernel<S><<<dim3(nblk, g.im), 256, 0, st>>>(g, t, ps, wsin, h, part_sum, part_w, nblk); \
+    buoy_finish_kernel<<<(g.im + 63) / 64, 64, 0, st>>>(g.im, nblk, part_sum, part_w, ref);               \
+}                                                                                                         \
+void launch_hydro(Grid g, const S* t, const S* ps, const S* v, const S* w, const double* ref,              \
+                  const double* rm_i, const double* cor_j, const double* pbaro, const double* pb0,         \
+                  double* pbf, double* ph, HydroConst h, int advance, cudaStream_t st){                    \
+    const int n = g.jm * g.km;                                                                            \
+    hydro_kernel<S><<<(n + 255) / 256, 256, 0, st>>>(g, t, ps, v, w, ref, rm_i, cor_j, pbaro, pb0, pbf,    \
+                                                    ph, h, advance);                                      \
+}                                                                                                         \
+void launch_satadj(const SatArgs<S>& a, cudaStream_t st){                                                  \
+    dim3 grid((a.g.km + 127) / 128, a.g.jm, a.g.im);                                                      \
+    satadj_kernel<S><<<grid, 128, 0, st>>>(a);                                                            \
+}                                                                                                         \
+void launch_gs_pre(Grid g, S* au, S* av, S* aw, const S* ru, const S* rv, const S* rw, const double* P,    \
+                   const GSW* w, PressConst c, double* incr, cudaStream_t st){                             \
+    gs_aux_bc_kernel<S><<<dim3((g.km - 1 + 127) / 128, g.jm - 2), 128, 0, st>>>(g, au, av, aw);           \
+    if(c.press_incr)                                                                                      \
+        gs_incr_kernel<S><<<dim3((g.km - 1 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(              \
+            g, ru, rv, rw, P, w, c, incr);                                                                \
+}                                                                                                         \
+void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S* av, const S* aw,         \
+                     const GSW* w, PressConst c, int s, cudaStream_t st){                                   \
+    const int n = (g.im - 2) * (g.jm - 2);                                                                \
+    gs_hyperplane_kernel<S><<<(n + 255) / 256, 256, 0, st>>>(g, P, incr, au, av, aw, w, c, s);            \
+}                                                                                                         \
+void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
+                    const RBW* w, PressConst c, double* src, cudaStream_t st){                             \
+    prep_rt_kernel<S><<<dim3((g.km - 1 + 127) / 128, (g.jm - 2) + (g.im - 2)), 128, 0, st>>>(             \
+        g, au, av, aw, ru, rv, rw, rigid_lid);                                                            \
+    prep_seam_kernel<S><<<(g.im * g.jm + 255) / 256, 256, 0, st>>>(g, au, av, aw, ru, rv, rw);            \
+    rb_src_kernel<S><<<dim3((g.km - 1 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(                   \
+        g, au, av, aw, w, c, src);                                                                        \
+}

@@ -1,0 +1,405 @@
+// RK4 step of the dynamical core: buoyancy reference level, hydrostatic column integral and the
+// four fused RHS + stage-update passes.
+//
+// Reference: planet/RungeKutta_Uran_Turb.cpp:18-404 and planet/RHS_Uran_Turb.cpp:20-1023.
+//
+// The reference runs each stage as two barrier-separated passes over all interior cells (pass A
+// evaluates RHSUran into 19 rhs_* arrays, pass B folds them into acc_* and writes the next stage
+// input). Here one kernel per stage does both for its cell: it reads the stage input X_s with a
+// 7-point stencil, forms the tendencies in registers and immediately writes acc and X_{s+1} to
+// a SEPARATE buffer (ping-pong), so no thread ever reads a value another thread of the same
+// launch writes. That removes the 19 rhs_* round trips through HBM. Stage 3 writes the new
+// state y_{n+1} in place of the state and the projection fields rhs_u/v/w, aux_u/v/w.
+//
+// Boundary rows (i = 0, im-1; j = 0, jm-1) are never integrated; the reference's stage inputs
+// keep the state's values there, so a neighbour on a boundary row is read from the state.
+//
+// Templates: S is the storage type of the state (double / float), C the arithmetic type. The
+// FP64 instantiation is compiled without FMA contraction and keeps the reference's operand order
+// in every expression, so it reproduces the CPU's IEEE results.
+#pragma once
+#include "common.cuh"
+
+namespace aturan {
+
+template <typename S, typename C>
+struct StageArgs {
+    Grid g;
+    const S* X;        // stage input: prognostic field q at X + q * fstride
+    const S* St;       // the state (read for boundary neighbours)
+    const S* Nc;       // start-of-step copies
+    S* acc;            // RK4 accumulator
+    S* Y;              // stage < 3: next stage input; stage 3: the state (y_{n+1})
+    const double* pdyn;      // FP64 always: p_dyn and p_hydro enter as differences
+    const double* phydro;
+    const S* forc;     // forcing group: field (id - ATURAN_NUE) at forc + m * fstride
+    S* proj;           // rhs_u, rhs_v, rhs_w, aux_u, aux_v, aux_w (stage 3 only)
+    const GeoIJ<C>* geo;
+    const C* cp_tab;
+    RhsConst<C> k;
+    C c_in, wgt;
+    int stage;
+};
+
+template <typename S>
+__device__ __forceinline__ S ld(const S* p){ return __ldg(p); }
+
+template <typename C>
+__device__ __forceinline__ C cmax(C a, C b){ return (a < b) ? b : a; }   // std::max
+template <typename C>
+__device__ __forceinline__ C cclamp(C v, C lo, C hi){ return v < lo ? lo : (v > hi ? hi : v); }
+
+// CpH2.h:77-84 and 122-134 (gas form): cp(T) from the equilibrium-H2 table.
+template <typename C>
+__device__ __forceinline__ C cp_lapse(const RhsConst<C>& k, const C* tab, C T){
+    C ch;
+    if(k.cp_mode <= 0) ch = k.cp_h2_const;
+    else {
+        const C Tc = T < C(5.0) ? C(5.0) : T;
+        const C x = ((Tc > C(1500.0) ? C(1500.0) : Tc) - C(5.0)) / C(0.5);
+        int i = (int)x; if(i > CP_TABLE_N - 2) i = CP_TABLE_N - 2;
+        const C f = x - (C)i;
+        const C a = __ldg(tab + i), b = __ldg(tab + i + 1);
+        ch = a + f * (b - a);
+    }
+    if(k.cp_gas) return (k.cp_rh2 * ch + k.cp_he_term + k.cp_ch4_term) / k.cp_rsum;
+    return k.cp_mix + k.cp_rh2 * (ch - k.cp_h2_const);   // cp_rh2 holds r_h2 / r_mix here
+}
+
+template <typename C>
+struct D6 { C c, d1r, d2r, d1t, d2t, d1p, d2p; };
+
+// RHS_Uran_Turb.cpp:93-176: central first and second differences of one field.
+template <typename S, typename C>
+__device__ __forceinline__ D6<C> stencil(const RhsConst<C>& k, const S* xc, const S* xim, const S* xip,
+                                         const S* xjm, const S* xjp, size_t o, size_t oim, size_t oip,
+                                         size_t ojm, size_t ojp, size_t okw, size_t oke){
+    D6<C> d;
+    const C c  = (C)ld(xc + o);
+    const C rp = (C)ld(xip + oip), rm = (C)ld(xim + oim);
+    const C tp = (C)ld(xjp + ojp), tm = (C)ld(xjm + ojm);
+    const C pe = (C)ld(xc + oke),  pw = (C)ld(xc + okw);
+    d.c   = c;
+    d.d1r = (rp - rm) * k.inv_2dr;
+    d.d2r = (rp - C(2.0) * c + rm) * k.inv_dr2;
+    d.d1t = (tp - tm) * k.inv_2dthe;
+    d.d2t = (tp - C(2.0) * c + tm) * k.inv_dthe2;
+    d.d1p = (pe - pw) * k.inv_2dphi;
+    d.d2p = (pe - C(2.0) * c + pw) * k.inv_dphi2;
+    return d;
+}
+
+// acc and next-stage / final update of one prognostic field (RungeKutta_Uran_Turb.cpp:291-403).
+// kind: 0 plain, 1 temperature (final clamp), 2 k* (clamp), 3 dis* (floor).
+template <typename S, typename C>
+__device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, size_t o, C r, int kind){
+    const size_t off = (size_t)q * a.g.fstride + o;
+    C accv;
+    if(a.stage == 0) accv = a.wgt * r;
+    else accv = (C)a.acc[off] + a.wgt * r;
+    const C yn = (C)ld(a.Nc + off);
+    if(a.stage < 3){
+        a.acc[off] = (S)accv;
+        C y = yn + a.c_in * r;
+        if(kind == 2) y = cclamp(y, C(0.0), a.k.tke_max);
+        else if(kind == 3) y = cmax(y, a.k.dis_min);
+        a.Y[off] = (S)y;
+    } else {
+        C y = yn + a.k.dt * accv / C(6.0);
+        if(kind == 1) y = cclamp(y, a.k.t_min, a.k.t_max);
+        else if(kind == 2) y = cclamp(cmax(y, C(0.0)), C(0.0), a.k.tke_max);
+        else if(kind == 3) y = cmax(y, a.k.dis_min);
+        a.Y[off] = (S)y;
+    }
+}
+
+template <typename S, typename C>
+__global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<C>& K = a.k;
+    const GeoIJ<C> geo = a.geo[i * g.jm + j];
+
+    const size_t o   = gidx(g, i, j, k);
+    const size_t oim = o - (size_t)g.jm * g.kp, oip = o + (size_t)g.jm * g.kp;
+    const size_t ojm = o - g.kp, ojp = o + g.kp;
+    const int kwi = phi_wrap(k - 1, g.km), kei = phi_wrap(k + 1, g.km);
+    const size_t okw = o - k + kwi, oke = o - k + kei;
+    const S* xim = (i == 1) ? a.St : a.X;
+    const S* xip = (i == g.im - 2) ? a.St : a.X;
+    const S* xjm = (j == 1) ? a.St : a.X;
+    const S* xjp = (j == g.jm - 2) ? a.St : a.X;
+    const size_t fs = g.fstride;
+#define STENCIL(q) stencil<S, C>(K, a.X + (size_t)(q) * fs, xim + (size_t)(q) * fs, xip + (size_t)(q) * fs, \
+                                 xjm + (size_t)(q) * fs, xjp + (size_t)(q) * fs, o, oim, oip, ojm, ojp, okw, oke)
+#define FORC(id) ((C)ld(a.forc + (size_t)((id) - ATURAN_NUE) * fs + o))
+
+    const C inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rmsinthe = geo.inv_rmsinthe;
+    const C inv_rm2sinthe = geo.inv_rm2sinthe, inv_rm2sinthe2 = geo.inv_rm2sinthe2;
+    const C costhe_inv_rm2sinthe = geo.costhe_inv_rm2sinthe, costhe = geo.costhe;
+    const C cotanthe = geo.cotanthe, two_inv_rm = geo.two_inv_rm;
+
+    // pressure gradients (:117, :146, :175), FP64 differences
+    const double* P = a.pdyn;
+    const C dpdr   = (C)((ld(P + oip) - ld(P + oim)) * (double)K.inv_2dr);
+    const C dpdthe = (C)((ld(P + ojp) - ld(P + ojm)) * (double)K.inv_2dthe);
+    const C dpdphi = (C)((ld(P + oke) - ld(P + okw)) * (double)K.inv_2dphi);
+
+    const D6<C> U = STENCIL(ATURAN_U), V = STENCIL(ATURAN_V), W = STENCIL(ATURAN_W);
+    const C u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
+
+    const C nue_c = FORC(ATURAN_NUE);
+    const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
+    const C nue_t_s = nue_t / C(0.9);
+    const C v_invrm = v_ijk * inv_rm;
+    const C w_invrs = w_ijk * inv_rmsinthe;
+
+    // ---- momentum (:208-331, :382-391, :717-788) ----
+    {
+        const C sinthe_bf = geo.sinthe_bf;
+        const C Coriolis_rad = K.m2om * sinthe_bf * w_ijk;
+        const C Coriolis_the = K.m2om * costhe * w_ijk;
+        const C Coriolis_phi = K.p2om * (costhe * v_ijk + sinthe_bf * u_ijk);
+        const C transport_u = u_ijk * U.d1r + v_invrm * U.d1t + w_invrs * U.d1p
+            - C(0.0) * (v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
+        const C transport_v = u_ijk * V.d1r + v_invrm * V.d1t + w_invrs * V.d1p
+            + (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
+        const C transport_w = u_ijk * W.d1r + v_invrm * W.d1t + w_invrs * W.d1p
+            + (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
+        const C v_metric = geo.v_metric;
+        const C diffusion_u = U.d2r + C(2.0) * u_ijk * inv_rm2 + U.d2t * inv_rm2
+            + C(4.0) * U.d1r * inv_rm + U.d1t * costhe_inv_rm2sinthe
+            + U.d2p * inv_rm2sinthe2;
+        const C diffusion_v = V.d2r + V.d1r * two_inv_rm + V.d2t * inv_rm2
+            + V.d1t * costhe_inv_rm2sinthe - v_metric * v_ijk
+            + V.d2p * inv_rm2sinthe2
+            + C(2.0) * U.d1t * inv_rm2
+            - W.d1p * C(2.0) * costhe * inv_rm2sinthe2;
+        const C diffusion_w = W.d2r + W.d1r * two_inv_rm + W.d2t * inv_rm2
+            + W.d1t * costhe_inv_rm2sinthe - v_metric * w_ijk
+            + W.d2p * inv_rm2sinthe2
+            + C(2.0) * U.d1p * inv_rm2sinthe
+            + V.d1p * C(2.0) * costhe * inv_rm2sinthe2;
+        const C dpdr_term   = dpdr   * K.scale_p;
+        const C dpdthe_term = dpdthe * K.scale_p * inv_rm;
+        const C dpdphi_term = dpdphi * K.scale_p * inv_rmsinthe;
+        const double* PH = a.phydro;
+        const C dphdthe_term = (C)((ld(PH + ojp) - ld(PH + ojm)) * (double)K.inv_2dthe) * inv_rm;
+        const C dphdphi_term = (C)((ld(PH + oke) - ld(PH + okw)) * (double)K.inv_2dphi) * inv_rmsinthe;
+        const C re_eff = K.re_eff;
+        const C rhs_u = - dpdr_term + C(0.0) - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
+                        - K.cor_rad_f * Coriolis_rad
+                        + K.cen_f * geo.cent_rad
+                        - geo.sponge * u_ijk;
+        const C rhs_v = - dpdthe_term - dphdthe_term - transport_v + diffusion_v / re_eff + diffusion_v * nue_t
+                        - K.cor_sc * Coriolis_the
+                        + K.cen_f * geo.cent_the;
+        const C rhs_w = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
+                        - K.cor_sc * Coriolis_phi;
+        stage_update(a, ATURAN_U, o, rhs_u, 0);
+        stage_update(a, ATURAN_V, o, rhs_v, 0);
+        stage_update(a, ATURAN_W, o, rhs_w, 0);
+        if(a.stage == 3){
+            a.proj[0 * fs + o] = (S)rhs_u;
+            a.proj[1 * fs + o] = (S)rhs_v;
+            a.proj[2 * fs + o] = (S)rhs_w;
+            a.proj[3 * fs + o] = (S)(rhs_u + dpdr_term);
+            a.proj[4 * fs + o] = (S)(rhs_v + dpdthe_term);
+            a.proj[5 * fs + o] = (S)(rhs_w + dpdphi_term);
+        }
+    }
+
+    // ---- temperature (:280-298, :329-334, :528-557) ----
+    {
+        const D6<C> T = STENCIL(ATURAN_T);
+        C pressure_t = K.ce_sp * (u_ijk * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
+        if(K.cp_dyn && T.c > C(0.0)) pressure_t *= K.cp_mix / cp_lapse(K, a.cp_tab, T.c * K.t_ref);
+        const C transport_t = u_ijk * T.d1r + v_invrm * T.d1t + w_invrs * T.d1p;
+        const C diffusion_t = T.d2r + T.d1r * two_inv_rm + T.d2t * inv_rm2
+            + T.d1t * costhe_inv_rm2sinthe + T.d2p * inv_rm2sinthe2;
+        const C tmf = (K.tmf != C(0.0)) ? K.tmf * FORC(ATURAN_THERMALMASSFLUX) : C(0.0);
+        C precip_t = C(0.0);
+        if(K.precip_coupling != C(0.0)){
+            precip_t = K.precip_coupling * FORC(ATURAN_Q_PRECIP) * K.precip_L / K.precip_den;
+            if(!isfinite(precip_t)) precip_t = C(0.0);
+            else if(precip_t >  C(0.5)) precip_t =  C(0.5);
+            else if(precip_t < -C(0.5)) precip_t = -C(0.5);
+        }
+        const C rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
+                        - tmf + C(0.0) + precip_t;
+        stage_update(a, ATURAN_T, o, rhs_t, 1);
+    }
+
+    // ---- the twelve condensables (:790-850), one at a time ----
+#pragma unroll 1
+    for(int s = 0; s < 12; s++){
+        const int q = ATURAN_CH4 + s;
+        const D6<C> Q = STENCIL(q);
+        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
+        const C diffusion = Q.d2r + Q.d1r * two_inv_rm + Q.d2t * inv_rm2
+            + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
+        C r = - transport + diffusion / K.sc_re[s / 3] + diffusion * nue_t_s;
+        if(q == ATURAN_H2S) r = r + K.chemical_reaction * FORC(ATURAN_MASSFLUX_H2S);
+        if(q == ATURAN_NH3) r = r + K.chemical_reaction * FORC(ATURAN_MASSFLUX_NH3);
+        r = r + K.precip_coupling * FORC(ATURAN_S_PRECIP_CH4 + s);
+        stage_update(a, q, o, r, 0);
+    }
+
+    // ---- NH4SH: flux limiter, chemistry and Stokes settling (:852-913) ----
+    {
+        const D6<C> Q = STENCIL(ATURAN_NH4SH);
+        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
+        const C diffusion = Q.d2r + Q.d1r * two_inv_rm + Q.d2t * inv_rm2
+            + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
+        const C v_stokes = K.stokes_a * (K.rho_cond_nh4sh - FORC(ATURAN_RHO_MIX)) * K.g / K.mue_mix;
+        const C r = - transport + FORC(ATURAN_FLUXLIM_NH4SH)
+                    + diffusion / K.sc_re[4] + diffusion * nue_t_s
+                    + K.chemical_reaction * FORC(ATURAN_MASSFLUX_NH4SH)
+                    + (v_stokes / K.u_0) * Q.d1r;
+        stage_update(a, ATURAN_NH4SH, o, r, 0);
+    }
+
+    // ---- k* and dis* (:989-1018) ----
+    if(K.turb_active){
+#pragma unroll 1
+        for(int n = 0; n < 2; n++){
+            const int q = ATURAN_TKE + n;
+            const D6<C> Q = STENCIL(q);
+            const C transport = u_ijk * Q.d1r + v_ijk * Q.d1t * inv_rm + w_ijk * Q.d1p * inv_rmsinthe;
+            const C diffusion = Q.d2r + Q.d1r * C(2.0) * inv_rm + Q.d2t * inv_rm2
+                + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
+            const C sig = n == 0 ? C(0.85) : C(0.5);
+            const C r = - transport + diffusion * (K.inv_re + nue_c / sig)
+                        + FORC(n == 0 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE);
+            stage_update(a, q, o, r, n == 0 ? 2 : 3);
+        }
+    }
+#undef STENCIL
+#undef FORC
+}
+
+// ---- RungeKutta_Uran_Turb.cpp:18-37: per level, sin(theta)-weighted mean of g p / (r R T t_ref)
+// over every cell with T > 0 and a finite value. Fast form: each block reduces a contiguous
+// chunk of one level in a fixed tree order into partials[level][block]; a second kernel adds a
+// level's partials in block order. Deterministic run to run; the order differs from the
+// reference's serial j, k sum, which moves the mean by about an ulp. ----
+template <typename S>
+__global__ void __launch_bounds__(256) buoy_partial_kernel(Grid g, const S* t, const S* ps, const double* wsin,
+                                                           HydroConst h, double* part_sum, double* part_w, int nblk){
+    const int lev = blockIdx.y;
+    const int ncell = g.jm * g.km;
+    double s = 0.0, w = 0.0;
+    for(int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += nblk * blockDim.x){
+        const int j = c / g.km, k = c - j * g.km;
+        const size_t o = gidx(g, lev, j, k);
+        const double T = (double)__ldg(t + o);
+        if(!(T > 0.0)) continue;
+        const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
+        if(!isfinite(b)) continue;
+        const double wg = wsin[j];
+        s += wg * b;
+        w += wg;
+    }
+    __shared__ double ss[256], sw[256];
+    ss[threadIdx.x] = s; sw[threadIdx.x] = w;
+    __syncthreads();
+    for(int st = 128; st > 0; st >>= 1){
+        if(threadIdx.x < st){ ss[threadIdx.x] += ss[threadIdx.x + st]; sw[threadIdx.x] += sw[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0){ part_sum[lev * nblk + blockIdx.x] = ss[0]; part_w[lev * nblk + blockIdx.x] = sw[0]; }
+}
+
+static __global__ void buoy_finish_kernel(int im, int nblk, const double* part_sum, const double* part_w, double* ref){
+    const int lev = blockIdx.x * blockDim.x + threadIdx.x;
+    if(lev >= im) return;
+    double s = 0.0, w = 0.0;
+    for(int b = 0; b < nblk; b++){ s += part_sum[lev * nblk + b]; w += part_w[lev * nblk + b]; }
+    ref[lev] = (w > 0.0) ? s / w : 0.0;
+}
+
+// Exact form: the reference's serial j-then-k order, one thread per level. Bit-equal to the
+// reference; kept for parity runs (exact_reductions = 1).
+template <typename S>
+__global__ void buoy_serial_kernel(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* ref){
+    const int lev = blockIdx.x * blockDim.x + threadIdx.x;
+    if(lev >= g.im) return;
+    double s = 0.0, w = 0.0;
+    for(int j = 0; j < g.jm; j++){
+        const double wg = wsin[j];
+        for(int k = 0; k < g.km; k++){
+            const size_t o = gidx(g, lev, j, k);
+            const double T = (double)__ldg(t + o);
+            if(!(T > 0.0)) continue;
+            const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
+            if(!isfinite(b)) continue;
+            s += wg * b;
+            w += wg;
+        }
+    }
+    ref[lev] = (w > 0.0) ? s / w : 0.0;
+}
+
+// ---- RungeKutta_Uran_Turb.cpp:62-177: per column (j, k) -- every column, the seam copy and the
+// pole rows included -- the trapezoid integral from the base of the buoyancy anomaly and the
+// metric + radial Coriolis force, plus p_baro minus what p_bfollow has taken up of B(t) - B0.
+// One thread per column, marching up i with coalesced rows along k. ----
+template <typename S>
+__global__ void __launch_bounds__(256) hydro_kernel(Grid g, const S* t, const S* ps, const S* v, const S* w,
+                                                    const double* ref, const double* rm_i, const double* cor_j,
+                                                    const double* pbaro, const double* pb0, double* pbf,
+                                                    double* ph, HydroConst h, int advance){
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= g.jm * g.km) return;
+    const int j = c / g.km, k = c - j * g.km;
+    const double cor_ = cor_j[j];
+    auto buoy = [&](int i) -> double {
+        const size_t o = gidx(g, i, j, k);
+        const double T = (double)__ldg(t + o);
+        if(!(T > 0.0)) return 0.0;
+        const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref) - ref[i];
+        const double f = h.m_nd_rel_b * b / ref[i];
+        return isfinite(f) ? f : 0.0;
+    };
+    auto met0 = [&](int i) -> double {
+        const size_t o = gidx(g, i, j, k);
+        const double vv = (double)__ldg(v + o), ww = (double)__ldg(w + o);
+        return (vv * vv + ww * ww) / rm_i[i] + cor_ * ww;
+    };
+    if(h.follow_on){
+        double Pm = 0.0, Pb = 0.0;
+        double m_prev = met0(0), b_prev = buoy(0);
+        for(int i = 0; i < g.im; i++){
+            if(i > 0){
+                const double m_i = met0(i), b_i = buoy(i);
+                Pm += 0.5 * (m_prev + m_i) * h.dr;
+                Pb += 0.5 * (b_prev + b_i) * h.dr;
+                m_prev = m_i; b_prev = b_i;
+            }
+            const size_t o = gidx(g, i, j, k);
+            double bf = pbf[o];
+            if(advance){ bf += (Pb - pb0[o] - bf) / h.follow_tau; pbf[o] = bf; }
+            ph[o] = Pm + Pb + pbaro[o] - bf;
+        }
+    } else {
+        // ATURAN_PBARO_FOLLOW=0: f_(i) = buoy(i) + (v^2 + w^2) / rm + cor_ w, :134-161
+        auto f_ = [&](int i) -> double {
+            const size_t o = gidx(g, i, j, k);
+            const double vv = (double)__ldg(v + o), ww = (double)__ldg(w + o);
+            return buoy(i) + (vv * vv + ww * ww) / rm_i[i] + cor_ * ww;
+        };
+        double prev = 0.0, fp = f_(0);
+        ph[gidx(g, 0, j, k)] = 0.0 + pbaro[gidx(g, 0, j, k)];
+        for(int i = 1; i < g.im; i++){
+            const double fi = f_(i);
+            prev = prev + 0.5 * (fp + fi) * h.dr;
+            fp = fi;
+            ph[gidx(g, i, j, k)] = prev + pbaro[gidx(g, i, j, k)];
+        }
+    }
+}
+
+}  // namespace aturan

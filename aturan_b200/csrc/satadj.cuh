@@ -1,0 +1,256 @@
+// Mixed-phase saturation adjustment (Tao et al. 1988) of up to four condensables, fused per cell.
+//
+// Reference: planet/SaturationAdjustment.h:255-746 (the shared routine the model selects,
+// SaturationAdjustmentUran.cpp:208-239), called for H2O, H2S, NH3, CH4 in that order
+// (cUranusModel.cpp:998-1027). Every cell is independent and each call ends with a clamp of its
+// own three fields, so running the four gases back to back inside one thread, temperature
+// carried in a register, gives the same result as four sweeps over the grid while reading
+// t, p_stat and rho_mix once and writing t once.
+//
+// The arithmetic is FP64 whatever the storage type S (the Clausius-Clapeyron Newton iteration
+// is the part of the step the mixed-precision form keeps in FP64). Every iteration is capped at
+// the reference's 15 passes; nothing here can spin.
+#pragma once
+#include "common.cuh"
+
+namespace aturan {
+
+struct GasConst {
+    double t_0, t_00, ep, lv, ls;
+    double C, L0, den, del_alf, del_bet;        // den = 1e-3 * R (ATPhys.h:52)
+    double C_i, L0_i, del_alf_i, del_bet_i;
+    double t_range_inv, Lf;
+    int freeze_on;
+};
+
+struct SatConst {
+    GasConst gas[4];
+    double cp_mix, t_ref, r_mix;
+    int conserve, newton, evap, ice_entry, bergeron, dry_exit, local_rho;
+};
+
+// ATPhys.h:49-53
+__device__ __forceinline__ double svp(double T, double C, double L0, double den, double a, double b){
+    return exp(C + (-L0 / T + a * log(T) + b * T) / den);
+}
+
+template <typename S>
+struct SatArgs {
+    Grid g;
+    S* t; const S* ps; const S* rho_mix;
+    S* spec[4][3];          // (vapour, cloud, ice) per gas in the loop's order
+    SatConst k;
+    int gas_mask;
+    unsigned long long* counters;   // [0] adjusted, [1] not converged (summed over gases)
+};
+
+template <typename S>
+__global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    unsigned n_adj = 0, n_nc = 0;
+    if(k < g.km){
+        const size_t q = gidx(g, i, j, k);
+        const SatConst& K = a.k;
+        double tt = (double)a.t[q];
+        const double p_u = (double)__ldg(a.ps + q);
+        double rho_c = K.r_mix;                               // rho_at, cUranusModel.h:526-531
+        if(K.local_rho){ const double r_ = (double)__ldg(a.rho_mix + q); rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : K.r_mix; }
+        const double cp_mix = K.cp_mix, t_ref = K.t_ref;
+        for(int gi = 0; gi < 4; gi++){
+            if(!(a.gas_mask & (1 << gi))) continue;
+            const GasConst& G = K.gas[gi];
+            S* cP = a.spec[gi][0]; S* clP = a.spec[gi][1]; S* iP = a.spec[gi][2];
+            double c = (double)cP[q], cloud = (double)clP[q], ice = (double)iP[q];
+            double t_u = tt * t_ref;
+            // :358 skip cells without a usable state
+            if((t_u > 0.0) && (p_u > 0.0)){
+                const double t_0 = G.t_0, t_00 = G.t_00, Lf = G.Lf;
+                if(t_u > t_0){                                        // :365-385
+                    if(K.conserve){
+                        if(ice > 0.0){
+                            double dm = ice;
+                            if(Lf > 0.0){
+                                const double hc = cp_mix * rho_c;
+                                const double cap = hc * (t_u - t_0) / Lf;
+                                if(dm > cap) dm = cap;
+                                t_u -= Lf * dm / hc;
+                                tt = t_u / t_ref;
+                            }
+                            ice -= dm;
+                            cloud += dm;
+                        }
+                    } else {
+                        ice = 0.0;
+                    }
+                }
+                if(G.freeze_on && t_u < t_00 && cloud > 0.0){         // :388-399
+                    double dm = cloud;
+                    if(Lf > 0.0){
+                        const double hc = cp_mix * rho_c;
+                        const double cap = hc * (t_00 - t_u) / Lf;
+                        if(dm > cap) dm = cap;
+                        t_u += Lf * dm / hc;
+                        tt = t_u / t_ref;
+                    }
+                    cloud -= dm;
+                    ice += dm;
+                }
+                if(c < 0.0) c = 0.0;                                  // :400-402
+                if(cloud < 0.0) cloud = 0.0;
+                if(ice < 0.0) ice = 0.0;
+
+                const double ep = G.ep, lv = G.lv, ls = G.ls, tri = G.t_range_inv;
+                const double q_Rain_0 = rho_c * ep * svp(t_u, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                bool go = q_Rain_0 > 0.0;                             // :422
+                if(go){
+                    double q_entry = q_Rain_0;
+                    if(K.ice_entry && cloud <= 0.0 && ice <= 0.0){
+                        const double cnd0 = t_u <= t_00 ? 0.0 : (t_u >= t_0 ? 1.0 : (t_u - t_00) * tri);
+                        if(cnd0 < 1.0)
+                            q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * rho_c * ep
+                                    * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                    }
+                    if(K.bergeron >= 2 && cloud <= 0.0 && ice <= 0.0 && t_u < t_0)
+                        q_entry = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                    if(c <= q_entry){                                 // :436-448
+                        const double q_c0 = cloud, q_i0 = ice;
+                        if(!K.evap || !K.conserve || (q_c0 <= 0.0 && q_i0 <= 0.0)) go = false;
+                        else {
+                            const double q_Ice_0 = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            double q_t0;
+                            if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
+                            else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
+                            else                         q_t0 = q_Ice_0;
+                            if(fabs(c - q_t0) <= 1.0e-3 * q_t0) go = false;
+                        }
+                    }
+                }
+                if(go){
+                    // ---- :450-590, at most 15 passes ----
+                    double q_v_b = c, q_c_b = cloud, q_i_b = ice;
+                    double T = t_u, q_v_hyp = q_v_b;
+                    bool found = false, dry = false;
+                    double q_rain_now = q_Rain_0;
+                    for(int itr = 1; itr <= 15; itr++){
+                        double CND = (T - t_00) * tri;
+                        double DEP = (t_0 - T) * tri;
+                        if(T <= t_00){ CND = 0.0; DEP = 1.0; }
+                        if(T >= t_0) { CND = 1.0; DEP = 0.0; }
+                        const bool berg = K.bergeron != 0 && T < t_0 && q_v_b <= q_rain_now
+                                        && (q_i_b > 0.0 || (K.bergeron >= 2 && q_c_b <= 0.0));
+                        if(berg){
+                            CND = 0.0; DEP = 1.0;
+                            if(q_c_b > 0.0){
+                                T -= lv * q_c_b / (cp_mix * rho_c);
+                                q_v_b += q_c_b;
+                                q_c_b = 0.0;
+                            }
+                        }
+                        double d_q_v = q_v_hyp - q_v_b;
+                        double d_q_c = -d_q_v * CND;
+                        double d_q_i = -d_q_v * DEP;
+                        if(K.conserve){
+                            if(d_q_v < -q_v_b){ d_q_v = -q_v_b; d_q_c = -d_q_v * CND; d_q_i = -d_q_v * DEP; }
+                            if(q_c_b + d_q_c < 0.0){ const double ex = -(q_c_b + d_q_c); d_q_c = -q_c_b; d_q_i -= ex; }
+                            if(q_i_b + d_q_i < 0.0){ const double ex = -(q_i_b + d_q_i); d_q_i = -q_i_b; d_q_c -= ex;
+                                                     if(q_c_b + d_q_c < 0.0) d_q_c = -q_c_b; }
+                            d_q_v = -(d_q_c + d_q_i);
+                        }
+                        T     += (lv * d_q_c + ls * d_q_i) / (cp_mix * rho_c);
+                        q_v_b += d_q_v;
+                        q_c_b += d_q_c;
+                        q_i_b += d_q_i;
+                        if(q_v_b < 0.0) q_v_b = 0.0;
+                        if(q_c_b < 0.0) q_c_b = 0.0;
+                        if(q_i_b < 0.0) q_i_b = 0.0;
+
+                        const double q_Rain = rho_c * ep * svp(T, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                        const double q_Ice  = rho_c * ep * svp(T, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                        q_rain_now = q_Rain;
+                        if(q_c_b > 0.0 && q_i_b > 0.0)
+                            q_v_hyp = (q_c_b * q_Rain + q_i_b * q_Ice) / (q_c_b + q_i_b);
+                        else if(K.bergeron >= 2 && q_c_b <= 0.0 && q_i_b <= 0.0 && T < t_0) q_v_hyp = q_Ice;
+                        else if(K.ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0){
+                            const double cn = T <= t_00 ? 0.0 : (T >= t_0 ? 1.0 : (T - t_00) * tri);
+                            q_v_hyp = cn * q_Rain + (1.0 - cn) * q_Ice; }
+                        else if(q_i_b == 0.0) q_v_hyp = q_Rain;
+                        else                  q_v_hyp = q_Ice;
+
+                        if(T >= t_0){
+                            if(K.conserve){
+                                if(q_i_b > 0.0){
+                                    double dm = q_i_b;
+                                    if(Lf > 0.0){
+                                        const double hc = cp_mix * rho_c;
+                                        const double cap = hc * (T - t_0) / Lf;
+                                        if(dm > cap) dm = cap;
+                                        T -= Lf * dm / hc;
+                                    }
+                                    q_i_b -= dm;
+                                    q_c_b += dm;
+                                }
+                            } else {
+                                q_i_b = 0.0;
+                            }
+                        }
+                        const double q_diff = fabs(q_v_b - q_v_hyp) / (q_v_hyp + 1e-20);
+                        if(q_diff <= 1.0e-3){ found = true; break; }
+                        if(K.dry_exit && K.conserve && q_c_b <= 0.0 && q_i_b <= 0.0 && q_v_b < q_v_hyp){ dry = true; break; }
+                        if(K.newton){
+                            const double dT = 0.1;
+                            const double q_Rain_d = rho_c * ep * svp(T + dT, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                            const double q_Ice_d  = rho_c * ep * svp(T + dT, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            double q_hyp_d;
+                            if(q_c_b > 0.0 && q_i_b > 0.0)
+                                q_hyp_d = (q_c_b * q_Rain_d + q_i_b * q_Ice_d) / (q_c_b + q_i_b);
+                            else if(K.bergeron >= 2 && q_c_b <= 0.0 && q_i_b <= 0.0 && T < t_0) q_hyp_d = q_Ice_d;
+                            else if(K.ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0){
+                                const double cn = T <= t_00 ? 0.0 : (T >= t_0 ? 1.0 : (T - t_00) * tri);
+                                q_hyp_d = cn * q_Rain_d + (1.0 - cn) * q_Ice_d; }
+                            else if(q_i_b == 0.0) q_hyp_d = q_Rain_d;
+                            else                  q_hyp_d = q_Ice_d;
+                            double CNDn = (T - t_00) * tri;
+                            if(T <= t_00) CNDn = 0.0;
+                            if(T >= t_0)  CNDn = 1.0;
+                            if(berg)      CNDn = 0.0;
+                            const double Gf = (lv * CNDn + ls * (1.0 - CNDn)) / (cp_mix * rho_c)
+                                            * (q_hyp_d - q_v_hyp) / dT;
+                            const double Gp = (Gf < 0.0) ? 0.0 : Gf;          // std::max(G, 0.0)
+                            double wn = 1.0 / (1.0 + Gp);
+                            if(wn < 0.05) wn = 0.05;
+                            q_v_hyp = q_v_b + wn * (q_v_hyp - q_v_b);
+                        } else {
+                            q_v_hyp = 0.5 * (q_v_hyp + q_v_b);
+                        }
+                    }
+                    n_adj++;
+                    if(!found && !dry) n_nc++;
+                    c = q_v_b; cloud = q_c_b; ice = q_i_b;
+                    tt = T / t_ref;
+                }
+            }
+            // final clamp of this gas's fields over every cell (:673-685)
+            if(c <= 0.0) c = 0.0;
+            if(cloud <= 0.0) cloud = 0.0;
+            if(ice <= 0.0) ice = 0.0;
+            cP[q] = (S)c; clP[q] = (S)cloud; iP[q] = (S)ice;
+        }
+        a.t[q] = (S)tt;
+    }
+    // per-block counter reduction: integer adds, order-independent
+    __shared__ unsigned s_adj, s_nc;
+    if(threadIdx.x == 0){ s_adj = 0; s_nc = 0; }
+    __syncthreads();
+    if(n_adj) atomicAdd(&s_adj, n_adj);
+    if(n_nc) atomicAdd(&s_nc, n_nc);
+    __syncthreads();
+    if(threadIdx.x == 0 && a.counters){
+        if(s_adj) atomicAdd(a.counters + 0, (unsigned long long)s_adj);
+        if(s_nc) atomicAdd(a.counters + 1, (unsigned long long)s_nc);
+    }
+}
+
+}  // namespace aturan

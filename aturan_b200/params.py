@@ -30,7 +30,8 @@ _INT_FIELDS = (
     "abi_version", "im", "jm", "km", "precision", "turb_active", "coriolis_full",
     "cp_h2_mode", "cp_gas", "cp_dyn", "press_consistent", "press_incr", "rigid_lid",
     "satadj_conserve", "satadj_newton", "satadj_evap", "satadj_ice_entry",
-    "satadj_bergeron", "satadj_freeze", "satadj_dry_exit", "local_rho", "nh4sh_sync")
+    "satadj_bergeron", "satadj_freeze", "satadj_dry_exit", "local_rho", "nh4sh_sync",
+    "exact_reductions")
 _DBL_FIELDS = (
     "r0", "dr", "the0", "dthe", "phi0", "dphi", "dt", "metric_R_km", "sinthe_min",
     "L_atm", "u_0", "t_ref", "g", "omega", "re", "pr",
@@ -45,7 +46,7 @@ _DBL_FIELDS = (
 
 class Params(ctypes.Structure):
     _fields_ = ([(n, ctypes.c_int32) for n in _INT_FIELDS]
-                + [("reserved_i", ctypes.c_int32 * 8)]
+                + [("reserved_i", ctypes.c_int32 * 7)]
                 + [(n, ctypes.c_double) for n in _DBL_FIELDS]
                 + [("reserved_d", ctypes.c_double * 8), ("gas", Gas * 4)])
 
@@ -79,6 +80,7 @@ DEFAULTS = dict(
     press_consistent=1, press_incr=1, rigid_lid=1,
     satadj_conserve=1, satadj_newton=1, satadj_evap=1, satadj_ice_entry=0,
     satadj_bergeron=2, satadj_freeze=1, satadj_dry_exit=1, local_rho=1, nh4sh_sync=1,
+    exact_reductions=0,
     r0=1.0, dr=0.025, the0=0.0, dthe=1.0 / (180.0 / math.pi), phi0=0.0,
     dphi=1.0 / (180.0 / math.pi), dt=0.001, metric_R_km=25362.0, sinthe_min=0.4,
     L_atm=225.0, u_0=100.0, t_ref=76.4, g=8.69, omega=0.000101, re=1000.0, pr=0.69,

@@ -1,0 +1,389 @@
+"""Throughput of the ATURAN dynamical-core step on B200: cell-steps/s at 41 x 181 x 361.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--press gs|rb|sor]
+
+A step is one pass of the hot path over the synthetic seeded state: the pressure solve, the four
+saturation adjustments (H2O, H2S, NH3, CH4), the n-copy sync and the RK4 step -- the in-scope
+calls of one even iteration of cUranusModel::Run (planet/cUranusModel.cpp:967-1123). The
+headline workload is the mixed-precision full step (FP32 state and stencils, FP64 pressure and
+saturation-adjustment Newton iteration); --precision fp64 runs the plain FP64 path.
+
+One process per GPU (torchrun for N > 1). The path has no exchange step at this grid size, so
+ranks run independent replicas (weak scaling); NCCL carries only the barrier and the max of the
+per-rank times. Rank 0 prints one JSON line.
+
+--impl reference times the reference's own CPU implementation (the compiled unmodified sources
+in oracle/_ref, all host threads; the C restatement in oracle/ when that was not built) on the
+same workload; under torchrun only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 41 * 181 * 361          # the metric's N: stored cells of the shell
+METRIC = "cell-steps/s at 41x181x361"
+
+# Algorithmic words per stored cell of one RK4 stage launch (fused RHS + stage update: stage
+# input, start-of-step copies, accumulator, pressure pair, pointwise inputs; writes acc and the
+# next stage input) and of the step's other kernels.
+STAGE_WORDS = (81, 119, 119, 106)
+STEP_OTHER_WORDS = {"hydro": 11, "satadj": 28, "gs_per_sweep": 3, "gs_source": 5}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def press_args(name):
+    from aturan_b200 import params as P
+    if name == "gs":
+        return dict(kind=P.PRESS_GS_LEX, omega=1.0, max_sweeps=1, tol=0.0), "GS_LEX: one lexicographic sweep (PressureSolverUran)"
+    if name == "rb":
+        return dict(kind=P.PRESS_RB_SHARED, omega=1.0, max_sweeps=1, tol=0.0), "RB_SHARED: one red-black sweep (PressureSolver)"
+    return dict(kind=P.PRESS_RB_SOR, omega=1.8, max_sweeps=400, tol=1e-6), "RB_SOR to relative residual 1e-6, omega 1.8"
+
+
+def algorithmic_stage_bytes(precision):
+    """Average algorithmic bytes per RK4 stage launch over the shell's stored cells."""
+    total = 0.0
+    for w in STAGE_WORDS:
+        if precision == "fp64":
+            total += w * 8
+        else:          # FP32 storage except the FP64 pressure pair read by every stage
+            total += (w - 2) * 4 + 2 * 8
+    return total / 4 * N_CELLS
+
+
+def cpu_reference_step_time(nsteps, press, budget_s=120.0):
+    """Time the reference's own step on the host cores after one untimed warm-up step; at most
+    nsteps steps and no more than fit in budget_s. Returns (seconds/step, kind, cores, note, n)."""
+    from oracle import ref as R
+    from aturan_b200 import params as P, state as S
+    cores = os.cpu_count() or 1
+    p = P.default_params()
+    if R.available():
+        m = R.Ref.get_instance()
+        m.load(S.perturb(m.state(), p, seed=20261204))
+
+        def one():
+            if press == "rb":
+                m.pressure_rb(1)
+            else:
+                m.pressure_gs()
+            for g in range(4):
+                m.satadj(g)
+            m.sync_ncopies()
+            m.rk4()
+        kind = "reference"
+        what = f"the compiled reference (oracle/_ref, -O3, OpenMP {cores} threads) on its own initialised state, perturbed"
+    else:
+        from oracle import Oracle
+        O = Oracle()
+        O.set_threads(cores)
+        st = S.synthetic_state(p, seed=20261204)
+        pk = P.PRESS_RB_SHARED if press == "rb" else P.PRESS_GS_LEX
+
+        def one():
+            O.step(p, st, pk)
+        kind = "port"
+        what = f"the C restatement (oracle/, OpenMP {cores} threads) on the synthetic state"
+    t0 = time.perf_counter()
+    one()                                          # warm-up, also the time estimate
+    t_warm = time.perf_counter() - t0
+    n = max(1, min(nsteps, int(budget_s / max(t_warm, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        one()
+    dt = (time.perf_counter() - t0) / n
+    return dt, kind, cores, f"{n} full steps (GS/RB pressure + 4 SatAdj + sync + RK4) of {what}, 41x181x361", n
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    dt, kind, cores, note, n = cpu_reference_step_time(max(1, args.steps), args.press)
+    value = N_CELLS / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "impl": "reference",
+        "n_gpus": world, "steps": n, "warmup": 1, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "dynamical-core full step (pressure + 4 SatAdj + n-copy sync + RK4), 41x181x361, "
+                               "FP64 on the host cores",
+                   "grid": [41, 181, 361], "cells": N_CELLS, "pressure": args.press},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind, "sample": note},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--press", default="gs", choices=["gs", "rb", "sor"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only the warm-up and the K timed steps (for ncu); prints a short line")
+    ap.add_argument("--grid", default="41x181x361", help="IxJxK of the shell (profiling cases)")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+
+    from aturan_b200 import api, params as P, state as S
+    prec = P.MIXED if args.precision == "mixed" else P.FP64
+    gi, gj, gk = (int(x) for x in args.grid.lower().split("x"))
+    p = P.default_params(gi, gj, gk, precision=prec)
+    st = S.synthetic_state(p, seed=20261203 + rank)
+    ctx = api.Context(p)
+    ctx.upload_state(st)
+    pa, press_note = press_args(args.press)
+
+    def step():
+        ctx.step(**pa)
+
+    W = max(3, args.warmup)
+    for _ in range(W):
+        step()
+    ctx.synchronize()
+    if args.profile_run:
+        for _ in range(args.steps):
+            step()
+        ctx.synchronize()
+        print(json.dumps({"profile_run": True, "grid": args.grid, "precision": args.precision,
+                          "steps": args.steps, "warmup": W}), flush=True)
+        ctx.close()
+        return
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: K steps, device time on the context's stream, max over ranks ----
+    K = args.steps
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.profile(timing=False)
+    e0.record(stream)
+    for _ in range(K):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = sum(v[0] for v in ctx.profile_read().values())
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = N_CELLS * K * world / (ms_max / 1e3)
+
+    # ---- per-kernel device times of the same steps (event-bracketed pass) ----
+    ctx.profile(timing=True)
+    for _ in range(K):
+        step()
+    prof = ctx.profile_read()
+    n_stage, ms_stage = prof["rk_stage"]
+    avg_stage_ms = ms_stage / max(n_stage, 1)
+    alg = algorithmic_stage_bytes(args.precision)
+    peak, peak_kind = peaks()
+    achieved = alg / (avg_stage_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", f"rk_stage_{args.precision}_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the C ABI with host buffers ----
+    from aturan_b200 import fields as F
+    in_names = F.NAMES
+    out_names = F.PROGNOSTIC + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION
+    pinned = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in in_names}
+    outs = {n: torch.empty(p.shape, dtype=torch.float64).pin_memory() for n in out_names}
+    barrier()
+    E = max(1, args.e2e_steps)
+    t0 = time.perf_counter()
+    for _ in range(E):
+        for n in in_names:
+            ctx.L.aturan_upload(ctx.h, F.ID[n], pinned[n].data_ptr())
+        step()
+        for n in out_names:
+            ctx.L.aturan_download(ctx.h, F.ID[n], outs[n].data_ptr())
+    e2e_s = time.perf_counter() - t0
+    tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = N_CELLS * E * world / float(tt.item())
+    fbytes = p.im * p.jm * p.km * 8
+
+    # ---- accuracy of the mixed step against the FP64 step (which matches the FP64 oracle) ----
+    accuracy = None
+    if args.precision == "mixed" and rank == 0:
+        accuracy = mixed_accuracy(api, P, S, F, pa)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            dt, kind, cores, note, _ = cpu_reference_step_time(max(1, args.cpu_steps), args.press, budget_s=30.0)
+            cpu = {"value": N_CELLS / dt, "unit": "cell-steps/s", "cores": cores, "kind": kind, "sample": note}
+        except Exception as ex:          # reported, never silently replaced
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": f"{type(ex).__name__}: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic seeded state (aturan_b200.state.synthetic_state)",
+            "config": {"workload": f"dynamical-core full step: pressure ({press_note}) + 4 SatAdj + n-copy sync + RK4, "
+                                   f"41x181x361, {args.precision}",
+                       "grid": [41, 181, 361], "cells": N_CELLS, "precision": args.precision,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (working set > 1.5 GB), no flush"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "rk_stage_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs", "avg_launch_ms": avg_stage_ms,
+                         "alg_bytes_per_launch": alg},
+            "kernels_ms_per_step": {k: v[1] / K for k, v in prof.items()},
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(in_names) * fbytes,
+                    "d2h_bytes_per_step": len(out_names) * fbytes, "steps": E},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        if accuracy is not None:
+            line["accuracy_vs_fp64"] = accuracy
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def mixed_accuracy(api, P, S, F, pa, steps=(1, 10)):
+    """Per-field max |mixed - fp64| / max |fp64| after 1 and 10 steps from the same state."""
+    p64 = P.default_params(precision=P.FP64)
+    p32 = P.default_params(precision=P.MIXED)
+    st = S.synthetic_state(p64, seed=99)
+    c64, c32 = api.Context(p64), api.Context(p32)
+    c64.upload_state(st)
+    c32.upload_state(st)
+    I = (slice(1, 40), slice(1, 180), slice(0, 360))
+    out = {}
+    done = 0
+    for n in steps:
+        while done < n:
+            c64.step(**pa)
+            c32.step(**pa)
+            done += 1
+        errs = {}
+        for f in ("t", "u", "v", "w", "p_dyn", "h2o", "ch4", "nh3", "h2s"):
+            a, b = c32.download(f)[I], c64.download(f)[I]
+            s = np.abs(b).max()
+            errs[f] = float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
+        out[f"step{n}"] = errs
+    c64.close()
+    c32.close()
+    return out
+
+
+if __name__ == "__main__":
+    main()

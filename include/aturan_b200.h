@@ -106,7 +106,10 @@ typedef struct aturan_params {
     int32_t satadj_conserve, satadj_newton, satadj_evap, satadj_ice_entry;
     int32_t satadj_bergeron, satadj_freeze, satadj_dry_exit, local_rho;
     int32_t nh4sh_sync;          /* RK_SCALAR_SYNC also copies nh4sh (ATURAN_NH4SH_EQ) */
-    int32_t reserved_i[8];
+    int32_t exact_reductions;    /* 1: the level means of the buoyancy reference are summed in
+                                    the reference's serial order (bit-exact, slow); 0: a fixed
+                                    tree order (deterministic run to run, ~1 ulp from serial) */
+    int32_t reserved_i[7];
 
     double r0, dr, the0, dthe, phi0, dphi, dt;
     double metric_R_km;          /* ATURAN_METRIC_RADIUS; <= 0 keeps the unshifted rad.z */
@@ -189,6 +192,24 @@ int aturan_sync_ncopies(aturan_ctx* ctx);
  * pressure (kind/omega/max_sweeps/tol as aturan_pressure), the four saturation adjustments,
  * the n-copy sync and the RK4 step. */
 int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol);
+
+/* Kernel classes for the per-class launch counts and timings below. */
+enum aturan_kernel_kind {
+    ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
+    ATURAN_K_SATADJ,         /* fused 4-gas saturation adjustment */
+    ATURAN_K_GS,             /* PressureSolverUran sweep (incl. its source and boundary passes) */
+    ATURAN_K_RB,             /* red-black sweeps, source, boundary passes, residual checks */
+    ATURAN_K_HYDRO,          /* buoyancy reference level + hydrostatic column integral */
+    ATURAN_K_COPY,           /* n-copy sync and layout conversions */
+    ATURAN_K_NKINDS
+};
+
+/* Reset the per-class counters; enable = 1 also brackets every class's launches with CUDA events
+ * on the context's stream (a few microseconds per bracket), enable = 0 counts launches only. */
+int aturan_profile(aturan_ctx* ctx, int enable);
+/* Read the counters since the last aturan_profile: launches[n] kernels of class n and, when timing
+ * was enabled, ms[n] their summed device time. Synchronizes the stream. Either pointer may be NULL. */
+int aturan_profile_read(aturan_ctx* ctx, double* ms, long* launches, int nkinds);
 
 /* Wait for all work queued on the context's stream. */
 int aturan_sync(aturan_ctx* ctx);

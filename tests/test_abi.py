@@ -1,0 +1,66 @@
+"""The C-ABI library loads, exports every entry point include/aturan_b200.h declares, agrees with
+the Python mirror of its parameter struct, and fails loudly (no CPU fallback) without a GPU."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from aturan_b200 import api, params as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "aturan_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void\*|const char\*)\s+(aturan_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.load_library()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in api.SIGNATURES, n
+
+
+def test_struct_layout_matches_header(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu %zu %zu\\n", sizeof(aturan_params), offsetof(aturan_params, r0),'
+                   ' offsetof(aturan_params, gas), sizeof(aturan_gas)); return 0; }\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_r0, off_gas, gsize = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.Params)
+    assert off_r0 == P.Params.r0.offset
+    assert off_gas == P.Params.gas.offset
+    assert gsize == ctypes.sizeof(P.Gas)
+
+
+def test_library_defaults_equal_python_defaults():
+    a, b = api.library_default_params(), P.default_params()
+    assert bytes(a) == bytes(b)
+
+
+def test_no_cpu_fallback_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.AturanError) as e:
+        api.Context(P.default_params(im=9, jm=13, km=17))
+    assert e.value.code == api.E_CUDA
+
+
+def test_invalid_parameters_rejected():
+    L = api.load_library()
+    p = P.default_params()
+    p.abi_version = 99
+    h = ctypes.c_void_p()
+    assert L.aturan_ctx_create(ctypes.byref(p), ctypes.byref(h)) == api.E_INVALID
+    p = P.default_params(km=18)              # km-1 odd: colours would not alternate across the seam
+    assert L.aturan_ctx_create(ctypes.byref(p), ctypes.byref(h)) == api.E_UNSUPPORTED
+    assert L.aturan_ctx_create(None, ctypes.byref(h)) == api.E_INVALID
