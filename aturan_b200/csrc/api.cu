@@ -19,6 +19,7 @@
 #include "rk4.cuh"
 #include "satadj.cuh"
 #include "pressure.cuh"
+#include "sor.cuh"
 
 using namespace aturan;
 
@@ -52,6 +53,12 @@ struct aturan_ctx {
     GSW* gsw;
     RBW* rbw;
     unsigned long long* counters;
+    // RB_SOR: Fourier tables, the 2-D correction's work arrays, FP32 correction fields
+    SorConst sorc;
+    double *sor_ct, *sor_st, *sor_lam, *sor_sj, *sor_colR, *sor_Ac, *sor_As, *sor_work, *sor_part;
+    float *r32, *e32;
+    int sor_nblk;
+    std::vector<double> host_part;
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -252,9 +259,10 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     const size_t fs = g.fstride;
     S* state = reinterpret_cast<S*>(ctx->state);
     {
-    Region reg(ctx, ATURAN_K_HYDRO, ctx->p.exact_reductions ? 2 : 3);
+    const int exact = ctx->mixed ? 0 : ctx->p.exact_reductions;   // the mixed form always sums in tree order
+    Region reg(ctx, ATURAN_K_HYDRO, exact ? 2 : 3);
     launch_buoy(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), ctx->wsin, ctx->hc,
-                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, ctx->p.exact_reductions, ctx->st);
+                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, ctx->st);
     CK_LAUNCH("buoyancy reference level");
     launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
                  grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
@@ -368,6 +376,110 @@ int run_rb(aturan_ctx* ctx, int sweeps, double omega){
     return ATURAN_OK;
 }
 
+// ---- RB_SOR: the shared solver's equation to a relative L2 residual (sor.cuh) ----
+template <typename T>
+void bc_passes(aturan_ctx* ctx, T* P){
+    const Grid g = ctx->g;
+    bc_r_kernel<T><<<dim3((g.km + 127) / 128, g.jm), 128, 0, ctx->st>>>(g, P);
+    bc_t_kernel<T><<<dim3((g.km + 127) / 128, g.im), 128, 0, ctx->st>>>(g, P);
+    bc_p_kernel<T><<<(g.im * g.jm + 255) / 256, 256, 0, ctx->st>>>(g, P);
+}
+
+// Residual of P against src: relative L2 norm (host sum of the block partials, fixed order).
+template <typename T>
+int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr){
+    const Grid g = ctx->g;
+    sor_colsum_kernel<T><<<ctx->sor_nblk, 256, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
+    CK_LAUNCH("residual");
+    CK(cudaMemcpyAsync(ctx->host_part.data(), ctx->sor_part, 2 * ctx->sor_nblk * 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    double rr = 0.0, ss = 0.0;
+    for(int n = 0; n < ctx->sor_nblk; n++){ rr += ctx->host_part[2 * n]; ss += ctx->host_part[2 * n + 1]; }
+    if(abs_rr) *abs_rr = std::sqrt(rr);
+    *rel = ss > 0.0 ? std::sqrt(rr / ss) : std::sqrt(rr);
+    return ATURAN_OK;
+}
+
+// The column-uniform correction from the column sums left in sor_colR by the last residual.
+template <typename T>
+int sor_correct(aturan_ctx* ctx, T* P){
+    const Grid g = ctx->g;
+    const SorConst& c = ctx->sorc;
+    sor_dft_kernel<<<((c.NM + 1) * c.J + 127) / 128, 128, 0, ctx->st>>>(c, ctx->sor_colR, ctx->sor_ct, ctx->sor_st, ctx->sor_Ac, ctx->sor_As);
+    sor_tridiag_kernel<<<(2 * (c.NM + 1) + 63) / 64, 64, 0, ctx->st>>>(c, ctx->sor_lam, ctx->sor_sj, ctx->sor_Ac, ctx->sor_As, ctx->sor_work);
+    sor_idft_add_kernel<T><<<(c.J * c.N + 127) / 128, 128, 0, ctx->st>>>(g, c, ctx->sor_Ac, ctx->sor_As, ctx->sor_ct, ctx->sor_st, P);
+    CK_LAUNCH("barotropic correction");
+    return ATURAN_OK;
+}
+
+template <typename S>
+int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, int* sweeps_done, double* resid){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* proj = reinterpret_cast<S*>(ctx->proj);
+    if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
+    if(max_sweeps < 1) max_sweeps = 1;
+    const int every = 4;                                       // correction and residual check cadence
+    long nl = 0;
+    Region reg(ctx, ATURAN_K_RB, 0);
+    launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
+                   grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->p.rigid_lid,
+                   ctx->rbw, ctx->pc, ctx->scratch, ctx->st);
+    sor_ysum_kernel<<<ctx->sor_nblk, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part);
+    sor_shift_kernel<<<148, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part, ctx->sor_nblk);
+    launch_pdyn_bcs(g, ctx->pdyn, ctx->st);                    // start from a boundary-consistent p
+    CK_LAUNCH("SOR source");
+    nl += 8;
+    double* P = ctx->pdyn;
+    const double* src = ctx->scratch;
+    double r = 0.0;
+    int s = 0;
+    if(!ctx->mixed){
+        int rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
+        while(s < max_sweeps && !(r <= tol)){
+            rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 3;
+            for(int n = 0; n < every && s < max_sweeps; n++, s++){
+                sor_colour_kernel<double><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, 0, omega);
+                sor_colour_kernel<double><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, 1, omega);
+                nl += 2;
+            }
+            CK_LAUNCH("SOR sweeps");
+            rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
+        }
+    } else {
+        // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
+        // Lc e = r by FP32 red-black SOR (with the column-uniform correction), p += e in FP64.
+        const int inner = 24;
+        int rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
+        while(s < max_sweeps && !(r <= tol)){
+            sor_resid32_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->r32, ctx->e32);
+            nl++;
+            double re;
+            for(int n = 0; n < inner && s < max_sweeps; n++, s++){
+                if(n % every == 0){
+                    rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, &re, nullptr); if(rc) return rc;
+                    rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
+                    nl += 4;
+                }
+                sor_colour_kernel<float><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, ctx->e32, ctx->r32, ctx->rbw, 0, omega);
+                sor_colour_kernel<float><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, ctx->e32, ctx->r32, ctx->rbw, 1, omega);
+                nl += 2;
+            }
+            sor_axpy_kernel<<<148 * 8, 256, 0, ctx->st>>>(fs, P, ctx->e32);
+            CK_LAUNCH("SOR refinement");
+            nl++;
+            rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
+        }
+    }
+    launch_pdyn_bcs(g, P, ctx->st);                            // the boundary rows of the solution
+    CK_LAUNCH("SOR boundary rows");
+    nl += 3;
+    reg.n = nl;
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    return r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
+}
+
 }  // namespace
 
 extern "C" {
@@ -382,7 +494,7 @@ int aturan_params_default(aturan_params* p){
     p->press_consistent = 1; p->press_incr = 1; p->rigid_lid = 1;
     p->satadj_conserve = 1; p->satadj_newton = 1; p->satadj_evap = 1; p->satadj_ice_entry = 0;
     p->satadj_bergeron = 2; p->satadj_freeze = 1; p->satadj_dry_exit = 1; p->local_rho = 1;
-    p->nh4sh_sync = 1; p->exact_reductions = 0;
+    p->nh4sh_sync = 1; p->exact_reductions = 1;
     const double pi180 = 180.0 / M_PI;                        // cUranusModel.cpp:340-351
     p->r0 = 1.0; p->dr = 0.025; p->the0 = 0.0; p->dthe = 1.0 / pi180; p->phi0 = 0.0; p->dphi = 1.0 / pi180;
     p->dt = 0.001; p->metric_R_km = 25362.0; p->sinthe_min = 0.4;
@@ -444,6 +556,12 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     add(g.im * 8); add(2 * (size_t)g.im * ctx->nblk * 8);
     add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
+    const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
+    ctx->sor_nblk = (sJ * sN + 255) / 256;
+    add((size_t)(sNM + 1) * sN * 8); add((size_t)(sNM + 1) * sN * 8); add((sNM + 1) * 8); add(sJ * 8);
+    add((size_t)sJ * sN * 8); add((size_t)(sNM + 1) * sJ * 8); add((size_t)(sNM + 1) * sJ * 8);
+    add((size_t)2 * (sNM + 1) * 2 * sJ * 8); add((size_t)2 * ctx->sor_nblk * 8);
+    add(fs * 4); add(fs * 4);
     ctx->mem_bytes = bytes;
     if(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess){
         delete ctx; return ATURAN_E_CUDA;
@@ -473,6 +591,14 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->cp_tab = carve<char>(cur, CP_TABLE_N * e);
     ctx->gsw = carve<GSW>(cur, nij); ctx->rbw = carve<RBW>(cur, nij);
     ctx->counters = carve<unsigned long long>(cur, 8);
+    ctx->sor_ct = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_st = carve<double>(cur, (size_t)(sNM + 1) * sN);
+    ctx->sor_lam = carve<double>(cur, sNM + 1); ctx->sor_sj = carve<double>(cur, sJ);
+    ctx->sor_colR = carve<double>(cur, (size_t)sJ * sN);
+    ctx->sor_Ac = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->sor_As = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->sor_work = carve<double>(cur, (size_t)2 * (sNM + 1) * 2 * sJ);
+    ctx->sor_part = carve<double>(cur, (size_t)2 * ctx->sor_nblk);
+    ctx->r32 = carve<float>(cur, fs); ctx->e32 = carve<float>(cur, fs);
+    ctx->host_part.resize(2 * ctx->sor_nblk);
 
     // zero everything once: padding columns and unused planes read as 0, never as garbage
     if(cudaMemsetAsync(ctx->mem, 0, bytes, ctx->st) != cudaSuccess){ aturan_ctx_destroy(ctx); return ATURAN_E_CUDA; }
@@ -591,6 +717,26 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     pc.src_scale = p->press_consistent ? (p->r_mix * p->u_0 * p->u_0) / 1.0e5 : 1.0;
     pc.press_incr = p->press_incr;
 
+    // RB_SOR tables: Fourier bases with the exact (m k mod N) reduction (PressureSolver.h:614-617),
+    // eigenvalues of the phi ring, the shared solver's floored sine of the interior rows, and
+    // A2y = sum_i y_i / rm_i^2 with the folded operator's left null vector y.
+    std::vector<double> sct((size_t)(sNM + 1) * sN), sst((size_t)(sNM + 1) * sN), slam(sNM + 1), ssj(sJ);
+    for(int m = 0; m <= sNM; m++){
+        for(int k = 0; k < sN; k++){
+            const double a = 2.0 * M_PI * (double)((long)m * k % sN) / sN;
+            sct[(size_t)m * sN + k] = std::cos(a); sst[(size_t)m * sN + k] = std::sin(a);
+        }
+        const double sl = std::sin(M_PI * m / sN);
+        slam[m] = 4.0 * sl * sl * inv_dphi2;
+    }
+    for(int q = 0; q < sJ; q++) ssj[q] = st_shared[q + 1];
+    double A2y = 0.0;
+    for(int i = 1; i < g.im - 1; i++){
+        const double rm = metric_radius(*p, rad[i]);
+        A2y += ((i == 1 || i == g.im - 2) ? 1.5 : 1.0) / (rm * rm);
+    }
+    ctx->sorc.J = sJ; ctx->sorc.N = sN; ctx->sorc.NM = sNM; ctx->sorc.inv_dthe2 = inv_dthe2; ctx->sorc.A2y = A2y;
+
     auto up = [&](void* dst, const void* src, size_t n) -> int {
         return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, ctx->st) == cudaSuccess ? 0 : 1;
     };
@@ -601,6 +747,10 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     bad |= up(ctx->cp_tab64, cp64.data(), CP_TABLE_N * 8);
     bad |= up(ctx->gsw, gsw.data(), nij * sizeof(GSW));
     bad |= up(ctx->rbw, rbw.data(), nij * sizeof(RBW));
+    bad |= up(ctx->sor_ct, sct.data(), sct.size() * 8);
+    bad |= up(ctx->sor_st, sst.data(), sst.size() * 8);
+    bad |= up(ctx->sor_lam, slam.data(), slam.size() * 8);
+    bad |= up(ctx->sor_sj, ssj.data(), ssj.size() * 8);
     std::vector<GeoIJ<float>> geo32;
     std::vector<float> cp32;
     if(ctx->mixed){
@@ -723,8 +873,8 @@ int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, dou
         if(!rc && sweeps_done) *sweeps_done = max_sweeps < 1 ? 1 : max_sweeps;
         return rc;
     case ATURAN_PRESS_RB_SOR:
-        (void)omega; (void)tol;
-        return fail(ctx, ATURAN_E_UNSUPPORTED, "RB_SOR is not built yet");
+        return ctx->mixed ? run_sor<float>(ctx, omega, max_sweeps, tol, sweeps_done, resid)
+                          : run_sor<double>(ctx, omega, max_sweeps, tol, sweeps_done, resid);
     }
     return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
 }

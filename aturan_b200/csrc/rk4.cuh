@@ -113,8 +113,15 @@ __device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, si
     }
 }
 
-template <typename S, typename C>
-__global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
+// Fused RHS evaluation and stage update of one cell. PART selects the equations: 0 all of them,
+// 1 momentum and temperature (u, v, w, t and the projection fields), 2 the fifteen scalar fields
+// (twelve condensables, NH4SH, k*, dis*). The two parts read disjoint stencil fields and write
+// disjoint accumulator / stage-output fields, so they may run as two launches of one stage; the
+// split halves the live registers per thread, which doubles the warps an SM keeps in flight
+// (the kernel is latency-bound on its stencil loads). SU unrolls the scalar loop so that SU
+// stencils' loads are in flight together; MINB is the launch bound on resident blocks per SM.
+template <typename S, typename C, int PART, int SU, int MINB>
+__global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, C> a){
     const Grid& g = a.g;
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int j = 1 + blockIdx.y * 4 + threadIdx.y;
@@ -142,6 +149,11 @@ __global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
     const C costhe_inv_rm2sinthe = geo.costhe_inv_rm2sinthe, costhe = geo.costhe;
     const C cotanthe = geo.cotanthe, two_inv_rm = geo.two_inv_rm;
 
+    const C nue_c = FORC(ATURAN_NUE);
+    const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
+    const C nue_t_s = nue_t / C(0.9);
+
+    if constexpr(PART != 2){
     // pressure gradients (:117, :146, :175), FP64 differences
     const double* P = a.pdyn;
     const C dpdr   = (C)((ld(P + oip) - ld(P + oim)) * (double)K.inv_2dr);
@@ -150,13 +162,8 @@ __global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
 
     const D6<C> U = STENCIL(ATURAN_U), V = STENCIL(ATURAN_V), W = STENCIL(ATURAN_W);
     const C u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
-
-    const C nue_c = FORC(ATURAN_NUE);
-    const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
-    const C nue_t_s = nue_t / C(0.9);
     const C v_invrm = v_ijk * inv_rm;
     const C w_invrs = w_ijk * inv_rmsinthe;
-
     // ---- momentum (:208-331, :382-391, :717-788) ----
     {
         const C sinthe_bf = geo.sinthe_bf;
@@ -233,8 +240,16 @@ __global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
         stage_update(a, ATURAN_T, o, rhs_t, 1);
     }
 
-    // ---- the twelve condensables (:790-850), one at a time ----
-#pragma unroll 1
+    }
+
+    if constexpr(PART != 1){
+    const C u_ijk = (C)ld(a.X + (size_t)ATURAN_U * fs + o);
+    const C v_ijk = (C)ld(a.X + (size_t)ATURAN_V * fs + o);
+    const C w_ijk = (C)ld(a.X + (size_t)ATURAN_W * fs + o);
+    const C v_invrm = v_ijk * inv_rm;
+    const C w_invrs = w_ijk * inv_rmsinthe;
+    // ---- the twelve condensables (:790-850) ----
+#pragma unroll SU
     for(int s = 0; s < 12; s++){
         const int q = ATURAN_CH4 + s;
         const D6<C> Q = STENCIL(q);
@@ -247,7 +262,6 @@ __global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
         r = r + K.precip_coupling * FORC(ATURAN_S_PRECIP_CH4 + s);
         stage_update(a, q, o, r, 0);
     }
-
     // ---- NH4SH: flux limiter, chemistry and Stokes settling (:852-913) ----
     {
         const D6<C> Q = STENCIL(ATURAN_NH4SH);
@@ -276,6 +290,7 @@ __global__ void __launch_bounds__(128) rk_stage_kernel(const StageArgs<S, C> a){
                         + FORC(n == 0 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE);
             stage_update(a, q, o, r, n == 0 ? 2 : 3);
         }
+    }
     }
 #undef STENCIL
 #undef FORC
@@ -321,26 +336,52 @@ static __global__ void buoy_finish_kernel(int im, int nblk, const double* part_s
     ref[lev] = (w > 0.0) ? s / w : 0.0;
 }
 
-// Exact form: the reference's serial j-then-k order, one thread per level. Bit-equal to the
-// reference; kept for parity runs (exact_reductions = 1).
+// Exact form: the reference's serial j-then-k order, bit-equal to the reference. A floating-point
+// running sum cannot be reassociated, so its dependent add chain (two adds per valid cell) is the
+// floor; everything else is taken off it. One block per level: warps 1..7 load t and p_stat
+// (coalesced along k), form w b and the validity of a chunk of 224 consecutive cells into shared
+// memory while lane 0 of warp 0 adds the previous chunk in order (double buffer, one barrier per
+// chunk).
 template <typename S>
-__global__ void buoy_serial_kernel(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* ref){
-    const int lev = blockIdx.x * blockDim.x + threadIdx.x;
-    if(lev >= g.im) return;
+__global__ void __launch_bounds__(256) buoy_serial_kernel(Grid g, const S* t, const S* ps, const double* wsin,
+                                                          HydroConst h, double* ref){
+    constexpr int CH = 224;                              // producers: threads 32..255
+    __shared__ double sb[2][CH], sw[2][CH];
+    const int lev = blockIdx.x;
+    const int ncell = g.jm * g.km;
+    const int nchunk = (ncell + CH - 1) / CH;
     double s = 0.0, w = 0.0;
-    for(int j = 0; j < g.jm; j++){
-        const double wg = wsin[j];
-        for(int k = 0; k < g.km; k++){
+    auto produce = [&](int chunk, int buf){
+        const int q = threadIdx.x - 32;
+        const int c = chunk * CH + q;
+        double bv = 0.0, wv = 0.0;                       // wv = 0 marks a skipped cell
+        if(c < ncell){
+            const int j = c / g.km, k = c - j * g.km;
             const size_t o = gidx(g, lev, j, k);
             const double T = (double)__ldg(t + o);
-            if(!(T > 0.0)) continue;
-            const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
-            if(!isfinite(b)) continue;
-            s += wg * b;
-            w += wg;
+            if(T > 0.0){
+                const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
+                if(isfinite(b)){ const double wg = wsin[j]; bv = wg * b; wv = wg; }
+            }
         }
+        sb[buf][q] = bv; sw[buf][q] = wv;
+    };
+    if(threadIdx.x >= 32) produce(0, 0);
+    __syncthreads();
+    for(int chunk = 0; chunk < nchunk; chunk++){
+        const int buf = chunk & 1;
+        if(threadIdx.x >= 32){
+            if(chunk + 1 < nchunk) produce(chunk + 1, buf ^ 1);
+        } else if(threadIdx.x == 0){
+            const int n = min(CH, ncell - chunk * CH);
+            for(int q = 0; q < n; q++){
+                const double wv = sw[buf][q];
+                if(wv != 0.0 || sb[buf][q] != 0.0){ s += sb[buf][q]; w += wv; }
+            }
+        }
+        __syncthreads();
     }
-    ref[lev] = (w > 0.0) ? s / w : 0.0;
+    if(threadIdx.x == 0) ref[lev] = (w > 0.0) ? s / w : 0.0;
 }
 
 // ---- RungeKutta_Uran_Turb.cpp:62-177: per column (j, k) -- every column, the seam copy and the

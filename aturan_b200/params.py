@@ -80,7 +80,7 @@ DEFAULTS = dict(
     press_consistent=1, press_incr=1, rigid_lid=1,
     satadj_conserve=1, satadj_newton=1, satadj_evap=1, satadj_ice_entry=0,
     satadj_bergeron=2, satadj_freeze=1, satadj_dry_exit=1, local_rho=1, nh4sh_sync=1,
-    exact_reductions=0,
+    exact_reductions=1,
     r0=1.0, dr=0.025, the0=0.0, dthe=1.0 / (180.0 / math.pi), phi0=0.0,
     dphi=1.0 / (180.0 / math.pi), dt=0.001, metric_R_km=25362.0, sinthe_min=0.4,
     L_atm=225.0, u_0=100.0, t_ref=76.4, g=8.69, omega=0.000101, re=1000.0, pr=0.69,

@@ -106,9 +106,11 @@ typedef struct aturan_params {
     int32_t satadj_conserve, satadj_newton, satadj_evap, satadj_ice_entry;
     int32_t satadj_bergeron, satadj_freeze, satadj_dry_exit, local_rho;
     int32_t nh4sh_sync;          /* RK_SCALAR_SYNC also copies nh4sh (ATURAN_NH4SH_EQ) */
-    int32_t exact_reductions;    /* 1: the level means of the buoyancy reference are summed in
-                                    the reference's serial order (bit-exact, slow); 0: a fixed
-                                    tree order (deterministic run to run, ~1 ulp from serial) */
+    int32_t exact_reductions;    /* FP64 only. 1 (default): the level means of the buoyancy
+                                    reference are summed in the reference's serial order, so the
+                                    RK4 step is bit-equal to the CPU's; 0: a fixed tree order
+                                    (deterministic run to run, within ~1e-12 of the serial sums).
+                                    The mixed form always uses the tree order. */
     int32_t reserved_i[7];
 
     double r0, dr, the0, dthe, phi0, dphi, dt;

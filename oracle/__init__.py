@@ -56,6 +56,7 @@ class Oracle:
             ("oracle_pressure_sor", [P, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                      ctypes.c_int, vp, vp], ctypes.c_int),
             ("oracle_pressure_source", [P, vp, vp], ctypes.c_int),
+            ("oracle_pressure_source_compat", [P, vp, vp], ctypes.c_int),
             ("oracle_pressure_residual", [P, vp, vp], ctypes.c_double),
             ("oracle_satadj", [P, vp, ctypes.c_int, vp, vp], ctypes.c_int),
             ("oracle_sync_ncopies", [P, vp], ctypes.c_int),
@@ -108,6 +109,11 @@ class Oracle:
     def pressure_source(self, p, state):
         src = np.zeros(p.shape)
         assert self.L.oracle_pressure_source(self._p(p), field_ptrs(state), src.ctypes.data) == 0
+        return src
+
+    def pressure_source_compat(self, p, state):
+        src = np.zeros(p.shape)
+        assert self.L.oracle_pressure_source_compat(self._p(p), field_ptrs(state), src.ctypes.data) == 0
         return src
 
     def pressure_residual(self, p, state, src):

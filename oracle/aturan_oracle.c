@@ -17,6 +17,9 @@
 #include <omp.h>
 #endif
 
+#ifndef M_PI
+#define M_PI 3.14159265358979323846   /* the value glibc math.h gives M_PI */
+#endif
 #define IDX(i, j, k) (((size_t)(i) * jm + (j)) * km + (k))
 #define NPROG ATURAN_NPROG
 
@@ -843,11 +846,184 @@ double oracle_pressure_residual(const aturan_params* p, double* const* f, const 
     return ss > 0.0 ? sqrt(rr / ss) : sqrt(rr);
 }
 
-/* Red-black SOR on the shared solver's equation to a relative residual (no reference oracle:
- * this is the restatement the GPU to-residual solver is checked against). The source is made
- * compatible with the all-Neumann operator by removing its component along the left null vector
+/* Remove the source's component along the all-Neumann operator's left null vector
  * y = a(i) b(j), a = b = (3/2, 1, ..., 1, 3/2) (PressureSolver.h:63-65 states it for theta; the
- * radial fold has the same form), using a constant shift. */
+ * radial fold has the same form), by a constant shift over the interior. */
+static void compat_shift(const aturan_params* p, double* src){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double ys = 0.0, yy = 0.0;
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++){
+        const double yi = (i == 1 || i == im-2) ? 1.5 : 1.0, yj = (j == 1 || j == jm-2) ? 1.5 : 1.0;
+        for(int k = 0; k < km-1; k++){ ys += yi * yj * src[IDX(i,j,k)]; yy += yi * yj; }
+    }
+    const double shift = ys / yy;
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++)
+        src[IDX(i,j,k)] -= shift;
+}
+
+int oracle_pressure_source_compat(const aturan_params* p, double* const* f, double* src){
+    oracle_pressure_source(p, f, src);
+    compat_shift(p, src);
+    return 0;
+}
+
+/* The shared solver's operator with the 2-point Neumann folds substituted into the rows instead
+ * of lagged boundary rows: at i = 1, p[0] = c43 p[1] - c13 p[2] puts c43 num1 on the diagonal
+ * and -c13 num1 on p[2]; likewise at i = im-2, j = 1, j = jm-2. Same linear operator on the
+ * interior unknowns (hence the same solution), but every row couples only to the other colour,
+ * so red-black SOR keeps its consistently-ordered convergence rate. Returns the off-diagonal
+ * sum and the diagonal. */
+static double folded_acc(const aturan_params* p, const double* P, int i, int j, int k,
+                         const pweights_t* w, double* diag){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+    double d = w->den;
+    const double aim = (i == 1)    ? (d -= C43 * w->num1, -C13 * P[IDX(i+1,j,k)]) : P[IDX(i-1,j,k)];
+    const double aip = (i == im-2) ? (d -= C43 * w->num1, -C13 * P[IDX(i-1,j,k)]) : P[IDX(i+1,j,k)];
+    const double ajm = (j == 1)    ? (d -= C43 * w->num2, -C13 * P[IDX(i,j+1,k)]) : P[IDX(i,j-1,k)];
+    const double ajp = (j == jm-2) ? (d -= C43 * w->num2, -C13 * P[IDX(i,j-1,k)]) : P[IDX(i,j+1,k)];
+    *diag = d;
+    return (aip + aim) * w->num1 + (ajp + ajm) * w->num2 + (P[IDX(i,j,ke)] + P[IDX(i,j,kw)]) * w->num3;
+}
+
+static void rbf_colour(const aturan_params* p, const double* rad, const double* st, double* P,
+                       const double* src, int colour, double omega){
+    const int im = p->im, jm = p->jm, km = p->km;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            pweights_t w; press_weights(p, rad, st, i, j, &w);
+            for(int k = 0; k < km-1; k++){
+                if(((i + j + k) & 1) != colour) continue;
+                double diag;
+                const double acc = folded_acc(p, P, i, j, k, &w, &diag);
+                const double pn = (acc - src[IDX(i,j,k)]) / diag;
+                P[IDX(i,j,k)] += omega * (pn - P[IDX(i,j,k)]);
+            }
+        }
+    }
+}
+
+/* Relative L2 residual of the folded operator (equal to the boundary-row form once the
+ * boundary rows are consistent). */
+static double folded_residual(const aturan_params* p, const double* rad, const double* st,
+                              const double* P, const double* src){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double rr = 0.0, ss = 0.0;
+    #pragma omp parallel for collapse(2) reduction(+:rr,ss) schedule(static)
+    for(int i = 1; i < im-1; i++){
+        for(int j = 1; j < jm-1; j++){
+            pweights_t w; press_weights(p, rad, st, i, j, &w);
+            for(int k = 0; k < km-1; k++){
+                double diag;
+                const double acc = folded_acc(p, P, i, j, k, &w, &diag);
+                const double r = src[IDX(i,j,k)] - (acc - diag * P[IDX(i,j,k)]);
+                rr += r * r; ss += src[IDX(i,j,k)] * src[IDX(i,j,k)];
+            }
+        }
+    }
+    return ss > 0.0 ? sqrt(rr / ss) : sqrt(rr);
+}
+
+/* The column-uniform correction: q(j,k) added to every level with
+ *   (sum_i y_i / rm_i^2) L2(q) = sum_i y_i (src - Lc p)_i,
+ * L2 the horizontal stencil, solved by a DFT over the km-1 meridians and one tridiagonal solve
+ * in theta per Fourier mode with the ends folded (the reference's PRESS_BAROTROPIC,
+ * PressureSolver.h:572-708, with the folded operator's left null vector as column weights). */
+static void column_correction(const aturan_params* p, const double* rad, const double* st,
+                              double* P, const double* src){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int J = jm - 2, N = km - 1, NM = N / 2;
+    double* R  = (double*)calloc((size_t)J * N, sizeof(double));
+    double* Ac = (double*)calloc((size_t)(NM + 1) * J, sizeof(double));
+    double* As = (double*)calloc((size_t)(NM + 1) * J, sizeof(double));
+    double A2y = 0.0;
+    for(int i = 1; i < im-1; i++){ const double rm = metric_radius(p, rad[i]); A2y += ((i == 1 || i == im-2) ? 1.5 : 1.0) / (rm * rm); }
+    #pragma omp parallel for schedule(static)
+    for(int jj = 0; jj < J; jj++){
+        const int j = jj + 1;
+        for(int k = 0; k < N; k++){
+            const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+            double acc_r = 0.0;
+            (void)kw; (void)ke;
+            for(int i = 1; i < im-1; i++){
+                pweights_t w; press_weights(p, rad, st, i, j, &w);
+                double diag;
+                const double accf = folded_acc(p, P, i, j, k, &w, &diag);
+                const double lc = accf - diag * P[IDX(i,j,k)];
+                acc_r += ((i == 1 || i == im-2) ? 1.5 : 1.0) * (src[IDX(i,j,k)] - lc);
+            }
+            R[(size_t)jj * N + k] = acc_r;
+        }
+    }
+    const double e = 1.0 / (p->dthe * p->dthe), inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+    #pragma omp parallel for schedule(static)
+    for(int m = 0; m <= NM; m++){
+        double* cp = (double*)malloc(sizeof(double) * J);
+        double* dp = (double*)malloc(sizeof(double) * J);
+        for(int jj = 0; jj < J; jj++){
+            double sc = 0.0, ss = 0.0;
+            for(int k = 0; k < N; k++){
+                const double a = 2.0 * M_PI * (double)((long)m * k % N) / N;
+                const double v = R[(size_t)jj * N + k] / A2y;
+                sc += v * cos(a); ss += v * sin(a);
+            }
+            Ac[(size_t)m * J + jj] = sc; As[(size_t)m * J + jj] = ss;
+        }
+        const double sl = sin(M_PI * m / N);
+        const double lam = 4.0 * sl * sl * inv_dphi2;
+        for(int part = 0; part < 2; part++){
+            double* d = (part == 0 ? Ac : As) + (size_t)m * J;
+            if(part == 1 && (m == 0 || 2 * m == N)){ for(int q = 0; q < J; q++) d[q] = 0.0; continue; }
+            if(m == 0){
+                double yr = 0.0, ys = 0.0;
+                for(int q = 0; q < J; q++){ const double y = (q == 0 || q == J-1) ? 1.5 : 1.0; yr += y * d[q]; ys += y; }
+                for(int q = 0; q < J; q++) d[q] -= yr / ys;
+            }
+            #define TA(q) ((q) == 0 ? 0.0 : ((q) == J-1 ? e - C13 * e : e))
+            #define TB(q) (-2.0 * e - lam / (st[(q)+1] * st[(q)+1]) + (((q) == 0 || (q) == J-1) ? C43 * e : 0.0))
+            #define TC(q) ((q) == J-1 ? 0.0 : ((q) == 0 ? e - C13 * e : e))
+            double b0 = TB(0), c0 = TC(0), d0 = d[0];
+            if(m == 0){ b0 = 1.0; c0 = 0.0; d0 = 0.0; }
+            cp[0] = c0 / b0; dp[0] = d0 / b0;
+            for(int q = 1; q < J; q++){
+                const double dn = TB(q) - TA(q) * cp[q-1];
+                cp[q] = TC(q) / dn;
+                dp[q] = (d[q] - TA(q) * dp[q-1]) / dn;
+            }
+            #undef TA
+            #undef TB
+            #undef TC
+            d[J-1] = dp[J-1];
+            for(int q = J-2; q >= 0; q--) d[q] = dp[q] - cp[q] * d[q+1];
+            if(m == 0){
+                double yq = 0.0, ys = 0.0;
+                for(int q = 0; q < J; q++){ const double y = (q == 0 || q == J-1) ? 1.5 : 1.0; yq += y * d[q]; ys += y; }
+                for(int q = 0; q < J; q++) d[q] -= yq / ys;
+            }
+        }
+        free(cp); free(dp);
+    }
+    #pragma omp parallel for schedule(static)
+    for(int jj = 0; jj < J; jj++){
+        for(int k = 0; k < N; k++){
+            double q = 0.0;
+            for(int m = 0; m <= NM; m++){
+                const int edge = (m == 0 || 2 * m == N);
+                const double a = 2.0 * M_PI * (double)((long)m * k % N) / N;
+                q += (edge ? 1.0 : 2.0) * (Ac[(size_t)m * J + jj] * cos(a) + (edge ? 0.0 : As[(size_t)m * J + jj] * sin(a)));
+            }
+            q /= N;
+            for(int i = 1; i < im-1; i++) P[IDX(i, jj + 1, k)] += q;
+        }
+    }
+    free(R); free(Ac); free(As);
+}
+
+/* Red-black SOR on the shared solver's equation to a relative residual, with the column-uniform
+ * correction before every block of check_every sweeps (no reference oracle exists for a
+ * converged solve: the reference sweeps a fixed count at omega = 1). The GPU's RB_SOR runs the
+ * same sequence. Returns 0 when the relative L2 residual reached tol, 1 at the sweep cap. */
 int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, int max_sweeps,
                         double tol, int check_every, int* sweeps_done, double* resid){
     const int im = p->im, jm = p->jm, km = p->km;
@@ -857,24 +1033,19 @@ int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, 
     double* src = (double*)malloc(sizeof(double) * (size_t)im * jm * km);
     oracle_coords(p, rad, the);
     press_sin_table(p, the, st, 1);
-    oracle_pressure_source(p, f, src);
-    double ys = 0.0, yy = 0.0;
-    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++){
-        const double yi = (i == 1 || i == im-2) ? 1.5 : 1.0, yj = (j == 1 || j == jm-2) ? 1.5 : 1.0;
-        for(int k = 0; k < km-1; k++){ ys += yi * yj * src[IDX(i,j,k)]; yy += yi * yj; }
-    }
-    const double shift = ys / yy;
-    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++)
-        src[IDX(i,j,k)] -= shift;
+    oracle_pressure_source_compat(p, f, src);
+    double* P = f[ATURAN_P_DYN];
     if(check_every < 1) check_every = 1;
-    int s = 0; double r = oracle_pressure_residual(p, f, src);
+    int s = 0; double r = folded_residual(p, rad, st, P, src);
     while(s < max_sweeps && !(r <= tol)){
-        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 0, omega);
-        rb_colour(p, rad, st, f[ATURAN_P_DYN], src, 1, omega);
-        p_dyn_bcs(p, f[ATURAN_P_DYN]);
-        s++;
-        if(s % check_every == 0 || s == max_sweeps) r = oracle_pressure_residual(p, f, src);
+        column_correction(p, rad, st, P, src);
+        for(int n = 0; n < check_every && s < max_sweeps; n++, s++){
+            rbf_colour(p, rad, st, P, src, 0, omega);
+            rbf_colour(p, rad, st, P, src, 1, omega);
+        }
+        r = folded_residual(p, rad, st, P, src);
     }
+    p_dyn_bcs(p, P);
     if(sweeps_done) *sweeps_done = s;
     if(resid) *resid = r;
     free(rad); free(the); free(st); free(src);

@@ -35,6 +35,7 @@ int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, 
                         double tol, int check_every, int* sweeps_done, double* resid);
 double oracle_pressure_residual(const aturan_params* p, double* const* f, const double* src);
 int oracle_pressure_source(const aturan_params* p, double* const* f, double* src);
+int oracle_pressure_source_compat(const aturan_params* p, double* const* f, double* src);
 int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adjusted, long* n_noconv);
 int oracle_sync_ncopies(const aturan_params* p, double* const* f);
 int oracle_step(const aturan_params* p, double* const* f, int press_kind, double omega,

@@ -77,9 +77,11 @@ def test_rk4_fp64(oracle_lib, synth, exact):
             ne = np.count_nonzero(g[n] != st[n])
             assert ne == 0, f"{n}: {ne} cells differ, max rel {rel_err(g[n], st[n])}"
     else:
-        assert rel_err(g["_buoy"], lev) < 1e-14
+        # a tree-ordered sum of 65k terms differs from the serial one by its rounding error
+        # (~1e-13 relative); p_hydro takes (b - ref) / ref of it and amplifies that by ~100
+        assert rel_err(g["_buoy"], lev) < 1e-12
         for n in RK_OUT:
-            assert rel_err(g[n], st[n]) < 1e-13, n
+            assert rel_err(g[n], st[n]) < (1e-9 if n in ("p_hydro", "p_bfollow") else 1e-11), n
 
 
 def test_pressure_gs_fp64(oracle_lib, synth):
@@ -220,3 +222,69 @@ def test_nonfinite_inputs_stay_local(oracle_lib):
         assert np.array_equal(np.isnan(a), np.isnan(b)), n
         m = ~np.isnan(b)
         assert rel_err(a[m], b[m]) < 1e-11, n
+
+
+# ---- RB_SOR: the shared solver's equation to a relative residual (no reference oracle) ----
+
+def sor_case(shape=(41, 91, 181), seed=31):
+    p = P.default_params(*shape)
+    st = S.synthetic_state(p, seed=seed)
+    st["p_dyn"][:] = 0.0
+    return p, st
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_sor_reaches_tolerance(oracle_lib, prec):
+    """The GPU solution satisfies the equation to the stated residual as measured by the
+    independent CPU code (its own source, compatibility shift and operator)."""
+    p, st = sor_case()
+    p.precision = P.FP64 if prec == "fp64" else P.MIXED
+    ctx = ctx_for(p)
+    ctx.upload_state(st)
+    rc, sweeps, res = ctx.pressure(P.PRESS_RB_SOR, omega=1.9, max_sweeps=2000, tol=1e-8)
+    got = ctx.download_state(["p_dyn"] + F.PROJECTION)
+    ctx.close()
+    assert rc == 0 and res <= 1e-8 and 0 < sweeps < 2000, (rc, sweeps, res)
+    chk = S.copy_state(st)
+    chk.update(got)                               # the aux the GPU used (FP32-rounded in mixed)
+    p64 = P.default_params(*p.shape)
+    src = oracle_lib.pressure_source_compat(p64, chk)
+    r_cpu = oracle_lib.pressure_residual(p64, chk, src)
+    assert r_cpu <= 2e-8, r_cpu
+    pd = got["p_dyn"]                              # boundary rows folded from the interior
+    assert np.allclose(pd[0], 4.0 / 3.0 * pd[1] - 1.0 / 3.0 * pd[2], rtol=0, atol=1e-12 * np.abs(pd).max())
+    assert np.array_equal(pd[:, :, -1], pd[:, :, 0])
+
+
+def test_sor_same_iteration_as_oracle(oracle_lib):
+    """Same algorithm on CPU and GPU in FP64: same sweep count to tolerance and solutions that
+    agree to the accuracy the residual implies."""
+    p, st = sor_case(shape=(21, 37, 73), seed=32)
+    ctx = ctx_for(p)
+    ctx.upload_state(st)
+    rc, sweeps, res = ctx.pressure(P.PRESS_RB_SOR, omega=1.8, max_sweeps=2000, tol=1e-9)
+    g = ctx.download("p_dyn")
+    ctx.close()
+    st2 = S.copy_state(st)
+    rc2, sweeps2, res2 = oracle_lib.pressure_sor(p, st2, 1.8, 2000, 1e-9, 4)
+    assert rc == 0 and rc2 == 0
+    assert abs(sweeps - sweeps2) <= 4, (sweeps, sweeps2)
+    assert rel_err(g, st2["p_dyn"]) < 1e-6
+
+
+def test_sor_reports_not_converged():
+    p, st = sor_case()
+    ctx = ctx_for(p)
+    ctx.upload_state(st)
+    rc, sweeps, res = ctx.pressure(P.PRESS_RB_SOR, omega=1.9, max_sweeps=8, tol=1e-12)
+    ctx.close()
+    assert rc == 1 and sweeps == 8 and res > 1e-12
+
+
+def test_sor_rejects_bad_omega():
+    from aturan_b200.api import AturanError
+    p, st = sor_case(shape=(9, 13, 17))
+    ctx = ctx_for(p)
+    with pytest.raises(AturanError):
+        ctx.pressure(P.PRESS_RB_SOR, omega=2.5, max_sweeps=10, tol=1e-8)
+    ctx.close()
