@@ -9,8 +9,8 @@
 void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                                             \
     const Grid& g = a.g;                                                                                  \
     dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);                                        \
-    rk_stage_kernel<S, C, 1, 1, 1><<<grid, dim3(32, 4), 0, st>>>(a);                                      \
-    rk_stage_kernel<S, C, 2, 1, 1><<<grid, dim3(32, 4), 0, st>>>(a);                                      \
+    rk_stage_kernel<S, C, 1, 1, 4><<<grid, dim3(32, 4), 0, st>>>(a);                                      \
+    rk_stage_kernel<S, C, 2, 2, 6><<<grid, dim3(32, 4), 0, st>>>(a);                                      \
 }                                                                                                         \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
                  double* part_w, int nblk, double* ref, int exact, cudaStream_t st){                       \

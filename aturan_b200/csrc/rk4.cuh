@@ -373,10 +373,17 @@ __global__ void __launch_bounds__(256) buoy_serial_kernel(Grid g, const S* t, co
         if(threadIdx.x >= 32){
             if(chunk + 1 < nchunk) produce(chunk + 1, buf ^ 1);
         } else if(threadIdx.x == 0){
+            // Skipped cells hold +0.0 in both arrays, and adding +0.0 leaves a sum of
+            // non-negative terms unchanged, so the chain can run without a branch; unrolled so
+            // the shared-memory loads run ahead of the two dependent add chains.
             const int n = min(CH, ncell - chunk * CH);
-            for(int q = 0; q < n; q++){
-                const double wv = sw[buf][q];
-                if(wv != 0.0 || sb[buf][q] != 0.0){ s += sb[buf][q]; w += wv; }
+            const double* pb = sb[buf];
+            const double* pw = sw[buf];
+            if(n == CH){
+#pragma unroll 32
+                for(int q = 0; q < CH; q++){ s += pb[q]; w += pw[q]; }
+            } else {
+                for(int q = 0; q < n; q++){ s += pb[q]; w += pw[q]; }
             }
         }
         __syncthreads();
