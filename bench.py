@@ -218,11 +218,11 @@ def main():
     else:
         torch.cuda.set_device(0)
 
-    from aturan_b200 import api, params as P, state as S
+    from aturan_b200 import api, params as P, replicas, state as S
     prec = P.MIXED if args.precision == "mixed" else P.FP64
     gi, gj, gk = (int(x) for x in args.grid.lower().split("x"))
     p = P.default_params(gi, gj, gk, precision=prec)
-    st = S.synthetic_state(p, seed=20261203 + rank)
+    st = S.synthetic_state(p, seed=replicas.replica_seed(20261203, rank))
     ctx = api.Context(p)
     ctx.upload_state(st)
     pa, press_note = press_args(args.press)
@@ -266,11 +266,8 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     launches = sum(v[0] for v in ctx.profile_read().values())
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = N_CELLS * K * world / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(ms, dist, device="cuda")
+    value = replicas.throughput(N_CELLS, K, world, ms_max / 1e3)
 
     # ---- per-kernel device times of the same steps (event-bracketed pass) ----
     ctx.profile(timing=True)
@@ -306,10 +303,7 @@ def main():
         for n in out_names:
             ctx.L.aturan_download(ctx.h, F.ID[n], outs[n].data_ptr())
     e2e_s = time.perf_counter() - t0
-    tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = N_CELLS * E * world / float(tt.item())
+    e2e_value = replicas.throughput(N_CELLS, E, world, replicas.max_over_ranks(e2e_s, dist, device="cuda"))
     fbytes = p.im * p.jm * p.km * 8
 
     # ---- accuracy of the mixed step against the FP64 step (which matches the FP64 oracle) ----
