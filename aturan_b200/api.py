@@ -48,7 +48,11 @@ SIGNATURES = {
     "aturan_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "aturan_profile": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "aturan_profile_read": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_buoy_ref_level_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p], ctypes.c_int),
 }
+
+STATIC_MAX_IM, STATIC_MAX_JM = 512, 4096
 
 KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy"]
 

@@ -23,6 +23,8 @@
 
 using namespace aturan;
 
+namespace aturan { const char* static_last_error(); }   // noalloc.cu: errors of calls without a context
+
 struct aturan_ctx {
     aturan_params p;
     Grid g;
@@ -519,7 +521,7 @@ int aturan_params_default(aturan_params* p){
 }
 
 const char* aturan_last_error(const aturan_ctx* ctx){
-    return ctx ? ctx->err.c_str() : "null context";
+    return ctx ? ctx->err.c_str() : aturan::static_last_error();
 }
 
 int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){

@@ -150,7 +150,8 @@ int aturan_params_default(aturan_params* p);
  * is allocated by cUranusModel::resetArrays, cUranusModel.cpp:1416). */
 int aturan_ctx_create(const aturan_params* p, aturan_ctx** out);
 int aturan_ctx_destroy(aturan_ctx* ctx);
-const char* aturan_last_error(const aturan_ctx* ctx);
+const char* aturan_last_error(const aturan_ctx* ctx);   /* NULL: the last error of the calls
+                                                          without a context, on this thread */
 
 /* Copy one field between host memory (contiguous FP64 [i][j][k], im*jm*km values) and the
  * device. Upload is asynchronous on the context's stream from pinned memory, synchronous from
@@ -212,6 +213,26 @@ int aturan_profile(aturan_ctx* ctx, int enable);
 /* Read the counters since the last aturan_profile: launches[n] kernels of class n and, when timing
  * was enabled, ms[n] their summed device time. Synchronizes the stream. Either pointer may be NULL. */
 int aturan_profile_read(aturan_ctx* ctx, double* ms, long* launches, int nkinds);
+
+/* The buoyancy reference level of RungeKutta_Uran_Turb.cpp:18-37 computed without allocating any
+ * device memory; no counterpart in the reference, which has no device. It is for callers that may
+ * not allocate: an application whose memory pool owns the whole GPU and hands this library only
+ * the buffers it holds, or code issuing work while a stream is being captured into a CUDA graph
+ * (where cudaMalloc is not allowed). t and p_stat are the caller's device arrays, contiguous FP64
+ * [i][j][k] with k fastest (im*jm*km values); ref_out receives im doubles on the device.
+ * The scratch (block partial sums and the sin(theta) weights) is a fixed array inside the library
+ * image, so every GPU that loads the library holds 288 KiB until the process exits; it bounds the
+ * grid to im <= ATURAN_STATIC_MAX_IM and jm <= ATURAN_STATIC_MAX_JM, larger grids are rejected with
+ * ATURAN_E_INVALID (message in aturan_last_error(NULL)). The first call on a device looks the
+ * array's address up (cudaGetSymbolAddress) with that device current; make it before any stream
+ * capture. The call is asynchronous on `stream` (a cudaStream_t, NULL for the legacy default
+ * stream). All calls on a device share the array: calls whose kernels may overlap on the GPU (on
+ * unordered streams) race and must not be issued. The result equals aturan_rk4_step's level means
+ * with exact_reductions = 0 (the same tree order). */
+#define ATURAN_STATIC_MAX_IM 512
+#define ATURAN_STATIC_MAX_JM 4096
+int aturan_buoy_ref_level_static(const aturan_params* p, const double* t, const double* p_stat,
+                                 double* ref_out, void* stream);
 
 /* Wait for all work queued on the context's stream. */
 int aturan_sync(aturan_ctx* ctx);
