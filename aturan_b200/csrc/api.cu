@@ -57,9 +57,12 @@ struct aturan_ctx {
     unsigned long long* counters;
     // RB_SOR: Fourier tables, the 2-D correction's work arrays, FP32 correction fields
     SorConst sorc;
-    double *sor_ct, *sor_st, *sor_lam, *sor_sj, *sor_colR, *sor_Ac, *sor_As, *sor_work, *sor_part;
+    double *sor_ct, *sor_st, *sor_ctT, *sor_stT, *sor_colR, *sor_Ac, *sor_As, *sor_part, *sor_q;
+    double *mlu_a, *mlu_cf, *mlu_idn;            // per-mode theta factorisations
+    double *llu_a, *llu_cf, *llu_idn;            // per-(i,j) radial-line factorisations
     float *r32, *e32;
     int sor_nblk;
+    int sor_pb;                // tridiagonal problems per block of the column correction
     std::vector<double> host_part;
     // host-side constants
     RhsConst<double> k64;
@@ -391,8 +394,9 @@ void bc_passes(aturan_ctx* ctx, T* P){
 template <typename T>
 int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr){
     const Grid g = ctx->g;
-    sor_colsum_kernel<T><<<ctx->sor_nblk, 256, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
+    sor_colsum_kernel<T><<<dim3((g.km - 1 + 31) / 32, g.jm - 2), dim3(32, 8), 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
     CK_LAUNCH("residual");
+    if(!rel) return ATURAN_OK;                                 // column sums only: no host round trip
     CK(cudaMemcpyAsync(ctx->host_part.data(), ctx->sor_part, 2 * ctx->sor_nblk * 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     double rr = 0.0, ss = 0.0;
@@ -407,31 +411,63 @@ template <typename T>
 int sor_correct(aturan_ctx* ctx, T* P){
     const Grid g = ctx->g;
     const SorConst& c = ctx->sorc;
-    sor_dft_kernel<<<((c.NM + 1) * c.J + 127) / 128, 128, 0, ctx->st>>>(c, ctx->sor_colR, ctx->sor_ct, ctx->sor_st, ctx->sor_Ac, ctx->sor_As);
-    sor_tridiag_kernel<<<(2 * (c.NM + 1) + 63) / 64, 64, 0, ctx->st>>>(c, ctx->sor_lam, ctx->sor_sj, ctx->sor_Ac, ctx->sor_As, ctx->sor_work);
-    sor_idft_add_kernel<T><<<(c.J * c.N + 127) / 128, 128, 0, ctx->st>>>(g, c, ctx->sor_Ac, ctx->sor_As, ctx->sor_ct, ctx->sor_st, P);
-    CK_LAUNCH("barotropic correction");
+    const MatRef none{nullptr, 0, 0};
+    const MatRef R{ctx->sor_colR, c.N, 1};                        // (jj, k)
+    const dim3 gf((c.NM + 1 + 31) / 32, (c.J + 31) / 32);
+    sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_ctT, c.NM + 1, 1}, none, none,
+                                            1.0 / c.A2y, ctx->sor_Ac, 1, c.J);
+    sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_stT, c.NM + 1, 1}, none, none,
+                                            1.0 / c.A2y, ctx->sor_As, 1, c.J);
+    ModeLU lu{ctx->mlu_a, ctx->mlu_cf, ctx->mlu_idn};
+    const int pb = ctx->sor_pb;
+    sor_tridiag_kernel<<<(2 * (c.NM + 1) + pb - 1) / pb, 128, (size_t)c.J * (pb + 1) * sizeof(double), ctx->st>>>(
+        c, lu, ctx->sor_Ac, ctx->sor_As, pb);
+    const dim3 gi((c.N + 31) / 32, (c.J + 31) / 32);
+    sor_gemm_kernel<<<gi, 256, 0, ctx->st>>>(c.J, c.N, c.NM + 1, MatRef{ctx->sor_Ac, 1, c.J}, MatRef{ctx->sor_ct, c.N, 1},
+                                            MatRef{ctx->sor_As, 1, c.J}, MatRef{ctx->sor_st, c.N, 1},
+                                            1.0, ctx->sor_q, c.N, 1);
+    sor_add_kernel<T><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P);
+    CK_LAUNCH("column-uniform correction");
     return ATURAN_OK;
 }
 
+// One relaxation sweep (both colours) of the folded operator: point (line = false) or radial line.
+template <typename T>
+void sor_sweep(aturan_ctx* ctx, T* E, const T* R, double omega, bool line){
+    const Grid g = ctx->g;
+    for(int colour = 0; colour < 2; colour++){
+        if(line)
+            sor_line_kernel<T><<<dim3((g.km / 2 + 31) / 32, g.jm - 2), 256, (size_t)(g.im - 2) * 32 * sizeof(double), ctx->st>>>(
+                g, E, R, ctx->rbw, ctx->llu_a, ctx->llu_cf, ctx->llu_idn, colour, omega);
+        else
+            sor_colour_kernel<T><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(
+                g, E, R, ctx->rbw, colour, omega);
+    }
+}
+
 template <typename S>
-int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, int* sweeps_done, double* resid){
+int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line, int* sweeps_done, double* resid){
     const Grid g = ctx->g;
     const size_t fs = g.fstride;
     S* proj = reinterpret_cast<S*>(ctx->proj);
     if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
+    if(ctx->sor_pb < 1) return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 3000");
+    if(line && (g.im - 2) * 32 * (int)sizeof(double) > 49152)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 194");
     if(max_sweeps < 1) max_sweeps = 1;
-    const int every = 4;                                       // correction and residual check cadence
+    // sweeps between column-uniform corrections and residual checks: point SOR needs ~200 sweeps and
+    // loses ~6 % of its rate with a correction every 16 (oracle measurement); line SOR needs ~7
+    const int every = line ? 1 : 16;
     long nl = 0;
     Region reg(ctx, ATURAN_K_RB, 0);
     launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
                    grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->p.rigid_lid,
                    ctx->rbw, ctx->pc, ctx->scratch, ctx->st);
-    sor_ysum_kernel<<<ctx->sor_nblk, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part);
-    sor_shift_kernel<<<148, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part, ctx->sor_nblk);
-    launch_pdyn_bcs(g, ctx->pdyn, ctx->st);                    // start from a boundary-consistent p
+    const int ny = ((g.jm - 2) * (g.km - 1) + 255) / 256;
+    sor_ysum_kernel<<<ny, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part);
+    sor_shift_kernel<<<148, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part, ny);
     CK_LAUNCH("SOR source");
-    nl += 8;
+    nl += 5;
     double* P = ctx->pdyn;
     const double* src = ctx->scratch;
     double r = 0.0;
@@ -439,32 +475,26 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, int* swee
     if(!ctx->mixed){
         int rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
-            rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 3;
-            for(int n = 0; n < every && s < max_sweeps; n++, s++){
-                sor_colour_kernel<double><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, 0, omega);
-                sor_colour_kernel<double><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, 1, omega);
-                nl += 2;
-            }
+            rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 4;
+            for(int n = 0; n < every && s < max_sweeps; n++, s++){ sor_sweep<double>(ctx, P, src, omega, line); nl += 2; }
             CK_LAUNCH("SOR sweeps");
             rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
         }
     } else {
         // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
-        // Lc e = r by FP32 red-black SOR (with the column-uniform correction), p += e in FP64.
-        const int inner = 24;
+        // Lc e = r by FP32 sweeps (with the column-uniform correction), p += e in FP64.
+        const int inner = line ? 3 : 48;
         int rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
             sor_resid32_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->r32, ctx->e32);
             nl++;
-            double re;
             for(int n = 0; n < inner && s < max_sweeps; n++, s++){
                 if(n % every == 0){
-                    rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, &re, nullptr); if(rc) return rc;
+                    rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc;
                     rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
-                    nl += 4;
+                    nl += 5;
                 }
-                sor_colour_kernel<float><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, ctx->e32, ctx->r32, ctx->rbw, 0, omega);
-                sor_colour_kernel<float><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(g, ctx->e32, ctx->r32, ctx->rbw, 1, omega);
+                sor_sweep<float>(ctx, ctx->e32, ctx->r32, omega, line);
                 nl += 2;
             }
             sor_axpy_kernel<<<148 * 8, 256, 0, ctx->st>>>(fs, P, ctx->e32);
@@ -559,10 +589,13 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
-    ctx->sor_nblk = (sJ * sN + 255) / 256;
-    add((size_t)(sNM + 1) * sN * 8); add((size_t)(sNM + 1) * sN * 8); add((sNM + 1) * 8); add(sJ * 8);
+    ctx->sor_nblk = ((sN + 31) / 32) * sJ;
+    ctx->sor_pb = std::min(32, 49152 / (8 * sJ) - 1);
+    for(int n = 0; n < 4; n++) add((size_t)(sNM + 1) * sN * 8);        // ct, st, ctT, stT
     add((size_t)sJ * sN * 8); add((size_t)(sNM + 1) * sJ * 8); add((size_t)(sNM + 1) * sJ * 8);
-    add((size_t)2 * (sNM + 1) * 2 * sJ * 8); add((size_t)2 * ctx->sor_nblk * 8);
+    add((size_t)2 * ctx->sor_nblk * 8); add((size_t)sJ * sN * 8);
+    for(int n = 0; n < 3; n++) add((size_t)(sNM + 1) * sJ * 8);        // mode factorisations
+    for(int n = 0; n < 3; n++) add(nij * 8);                           // line factorisations
     add(fs * 4); add(fs * 4);
     ctx->mem_bytes = bytes;
     if(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess){
@@ -594,11 +627,14 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->gsw = carve<GSW>(cur, nij); ctx->rbw = carve<RBW>(cur, nij);
     ctx->counters = carve<unsigned long long>(cur, 8);
     ctx->sor_ct = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_st = carve<double>(cur, (size_t)(sNM + 1) * sN);
-    ctx->sor_lam = carve<double>(cur, sNM + 1); ctx->sor_sj = carve<double>(cur, sJ);
+    ctx->sor_ctT = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_stT = carve<double>(cur, (size_t)(sNM + 1) * sN);
     ctx->sor_colR = carve<double>(cur, (size_t)sJ * sN);
     ctx->sor_Ac = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->sor_As = carve<double>(cur, (size_t)(sNM + 1) * sJ);
-    ctx->sor_work = carve<double>(cur, (size_t)2 * (sNM + 1) * 2 * sJ);
     ctx->sor_part = carve<double>(cur, (size_t)2 * ctx->sor_nblk);
+    ctx->sor_q = carve<double>(cur, (size_t)sJ * sN);
+    ctx->mlu_a = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->mlu_cf = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->mlu_idn = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->llu_a = carve<double>(cur, nij); ctx->llu_cf = carve<double>(cur, nij); ctx->llu_idn = carve<double>(cur, nij);
     ctx->r32 = carve<float>(cur, fs); ctx->e32 = carve<float>(cur, fs);
     ctx->host_part.resize(2 * ctx->sor_nblk);
 
@@ -722,16 +758,55 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     // RB_SOR tables: Fourier bases with the exact (m k mod N) reduction (PressureSolver.h:614-617),
     // eigenvalues of the phi ring, the shared solver's floored sine of the interior rows, and
     // A2y = sum_i y_i / rm_i^2 with the folded operator's left null vector y.
-    std::vector<double> sct((size_t)(sNM + 1) * sN), sst((size_t)(sNM + 1) * sN), slam(sNM + 1), ssj(sJ);
+    std::vector<double> sct((size_t)(sNM + 1) * sN), sst((size_t)(sNM + 1) * sN);
+    std::vector<double> sctT((size_t)(sNM + 1) * sN), sstT((size_t)(sNM + 1) * sN);
+    std::vector<double> ma((size_t)(sNM + 1) * sJ), mcf((size_t)(sNM + 1) * sJ), midn((size_t)(sNM + 1) * sJ);
     for(int m = 0; m <= sNM; m++){
         for(int k = 0; k < sN; k++){
             const double a = 2.0 * M_PI * (double)((long)m * k % sN) / sN;
             sct[(size_t)m * sN + k] = std::cos(a); sst[(size_t)m * sN + k] = std::sin(a);
+            sctT[(size_t)k * (sNM + 1) + m] = std::cos(a); sstT[(size_t)k * (sNM + 1) + m] = std::sin(a);
         }
+        // theta tridiagonal of mode m, ends folded (q0 = c43 q1 - c13 q2), factored once
         const double sl = std::sin(M_PI * m / sN);
-        slam[m] = 4.0 * sl * sl * inv_dphi2;
+        const double lam = 4.0 * sl * sl * inv_dphi2;
+        const double e = inv_dthe2;
+        std::vector<double> A(sJ), B(sJ), Cc(sJ);
+        for(int q = 0; q < sJ; q++){
+            const double s_ = st_shared[q + 1];
+            A[q] = e; Cc[q] = e; B[q] = -2.0 * e - lam / (s_ * s_);
+        }
+        A[0] = 0.0;       B[0] += C43 * e;      Cc[0] -= C13 * e;
+        Cc[sJ - 1] = 0.0; B[sJ - 1] += C43 * e; A[sJ - 1] -= C13 * e;
+        if(m == 0){ B[0] = 1.0; Cc[0] = 0.0; }                         // pin q at the first row
+        double* fa = &ma[(size_t)m * sJ]; double* fc = &mcf[(size_t)m * sJ]; double* fi = &midn[(size_t)m * sJ];
+        fa[0] = 0.0; fi[0] = 1.0 / B[0]; fc[0] = Cc[0] * fi[0];
+        for(int q = 1; q < sJ; q++){
+            const double dn = B[q] - A[q] * fc[q - 1];
+            fa[q] = A[q]; fi[q] = 1.0 / dn; fc[q] = Cc[q] * fi[q];
+        }
     }
-    for(int q = 0; q < sJ; q++) ssj[q] = st_shared[q + 1];
+    // radial-line tridiagonal of every (i,j) column of the folded operator, factored once
+    std::vector<double> la(nij, 0.0), lcf(nij, 0.0), lidn(nij, 0.0);
+    for(int j = 1; j < g.jm - 1; j++){
+        const int n = g.im - 2;
+        std::vector<double> A(n), B(n), Cc(n);
+        for(int q = 0; q < n; q++){
+            const RBW& R = rbw[(size_t)(q + 1) * g.jm + j];
+            double d = R.den;
+            if(j == 1) d -= C43 * R.num2;
+            if(j == g.jm - 2) d -= C43 * R.num2;
+            A[q] = -R.num1; B[q] = d; Cc[q] = -R.num1;
+        }
+        B[0] += A[0] * C43; Cc[0] -= A[0] * C13; A[0] = 0.0;
+        B[n - 1] += Cc[n - 1] * C43; A[n - 1] -= Cc[n - 1] * C13; Cc[n - 1] = 0.0;
+        double cfp = 0.0;
+        for(int q = 0; q < n; q++){
+            const double dn = (q == 0) ? B[0] : B[q] - A[q] * cfp;
+            const size_t f = (size_t)(q + 1) * g.jm + j;
+            la[f] = A[q]; lidn[f] = 1.0 / dn; cfp = Cc[q] * lidn[f]; lcf[f] = cfp;
+        }
+    }
     double A2y = 0.0;
     for(int i = 1; i < g.im - 1; i++){
         const double rm = metric_radius(*p, rad[i]);
@@ -751,8 +826,14 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     bad |= up(ctx->rbw, rbw.data(), nij * sizeof(RBW));
     bad |= up(ctx->sor_ct, sct.data(), sct.size() * 8);
     bad |= up(ctx->sor_st, sst.data(), sst.size() * 8);
-    bad |= up(ctx->sor_lam, slam.data(), slam.size() * 8);
-    bad |= up(ctx->sor_sj, ssj.data(), ssj.size() * 8);
+    bad |= up(ctx->sor_ctT, sctT.data(), sctT.size() * 8);
+    bad |= up(ctx->sor_stT, sstT.data(), sstT.size() * 8);
+    bad |= up(ctx->mlu_a, ma.data(), ma.size() * 8);
+    bad |= up(ctx->mlu_cf, mcf.data(), mcf.size() * 8);
+    bad |= up(ctx->mlu_idn, midn.data(), midn.size() * 8);
+    bad |= up(ctx->llu_a, la.data(), nij * 8);
+    bad |= up(ctx->llu_cf, lcf.data(), nij * 8);
+    bad |= up(ctx->llu_idn, lidn.data(), nij * 8);
     std::vector<GeoIJ<float>> geo32;
     std::vector<float> cp32;
     if(ctx->mixed){
@@ -875,8 +956,9 @@ int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, dou
         if(!rc && sweeps_done) *sweeps_done = max_sweeps < 1 ? 1 : max_sweeps;
         return rc;
     case ATURAN_PRESS_RB_SOR:
-        return ctx->mixed ? run_sor<float>(ctx, omega, max_sweeps, tol, sweeps_done, resid)
-                          : run_sor<double>(ctx, omega, max_sweeps, tol, sweeps_done, resid);
+    case ATURAN_PRESS_RB_LINE:
+        return ctx->mixed ? run_sor<float>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, sweeps_done, resid)
+                          : run_sor<double>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, sweeps_done, resid);
     }
     return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
 }

@@ -69,35 +69,67 @@ __device__ __forceinline__ C cp_lapse(const RhsConst<C>& k, const C* tab, C T){
 template <typename C>
 struct D6 { C c, d1r, d2r, d1t, d2t, d1p, d2p; };
 
-// RHS_Uran_Turb.cpp:93-176: central first and second differences of one field.
+// The seven stencil values of one field at one cell, as loaded.
+template <typename C>
+struct R7 { C c, rp, rm, tp, tm, pe, pw; };
+
+// Neighbour addressing of one cell: offsets and, per direction, the array a neighbour is read
+// from (the stage input, or the state on a boundary row).
+template <typename S>
+struct Nbr {
+    size_t o, oim, oip, ojm, ojp, okw, oke, fs;
+    const S *X, *xim, *xip, *xjm, *xjp;
+};
+
 template <typename S, typename C>
-__device__ __forceinline__ D6<C> stencil(const RhsConst<C>& k, const S* xc, const S* xim, const S* xip,
-                                         const S* xjm, const S* xjp, size_t o, size_t oim, size_t oip,
-                                         size_t ojm, size_t ojp, size_t okw, size_t oke){
+__device__ __forceinline__ R7<C> load7(const Nbr<S>& n, int q){
+    const size_t f = (size_t)q * n.fs;
+    R7<C> r;
+    r.c  = (C)ld(n.X + f + n.o);
+    r.rp = (C)ld(n.xip + f + n.oip); r.rm = (C)ld(n.xim + f + n.oim);
+    r.tp = (C)ld(n.xjp + f + n.ojp); r.tm = (C)ld(n.xjm + f + n.ojm);
+    r.pe = (C)ld(n.X + f + n.oke);   r.pw = (C)ld(n.X + f + n.okw);
+    return r;
+}
+
+// RHS_Uran_Turb.cpp:93-176: central first and second differences of one field.
+template <typename C>
+__device__ __forceinline__ D6<C> diff6(const RhsConst<C>& k, const R7<C>& v){
     D6<C> d;
-    const C c  = (C)ld(xc + o);
-    const C rp = (C)ld(xip + oip), rm = (C)ld(xim + oim);
-    const C tp = (C)ld(xjp + ojp), tm = (C)ld(xjm + ojm);
-    const C pe = (C)ld(xc + oke),  pw = (C)ld(xc + okw);
+    const C c = v.c;
     d.c   = c;
-    d.d1r = (rp - rm) * k.inv_2dr;
-    d.d2r = (rp - C(2.0) * c + rm) * k.inv_dr2;
-    d.d1t = (tp - tm) * k.inv_2dthe;
-    d.d2t = (tp - C(2.0) * c + tm) * k.inv_dthe2;
-    d.d1p = (pe - pw) * k.inv_2dphi;
-    d.d2p = (pe - C(2.0) * c + pw) * k.inv_dphi2;
+    d.d1r = (v.rp - v.rm) * k.inv_2dr;
+    d.d2r = (v.rp - C(2.0) * c + v.rm) * k.inv_dr2;
+    d.d1t = (v.tp - v.tm) * k.inv_2dthe;
+    d.d2t = (v.tp - C(2.0) * c + v.tm) * k.inv_dthe2;
+    d.d1p = (v.pe - v.pw) * k.inv_2dphi;
+    d.d2p = (v.pe - C(2.0) * c + v.pw) * k.inv_dphi2;
     return d;
+}
+
+// The accumulator (stages 1-3) and the start-of-step copy of one field at one cell.
+template <typename C>
+struct AccNc { C acc, nc; };
+
+template <typename S, typename C>
+__device__ __forceinline__ AccNc<C> load_acc_nc(const StageArgs<S, C>& a, int q, size_t o){
+    const size_t off = (size_t)q * a.g.fstride + o;
+    AccNc<C> v;
+    v.acc = (a.stage == 0) ? C(0.0) : (C)a.acc[off];
+    v.nc = (C)ld(a.Nc + off);
+    return v;
 }
 
 // acc and next-stage / final update of one prognostic field (RungeKutta_Uran_Turb.cpp:291-403).
 // kind: 0 plain, 1 temperature (final clamp), 2 k* (clamp), 3 dis* (floor).
 template <typename S, typename C>
-__device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, size_t o, C r, int kind){
+__device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, size_t o, C r, int kind,
+                                             const AccNc<C>& an){
     const size_t off = (size_t)q * a.g.fstride + o;
     C accv;
     if(a.stage == 0) accv = a.wgt * r;
-    else accv = (C)a.acc[off] + a.wgt * r;
-    const C yn = (C)ld(a.Nc + off);
+    else accv = an.acc + a.wgt * r;
+    const C yn = an.nc;
     if(a.stage < 3){
         a.acc[off] = (S)accv;
         C y = yn + a.c_in * r;
@@ -113,14 +145,91 @@ __device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, si
     }
 }
 
-// Fused RHS evaluation and stage update of one cell. PART selects the equations: 0 all of them,
-// 1 momentum and temperature (u, v, w, t and the projection fields), 2 the fifteen scalar fields
-// (twelve condensables, NH4SH, k*, dis*). The two parts read disjoint stencil fields and write
-// disjoint accumulator / stage-output fields, so they may run as two launches of one stage; the
-// split halves the live registers per thread, which doubles the warps an SM keeps in flight
-// (the kernel is latency-bound on its stencil loads). SU unrolls the scalar loop so that SU
-// stencils' loads are in flight together; MINB is the launch bound on resident blocks per SM.
-template <typename S, typename C, int PART, int SU, int MINB>
+// Everything one scalar field's tendency reads at one cell: its stencil, accumulator, n-copy and
+// up to three forcing values.
+template <typename C>
+struct ScalarIn { R7<C> v; AccNc<C> an; C f1, f2, f3; };
+
+// Scalar field n of the stage's second part: 0..11 the condensables (ATURAN_CH4 + n), 12 NH4SH,
+// 13 k*, 14 dis*.
+constexpr int N_SCALARS = 15;
+__host__ __device__ constexpr int scalar_field(int n){
+    return n < 12 ? ATURAN_CH4 + n : (n == 12 ? ATURAN_NH4SH : (n == 13 ? ATURAN_TKE : ATURAN_DIS));
+}
+
+template <typename S, typename C>
+__device__ __forceinline__ void load_scalar(ScalarIn<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
+    const int q = scalar_field(n);
+    const S* F = a.forc + nb.o;
+    const size_t fs = nb.fs;
+    in.v = load7<S, C>(nb, q);
+    in.an = load_acc_nc(a, q, nb.o);
+    in.f2 = C(0.0); in.f3 = C(0.0);
+    if(n < 12){
+        in.f1 = (C)ld(F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs);
+        if(q == ATURAN_H2S) in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs);
+        if(q == ATURAN_NH3) in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs);
+    } else if(n == 12){
+        in.f1 = (C)ld(F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs);
+        in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs);
+        in.f3 = (C)ld(F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs);
+    } else {
+        in.f1 = (C)ld(F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs);
+    }
+}
+
+// Tendency and stage update of scalar field n from its loaded inputs (:790-913, :989-1018).
+template <typename S, typename C>
+__device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const ScalarIn<C>& in, int n, size_t o,
+                                              const GeoIJ<C>& geo, C u_ijk, C v_ijk, C w_ijk, C v_invrm,
+                                              C w_invrs, C nue_c, C nue_t_s){
+    const RhsConst<C>& K = a.k;
+    const int q = scalar_field(n);
+    const D6<C> Q = diff6(K, in.v);
+    if(n < 12){
+        // ---- the twelve condensables (:790-850) ----
+        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
+        const C diffusion = Q.d2r + Q.d1r * geo.two_inv_rm + Q.d2t * geo.inv_rm2
+            + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
+        C r = - transport + diffusion / K.sc_re[n / 3] + diffusion * nue_t_s;
+        if(q == ATURAN_H2S || q == ATURAN_NH3) r = r + K.chemical_reaction * in.f2;
+        r = r + K.precip_coupling * in.f1;
+        stage_update(a, q, o, r, 0, in.an);
+    } else if(n == 12){
+        // ---- NH4SH: flux limiter, chemistry and Stokes settling (:852-913) ----
+        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
+        const C diffusion = Q.d2r + Q.d1r * geo.two_inv_rm + Q.d2t * geo.inv_rm2
+            + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
+        const C v_stokes = K.stokes_a * (K.rho_cond_nh4sh - in.f3) * K.g / K.mue_mix;
+        const C r = - transport + in.f1
+                    + diffusion / K.sc_re[4] + diffusion * nue_t_s
+                    + K.chemical_reaction * in.f2
+                    + (v_stokes / K.u_0) * Q.d1r;
+        stage_update(a, q, o, r, 0, in.an);
+    } else {
+        // ---- k* and dis* (:989-1018) ----
+        const C transport = u_ijk * Q.d1r + v_ijk * Q.d1t * geo.inv_rm + w_ijk * Q.d1p * geo.inv_rmsinthe;
+        const C diffusion = Q.d2r + Q.d1r * C(2.0) * geo.inv_rm + Q.d2t * geo.inv_rm2
+            + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
+        const C sig = n == 13 ? C(0.85) : C(0.5);
+        const C r = - transport + diffusion * (K.inv_re + nue_c / sig) + in.f1;
+        stage_update(a, q, o, r, n == 13 ? 2 : 3, in.an);
+    }
+}
+
+// Fused RHS evaluation and stage update of one cell. PART selects the equations: 1 momentum and
+// temperature (u, v, w, t and the projection fields), 2 the fifteen scalar fields (twelve
+// condensables, NH4SH, k*, dis*). The two parts read disjoint stencil fields and write disjoint
+// accumulator / stage-output fields, so they run as two launches of one stage with half the
+// live registers each.
+//
+// The kernel is bound by the latency of its loads, not by HBM bytes, so it is written to keep
+// many loads in flight per thread: a store to acc or Y could alias any later load as far as the
+// compiler knows, so no load is ever placed after a store in program order. Part 1 issues all
+// of its ~50 loads before its first store; part 2 walks its 15 fields with the inputs of the
+// next PD fields already loading while one field is computed and stored. MINB is the launch
+// bound on resident blocks per SM.
+template <typename S, typename C, int PART, int PD, int MINB>
 __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, C> a){
     const Grid& g = a.g;
     const int k = blockIdx.x * 32 + threadIdx.x;
@@ -130,18 +239,20 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
     const RhsConst<C>& K = a.k;
     const GeoIJ<C> geo = a.geo[i * g.jm + j];
 
-    const size_t o   = gidx(g, i, j, k);
-    const size_t oim = o - (size_t)g.jm * g.kp, oip = o + (size_t)g.jm * g.kp;
-    const size_t ojm = o - g.kp, ojp = o + g.kp;
-    const int kwi = phi_wrap(k - 1, g.km), kei = phi_wrap(k + 1, g.km);
-    const size_t okw = o - k + kwi, oke = o - k + kei;
-    const S* xim = (i == 1) ? a.St : a.X;
-    const S* xip = (i == g.im - 2) ? a.St : a.X;
-    const S* xjm = (j == 1) ? a.St : a.X;
-    const S* xjp = (j == g.jm - 2) ? a.St : a.X;
-    const size_t fs = g.fstride;
-#define STENCIL(q) stencil<S, C>(K, a.X + (size_t)(q) * fs, xim + (size_t)(q) * fs, xip + (size_t)(q) * fs, \
-                                 xjm + (size_t)(q) * fs, xjp + (size_t)(q) * fs, o, oim, oip, ojm, ojp, okw, oke)
+    Nbr<S> nb;
+    nb.fs  = g.fstride;
+    nb.o   = gidx(g, i, j, k);
+    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
+    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
+    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
+    nb.oke = nb.o - k + phi_wrap(k + 1, g.km);
+    nb.X   = a.X;
+    nb.xim = (i == 1) ? a.St : a.X;
+    nb.xip = (i == g.im - 2) ? a.St : a.X;
+    nb.xjm = (j == 1) ? a.St : a.X;
+    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
+    const size_t o = nb.o, fs = g.fstride;
+    const size_t oim = nb.oim, oip = nb.oip, ojm = nb.ojm, ojp = nb.ojp, okw = nb.okw, oke = nb.oke;
 #define FORC(id) ((C)ld(a.forc + (size_t)((id) - ATURAN_NUE) * fs + o))
 
     const C inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rmsinthe = geo.inv_rmsinthe;
@@ -153,14 +264,26 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
     const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
     const C nue_t_s = nue_t / C(0.9);
 
-    if constexpr(PART != 2){
-    // pressure gradients (:117, :146, :175), FP64 differences
+    if constexpr(PART == 1){
+    // ---- every load of the cell first ----
     const double* P = a.pdyn;
-    const C dpdr   = (C)((ld(P + oip) - ld(P + oim)) * (double)K.inv_2dr);
-    const C dpdthe = (C)((ld(P + ojp) - ld(P + ojm)) * (double)K.inv_2dthe);
-    const C dpdphi = (C)((ld(P + oke) - ld(P + okw)) * (double)K.inv_2dphi);
+    const double* PH = a.phydro;
+    const double p_ip = ld(P + oip), p_im = ld(P + oim), p_jp = ld(P + ojp), p_jm = ld(P + ojm);
+    const double p_ke = ld(P + oke), p_kw = ld(P + okw);
+    const double ph_jp = ld(PH + ojp), ph_jm = ld(PH + ojm), ph_ke = ld(PH + oke), ph_kw = ld(PH + okw);
+    const R7<C> rU = load7<S, C>(nb, ATURAN_U), rV = load7<S, C>(nb, ATURAN_V), rW = load7<S, C>(nb, ATURAN_W);
+    const R7<C> rT = load7<S, C>(nb, ATURAN_T);
+    const AccNc<C> anU = load_acc_nc(a, ATURAN_U, o), anV = load_acc_nc(a, ATURAN_V, o);
+    const AccNc<C> anW = load_acc_nc(a, ATURAN_W, o), anT = load_acc_nc(a, ATURAN_T, o);
+    const C f_tmf = (K.tmf != C(0.0)) ? FORC(ATURAN_THERMALMASSFLUX) : C(0.0);
+    const C f_qp = (K.precip_coupling != C(0.0)) ? FORC(ATURAN_Q_PRECIP) : C(0.0);
 
-    const D6<C> U = STENCIL(ATURAN_U), V = STENCIL(ATURAN_V), W = STENCIL(ATURAN_W);
+    // pressure gradients (:117, :146, :175), FP64 differences
+    const C dpdr   = (C)((p_ip - p_im) * (double)K.inv_2dr);
+    const C dpdthe = (C)((p_jp - p_jm) * (double)K.inv_2dthe);
+    const C dpdphi = (C)((p_ke - p_kw) * (double)K.inv_2dphi);
+
+    const D6<C> U = diff6(K, rU), V = diff6(K, rV), W = diff6(K, rW);
     const C u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
     const C v_invrm = v_ijk * inv_rm;
     const C w_invrs = w_ijk * inv_rmsinthe;
@@ -193,9 +316,8 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
         const C dpdr_term   = dpdr   * K.scale_p;
         const C dpdthe_term = dpdthe * K.scale_p * inv_rm;
         const C dpdphi_term = dpdphi * K.scale_p * inv_rmsinthe;
-        const double* PH = a.phydro;
-        const C dphdthe_term = (C)((ld(PH + ojp) - ld(PH + ojm)) * (double)K.inv_2dthe) * inv_rm;
-        const C dphdphi_term = (C)((ld(PH + oke) - ld(PH + okw)) * (double)K.inv_2dphi) * inv_rmsinthe;
+        const C dphdthe_term = (C)((ph_jp - ph_jm) * (double)K.inv_2dthe) * inv_rm;
+        const C dphdphi_term = (C)((ph_ke - ph_kw) * (double)K.inv_2dphi) * inv_rmsinthe;
         const C re_eff = K.re_eff;
         const C rhs_u = - dpdr_term + C(0.0) - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
                         - K.cor_rad_f * Coriolis_rad
@@ -206,9 +328,9 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
                         + K.cen_f * geo.cent_the;
         const C rhs_w = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
                         - K.cor_sc * Coriolis_phi;
-        stage_update(a, ATURAN_U, o, rhs_u, 0);
-        stage_update(a, ATURAN_V, o, rhs_v, 0);
-        stage_update(a, ATURAN_W, o, rhs_w, 0);
+        stage_update(a, ATURAN_U, o, rhs_u, 0, anU);
+        stage_update(a, ATURAN_V, o, rhs_v, 0, anV);
+        stage_update(a, ATURAN_W, o, rhs_w, 0, anW);
         if(a.stage == 3){
             a.proj[0 * fs + o] = (S)rhs_u;
             a.proj[1 * fs + o] = (S)rhs_v;
@@ -221,78 +343,44 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
 
     // ---- temperature (:280-298, :329-334, :528-557) ----
     {
-        const D6<C> T = STENCIL(ATURAN_T);
+        const D6<C> T = diff6(K, rT);
         C pressure_t = K.ce_sp * (u_ijk * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
         if(K.cp_dyn && T.c > C(0.0)) pressure_t *= K.cp_mix / cp_lapse(K, a.cp_tab, T.c * K.t_ref);
         const C transport_t = u_ijk * T.d1r + v_invrm * T.d1t + w_invrs * T.d1p;
         const C diffusion_t = T.d2r + T.d1r * two_inv_rm + T.d2t * inv_rm2
             + T.d1t * costhe_inv_rm2sinthe + T.d2p * inv_rm2sinthe2;
-        const C tmf = (K.tmf != C(0.0)) ? K.tmf * FORC(ATURAN_THERMALMASSFLUX) : C(0.0);
+        const C tmf = (K.tmf != C(0.0)) ? K.tmf * f_tmf : C(0.0);
         C precip_t = C(0.0);
         if(K.precip_coupling != C(0.0)){
-            precip_t = K.precip_coupling * FORC(ATURAN_Q_PRECIP) * K.precip_L / K.precip_den;
+            precip_t = K.precip_coupling * f_qp * K.precip_L / K.precip_den;
             if(!isfinite(precip_t)) precip_t = C(0.0);
             else if(precip_t >  C(0.5)) precip_t =  C(0.5);
             else if(precip_t < -C(0.5)) precip_t = -C(0.5);
         }
         const C rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
                         - tmf + C(0.0) + precip_t;
-        stage_update(a, ATURAN_T, o, rhs_t, 1);
+        stage_update(a, ATURAN_T, o, rhs_t, 1, anT);
+    }
     }
 
-    }
-
-    if constexpr(PART != 1){
+    if constexpr(PART == 2){
     const C u_ijk = (C)ld(a.X + (size_t)ATURAN_U * fs + o);
     const C v_ijk = (C)ld(a.X + (size_t)ATURAN_V * fs + o);
     const C w_ijk = (C)ld(a.X + (size_t)ATURAN_W * fs + o);
     const C v_invrm = v_ijk * inv_rm;
     const C w_invrs = w_ijk * inv_rmsinthe;
-    // ---- the twelve condensables (:790-850) ----
-#pragma unroll SU
-    for(int s = 0; s < 12; s++){
-        const int q = ATURAN_CH4 + s;
-        const D6<C> Q = STENCIL(q);
-        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
-        const C diffusion = Q.d2r + Q.d1r * two_inv_rm + Q.d2t * inv_rm2
-            + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
-        C r = - transport + diffusion / K.sc_re[s / 3] + diffusion * nue_t_s;
-        if(q == ATURAN_H2S) r = r + K.chemical_reaction * FORC(ATURAN_MASSFLUX_H2S);
-        if(q == ATURAN_NH3) r = r + K.chemical_reaction * FORC(ATURAN_MASSFLUX_NH3);
-        r = r + K.precip_coupling * FORC(ATURAN_S_PRECIP_CH4 + s);
-        stage_update(a, q, o, r, 0);
-    }
-    // ---- NH4SH: flux limiter, chemistry and Stokes settling (:852-913) ----
-    {
-        const D6<C> Q = STENCIL(ATURAN_NH4SH);
-        const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
-        const C diffusion = Q.d2r + Q.d1r * two_inv_rm + Q.d2t * inv_rm2
-            + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
-        const C v_stokes = K.stokes_a * (K.rho_cond_nh4sh - FORC(ATURAN_RHO_MIX)) * K.g / K.mue_mix;
-        const C r = - transport + FORC(ATURAN_FLUXLIM_NH4SH)
-                    + diffusion / K.sc_re[4] + diffusion * nue_t_s
-                    + K.chemical_reaction * FORC(ATURAN_MASSFLUX_NH4SH)
-                    + (v_stokes / K.u_0) * Q.d1r;
-        stage_update(a, ATURAN_NH4SH, o, r, 0);
-    }
-
-    // ---- k* and dis* (:989-1018) ----
-    if(K.turb_active){
-#pragma unroll 1
-        for(int n = 0; n < 2; n++){
-            const int q = ATURAN_TKE + n;
-            const D6<C> Q = STENCIL(q);
-            const C transport = u_ijk * Q.d1r + v_ijk * Q.d1t * inv_rm + w_ijk * Q.d1p * inv_rmsinthe;
-            const C diffusion = Q.d2r + Q.d1r * C(2.0) * inv_rm + Q.d2t * inv_rm2
-                + Q.d1t * costhe_inv_rm2sinthe + Q.d2p * inv_rm2sinthe2;
-            const C sig = n == 0 ? C(0.85) : C(0.5);
-            const C r = - transport + diffusion * (K.inv_re + nue_c / sig)
-                        + FORC(n == 0 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE);
-            stage_update(a, q, o, r, n == 0 ? 2 : 3);
-        }
+    const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
+    // ring of PD + 1 field inputs: fields n+1..n+PD load while field n is computed and stored
+    ScalarIn<C> ring[PD + 1];
+#pragma unroll
+    for(int n = 0; n < PD; n++) if(n < nfield) load_scalar(ring[n], a, nb, n);
+#pragma unroll
+    for(int n = 0; n < N_SCALARS; n++){
+        if(n + PD < nfield) load_scalar(ring[(n + PD) % (PD + 1)], a, nb, n + PD);
+        if(n < nfield)
+            scalar_update(a, ring[n % (PD + 1)], n, o, geo, u_ijk, v_ijk, w_ijk, v_invrm, w_invrs, nue_c, nue_t_s);
     }
     }
-#undef STENCIL
 #undef FORC
 }
 

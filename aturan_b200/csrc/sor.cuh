@@ -34,6 +34,11 @@ struct SorConst {
     double inv_dthe2, A2y;
 };
 
+// Host-factored tridiagonal of one Fourier mode of the column correction (rows q = 0..J-1):
+// forward y_q = (d_q - a_q y_{q-1}) * idn_q, back x_q = y_q - cf_q x_{q+1}. Mode 0 carries the pin
+// q_0 = 0 in its first row.
+struct ModeLU { const double *a, *cf, *idn; };
+
 __device__ __forceinline__ double ywt(int n, int lo, int hi){ return (n == lo || n == hi) ? 1.5 : 1.0; }
 
 // The shared solver's operator with the 2-point Neumann folds substituted into the rows (at i = 1
@@ -59,21 +64,21 @@ __device__ __forceinline__ double folded_acc(const Grid& g, const T* P, size_t o
          + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
 }
 
-// Per (j,k) column: y-weighted sum of r = src - Lc p over the interior levels, and per-block
-// partial sums of r^2 and src^2 (fixed tree order). P of type T (double for the FP64 solve,
-// float for the correction solve of the mixed form), src of type T.
+// Residual r = src - Lc p of the folded operator: per (j,k) column its y-weighted sum over the
+// interior levels, and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
+// groups; the groups' column sums are added in group order and the block's norms in a fixed tree
+// order, so the result is deterministic. P and src of type T (double: FP64 solve; float: the
+// correction solve of the mixed form).
 template <typename T>
 __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, const T* src, const RBW* w,
                                                          double* colR, double* part, int want_col){
-    const int J = g.jm - 2, N = g.km - 1;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double rr = 0.0, ss = 0.0;
-    if(c < J * N){
-        const int j = 1 + c / N, k = c - (j - 1) * N;
-        const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
-        double R = 0.0;
-        (void)kw; (void)ke;
-        for(int i = 1; i < g.im - 1; i++){
+    const int N = g.km - 1;
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    const int grp = threadIdx.y;
+    double R = 0.0, rr = 0.0, ss = 0.0;
+    if(k < N){
+        for(int i = 1 + grp; i < g.im - 1; i += 8){
             const RBW W = w[i * g.jm + j];
             const size_t o = gidx(g, i, j, k);
             double diag;
@@ -85,95 +90,155 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
             rr += r * r;
             ss += s * s;
         }
-        if(want_col) colR[(size_t)(j - 1) * N + k] = R;
     }
-    __shared__ double sr[256], sq[256];
-    sr[threadIdx.x] = rr; sq[threadIdx.x] = ss;
+    __shared__ double sR[8][32], sr[256], sq[256];
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    sR[grp][threadIdx.x] = R; sr[t] = rr; sq[t] = ss;
     __syncthreads();
+    if(grp == 0 && want_col && k < N){
+        double c = 0.0;
+        for(int q = 0; q < 8; q++) c += sR[q][threadIdx.x];
+        colR[(size_t)(j - 1) * N + k] = c;
+    }
     for(int st = 128; st > 0; st >>= 1){
-        if(threadIdx.x < st){ sr[threadIdx.x] += sr[threadIdx.x + st]; sq[threadIdx.x] += sq[threadIdx.x + st]; }
+        if(t < st){ sr[t] += sr[t + st]; sq[t] += sq[t + st]; }
         __syncthreads();
     }
-    if(threadIdx.x == 0){ part[2 * blockIdx.x] = sr[0]; part[2 * blockIdx.x + 1] = sq[0]; }
+    if(t == 0){
+        const int b = blockIdx.y * gridDim.x + blockIdx.x;
+        part[2 * b] = sr[0]; part[2 * b + 1] = sq[0];
+    }
 }
 
-// DFT in phi of colR / A2y: Ac[m][j] = sum_k R cos(2 pi m k / N), As likewise with sin.
-// ct/st are host-built tables with the (m k mod N) reduction of PressureSolver.h:614-617.
-__global__ void sor_dft_kernel(SorConst s, const double* colR, const double* ct, const double* st,
-                               double* Ac, double* As){
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if(t >= (s.NM + 1) * s.J) return;
-    const int m = t / s.J, jj = t - m * s.J;
-    const double* r = colR + (size_t)jj * s.N;
-    const double* c = ct + (size_t)m * s.N;
-    const double* sn = st + (size_t)m * s.N;
-    double sc = 0.0, ss = 0.0;
-    for(int k = 0; k < s.N; k++){ const double v = r[k] / s.A2y; sc += v * c[k]; ss += v * sn[k]; }
-    Ac[(size_t)m * s.J + jj] = sc;
-    As[(size_t)m * s.J + jj] = ss;
+// The two transforms of the correction are small dense products (J x N by N x (N/2+1) and back),
+// so they run as one tiled FP64 product kernel: C(r,c) = scale * sum_k A1(r,k) B1(k,c)
+// [+ A2(r,k) B2(k,c)], every operand addressed by (row, column) strides. A block computes a 32 x 32
+// tile of C from 32-wide k-chunks of A and B staged in shared memory (rows padded to 33: no bank
+// conflicts); each operand tile is loaded along whichever of its two indices has unit stride.
+//   forward:  Ac^T = (colR / A2y) . ctT,   As^T = (colR / A2y) . stT   (ctT[k][m] = cos(2 pi m k/N))
+//   inverse:  q = Ac^T . ct + As^T . st,  Ac/As carrying the weights w_m / N (tridiagonal write-back)
+// ct/st are host-built with the (m k mod N) argument reduction of PressureSolver.h:614-617.
+struct MatRef { const double* p; long rs, cs; };      // element (r, c) at p[r * rs + c * cs]
+
+__device__ __forceinline__ void gemm_stage(double (*t)[33], const MatRef& A, int r0, int k0, int R, int K){
+    const bool kfast = (A.cs == 1);
+    for(int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x){
+        const int a = idx >> 5, b = idx & 31;          // b runs along the unit-stride index
+        const int r = kfast ? a : b, k = kfast ? b : a;
+        const int gr = r0 + r, gk = k0 + k;
+        t[r][k] = (gr < R && gk < K) ? A.p[(long)gr * A.rs + (long)gk * A.cs] : 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, MatRef A1, MatRef B1, MatRef A2,
+                                                       MatRef B2, double scale, double* C, long crs, long ccs){
+    __shared__ double sa[32][33], sb[32][33];           // sa[r][k], sb[c][k]
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int npair = A2.p ? 2 : 1;
+    for(int pr = 0; pr < npair; pr++){
+        const MatRef& A = pr ? A2 : A1;
+        const MatRef& B = pr ? B2 : B1;
+        const MatRef Bt{B.p, B.cs, B.rs};               // B^T: (c, k)
+        for(int k0 = 0; k0 < K; k0 += 32){
+            gemm_stage(sa, A, r0, k0, M, K);
+            gemm_stage(sb, Bt, c0, k0, Nn, K);
+            __syncthreads();
+#pragma unroll 8
+            for(int k = 0; k < 32; k++){
+                const double bv = sb[tx][k];
+#pragma unroll
+                for(int q = 0; q < 4; q++) acc[q] += sa[ty + 8 * q][k] * bv;
+            }
+            __syncthreads();
+        }
+    }
+    const int c = c0 + tx;
+#pragma unroll
+    for(int q = 0; q < 4; q++){
+        const int r = r0 + ty + 8 * q;
+        if(r < M && c < Nn) C[(long)r * crs + (long)c * ccs] = scale * acc[q];
+    }
 }
 
 // One tridiagonal solve per (mode, cos/sin part) in theta:
 //   (q[j+1] - 2 q[j] + q[j-1]) / dthe^2 - lam_m / s_j^2 q[j] = rhs[j],  lam_m = 4 sin^2(pi m/N)/dphi^2,
-// the ends folded with q0 = c43 q1 - c13 q2. Mode 0 is singular: its source is made consistent
-// with the left null vector (3/2, 1, ..., 1, 3/2) and q pinned to zero mean with those weights.
-// Thomas needs no pivoting: every row is diagonally dominant (|b| >= |a| + |c|, strictly for
-// m > 0; the folded end rows keep 2/3 e against 2/3 e).
-__global__ void sor_tridiag_kernel(SorConst s, const double* lam, const double* sj, double* Ac, double* As,
-                                   double* work){
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if(t >= 2 * (s.NM + 1)) return;
-    const int m = t >> 1, part = t & 1;
-    if(part == 1 && (m == 0 || 2 * m == s.N)) { if(part == 1){ double* d = As + (size_t)m * s.J; for(int q = 0; q < s.J; q++) d[q] = 0.0; } return; }
-    double* d = (part == 0 ? Ac : As) + (size_t)m * s.J;
-    double* cp = work + (size_t)t * 2 * s.J;
-    double* dp = cp + s.J;
-    const int J = s.J;
-    const double e = s.inv_dthe2;
-    if(m == 0){
-        double yr = 0.0, ys = 0.0;
-        for(int q = 0; q < J; q++){ const double y = ywt(q, 0, J - 1); yr += y * d[q]; ys += y; }
-        for(int q = 0; q < J; q++) d[q] -= yr / ys;
+// the ends folded with q0 = c43 q1 - c13 q2, factored on the host once per context (ModeLU). Every
+// row is diagonally dominant, so the factorisation needs no pivoting. Mode 0 is singular: its
+// source is made consistent with the left null vector (3/2, 1, ..., 1, 3/2), q pinned at the first
+// row, and q returned with zero weighted mean. The result is written back times the inverse
+// transform's weight w_m / N (w = 1 for m = 0 and m = N/2, else 2).
+//
+// A block takes pb problems (problem t = 2 m + part): all of its threads stage the right-hand sides
+// into shared memory as [q][t] (row stride pb + 1: conflict-free), then one thread per problem runs
+// the two dependent recurrences on shared-memory latency, in place, and the block writes back.
+__global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pb){
+    extern __shared__ double sd[];
+    const int J = s.J, ld_ = pb + 1;
+    const int nprob = 2 * (s.NM + 1);
+    const int t0 = blockIdx.x * pb;
+    for(int idx = threadIdx.x; idx < pb * J; idx += blockDim.x){
+        const int lt = idx / J, q = idx - lt * J;
+        const int t = t0 + lt;
+        double v = 0.0;
+        if(t < nprob) v = ((t & 1) ? As : Ac)[(size_t)(t >> 1) * J + q];
+        sd[q * ld_ + lt] = v;
     }
-    auto A = [&](int q){ double a = e; if(q == 0) a = 0.0; if(q == J - 1) a -= C13 * e; return a; };
-    auto B = [&](int q){ double b = -2.0 * e - lam[m] / (sj[q] * sj[q]); if(q == 0 || q == J - 1) b += C43 * e; return b; };
-    auto Cc = [&](int q){ double c = e; if(q == J - 1) c = 0.0; if(q == 0) c -= C13 * e; return c; };
-    double b0 = B(0), c0 = Cc(0), d0 = d[0];
-    if(m == 0){ b0 = 1.0; c0 = 0.0; d0 = 0.0; }           // pin q at j = 1
-    cp[0] = c0 / b0; dp[0] = d0 / b0;
-    for(int q = 1; q < J; q++){
-        const double dn = B(q) - A(q) * cp[q - 1];
-        cp[q] = Cc(q) / dn;
-        dp[q] = (d[q] - A(q) * dp[q - 1]) / dn;
+    __syncthreads();
+    const int lt = threadIdx.x, t = t0 + lt;
+    if(lt < pb && t < nprob){
+        const int m = t >> 1, part = t & 1;
+        double* d = sd + lt;
+        if(part == 1 && (m == 0 || 2 * m == s.N)){
+            for(int q = 0; q < J; q++) d[q * ld_] = 0.0;
+        } else {
+            const double* a = lu.a + (size_t)m * J;
+            const double* cf = lu.cf + (size_t)m * J;
+            const double* idn = lu.idn + (size_t)m * J;
+            if(m == 0){
+                double yr = 0.0, ys = 0.0;
+                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yr += wq * d[q * ld_]; ys += wq; }
+                const double sh = yr / ys;
+                for(int q = 0; q < J; q++) d[q * ld_] -= sh;
+                d[0] = 0.0;                                   // the pinned row
+            }
+            double yp = 0.0;
+#pragma unroll 4
+            for(int q = 0; q < J; q++){ yp = (d[q * ld_] - a[q] * yp) * idn[q]; d[q * ld_] = yp; }
+            double x = d[(J - 1) * ld_];
+#pragma unroll 4
+            for(int q = J - 2; q >= 0; q--){ x = d[q * ld_] - cf[q] * x; d[q * ld_] = x; }
+            if(m == 0){
+                double yq = 0.0, ys = 0.0;
+                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yq += wq * d[q * ld_]; ys += wq; }
+                const double sh = yq / ys;
+                for(int q = 0; q < J; q++) d[q * ld_] -= sh;
+            }
+        }
     }
-    d[J - 1] = dp[J - 1];
-    for(int q = J - 2; q >= 0; q--) d[q] = dp[q] - cp[q] * d[q + 1];
-    if(m == 0){                                           // zero y-weighted mean
-        double yq = 0.0, ys = 0.0;
-        for(int q = 0; q < J; q++){ const double y = ywt(q, 0, J - 1); yq += y * d[q]; ys += y; }
-        for(int q = 0; q < J; q++) d[q] -= yq / ys;
+    __syncthreads();
+    for(int idx = threadIdx.x; idx < pb * J; idx += blockDim.x){
+        const int lt2 = idx / J, q = idx - lt2 * J;
+        const int t2 = t0 + lt2;
+        if(t2 < nprob){
+            const int m2 = t2 >> 1;
+            const double wm = ((m2 == 0 || 2 * m2 == s.N) ? 1.0 : 2.0) / s.N;   // inverse-transform weight
+            ((t2 & 1) ? As : Ac)[(size_t)m2 * J + q] = wm * sd[q * ld_ + lt2];
+        }
     }
 }
 
-// Back to phi and onto every interior level of the column: P[i][j][k] += q(j,k).
+// Onto every interior level of the column: P[i][j][k] += q(j,k).
 template <typename T>
-__global__ void sor_idft_add_kernel(Grid g, SorConst s, const double* Ac, const double* As, const double* ct,
-                                    const double* st, T* P){
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if(c >= s.J * s.N) return;
-    const int jj = c / s.N, k = c - jj * s.N;
-    double q = 0.0;
-    for(int m = 0; m <= s.NM; m++){
-        const bool edge = (m == 0 || 2 * m == s.N);
-        const double w_ = edge ? 1.0 : 2.0;
-        q += w_ * (Ac[(size_t)m * s.J + jj] * ct[(size_t)m * s.N + k]
-                   + (edge ? 0.0 : As[(size_t)m * s.J + jj] * st[(size_t)m * s.N + k]));
-    }
-    q /= s.N;
-    for(int i = 1; i < g.im - 1; i++){
-        const size_t o = gidx(g, i, jj + 1, k);
-        P[o] = (T)((double)P[o] + q);
-    }
+__global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf, T* P){
+    const int N = g.km - 1;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k >= N) return;
+    const size_t o = gidx(g, i, j, k);
+    P[o] = (T)((double)P[o] + qbuf[(size_t)(j - 1) * N + k]);
 }
 
 // Red-black SOR colour pass of the folded operator, Lc e = r, for T = double (the FP64 solve) or
@@ -195,6 +260,70 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
     const double e0 = (double)E[o];
     const double pn = (acc - (double)R[o]) / diag;
     E[o] = (T)(e0 + omega * (pn - e0));
+}
+
+// One colour of red-black LINE relaxation of the folded operator: every column (j,k) with
+// (j + k) & 1 == colour is solved exactly in r, its horizontal neighbours (the other colour, or the
+// column itself through the theta fold) held at their current values, then over-relaxed,
+// p += omega (p_line - p) -- the reference's PRESS_LINE (PressureSolver.h:497-570) on the folded
+// operator. The radial tridiagonal of each column (radial ends folded as :547-550) is factored on
+// the host: per (i,j) the row's sub-diagonal `la`, the factor `lcf` and the pivot reciprocal `lidn`
+// (the theta fold changes the diagonal on the first and last rows).
+//
+// A block takes 32 columns of one colour in one row j. Its 8 warps form the right-hand sides of
+// all levels in parallel (coalesced along k, one level per warp at a time) into shared memory
+// [level][column]; warp 0 then runs the 32 columns' forward and back recurrences on
+// shared-memory latency, in place; all warps write the relaxed columns back. Shared memory:
+// (im - 2) * 32 doubles.
+template <typename T>
+__global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
+                                                       const double* lcf, const double* lidn, int colour, double omega){
+    extern __shared__ double ds[];
+    const int n = g.im - 2;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int k2 = blockIdx.x * 32 + lane;
+    const int j = 1 + blockIdx.y;
+    const int k = 2 * k2 + ((j + colour) & 1);
+    const bool valid = k2 < g.km / 2 && k <= g.km - 2;
+    const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+    const size_t sj = g.kp;
+    for(int i = 1 + wp; i <= n; i += 8){
+        double d = 0.0;
+        if(valid){
+            const RBW W = w[i * g.jm + j];
+            const size_t o = gidx(g, i, j, k);
+            const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
+            const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
+            const double h = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+            d = h - (double)R[o];
+        }
+        ds[(i - 1) * 32 + lane] = d;
+    }
+    __syncthreads();
+    if(wp == 0){
+        double yp = 0.0;
+#pragma unroll 4
+        for(int i = 1; i <= n; i++){
+            const size_t f = (size_t)i * g.jm + j;
+            yp = (ds[(i - 1) * 32 + lane] - la[f] * yp) * lidn[f];
+            ds[(i - 1) * 32 + lane] = yp;
+        }
+        double x = ds[(n - 1) * 32 + lane];
+#pragma unroll 4
+        for(int i = n - 1; i >= 1; i--){
+            const size_t f = (size_t)i * g.jm + j;
+            x = ds[(i - 1) * 32 + lane] - lcf[f] * x;
+            ds[(i - 1) * 32 + lane] = x;
+        }
+    }
+    __syncthreads();
+    if(valid){
+        for(int i = 1 + wp; i <= n; i += 8){
+            const size_t o = gidx(g, i, j, k);
+            const double p0 = (double)P[o];
+            P[o] = (T)(p0 + omega * (ds[(i - 1) * 32 + lane] - p0));
+        }
+    }
 }
 
 // The folded boundary passes for any T (same order as pdyn_bc_*).

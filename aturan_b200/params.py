@@ -17,7 +17,7 @@ import math
 
 ABI_VERSION = 1
 FP64, MIXED = 0, 1
-PRESS_GS_LEX, PRESS_RB_SHARED, PRESS_RB_SOR = 0, 1, 2
+PRESS_GS_LEX, PRESS_RB_SHARED, PRESS_RB_SOR, PRESS_RB_LINE = 0, 1, 2, 3
 
 
 class Gas(ctypes.Structure):

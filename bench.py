@@ -111,6 +111,8 @@ def press_args(name):
         return dict(kind=P.PRESS_GS_LEX, omega=1.0, max_sweeps=1, tol=0.0), "GS_LEX: one lexicographic sweep (PressureSolverUran)"
     if name == "rb":
         return dict(kind=P.PRESS_RB_SHARED, omega=1.0, max_sweeps=1, tol=0.0), "RB_SHARED: one red-black sweep (PressureSolver)"
+    if name == "line":
+        return dict(kind=P.PRESS_RB_LINE, omega=1.0, max_sweeps=50, tol=1e-6), "RB_LINE to relative residual 1e-6, omega 1.0"
     return dict(kind=P.PRESS_RB_SOR, omega=1.8, max_sweeps=400, tol=1e-6), "RB_SOR to relative residual 1e-6, omega 1.8"
 
 
@@ -194,7 +196,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--press", default="gs", choices=["gs", "rb", "sor"])
+    ap.add_argument("--press", default="gs", choices=["gs", "rb", "sor", "line"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)

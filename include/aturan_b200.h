@@ -136,8 +136,10 @@ typedef struct aturan_params {
 enum aturan_pressure_kind {
     ATURAN_PRESS_GS_LEX    = 0, /* PressureSolverUran::run, one lexicographic GS sweep (default) */
     ATURAN_PRESS_RB_SHARED = 1, /* PressureSolver<cUranusModel>::run, max_sweeps red-black sweeps */
-    ATURAN_PRESS_RB_SOR    = 2  /* the shared solver's equation solved to a relative residual with
-                                   red-black SOR at omega (new behaviour, no reference oracle) */
+    ATURAN_PRESS_RB_SOR    = 2, /* the shared solver's equation solved to a relative residual with
+                                   point red-black SOR at omega (new behaviour, no reference oracle) */
+    ATURAN_PRESS_RB_LINE   = 3  /* the same equation and tolerance with red-black radial-line SOR,
+                                   each column solved exactly in r (the reference's PRESS_LINE) */
 };
 
 typedef struct aturan_ctx aturan_ctx;
@@ -175,7 +177,11 @@ int aturan_rk4_step(aturan_ctx* ctx);
  *   RB_SHARED: replaces PressureSolver<cUranusModel>(m).run() (PressureSolver.h:145-766) with
  *              ATURAN_PRESS_SWEEPS = max_sweeps; omega and tol ignored.
  *   RB_SOR:    the shared solver's equation (its source, clamp and boundary folds) solved with
- *              red-black SOR at omega until the relative L2 residual <= tol or max_sweeps.
+ *              point red-black SOR at omega until the relative L2 residual <= tol or max_sweeps.
+ *   RB_LINE:   the same with red-black radial-line SOR; max_sweeps counts line sweeps.
+ *   Both to-residual kinds add an exact correction of the column-uniform mode every few sweeps,
+ *   return ATURAN_NOT_CONVERGED at the cap, and compute in FP64, or in the mixed form as FP32
+ *   correction solves inside FP64 iterative refinement.
  * sweeps_done and resid (relative L2 residual at exit; RB_SOR only, else 0) may be NULL. */
 int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
                     int* sweeps_done, double* resid);

@@ -55,6 +55,7 @@ class Oracle:
             ("oracle_pressure_rb", [P, vp, ctypes.c_int], ctypes.c_int),
             ("oracle_pressure_sor", [P, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                      ctypes.c_int, vp, vp], ctypes.c_int),
+            ("oracle_pressure_line", [P, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, vp, vp], ctypes.c_int),
             ("oracle_pressure_source", [P, vp, vp], ctypes.c_int),
             ("oracle_pressure_source_compat", [P, vp, vp], ctypes.c_int),
             ("oracle_pressure_residual", [P, vp, vp], ctypes.c_double),
@@ -104,6 +105,13 @@ class Oracle:
         rc = self.L.oracle_pressure_sor(self._p(p), field_ptrs(state), float(omega), int(max_sweeps),
                                         float(tol), int(check_every), ctypes.addressof(s),
                                         ctypes.addressof(r))
+        return rc, s.value, r.value
+
+    def pressure_line(self, p, state, omega, max_iter, tol):
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        rc = self.L.oracle_pressure_line(self._p(p), field_ptrs(state), float(omega), int(max_iter), float(tol),
+                                         ctypes.addressof(s), ctypes.addressof(r))
         return rc, s.value, r.value
 
     def pressure_source(self, p, state):

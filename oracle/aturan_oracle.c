@@ -1020,6 +1020,86 @@ static void column_correction(const aturan_params* p, const double* rad, const d
     free(R); free(Ac); free(As);
 }
 
+/* One colour of red-black LINE relaxation of the folded operator: columns (j,k) with
+ * (j + k) & 1 == colour are solved exactly in r (Thomas; the radial ends folded into the first and
+ * last rows as PressureSolver.h:547-550 does), their horizontal neighbours -- the other colour, or
+ * the column itself through the theta fold -- held at their current values, then over-relaxed:
+ * p += omega (p_line - p). The reference's PRESS_LINE (:497-570) on the folded operator. */
+static void line_colour(const aturan_params* p, const double* rad, const double* st, double* P,
+                        const double* src, int colour, double omega){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int n = im - 2;
+    #pragma omp parallel
+    {
+        double* aa = (double*)malloc(sizeof(double) * n);
+        double* bb = (double*)malloc(sizeof(double) * n);
+        double* cc = (double*)malloc(sizeof(double) * n);
+        double* dd = (double*)malloc(sizeof(double) * n);
+        #pragma omp for collapse(2) schedule(static)
+        for(int j = 1; j < jm-1; j++){
+            for(int k = 0; k < km-1; k++){
+                if(((j + k) & 1) != colour) continue;
+                const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+                for(int i = 1; i < im-1; i++){
+                    pweights_t w; press_weights(p, rad, st, i, j, &w);
+                    double d = w.den;
+                    double hj;
+                    const double ajm = (j == 1)    ? (d -= C43 * w.num2, -C13 * P[IDX(i,j+1,k)]) : P[IDX(i,j-1,k)];
+                    const double ajp = (j == jm-2) ? (d -= C43 * w.num2, -C13 * P[IDX(i,j-1,k)]) : P[IDX(i,j+1,k)];
+                    hj = (ajp + ajm) * w.num2 + (P[IDX(i,j,ke)] + P[IDX(i,j,kw)]) * w.num3;
+                    const int q = i - 1;
+                    aa[q] = -w.num1; cc[q] = -w.num1; bb[q] = d;
+                    dd[q] = hj - src[IDX(i,j,k)];
+                }
+                /* radial folds: p0 = c43 p1 - c13 p2 (row 1), p_{im-1} = c43 p_{im-2} - c13 p_{im-3} */
+                bb[0] += aa[0] * C43; cc[0] -= aa[0] * C13; aa[0] = 0.0;
+                bb[n-1] += cc[n-1] * C43; aa[n-1] -= cc[n-1] * C13; cc[n-1] = 0.0;
+                double cprev = cc[0] / bb[0];
+                dd[0] = dd[0] / bb[0];
+                cc[0] = cprev;
+                for(int q = 1; q < n; q++){
+                    const double dn = bb[q] - aa[q] * cc[q-1];
+                    cc[q] = cc[q] / dn;
+                    dd[q] = (dd[q] - aa[q] * dd[q-1]) / dn;
+                }
+                double x = dd[n-1];
+                P[IDX(n, j, k)] += omega * (x - P[IDX(n, j, k)]);
+                for(int q = n - 2; q >= 0; q--){
+                    x = dd[q] - cc[q] * x;
+                    P[IDX(q+1, j, k)] += omega * (x - P[IDX(q+1, j, k)]);
+                }
+            }
+        }
+        free(aa); free(bb); free(cc); free(dd);
+    }
+}
+
+int oracle_pressure_line(const aturan_params* p, double* const* f, double omega, int max_iter,
+                         double tol, int* iters_done, double* resid){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    double* src = (double*)malloc(sizeof(double) * (size_t)im * jm * km);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    oracle_pressure_source_compat(p, f, src);
+    double* P = f[ATURAN_P_DYN];
+    int s = 0; double r = folded_residual(p, rad, st, P, src);
+    while(s < max_iter && !(r <= tol)){
+        column_correction(p, rad, st, P, src);
+        line_colour(p, rad, st, P, src, 0, omega);
+        line_colour(p, rad, st, P, src, 1, omega);
+        s++;
+        r = folded_residual(p, rad, st, P, src);
+    }
+    p_dyn_bcs(p, P);
+    if(iters_done) *iters_done = s;
+    if(resid) *resid = r;
+    free(rad); free(the); free(st); free(src);
+    return r <= tol ? 0 : 1;
+}
+
 /* Red-black SOR on the shared solver's equation to a relative residual, with the column-uniform
  * correction before every block of check_every sweeps (no reference oracle exists for a
  * converged solve: the reference sweeps a fixed count at omega = 1). The GPU's RB_SOR runs the
@@ -1275,7 +1355,8 @@ int oracle_step(const aturan_params* p, double* const* f, int press_kind, double
                 int max_sweeps, double tol, double* ref_out){
     if(press_kind == ATURAN_PRESS_GS_LEX) oracle_pressure_gs(p, f);
     else if(press_kind == ATURAN_PRESS_RB_SHARED) oracle_pressure_rb(p, f, max_sweeps);
-    else { int s; double r; oracle_pressure_sor(p, f, omega, max_sweeps, tol, 1, &s, &r); }
+    else if(press_kind == ATURAN_PRESS_RB_LINE) { int s; double r; oracle_pressure_line(p, f, omega, max_sweeps, tol, &s, &r); }
+    else { int s; double r; oracle_pressure_sor(p, f, omega, max_sweeps, tol, 16, &s, &r); }
     for(int g = 0; g < 4; g++) oracle_satadj(p, f, g, NULL, NULL);
     oracle_sync_ncopies(p, f);
     return oracle_rk4(p, f, ref_out);

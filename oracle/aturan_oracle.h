@@ -33,6 +33,8 @@ int oracle_pressure_gs(const aturan_params* p, double* const* f);
 int oracle_pressure_rb(const aturan_params* p, double* const* f, int sweeps);
 int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, int max_sweeps,
                         double tol, int check_every, int* sweeps_done, double* resid);
+int oracle_pressure_line(const aturan_params* p, double* const* f, double omega, int max_iter,
+                         double tol, int* iters_done, double* resid);
 double oracle_pressure_residual(const aturan_params* p, double* const* f, const double* src);
 int oracle_pressure_source(const aturan_params* p, double* const* f, double* src);
 int oracle_pressure_source_compat(const aturan_params* p, double* const* f, double* src);

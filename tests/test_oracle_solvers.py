@@ -1,0 +1,69 @@
+"""The oracle's to-residual Poisson solvers (point and line red-black SOR with the column-uniform
+correction). The reference has no converged solve to compare with (it sweeps a fixed count), so
+these are pinned to the reference through its own sweep: a converged solution must be a fixed
+point of PressureSolver<cUranusModel>::run's red-black sweep (PressureSolver.h:318-495), which the
+oracle reproduces bit for bit (tests/test_golden.py, case pressure_rb3)."""
+import numpy as np
+import pytest
+
+from aturan_b200 import params as P, state as S
+
+
+def case(shape=(21, 37, 73), seed=40):
+    p = P.default_params(*shape)
+    st = S.synthetic_state(p, seed=seed)
+    st["p_dyn"][:] = 0.0
+    return p, st
+
+
+def interior_centered(a):
+    x = a[1:-1, 1:-1, :-1]
+    return x - x.mean()
+
+
+def test_point_and_line_reach_tolerance_and_agree(oracle_lib):
+    p, st = case()
+    a, b = S.copy_state(st), S.copy_state(st)
+    rc, sweeps, res = oracle_lib.pressure_sor(p, a, 1.8, 3000, 1e-10, 16)
+    assert rc == 0 and res <= 1e-10 and sweeps < 3000
+    rc, its, res = oracle_lib.pressure_line(p, b, 1.0, 200, 1e-10)
+    assert rc == 0 and res <= 1e-10 and its <= 10, its
+    # the all-Neumann equation fixes p up to a constant: compare without it
+    da, db = interior_centered(a["p_dyn"]), interior_centered(b["p_dyn"])
+    assert np.abs(da - db).max() <= 1e-8 * np.abs(db).max()
+
+
+def test_converged_solution_is_a_fixed_point_of_the_reference_sweep(oracle_lib):
+    p, st = case(seed=41)
+    rc, its, res = oracle_lib.pressure_line(p, st, 1.0, 200, 1e-11)
+    assert rc == 0
+    moved = S.copy_state(st)
+    oracle_lib.pressure_rb(p, moved, 1)
+    # what is left is the compatibility shift of the source (a few 1e-5 of it) divided by the
+    # operator's diagonal
+    scale = np.abs(st["p_dyn"]).max()
+    assert np.abs(moved["p_dyn"] - st["p_dyn"]).max() <= 1e-7 * scale
+
+
+def test_cap_reports_not_converged(oracle_lib):
+    p, st = case(seed=42)
+    rc, its, res = oracle_lib.pressure_line(p, st, 1.0, 1, 1e-14)
+    assert rc == 1 and its == 1 and res > 1e-14
+    p, st = case(seed=42)
+    rc, sweeps, res = oracle_lib.pressure_sor(p, st, 1.8, 5, 1e-14, 16)
+    assert rc == 1 and sweeps == 5
+
+
+@pytest.mark.parametrize("kind", [P.PRESS_RB_SOR, P.PRESS_RB_LINE])
+def test_step_with_converged_solvers_agree(oracle_lib, kind):
+    """The whole step with either solver (their solutions differ only by the constant, which no
+    gradient sees)."""
+    p, st = case(shape=(12, 20, 33), seed=43)
+    ref = S.copy_state(st)
+    oracle_lib.step(p, ref, P.PRESS_RB_LINE, 1.0, 100, 1e-11)
+    got = S.copy_state(st)
+    omega = 1.8 if kind == P.PRESS_RB_SOR else 1.0
+    oracle_lib.step(p, got, kind, omega, 5000, 1e-11)
+    for n in ("t", "u", "v", "w"):
+        scale = np.abs(ref[n]).max()
+        assert np.abs(got[n] - ref[n]).max() <= 1e-9 * scale, n
