@@ -39,6 +39,8 @@ SIGNATURES = {
     "aturan_download_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "aturan_download_buoy_ref": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_rk4_step": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_tape": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_rk4_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_pressure": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                          ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_satadj": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -54,7 +56,7 @@ SIGNATURES = {
 
 STATIC_MAX_IM, STATIC_MAX_JM = 512, 4096
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint"]
 
 _LIB = None
 
@@ -158,6 +160,16 @@ class Context:
     # ---- the path ----
     def rk4_step(self):
         self._check(self.L.aturan_rk4_step(self.h), "rk4_step")
+
+    def tape(self, on=True):
+        """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""
+        self._check(self.L.aturan_tape(self.h, 1 if on else 0), "tape")
+
+    def rk4_adjoint(self, ybar_ptrs, xbar_ptrs):
+        """aturan_rk4_adjoint on device pointers (t, u, v, w order) to contiguous FP64 arrays."""
+        yb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
+        xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
+        self._check(self.L.aturan_rk4_adjoint(self.h, yb, xb), "rk4_adjoint")
 
     def pressure(self, kind=0, omega=1.0, max_sweeps=1, tol=0.0):
         s = ctypes.c_int()

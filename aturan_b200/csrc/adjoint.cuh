@@ -1,0 +1,316 @@
+// Hand-written adjoint of one RK4 step of the dry dynamics (t, u, v, w), FP64.
+//
+// Forward (rk4.cuh, RungeKutta_Uran_Turb.cpp:18-403): level means ref(T), p_hydro = H(T, v, w, ref),
+// then four stages k_s = RHS(X_s, p_hydro) with X_0 = y, X_{s+1} = y + c_s k_s on the interior
+// (boundary rows of every X_s are y's), and y' = y + dt/6 sum_s w_s k_s, T' clamped. The inputs y
+// are the state and its start-of-step copies together; p_dyn, p_stat, the forcing and every
+// other field are held fixed (the tendencies of t, u, v, w do not read the scalars).
+//
+// Reverse: with g = ybar' masked by the clamp, ybar = g, kbar_3 = dt/6 w_3 g, and for s = 3..0
+//   Xbar_s = J_s^T kbar_s (+ p_hydro part), ybar += Xbar_s, kbar_{s-1} = dt/6 w_{s-1} g + c_{s-1} Xbar_s,
+// then the hydrostatic integral's and the level means' adjoints add into ybar (T, v, w).
+//
+// J_s^T is a scatter of every interior cell's local partial derivatives onto its 7-point stencil.
+// It runs as gather, without atomics and in a fixed order: adj_local_kernel writes, per cell and
+// per field, the seven contributions the cell sends to its stencil points (ADJ_SLOTS arrays), and
+// adj_gather_kernel sums, per cell, the seven it receives from the cells whose stencils contain it.
+// The partial derivatives are those of the forward's formulas (RHS_Uran_Turb.cpp:92-788), derived
+// term by term; cp(T) is the piecewise-linear table, differentiated within its interval (a kink
+// convention: the derivative of the interval the value falls in).
+#pragma once
+#include "common.cuh"
+#include "rk4.cuh"
+
+namespace aturan {
+
+constexpr int ADJ_NF = 4;                          // t, u, v, w (state fields 0..3)
+constexpr int ADJ_SLOTS = 7 * ADJ_NF + 4;          // per field rp, rm, tp, tm, pe, pw, c; p_hydro tp, tm, pe, pw
+
+struct AdjArgs {
+    Grid g;
+    const double* X;            // stage input, field q (0..3) at X + q * fstride
+    const double* X0;           // the step's input (boundary rows of every stage input)
+    const double* kbar;         // adjoint of the stage's tendencies, field q at kbar + q * fstride
+    const double* pdyn;
+    const double* forc;         // forcing group (nue at offset 0)
+    const GeoIJ<double>* geo;
+    const double* cp_tab;
+    RhsConst<double> k;
+    double* slot;               // ADJ_SLOTS fields
+};
+
+// cp_lapse (rk4.cuh) and its derivative in T (K), the table's slope inside its 0.5 K interval.
+__device__ __forceinline__ void cp_lapse_d(const RhsConst<double>& k, const double* tab, double T,
+                                           double* cp, double* dcp){
+    double ch, dch;
+    if(k.cp_mode <= 0){ ch = k.cp_h2_const; dch = 0.0; }
+    else {
+        const double Tc = T < 5.0 ? 5.0 : T;
+        const double x = ((Tc > 1500.0 ? 1500.0 : Tc) - 5.0) / 0.5;
+        int i = (int)x; if(i > CP_TABLE_N - 2) i = CP_TABLE_N - 2;
+        const double f = x - (double)i;
+        const double a = __ldg(tab + i), b = __ldg(tab + i + 1);
+        ch = a + f * (b - a);
+        dch = (T > 5.0 && T < 1500.0) ? (b - a) / 0.5 : 0.0;
+    }
+    if(k.cp_gas){ *cp = (k.cp_rh2 * ch + k.cp_he_term + k.cp_ch4_term) / k.cp_rsum; *dcp = k.cp_rh2 * dch / k.cp_rsum; }
+    else        { *cp = k.cp_mix + k.cp_rh2 * (ch - k.cp_h2_const);               *dcp = k.cp_rh2 * dch; }
+}
+
+// Adjoints of one field's six differences -> the seven stencil values it was formed from.
+struct G6 { double d1r, d2r, d1t, d2t, d1p, d2p; };
+
+__device__ __forceinline__ void put7(double* slot, size_t fs, size_t o, int field, const G6& g, double dc,
+                                     const RhsConst<double>& k){
+    double* S = slot + (size_t)field * 7 * fs + o;
+    S[0 * fs] =  g.d1r * k.inv_2dr   + g.d2r * k.inv_dr2;      // to (i+1)
+    S[1 * fs] = -g.d1r * k.inv_2dr   + g.d2r * k.inv_dr2;      // to (i-1)
+    S[2 * fs] =  g.d1t * k.inv_2dthe + g.d2t * k.inv_dthe2;    // to (j+1)
+    S[3 * fs] = -g.d1t * k.inv_2dthe + g.d2t * k.inv_dthe2;    // to (j-1)
+    S[4 * fs] =  g.d1p * k.inv_2dphi + g.d2p * k.inv_dphi2;    // to (k+1)
+    S[5 * fs] = -g.d1p * k.inv_2dphi + g.d2p * k.inv_dphi2;    // to (k-1)
+    S[6 * fs] = dc - 2.0 * (g.d2r * k.inv_dr2 + g.d2t * k.inv_dthe2 + g.d2p * k.inv_dphi2);
+}
+
+// Per interior cell: the local partial derivatives of rhs_t, rhs_u, rhs_v, rhs_w times the
+// tendencies' adjoints, as the contributions to each stencil point (RHS_Uran_Turb.cpp:92-788).
+__global__ void __launch_bounds__(128) adj_local_kernel(const AdjArgs a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<double>& K = a.k;
+    const GeoIJ<double> geo = a.geo[i * g.jm + j];
+    Nbr<double> nb;
+    nb.fs  = g.fstride;
+    nb.o   = gidx(g, i, j, k);
+    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
+    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
+    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
+    nb.oke = nb.o - k + phi_wrap(k + 1, g.km);
+    nb.X   = a.X;
+    nb.xim = (i == 1) ? a.X0 : a.X;
+    nb.xip = (i == g.im - 2) ? a.X0 : a.X;
+    nb.xjm = (j == 1) ? a.X0 : a.X;
+    nb.xjp = (j == g.jm - 2) ? a.X0 : a.X;
+    const size_t o = nb.o, fs = g.fstride;
+
+    const D6<double> T = diff6(K, load7<double, double>(nb, 0));
+    const D6<double> U = diff6(K, load7<double, double>(nb, 1));
+    const D6<double> V = diff6(K, load7<double, double>(nb, 2));
+    const D6<double> W = diff6(K, load7<double, double>(nb, 3));
+    const double* P = a.pdyn;
+    const double dpdr   = (ld(P + nb.oip) - ld(P + nb.oim)) * K.inv_2dr;
+    const double dpdthe = (ld(P + nb.ojp) - ld(P + nb.ojm)) * K.inv_2dthe;
+    const double dpdphi = (ld(P + nb.oke) - ld(P + nb.okw)) * K.inv_2dphi;
+    const double nue_c = ld(a.forc + o);
+    const double nue_t = (K.turb_coupling != 0.0 && isfinite(nue_c)) ? K.turb_coupling * cmax(0.0, nue_c) : 0.0;
+    const double nue_t_s = nue_t / 0.9;
+    const double at = a.kbar[0 * fs + o], au = a.kbar[1 * fs + o];
+    const double av = a.kbar[2 * fs + o], aw = a.kbar[3 * fs + o];
+
+    const double u = U.c, v = V.c, w = W.c;
+    const double inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rs = geo.inv_rmsinthe;
+    const double inv_rm2s = geo.inv_rm2sinthe, inv_rm2s2 = geo.inv_rm2sinthe2, cir = geo.costhe_inv_rm2sinthe;
+    const double costhe = geo.costhe, cot = geo.cotanthe, tir = geo.two_inv_rm;
+    const double D = 1.0 / K.re_eff + nue_t, Dt = 1.0 / K.re_pr + nue_t_s;
+
+    // pressure work and its cp(T) factor
+    double cpf = 1.0, dcpf = 0.0;
+    if(K.cp_dyn && T.c > 0.0){
+        double cp, dcp;
+        cp_lapse_d(K, a.cp_tab, T.c * K.t_ref, &cp, &dcp);
+        cpf = K.cp_mix / cp;
+        dcpf = -K.cp_mix / (cp * cp) * dcp * K.t_ref;
+    }
+    const double P0 = K.ce_sp * (u * dpdr + v * inv_rm * dpdthe + w * inv_rs * dpdphi);
+
+    // direct (centre) partials of the four tendencies
+    const double du = au * (-U.d1r + 2.0 * inv_rm2 * D - geo.sponge)
+                    + av * (-V.d1r - v * inv_rm)
+                    + aw * (-W.d1r - w * inv_rm - K.cor_sc * K.p2om * geo.sinthe_bf)
+                    + at * (K.ce_sp * dpdr * cpf - T.d1r);
+    const double dv = au * (-inv_rm * U.d1t)
+                    + av * (-inv_rm * V.d1t - u * inv_rm - geo.v_metric * D)
+                    + aw * (-inv_rm * W.d1t - w * cot * inv_rm - K.cor_sc * K.p2om * costhe)
+                    + at * (K.ce_sp * inv_rm * dpdthe * cpf - inv_rm * T.d1t);
+    const double dw = au * (-inv_rs * U.d1p - K.cor_rad_f * K.m2om * geo.sinthe_bf)
+                    + av * (-inv_rs * V.d1p + 2.0 * w * cot * inv_rm - K.cor_sc * K.m2om * costhe)
+                    + aw * (-inv_rs * W.d1p - (u + v * cot) * inv_rm - geo.v_metric * D)
+                    + at * (K.ce_sp * inv_rs * dpdphi * cpf - inv_rs * T.d1p);
+    const double dT = at * P0 * dcpf;
+
+    G6 gT, gU, gV, gW;
+    gT.d1r = at * (-u + tir * Dt);            gT.d2r = at * Dt;
+    gT.d1t = at * (-v * inv_rm + cir * Dt);   gT.d2t = at * inv_rm2 * Dt;
+    gT.d1p = at * (-w * inv_rs);              gT.d2p = at * inv_rm2s2 * Dt;
+
+    gU.d1r = au * (-u + 4.0 * inv_rm * D);    gU.d2r = au * D;
+    gU.d1t = au * (-v * inv_rm + cir * D) + av * (2.0 * inv_rm2 * D);
+    gU.d2t = au * inv_rm2 * D;
+    gU.d1p = au * (-w * inv_rs) + aw * (2.0 * inv_rm2s * D);
+    gU.d2p = au * inv_rm2s2 * D;
+
+    gV.d1r = av * (-u + tir * D);             gV.d2r = av * D;
+    gV.d1t = av * (-v * inv_rm + cir * D);    gV.d2t = av * inv_rm2 * D;
+    gV.d1p = av * (-w * inv_rs) + aw * (2.0 * costhe * inv_rm2s2 * D);
+    gV.d2p = av * inv_rm2s2 * D;
+
+    gW.d1r = aw * (-u + tir * D);             gW.d2r = aw * D;
+    gW.d1t = aw * (-v * inv_rm + cir * D);    gW.d2t = aw * inv_rm2 * D;
+    gW.d1p = aw * (-w * inv_rs) - av * (2.0 * costhe * inv_rm2s2 * D);
+    gW.d2p = aw * inv_rm2s2 * D;
+
+    put7(a.slot, fs, o, 0, gT, dT, K);
+    put7(a.slot, fs, o, 1, gU, du, K);
+    put7(a.slot, fs, o, 2, gV, dv, K);
+    put7(a.slot, fs, o, 3, gW, dw, K);
+    // p_hydro: rhs_v -= (ph[j+1] - ph[j-1]) inv_2dthe inv_rm, rhs_w -= (ph[k+1] - ph[k-1]) inv_2dphi inv_rs
+    double* S = a.slot + (size_t)7 * ADJ_NF * fs + o;
+    S[0 * fs] = -av * K.inv_2dthe * inv_rm;   // to (j+1)
+    S[1 * fs] =  av * K.inv_2dthe * inv_rm;   // to (j-1)
+    S[2 * fs] = -aw * K.inv_2dphi * inv_rs;   // to (k+1)
+    S[3 * fs] =  aw * K.inv_2dphi * inv_rs;   // to (k-1)
+}
+
+// Per cell (every row, every meridian; the seam copy k = km-1 is read by no stencil and receives
+// nothing): the sum of what the cells whose stencils contain it sent, in a fixed order. Adds the
+// result into ybar and phbar; for s > 0 also forms the previous stage's kbar on the interior.
+__global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* slot, double* ybar, double* phbar,
+                                                         const double* g0, double* kbar, double w_prev,
+                                                         double c_prev, int has_prev){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    if(k >= g.km - 1) return;
+    const size_t fs = g.fstride, si = (size_t)g.jm * g.kp, sj = g.kp;
+    const size_t o = gidx(g, i, j, k);
+    const size_t okw = o - k + phi_wrap(k - 1, g.km), oke = o - k + phi_wrap(k + 1, g.km);
+    const bool interior = i >= 1 && i <= g.im - 2 && j >= 1 && j <= g.jm - 2;
+#pragma unroll
+    for(int q = 0; q < ADJ_NF; q++){
+        const double* S = slot + (size_t)q * 7 * fs;
+        double x = S[6 * fs + o];
+        if(i >= 1)        x += S[0 * fs + o - si];
+        if(i <= g.im - 2) x += S[1 * fs + o + si];
+        if(j >= 1)        x += S[2 * fs + o - sj];
+        if(j <= g.jm - 2) x += S[3 * fs + o + sj];
+        x += S[4 * fs + okw];
+        x += S[5 * fs + oke];
+        ybar[q * fs + o] += x;
+        if(has_prev && interior) kbar[q * fs + o] = w_prev * g0[q * fs + o] + c_prev * x;
+    }
+    const double* S = slot + (size_t)7 * ADJ_NF * fs;
+    double h = 0.0;
+    if(j >= 1)        h += S[0 * fs + o - sj];
+    if(j <= g.jm - 2) h += S[1 * fs + o + sj];
+    h += S[2 * fs + okw];
+    h += S[3 * fs + oke];
+    phbar[o] += h;
+}
+
+// The final update's adjoint: g = ybar' (times 0 where T' was clamped), ybar = g, kbar_3 =
+// dt/6 w_3 g on the interior. ybar_in is the caller's adjoint of the step's output.
+__global__ void adj_init_kernel(Grid g, const double* ybar_in, const double* t_out, double t_min, double t_max,
+                                double w3, double* g0, double* ybar, double* kbar, double* phbar){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    if(k >= g.km) return;
+    const size_t fs = g.fstride;
+    const size_t o = gidx(g, i, j, k);
+    const bool interior = i >= 1 && i <= g.im - 2 && j >= 1 && j <= g.jm - 2 && k <= g.km - 2;
+#pragma unroll
+    for(int q = 0; q < ADJ_NF; q++){
+        double v = ybar_in[q * fs + o];
+        if(q == 0 && interior && !(t_out[o] > t_min && t_out[o] < t_max)) v = 0.0;
+        g0[q * fs + o] = interior ? v : 0.0;
+        ybar[q * fs + o] = v;
+        kbar[q * fs + o] = interior ? w3 * v : 0.0;
+    }
+    phbar[o] = 0.0;
+}
+
+// Hydrostatic integral's adjoint, per column (RungeKutta_Uran_Turb.cpp:62-177): p_hydro(i) =
+// sum_{n=1..i} (F(n-1) + F(n)) dr / 2 + const, F = cB buoy + met (cB = 1 - 1/follow_tau when the
+// follow filter advances, else 1). Fbar(m) = dr/2 (S(m+1) + [m >= 1] S(m)), S the suffix sums of
+// phbar. Adds the met part into vbar, wbar and the local buoy part into Tbar; leaves, per cell,
+// the contribution to its level mean's adjoint in rbar.
+__global__ void __launch_bounds__(256) adj_hydro_kernel(Grid g, const double* t, const double* ps, const double* v,
+                                                        const double* w, const double* ref, const double* rm_i,
+                                                        const double* cor_j, const double* phbar, double* ybar,
+                                                        double* rbar, HydroConst h){
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= g.jm * g.km) return;
+    const int j = c / g.km, k = c - j * g.km;
+    const size_t fs = g.fstride;
+    const double cB = h.follow_on ? 1.0 - 1.0 / h.follow_tau : 1.0;
+    const double cor = cor_j[j];
+    double S_next = 0.0;                           // S(m+1)
+    for(int m = g.im - 1; m >= 0; m--){
+        const size_t o = gidx(g, m, j, k);
+        const double Sm = S_next + phbar[o];
+        const double Fb = 0.5 * h.dr * (S_next + (m >= 1 ? Sm : 0.0));
+        S_next = Sm;
+        const double vv = v[o], ww = w[o];
+        ybar[2 * fs + o] += Fb * 2.0 * vv / rm_i[m];
+        ybar[3 * fs + o] += Fb * (2.0 * ww / rm_i[m] + cor);
+        const double T = t[o];
+        double rb = 0.0;
+        if(T > 0.0){
+            const double b = h.g * ps[o] / (h.rR * T * h.t_ref);
+            const double f = h.m_nd_rel_b * (b - ref[m]) / ref[m];
+            if(isfinite(f)){
+                const double FbB = cB * Fb;
+                ybar[o] += FbB * h.m_nd_rel_b / ref[m] * (-b / T);
+                rb = FbB * (-h.m_nd_rel_b * b / (ref[m] * ref[m]));
+            }
+        }
+        rbar[o] = rb;
+    }
+}
+
+// Level mean's adjoint (RungeKutta_Uran_Turb.cpp:18-37): per level, Rbar = sum rbar and the
+// weight sum W over the valid cells, in a fixed tree order; then per valid cell
+// Tbar += Rbar / W * wsin_j * db/dT, db/dT = -b / T.
+__global__ void __launch_bounds__(256) adj_level_sum_kernel(Grid g, const double* t, const double* ps,
+                                                            const double* wsin, const double* rbar,
+                                                            HydroConst h, double* lev){
+    const int m = blockIdx.x;
+    double s = 0.0, ws = 0.0;
+    for(int c = threadIdx.x; c < g.jm * g.km; c += blockDim.x){
+        const int j = c / g.km, k = c - j * g.km;
+        const size_t o = gidx(g, m, j, k);
+        const double T = t[o];
+        if(!(T > 0.0)) continue;
+        const double b = h.g * ps[o] / (h.rR * T * h.t_ref);
+        if(!isfinite(b)) continue;
+        s += rbar[o];
+        ws += wsin[j];
+    }
+    __shared__ double ss[256], sw[256];
+    ss[threadIdx.x] = s; sw[threadIdx.x] = ws;
+    __syncthreads();
+    for(int st = 128; st > 0; st >>= 1){
+        if(threadIdx.x < st){ ss[threadIdx.x] += ss[threadIdx.x + st]; sw[threadIdx.x] += sw[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0){ lev[2 * m] = ss[0]; lev[2 * m + 1] = sw[0]; }
+}
+
+__global__ void adj_level_apply_kernel(Grid g, const double* t, const double* ps, const double* wsin,
+                                       const double* lev, HydroConst h, double* ybar){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int m = blockIdx.z;
+    if(k >= g.km) return;
+    const size_t o = gidx(g, m, j, k);
+    const double T = t[o];
+    if(!(T > 0.0) || !(lev[2 * m + 1] > 0.0)) return;
+    const double b = h.g * ps[o] / (h.rR * T * h.t_ref);
+    if(!isfinite(b)) return;
+    ybar[o] += lev[2 * m] / lev[2 * m + 1] * wsin[j] * (-b / T);
+}
+
+}  // namespace aturan

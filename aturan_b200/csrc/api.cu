@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "aturan_b200.h"
@@ -20,6 +21,7 @@
 #include "satadj.cuh"
 #include "pressure.cuh"
 #include "sor.cuh"
+#include "adjoint.cuh"
 
 using namespace aturan;
 
@@ -62,8 +64,13 @@ struct aturan_ctx {
     double *llu_a, *llu_cf, *llu_idn;            // per-(i,j) radial-line factorisations
     float *r32, *e32;
     int sor_nblk;
-    int sor_pb;                // tridiagonal problems per block of the column correction
+    int sor_pm;                // Fourier modes per block of the column correction's tridiagonal solves
     std::vector<double> host_part;
+    // adjoint tape (aturan_tape): stage inputs of t, u, v, w, the step's T output and level means,
+    // and the adjoint's work arrays; null when the tape is off
+    double* tape;
+    bool tape_valid;           // a taped RK4 step has run since the tape was switched on
+    double *tX, *tTout, *tref, *aslot, *aybar, *akbar, *ag0, *aphbar, *arbar, *alev;
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -258,6 +265,9 @@ void* field_ptr(aturan_ctx* c, int id, bool* is64){
 
 template <typename S> S* grp(void* base, int q, size_t fs){ return reinterpret_cast<S*>(base) + (size_t)q * fs; }
 
+template <typename S>
+bool taping(const aturan_ctx* ctx){ return std::is_same<S, double>::value && ctx->tape != nullptr; }
+
 template <typename S, typename C>
 int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     const Grid g = ctx->g;
@@ -269,6 +279,10 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     launch_buoy(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), ctx->wsin, ctx->hc,
                 ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, ctx->st);
     CK_LAUNCH("buoyancy reference level");
+    if(taping<S>(ctx)){
+        CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->tX, state, ADJ_NF * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    }
     launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
                  grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
                  ctx->phydro, ctx->hc, 1, ctx->st);
@@ -295,10 +309,18 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
         a.wgt  = (C)((stage == 0 || stage == 3) ? 1.0 : 2.0);
         a.X = stage == 0 ? state : (stage == 1 ? y0 : (stage == 2 ? y1 : y0));
         a.Y = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : state));
+        {
         Region reg(ctx, ATURAN_K_RK_STAGE, 1);
         launch_stage(a, ctx->st);
         CK_LAUNCH("RK4 stage");
+        }
+        if(taping<S>(ctx)){      // the next stage's input of t, u, v, w; after stage 3 the new T
+            if(stage < 3) CK(cudaMemcpyAsync(ctx->tX + (size_t)(stage + 1) * ADJ_NF * fs, a.Y, ADJ_NF * fs * 8,
+                                             cudaMemcpyDeviceToDevice, ctx->st));
+            else CK(cudaMemcpyAsync(ctx->tTout, state, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        }
     }
+    if(taping<S>(ctx)) ctx->tape_valid = true;
     return ATURAN_OK;
 }
 
@@ -419,9 +441,9 @@ int sor_correct(aturan_ctx* ctx, T* P){
     sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_stT, c.NM + 1, 1}, none, none,
                                             1.0 / c.A2y, ctx->sor_As, 1, c.J);
     ModeLU lu{ctx->mlu_a, ctx->mlu_cf, ctx->mlu_idn};
-    const int pb = ctx->sor_pb;
-    sor_tridiag_kernel<<<(2 * (c.NM + 1) + pb - 1) / pb, 128, (size_t)c.J * (pb + 1) * sizeof(double), ctx->st>>>(
-        c, lu, ctx->sor_Ac, ctx->sor_As, pb);
+    const int pm = ctx->sor_pm;
+    sor_tridiag_kernel<<<(c.NM + 1 + pm - 1) / pm, 128, (size_t)8 * c.J * (5 * pm + 4), ctx->st>>>(
+        c, lu, ctx->sor_Ac, ctx->sor_As, pm);
     const dim3 gi((c.N + 31) / 32, (c.J + 31) / 32);
     sor_gemm_kernel<<<gi, 256, 0, ctx->st>>>(c.J, c.N, c.NM + 1, MatRef{ctx->sor_Ac, 1, c.J}, MatRef{ctx->sor_ct, c.N, 1},
                                             MatRef{ctx->sor_As, 1, c.J}, MatRef{ctx->sor_st, c.N, 1},
@@ -451,13 +473,17 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     const size_t fs = g.fstride;
     S* proj = reinterpret_cast<S*>(ctx->proj);
     if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
-    if(ctx->sor_pb < 1) return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 3000");
+    if(8 * ctx->sorc.J * (5 * ctx->sor_pm + 4) > 227 * 1024)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 2900");
     if(line && (g.im - 2) * 32 * (int)sizeof(double) > 49152)
         return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 194");
     if(max_sweeps < 1) max_sweeps = 1;
-    // sweeps between column-uniform corrections and residual checks: point SOR needs ~200 sweeps and
-    // loses ~6 % of its rate with a correction every 16 (oracle measurement); line SOR needs ~7
-    const int every = line ? 1 : 16;
+    // Sweeps between residual checks and between column-uniform corrections. Point SOR needs ~200
+    // sweeps and loses ~6 % of its rate with a correction every 16; line SOR needs 5-7 iterations
+    // and converges at the same rate with one correction per 8 as with one per iteration (the
+    // first correction removes the column-uniform error; oracle measurements at 41x181x361).
+    const int check_every = line ? 1 : 16;
+    const int every = line ? 8 : 16;
     long nl = 0;
     Region reg(ctx, ATURAN_K_RB, 0);
     launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
@@ -475,10 +501,10 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     if(!ctx->mixed){
         int rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
-            rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 4;
-            for(int n = 0; n < every && s < max_sweeps; n++, s++){ sor_sweep<double>(ctx, P, src, omega, line); nl += 2; }
+            if(s % every == 0){ rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 5; }
+            for(int n = 0; n < check_every && s < max_sweeps; n++, s++){ sor_sweep<double>(ctx, P, src, omega, line); nl += 2; }
             CK_LAUNCH("SOR sweeps");
-            rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
+            rc = sor_residual<double>(ctx, P, src, s % every == 0, &r, nullptr); if(rc) return rc; nl++;
         }
     } else {
         // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
@@ -492,7 +518,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
                 if(n % every == 0){
                     rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc;
                     rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
-                    nl += 5;
+                    nl += 6;
                 }
                 sor_sweep<float>(ctx, ctx->e32, ctx->r32, omega, line);
                 nl += 2;
@@ -590,7 +616,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
     ctx->sor_nblk = ((sN + 31) / 32) * sJ;
-    ctx->sor_pb = std::min(32, 49152 / (8 * sJ) - 1);
+    ctx->sor_pm = std::max(1, std::min(16, (200 * 1024 / (8 * sJ) - 4) / 5));
     for(int n = 0; n < 4; n++) add((size_t)(sNM + 1) * sN * 8);        // ct, st, ctT, stT
     add((size_t)sJ * sN * 8); add((size_t)(sNM + 1) * sJ * 8); add((size_t)(sNM + 1) * sJ * 8);
     add((size_t)2 * ctx->sor_nblk * 8); add((size_t)sJ * sN * 8);
@@ -813,6 +839,15 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
         A2y += ((i == 1 || i == g.im - 2) ? 1.5 : 1.0) / (rm * rm);
     }
     ctx->sorc.J = sJ; ctx->sorc.N = sN; ctx->sorc.NM = sNM; ctx->sorc.inv_dthe2 = inv_dthe2; ctx->sorc.A2y = A2y;
+    {
+        const size_t tri = (size_t)8 * sJ * (5 * ctx->sor_pm + 4);   // the tridiagonal kernel's shared memory
+        if(tri > 48 * 1024 && tri <= 227 * 1024 &&
+           cudaFuncSetAttribute(sor_tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri) != cudaSuccess){
+            cudaGetLastError();
+            aturan_ctx_destroy(ctx);
+            return ATURAN_E_CUDA;
+        }
+    }
 
     auto up = [&](void* dst, const void* src, size_t n) -> int {
         return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, ctx->st) == cudaSuccess ? 0 : 1;
@@ -864,6 +899,7 @@ int aturan_ctx_destroy(aturan_ctx* ctx){
     if(!ctx) return ATURAN_E_INVALID;
     if(ctx->st) cudaStreamSynchronize(ctx->st);
     if(ctx->gs_exec) cudaGraphExecDestroy(ctx->gs_exec);
+    if(ctx->tape) cudaFree(ctx->tape);
     for(auto& e : ctx->evs){ cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if(ctx->mem) cudaFree(ctx->mem);
     if(ctx->st) cudaStreamDestroy(ctx->st);
@@ -909,6 +945,98 @@ int aturan_download_buoy_ref(aturan_ctx* ctx, double* host){
 int aturan_rk4_step(aturan_ctx* ctx){
     if(!ctx) return ATURAN_E_INVALID;
     return ctx->mixed ? run_rk4<float, float>(ctx, ctx->k32) : run_rk4<double, double>(ctx, ctx->k64);
+}
+
+int aturan_tape(aturan_ctx* ctx, int on){
+    if(!ctx) return ATURAN_E_INVALID;
+    if(!on){
+        if(ctx->tape){ CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->tape); }
+        ctx->tape = nullptr;
+        ctx->tape_valid = false;
+        return ATURAN_OK;
+    }
+    if(ctx->mixed) return fail(ctx, ATURAN_E_UNSUPPORTED, "the RK4 adjoint needs an FP64 context");
+    if(ctx->tape) return ATURAN_OK;
+    const Grid& g = ctx->g;
+    const size_t fs = g.fstride;
+    // stage inputs 4 x 4, T output 1, slots, ybar 4, kbar 4, g0 4, phbar 1, rbar 1; level means + sums
+    const size_t nf = 4 * ADJ_NF + 1 + ADJ_SLOTS + 3 * ADJ_NF + 2;
+    const size_t bytes = (nf * fs + 3 * (size_t)g.im) * sizeof(double);
+    void* mem = nullptr;
+    if(cudaMalloc(&mem, bytes) != cudaSuccess){ cudaGetLastError(); return fail(ctx, ATURAN_E_NOMEM, "tape allocation"); }
+    CK(cudaMemsetAsync(mem, 0, bytes, ctx->st));      // slots stay zero outside the interior
+    double* cur = reinterpret_cast<double*>(mem);
+    auto take = [&](size_t n){ double* r = cur; cur += n; return r; };
+    ctx->tape = reinterpret_cast<double*>(mem);
+    ctx->tX = take(4 * ADJ_NF * fs);
+    ctx->tTout = take(fs);
+    ctx->aslot = take(ADJ_SLOTS * fs);
+    ctx->aybar = take(ADJ_NF * fs);
+    ctx->akbar = take(ADJ_NF * fs);
+    ctx->ag0 = take(ADJ_NF * fs);
+    ctx->aphbar = take(fs);
+    ctx->arbar = take(fs);
+    ctx->tref = take(g.im);
+    ctx->alev = take(2 * g.im);
+    ctx->tape_valid = false;
+    return ATURAN_OK;
+}
+
+int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const* xbar){
+    if(!ctx || !ybar || !xbar) return ATURAN_E_INVALID;
+    for(int q = 0; q < ADJ_NF; q++) if(!ybar[q] || !xbar[q]) return fail(ctx, ATURAN_E_INVALID, "null adjoint pointer");
+    if(!ctx->tape || !ctx->tape_valid) return fail(ctx, ATURAN_E_INVALID, "no taped RK4 step (aturan_tape, then aturan_rk4_step)");
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride, rows = (size_t)g.im * g.jm;
+    const double dt = ctx->p.dt;
+    Region reg(ctx, ATURAN_K_ADJOINT, 0);
+    long nl = 0;
+    for(int q = 0; q < ADJ_NF; q++)                    // the caller's ybar' into the padded layout
+        CK(cudaMemcpy2DAsync(ctx->ag0 + q * fs, g.kp * 8, ybar[q], g.km * 8, g.km * 8, rows,
+                             cudaMemcpyDeviceToDevice, ctx->st));
+    const RhsConst<double>& K = ctx->k64;
+    const double t_min = K.t_min, t_max = K.t_max;
+    const dim3 gc((g.km + 127) / 128, g.jm, g.im);
+    adj_init_kernel<<<gc, 128, 0, ctx->st>>>(g, ctx->ag0, ctx->tTout, t_min, t_max, dt / 6.0 * 1.0,
+                                             ctx->ag0, ctx->aybar, ctx->akbar, ctx->aphbar);
+    CK_LAUNCH("adjoint init"); nl++;
+    AdjArgs a;
+    a.g = g;
+    a.X0 = ctx->tX;
+    a.kbar = ctx->akbar;
+    a.pdyn = ctx->pdyn;
+    a.forc = reinterpret_cast<const double*>(ctx->forc);
+    a.geo = reinterpret_cast<const GeoIJ<double>*>(ctx->geo);
+    a.cp_tab = reinterpret_cast<const double*>(ctx->cp_tab);
+    a.k = K;
+    a.slot = ctx->aslot;
+    const dim3 gs((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);
+    const dim3 gg((g.km - 1 + 127) / 128, g.jm, g.im);
+    for(int stage = 3; stage >= 0; stage--){
+        a.X = ctx->tX + (size_t)stage * ADJ_NF * fs;
+        adj_local_kernel<<<gs, dim3(32, 4), 0, ctx->st>>>(a);
+        const int prev = stage - 1;
+        const double w_prev = prev >= 0 ? dt / 6.0 * ((prev == 0 || prev == 3) ? 1.0 : 2.0) : 0.0;
+        const double c_prev = prev >= 0 ? ((prev == 0 || prev == 1) ? 0.5 * dt : (prev == 2 ? dt : 0.0)) : 0.0;
+        adj_gather_kernel<<<gg, 128, 0, ctx->st>>>(g, ctx->aslot, ctx->aybar, ctx->aphbar, ctx->ag0, ctx->akbar,
+                                                  w_prev, c_prev, prev >= 0 ? 1 : 0);
+        CK_LAUNCH("adjoint stage"); nl += 2;
+    }
+    const double* t0 = ctx->tX;
+    adj_hydro_kernel<<<(g.jm * g.km + 255) / 256, 256, 0, ctx->st>>>(
+        g, t0, reinterpret_cast<const double*>(ctx->pstat), t0 + 2 * fs, t0 + 3 * fs, ctx->tref, ctx->rm_i, ctx->cor_j,
+        ctx->aphbar, ctx->aybar, ctx->arbar, ctx->hc);
+    adj_level_sum_kernel<<<g.im, 256, 0, ctx->st>>>(g, t0, reinterpret_cast<const double*>(ctx->pstat), ctx->wsin,
+                                                   ctx->arbar, ctx->hc, ctx->alev);
+    adj_level_apply_kernel<<<gc, 128, 0, ctx->st>>>(g, t0, reinterpret_cast<const double*>(ctx->pstat), ctx->wsin,
+                                                    ctx->alev, ctx->hc, ctx->aybar);
+    CK_LAUNCH("adjoint hydrostatic"); nl += 3;
+    reg.n = nl;
+    for(int q = 0; q < ADJ_NF; q++)
+        CK(cudaMemcpy2DAsync(xbar[q], g.km * 8, ctx->aybar + q * fs, g.kp * 8, g.km * 8, rows,
+                             cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return ATURAN_OK;
 }
 
 int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_noconv){

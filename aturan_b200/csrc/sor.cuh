@@ -170,61 +170,72 @@ __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, Mat
 // row, and q returned with zero weighted mean. The result is written back times the inverse
 // transform's weight w_m / N (w = 1 for m = 0 and m = N/2, else 2).
 //
-// A block takes pb problems (problem t = 2 m + part): all of its threads stage the right-hand sides
-// into shared memory as [q][t] (row stride pb + 1: conflict-free), then one thread per problem runs
-// the two dependent recurrences on shared-memory latency, in place, and the block writes back.
-__global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pb){
-    extern __shared__ double sd[];
-    const int J = s.J, ld_ = pb + 1;
-    const int nprob = 2 * (s.NM + 1);
-    const int t0 = blockIdx.x * pb;
-    for(int idx = threadIdx.x; idx < pb * J; idx += blockDim.x){
-        const int lt = idx / J, q = idx - lt * J;
-        const int t = t0 + lt;
-        double v = 0.0;
-        if(t < nprob) v = ((t & 1) ? As : Ac)[(size_t)(t >> 1) * J + q];
-        sd[q * ld_ + lt] = v;
+// A block takes pm modes (2 pm problems, problem t = 2 m + part): all of its threads stage the
+// right-hand sides into shared memory as [q][t] (row stride 2 pm + 1: conflict-free) and the
+// modes' factors as [q][m] (stride pm + 1); then one thread per problem runs the two dependent
+// recurrences on shared-memory latency, in place, and the block writes back. Shared memory:
+// 8 J (5 pm + 4) bytes.
+__global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pm){
+    extern __shared__ double sm[];
+    const int J = s.J, np = 2 * pm, ldr = np + 1, ldf = pm + 1;
+    double* sd = sm;                                     // [J][ldr]
+    double* fa = sd + (size_t)J * ldr;                   // [J][ldf] each
+    double* fc = fa + (size_t)J * ldf;
+    double* fi = fc + (size_t)J * ldf;
+    const int nmode = s.NM + 1;
+    const int m0 = blockIdx.x * pm;
+    for(int idx = threadIdx.x; idx < pm * J; idx += blockDim.x){
+        const int lm = idx / J, q = idx - lm * J;
+        const int m = m0 + lm;
+        double c = 0.0, sn = 0.0, va = 0.0, vc = 0.0, vi = 0.0;
+        if(m < nmode){
+            const size_t g = (size_t)m * J + q;
+            c = Ac[g]; sn = As[g]; va = lu.a[g]; vc = lu.cf[g]; vi = lu.idn[g];
+        }
+        sd[q * ldr + 2 * lm] = c; sd[q * ldr + 2 * lm + 1] = sn;
+        fa[q * ldf + lm] = va; fc[q * ldf + lm] = vc; fi[q * ldf + lm] = vi;
     }
     __syncthreads();
-    const int lt = threadIdx.x, t = t0 + lt;
-    if(lt < pb && t < nprob){
-        const int m = t >> 1, part = t & 1;
+    const int lt = threadIdx.x;
+    const int lm = lt >> 1, part = lt & 1, m = m0 + lm;
+    if(lt < np && m < nmode){
         double* d = sd + lt;
         if(part == 1 && (m == 0 || 2 * m == s.N)){
-            for(int q = 0; q < J; q++) d[q * ld_] = 0.0;
+            for(int q = 0; q < J; q++) d[q * ldr] = 0.0;
         } else {
-            const double* a = lu.a + (size_t)m * J;
-            const double* cf = lu.cf + (size_t)m * J;
-            const double* idn = lu.idn + (size_t)m * J;
+            const double* a = fa + lm;
+            const double* cf = fc + lm;
+            const double* idn = fi + lm;
             if(m == 0){
                 double yr = 0.0, ys = 0.0;
-                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yr += wq * d[q * ld_]; ys += wq; }
+                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yr += wq * d[q * ldr]; ys += wq; }
                 const double sh = yr / ys;
-                for(int q = 0; q < J; q++) d[q * ld_] -= sh;
+                for(int q = 0; q < J; q++) d[q * ldr] -= sh;
                 d[0] = 0.0;                                   // the pinned row
             }
             double yp = 0.0;
 #pragma unroll 4
-            for(int q = 0; q < J; q++){ yp = (d[q * ld_] - a[q] * yp) * idn[q]; d[q * ld_] = yp; }
-            double x = d[(J - 1) * ld_];
+            for(int q = 0; q < J; q++){ yp = (d[q * ldr] - a[q * ldf] * yp) * idn[q * ldf]; d[q * ldr] = yp; }
+            double x = d[(J - 1) * ldr];
 #pragma unroll 4
-            for(int q = J - 2; q >= 0; q--){ x = d[q * ld_] - cf[q] * x; d[q * ld_] = x; }
+            for(int q = J - 2; q >= 0; q--){ x = d[q * ldr] - cf[q * ldf] * x; d[q * ldr] = x; }
             if(m == 0){
                 double yq = 0.0, ys = 0.0;
-                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yq += wq * d[q * ld_]; ys += wq; }
+                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yq += wq * d[q * ldr]; ys += wq; }
                 const double sh = yq / ys;
-                for(int q = 0; q < J; q++) d[q * ld_] -= sh;
+                for(int q = 0; q < J; q++) d[q * ldr] -= sh;
             }
         }
     }
     __syncthreads();
-    for(int idx = threadIdx.x; idx < pb * J; idx += blockDim.x){
-        const int lt2 = idx / J, q = idx - lt2 * J;
-        const int t2 = t0 + lt2;
-        if(t2 < nprob){
-            const int m2 = t2 >> 1;
+    for(int idx = threadIdx.x; idx < pm * J; idx += blockDim.x){
+        const int lm2 = idx / J, q = idx - lm2 * J;
+        const int m2 = m0 + lm2;
+        if(m2 < nmode){
             const double wm = ((m2 == 0 || 2 * m2 == s.N) ? 1.0 : 2.0) / s.N;   // inverse-transform weight
-            ((t2 & 1) ? As : Ac)[(size_t)m2 * J + q] = wm * sd[q * ld_ + lt2];
+            const size_t g = (size_t)m2 * J + q;
+            Ac[g] = wm * sd[q * ldr + 2 * lm2];
+            As[g] = wm * sd[q * ldr + 2 * lm2 + 1];
         }
     }
 }

@@ -52,18 +52,62 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clocks and throttle reasons sampled every ~2 ms through NVML while the timed region runs
+    (nvidia-smi's 100 ms period would see a few-millisecond region once or not at all); falls
+    back to nvidia-smi when NVML is not importable. Reads only."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.sm, self.mx, self.reasons = [], [], set()
         self.proc = None
+        self.nv = None
+        self.run = False
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:
+                import torch
+                pr = torch.cuda.get_device_properties(index)
+                bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+                h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.nv, self.h = nv, h
+            self.bits = [(n, getattr(nv, attr, val)) for n, attr, val in self.REASONS]
+        except Exception:
+            self.nv = None
+
+    def _poll(self):
+        nv = self.nv
+        while self.run:
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.mx.append(float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h) if hasattr(
+                    nv, "nvmlDeviceGetCurrentClocksEventReasons") else nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for n, bit in self.bits:
+                    if r & bit:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def start(self):
+        if self.nv is not None:
+            self.run = True
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         try:
+            self.rows = []
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -77,6 +121,12 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        if self.nv is not None:
+            self.run = False
+            self.t.join(timeout=2)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                    "sm_max_mhz": max(self.mx) if self.mx else None,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -87,7 +137,7 @@ class ClockSampler:
         self.t.join(timeout=2)
         sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _, _ in self.REASONS]
         reasons = set()
         for r in self.rows:
             if len(r) >= 9:
@@ -95,7 +145,43 @@ class ClockSampler:
                     if v.lower() == "active":
                         reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
+
+
+def adjoint_timing(api, P, S, torch, reps=5):
+    """Device time of one taped FP64 RK4 step and of its hand-written adjoint on the full grid
+    (41x181x361), CUDA events on the context's stream, after two warm-up pairs."""
+    p = P.default_params(precision=P.FP64)
+    ctx = api.Context(p)
+    ctx.upload_state(S.synthetic_state(p, seed=20261206))
+    ctx.tape(True)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    ybar = [torch.randn(p.shape, dtype=torch.float64, device="cuda", generator=g) for _ in range(4)]
+    xbar = [torch.empty(p.shape, dtype=torch.float64, device="cuda") for _ in range(4)]
+    torch.cuda.synchronize()
+    yp, xp = [t.data_ptr() for t in ybar], [t.data_ptr() for t in xbar]
+    for _ in range(2):
+        ctx.rk4_step()
+        ctx.rk4_adjoint(yp, xp)
+    ctx.synchronize()
+    fwd = adj = 0.0
+    for _ in range(reps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        ctx.rk4_step()
+        e[1].record(stream)
+        ctx.rk4_adjoint(yp, xp)
+        e[2].record(stream)
+        e[2].synchronize()
+        fwd += e[0].elapsed_time(e[1])
+        adj += e[1].elapsed_time(e[2])
+    ctx.close()
+    return {"fwd_ms": fwd / reps, "adj_ms": adj / reps, "adj_over_fwd": adj / fwd, "precision": "fp64",
+            "grid": [p.im, p.jm, p.km],
+            "what": "forward = aturan_rk4_step with the tape on (level means, hydrostatic integral, 4 stages, "
+                    "tape copies); adjoint = aturan_rk4_adjoint (4 reverse stages, hydrostatic and level-mean "
+                    "adjoints, layout copies in and out)"}
 
 
 def dist_env():
@@ -168,7 +254,10 @@ def cpu_reference_step_time(nsteps, press, budget_s=120.0):
     for _ in range(n):
         one()
     dt = (time.perf_counter() - t0) / n
-    return dt, kind, cores, f"{n} full steps (GS/RB pressure + 4 SatAdj + sync + RK4) of {what}, 41x181x361", n
+    ptxt = ("1 red-black sweep (PressureSolver)" if press == "rb" else
+            "1 lexicographic GS sweep (PressureSolverUran, the reference's default; the reference has no "
+            "solve to a residual, so this is its step for every GPU pressure kind)")
+    return dt, kind, cores, f"{n} full steps (pressure: {ptxt} + 4 SatAdj + sync + RK4) of {what}, 41x181x361", n
 
 
 def run_reference_arm(args, rank, world):
@@ -196,8 +285,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--press", default="gs", choices=["gs", "rb", "sor", "line"])
+    ap.add_argument("--press", default="line", choices=["gs", "rb", "sor", "line"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the RK4 adjoint / forward timing")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-run", action="store_true",
@@ -311,7 +401,14 @@ def main():
     # ---- accuracy of the mixed step against the FP64 step (which matches the FP64 oracle) ----
     accuracy = None
     if args.precision == "mixed" and rank == 0:
-        accuracy = mixed_accuracy(api, P, S, F, pa)
+        accuracy = mixed_accuracy(api, P, S, F, pa, torch)
+
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            adjoint = adjoint_timing(api, P, S, torch)
+        except Exception as ex:          # reported, never silently replaced
+            adjoint = {"error": f"{type(ex).__name__}: {ex}"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -343,6 +440,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(in_names) * fbytes,
                     "d2h_bytes_per_step": len(out_names) * fbytes, "steps": E},
             "clocks": clk,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
         }
         if accuracy is not None:
@@ -354,30 +452,48 @@ def main():
         dist.destroy_process_group()
 
 
-def mixed_accuracy(api, P, S, F, pa, steps=(1, 10)):
-    """Per-field max |mixed - fp64| / max |fp64| after 1 and 10 steps from the same state."""
+def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
+    """The mixed step against the FP64 step (which matches the FP64 oracle) from the same state:
+    per-field max |mixed - fp64| / max |fp64| over the interior after 1, 10 and 200 steps, and both
+    step times (CUDA events on each context's stream, median over steps 2..10)."""
     p64 = P.default_params(precision=P.FP64)
     p32 = P.default_params(precision=P.MIXED)
     st = S.synthetic_state(p64, seed=99)
     c64, c32 = api.Context(p64), api.Context(p32)
     c64.upload_state(st)
     c32.upload_state(st)
-    I = (slice(1, 40), slice(1, 180), slice(0, 360))
-    out = {}
+    s64, s32 = torch.cuda.ExternalStream(c64.stream), torch.cuda.ExternalStream(c32.stream)
+    I = (slice(1, p64.im - 1), slice(1, p64.jm - 1), slice(0, p64.km - 1))
+    out, t64, t32 = {}, [], []
     done = 0
+
+    def timed(ctx, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step(**pa)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
     for n in steps:
         while done < n:
-            c64.step(**pa)
-            c32.step(**pa)
+            a, b = timed(c64, s64), timed(c32, s32)
             done += 1
+            if 2 <= done <= 10:
+                t64.append(a)
+                t32.append(b)
         errs = {}
-        for f in ("t", "u", "v", "w", "p_dyn", "h2o", "ch4", "nh3", "h2s"):
+        for f in F.PROGNOSTIC + ["p_dyn"]:
             a, b = c32.download(f)[I], c64.download(f)[I]
             s = np.abs(b).max()
             errs[f] = float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
         out[f"step{n}"] = errs
     c64.close()
     c32.close()
+    m64, m32 = statistics.median(t64), statistics.median(t32)
+    out["fp64_ms_per_step"] = m64
+    out["mixed_ms_per_step"] = m32
+    out["mixed_speedup_over_fp64"] = m64 / m32
     return out
 
 

@@ -171,6 +171,22 @@ int aturan_download_buoy_ref(aturan_ctx* ctx, double* host_im);
  * Replaces cUranusModel::RungeKuttaUran() (RungeKutta_Uran_Turb.cpp:179-404). */
 int aturan_rk4_step(aturan_ctx* ctx);
 
+/* Adjoint of one RK4 step of the dry dynamics, FP64 contexts. No counterpart in the reference,
+ * which has no adjoint; it differentiates RungeKutta_Uran_Turb.cpp:18-403 with RHS_Uran_Turb.cpp's
+ * tendencies of t, u, v, w.
+ * aturan_tape(ctx, 1): every later aturan_rk4_step keeps what its adjoint needs (the stage inputs
+ *   of t, u, v, w, the new T and the level means: 17 fields, plus 42 fields of work arrays, of
+ *   device memory); aturan_tape(ctx, 0) frees it. ATURAN_E_UNSUPPORTED on a mixed context.
+ * aturan_rk4_adjoint(ctx, ybar, xbar): ybar[4] and xbar[4] are device pointers to contiguous
+ *   [im][jm][km] FP64 arrays in the order t, u, v, w. Given the adjoint ybar of those fields after
+ *   the last taped aturan_rk4_step, writes xbar = J^T ybar, J the step's Jacobian with respect to
+ *   the fields before it, taken as the state and its start-of-step copies together (as after
+ *   aturan_sync_ncopies). p_dyn, p_stat, p_baro, p_b0, p_bfollow, the forcing and the other
+ *   prognostic fields are held fixed. The T clamp and cp(T)'s 0.5 K table are differentiated
+ *   piecewise (0 where clamped, the interval's slope). Synchronous. */
+int aturan_tape(aturan_ctx* ctx, int on);
+int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const* xbar);
+
 /* The pressure solve.
  *   GS_LEX:    replaces PressureSolverUran(m).run() (PressureSolverUran.h:33-250); omega,
  *              max_sweeps and tol are ignored (exactly one sweep, as the reference).
@@ -210,6 +226,7 @@ enum aturan_kernel_kind {
     ATURAN_K_RB,             /* red-black sweeps, source, boundary passes, residual checks */
     ATURAN_K_HYDRO,          /* buoyancy reference level + hydrostatic column integral */
     ATURAN_K_COPY,           /* n-copy sync and layout conversions */
+    ATURAN_K_ADJOINT,        /* the RK4 step's adjoint (aturan_rk4_adjoint) */
     ATURAN_K_NKINDS
 };
 

@@ -1074,6 +1074,11 @@ static void line_colour(const aturan_params* p, const double* rad, const double*
     }
 }
 
+/* Red-black line SOR on the shared solver's equation to a relative residual (no reference oracle:
+ * the reference's PRESS_LINE sweeps a fixed count). The column-uniform correction runs before
+ * iterations 0, 8, 16, ...: with exact column solves the first correction removes the
+ * column-uniform error and later ones do not change the rate. The GPU's RB_LINE runs the same
+ * sequence. Returns 0 at tol, 1 at the iteration cap. */
 int oracle_pressure_line(const aturan_params* p, double* const* f, double omega, int max_iter,
                          double tol, int* iters_done, double* resid){
     const int im = p->im, jm = p->jm, km = p->km;
@@ -1087,7 +1092,7 @@ int oracle_pressure_line(const aturan_params* p, double* const* f, double omega,
     double* P = f[ATURAN_P_DYN];
     int s = 0; double r = folded_residual(p, rad, st, P, src);
     while(s < max_iter && !(r <= tol)){
-        column_correction(p, rad, st, P, src);
+        if(s % 8 == 0) column_correction(p, rad, st, P, src);
         line_colour(p, rad, st, P, src, 0, omega);
         line_colour(p, rad, st, P, src, 1, omega);
         s++;

@@ -1,0 +1,106 @@
+"""The hand-written adjoint of the RK4 step (aturan_rk4_adjoint via aturan_b200.autograd) against
+(1) torch.autograd through the FP64 torch restatement of the dry step (oracle/dry_ref.py, whose
+forward matches the C restatement to 1e-12, tests/test_dry_ref.py), as a full vector-Jacobian
+product with random cotangents, and (2) central finite differences of the GPU forward in seeded
+random directions of (T, zonal-wind template) on the 41 x 91 x 181 grid, loss = mean T^2 on the
+last integrated layer i = im - 2."""
+import numpy as np
+import pytest
+import torch
+
+from aturan_b200 import api, params as P, state as S
+from aturan_b200.autograd import DryRK4Step, DryStepper, DRY
+
+pytestmark = pytest.mark.gpu
+
+FIXED = ("p_dyn", "p_stat", "p_baro", "p_b0", "p_bfollow", "nue", "thermalmassflux", "Q_precip")
+
+
+def make(shape, seed):
+    p = P.default_params(*shape)
+    st = S.synthetic_state(p, seed=seed)
+    ctx = api.Context(p)
+    ctx.upload_state(st)
+    return p, st, ctx
+
+
+@pytest.mark.parametrize("shape,seed", [((12, 20, 33), 61), ((21, 37, 73), 62)])
+def test_adjoint_matches_torch_autograd(oracle_lib, shape, seed):
+    from oracle.dry_ref import DryStep
+    p, st, ctx = make(shape, seed)
+    stepper = DryStepper(ctx)
+    x = [torch.tensor(st[n], device="cuda", requires_grad=True) for n in DRY]
+    y = DryRK4Step.apply(stepper, *x)
+    rng = np.random.default_rng(seed)
+    ybar = [torch.tensor(rng.standard_normal(p.shape), device="cuda") for _ in DRY]
+    g_gpu = torch.autograd.grad(y, x, ybar)
+    ctx.close()
+
+    ref = DryStep(p, {n: st[n] for n in FIXED}, oracle_lib)
+    xc = [torch.tensor(st[n], requires_grad=True) for n in DRY]
+    yc = ref(*xc)
+    for a, b in zip(y, yc):                       # the same forward
+        assert (a.detach().cpu() - b.detach()).abs().max() <= 1e-11 * b.detach().abs().max()
+    g_ref = torch.autograd.grad(yc, xc, [g.cpu() for g in ybar])
+    for n, a, b in zip(DRY, g_gpu, g_ref):
+        a = a.cpu()
+        err = float((a - b).abs().max() / b.abs().max())
+        assert err < 1e-9, (n, err)
+
+
+def template_to_rows(tmpl, p):
+    """The 181-point (1 degree) zonal-wind template on the grid's rows: linear in latitude."""
+    lat_t = torch.linspace(-90.0, 90.0, tmpl.numel(), dtype=torch.float64, device=tmpl.device)
+    _, the = S.coords(p)
+    lat = torch.tensor(90.0 - np.degrees(the), device=tmpl.device)
+    x = (lat + 90.0) / 180.0 * (tmpl.numel() - 1)
+    i0 = torch.clamp(x.floor().long(), 0, tmpl.numel() - 2)
+    f = x - i0.to(x.dtype)
+    assert lat_t.numel() == tmpl.numel()
+    return tmpl[i0] * (1.0 - f) + tmpl[i0 + 1] * f
+
+
+def test_adjoint_finite_differences_config3():
+    p, st, ctx = make((41, 91, 181), 20261206)
+    stepper = DryStepper(ctx)
+    x0 = [torch.tensor(st[n], device="cuda") for n in DRY]
+    tmpl0 = torch.zeros(181, dtype=torch.float64, device="cuda")
+
+    def loss(T, tmpl):
+        w = x0[3] + (template_to_rows(tmpl, p) / p.u_0)[None, :, None]
+        y = DryRK4Step.apply(stepper, T, x0[1], x0[2], w)
+        return (y[0][p.im - 2, 1:-1, :-1] ** 2).mean()
+
+    T = x0[0].clone().requires_grad_(True)
+    tm = tmpl0.clone().requires_grad_(True)
+    L = loss(T, tm)
+    gT, gtm = torch.autograd.grad(L, (T, tm))
+    rng = np.random.default_rng(20261206)
+    worst = 0.0
+    with torch.no_grad():
+        for _ in range(32):
+            dT = torch.tensor(rng.standard_normal(p.shape), device="cuda") * 1e-3 * float(x0[0].abs().max())
+            dtm = torch.tensor(rng.standard_normal(181), device="cuda")          # m/s
+            h = 1e-3
+            lp = loss(x0[0] + h * dT, tmpl0 + h * dtm)
+            lm = loss(x0[0] - h * dT, tmpl0 - h * dtm)
+            fd = float((lp - lm) / (2 * h))
+            an = float((gT * dT).sum() + (gtm * dtm).sum())
+            worst = max(worst, abs(fd - an) / max(abs(an), 1e-300))
+    ctx.close()
+    assert worst <= 1e-4, worst
+
+
+def test_adjoint_requires_tape_and_fp64():
+    p = P.default_params(9, 13, 17)
+    ctx = api.Context(p)
+    ctx.upload_state(S.synthetic_state(p, seed=3))
+    t = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(api.AturanError):
+        ctx.rk4_adjoint([t.data_ptr()] * 4, [t.data_ptr()] * 4)
+    ctx.close()
+    pm = P.default_params(9, 13, 17, precision=P.MIXED)
+    cm = api.Context(pm)
+    with pytest.raises(api.AturanError):
+        cm.tape(True)
+    cm.close()
