@@ -40,6 +40,9 @@ SIGNATURES = {
     "aturan_download_buoy_ref": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_rk4_step": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_tape": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_pressure_solve": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                               ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                              ctypes.c_int),
     "aturan_rk4_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_pressure": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                          ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -170,6 +173,16 @@ class Context:
         yb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
         xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
         self._check(self.L.aturan_rk4_adjoint(self.h, yb, xb), "rk4_adjoint")
+
+    def pressure_solve(self, b_ptr, x_ptr, kind=3, transposed=False, omega=1.0, max_sweeps=200, tol=1e-10):
+        """aturan_pressure_solve on device pointers: Lc x = b (or Lc^T x = b); (rc, sweeps, resid)."""
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        rc = self._check(self.L.aturan_pressure_solve(self.h, int(kind), 1 if transposed else 0, float(omega),
+                                                      int(max_sweeps), float(tol), ctypes.c_void_p(int(b_ptr)),
+                                                      ctypes.c_void_p(int(x_ptr)), ctypes.byref(s), ctypes.byref(r)),
+                         "pressure_solve")
+        return rc, s.value, r.value
 
     def pressure(self, kind=0, omega=1.0, max_sweeps=1, tol=0.0):
         s = ctypes.c_int()

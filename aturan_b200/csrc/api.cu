@@ -62,6 +62,8 @@ struct aturan_ctx {
     double *sor_ct, *sor_st, *sor_ctT, *sor_stT, *sor_colR, *sor_Ac, *sor_As, *sor_part, *sor_q;
     double *mlu_a, *mlu_cf, *mlu_idn;            // per-mode theta factorisations
     double *llu_a, *llu_cf, *llu_idn;            // per-(i,j) radial-line factorisations
+    double *mluT_a, *mluT_cf, *mluT_idn;         // the same for the transposed operator
+    double *lluT_a, *lluT_cf, *lluT_idn;
     float *r32, *e32;
     int sor_nblk;
     int sor_pm;                // Fourier modes per block of the column correction's tridiagonal solves
@@ -413,10 +415,12 @@ void bc_passes(aturan_ctx* ctx, T* P){
 }
 
 // Residual of P against src: relative L2 norm (host sum of the block partials, fixed order).
-template <typename T>
+// TR: of the transposed operator.
+template <typename T, bool TR = false>
 int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr){
     const Grid g = ctx->g;
-    sor_colsum_kernel<T><<<dim3((g.km - 1 + 31) / 32, g.jm - 2), dim3(32, 8), 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
+    sor_colsum_kernel<T, TR><<<dim3((g.km - 1 + 31) / 32, g.jm - 2), dim3(32, 8), 0, ctx->st>>>(
+        g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
     CK_LAUNCH("residual");
     if(!rel) return ATURAN_OK;                                 // column sums only: no host round trip
     CK(cudaMemcpyAsync(ctx->host_part.data(), ctx->sor_part, 2 * ctx->sor_nblk * 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -428,43 +432,91 @@ int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, doubl
     return ATURAN_OK;
 }
 
-// The column-uniform correction from the column sums left in sor_colR by the last residual.
-template <typename T>
+// The column-uniform correction (TR: the transposed system's y-shaped one) from the column sums
+// left in sor_colR by the last residual.
+template <typename T, bool TR = false>
 int sor_correct(aturan_ctx* ctx, T* P){
     const Grid g = ctx->g;
     const SorConst& c = ctx->sorc;
-    const MatRef none{nullptr, 0, 0};
     const MatRef R{ctx->sor_colR, c.N, 1};                        // (jj, k)
     const dim3 gf((c.NM + 1 + 31) / 32, (c.J + 31) / 32);
-    sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_ctT, c.NM + 1, 1}, none, none,
-                                            1.0 / c.A2y, ctx->sor_Ac, 1, c.J);
-    sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_stT, c.NM + 1, 1}, none, none,
-                                            1.0 / c.A2y, ctx->sor_As, 1, c.J);
-    ModeLU lu{ctx->mlu_a, ctx->mlu_cf, ctx->mlu_idn};
+    sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_ctT, c.NM + 1, 1},
+                                            R, MatRef{ctx->sor_stT, c.NM + 1, 1}, 1.0 / c.A2y,
+                                            ctx->sor_Ac, ctx->sor_As, 1, c.J);
+    ModeLU lu = TR ? ModeLU{ctx->mluT_a, ctx->mluT_cf, ctx->mluT_idn} : ModeLU{ctx->mlu_a, ctx->mlu_cf, ctx->mlu_idn};
     const int pm = ctx->sor_pm;
     sor_tridiag_kernel<<<(c.NM + 1 + pm - 1) / pm, 128, (size_t)8 * c.J * (5 * pm + 4), ctx->st>>>(
-        c, lu, ctx->sor_Ac, ctx->sor_As, pm);
+        c, lu, ctx->sor_Ac, ctx->sor_As, pm, TR ? 1 : 0);
     const dim3 gi((c.N + 31) / 32, (c.J + 31) / 32);
     sor_gemm_kernel<<<gi, 256, 0, ctx->st>>>(c.J, c.N, c.NM + 1, MatRef{ctx->sor_Ac, 1, c.J}, MatRef{ctx->sor_ct, c.N, 1},
                                             MatRef{ctx->sor_As, 1, c.J}, MatRef{ctx->sor_st, c.N, 1},
-                                            1.0, ctx->sor_q, c.N, 1);
-    sor_add_kernel<T><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P);
+                                            1.0, ctx->sor_q, nullptr, c.N, 1);
+    sor_add_kernel<T, TR><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P);
     CK_LAUNCH("column-uniform correction");
     return ATURAN_OK;
 }
 
-// One relaxation sweep (both colours) of the folded operator: point (line = false) or radial line.
-template <typename T>
+// One relaxation sweep (both colours) of the folded operator (TR: its transpose): point
+// (line = false) or radial line.
+template <typename T, bool TR = false>
 void sor_sweep(aturan_ctx* ctx, T* E, const T* R, double omega, bool line){
     const Grid g = ctx->g;
     for(int colour = 0; colour < 2; colour++){
         if(line)
-            sor_line_kernel<T><<<dim3((g.km / 2 + 31) / 32, g.jm - 2), 256, (size_t)(g.im - 2) * 32 * sizeof(double), ctx->st>>>(
-                g, E, R, ctx->rbw, ctx->llu_a, ctx->llu_cf, ctx->llu_idn, colour, omega);
+            sor_line_kernel<T, TR><<<dim3((g.km / 2 + 31) / 32, g.jm - 2), 256, (size_t)(g.im - 2) * 35 * sizeof(double), ctx->st>>>(
+                g, E, R, ctx->rbw, TR ? ctx->lluT_a : ctx->llu_a, TR ? ctx->lluT_cf : ctx->llu_cf,
+                TR ? ctx->lluT_idn : ctx->llu_idn, colour, omega);
         else
-            sor_colour_kernel<T><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(
+            sor_colour_kernel<T, TR><<<dim3((g.km / 2 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(
                 g, E, R, ctx->rbw, colour, omega);
     }
+}
+
+int sor_check_sizes(aturan_ctx* ctx, double omega, bool line){
+    const Grid& g = ctx->g;
+    if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
+    if(8 * ctx->sorc.J * (5 * ctx->sor_pm + 4) > 227 * 1024)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 2900");
+    if(line && (g.im - 2) * 35 * (int)sizeof(double) > 49152)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 177");
+    return ATURAN_OK;
+}
+
+// Sweeps between residual checks and between column-uniform corrections. Point SOR needs ~200
+// sweeps and loses ~6 % of its rate with a correction every 16; line SOR needs 5-7 iterations
+// and converges at the same rate with one correction per 8 as with one per iteration (the first
+// correction removes the column-uniform error; oracle measurements at 41x181x361).
+inline int sor_check_every(bool line){ return line ? 1 : 16; }
+inline int sor_correct_every(bool line){ return line ? 8 : 16; }
+
+// Remove src's component along the operator's left null vector (y_i y_j for Lc, the constant for
+// Lc^T) by a shift of the interior, all on the device.
+void sor_compat(aturan_ctx* ctx, double* src, bool transposed){
+    const Grid& g = ctx->g;
+    const int ny = ((g.jm - 2) * (g.km - 1) + 255) / 256;
+    sor_ysum_kernel<<<ny, 256, 0, ctx->st>>>(g, src, ctx->sor_part, transposed ? 1 : 0);
+    sor_shift_finish_kernel<<<1, 256, 0, ctx->st>>>(ctx->sor_part, ny, ctx->sor_part + 2 * ny);
+    sor_shift_kernel<<<148 * 4, 256, 0, ctx->st>>>(g, src, ctx->sor_part + 2 * ny);
+}
+
+// FP64 red-black solve of Lc P = src (TR: Lc^T P = src) on the interior from the given P, src
+// compatible. Returns ATURAN_OK at tol, ATURAN_NOT_CONVERGED at the cap; counts launches into nl.
+template <bool TR>
+int solve_fp64(aturan_ctx* ctx, double* P, const double* src, double omega, int max_sweeps, double tol, bool line,
+               int* sweeps_done, double* resid, long& nl){
+    const int check_every = sor_check_every(line), every = sor_correct_every(line);
+    double r = 0.0;
+    int s = 0;
+    int rc = sor_residual<double, TR>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
+    while(s < max_sweeps && !(r <= tol)){
+        if(s % every == 0){ rc = sor_correct<double, TR>(ctx, P); if(rc) return rc; nl += 4; }
+        for(int n = 0; n < check_every && s < max_sweeps; n++, s++){ sor_sweep<double, TR>(ctx, P, src, omega, line); nl += 2; }
+        CK_LAUNCH("SOR sweeps");
+        rc = sor_residual<double, TR>(ctx, P, src, s % every == 0, &r, nullptr); if(rc) return rc; nl++;
+    }
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    return r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
 }
 
 template <typename S>
@@ -472,45 +524,30 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     const Grid g = ctx->g;
     const size_t fs = g.fstride;
     S* proj = reinterpret_cast<S*>(ctx->proj);
-    if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
-    if(8 * ctx->sorc.J * (5 * ctx->sor_pm + 4) > 227 * 1024)
-        return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 2900");
-    if(line && (g.im - 2) * 32 * (int)sizeof(double) > 49152)
-        return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 194");
+    int rc = sor_check_sizes(ctx, omega, line); if(rc) return rc;
     if(max_sweeps < 1) max_sweeps = 1;
-    // Sweeps between residual checks and between column-uniform corrections. Point SOR needs ~200
-    // sweeps and loses ~6 % of its rate with a correction every 16; line SOR needs 5-7 iterations
-    // and converges at the same rate with one correction per 8 as with one per iteration (the
-    // first correction removes the column-uniform error; oracle measurements at 41x181x361).
-    const int check_every = line ? 1 : 16;
-    const int every = line ? 8 : 16;
+    const int every = sor_correct_every(line);
     long nl = 0;
     Region reg(ctx, ATURAN_K_RB, 0);
     launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
                    grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->p.rigid_lid,
                    ctx->rbw, ctx->pc, ctx->scratch, ctx->st);
-    const int ny = ((g.jm - 2) * (g.km - 1) + 255) / 256;
-    sor_ysum_kernel<<<ny, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part);
-    sor_shift_kernel<<<148, 256, 0, ctx->st>>>(g, ctx->scratch, ctx->sor_part, ny);
+    sor_compat(ctx, ctx->scratch, false);
     CK_LAUNCH("SOR source");
-    nl += 5;
+    nl += 6;
     double* P = ctx->pdyn;
     const double* src = ctx->scratch;
     double r = 0.0;
     int s = 0;
+    int status;
     if(!ctx->mixed){
-        int rc = sor_residual<double>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
-        while(s < max_sweeps && !(r <= tol)){
-            if(s % every == 0){ rc = sor_correct<double>(ctx, P); if(rc) return rc; nl += 5; }
-            for(int n = 0; n < check_every && s < max_sweeps; n++, s++){ sor_sweep<double>(ctx, P, src, omega, line); nl += 2; }
-            CK_LAUNCH("SOR sweeps");
-            rc = sor_residual<double>(ctx, P, src, s % every == 0, &r, nullptr); if(rc) return rc; nl++;
-        }
+        status = solve_fp64<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl);
+        if(status < 0) return status;
     } else {
         // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
         // Lc e = r by FP32 sweeps (with the column-uniform correction), p += e in FP64.
         const int inner = line ? 3 : 48;
-        int rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
+        rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
             sor_resid32_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->r32, ctx->e32);
             nl++;
@@ -518,7 +555,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
                 if(n % every == 0){
                     rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc;
                     rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
-                    nl += 6;
+                    nl += 5;
                 }
                 sor_sweep<float>(ctx, ctx->e32, ctx->r32, omega, line);
                 nl += 2;
@@ -528,6 +565,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
             nl++;
             rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
         }
+        status = r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
     }
     launch_pdyn_bcs(g, P, ctx->st);                            // the boundary rows of the solution
     CK_LAUNCH("SOR boundary rows");
@@ -535,7 +573,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     reg.n = nl;
     if(sweeps_done) *sweeps_done = s;
     if(resid) *resid = r;
-    return r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
+    return status;
 }
 
 }  // namespace
@@ -616,12 +654,12 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
     ctx->sor_nblk = ((sN + 31) / 32) * sJ;
-    ctx->sor_pm = std::max(1, std::min(16, (200 * 1024 / (8 * sJ) - 4) / 5));
+    ctx->sor_pm = std::max(1, std::min(4, (200 * 1024 / (8 * sJ) - 4) / 5));
     for(int n = 0; n < 4; n++) add((size_t)(sNM + 1) * sN * 8);        // ct, st, ctT, stT
     add((size_t)sJ * sN * 8); add((size_t)(sNM + 1) * sJ * 8); add((size_t)(sNM + 1) * sJ * 8);
-    add((size_t)2 * ctx->sor_nblk * 8); add((size_t)sJ * sN * 8);
-    for(int n = 0; n < 3; n++) add((size_t)(sNM + 1) * sJ * 8);        // mode factorisations
-    for(int n = 0; n < 3; n++) add(nij * 8);                           // line factorisations
+    add((size_t)(2 * ctx->sor_nblk + 2) * 8); add((size_t)sJ * sN * 8);     // partials (+ the shift)
+    for(int n = 0; n < 6; n++) add((size_t)(sNM + 1) * sJ * 8);        // mode factorisations (Lc, Lc^T)
+    for(int n = 0; n < 6; n++) add(nij * 8);                           // line factorisations (Lc, Lc^T)
     add(fs * 4); add(fs * 4);
     ctx->mem_bytes = bytes;
     if(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess){
@@ -656,11 +694,14 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->sor_ctT = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_stT = carve<double>(cur, (size_t)(sNM + 1) * sN);
     ctx->sor_colR = carve<double>(cur, (size_t)sJ * sN);
     ctx->sor_Ac = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->sor_As = carve<double>(cur, (size_t)(sNM + 1) * sJ);
-    ctx->sor_part = carve<double>(cur, (size_t)2 * ctx->sor_nblk);
+    ctx->sor_part = carve<double>(cur, (size_t)2 * ctx->sor_nblk + 2);
     ctx->sor_q = carve<double>(cur, (size_t)sJ * sN);
     ctx->mlu_a = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->mlu_cf = carve<double>(cur, (size_t)(sNM + 1) * sJ);
     ctx->mlu_idn = carve<double>(cur, (size_t)(sNM + 1) * sJ);
     ctx->llu_a = carve<double>(cur, nij); ctx->llu_cf = carve<double>(cur, nij); ctx->llu_idn = carve<double>(cur, nij);
+    ctx->mluT_a = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->mluT_cf = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->mluT_idn = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->lluT_a = carve<double>(cur, nij); ctx->lluT_cf = carve<double>(cur, nij); ctx->lluT_idn = carve<double>(cur, nij);
     ctx->r32 = carve<float>(cur, fs); ctx->e32 = carve<float>(cur, fs);
     ctx->host_part.resize(2 * ctx->sor_nblk);
 
@@ -787,6 +828,26 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     std::vector<double> sct((size_t)(sNM + 1) * sN), sst((size_t)(sNM + 1) * sN);
     std::vector<double> sctT((size_t)(sNM + 1) * sN), sstT((size_t)(sNM + 1) * sN);
     std::vector<double> ma((size_t)(sNM + 1) * sJ), mcf((size_t)(sNM + 1) * sJ), midn((size_t)(sNM + 1) * sJ);
+    std::vector<double> maT(ma.size()), mcfT(ma.size()), midnT(ma.size());
+    // LU of a tridiagonal (sub A, diagonal B, super C) without pivoting: forward y_q = (d_q -
+    // A_q y_{q-1}) idn_q, back x_q = y_q - cf_q x_{q+1}; and the transpose's (sub and super swap
+    // and shift by one row).
+    auto factor = [](const std::vector<double>& A, const std::vector<double>& B, const std::vector<double>& Cc,
+                     double* fa, double* fc, double* fi, size_t stride){
+        const int n = (int)B.size();
+        for(int q = 0; q < n; q++){
+            const double dn = (q == 0) ? B[0] : B[q] - A[q] * fc[(q - 1) * stride];
+            fa[q * stride] = (q == 0) ? 0.0 : A[q]; fi[q * stride] = 1.0 / dn; fc[q * stride] = Cc[q] * fi[q * stride];
+        }
+    };
+    auto transpose3 = [](const std::vector<double>& A, const std::vector<double>& Cc,
+                         std::vector<double>& AT, std::vector<double>& CT){
+        const int n = (int)A.size();
+        for(int q = 0; q < n; q++){
+            AT[q] = (q == 0) ? 0.0 : Cc[q - 1];
+            CT[q] = (q == n - 1) ? 0.0 : A[q + 1];
+        }
+    };
     for(int m = 0; m <= sNM; m++){
         for(int k = 0; k < sN; k++){
             const double a = 2.0 * M_PI * (double)((long)m * k % sN) / sN;
@@ -804,16 +865,16 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
         }
         A[0] = 0.0;       B[0] += C43 * e;      Cc[0] -= C13 * e;
         Cc[sJ - 1] = 0.0; B[sJ - 1] += C43 * e; A[sJ - 1] -= C13 * e;
-        if(m == 0){ B[0] = 1.0; Cc[0] = 0.0; }                         // pin q at the first row
-        double* fa = &ma[(size_t)m * sJ]; double* fc = &mcf[(size_t)m * sJ]; double* fi = &midn[(size_t)m * sJ];
-        fa[0] = 0.0; fi[0] = 1.0 / B[0]; fc[0] = Cc[0] * fi[0];
-        for(int q = 1; q < sJ; q++){
-            const double dn = B[q] - A[q] * fc[q - 1];
-            fa[q] = A[q]; fi[q] = 1.0 / dn; fc[q] = Cc[q] * fi[q];
-        }
+        std::vector<double> AT(sJ), BT(B), CT(sJ);
+        transpose3(A, Cc, AT, CT);
+        if(m == 0){ B[0] = 1.0; Cc[0] = 0.0; BT[0] = 1.0; CT[0] = 0.0; }   // pin q at the first row
+        factor(A, B, Cc, &ma[(size_t)m * sJ], &mcf[(size_t)m * sJ], &midn[(size_t)m * sJ], 1);
+        factor(AT, BT, CT, &maT[(size_t)m * sJ], &mcfT[(size_t)m * sJ], &midnT[(size_t)m * sJ], 1);
     }
-    // radial-line tridiagonal of every (i,j) column of the folded operator, factored once
+    // radial-line tridiagonal of every (i,j) column of the folded operator, and of its transpose,
+    // factored once (row q of column j at index (q+1)*jm + j)
     std::vector<double> la(nij, 0.0), lcf(nij, 0.0), lidn(nij, 0.0);
+    std::vector<double> laT(nij, 0.0), lcfT(nij, 0.0), lidnT(nij, 0.0);
     for(int j = 1; j < g.jm - 1; j++){
         const int n = g.im - 2;
         std::vector<double> A(n), B(n), Cc(n);
@@ -826,12 +887,11 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
         }
         B[0] += A[0] * C43; Cc[0] -= A[0] * C13; A[0] = 0.0;
         B[n - 1] += Cc[n - 1] * C43; A[n - 1] -= Cc[n - 1] * C13; Cc[n - 1] = 0.0;
-        double cfp = 0.0;
-        for(int q = 0; q < n; q++){
-            const double dn = (q == 0) ? B[0] : B[q] - A[q] * cfp;
-            const size_t f = (size_t)(q + 1) * g.jm + j;
-            la[f] = A[q]; lidn[f] = 1.0 / dn; cfp = Cc[q] * lidn[f]; lcf[f] = cfp;
-        }
+        std::vector<double> AT(n), CT(n);
+        transpose3(A, Cc, AT, CT);
+        const size_t f0 = (size_t)g.jm + j;
+        factor(A, B, Cc, &la[f0], &lcf[f0], &lidn[f0], g.jm);
+        factor(AT, B, CT, &laT[f0], &lcfT[f0], &lidnT[f0], g.jm);
     }
     double A2y = 0.0;
     for(int i = 1; i < g.im - 1; i++){
@@ -869,6 +929,12 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     bad |= up(ctx->llu_a, la.data(), nij * 8);
     bad |= up(ctx->llu_cf, lcf.data(), nij * 8);
     bad |= up(ctx->llu_idn, lidn.data(), nij * 8);
+    bad |= up(ctx->mluT_a, maT.data(), maT.size() * 8);
+    bad |= up(ctx->mluT_cf, mcfT.data(), mcfT.size() * 8);
+    bad |= up(ctx->mluT_idn, midnT.data(), midnT.size() * 8);
+    bad |= up(ctx->lluT_a, laT.data(), nij * 8);
+    bad |= up(ctx->lluT_cf, lcfT.data(), nij * 8);
+    bad |= up(ctx->lluT_idn, lidnT.data(), nij * 8);
     std::vector<GeoIJ<float>> geo32;
     std::vector<float> cp32;
     if(ctx->mixed){
@@ -1089,6 +1155,40 @@ int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, dou
                           : run_sor<double>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, sweeps_done, resid);
     }
     return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
+}
+
+int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omega, int max_sweeps, double tol,
+                          const double* b, double* x, int* sweeps_done, double* resid){
+    if(!ctx || !b || !x) return ATURAN_E_INVALID;
+    if(sweeps_done) *sweeps_done = 0;
+    if(resid) *resid = 0.0;
+    if(kind != ATURAN_PRESS_RB_SOR && kind != ATURAN_PRESS_RB_LINE)
+        return fail(ctx, ATURAN_E_INVALID, "aturan_pressure_solve takes ATURAN_PRESS_RB_SOR or ATURAN_PRESS_RB_LINE");
+    const bool line = kind == ATURAN_PRESS_RB_LINE;
+    int rc = sor_check_sizes(ctx, omega, line); if(rc) return rc;
+    if(max_sweeps < 1) max_sweeps = 1;
+    const Grid g = ctx->g;
+    const size_t rows = (size_t)g.im * g.jm;
+    long nl = 0;
+    Region reg(ctx, ATURAN_K_RB, 0);
+    // working copies in the padded layout: the right-hand side in scratch, the iterate in stage64
+    CK(cudaMemcpy2DAsync(ctx->scratch, g.kp * 8, b, g.km * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpy2DAsync(ctx->stage64, g.kp * 8, x, g.km * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
+    sor_compat(ctx, ctx->scratch, transposed != 0);
+    CK_LAUNCH("solve right-hand side");
+    nl += 3;
+    int s = 0;
+    double r = 0.0;
+    const int status = transposed
+        ? solve_fp64<true>(ctx, ctx->stage64, ctx->scratch, omega, max_sweeps, tol, line, &s, &r, nl)
+        : solve_fp64<false>(ctx, ctx->stage64, ctx->scratch, omega, max_sweeps, tol, line, &s, &r, nl);
+    if(status < 0) return status;
+    CK(cudaMemcpy2DAsync(x, g.km * 8, ctx->stage64, g.kp * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    reg.n = nl;
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    return status;
 }
 
 int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol){

@@ -178,12 +178,10 @@ __device__ __forceinline__ void load_scalar(ScalarIn<C>& in, const StageArgs<S, 
     }
 }
 
-// Tendency and stage update of scalar field n from its loaded inputs (:790-913, :989-1018).
-template <typename S, typename C>
-__device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const ScalarIn<C>& in, int n, size_t o,
-                                              const GeoIJ<C>& geo, C u_ijk, C v_ijk, C w_ijk, C v_invrm,
-                                              C w_invrs, C nue_c, C nue_t_s){
-    const RhsConst<C>& K = a.k;
+// Tendency of scalar field n from its loaded inputs (:790-913, :989-1018).
+template <typename C>
+__device__ __forceinline__ C scalar_rhs(const RhsConst<C>& K, const ScalarIn<C>& in, int n, const GeoIJ<C>& geo,
+                                        C u_ijk, C v_ijk, C w_ijk, C v_invrm, C w_invrs, C nue_c, C nue_t_s){
     const int q = scalar_field(n);
     const D6<C> Q = diff6(K, in.v);
     if(n < 12){
@@ -194,26 +192,171 @@ __device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const Sc
         C r = - transport + diffusion / K.sc_re[n / 3] + diffusion * nue_t_s;
         if(q == ATURAN_H2S || q == ATURAN_NH3) r = r + K.chemical_reaction * in.f2;
         r = r + K.precip_coupling * in.f1;
-        stage_update(a, q, o, r, 0, in.an);
+        return r;
     } else if(n == 12){
         // ---- NH4SH: flux limiter, chemistry and Stokes settling (:852-913) ----
         const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
         const C diffusion = Q.d2r + Q.d1r * geo.two_inv_rm + Q.d2t * geo.inv_rm2
             + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
         const C v_stokes = K.stokes_a * (K.rho_cond_nh4sh - in.f3) * K.g / K.mue_mix;
-        const C r = - transport + in.f1
-                    + diffusion / K.sc_re[4] + diffusion * nue_t_s
-                    + K.chemical_reaction * in.f2
-                    + (v_stokes / K.u_0) * Q.d1r;
-        stage_update(a, q, o, r, 0, in.an);
+        return - transport + in.f1
+               + diffusion / K.sc_re[4] + diffusion * nue_t_s
+               + K.chemical_reaction * in.f2
+               + (v_stokes / K.u_0) * Q.d1r;
     } else {
         // ---- k* and dis* (:989-1018) ----
         const C transport = u_ijk * Q.d1r + v_ijk * Q.d1t * geo.inv_rm + w_ijk * Q.d1p * geo.inv_rmsinthe;
         const C diffusion = Q.d2r + Q.d1r * C(2.0) * geo.inv_rm + Q.d2t * geo.inv_rm2
             + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
         const C sig = n == 13 ? C(0.85) : C(0.5);
-        const C r = - transport + diffusion * (K.inv_re + nue_c / sig) + in.f1;
-        stage_update(a, q, o, r, n == 13 ? 2 : 3, in.an);
+        return - transport + diffusion * (K.inv_re + nue_c / sig) + in.f1;
+    }
+}
+__host__ __device__ constexpr int scalar_kind(int n){ return n < 13 ? 0 : (n == 13 ? 2 : 3); }
+
+template <typename S, typename C>
+__device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const ScalarIn<C>& in, int n, size_t o,
+                                              const GeoIJ<C>& geo, C u_ijk, C v_ijk, C w_ijk, C v_invrm,
+                                              C w_invrs, C nue_c, C nue_t_s){
+    const C r = scalar_rhs(a.k, in, n, geo, u_ijk, v_ijk, w_ijk, v_invrm, w_invrs, nue_c, nue_t_s);
+    stage_update(a, scalar_field(n), o, r, scalar_kind(n), in.an);
+}
+
+// ---- two cells per thread along k (the scalar launch's vectorised form) ----
+// Cells k0 and k0 + 1 (k0 even; km - 1 is even, so a pair never straddles the seam): the centre,
+// r and theta neighbours come as one 8-byte (FP32) or 16-byte (FP64) load each, the k neighbours
+// of the pair are the pair's own values plus one load on each side; accumulator, n-copy, forcing
+// and the stores are vector accesses too. Half the memory instructions and address arithmetic
+// per cell of the one-cell form, the same arithmetic per cell.
+template <typename S> struct Pair;
+template <> struct Pair<float>  { using T = float2; };
+template <> struct Pair<double> { using T = double2; };
+
+template <typename S, typename C>
+__device__ __forceinline__ void ld2(const S* p, C& x, C& y){
+    const typename Pair<S>::T v = __ldg(reinterpret_cast<const typename Pair<S>::T*>(p));
+    x = (C)v.x; y = (C)v.y;
+}
+template <typename S, typename C>
+__device__ __forceinline__ void ld2_rw(const S* p, C& x, C& y){      // memory this launch also writes
+    const typename Pair<S>::T v = *reinterpret_cast<const typename Pair<S>::T*>(p);
+    x = (C)v.x; y = (C)v.y;
+}
+template <typename S, typename C>
+__device__ __forceinline__ void st2(S* p, C x, C y){
+    typename Pair<S>::T v; v.x = (S)x; v.y = (S)y;
+    *reinterpret_cast<typename Pair<S>::T*>(p) = v;
+}
+
+template <typename C>
+struct ScalarIn2 { ScalarIn<C> c0, c1; };
+
+template <typename S, typename C>
+__device__ __forceinline__ void load_scalar2(ScalarIn2<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
+    const int q = scalar_field(n);
+    const size_t f = (size_t)q * nb.fs, o = nb.o;
+    ScalarIn<C>& A = in.c0;
+    ScalarIn<C>& B = in.c1;
+    ld2<S, C>(nb.X + f + o, A.v.c, B.v.c);
+    ld2<S, C>(nb.xip + f + nb.oip, A.v.rp, B.v.rp);
+    ld2<S, C>(nb.xim + f + nb.oim, A.v.rm, B.v.rm);
+    ld2<S, C>(nb.xjp + f + nb.ojp, A.v.tp, B.v.tp);
+    ld2<S, C>(nb.xjm + f + nb.ojm, A.v.tm, B.v.tm);
+    A.v.pw = (C)ld(nb.X + f + nb.okw);            // k0 - 1
+    B.v.pe = (C)ld(nb.X + f + nb.oke);            // k0 + 2
+    A.v.pe = B.v.c;
+    B.v.pw = A.v.c;
+    if(a.stage == 0){ A.an.acc = C(0.0); B.an.acc = C(0.0); }
+    else ld2_rw<S, C>(a.acc + f + o, A.an.acc, B.an.acc);
+    ld2<S, C>(a.Nc + f + o, A.an.nc, B.an.nc);
+    const S* F = a.forc + o;
+    const size_t fs = nb.fs;
+    A.f2 = B.f2 = C(0.0); A.f3 = B.f3 = C(0.0);
+    if(n < 12){
+        ld2<S, C>(F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs, A.f1, B.f1);
+        if(q == ATURAN_H2S) ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs, A.f2, B.f2);
+        if(q == ATURAN_NH3) ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs, A.f2, B.f2);
+    } else if(n == 12){
+        ld2<S, C>(F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs, A.f1, B.f1);
+        ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs, A.f2, B.f2);
+        ld2<S, C>(F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs, A.f3, B.f3);
+    } else {
+        ld2<S, C>(F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs, A.f1, B.f1);
+    }
+}
+
+// stage_update for the pair, with vector stores.
+template <typename S, typename C>
+__device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, int q, size_t o, C r0, C r1, int kind,
+                                              const AccNc<C>& n0, const AccNc<C>& n1){
+    const size_t off = (size_t)q * a.g.fstride + o;
+    C acc0, acc1;
+    if(a.stage == 0){ acc0 = a.wgt * r0; acc1 = a.wgt * r1; }
+    else { acc0 = n0.acc + a.wgt * r0; acc1 = n1.acc + a.wgt * r1; }
+    C y0, y1;
+    if(a.stage < 3){
+        st2<S, C>(a.acc + off, acc0, acc1);
+        y0 = n0.nc + a.c_in * r0; y1 = n1.nc + a.c_in * r1;
+        if(kind == 2){ y0 = cclamp(y0, C(0.0), a.k.tke_max); y1 = cclamp(y1, C(0.0), a.k.tke_max); }
+        else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
+    } else {
+        y0 = n0.nc + a.k.dt * acc0 / C(6.0); y1 = n1.nc + a.k.dt * acc1 / C(6.0);
+        if(kind == 1){ y0 = cclamp(y0, a.k.t_min, a.k.t_max); y1 = cclamp(y1, a.k.t_min, a.k.t_max); }
+        else if(kind == 2){ y0 = cclamp(cmax(y0, C(0.0)), C(0.0), a.k.tke_max); y1 = cclamp(cmax(y1, C(0.0)), C(0.0), a.k.tke_max); }
+        else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
+    }
+    st2<S, C>(a.Y + off, y0, y1);
+}
+
+// The scalar part of a stage (the fifteen scalar fields), two cells per thread; the same
+// arithmetic per cell, in the same order, as rk_stage_kernel<..., 2, ...>.
+template <typename S, typename C, int PD, int MINB>
+__global__ void __launch_bounds__(128, MINB) rk_scalar_pair_kernel(const StageArgs<S, C> a){
+    const Grid& g = a.g;
+    const int k = 2 * (blockIdx.x * 32 + threadIdx.x);
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<C>& K = a.k;
+    const GeoIJ<C> geo = a.geo[i * g.jm + j];
+    Nbr<S> nb;
+    nb.fs  = g.fstride;
+    nb.o   = gidx(g, i, j, k);
+    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
+    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
+    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
+    nb.oke = nb.o - k + phi_wrap(k + 2, g.km);
+    nb.X   = a.X;
+    nb.xim = (i == 1) ? a.St : a.X;
+    nb.xip = (i == g.im - 2) ? a.St : a.X;
+    nb.xjm = (j == 1) ? a.St : a.X;
+    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
+    const size_t o = nb.o, fs = g.fstride;
+    C nue0, nue1, u0, u1, v0, v1, w0, w1;
+    ld2<S, C>(a.forc + (size_t)(ATURAN_NUE - ATURAN_NUE) * fs + o, nue0, nue1);
+    ld2<S, C>(a.X + (size_t)ATURAN_U * fs + o, u0, u1);
+    ld2<S, C>(a.X + (size_t)ATURAN_V * fs + o, v0, v1);
+    ld2<S, C>(a.X + (size_t)ATURAN_W * fs + o, w0, w1);
+    auto nts = [&](C nue_c) -> C {
+        const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
+        return nue_t / C(0.9);
+    };
+    const C nts0 = nts(nue0), nts1 = nts(nue1);
+    const C vr0 = v0 * geo.inv_rm, vr1 = v1 * geo.inv_rm;
+    const C wr0 = w0 * geo.inv_rmsinthe, wr1 = w1 * geo.inv_rmsinthe;
+    const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
+    ScalarIn2<C> ring[PD + 1];
+#pragma unroll
+    for(int n = 0; n < PD; n++) if(n < nfield) load_scalar2(ring[n], a, nb, n);
+#pragma unroll
+    for(int n = 0; n < N_SCALARS; n++){
+        if(n + PD < nfield) load_scalar2(ring[(n + PD) % (PD + 1)], a, nb, n + PD);
+        if(n < nfield){
+            const ScalarIn2<C>& in = ring[n % (PD + 1)];
+            const C r0 = scalar_rhs(K, in.c0, n, geo, u0, v0, w0, vr0, wr0, nue0, nts0);
+            const C r1 = scalar_rhs(K, in.c1, n, geo, u1, v1, w1, vr1, wr1, nue1, nts1);
+            stage_update2(a, scalar_field(n), o, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
+        }
     }
 }
 

@@ -29,10 +29,9 @@ struct SatConst {
     int conserve, newton, evap, ice_entry, bergeron, dry_exit, local_rho;
 };
 
-// ATPhys.h:49-53, exp(C + (-L0 / T + a log T + b T) / den), with log(T) passed in: the liquid and
-// ice pressures at one T share it (the same value, so the same roundings, as computing it twice).
-__device__ __forceinline__ double svp_l(double T, double lgT, double C, double L0, double den, double a, double b){
-    return exp(C + (-L0 / T + a * lgT + b * T) / den);
+// ATPhys.h:49-53
+__device__ __forceinline__ double svp(double T, double C, double L0, double den, double a, double b){
+    return exp(C + (-L0 / T + a * log(T) + b * T) / den);
 }
 
 template <typename S>
@@ -104,8 +103,7 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                 if(ice < 0.0) ice = 0.0;
 
                 const double ep = G.ep, lv = G.lv, ls = G.ls, tri = G.t_range_inv;
-                const double lg0 = log(t_u);
-                const double q_Rain_0 = rho_c * ep * svp_l(t_u, lg0, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                const double q_Rain_0 = rho_c * ep * svp(t_u, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
                 bool go = q_Rain_0 > 0.0;                             // :422
                 if(go){
                     double q_entry = q_Rain_0;
@@ -113,15 +111,15 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                         const double cnd0 = t_u <= t_00 ? 0.0 : (t_u >= t_0 ? 1.0 : (t_u - t_00) * tri);
                         if(cnd0 < 1.0)
                             q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * rho_c * ep
-                                    * svp_l(t_u, lg0, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                                    * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
                     }
                     if(K.bergeron >= 2 && cloud <= 0.0 && ice <= 0.0 && t_u < t_0)
-                        q_entry = rho_c * ep * svp_l(t_u, lg0, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                        q_entry = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
                     if(c <= q_entry){                                 // :436-448
                         const double q_c0 = cloud, q_i0 = ice;
                         if(!K.evap || !K.conserve || (q_c0 <= 0.0 && q_i0 <= 0.0)) go = false;
                         else {
-                            const double q_Ice_0 = rho_c * ep * svp_l(t_u, lg0, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            const double q_Ice_0 = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
                             double q_t0;
                             if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
                             else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
@@ -169,9 +167,17 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                         if(q_c_b < 0.0) q_c_b = 0.0;
                         if(q_i_b < 0.0) q_i_b = 0.0;
 
-                        const double lgT = log(T);
-                        const double q_Rain = rho_c * ep * svp_l(T, lgT, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
-                        const double q_Ice  = rho_c * ep * svp_l(T, lgT, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                        // Which saturation pressures the closure below reads (1 liquid, 2 ice, 3 both):
+                        // the one it does not read is not computed (same values where read).
+                        auto need = [&](double Tx) -> int {
+                            if(q_c_b > 0.0 && q_i_b > 0.0) return 3;
+                            if(K.bergeron >= 2 && q_c_b <= 0.0 && q_i_b <= 0.0 && Tx < t_0) return 2;
+                            if(K.ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0) return 3;
+                            return (q_i_b == 0.0) ? 1 : 2;
+                        };
+                        const double q_Rain = rho_c * ep * svp(T, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                        const double q_Ice  = (need(T) & 2)
+                            ? rho_c * ep * svp(T, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u : 0.0;
                         q_rain_now = q_Rain;
                         if(q_c_b > 0.0 && q_i_b > 0.0)
                             q_v_hyp = (q_c_b * q_Rain + q_i_b * q_Ice) / (q_c_b + q_i_b);
@@ -204,9 +210,11 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                         if(K.dry_exit && K.conserve && q_c_b <= 0.0 && q_i_b <= 0.0 && q_v_b < q_v_hyp){ dry = true; break; }
                         if(K.newton){
                             const double dT = 0.1;
-                            const double Td = T + dT, lgTd = log(Td);
-                            const double q_Rain_d = rho_c * ep * svp_l(Td, lgTd, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
-                            const double q_Ice_d  = rho_c * ep * svp_l(Td, lgTd, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            const int nd = need(T);
+                            const double q_Rain_d = (nd & 1)
+                                ? rho_c * ep * svp(T + dT, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u : 0.0;
+                            const double q_Ice_d  = (nd & 2)
+                                ? rho_c * ep * svp(T + dT, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u : 0.0;
                             double q_hyp_d;
                             if(q_c_b > 0.0 && q_i_b > 0.0)
                                 q_hyp_d = (q_c_b * q_Rain_d + q_i_b * q_Ice_d) / (q_c_b + q_i_b);

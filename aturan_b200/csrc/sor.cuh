@@ -64,12 +64,44 @@ __device__ __forceinline__ double folded_acc(const Grid& g, const T* P, size_t o
          + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
 }
 
-// Residual r = src - Lc p of the folded operator: per (j,k) column its y-weighted sum over the
-// interior levels, and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
+// The transposed folded operator (the pressure solve's adjoint): the gather of every row's
+// coefficient on (i,j,k). Row (1,j,k) of Lc puts num1 (1 - c13) on (2,j,k) and nothing on
+// (0,j,k), so row (2,j,k) of Lc^T takes num1 (1 - c13) from (1,j,k); likewise at i = im-2 and in
+// theta at j = 1, jm-2, with the neighbouring row's own weights. The diagonal is Lc's.
+template <typename T>
+__device__ __forceinline__ double folded_accT(const Grid& g, const T* P, size_t o, int i, int j, int k,
+                                              const RBW* w, double* diag){
+    const size_t si = (size_t)g.jm * g.kp, sj = g.kp;
+    const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+    const RBW W = w[i * g.jm + j];
+    double d = W.den;
+    if(i == 1)        d -= C43 * W.num1;
+    if(i == g.im - 2) d -= C43 * W.num1;
+    if(j == 1)        d -= C43 * W.num2;
+    if(j == g.jm - 2) d -= C43 * W.num2;
+    *diag = d;
+    double acc = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+    if(i - 1 >= 1)        acc += w[(i - 1) * g.jm + j].num1 * (i - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - si];
+    if(i + 1 <= g.im - 2) acc += w[(i + 1) * g.jm + j].num1 * (i + 1 == g.im - 2 ? 1.0 - C13 : 1.0) * (double)P[o + si];
+    if(j - 1 >= 1)        acc += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
+    if(j + 1 <= g.jm - 2) acc += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
+    return acc;
+}
+
+// Row of Lc (TR = false) or Lc^T (TR = true): the off-diagonal sum, *diag the diagonal.
+template <bool TR, typename T>
+__device__ __forceinline__ double row_acc(const Grid& g, const T* P, size_t o, int i, int j, int k,
+                                          const RBW* w, double* diag){
+    if constexpr(TR) return folded_accT<T>(g, P, o, i, j, k, w, diag);
+    else return folded_acc<T>(g, P, o, i, j, k, w[i * g.jm + j], diag);
+}
+
+// Residual r = src - Lc p of the folded operator (or src - Lc^T p, TR): per (j,k) column its
+// y-weighted (TR: plain) sum over the interior levels, and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
 // groups; the groups' column sums are added in group order and the block's norms in a fixed tree
 // order, so the result is deterministic. P and src of type T (double: FP64 solve; float: the
 // correction solve of the mixed form).
-template <typename T>
+template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, const T* src, const RBW* w,
                                                          double* colR, double* part, int want_col){
     const int N = g.km - 1;
@@ -78,15 +110,15 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
     const int grp = threadIdx.y;
     double R = 0.0, rr = 0.0, ss = 0.0;
     if(k < N){
+#pragma unroll 5
         for(int i = 1 + grp; i < g.im - 1; i += 8){
-            const RBW W = w[i * g.jm + j];
             const size_t o = gidx(g, i, j, k);
             double diag;
-            const double acc = folded_acc<T>(g, P, o, i, j, k, W, &diag);
+            const double acc = row_acc<TR, T>(g, P, o, i, j, k, w, &diag);
             const double lc = acc - diag * (double)P[o];
             const double s = (double)src[o];
             const double r = s - lc;
-            R += ywt(i, 1, g.im - 2) * r;
+            R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
             rr += r * r;
             ss += s * s;
         }
@@ -111,17 +143,19 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
 }
 
 // The two transforms of the correction are small dense products (J x N by N x (N/2+1) and back),
-// so they run as one tiled FP64 product kernel: C(r,c) = scale * sum_k A1(r,k) B1(k,c)
-// [+ A2(r,k) B2(k,c)], every operand addressed by (row, column) strides. A block computes a 32 x 32
-// tile of C from 32-wide k-chunks of A and B staged in shared memory (rows padded to 33: no bank
-// conflicts); each operand tile is loaded along whichever of its two indices has unit stride.
-//   forward:  Ac^T = (colR / A2y) . ctT,   As^T = (colR / A2y) . stT   (ctT[k][m] = cos(2 pi m k/N))
+// so they run as one tiled FP64 product kernel computing P1 = A1 B1 and P2 = A2 B2 at once, every
+// operand addressed by (row, column) strides; it writes C1 = scale P1 and C2 = scale P2, or, with
+// no C2, C1 = scale (P1 + P2). A block computes a 32 x 32 tile from 32-wide k-chunks of the
+// operands staged in shared memory (rows padded to 33: no bank conflicts); each operand tile is
+// loaded along whichever of its two indices has unit stride.
+//   forward:  Ac^T = (colR / A2y) . ctT  and  As^T = (colR / A2y) . stT  (one launch, A shared)
 //   inverse:  q = Ac^T . ct + As^T . st,  Ac/As carrying the weights w_m / N (tridiagonal write-back)
 // ct/st are host-built with the (m k mod N) argument reduction of PressureSolver.h:614-617.
 struct MatRef { const double* p; long rs, cs; };      // element (r, c) at p[r * rs + c * cs]
 
 __device__ __forceinline__ void gemm_stage(double (*t)[33], const MatRef& A, int r0, int k0, int R, int K){
     const bool kfast = (A.cs == 1);
+#pragma unroll 4
     for(int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x){
         const int a = idx >> 5, b = idx & 31;          // b runs along the unit-stride index
         const int r = kfast ? a : b, k = kfast ? b : a;
@@ -131,34 +165,41 @@ __device__ __forceinline__ void gemm_stage(double (*t)[33], const MatRef& A, int
 }
 
 __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, MatRef A1, MatRef B1, MatRef A2,
-                                                       MatRef B2, double scale, double* C, long crs, long ccs){
-    __shared__ double sa[32][33], sb[32][33];           // sa[r][k], sb[c][k]
+                                                       MatRef B2, double scale, double* C1, double* C2,
+                                                       long crs, long ccs){
+    __shared__ double sa1[32][33], sb1[32][33], sa2[32][33], sb2[32][33];   // sa[r][k], sb[c][k]
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int npair = A2.p ? 2 : 1;
-    for(int pr = 0; pr < npair; pr++){
-        const MatRef& A = pr ? A2 : A1;
-        const MatRef& B = pr ? B2 : B1;
-        const MatRef Bt{B.p, B.cs, B.rs};               // B^T: (c, k)
-        for(int k0 = 0; k0 < K; k0 += 32){
-            gemm_stage(sa, A, r0, k0, M, K);
-            gemm_stage(sb, Bt, c0, k0, Nn, K);
-            __syncthreads();
+    const bool sharedA = (A2.p == A1.p && A2.rs == A1.rs && A2.cs == A1.cs);
+    const MatRef Bt1{B1.p, B1.cs, B1.rs}, Bt2{B2.p, B2.cs, B2.rs};   // B^T: (c, k)
+    double acc1[4] = {0.0, 0.0, 0.0, 0.0}, acc2[4] = {0.0, 0.0, 0.0, 0.0};
+    for(int k0 = 0; k0 < K; k0 += 32){
+        gemm_stage(sa1, A1, r0, k0, M, K);
+        if(!sharedA) gemm_stage(sa2, A2, r0, k0, M, K);
+        gemm_stage(sb1, Bt1, c0, k0, Nn, K);
+        gemm_stage(sb2, Bt2, c0, k0, Nn, K);
+        __syncthreads();
+        double (*a2)[33] = sharedA ? sa1 : sa2;
 #pragma unroll 8
-            for(int k = 0; k < 32; k++){
-                const double bv = sb[tx][k];
+        for(int k = 0; k < 32; k++){
+            const double b1 = sb1[tx][k], b2 = sb2[tx][k];
 #pragma unroll
-                for(int q = 0; q < 4; q++) acc[q] += sa[ty + 8 * q][k] * bv;
+            for(int q = 0; q < 4; q++){
+                acc1[q] += sa1[ty + 8 * q][k] * b1;
+                acc2[q] += a2[ty + 8 * q][k] * b2;
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
     const int c = c0 + tx;
 #pragma unroll
     for(int q = 0; q < 4; q++){
         const int r = r0 + ty + 8 * q;
-        if(r < M && c < Nn) C[(long)r * crs + (long)c * ccs] = scale * acc[q];
+        if(r < M && c < Nn){
+            const long off = (long)r * crs + (long)c * ccs;
+            if(C2){ C1[off] = scale * acc1[q]; C2[off] = scale * acc2[q]; }
+            else C1[off] = scale * (acc1[q] + acc2[q]);
+        }
     }
 }
 
@@ -167,7 +208,8 @@ __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, Mat
 // the ends folded with q0 = c43 q1 - c13 q2, factored on the host once per context (ModeLU). Every
 // row is diagonally dominant, so the factorisation needs no pivoting. Mode 0 is singular: its
 // source is made consistent with the left null vector (3/2, 1, ..., 1, 3/2), q pinned at the first
-// row, and q returned with zero weighted mean. The result is written back times the inverse
+// row, and q returned with zero weighted mean. For the transposed system (tr) the null vectors
+// swap: the source is made zero-sum and the pinned row alone fixes q's free multiple of y. The result is written back times the inverse
 // transform's weight w_m / N (w = 1 for m = 0 and m = N/2, else 2).
 //
 // A block takes pm modes (2 pm problems, problem t = 2 m + part): all of its threads stage the
@@ -175,7 +217,8 @@ __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, Mat
 // modes' factors as [q][m] (stride pm + 1); then one thread per problem runs the two dependent
 // recurrences on shared-memory latency, in place, and the block writes back. Shared memory:
 // 8 J (5 pm + 4) bytes.
-__global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pm){
+__global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pm,
+                                                          int tr){
     extern __shared__ double sm[];
     const int J = s.J, np = 2 * pm, ldr = np + 1, ldf = pm + 1;
     double* sd = sm;                                     // [J][ldr]
@@ -184,6 +227,7 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
     double* fi = fc + (size_t)J * ldf;
     const int nmode = s.NM + 1;
     const int m0 = blockIdx.x * pm;
+#pragma unroll 4
     for(int idx = threadIdx.x; idx < pm * J; idx += blockDim.x){
         const int lm = idx / J, q = idx - lm * J;
         const int m = m0 + lm;
@@ -206,9 +250,9 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
             const double* a = fa + lm;
             const double* cf = fc + lm;
             const double* idn = fi + lm;
-            if(m == 0){
+            if(m == 0){                                       // compatible with the left null vector
                 double yr = 0.0, ys = 0.0;
-                for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yr += wq * d[q * ldr]; ys += wq; }
+                for(int q = 0; q < J; q++){ const double wq = tr ? 1.0 : ywt(q, 0, J - 1); yr += wq * d[q * ldr]; ys += wq; }
                 const double sh = yr / ys;
                 for(int q = 0; q < J; q++) d[q * ldr] -= sh;
                 d[0] = 0.0;                                   // the pinned row
@@ -219,7 +263,7 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
             double x = d[(J - 1) * ldr];
 #pragma unroll 4
             for(int q = J - 2; q >= 0; q--){ x = d[q * ldr] - cf[q * ldf] * x; d[q * ldr] = x; }
-            if(m == 0){
+            if(m == 0 && !tr){                                // the free constant: zero y-weighted mean
                 double yq = 0.0, ys = 0.0;
                 for(int q = 0; q < J; q++){ const double wq = ywt(q, 0, J - 1); yq += wq * d[q * ldr]; ys += wq; }
                 const double sh = yq / ys;
@@ -241,7 +285,8 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
 }
 
 // Onto every interior level of the column: P[i][j][k] += q(j,k).
-template <typename T>
+// (TR: y_i q, the trial functions of the transposed system's correction.)
+template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf, T* P){
     const int N = g.km - 1;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -249,13 +294,14 @@ __global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf
     const int i = 1 + blockIdx.z;
     if(k >= N) return;
     const size_t o = gidx(g, i, j, k);
-    P[o] = (T)((double)P[o] + qbuf[(size_t)(j - 1) * N + k]);
+    const double q = qbuf[(size_t)(j - 1) * N + k];
+    P[o] = (T)((double)P[o] + (TR ? ywt(i, 1, g.im - 2) * q : q));
 }
 
 // Red-black SOR colour pass of the folded operator, Lc e = r, for T = double (the FP64 solve) or
 // float (the correction solve of the mixed form: e and r in FP32, the row assembled in FP64 and
 // rounded once).
-template <typename T>
+template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* R, const RBW* w, int colour, double omega){
     const int half = g.km / 2;
     const int k2 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -264,10 +310,9 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
     if(k2 >= half || j > g.jm - 2) return;
     const int k = 2 * k2 + ((i + j + colour) & 1);
     if(k > g.km - 2) return;
-    const RBW W = w[i * g.jm + j];
     const size_t o = gidx(g, i, j, k);
     double diag;
-    const double acc = folded_acc<T>(g, E, o, i, j, k, W, &diag);
+    const double acc = row_acc<TR, T>(g, E, o, i, j, k, w, &diag);
     const double e0 = (double)E[o];
     const double pn = (acc - (double)R[o]) / diag;
     E[o] = (T)(e0 + omega * (pn - e0));
@@ -279,18 +324,22 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
 // p += omega (p_line - p) -- the reference's PRESS_LINE (PressureSolver.h:497-570) on the folded
 // operator. The radial tridiagonal of each column (radial ends folded as :547-550) is factored on
 // the host: per (i,j) the row's sub-diagonal `la`, the factor `lcf` and the pivot reciprocal `lidn`
-// (the theta fold changes the diagonal on the first and last rows).
+// (the theta fold changes the diagonal on the first and last rows). TR relaxes Lc^T instead: the
+// transposed theta couplings and the host-factored transposed column tridiagonals.
 //
 // A block takes 32 columns of one colour in one row j. Its 8 warps form the right-hand sides of
 // all levels in parallel (coalesced along k, one level per warp at a time) into shared memory
-// [level][column]; warp 0 then runs the 32 columns' forward and back recurrences on
-// shared-memory latency, in place; all warps write the relaxed columns back. Shared memory:
-// (im - 2) * 32 doubles.
-template <typename T>
+// [level][column] and stage the row's factors beside them; warp 0 then runs the 32 columns'
+// forward and back recurrences entirely on shared-memory latency, in place; all warps write the
+// relaxed columns back. Shared memory: (im - 2) * 35 doubles.
+template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
                                                        const double* lcf, const double* lidn, int colour, double omega){
     extern __shared__ double ds[];
     const int n = g.im - 2;
+    double* fa = ds + (size_t)n * 32;                  // the row's factors by level
+    double* fc = fa + n;
+    double* fi = fc + n;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const int k2 = blockIdx.x * 32 + lane;
     const int j = 1 + blockIdx.y;
@@ -298,14 +347,26 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
     const bool valid = k2 < g.km / 2 && k <= g.km - 2;
     const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
     const size_t sj = g.kp;
+    for(int i = threadIdx.x; i < n; i += blockDim.x){
+        const size_t f = (size_t)(i + 1) * g.jm + j;
+        fa[i] = la[f]; fc[i] = lcf[f]; fi[i] = lidn[f];
+    }
+#pragma unroll 5
     for(int i = 1 + wp; i <= n; i += 8){
         double d = 0.0;
         if(valid){
             const RBW W = w[i * g.jm + j];
             const size_t o = gidx(g, i, j, k);
-            const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
-            const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
-            const double h = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+            double h;
+            if constexpr(TR){                          // the transposed theta couplings (folded_accT)
+                h = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+                if(j - 1 >= 1)        h += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
+                if(j + 1 <= g.jm - 2) h += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
+            } else {
+                const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
+                const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
+                h = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+            }
             d = h - (double)R[o];
         }
         ds[(i - 1) * 32 + lane] = d;
@@ -314,21 +375,20 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
     if(wp == 0){
         double yp = 0.0;
 #pragma unroll 4
-        for(int i = 1; i <= n; i++){
-            const size_t f = (size_t)i * g.jm + j;
-            yp = (ds[(i - 1) * 32 + lane] - la[f] * yp) * lidn[f];
-            ds[(i - 1) * 32 + lane] = yp;
+        for(int i = 0; i < n; i++){
+            yp = (ds[i * 32 + lane] - fa[i] * yp) * fi[i];
+            ds[i * 32 + lane] = yp;
         }
         double x = ds[(n - 1) * 32 + lane];
 #pragma unroll 4
-        for(int i = n - 1; i >= 1; i--){
-            const size_t f = (size_t)i * g.jm + j;
-            x = ds[(i - 1) * 32 + lane] - lcf[f] * x;
-            ds[(i - 1) * 32 + lane] = x;
+        for(int i = n - 2; i >= 0; i--){
+            x = ds[i * 32 + lane] - fc[i] * x;
+            ds[i * 32 + lane] = x;
         }
     }
     __syncthreads();
     if(valid){
+#pragma unroll 5
         for(int i = 1 + wp; i <= n; i += 8){
             const size_t o = gidx(g, i, j, k);
             const double p0 = (double)P[o];
@@ -362,16 +422,17 @@ __global__ void bc_p_kernel(Grid g, T* P){
     P[gidx(g, i, j, g.km - 1)] = P[gidx(g, i, j, 0)];
 }
 
-// Compatibility: per-block partial sums of y_i y_j src and y_i y_j over the interior.
-__global__ void __launch_bounds__(256) sor_ysum_kernel(Grid g, const double* src, double* part){
+// Compatibility: per-block partial sums of y_i y_j src and y_i y_j over the interior (plain: of
+// src and 1, the transposed operator's left null vector being the constant).
+__global__ void __launch_bounds__(256) sor_ysum_kernel(Grid g, const double* src, double* part, int plain){
     const int J = g.jm - 2, N = g.km - 1;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double a = 0.0, b = 0.0;
     if(c < J * N){
         const int j = 1 + c / N, k = c - (j - 1) * N;
-        const double yj = ywt(j, 1, g.jm - 2);
+        const double yj = plain ? 1.0 : ywt(j, 1, g.jm - 2);
         for(int i = 1; i < g.im - 1; i++){
-            const double y = ywt(i, 1, g.im - 2) * yj;
+            const double y = plain ? 1.0 : ywt(i, 1, g.im - 2) * yj;
             a += y * src[gidx(g, i, j, k)];
             b += y;
         }
@@ -386,15 +447,23 @@ __global__ void __launch_bounds__(256) sor_ysum_kernel(Grid g, const double* src
     if(threadIdx.x == 0){ part[2 * blockIdx.x] = sa[0]; part[2 * blockIdx.x + 1] = sb[0]; }
 }
 
-// src -= shift on the interior (the shift is read from device memory: no host round trip).
-__global__ void sor_shift_kernel(Grid g, double* src, const double* part, int nblk){
-    __shared__ double shift;
-    if(threadIdx.x == 0){
-        double a = 0.0, b = 0.0;
-        for(int n = 0; n < nblk; n++){ a += part[2 * n]; b += part[2 * n + 1]; }
-        shift = a / b;
-    }
+// The shift = sum(y y src) / sum(y y) from the partials, in a fixed tree order (one block).
+__global__ void __launch_bounds__(256) sor_shift_finish_kernel(const double* part, int nblk, double* shift){
+    __shared__ double sa[256], sb[256];
+    double a = 0.0, b = 0.0;
+    for(int n = threadIdx.x; n < nblk; n += 256){ a += part[2 * n]; b += part[2 * n + 1]; }
+    sa[threadIdx.x] = a; sb[threadIdx.x] = b;
     __syncthreads();
+    for(int st = 128; st > 0; st >>= 1){
+        if(threadIdx.x < st){ sa[threadIdx.x] += sa[threadIdx.x + st]; sb[threadIdx.x] += sb[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) *shift = sa[0] / sb[0];
+}
+
+// src -= shift on the interior (the shift is read from device memory: no host round trip).
+__global__ void sor_shift_kernel(Grid g, double* src, const double* shift_p){
+    const double shift = *shift_p;
     const int J = g.jm - 2, N = g.km - 1;
     for(int c = blockIdx.x * blockDim.x + threadIdx.x; c < J * N; c += gridDim.x * blockDim.x){
         const int j = 1 + c / N, k = c - (j - 1) * N;

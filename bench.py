@@ -381,8 +381,13 @@ def main():
 
     # ---- end to end through the C ABI with host buffers ----
     from aturan_b200 import fields as F
-    in_names = F.NAMES
-    out_names = F.PROGNOSTIC + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION
+    # what a CPU driver hands the drop-in every step (INTEGRATION.md's glue): the prognostic fields
+    # and the pointwise RHS inputs its CPU modules (chemistry, precipitation, turbulence closure,
+    # boundary conditions, filters) changed; the n-copies, p_dyn, p_hydro, p_bfollow and the
+    # constant fields stay resident. Back: the new prognostic fields, p_dyn, p_hydro and the
+    # projection fields.
+    in_names = F.PROGNOSTIC + F.FORCING
+    out_names = F.PROGNOSTIC + ["p_dyn", "p_hydro"] + F.PROJECTION
     pinned = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in in_names}
     outs = {n: torch.empty(p.shape, dtype=torch.float64).pin_memory() for n in out_names}
     barrier()
@@ -454,8 +459,9 @@ def main():
 
 def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
     """The mixed step against the FP64 step (which matches the FP64 oracle) from the same state:
-    per-field max |mixed - fp64| / max |fp64| over the interior after 1, 10 and 200 steps, and both
-    step times (CUDA events on each context's stream, median over steps 2..10)."""
+    per-field max |mixed - fp64| / max |fp64| over the interior after 1, 10 and 200 steps (and the
+    99.99th percentile of the same ratio over cells), and both step times (CUDA events on each
+    context's stream, median over steps 2..10)."""
     p64 = P.default_params(precision=P.FP64)
     p32 = P.default_params(precision=P.MIXED)
     st = S.synthetic_state(p64, seed=99)
@@ -482,12 +488,15 @@ def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
             if 2 <= done <= 10:
                 t64.append(a)
                 t32.append(b)
-        errs = {}
+        errs, p9999 = {}, {}
         for f in F.PROGNOSTIC + ["p_dyn"]:
             a, b = c32.download(f)[I], c64.download(f)[I]
             s = np.abs(b).max()
-            errs[f] = float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a - b).max())
+            d = np.abs(a - b) / (s if s > 0 else 1.0)
+            errs[f] = float(d.max())
+            p9999[f] = float(np.quantile(d, 0.9999))
         out[f"step{n}"] = errs
+        out[f"step{n}_p99.99"] = p9999
     c64.close()
     c32.close()
     m64, m32 = statistics.median(t64), statistics.median(t32)

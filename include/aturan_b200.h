@@ -202,6 +202,21 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
 int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
                     int* sweeps_done, double* resid);
 
+/* Solve the pressure equation's folded operator, or its transpose, on caller buffers: the linear
+ * solve inside ATURAN_PRESS_RB_SOR / RB_LINE, and with transposed = 1 the adjoint of that solve
+ * (no counterpart in the reference, which has no adjoint). b and x are device pointers to
+ * contiguous [im][jm][km] FP64 arrays; x holds the initial guess and receives the solution on the
+ * interior (i = 1..im-2, j = 1..jm-2, k = 0..km-2; its other entries are left as given).
+ *   transposed = 0: Lc x = b, b first made compatible by removing its component along Lc's left
+ *     null vector y_i y_j, y = (3/2, 1, ..., 1, 3/2); x is then defined up to a constant.
+ *   transposed = 1: Lc^T x = b, b first made zero-mean (Lc^T's left null vector is the constant);
+ *     x is defined up to a multiple of y_i y_j. For compatible s and g,
+ *     <solve(s), g> = <s, solve^T(g)>: the adjoint of the pressure solve.
+ * kind is ATURAN_PRESS_RB_SOR or ATURAN_PRESS_RB_LINE (as aturan_pressure, FP64 arithmetic in
+ * either context precision); ATURAN_NOT_CONVERGED at the cap. Synchronous. */
+int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omega, int max_sweeps, double tol,
+                          const double* b, double* x, int* sweeps_done, double* resid);
+
 /* The saturation adjustment of every gas whose bit is set in gas_mask (bit 0 H2O, 1 H2S, 2 NH3,
  * 3 CH4), in that order, fused per cell. Replaces the four
  * SaturationAdjustmentUran(m).run(...) calls of cUranusModel.cpp:998-1027 (and each one alone).

@@ -59,6 +59,9 @@ class Oracle:
             ("oracle_pressure_source", [P, vp, vp], ctypes.c_int),
             ("oracle_pressure_source_compat", [P, vp, vp], ctypes.c_int),
             ("oracle_pressure_residual", [P, vp, vp], ctypes.c_double),
+            ("oracle_laplace_apply", [P, vp, vp, ctypes.c_int], ctypes.c_int),
+            ("oracle_solve", [P, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                              vp, vp], ctypes.c_int),
             ("oracle_satadj", [P, vp, ctypes.c_int, vp, vp], ctypes.c_int),
             ("oracle_sync_ncopies", [P, vp], ctypes.c_int),
             ("oracle_step", [P, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
@@ -112,6 +115,23 @@ class Oracle:
         r = ctypes.c_double()
         rc = self.L.oracle_pressure_line(self._p(p), field_ptrs(state), float(omega), int(max_iter), float(tol),
                                          ctypes.addressof(s), ctypes.addressof(r))
+        return rc, s.value, r.value
+
+    def laplace_apply(self, p, x, transposed=False):
+        """Lc x or Lc^T x (the folded pressure operator) on the interior."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros(p.shape)
+        assert self.L.oracle_laplace_apply(self._p(p), x.ctypes.data, out.ctypes.data, int(transposed)) == 0
+        return out
+
+    def solve(self, p, b, x, transposed=False, line=True, omega=1.0, max_iter=200, tol=1e-10):
+        """Solve Lc x = b or Lc^T x = b (b made compatible), x updated in place; (rc, iters, resid)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        assert x.flags.c_contiguous and x.dtype == np.float64
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        rc = self.L.oracle_solve(self._p(p), b.ctypes.data, x.ctypes.data, int(transposed), int(line), float(omega),
+                                 int(max_iter), float(tol), ctypes.addressof(s), ctypes.addressof(r))
         return rc, s.value, r.value
 
     def pressure_source(self, p, state):

@@ -1137,6 +1137,264 @@ int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, 
     return r <= tol ? 0 : 1;
 }
 
+/* ---- The transposed folded operator, for the adjoint of the pressure solve (no reference
+ * counterpart: the reference has no adjoint). Lc^T has Lc's sparsity, so red-black point and line
+ * relaxation apply unchanged in structure; what changes is where the fold coefficients sit:
+ * row (1,j,k) of Lc puts num1 (1 - c13) on (2,j,k) and nothing on (0,j,k), so column (2,j,k) of
+ * Lc -- row (2,j,k) of Lc^T -- carries num1 (1 - c13) from (1,j,k); likewise at i = im-2 and in
+ * theta at j = 1, jm-2. The left null vector of Lc^T is the constant (Lc's rows sum to zero), so
+ * a right-hand side is made compatible by removing its plain mean. The coarse correction swaps
+ * the roles of the two radial null vectors: its trial functions are y_i q(j,k) (the radial block
+ * of Lc^T annihilates y, as y^T T_r = 0) and its test functions are the plain column sums (the
+ * constant annihilates it from the left, as T_r 1 = 0), so sum_i (Lc^T (y q))_i = A2y L2^T q
+ * exactly, A2y = sum_i y_i / rm_i^2. ---- */
+static double folded_accT(const aturan_params* p, const double* rad, const double* st, const double* L,
+                          int i, int j, int k, double* diag){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+    pweights_t w; press_weights(p, rad, st, i, j, &w);
+    double d = w.den;
+    if(i == 1)    d -= C43 * w.num1;
+    if(i == im-2) d -= C43 * w.num1;
+    if(j == 1)    d -= C43 * w.num2;
+    if(j == jm-2) d -= C43 * w.num2;
+    *diag = d;
+    double acc = (L[IDX(i,j,ke)] + L[IDX(i,j,kw)]) * w.num3;
+    pweights_t v;
+    if(i - 1 >= 1){ press_weights(p, rad, st, i-1, j, &v); acc += v.num1 * (i - 1 == 1 ? 1.0 - C13 : 1.0) * L[IDX(i-1,j,k)]; }
+    if(i + 1 <= im-2){ press_weights(p, rad, st, i+1, j, &v); acc += v.num1 * (i + 1 == im-2 ? 1.0 - C13 : 1.0) * L[IDX(i+1,j,k)]; }
+    if(j - 1 >= 1){ press_weights(p, rad, st, i, j-1, &v); acc += v.num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * L[IDX(i,j-1,k)]; }
+    if(j + 1 <= jm-2){ press_weights(p, rad, st, i, j+1, &v); acc += v.num2 * (j + 1 == jm-2 ? 1.0 - C13 : 1.0) * L[IDX(i,j+1,k)]; }
+    return acc;
+}
+
+/* out = Lc x (tr = 0) or Lc^T x (tr = 1) on the interior of a [im][jm][km] field. */
+int oracle_laplace_apply(const aturan_params* p, const double* x, double* out, int tr){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    memset(out, 0, sizeof(double) * (size_t)im * jm * km);
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++){
+        pweights_t w; press_weights(p, rad, st, i, j, &w);
+        for(int k = 0; k < km-1; k++){
+            double diag, acc;
+            if(tr) acc = folded_accT(p, rad, st, x, i, j, k, &diag);
+            else   acc = folded_acc(p, x, i, j, k, &w, &diag);
+            out[IDX(i,j,k)] = acc - diag * x[IDX(i,j,k)];
+        }
+    }
+    free(rad); free(the); free(st);
+    return 0;
+}
+
+static double residualT(const aturan_params* p, const double* rad, const double* st, const double* L, const double* g){
+    const int im = p->im, jm = p->jm, km = p->km;
+    double rr = 0.0, ss = 0.0;
+    #pragma omp parallel for collapse(2) reduction(+:rr,ss) schedule(static)
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++){
+        double diag;
+        const double acc = folded_accT(p, rad, st, L, i, j, k, &diag);
+        const double r = g[IDX(i,j,k)] - (acc - diag * L[IDX(i,j,k)]);
+        rr += r * r; ss += g[IDX(i,j,k)] * g[IDX(i,j,k)];
+    }
+    return ss > 0.0 ? sqrt(rr / ss) : sqrt(rr);
+}
+
+static void rbT_colour(const aturan_params* p, const double* rad, const double* st, double* L, const double* g,
+                       int colour, double omega){
+    const int im = p->im, jm = p->jm, km = p->km;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++){
+        if(((i + j + k) & 1) != colour) continue;
+        double diag;
+        const double acc = folded_accT(p, rad, st, L, i, j, k, &diag);
+        const double ln = (acc - g[IDX(i,j,k)]) / diag;
+        L[IDX(i,j,k)] += omega * (ln - L[IDX(i,j,k)]);
+    }
+}
+
+/* Line relaxation of Lc^T: per column the transposed radial tridiagonal (sub-diagonal from the
+ * row below's super-diagonal and the other way round), horizontal neighbours from the transposed
+ * theta and phi couplings. */
+static void lineT_colour(const aturan_params* p, const double* rad, const double* st, double* L, const double* g,
+                         int colour, double omega){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int n = im - 2;
+    #pragma omp parallel
+    {
+        double* aa = (double*)malloc(sizeof(double) * n);
+        double* bb = (double*)malloc(sizeof(double) * n);
+        double* cc = (double*)malloc(sizeof(double) * n);
+        double* dd = (double*)malloc(sizeof(double) * n);
+        #pragma omp for collapse(2) schedule(static)
+        for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++){
+            if(((j + k) & 1) != colour) continue;
+            const int kw = phi_wrap(k-1, km), ke = phi_wrap(k+1, km);
+            for(int i = 1; i < im-1; i++){
+                pweights_t w, v; press_weights(p, rad, st, i, j, &w);
+                double d = w.den;
+                if(i == 1)    d -= C43 * w.num1;
+                if(i == im-2) d -= C43 * w.num1;
+                if(j == 1)    d -= C43 * w.num2;
+                if(j == jm-2) d -= C43 * w.num2;
+                double h = (L[IDX(i,j,ke)] + L[IDX(i,j,kw)]) * w.num3;
+                if(j - 1 >= 1){ press_weights(p, rad, st, i, j-1, &v); h += v.num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * L[IDX(i,j-1,k)]; }
+                if(j + 1 <= jm-2){ press_weights(p, rad, st, i, j+1, &v); h += v.num2 * (j + 1 == jm-2 ? 1.0 - C13 : 1.0) * L[IDX(i,j+1,k)]; }
+                const int q = i - 1;
+                double sub = 0.0, sup = 0.0;
+                if(i - 1 >= 1){ press_weights(p, rad, st, i-1, j, &v); sub = -v.num1 * (i - 1 == 1 ? 1.0 - C13 : 1.0); }
+                if(i + 1 <= im-2){ press_weights(p, rad, st, i+1, j, &v); sup = -v.num1 * (i + 1 == im-2 ? 1.0 - C13 : 1.0); }
+                aa[q] = sub; bb[q] = d; cc[q] = sup;
+                dd[q] = h - g[IDX(i,j,k)];
+            }
+            cc[0] = cc[0] / bb[0];
+            dd[0] = dd[0] / bb[0];
+            for(int q = 1; q < n; q++){
+                const double dn = bb[q] - aa[q] * cc[q-1];
+                cc[q] = cc[q] / dn;
+                dd[q] = (dd[q] - aa[q] * dd[q-1]) / dn;
+            }
+            double x = dd[n-1];
+            L[IDX(n, j, k)] += omega * (x - L[IDX(n, j, k)]);
+            for(int q = n - 2; q >= 0; q--){
+                x = dd[q] - cc[q] * x;
+                L[IDX(q+1, j, k)] += omega * (x - L[IDX(q+1, j, k)]);
+            }
+        }
+        free(aa); free(bb); free(cc); free(dd);
+    }
+}
+
+/* The coarse correction of the transposed system: A2y L2^T q = sum_i r_i, then y_i q added to
+ * level i; per Fourier mode the transposed theta tridiagonal (the folds' c13 terms move to the
+ * neighbouring rows). Mode 0 is singular, left null vector 1 and right null vector y_j: its
+ * right-hand side is made zero-sum and q pinned at the first row (which fixes the multiple of y). */
+static void column_correction_T(const aturan_params* p, const double* rad, const double* st, double* L, const double* g){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int J = jm - 2, N = km - 1, NM = N / 2;
+    double* R  = (double*)calloc((size_t)J * N, sizeof(double));
+    double* Ac = (double*)calloc((size_t)(NM + 1) * J, sizeof(double));
+    double* As = (double*)calloc((size_t)(NM + 1) * J, sizeof(double));
+    double A2 = 0.0;
+    for(int i = 1; i < im-1; i++){ const double rm = metric_radius(p, rad[i]); A2 += ((i == 1 || i == im-2) ? 1.5 : 1.0) / (rm * rm); }
+    #pragma omp parallel for schedule(static)
+    for(int jj = 0; jj < J; jj++){
+        const int j = jj + 1;
+        for(int k = 0; k < N; k++){
+            double acc_r = 0.0;
+            for(int i = 1; i < im-1; i++){
+                double diag;
+                const double acc = folded_accT(p, rad, st, L, i, j, k, &diag);
+                acc_r += g[IDX(i,j,k)] - (acc - diag * L[IDX(i,j,k)]);
+            }
+            R[(size_t)jj * N + k] = acc_r;
+        }
+    }
+    const double e = 1.0 / (p->dthe * p->dthe), inv_dphi2 = 1.0 / (p->dphi * p->dphi);
+    #pragma omp parallel for schedule(static)
+    for(int m = 0; m <= NM; m++){
+        double* cp = (double*)malloc(sizeof(double) * J);
+        double* dp = (double*)malloc(sizeof(double) * J);
+        for(int jj = 0; jj < J; jj++){
+            double sc = 0.0, ss = 0.0;
+            for(int k = 0; k < N; k++){
+                const double a = 2.0 * M_PI * (double)((long)m * k % N) / N;
+                const double v = R[(size_t)jj * N + k] / A2;
+                sc += v * cos(a); ss += v * sin(a);
+            }
+            Ac[(size_t)m * J + jj] = sc; As[(size_t)m * J + jj] = ss;
+        }
+        const double sl = sin(M_PI * m / N);
+        const double lam = 4.0 * sl * sl * inv_dphi2;
+        for(int part = 0; part < 2; part++){
+            double* d = (part == 0 ? Ac : As) + (size_t)m * J;
+            if(part == 1 && (m == 0 || 2 * m == N)){ for(int q = 0; q < J; q++) d[q] = 0.0; continue; }
+            if(m == 0){
+                double sr = 0.0;
+                for(int q = 0; q < J; q++) sr += d[q];
+                for(int q = 0; q < J; q++) d[q] -= sr / J;
+            }
+            /* transposed rows: sub(q) = super_fwd(q-1), super(q) = sub_fwd(q+1) */
+            #define TA(q) ((q) == 0 ? 0.0 : ((q) == 1 ? e - C13 * e : e))
+            #define TB(q) (-2.0 * e - lam / (st[(q)+1] * st[(q)+1]) + (((q) == 0 || (q) == J-1) ? C43 * e : 0.0))
+            #define TC(q) ((q) == J-1 ? 0.0 : ((q) == J-2 ? e - C13 * e : e))
+            double b0 = TB(0), c0 = TC(0), d0 = d[0];
+            if(m == 0){ b0 = 1.0; c0 = 0.0; d0 = 0.0; }
+            cp[0] = c0 / b0; dp[0] = d0 / b0;
+            for(int q = 1; q < J; q++){
+                const double dn = TB(q) - TA(q) * cp[q-1];
+                cp[q] = TC(q) / dn;
+                dp[q] = (d[q] - TA(q) * dp[q-1]) / dn;
+            }
+            #undef TA
+            #undef TB
+            #undef TC
+            d[J-1] = dp[J-1];
+            for(int q = J-2; q >= 0; q--) d[q] = dp[q] - cp[q] * d[q+1];
+        }
+        free(cp); free(dp);
+    }
+    #pragma omp parallel for schedule(static)
+    for(int jj = 0; jj < J; jj++){
+        for(int k = 0; k < N; k++){
+            double q = 0.0;
+            for(int m = 0; m <= NM; m++){
+                const int edge = (m == 0 || 2 * m == N);
+                const double a = 2.0 * M_PI * (double)((long)m * k % N) / N;
+                q += (edge ? 1.0 : 2.0) * (Ac[(size_t)m * J + jj] * cos(a) + (edge ? 0.0 : As[(size_t)m * J + jj] * sin(a)));
+            }
+            q /= N;
+            for(int i = 1; i < im-1; i++) L[IDX(i, jj + 1, k)] += ((i == 1 || i == im-2) ? 1.5 : 1.0) * q;
+        }
+    }
+    free(R); free(Ac); free(As);
+}
+
+/* Solve Lc x = b (tr = 0) or Lc^T x = b (tr = 1) on the interior to a relative residual, by point
+ * (line = 0, check and correction every 16 sweeps) or line (line = 1, check every iteration,
+ * correction every 8) red-black SOR from the given x. b is first made compatible (its component
+ * along the operator's left null vector removed: y_i y_j for Lc, the constant for Lc^T); the
+ * boundary rows of x are not touched. Returns 0 at tol, 1 at the cap. */
+int oracle_solve(const aturan_params* p, const double* b_in, double* x, int tr, int line, double omega,
+                 int max_iter, double tol, int* iters_done, double* resid){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const size_t NF = (size_t)im * jm * km;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* st  = (double*)malloc(sizeof(double) * jm);
+    double* b   = (double*)malloc(sizeof(double) * NF);
+    oracle_coords(p, rad, the);
+    press_sin_table(p, the, st, 1);
+    memcpy(b, b_in, sizeof(double) * NF);
+    if(!tr) compat_shift(p, b);
+    else {
+        double sm = 0.0; long nn = 0;
+        for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++){ sm += b[IDX(i,j,k)]; nn++; }
+        for(int i = 1; i < im-1; i++) for(int j = 1; j < jm-1; j++) for(int k = 0; k < km-1; k++) b[IDX(i,j,k)] -= sm / nn;
+    }
+    const int check_every = line ? 1 : 16, every = line ? 8 : 16;
+    int s = 0;
+    double r = tr ? residualT(p, rad, st, x, b) : folded_residual(p, rad, st, x, b);
+    while(s < max_iter && !(r <= tol)){
+        if(s % every == 0){ if(tr) column_correction_T(p, rad, st, x, b); else column_correction(p, rad, st, x, b); }
+        for(int n = 0; n < check_every && s < max_iter; n++, s++){
+            for(int colour = 0; colour < 2; colour++){
+                if(tr){ if(line) lineT_colour(p, rad, st, x, b, colour, omega); else rbT_colour(p, rad, st, x, b, colour, omega); }
+                else  { if(line) line_colour(p, rad, st, x, b, colour, omega);  else rbf_colour(p, rad, st, x, b, colour, omega); }
+            }
+        }
+        r = tr ? residualT(p, rad, st, x, b) : folded_residual(p, rad, st, x, b);
+    }
+    if(iters_done) *iters_done = s;
+    if(resid) *resid = r;
+    free(rad); free(the); free(st); free(b);
+    return r <= tol ? 0 : 1;
+}
+
 /* ---- SaturationAdjustment.h:255-746 for one gas, the non-diagnostic arithmetic ---- */
 int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adjusted, long* n_noconv){
     const int im = p->im, jm = p->jm, km = p->km;

@@ -36,6 +36,9 @@ int oracle_pressure_sor(const aturan_params* p, double* const* f, double omega, 
 int oracle_pressure_line(const aturan_params* p, double* const* f, double omega, int max_iter,
                          double tol, int* iters_done, double* resid);
 double oracle_pressure_residual(const aturan_params* p, double* const* f, const double* src);
+int oracle_laplace_apply(const aturan_params* p, const double* x, double* out, int transposed);
+int oracle_solve(const aturan_params* p, const double* b, double* x, int transposed, int line, double omega,
+                 int max_iter, double tol, int* iters_done, double* resid);
 int oracle_pressure_source(const aturan_params* p, double* const* f, double* src);
 int oracle_pressure_source_compat(const aturan_params* p, double* const* f, double* src);
 int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adjusted, long* n_noconv);

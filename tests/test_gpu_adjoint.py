@@ -104,3 +104,71 @@ def test_adjoint_requires_tape_and_fp64():
     with pytest.raises(api.AturanError):
         cm.tape(True)
     cm.close()
+
+
+# ---- the pressure solve's adjoint: the transposed folded operator (aturan_pressure_solve) ----
+
+def _interior(p, rng):
+    a = np.zeros(p.shape)
+    a[1:-1, 1:-1, :-1] = rng.standard_normal((p.im - 2, p.jm - 2, p.km - 1))
+    return a
+
+
+@pytest.mark.parametrize("transposed", [False, True])
+@pytest.mark.parametrize("kind", [P.PRESS_RB_LINE, P.PRESS_RB_SOR])
+def test_pressure_solve_matches_oracle(oracle_lib, kind, transposed):
+    p = P.default_params(21, 37, 73)
+    rng = np.random.default_rng(71)
+    b = _interior(p, rng)
+    line = kind == P.PRESS_RB_LINE
+    om = 1.0 if line else 1.8
+    ctx = api.Context(p)
+    bd = torch.tensor(b, device="cuda")
+    xd = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc, its, res = ctx.pressure_solve(bd.data_ptr(), xd.data_ptr(), kind, transposed, om, 3000, 1e-10)
+    ctx.close()
+    x_ref = np.zeros(p.shape)
+    rc2, its2, res2 = oracle_lib.solve(p, b, x_ref, transposed, line, om, 3000, 1e-10)
+    assert rc == 0 and rc2 == 0 and res <= 1e-10
+    assert abs(its - its2) <= (1 if line else 16), (its, its2)
+    # the CPU operator's residual of the GPU solution, against the compatible right-hand side
+    I = (slice(1, -1), slice(1, -1), slice(0, -1))
+    x = xd.cpu().numpy()
+    Lx = oracle_lib.laplace_apply(p, x, transposed)[I]
+    if transposed:
+        bc = b[I] - b[I].mean()
+    else:
+        yi = np.ones(p.im); yi[[1, -2]] = 1.5
+        yj = np.ones(p.jm); yj[[1, -2]] = 1.5
+        W = (yi[:, None, None] * yj[None, :, None] * np.ones(p.km)[None, None, :])[I]
+        bc = b[I] - (W * b[I]).sum() / W.sum()
+    rel = np.linalg.norm(bc - Lx) / np.linalg.norm(bc)
+    assert rel <= 2e-10, rel
+
+
+@pytest.mark.parametrize("kind", [P.PRESS_RB_LINE, P.PRESS_RB_SOR])
+def test_pressure_adjoint_dot_product(kind):
+    """<Lc^-1 s, g> = <s, Lc^-T g> for compatible s, g on the GPU (41 x 91 x 181)."""
+    p = P.default_params(41, 91, 181)
+    rng = np.random.default_rng(72)
+    I = (slice(1, -1), slice(1, -1), slice(0, -1))
+    s, g = _interior(p, rng), _interior(p, rng)
+    yi = np.ones(p.im); yi[[1, -2]] = 1.5
+    yj = np.ones(p.jm); yj[[1, -2]] = 1.5
+    W = (yi[:, None, None] * yj[None, :, None] * np.ones(p.km)[None, None, :])[I]
+    s[I] -= (W * s[I]).sum() / W.sum()
+    g[I] -= g[I].mean()
+    om = 1.0 if kind == P.PRESS_RB_LINE else 1.8
+    ctx = api.Context(p)
+    sd, gd = torch.tensor(s, device="cuda"), torch.tensor(g, device="cuda")
+    xd = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    ld = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc1, _, _ = ctx.pressure_solve(sd.data_ptr(), xd.data_ptr(), kind, False, om, 5000, 1e-10)
+    rc2, _, _ = ctx.pressure_solve(gd.data_ptr(), ld.data_ptr(), kind, True, om, 5000, 1e-10)
+    ctx.close()
+    assert rc1 == 0 and rc2 == 0
+    x, lam = xd.cpu().numpy(), ld.cpu().numpy()
+    lhs, rhs = float((x[I] * g[I]).sum()), float((s[I] * lam[I]).sum())
+    assert abs(lhs - rhs) <= 1e-8 * abs(lhs), (lhs, rhs)

@@ -67,3 +67,44 @@ def test_step_with_converged_solvers_agree(oracle_lib, kind):
     for n in ("t", "u", "v", "w"):
         scale = np.abs(ref[n]).max()
         assert np.abs(got[n] - ref[n]).max() <= 1e-9 * scale, n
+
+
+# ---- the transposed operator and its solve (the pressure solve's adjoint) ----
+
+def _interior_random(p, rng):
+    a = np.zeros(p.shape)
+    a[1:-1, 1:-1, :-1] = rng.standard_normal((p.im - 2, p.jm - 2, p.km - 1))
+    return a
+
+
+def test_transposed_operator_is_the_transpose(oracle_lib):
+    p = P.default_params(13, 21, 33)
+    rng = np.random.default_rng(11)
+    x, y = _interior_random(p, rng), _interior_random(p, rng)
+    a = float((oracle_lib.laplace_apply(p, x) * y).sum())
+    b = float((x * oracle_lib.laplace_apply(p, y, transposed=True)).sum())
+    assert abs(a - b) <= 1e-13 * abs(a)
+
+
+@pytest.mark.parametrize("line", [True, False])
+def test_adjoint_solve_dot_product(oracle_lib, line):
+    """<Lc^-1 s, g> = <s, Lc^-T g> for compatible s and g: the transposed solve is the adjoint of
+    the forward solve (the free constant of p and the free multiple of y y of the adjoint solution
+    drop out against the compatible partners)."""
+    p = P.default_params(21, 37, 73)
+    rng = np.random.default_rng(12)
+    s, g = _interior_random(p, rng), _interior_random(p, rng)
+    x, lam = np.zeros(p.shape), np.zeros(p.shape)
+    om = 1.0 if line else 1.8
+    rc1, it1, _ = oracle_lib.solve(p, s, x, False, line, om, 3000, 1e-10)
+    rc2, it2, _ = oracle_lib.solve(p, g, lam, True, line, om, 3000, 1e-10)
+    assert rc1 == 0 and rc2 == 0
+    assert abs(it1 - it2) <= (1 if line else 16)           # same convergence for both systems
+    I = (slice(1, -1), slice(1, -1), slice(0, -1))
+    yi = np.ones(p.im); yi[[1, -2]] = 1.5
+    yj = np.ones(p.jm); yj[[1, -2]] = 1.5
+    W = (yi[:, None, None] * yj[None, :, None] * np.ones(p.km)[None, None, :])[I]
+    sc = s[I] - (W * s[I]).sum() / W.sum()
+    gc = g[I] - g[I].mean()
+    lhs, rhs = float((x[I] * gc).sum()), float((sc * lam[I]).sum())
+    assert abs(lhs - rhs) <= 1e-8 * abs(lhs), (lhs, rhs)
