@@ -40,10 +40,15 @@ SIGNATURES = {
     "aturan_download_buoy_ref": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_rk4_step": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_tape": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_restore_ncopies": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
     "aturan_pressure_solve": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                               ctypes.c_int),
     "aturan_rk4_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_rk4_adjoint_ex": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                              ctypes.c_int),
+    "aturan_pressure_adjoint": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_pressure": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                          ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_satadj": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -164,6 +169,10 @@ class Context:
     def rk4_step(self):
         self._check(self.L.aturan_rk4_step(self.h), "rk4_step")
 
+    def restore_ncopies(self, coeff=1.0):
+        """aturan_restore_ncopies: the reference's restoreVar(coeff) after a step."""
+        self._check(self.L.aturan_restore_ncopies(self.h, float(coeff)), "restore_ncopies")
+
     def tape(self, on=True):
         """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""
         self._check(self.L.aturan_tape(self.h, 1 if on else 0), "tape")
@@ -173,6 +182,24 @@ class Context:
         yb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
         xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
         self._check(self.L.aturan_rk4_adjoint(self.h, yb, xb), "rk4_adjoint")
+
+    def rk4_adjoint_ex(self, ybar_ptrs, auxbar_ptrs, xbar_ptrs, pbar_ptr):
+        """aturan_rk4_adjoint_ex: auxbar_ptrs (3, or None) in, pbar_ptr (or None) out."""
+        yb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
+        xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
+        ab = (ctypes.c_void_p * 3)(*[ctypes.c_void_p(int(x)) for x in auxbar_ptrs]) if auxbar_ptrs else None
+        self._check(self.L.aturan_rk4_adjoint_ex(self.h, yb, ab, xb, ctypes.c_void_p(int(pbar_ptr)) if pbar_ptr else None),
+                    "rk4_adjoint_ex")
+
+    def pressure_adjoint(self, pbar_ptr, auxbar_ptrs, kind=3, omega=1.0, max_sweeps=200, tol=1e-10):
+        """aturan_pressure_adjoint; (rc, sweeps, resid)."""
+        ab = (ctypes.c_void_p * 3)(*[ctypes.c_void_p(int(x)) for x in auxbar_ptrs])
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        rc = self._check(self.L.aturan_pressure_adjoint(self.h, int(kind), float(omega), int(max_sweeps), float(tol),
+                                                        ctypes.c_void_p(int(pbar_ptr)), ab, ctypes.byref(s),
+                                                        ctypes.byref(r)), "pressure_adjoint")
+        return rc, s.value, r.value
 
     def pressure_solve(self, b_ptr, x_ptr, kind=3, transposed=False, omega=1.0, max_sweeps=200, tol=1e-10):
         """aturan_pressure_solve on device pointers: Lc x = b (or Lc^T x = b); (rc, sweeps, resid)."""

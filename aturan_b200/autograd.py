@@ -76,3 +76,107 @@ class DryRK4Step(torch.autograd.Function):
 
 
 assert all(n in F.ID for n in DRY + tuple(n + "n" for n in DRY) + _RESTORE)
+
+
+AUX = ("aux_u", "aux_v", "aux_w")
+
+
+class DryFullStepper(DryStepper):
+    """One full dry step with the pressure solve inside: (t, u, v, w, aux_u, aux_v, aux_w) ->
+    the same after it. The step solves the pressure equation from the aux fields (the projection
+    outputs of the previous step's RK4) with kind/omega/tol (RB_SOR or RB_LINE, from p_dyn = 0 so
+    that the result does not depend on an earlier call) and runs the RK4 step, whose stage 3
+    writes the next aux. The saturation adjustment is the identity on a dry state and is not run.
+    Backward: aturan_rk4_adjoint_ex (the state's and p_dyn's adjoints from the outputs', the aux
+    outputs' adjoint entering at stage 3), then aturan_pressure_adjoint (p_dyn's adjoint back to
+    the aux inputs'). Only the aux interior enters the next solve; boundary rows get no gradient."""
+
+    def __init__(self, ctx, kind=3, omega=1.0, max_sweeps=200, tol=1e-10):
+        super().__init__(ctx)
+        self.press = (kind, omega, max_sweeps, tol)
+        self.zero = torch.zeros(self.shape, dtype=torch.float64, device="cuda")
+
+    def forward(self, xs, aux):
+        ctx = self.ctx
+        xs = [x.detach().contiguous() for x in xs]
+        aux = [a.detach().contiguous() for a in aux]
+        torch.cuda.synchronize()
+        for n, t in self.saved.items():
+            ctx.upload_device(n, t.data_ptr())
+        ctx.upload_device("p_dyn", self.zero.data_ptr())
+        for n, x in zip(DRY, xs):
+            ctx.upload_device(n, x.data_ptr())
+            ctx.upload_device(n + "n", x.data_ptr())
+        for n, a in zip(AUX, aux):
+            ctx.upload_device(n, a.data_ptr())
+        kind, omega, ms, tol = self.press
+        ctx.pressure(kind, omega=omega, max_sweeps=ms, tol=tol)
+        ctx.rk4_step()
+        self.n_forward += 1
+        out = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in DRY + AUX]
+        for n, o in zip(DRY + AUX, out):
+            ctx.download_device(n, o.data_ptr())
+        return out[:4], out[4:]
+
+    def backward(self, ybar, auxbar):
+        z = lambda g: torch.zeros(self.shape, dtype=torch.float64, device="cuda") if g is None else g.contiguous()
+        ybar = [z(g) for g in ybar]
+        auxbar = [z(g) for g in auxbar]
+        xbar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in DRY]
+        pbar = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        abar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in AUX]
+        torch.cuda.synchronize()
+        self.ctx.rk4_adjoint_ex([g.data_ptr() for g in ybar], [g.data_ptr() for g in auxbar],
+                                [x.data_ptr() for x in xbar], pbar.data_ptr())
+        kind, omega, ms, tol = self.press
+        self.ctx.pressure_adjoint(pbar.data_ptr(), [a.data_ptr() for a in abar], kind, omega, ms, tol)
+        return xbar, abar
+
+
+class DryFullStep(torch.autograd.Function):
+    """t1, u1, v1, w1, au1, av1, aw1 = DryFullStep.apply(stepper, t, u, v, w, au, av, aw)."""
+
+    @staticmethod
+    def forward(fctx, stepper, t, u, v, w, au, av, aw):
+        fctx.stepper = stepper
+        xs, aux = stepper.forward([t, u, v, w], [au, av, aw])
+        fctx.step_id = stepper.n_forward
+        return tuple(xs + aux)
+
+    @staticmethod
+    def backward(fctx, *gr):
+        if fctx.step_id != fctx.stepper.n_forward:
+            raise RuntimeError("DryFullStep: the tape holds a later step; run backward before the next forward")
+        xbar, abar = fctx.stepper.backward(list(gr[:4]), list(gr[4:]))
+        return (None, *xbar, *abar)
+
+
+def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn):
+    """Loss after nsteps DryFullStepper steps from (xs0, aux0) and its gradient with respect to
+    xs0 and aux0, by the hand-written adjoint with checkpointing: the forward keeps the inputs of
+    every `every`-th step; the backward recomputes a segment's step inputs from its checkpoint,
+    then re-runs each step (which tapes it) right before its adjoint, last step first. Memory:
+    (nsteps / every + every) step inputs; cost about three forward passes plus the adjoints.
+    loss_fn maps the final (t, u, v, w) to a scalar tensor (differentiated by torch.autograd)."""
+    ck = {0: ([x.detach() for x in xs0], [a.detach() for a in aux0])}
+    xs, aux = ck[0]
+    with torch.no_grad():
+        for n in range(nsteps):
+            xs, aux = stepper.forward(xs, aux)
+            if (n + 1) % every == 0 and n + 1 < nsteps:
+                ck[n + 1] = (xs, aux)
+    xf = [x.detach().requires_grad_(True) for x in xs]
+    loss = loss_fn(xf)
+    ybar = list(torch.autograd.grad(loss, xf, allow_unused=True))
+    ybar = [torch.zeros_like(x) if g is None else g for x, g in zip(xf, ybar)]
+    abar = [torch.zeros_like(a) for a in aux]
+    for start in sorted(ck, reverse=True):
+        end = min(start + every, nsteps)
+        inputs = [ck[start]]
+        with torch.no_grad():
+            for _ in range(start, end - 1):
+                inputs.append(stepper.forward(*inputs[-1]))
+        for n in reversed(range(start, end)):
+            stepper.forward(*inputs[n - start])            # tapes step n
+            ybar, abar = stepper.backward(ybar, abar)
+    return loss.detach(), ybar, abar

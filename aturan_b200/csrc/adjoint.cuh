@@ -24,13 +24,17 @@
 namespace aturan {
 
 constexpr int ADJ_NF = 4;                          // t, u, v, w (state fields 0..3)
-constexpr int ADJ_SLOTS = 7 * ADJ_NF + 4;          // per field rp, rm, tp, tm, pe, pw, c; p_hydro tp, tm, pe, pw
+constexpr int ADJ_SLOT_PH = 7 * ADJ_NF;            // p_hydro tp, tm, pe, pw
+constexpr int ADJ_SLOT_PD = ADJ_SLOT_PH + 4;       // p_dyn rp, rm, tp, tm, pe, pw
+constexpr int ADJ_SLOTS = ADJ_SLOT_PD + 6;         // per field rp, rm, tp, tm, pe, pw, c; then p_hydro, p_dyn
 
 struct AdjArgs {
     Grid g;
     const double* X;            // stage input, field q (0..3) at X + q * fstride
     const double* X0;           // the step's input (boundary rows of every stage input)
     const double* kbar;         // adjoint of the stage's tendencies, field q at kbar + q * fstride
+    const double* auxbar;       // stage 3 only, else null: adjoint of aux_u, aux_v, aux_w (the tendencies
+                                // of u, v, w without the p_dyn gradient, RHS_Uran_Turb.cpp:1020-1022)
     const double* pdyn;
     const double* forc;         // forcing group (nue at offset 0)
     const GeoIJ<double>* geo;
@@ -107,8 +111,13 @@ __global__ void __launch_bounds__(128) adj_local_kernel(const AdjArgs a){
     const double nue_c = ld(a.forc + o);
     const double nue_t = (K.turb_coupling != 0.0 && isfinite(nue_c)) ? K.turb_coupling * cmax(0.0, nue_c) : 0.0;
     const double nue_t_s = nue_t / 0.9;
-    const double at = a.kbar[0 * fs + o], au = a.kbar[1 * fs + o];
-    const double av = a.kbar[2 * fs + o], aw = a.kbar[3 * fs + o];
+    const double at = a.kbar[0 * fs + o];
+    const double au0 = a.kbar[1 * fs + o], av0 = a.kbar[2 * fs + o], aw0 = a.kbar[3 * fs + o];
+    // aux = the tendency without the p_dyn gradient: its adjoint joins the tendency's in every
+    // partial except those in p_dyn
+    const double au = au0 + (a.auxbar ? a.auxbar[0 * fs + o] : 0.0);
+    const double av = av0 + (a.auxbar ? a.auxbar[1 * fs + o] : 0.0);
+    const double aw = aw0 + (a.auxbar ? a.auxbar[2 * fs + o] : 0.0);
 
     const double u = U.c, v = V.c, w = W.c;
     const double inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rs = geo.inv_rmsinthe;
@@ -167,18 +176,30 @@ __global__ void __launch_bounds__(128) adj_local_kernel(const AdjArgs a){
     put7(a.slot, fs, o, 2, gV, dv, K);
     put7(a.slot, fs, o, 3, gW, dw, K);
     // p_hydro: rhs_v -= (ph[j+1] - ph[j-1]) inv_2dthe inv_rm, rhs_w -= (ph[k+1] - ph[k-1]) inv_2dphi inv_rs
-    double* S = a.slot + (size_t)7 * ADJ_NF * fs + o;
+    double* S = a.slot + (size_t)ADJ_SLOT_PH * fs + o;
     S[0 * fs] = -av * K.inv_2dthe * inv_rm;   // to (j+1)
     S[1 * fs] =  av * K.inv_2dthe * inv_rm;   // to (j-1)
     S[2 * fs] = -aw * K.inv_2dphi * inv_rs;   // to (k+1)
     S[3 * fs] =  aw * K.inv_2dphi * inv_rs;   // to (k-1)
+    // p_dyn: rhs_u -= dpdr scale_p, rhs_v -= dpdthe scale_p inv_rm, rhs_w -= dpdphi scale_p inv_rs,
+    // rhs_t += ce_sp (u dpdr + v inv_rm dpdthe + w inv_rs dpdphi) cpf (aux carries none of it)
+    const double gdr = -K.scale_p * au0 + K.ce_sp * u * cpf * at;
+    const double gdt = -K.scale_p * inv_rm * av0 + K.ce_sp * v * inv_rm * cpf * at;
+    const double gdp = -K.scale_p * inv_rs * aw0 + K.ce_sp * w * inv_rs * cpf * at;
+    double* Q = a.slot + (size_t)ADJ_SLOT_PD * fs + o;
+    Q[0 * fs] =  gdr * K.inv_2dr;             // to (i+1)
+    Q[1 * fs] = -gdr * K.inv_2dr;             // to (i-1)
+    Q[2 * fs] =  gdt * K.inv_2dthe;           // to (j+1)
+    Q[3 * fs] = -gdt * K.inv_2dthe;           // to (j-1)
+    Q[4 * fs] =  gdp * K.inv_2dphi;           // to (k+1)
+    Q[5 * fs] = -gdp * K.inv_2dphi;           // to (k-1)
 }
 
 // Per cell (every row, every meridian; the seam copy k = km-1 is read by no stencil and receives
 // nothing): the sum of what the cells whose stencils contain it sent, in a fixed order. Adds the
 // result into ybar and phbar; for s > 0 also forms the previous stage's kbar on the interior.
 __global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* slot, double* ybar, double* phbar,
-                                                         const double* g0, double* kbar, double w_prev,
+                                                         double* pdbar, const double* g0, double* kbar, double w_prev,
                                                          double c_prev, int has_prev){
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -201,19 +222,28 @@ __global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* s
         ybar[q * fs + o] += x;
         if(has_prev && interior) kbar[q * fs + o] = w_prev * g0[q * fs + o] + c_prev * x;
     }
-    const double* S = slot + (size_t)7 * ADJ_NF * fs;
+    const double* S = slot + (size_t)ADJ_SLOT_PH * fs;
     double h = 0.0;
     if(j >= 1)        h += S[0 * fs + o - sj];
     if(j <= g.jm - 2) h += S[1 * fs + o + sj];
     h += S[2 * fs + okw];
     h += S[3 * fs + oke];
     phbar[o] += h;
+    const double* Q = slot + (size_t)ADJ_SLOT_PD * fs;
+    double pd = 0.0;
+    if(i >= 1)        pd += Q[0 * fs + o - si];
+    if(i <= g.im - 2) pd += Q[1 * fs + o + si];
+    if(j >= 1)        pd += Q[2 * fs + o - sj];
+    if(j <= g.jm - 2) pd += Q[3 * fs + o + sj];
+    pd += Q[4 * fs + okw];
+    pd += Q[5 * fs + oke];
+    pdbar[o] += pd;
 }
 
 // The final update's adjoint: g = ybar' (times 0 where T' was clamped), ybar = g, kbar_3 =
 // dt/6 w_3 g on the interior. ybar_in is the caller's adjoint of the step's output.
 __global__ void adj_init_kernel(Grid g, const double* ybar_in, const double* t_out, double t_min, double t_max,
-                                double w3, double* g0, double* ybar, double* kbar, double* phbar){
+                                double w3, double* g0, double* ybar, double* kbar, double* phbar, double* pdbar){
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     const int i = blockIdx.z;
@@ -230,6 +260,7 @@ __global__ void adj_init_kernel(Grid g, const double* ybar_in, const double* t_o
         kbar[q * fs + o] = interior ? w3 * v : 0.0;
     }
     phbar[o] = 0.0;
+    pdbar[o] = 0.0;
 }
 
 // Hydrostatic integral's adjoint, per column (RungeKutta_Uran_Turb.cpp:62-177): p_hydro(i) =
@@ -311,6 +342,88 @@ __global__ void adj_level_apply_kernel(Grid g, const double* t, const double* ps
     const double b = h.g * ps[o] / (h.rR * T * h.t_ref);
     if(!isfinite(b)) return;
     ybar[o] += lev[2 * m] / lev[2 * m + 1] * wsin[j] * (-b / T);
+}
+
+// ---- The pressure step's adjoint (RB_SOR / RB_LINE path): p_dyn = F(solve(compat(clamp(div aux))))
+// with F the boundary passes. Reverse: F^T, the transposed solve, compat^T, the clamp mask, div^T. ----
+
+// F^T in reverse order of launch_pdyn_bcs: seam copy, theta folds (every level), radial folds.
+__global__ void adj_pbc_p_kernel(Grid g, double* B){
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= g.im * g.jm) return;
+    const int i = c / g.jm, j = c - i * g.jm;
+    B[gidx(g, i, j, 0)] += B[gidx(g, i, j, g.km - 1)];
+    B[gidx(g, i, j, g.km - 1)] = 0.0;
+}
+__global__ void adj_pbc_t_kernel(Grid g, double* B){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if(k >= g.km) return;
+    const double b0 = B[gidx(g, i, 0, k)], bn = B[gidx(g, i, g.jm - 1, k)];
+    B[gidx(g, i, 0, k)] = 0.0; B[gidx(g, i, g.jm - 1, k)] = 0.0;
+    B[gidx(g, i, 1, k)] += C43 * b0;        B[gidx(g, i, 2, k)] -= C13 * b0;
+    B[gidx(g, i, g.jm - 2, k)] += C43 * bn; B[gidx(g, i, g.jm - 3, k)] -= C13 * bn;
+}
+__global__ void adj_pbc_r_kernel(Grid g, double* B){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if(k >= g.km) return;
+    const double b0 = B[gidx(g, 0, j, k)], bn = B[gidx(g, g.im - 1, j, k)];
+    B[gidx(g, 0, j, k)] = 0.0; B[gidx(g, g.im - 1, j, k)] = 0.0;
+    B[gidx(g, 1, j, k)] += C43 * b0;        B[gidx(g, 2, j, k)] -= C13 * b0;
+    B[gidx(g, g.im - 2, j, k)] += C43 * bn; B[gidx(g, g.im - 3, j, k)] -= C13 * bn;
+}
+
+// compat^T: the forward subtracts the constant (sum w src) / (sum w) from the interior source
+// (w = y_i y_j), so its transpose maps lam to lam - w (sum lam) / (sum w); `mean` holds
+// sum lam / n_interior and ratio = n_interior / sum w. Then the clamp mask from the forward's
+// clamped source.
+__global__ void adj_compat_mask_kernel(Grid g, const double* lam, const double* mean, double ratio,
+                                       const double* src_fwd, const RBW* w, double* sbar){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2) return;
+    const size_t o = gidx(g, i, j, k);
+    const double wy = ywt(i, 1, g.im - 2) * ywt(j, 1, g.jm - 2);
+    const double v = lam[o] - wy * ratio * (*mean);
+    const double s = src_fwd[o];
+    const bool free_ = fabs(s) < w[i * g.jm + j].src_max;   // not clamped (clamped values sit at the bound)
+    sbar[o] = free_ ? v : 0.0;
+}
+
+// div^T (rb_src_kernel): src(i,j,k) = (au[i+1] - au[i-1]) inv_2dr + (av[j+1] - av[j-1]) inv_2dthe inv_rm
+// + (aw[k+1] - aw[k-1]) inv_2dphi inv_rmsinthe, with au = 0 on the radial boundary rows (rigid lid)
+// or cubically extrapolated from the interior, and av = 0 on the polar rows (Pressure_Uran.cpp:30-146).
+__global__ void adj_div_kernel(Grid g, const double* sbar, const RBW* w, PressConst c, int rigid_lid,
+                               double* aub, double* avb, double* awb){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int i = blockIdx.z;
+    if(k >= g.km) return;
+    const size_t o = gidx(g, i, j, k);
+    const bool inner = i >= 1 && i <= g.im - 2 && j >= 1 && j <= g.jm - 2 && k <= g.km - 2;
+    double u = 0.0, v = 0.0, ww = 0.0;
+    if(inner){
+        const size_t si = (size_t)g.jm * g.kp, sj = g.kp;
+        if(i - 1 >= 1)        u += sbar[o - si] * c.inv_2dr;
+        if(i + 1 <= g.im - 2) u -= sbar[o + si] * c.inv_2dr;
+        if(!rigid_lid){       // au[0] = au[3] - 3 au[2] + 3 au[1], au[im-1] likewise (reads of the rows 1, im-2)
+            const double b0 = -sbar[gidx(g, 1, j, k)] * c.inv_2dr;        // adjoint of au[0]
+            const double bn =  sbar[gidx(g, g.im - 2, j, k)] * c.inv_2dr; // adjoint of au[im-1]
+            if(i == 1) u += 3.0 * b0;
+            if(i == 2) u -= 3.0 * b0;
+            if(i == 3) u += b0;
+            if(i == g.im - 2) u += 3.0 * bn;
+            if(i == g.im - 3) u -= 3.0 * bn;
+            if(i == g.im - 4) u += bn;
+        }
+        if(j - 1 >= 1)        v += sbar[o - sj] * c.inv_2dthe * w[i * g.jm + j - 1].inv_rm;
+        if(j + 1 <= g.jm - 2) v -= sbar[o + sj] * c.inv_2dthe * w[i * g.jm + j + 1].inv_rm;
+        const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+        ww = (sbar[o - k + kw] - sbar[o - k + ke]) * c.inv_2dphi * w[i * g.jm + j].inv_rmsinthe;
+    }
+    aub[o] = u; avb[o] = v; awb[o] = ww;
 }
 
 }  // namespace aturan

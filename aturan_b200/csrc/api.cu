@@ -72,7 +72,8 @@ struct aturan_ctx {
     // and the adjoint's work arrays; null when the tape is off
     double* tape;
     bool tape_valid;           // a taped RK4 step has run since the tape was switched on
-    double *tX, *tTout, *tref, *aslot, *aybar, *akbar, *ag0, *aphbar, *arbar, *alev;
+    double *tX, *tTout, *tPd, *tSrc, *tref, *aslot, *aybar, *akbar, *ag0, *aphbar, *arbar, *apdbar, *aaux, *alev;
+    bool tape_p_valid;         // a taped RB_SOR / RB_LINE pressure call has run since the tape was switched on
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -91,6 +92,8 @@ struct aturan_ctx {
 };
 
 namespace {
+
+constexpr int SOR_KSPLIT = 4;   // k-splits of the correction's transforms (more blocks in flight)
 
 int fail(aturan_ctx* c, int code, const std::string& msg){
     if(c) c->err = msg;
@@ -284,6 +287,7 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     if(taping<S>(ctx)){
         CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->tX, state, ADJ_NF * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->tPd, ctx->pdyn, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
     }
     launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
                  grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
@@ -439,19 +443,22 @@ int sor_correct(aturan_ctx* ctx, T* P){
     const Grid g = ctx->g;
     const SorConst& c = ctx->sorc;
     const MatRef R{ctx->sor_colR, c.N, 1};                        // (jj, k)
-    const dim3 gf((c.NM + 1 + 31) / 32, (c.J + 31) / 32);
+    const long sz_ac = (long)(c.NM + 1) * c.J, sz_q = (long)c.J * c.N;
+    const int kcf = ((c.N + SOR_KSPLIT - 1) / SOR_KSPLIT + 31) / 32 * 32;
+    const dim3 gf((c.NM + 1 + 31) / 32, (c.J + 31) / 32, SOR_KSPLIT);
     sor_gemm_kernel<<<gf, 256, 0, ctx->st>>>(c.J, c.NM + 1, c.N, R, MatRef{ctx->sor_ctT, c.NM + 1, 1},
                                             R, MatRef{ctx->sor_stT, c.NM + 1, 1}, 1.0 / c.A2y,
-                                            ctx->sor_Ac, ctx->sor_As, 1, c.J);
+                                            ctx->sor_Ac, ctx->sor_As, 1, c.J, kcf, sz_ac);
     ModeLU lu = TR ? ModeLU{ctx->mluT_a, ctx->mluT_cf, ctx->mluT_idn} : ModeLU{ctx->mlu_a, ctx->mlu_cf, ctx->mlu_idn};
     const int pm = ctx->sor_pm;
     sor_tridiag_kernel<<<(c.NM + 1 + pm - 1) / pm, 128, (size_t)8 * c.J * (5 * pm + 4), ctx->st>>>(
-        c, lu, ctx->sor_Ac, ctx->sor_As, pm, TR ? 1 : 0);
-    const dim3 gi((c.N + 31) / 32, (c.J + 31) / 32);
+        c, lu, ctx->sor_Ac, ctx->sor_As, pm, TR ? 1 : 0, SOR_KSPLIT, sz_ac);
+    const int kci = ((c.NM + 1 + SOR_KSPLIT - 1) / SOR_KSPLIT + 31) / 32 * 32;
+    const dim3 gi((c.N + 31) / 32, (c.J + 31) / 32, SOR_KSPLIT);
     sor_gemm_kernel<<<gi, 256, 0, ctx->st>>>(c.J, c.N, c.NM + 1, MatRef{ctx->sor_Ac, 1, c.J}, MatRef{ctx->sor_ct, c.N, 1},
                                             MatRef{ctx->sor_As, 1, c.J}, MatRef{ctx->sor_st, c.N, 1},
-                                            1.0, ctx->sor_q, nullptr, c.N, 1);
-    sor_add_kernel<T, TR><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P);
+                                            1.0, ctx->sor_q, nullptr, c.N, 1, kci, sz_q);
+    sor_add_kernel<T, TR><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P, SOR_KSPLIT, sz_q);
     CK_LAUNCH("column-uniform correction");
     return ATURAN_OK;
 }
@@ -532,6 +539,10 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
                    grp<S>(proj, 0, fs), grp<S>(proj, 1, fs), grp<S>(proj, 2, fs), ctx->p.rigid_lid,
                    ctx->rbw, ctx->pc, ctx->scratch, ctx->st);
+    if(taping<S>(ctx)){           // the clamped source, for the clamp mask of the adjoint
+        CK(cudaMemcpyAsync(ctx->tSrc, ctx->scratch, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        ctx->tape_p_valid = true;
+    }
     sor_compat(ctx, ctx->scratch, false);
     CK_LAUNCH("SOR source");
     nl += 6;
@@ -656,8 +667,8 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->sor_nblk = ((sN + 31) / 32) * sJ;
     ctx->sor_pm = std::max(1, std::min(4, (200 * 1024 / (8 * sJ) - 4) / 5));
     for(int n = 0; n < 4; n++) add((size_t)(sNM + 1) * sN * 8);        // ct, st, ctT, stT
-    add((size_t)sJ * sN * 8); add((size_t)(sNM + 1) * sJ * 8); add((size_t)(sNM + 1) * sJ * 8);
-    add((size_t)(2 * ctx->sor_nblk + 2) * 8); add((size_t)sJ * sN * 8);     // partials (+ the shift)
+    add((size_t)sJ * sN * 8); add((size_t)SOR_KSPLIT * (sNM + 1) * sJ * 8); add((size_t)SOR_KSPLIT * (sNM + 1) * sJ * 8);
+    add((size_t)(2 * ctx->sor_nblk + 2) * 8); add((size_t)SOR_KSPLIT * sJ * sN * 8);     // partials (+ the shift); q
     for(int n = 0; n < 6; n++) add((size_t)(sNM + 1) * sJ * 8);        // mode factorisations (Lc, Lc^T)
     for(int n = 0; n < 6; n++) add(nij * 8);                           // line factorisations (Lc, Lc^T)
     add(fs * 4); add(fs * 4);
@@ -693,9 +704,10 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->sor_ct = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_st = carve<double>(cur, (size_t)(sNM + 1) * sN);
     ctx->sor_ctT = carve<double>(cur, (size_t)(sNM + 1) * sN); ctx->sor_stT = carve<double>(cur, (size_t)(sNM + 1) * sN);
     ctx->sor_colR = carve<double>(cur, (size_t)sJ * sN);
-    ctx->sor_Ac = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->sor_As = carve<double>(cur, (size_t)(sNM + 1) * sJ);
+    ctx->sor_Ac = carve<double>(cur, (size_t)SOR_KSPLIT * (sNM + 1) * sJ);
+    ctx->sor_As = carve<double>(cur, (size_t)SOR_KSPLIT * (sNM + 1) * sJ);
     ctx->sor_part = carve<double>(cur, (size_t)2 * ctx->sor_nblk + 2);
-    ctx->sor_q = carve<double>(cur, (size_t)sJ * sN);
+    ctx->sor_q = carve<double>(cur, (size_t)SOR_KSPLIT * sJ * sN);
     ctx->mlu_a = carve<double>(cur, (size_t)(sNM + 1) * sJ); ctx->mlu_cf = carve<double>(cur, (size_t)(sNM + 1) * sJ);
     ctx->mlu_idn = carve<double>(cur, (size_t)(sNM + 1) * sJ);
     ctx->llu_a = carve<double>(cur, nij); ctx->llu_cf = carve<double>(cur, nij); ctx->llu_idn = carve<double>(cur, nij);
@@ -1019,14 +1031,16 @@ int aturan_tape(aturan_ctx* ctx, int on){
         if(ctx->tape){ CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->tape); }
         ctx->tape = nullptr;
         ctx->tape_valid = false;
+        ctx->tape_p_valid = false;
         return ATURAN_OK;
     }
     if(ctx->mixed) return fail(ctx, ATURAN_E_UNSUPPORTED, "the RK4 adjoint needs an FP64 context");
     if(ctx->tape) return ATURAN_OK;
     const Grid& g = ctx->g;
     const size_t fs = g.fstride;
-    // stage inputs 4 x 4, T output 1, slots, ybar 4, kbar 4, g0 4, phbar 1, rbar 1; level means + sums
-    const size_t nf = 4 * ADJ_NF + 1 + ADJ_SLOTS + 3 * ADJ_NF + 2;
+    // stage inputs 4 x 4, T output, p_dyn, pressure source, slots, ybar 4, kbar 4, g0 4, phbar, rbar,
+    // pdbar, aux adjoint 3; level means + sums
+    const size_t nf = 4 * ADJ_NF + 3 + ADJ_SLOTS + 3 * ADJ_NF + 3 + 3;
     const size_t bytes = (nf * fs + 3 * (size_t)g.im) * sizeof(double);
     void* mem = nullptr;
     if(cudaMalloc(&mem, bytes) != cudaSuccess){ cudaGetLastError(); return fail(ctx, ATURAN_E_NOMEM, "tape allocation"); }
@@ -1036,20 +1050,31 @@ int aturan_tape(aturan_ctx* ctx, int on){
     ctx->tape = reinterpret_cast<double*>(mem);
     ctx->tX = take(4 * ADJ_NF * fs);
     ctx->tTout = take(fs);
+    ctx->tPd = take(fs);
+    ctx->tSrc = take(fs);
     ctx->aslot = take(ADJ_SLOTS * fs);
     ctx->aybar = take(ADJ_NF * fs);
     ctx->akbar = take(ADJ_NF * fs);
     ctx->ag0 = take(ADJ_NF * fs);
     ctx->aphbar = take(fs);
     ctx->arbar = take(fs);
+    ctx->apdbar = take(fs);
+    ctx->aaux = take(3 * fs);
     ctx->tref = take(g.im);
     ctx->alev = take(2 * g.im);
     ctx->tape_valid = false;
+    ctx->tape_p_valid = false;
     return ATURAN_OK;
 }
 
 int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const* xbar){
+    return aturan_rk4_adjoint_ex(ctx, ybar, nullptr, xbar, nullptr);
+}
+
+int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
+                          double* const* xbar, double* pbar){
     if(!ctx || !ybar || !xbar) return ATURAN_E_INVALID;
+    if(auxbar) for(int q = 0; q < 3; q++) if(!auxbar[q]) return fail(ctx, ATURAN_E_INVALID, "null aux adjoint pointer");
     for(int q = 0; q < ADJ_NF; q++) if(!ybar[q] || !xbar[q]) return fail(ctx, ATURAN_E_INVALID, "null adjoint pointer");
     if(!ctx->tape || !ctx->tape_valid) return fail(ctx, ATURAN_E_INVALID, "no taped RK4 step (aturan_tape, then aturan_rk4_step)");
     const Grid g = ctx->g;
@@ -1064,13 +1089,17 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
     const double t_min = K.t_min, t_max = K.t_max;
     const dim3 gc((g.km + 127) / 128, g.jm, g.im);
     adj_init_kernel<<<gc, 128, 0, ctx->st>>>(g, ctx->ag0, ctx->tTout, t_min, t_max, dt / 6.0 * 1.0,
-                                             ctx->ag0, ctx->aybar, ctx->akbar, ctx->aphbar);
+                                             ctx->ag0, ctx->aybar, ctx->akbar, ctx->aphbar, ctx->apdbar);
     CK_LAUNCH("adjoint init"); nl++;
+    if(auxbar)                                         // the aux adjoint into the padded layout
+        for(int q = 0; q < 3; q++)
+            CK(cudaMemcpy2DAsync(ctx->aaux + q * fs, g.kp * 8, auxbar[q], g.km * 8, g.km * 8, rows,
+                                 cudaMemcpyDeviceToDevice, ctx->st));
     AdjArgs a;
     a.g = g;
     a.X0 = ctx->tX;
     a.kbar = ctx->akbar;
-    a.pdyn = ctx->pdyn;
+    a.pdyn = ctx->tPd;                                  // p_dyn as the taped step read it
     a.forc = reinterpret_cast<const double*>(ctx->forc);
     a.geo = reinterpret_cast<const GeoIJ<double>*>(ctx->geo);
     a.cp_tab = reinterpret_cast<const double*>(ctx->cp_tab);
@@ -1080,12 +1109,13 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
     const dim3 gg((g.km - 1 + 127) / 128, g.jm, g.im);
     for(int stage = 3; stage >= 0; stage--){
         a.X = ctx->tX + (size_t)stage * ADJ_NF * fs;
+        a.auxbar = (stage == 3 && auxbar) ? ctx->aaux : nullptr;   // aux is stage 3's output
         adj_local_kernel<<<gs, dim3(32, 4), 0, ctx->st>>>(a);
         const int prev = stage - 1;
         const double w_prev = prev >= 0 ? dt / 6.0 * ((prev == 0 || prev == 3) ? 1.0 : 2.0) : 0.0;
         const double c_prev = prev >= 0 ? ((prev == 0 || prev == 1) ? 0.5 * dt : (prev == 2 ? dt : 0.0)) : 0.0;
-        adj_gather_kernel<<<gg, 128, 0, ctx->st>>>(g, ctx->aslot, ctx->aybar, ctx->aphbar, ctx->ag0, ctx->akbar,
-                                                  w_prev, c_prev, prev >= 0 ? 1 : 0);
+        adj_gather_kernel<<<gg, 128, 0, ctx->st>>>(g, ctx->aslot, ctx->aybar, ctx->aphbar, ctx->apdbar, ctx->ag0,
+                                                  ctx->akbar, w_prev, c_prev, prev >= 0 ? 1 : 0);
         CK_LAUNCH("adjoint stage"); nl += 2;
     }
     const double* t0 = ctx->tX;
@@ -1101,8 +1131,65 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
     for(int q = 0; q < ADJ_NF; q++)
         CK(cudaMemcpy2DAsync(xbar[q], g.km * 8, ctx->aybar + q * fs, g.kp * 8, g.km * 8, rows,
                              cudaMemcpyDeviceToDevice, ctx->st));
+    if(pbar)
+        CK(cudaMemcpy2DAsync(pbar, g.km * 8, ctx->apdbar, g.kp * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return ATURAN_OK;
+}
+
+int aturan_pressure_adjoint(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
+                            const double* pbar, double* const* auxbar, int* sweeps_done, double* resid){
+    if(!ctx || !pbar || !auxbar) return ATURAN_E_INVALID;
+    for(int q = 0; q < 3; q++) if(!auxbar[q]) return fail(ctx, ATURAN_E_INVALID, "null aux adjoint pointer");
+    if(sweeps_done) *sweeps_done = 0;
+    if(resid) *resid = 0.0;
+    if(kind != ATURAN_PRESS_RB_SOR && kind != ATURAN_PRESS_RB_LINE)
+        return fail(ctx, ATURAN_E_INVALID, "the pressure adjoint is that of ATURAN_PRESS_RB_SOR / RB_LINE");
+    if(!ctx->tape || !ctx->tape_p_valid)
+        return fail(ctx, ATURAN_E_INVALID, "no taped pressure solve (aturan_tape, then aturan_pressure)");
+    const bool line = kind == ATURAN_PRESS_RB_LINE;
+    int rc = sor_check_sizes(ctx, omega, line); if(rc) return rc;
+    if(max_sweeps < 1) max_sweeps = 1;
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride, rows = (size_t)g.im * g.jm;
+    long nl = 0;
+    Region reg(ctx, ATURAN_K_ADJOINT, 0);
+    double* B = ctx->akbar;                 // work fields: p_dyn's adjoint, the transposed solution,
+    double* lam = ctx->akbar + fs;          // the source's adjoint
+    double* sbar = ctx->akbar + 2 * fs;
+    CK(cudaMemsetAsync(B, 0, 3 * fs * 8, ctx->st));
+    CK(cudaMemcpy2DAsync(B, g.kp * 8, pbar, g.km * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
+    // the boundary passes' adjoint, in reverse order
+    adj_pbc_p_kernel<<<(g.im * g.jm + 255) / 256, 256, 0, ctx->st>>>(g, B);
+    adj_pbc_t_kernel<<<dim3((g.km + 127) / 128, g.im), 128, 0, ctx->st>>>(g, B);
+    adj_pbc_r_kernel<<<dim3((g.km + 127) / 128, g.jm), 128, 0, ctx->st>>>(g, B);
+    sor_compat(ctx, B, true);               // zero-mean (it is, up to rounding, when p_dyn enters by differences)
+    CK_LAUNCH("pressure adjoint: boundary passes");
+    nl += 6;
+    int s = 0;
+    double r = 0.0;
+    const int status = solve_fp64<true>(ctx, lam, B, omega, max_sweeps, tol, line, &s, &r, nl);
+    if(status < 0) return status;
+    const int ny = ((g.jm - 2) * (g.km - 1) + 255) / 256;
+    sor_ysum_kernel<<<ny, 256, 0, ctx->st>>>(g, lam, ctx->sor_part, 1);
+    sor_shift_finish_kernel<<<1, 256, 0, ctx->st>>>(ctx->sor_part, ny, ctx->sor_part + 2 * ny);
+    const double n_int = (double)(g.im - 2) * (g.jm - 2) * (g.km - 1);
+    const double sum_w = (double)(g.im - 1) * (g.jm - 1) * (g.km - 1);   // sum of y_i y_j over the interior
+    adj_compat_mask_kernel<<<dim3((g.km - 1 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, ctx->st>>>(
+        g, lam, ctx->sor_part + 2 * ny, n_int / sum_w, ctx->tSrc, ctx->rbw, sbar);
+    double* aub = ctx->ag0;
+    adj_div_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(
+        g, sbar, ctx->rbw, ctx->pc, ctx->p.rigid_lid, aub, aub + fs, aub + 2 * fs);
+    CK_LAUNCH("pressure adjoint: source");
+    nl += 4;
+    for(int q = 0; q < 3; q++)
+        CK(cudaMemcpy2DAsync(auxbar[q], g.km * 8, aub + q * fs, g.kp * 8, g.km * 8, rows,
+                             cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    reg.n = nl;
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    return status;
 }
 
 int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_noconv){
@@ -1131,6 +1218,20 @@ int aturan_sync_ncopies(aturan_ctx* ctx){
     CK(cudaMemcpyAsync(n, s, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
     if(ctx->p.nh4sh_sync)
         CK(cudaMemcpyAsync(n + ATURAN_NH4SH * fs * e, s + ATURAN_NH4SH * fs * e, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    return ATURAN_OK;
+}
+
+int aturan_restore_ncopies(aturan_ctx* ctx, double coeff){
+    if(!ctx) return ATURAN_E_INVALID;
+    const size_t fs = ctx->g.fstride, e = ctx->esz;
+    Region reg(ctx, ATURAN_K_COPY, coeff == 1.0 ? 0 : 1);
+    if(coeff == 1.0){                                     // 1.0 * x == x: a copy
+        CK(cudaMemcpyAsync(ctx->ncopy, ctx->state, 19 * fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    } else {
+        if(ctx->mixed) launch_scale_copy_f32(reinterpret_cast<const float*>(ctx->state), reinterpret_cast<float*>(ctx->ncopy), 19 * fs, coeff, ctx->st);
+        else launch_scale_copy_f64(reinterpret_cast<const double*>(ctx->state), reinterpret_cast<double*>(ctx->ncopy), 19 * fs, coeff, ctx->st);
+        CK_LAUNCH("restore n-copies");
+    }
     return ATURAN_OK;
 }
 

@@ -15,6 +15,14 @@
 namespace aturan {
 ATURAN_DEFINE_LAUNCHERS(double, double)
 
+__global__ void scale_copy_f64_kernel(const double* in, double* out, size_t n, double coeff){
+    for(size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        out[t] = coeff * in[t];
+}
+void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff, cudaStream_t st){
+    scale_copy_f64_kernel<<<148 * 8, 256, 0, st>>>(in, out, n, coeff);
+}
+
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st){
     pdyn_bc_r_kernel<<<dim3((g.km + 127) / 128, g.jm), 128, 0, st>>>(g, P);
     pdyn_bc_t_kernel<<<dim3((g.km + 127) / 128, g.im), 128, 0, st>>>(g, P);

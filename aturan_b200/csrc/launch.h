@@ -31,6 +31,8 @@ ATURAN_DECLARE_LAUNCHERS(float, float)
 
 // FP64-only kernels (p_dyn is FP64 in both precisions).
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st);
+void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff, cudaStream_t st);
+void launch_scale_copy_f32(const float* in, float* out, size_t n, double coeff, cudaStream_t st);
 void launch_rb_colour(Grid g, double* P, const double* src, const RBW* w, int colour, double omega, cudaStream_t st);
 
 // Layout conversions for the mixed-precision context (FP64 exchange <-> FP32 storage).

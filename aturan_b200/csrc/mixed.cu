@@ -19,6 +19,14 @@ __global__ void f32_to_f64_kernel(const float* in, double* out, size_t n){
     for(size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
         out[t] = (double)in[t];
 }
+__global__ void scale_copy_f32_kernel(const float* in, float* out, size_t n, double coeff){
+    for(size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        out[t] = (float)(coeff * (double)in[t]);
+}
+void launch_scale_copy_f32(const float* in, float* out, size_t n, double coeff, cudaStream_t st){
+    scale_copy_f32_kernel<<<148 * 8, 256, 0, st>>>(in, out, n, coeff);
+}
+
 void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st){
     f64_to_f32_kernel<<<148 * 8, 256, 0, st>>>(in, out, n);
 }

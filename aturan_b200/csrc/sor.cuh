@@ -164,20 +164,23 @@ __device__ __forceinline__ void gemm_stage(double (*t)[33], const MatRef& A, int
     }
 }
 
+// Split K: block z sums k in [z kc, (z + 1) kc) and writes its partial products at C + z * cz; the
+// consumer (the tridiagonal kernel, the add kernel) sums the gridDim.z partials in order.
 __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, MatRef A1, MatRef B1, MatRef A2,
                                                        MatRef B2, double scale, double* C1, double* C2,
-                                                       long crs, long ccs){
+                                                       long crs, long ccs, int kc, long cz){
     __shared__ double sa1[32][33], sb1[32][33], sa2[32][33], sb2[32][33];   // sa[r][k], sb[c][k]
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const bool sharedA = (A2.p == A1.p && A2.rs == A1.rs && A2.cs == A1.cs);
     const MatRef Bt1{B1.p, B1.cs, B1.rs}, Bt2{B2.p, B2.cs, B2.rs};   // B^T: (c, k)
     double acc1[4] = {0.0, 0.0, 0.0, 0.0}, acc2[4] = {0.0, 0.0, 0.0, 0.0};
-    for(int k0 = 0; k0 < K; k0 += 32){
-        gemm_stage(sa1, A1, r0, k0, M, K);
-        if(!sharedA) gemm_stage(sa2, A2, r0, k0, M, K);
-        gemm_stage(sb1, Bt1, c0, k0, Nn, K);
-        gemm_stage(sb2, Bt2, c0, k0, Nn, K);
+    for(int k0 = kb; k0 < ke; k0 += 32){
+        gemm_stage(sa1, A1, r0, k0, M, ke);
+        if(!sharedA) gemm_stage(sa2, A2, r0, k0, M, ke);
+        gemm_stage(sb1, Bt1, c0, k0, Nn, ke);
+        gemm_stage(sb2, Bt2, c0, k0, Nn, ke);
         __syncthreads();
         double (*a2)[33] = sharedA ? sa1 : sa2;
 #pragma unroll 8
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, Mat
     for(int q = 0; q < 4; q++){
         const int r = r0 + ty + 8 * q;
         if(r < M && c < Nn){
-            const long off = (long)r * crs + (long)c * ccs;
+            const long off = (long)r * crs + (long)c * ccs + (long)blockIdx.z * cz;
             if(C2){ C1[off] = scale * acc1[q]; C2[off] = scale * acc2[q]; }
             else C1[off] = scale * (acc1[q] + acc2[q]);
         }
@@ -213,12 +216,12 @@ __global__ void __launch_bounds__(256) sor_gemm_kernel(int M, int Nn, int K, Mat
 // transform's weight w_m / N (w = 1 for m = 0 and m = N/2, else 2).
 //
 // A block takes pm modes (2 pm problems, problem t = 2 m + part): all of its threads stage the
-// right-hand sides into shared memory as [q][t] (row stride 2 pm + 1: conflict-free) and the
+// right-hand sides (the sum of the transform's nsplit partials) into shared memory as [q][t] (row stride 2 pm + 1: conflict-free) and the
 // modes' factors as [q][m] (stride pm + 1); then one thread per problem runs the two dependent
 // recurrences on shared-memory latency, in place, and the block writes back. Shared memory:
 // 8 J (5 pm + 4) bytes.
 __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu, double* Ac, double* As, int pm,
-                                                          int tr){
+                                                          int tr, int nsplit, long split_stride){
     extern __shared__ double sm[];
     const int J = s.J, np = 2 * pm, ldr = np + 1, ldf = pm + 1;
     double* sd = sm;                                     // [J][ldr]
@@ -234,7 +237,8 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
         double c = 0.0, sn = 0.0, va = 0.0, vc = 0.0, vi = 0.0;
         if(m < nmode){
             const size_t g = (size_t)m * J + q;
-            c = Ac[g]; sn = As[g]; va = lu.a[g]; vc = lu.cf[g]; vi = lu.idn[g];
+            for(int z = 0; z < nsplit; z++){ c += Ac[g + z * split_stride]; sn += As[g + z * split_stride]; }
+            va = lu.a[g]; vc = lu.cf[g]; vi = lu.idn[g];
         }
         sd[q * ldr + 2 * lm] = c; sd[q * ldr + 2 * lm + 1] = sn;
         fa[q * ldf + lm] = va; fc[q * ldf + lm] = vc; fi[q * ldf + lm] = vi;
@@ -287,14 +291,15 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
 // Onto every interior level of the column: P[i][j][k] += q(j,k).
 // (TR: y_i q, the trial functions of the transposed system's correction.)
 template <typename T, bool TR = false>
-__global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf, T* P){
+__global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf, T* P, int nsplit, long split_stride){
     const int N = g.km - 1;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
     const int i = 1 + blockIdx.z;
     if(k >= N) return;
     const size_t o = gidx(g, i, j, k);
-    const double q = qbuf[(size_t)(j - 1) * N + k];
+    double q = 0.0;
+    for(int z = 0; z < nsplit; z++) q += qbuf[(size_t)(j - 1) * N + k + z * split_stride];   // the partials
     P[o] = (T)((double)P[o] + (TR ? ywt(i, 1, g.im - 2) * q : q));
 }
 

@@ -174,9 +174,10 @@ int aturan_rk4_step(aturan_ctx* ctx);
 /* Adjoint of one RK4 step of the dry dynamics, FP64 contexts. No counterpart in the reference,
  * which has no adjoint; it differentiates RungeKutta_Uran_Turb.cpp:18-403 with RHS_Uran_Turb.cpp's
  * tendencies of t, u, v, w.
- * aturan_tape(ctx, 1): every later aturan_rk4_step keeps what its adjoint needs (the stage inputs
- *   of t, u, v, w, the new T and the level means: 17 fields, plus 42 fields of work arrays, of
- *   device memory); aturan_tape(ctx, 0) frees it. ATURAN_E_UNSUPPORTED on a mixed context.
+ * aturan_tape(ctx, 1): every later aturan_rk4_step and RB_SOR / RB_LINE aturan_pressure keeps what
+ *   its adjoint needs (the stage inputs of t, u, v, w, the new T, p_dyn, the clamped pressure
+ *   source and the level means: 19 fields, plus 56 fields of work arrays, of device memory);
+ *   aturan_tape(ctx, 0) frees it. ATURAN_E_UNSUPPORTED on a mixed context.
  * aturan_rk4_adjoint(ctx, ybar, xbar): ybar[4] and xbar[4] are device pointers to contiguous
  *   [im][jm][km] FP64 arrays in the order t, u, v, w. Given the adjoint ybar of those fields after
  *   the last taped aturan_rk4_step, writes xbar = J^T ybar, J the step's Jacobian with respect to
@@ -186,6 +187,25 @@ int aturan_rk4_step(aturan_ctx* ctx);
  *   piecewise (0 where clamped, the interval's slope). Synchronous. */
 int aturan_tape(aturan_ctx* ctx, int on);
 int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const* xbar);
+
+/* The same with the two links to the pressure solve (no counterpart in the reference):
+ * auxbar[3] (or NULL) is the adjoint of the step's projection outputs aux_u, aux_v, aux_w (the
+ * stage-3 tendencies of u, v, w without the p_dyn gradient, which the next pressure solve reads;
+ * RHS_Uran_Turb.cpp:1020-1022), and pbar (or NULL) receives the adjoint of the p_dyn the step
+ * read, all [im][jm][km] FP64 device arrays. */
+int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
+                          double* const* xbar, double* pbar);
+
+/* Adjoint of the last taped ATURAN_PRESS_RB_SOR / RB_LINE pressure call (no counterpart in the
+ * reference): given pbar, the adjoint of the p_dyn it produced (boundary rows included), writes
+ * auxbar[3], the adjoint of the aux_u, aux_v, aux_w it read. The chain reversed: the boundary
+ * passes, the solve (a solve with the transposed operator, kind/omega/max_sweeps/tol as for the
+ * forward; ATURAN_NOT_CONVERGED at the cap), the compatibility shift, the source clamp (0 where the
+ * forward clamped) and the divergence (PressureSolver.h:370-487 with prepareProjectionBoundaries,
+ * Pressure_Uran.cpp:30-146). The free constant of p_dyn is taken as not differentiated (its
+ * adjoint is made zero-mean). FP64 contexts with the tape on. Synchronous. */
+int aturan_pressure_adjoint(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
+                            const double* pbar, double* const* auxbar, int* sweeps_done, double* resid);
 
 /* The pressure solve.
  *   GS_LEX:    replaces PressureSolverUran(m).run() (PressureSolverUran.h:33-250); omega,
@@ -227,6 +247,12 @@ int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_nocon
 /* The ATURAN_RK_SCALAR_SYNC=2 copy of the condensables and T (and NH4SH when nh4sh_sync) into
  * their start-of-step copies, cUranusModel.cpp:1049-1073. */
 int aturan_sync_ncopies(aturan_ctx* ctx);
+
+/* restoreVar(coeff) at the end of an iteration (cUranusModel.cpp:1264, :1638-1680): every
+ * prognostic field's start-of-step copy set to coeff times the field (p_dynn and chromn, which the
+ * library does not hold, excepted). A driver running several steps on the device calls it after
+ * each step, where the reference's loop does. */
+int aturan_restore_ncopies(aturan_ctx* ctx, double coeff);
 
 /* The in-scope part of one even iteration of cUranusModel::Run (cUranusModel.cpp:967-1123):
  * pressure (kind/omega/max_sweeps/tol as aturan_pressure), the four saturation adjustments,

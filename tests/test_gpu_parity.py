@@ -326,3 +326,20 @@ def test_sor_rejects_bad_omega():
     with pytest.raises(AturanError):
         ctx.pressure(P.PRESS_RB_SOR, omega=2.5, max_sweeps=10, tol=1e-8)
     ctx.close()
+
+
+def test_restore_ncopies_is_restorevar():
+    """aturan_restore_ncopies(coeff): every prognostic n-copy = coeff * its field
+    (cUranusModel::restoreVar, cUranusModel.cpp:1638-1680)."""
+    p = P.default_params(12, 20, 33)
+    st = S.synthetic_state(p, seed=91)
+    ctx = ctx_for(p)
+    ctx.upload_state(st)
+    ctx.rk4_step()
+    ctx.restore_ncopies(1.0)
+    for n in F.PROGNOSTIC:
+        assert np.array_equal(ctx.download(n + "n"), ctx.download(n)), n
+    ctx.restore_ncopies(0.5)
+    for n in F.PROGNOSTIC:
+        assert np.array_equal(ctx.download(n + "n"), 0.5 * ctx.download(n)), n
+    ctx.close()
