@@ -45,8 +45,9 @@ SIGNATURES = {
                                ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                               ctypes.c_int),
     "aturan_rk4_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
-    "aturan_rk4_adjoint_ex": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
-                              ctypes.c_int),
+    "aturan_rk4_adjoint_ex": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p], ctypes.c_int),
+    "aturan_set_heating": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "aturan_pressure_adjoint": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_pressure": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
@@ -183,13 +184,18 @@ class Context:
         xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
         self._check(self.L.aturan_rk4_adjoint(self.h, yb, xb), "rk4_adjoint")
 
-    def rk4_adjoint_ex(self, ybar_ptrs, auxbar_ptrs, xbar_ptrs, pbar_ptr):
-        """aturan_rk4_adjoint_ex: auxbar_ptrs (3, or None) in, pbar_ptr (or None) out."""
+    def rk4_adjoint_ex(self, ybar_ptrs, auxbar_ptrs, xbar_ptrs, pbar_ptr, heatbar_ptr=None):
+        """aturan_rk4_adjoint_ex: auxbar_ptrs (3, or None) in; pbar_ptr, heatbar_ptr (or None) out."""
         yb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
         xb = (ctypes.c_void_p * 4)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
         ab = (ctypes.c_void_p * 3)(*[ctypes.c_void_p(int(x)) for x in auxbar_ptrs]) if auxbar_ptrs else None
-        self._check(self.L.aturan_rk4_adjoint_ex(self.h, yb, ab, xb, ctypes.c_void_p(int(pbar_ptr)) if pbar_ptr else None),
-                    "rk4_adjoint_ex")
+        opt = lambda x: ctypes.c_void_p(int(x)) if x else None
+        self._check(self.L.aturan_rk4_adjoint_ex(self.h, yb, ab, xb, opt(pbar_ptr), opt(heatbar_ptr)), "rk4_adjoint_ex")
+
+    def set_heating(self, ptr, on_device=True):
+        """aturan_set_heating: a [jm][km] FP64 heating rate in K/s (device or host pointer), None removes it."""
+        self._check(self.L.aturan_set_heating(self.h, ctypes.c_void_p(int(ptr)) if ptr else None,
+                                              1 if on_device else 0), "set_heating")
 
     def pressure_adjoint(self, pbar_ptr, auxbar_ptrs, kind=3, omega=1.0, max_sweeps=200, tol=1e-10):
         """aturan_pressure_adjoint; (rc, sweeps, resid)."""

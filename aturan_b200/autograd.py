@@ -96,11 +96,16 @@ class DryFullStepper(DryStepper):
         self.press = (kind, omega, max_sweeps, tol)
         self.zero = torch.zeros(self.shape, dtype=torch.float64, device="cuda")
 
-    def forward(self, xs, aux):
+    def forward(self, xs, aux, heat=None):
+        """heat: an optional [jm][km] heating rate in K/s (aturan_set_heating) held for the step."""
         ctx = self.ctx
         xs = [x.detach().contiguous() for x in xs]
         aux = [a.detach().contiguous() for a in aux]
+        if heat is not None:
+            heat = heat.detach().contiguous()
         torch.cuda.synchronize()
+        ctx.set_heating(heat.data_ptr() if heat is not None else None)
+        self.heated = heat is not None
         for n, t in self.saved.items():
             ctx.upload_device(n, t.data_ptr())
         ctx.upload_device("p_dyn", self.zero.data_ptr())
@@ -119,18 +124,21 @@ class DryFullStepper(DryStepper):
         return out[:4], out[4:]
 
     def backward(self, ybar, auxbar):
+        """(xbar, abar), or (xbar, abar, hbar) when the step had a heating field."""
         z = lambda g: torch.zeros(self.shape, dtype=torch.float64, device="cuda") if g is None else g.contiguous()
         ybar = [z(g) for g in ybar]
         auxbar = [z(g) for g in auxbar]
         xbar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in DRY]
         pbar = torch.empty(self.shape, dtype=torch.float64, device="cuda")
         abar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in AUX]
+        hbar = torch.empty(self.shape[1:], dtype=torch.float64, device="cuda") if self.heated else None
         torch.cuda.synchronize()
         self.ctx.rk4_adjoint_ex([g.data_ptr() for g in ybar], [g.data_ptr() for g in auxbar],
-                                [x.data_ptr() for x in xbar], pbar.data_ptr())
+                                [x.data_ptr() for x in xbar], pbar.data_ptr(),
+                                hbar.data_ptr() if hbar is not None else None)
         kind, omega, ms, tol = self.press
         self.ctx.pressure_adjoint(pbar.data_ptr(), [a.data_ptr() for a in abar], kind, omega, ms, tol)
-        return xbar, abar
+        return (xbar, abar) if hbar is None else (xbar, abar, hbar)
 
 
 class DryFullStep(torch.autograd.Function):
@@ -151,18 +159,20 @@ class DryFullStep(torch.autograd.Function):
         return (None, *xbar, *abar)
 
 
-def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn):
+def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn, heat=None):
     """Loss after nsteps DryFullStepper steps from (xs0, aux0) and its gradient with respect to
     xs0 and aux0, by the hand-written adjoint with checkpointing: the forward keeps the inputs of
     every `every`-th step; the backward recomputes a segment's step inputs from its checkpoint,
     then re-runs each step (which tapes it) right before its adjoint, last step first. Memory:
     (nsteps / every + every) step inputs; cost about three forward passes plus the adjoints.
-    loss_fn maps the final (t, u, v, w) to a scalar tensor (differentiated by torch.autograd)."""
+    loss_fn maps the final (t, u, v, w) to a scalar tensor (differentiated by torch.autograd).
+    With heat (a [jm][km] heating rate held over the trajectory) the gradient with respect to it,
+    summed over the steps, is returned too."""
     ck = {0: ([x.detach() for x in xs0], [a.detach() for a in aux0])}
     xs, aux = ck[0]
     with torch.no_grad():
         for n in range(nsteps):
-            xs, aux = stepper.forward(xs, aux)
+            xs, aux = stepper.forward(xs, aux, heat)
             if (n + 1) % every == 0 and n + 1 < nsteps:
                 ck[n + 1] = (xs, aux)
     xf = [x.detach().requires_grad_(True) for x in xs]
@@ -170,13 +180,19 @@ def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn):
     ybar = list(torch.autograd.grad(loss, xf, allow_unused=True))
     ybar = [torch.zeros_like(x) if g is None else g for x, g in zip(xf, ybar)]
     abar = [torch.zeros_like(a) for a in aux]
+    hsum = None if heat is None else torch.zeros_like(heat)
     for start in sorted(ck, reverse=True):
         end = min(start + every, nsteps)
         inputs = [ck[start]]
         with torch.no_grad():
             for _ in range(start, end - 1):
-                inputs.append(stepper.forward(*inputs[-1]))
+                inputs.append(stepper.forward(*inputs[-1], heat))
         for n in reversed(range(start, end)):
-            stepper.forward(*inputs[n - start])            # tapes step n
-            ybar, abar = stepper.backward(ybar, abar)
-    return loss.detach(), ybar, abar
+            stepper.forward(*inputs[n - start], heat)      # tapes step n
+            out = stepper.backward(ybar, abar)
+            ybar, abar = out[0], out[1]
+            if heat is not None:
+                hsum += out[2]
+    if heat is None:
+        return loss.detach(), ybar, abar
+    return loss.detach(), ybar, abar, hsum

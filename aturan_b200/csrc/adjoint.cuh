@@ -41,6 +41,7 @@ struct AdjArgs {
     const double* cp_tab;
     RhsConst<double> k;
     double* slot;               // ADJ_SLOTS fields
+    double* hacc;               // null, or the T tendencies' adjoint summed over the stages (heating)
 };
 
 // cp_lapse (rk4.cuh) and its derivative in T (K), the table's slope inside its 0.5 K interval.
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(128) adj_local_kernel(const AdjArgs a){
     const double nue_t = (K.turb_coupling != 0.0 && isfinite(nue_c)) ? K.turb_coupling * cmax(0.0, nue_c) : 0.0;
     const double nue_t_s = nue_t / 0.9;
     const double at = a.kbar[0 * fs + o];
+    if(a.hacc) a.hacc[o] += at;                 // rhs_t += heat_scale H(j,k) (aturan_set_heating)
     const double au0 = a.kbar[1 * fs + o], av0 = a.kbar[2 * fs + o], aw0 = a.kbar[3 * fs + o];
     // aux = the tendency without the p_dyn gradient: its adjoint joins the tendency's in every
     // partial except those in p_dyn
@@ -342,6 +344,18 @@ __global__ void adj_level_apply_kernel(Grid g, const double* t, const double* ps
     const double b = h.g * ps[o] / (h.rR * T * h.t_ref);
     if(!isfinite(b)) return;
     ybar[o] += lev[2 * m] / lev[2 * m + 1] * wsin[j] * (-b / T);
+}
+
+// The heating field's adjoint: heat_scale times the T tendencies' adjoint summed over the stages and
+// the interior levels, per (j,k); 0 on the polar rows and the seam column, which no stage reads.
+__global__ void adj_heat_reduce_kernel(Grid g, const double* hacc, double scale, double* out){
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= g.jm * g.km) return;
+    const int j = c / g.km, k = c - j * g.km;
+    double s = 0.0;
+    if(j >= 1 && j <= g.jm - 2 && k <= g.km - 2)
+        for(int i = 1; i < g.im - 1; i++) s += hacc[gidx(g, i, j, k)];
+    out[c] = scale * s;
 }
 
 // ---- The pressure step's adjoint (RB_SOR / RB_LINE path): p_dyn = F(solve(compat(clamp(div aux))))

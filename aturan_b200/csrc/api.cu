@@ -74,6 +74,8 @@ struct aturan_ctx {
     bool tape_valid;           // a taped RK4 step has run since the tape was switched on
     double *tX, *tTout, *tPd, *tSrc, *tref, *aslot, *aybar, *akbar, *ag0, *aphbar, *arbar, *apdbar, *aaux, *alev;
     bool tape_p_valid;         // a taped RB_SOR / RB_LINE pressure call has run since the tape was switched on
+    double* ahacc;             // the T tendencies' adjoint summed over the stages (heating gradient)
+    double* heat;              // aturan_set_heating: [jm][km] K/s, or null
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -199,6 +201,7 @@ RhsConst<C> make_rhs_const(const aturan_params& p){
     k.t_min = p.t_min_K / p.t_ref;
     k.t_max = p.t_max_K / p.t_ref;
     k.dt = p.dt;
+    k.heat_scale = (p.L_atm * 1.0e3 / p.u_0) / p.t_ref;
     k.cp_dyn = p.cp_dyn; k.cp_gas = p.cp_gas; k.cp_mode = p.cp_h2_mode; k.turb_active = p.turb_active;
     RhsConst<C> out;
     const double* src = reinterpret_cast<const double*>(&k);
@@ -305,6 +308,7 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     a.proj = reinterpret_cast<S*>(ctx->proj);
     a.geo = reinterpret_cast<const GeoIJ<C>*>(ctx->geo);
     a.cp_tab = reinterpret_cast<const C*>(ctx->cp_tab);
+    a.heat = ctx->heat;
     a.k = K;
     S* y0 = reinterpret_cast<S*>(ctx->ybuf[0]);
     S* y1 = reinterpret_cast<S*>(ctx->ybuf[1]);
@@ -557,13 +561,19 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     } else {
         // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
         // Lc e = r by FP32 sweeps (with the column-uniform correction), p += e in FP64.
-        const int inner = line ? 3 : 48;
+        // FP32 sweeps per refinement step: for line SOR 2 (measured at 41x181x361, warm: two
+        // refinement steps of 2 reach 3e-8 against 6 sweeps with 3 per step, 0.53 vs 0.59 ms)
+        const int inner = line ? 2 : 48;
         rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
             sor_resid32_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->r32, ctx->e32);
             nl++;
             for(int n = 0; n < inner && s < max_sweeps; n++, s++){
-                if(n % every == 0){
+                // the correction on the same cadence as the FP64 solve (once per `every` sweeps,
+                // counted over the whole solve): after the first one the column-uniform error is
+                // gone and a later refinement step's correction changes nothing (measured: same
+                // sweep count, 0.14 ms less at 41x181x361)
+                if(s % every == 0){
                     rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc;
                     rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
                     nl += 5;
@@ -819,6 +829,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
         GasConst& K = sc.gas[n];
         K.t_0 = G.t_0; K.t_00 = G.t_00; K.ep = G.ep; K.lv = G.lv; K.ls = G.ls;
         K.C = G.C; K.L0 = G.L0; K.den = 1e-3 * G.R; K.del_alf = G.del_alf; K.del_bet = G.del_bet;
+        K.inv_den = 1.0 / K.den;
         K.C_i = G.C_i; K.L0_i = G.L0_i; K.del_alf_i = G.del_alf_i; K.del_bet_i = G.del_bet_i;
         K.t_range_inv = 1.0 / (G.t_0 - G.t_00);
         K.Lf = G.ls - G.lv;
@@ -978,6 +989,7 @@ int aturan_ctx_destroy(aturan_ctx* ctx){
     if(ctx->st) cudaStreamSynchronize(ctx->st);
     if(ctx->gs_exec) cudaGraphExecDestroy(ctx->gs_exec);
     if(ctx->tape) cudaFree(ctx->tape);
+    if(ctx->heat) cudaFree(ctx->heat);
     for(auto& e : ctx->evs){ cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if(ctx->mem) cudaFree(ctx->mem);
     if(ctx->st) cudaStreamDestroy(ctx->st);
@@ -1039,8 +1051,8 @@ int aturan_tape(aturan_ctx* ctx, int on){
     const Grid& g = ctx->g;
     const size_t fs = g.fstride;
     // stage inputs 4 x 4, T output, p_dyn, pressure source, slots, ybar 4, kbar 4, g0 4, phbar, rbar,
-    // pdbar, aux adjoint 3; level means + sums
-    const size_t nf = 4 * ADJ_NF + 3 + ADJ_SLOTS + 3 * ADJ_NF + 3 + 3;
+    // pdbar, aux adjoint 3, heating accumulator; level means + sums
+    const size_t nf = 4 * ADJ_NF + 3 + ADJ_SLOTS + 3 * ADJ_NF + 3 + 3 + 1;
     const size_t bytes = (nf * fs + 3 * (size_t)g.im) * sizeof(double);
     void* mem = nullptr;
     if(cudaMalloc(&mem, bytes) != cudaSuccess){ cudaGetLastError(); return fail(ctx, ATURAN_E_NOMEM, "tape allocation"); }
@@ -1060,6 +1072,7 @@ int aturan_tape(aturan_ctx* ctx, int on){
     ctx->arbar = take(fs);
     ctx->apdbar = take(fs);
     ctx->aaux = take(3 * fs);
+    ctx->ahacc = take(fs);
     ctx->tref = take(g.im);
     ctx->alev = take(2 * g.im);
     ctx->tape_valid = false;
@@ -1068,11 +1081,11 @@ int aturan_tape(aturan_ctx* ctx, int on){
 }
 
 int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const* xbar){
-    return aturan_rk4_adjoint_ex(ctx, ybar, nullptr, xbar, nullptr);
+    return aturan_rk4_adjoint_ex(ctx, ybar, nullptr, xbar, nullptr, nullptr);
 }
 
 int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
-                          double* const* xbar, double* pbar){
+                          double* const* xbar, double* pbar, double* heatbar){
     if(!ctx || !ybar || !xbar) return ATURAN_E_INVALID;
     if(auxbar) for(int q = 0; q < 3; q++) if(!auxbar[q]) return fail(ctx, ATURAN_E_INVALID, "null aux adjoint pointer");
     for(int q = 0; q < ADJ_NF; q++) if(!ybar[q] || !xbar[q]) return fail(ctx, ATURAN_E_INVALID, "null adjoint pointer");
@@ -1105,6 +1118,8 @@ int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const doub
     a.cp_tab = reinterpret_cast<const double*>(ctx->cp_tab);
     a.k = K;
     a.slot = ctx->aslot;
+    a.hacc = heatbar ? ctx->ahacc : nullptr;
+    if(heatbar) CK(cudaMemsetAsync(ctx->ahacc, 0, fs * 8, ctx->st));
     const dim3 gs((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);
     const dim3 gg((g.km - 1 + 127) / 128, g.jm, g.im);
     for(int stage = 3; stage >= 0; stage--){
@@ -1133,6 +1148,27 @@ int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const doub
                              cudaMemcpyDeviceToDevice, ctx->st));
     if(pbar)
         CK(cudaMemcpy2DAsync(pbar, g.km * 8, ctx->apdbar, g.kp * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
+    if(heatbar){
+        adj_heat_reduce_kernel<<<(g.jm * g.km + 255) / 256, 256, 0, ctx->st>>>(g, ctx->ahacc, K.heat_scale, heatbar);
+        CK_LAUNCH("heating adjoint");
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return ATURAN_OK;
+}
+
+int aturan_set_heating(aturan_ctx* ctx, const double* H, int on_device){
+    if(!ctx) return ATURAN_E_INVALID;
+    const Grid& g = ctx->g;
+    if(!H){
+        if(ctx->heat){ CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->heat); ctx->heat = nullptr; }
+        return ATURAN_OK;
+    }
+    if(!ctx->heat){
+        void* m = nullptr;
+        if(cudaMalloc(&m, (size_t)g.jm * g.km * 8) != cudaSuccess){ cudaGetLastError(); return fail(ctx, ATURAN_E_NOMEM, "heating field"); }
+        ctx->heat = reinterpret_cast<double*>(m);
+    }
+    CK(cudaMemcpyAsync(ctx->heat, H, (size_t)g.jm * g.km * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return ATURAN_OK;
 }

@@ -58,6 +58,7 @@ struct RhsConst {
     T cp_mix, t_ref;
     T cp_rh2, cp_he_term, cp_ch4_term, cp_rsum, cp_h2_const;   // cp(T), CpH2.h:122-134
     T tke_max, dis_min, t_min, t_max, dt;
+    T heat_scale;       // (L_atm * 1e3 / u_0) / t_ref: a heating rate in K/s as a tendency of t
     int cp_dyn, cp_gas, cp_mode, turb_active;
 };
 

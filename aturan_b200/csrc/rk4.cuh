@@ -36,6 +36,7 @@ struct StageArgs {
     S* proj;           // rhs_u, rhs_v, rhs_w, aux_u, aux_v, aux_w (stage 3 only)
     const GeoIJ<C>* geo;
     const C* cp_tab;
+    const double* heat;      // [jm][km] heating rate in K/s (aturan_set_heating), or null: no such term
     RhsConst<C> k;
     C c_in, wgt;
     int stage;
@@ -500,8 +501,9 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
             else if(precip_t >  C(0.5)) precip_t =  C(0.5);
             else if(precip_t < -C(0.5)) precip_t = -C(0.5);
         }
-        const C rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
-                        - tmf + C(0.0) + precip_t;
+        C rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
+                  - tmf + C(0.0) + precip_t;
+        if(a.heat) rhs_t = rhs_t + K.heat_scale * (C)a.heat[(size_t)j * g.km + k];   // not in the reference
         stage_update(a, ATURAN_T, o, rhs_t, 1, anT);
     }
     }
@@ -625,12 +627,15 @@ __global__ void __launch_bounds__(256) buoy_serial_kernel(Grid g, const S* t, co
 // ---- RungeKutta_Uran_Turb.cpp:62-177: per column (j, k) -- every column, the seam copy and the
 // pole rows included -- the trapezoid integral from the base of the buoyancy anomaly and the
 // metric + radial Coriolis force, plus p_baro minus what p_bfollow has taken up of B(t) - B0.
-// One thread per column, marching up i with coalesced rows along k. ----
+// One thread per column, marching up i with coalesced rows along k; the inputs and outputs do not
+// alias (restrict), so the loads of later levels run ahead of the stores of earlier ones. ----
 template <typename S>
-__global__ void __launch_bounds__(256) hydro_kernel(Grid g, const S* t, const S* ps, const S* v, const S* w,
-                                                    const double* ref, const double* rm_i, const double* cor_j,
-                                                    const double* pbaro, const double* pb0, double* pbf,
-                                                    double* ph, HydroConst h, int advance){
+__global__ void __launch_bounds__(256) hydro_kernel(Grid g, const S* __restrict__ t, const S* __restrict__ ps,
+                                                    const S* __restrict__ v, const S* __restrict__ w,
+                                                    const double* __restrict__ ref, const double* __restrict__ rm_i,
+                                                    const double* __restrict__ cor_j, const double* __restrict__ pbaro,
+                                                    const double* __restrict__ pb0, double* __restrict__ pbf,
+                                                    double* __restrict__ ph, HydroConst h, int advance){
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if(c >= g.jm * g.km) return;
     const int j = c / g.km, k = c - j * g.km;
@@ -651,6 +656,7 @@ __global__ void __launch_bounds__(256) hydro_kernel(Grid g, const S* t, const S*
     if(h.follow_on){
         double Pm = 0.0, Pb = 0.0;
         double m_prev = met0(0), b_prev = buoy(0);
+#pragma unroll 4
         for(int i = 0; i < g.im; i++){
             if(i > 0){
                 const double m_i = met0(i), b_i = buoy(i);

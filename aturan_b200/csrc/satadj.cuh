@@ -18,6 +18,7 @@ namespace aturan {
 struct GasConst {
     double t_0, t_00, ep, lv, ls;
     double C, L0, den, del_alf, del_bet;        // den = 1e-3 * R (ATPhys.h:52)
+    double inv_den;                             // 1 / den (the mixed form's fast vapour pressure)
     double C_i, L0_i, del_alf_i, del_bet_i;
     double t_range_inv, Lf;
     int freeze_on;
@@ -44,8 +45,26 @@ struct SatArgs {
     unsigned long long* counters;   // [0] adjusted, [1] not converged (summed over gases)
 };
 
+// The saturation vapour density rho ep svp(T) / p of the liquid (ice = false) or ice set.
+// FP64 path (exact): the reference's expression and operand order, bit for bit. Mixed path
+// (FAST): the same FP64 mathematics with the divisions folded into per-cell and per-gas
+// reciprocals and log(T), 1/T shared by the liquid and ice sets at one T -- a few ulps
+// different, which the mixed form allows, and about a third fewer FP64 divisions and logs.
+struct SatT { double T, lg, inv; };
+__device__ __forceinline__ SatT sat_t(double T){ SatT r; r.T = T; r.lg = log(T); r.inv = 1.0 / T; return r; }
+
+template <bool FAST>
+__device__ __forceinline__ double qsat(const GasConst& G, bool ice, double rho_c, double ep, double p_u,
+                                       double rep, double T, const SatT& st){
+    const double C = ice ? G.C_i : G.C, L0 = ice ? G.L0_i : G.L0;
+    const double al = ice ? G.del_alf_i : G.del_alf, be = ice ? G.del_bet_i : G.del_bet;
+    if constexpr(FAST) return rep * exp(C + (-L0 * st.inv + al * st.lg + be * st.T) * G.inv_den);
+    else return rho_c * ep * svp(T, C, L0, G.den, al, be) / p_u;
+}
+
 template <typename S>
 __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
+    constexpr bool FAST = sizeof(S) == 4;            // the mixed form
     const Grid& g = a.g;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -103,23 +122,25 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                 if(ice < 0.0) ice = 0.0;
 
                 const double ep = G.ep, lv = G.lv, ls = G.ls, tri = G.t_range_inv;
-                const double q_Rain_0 = rho_c * ep * svp(t_u, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
+                const double rep = FAST ? rho_c * ep / p_u : 0.0;
+                SatT st0;
+                if constexpr(FAST) st0 = sat_t(t_u);
+                const double q_Rain_0 = qsat<FAST>(G, false, rho_c, ep, p_u, rep, t_u, st0);
                 bool go = q_Rain_0 > 0.0;                             // :422
                 if(go){
                     double q_entry = q_Rain_0;
                     if(K.ice_entry && cloud <= 0.0 && ice <= 0.0){
                         const double cnd0 = t_u <= t_00 ? 0.0 : (t_u >= t_0 ? 1.0 : (t_u - t_00) * tri);
                         if(cnd0 < 1.0)
-                            q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * rho_c * ep
-                                    * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * qsat<FAST>(G, true, rho_c, ep, p_u, rep, t_u, st0);
                     }
                     if(K.bergeron >= 2 && cloud <= 0.0 && ice <= 0.0 && t_u < t_0)
-                        q_entry = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                        q_entry = qsat<FAST>(G, true, rho_c, ep, p_u, rep, t_u, st0);
                     if(c <= q_entry){                                 // :436-448
                         const double q_c0 = cloud, q_i0 = ice;
                         if(!K.evap || !K.conserve || (q_c0 <= 0.0 && q_i0 <= 0.0)) go = false;
                         else {
-                            const double q_Ice_0 = rho_c * ep * svp(t_u, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u;
+                            const double q_Ice_0 = qsat<FAST>(G, true, rho_c, ep, p_u, rep, t_u, st0);
                             double q_t0;
                             if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
                             else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
@@ -175,9 +196,10 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                             if(K.ice_entry && q_c_b <= 0.0 && q_i_b <= 0.0) return 3;
                             return (q_i_b == 0.0) ? 1 : 2;
                         };
-                        const double q_Rain = rho_c * ep * svp(T, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u;
-                        const double q_Ice  = (need(T) & 2)
-                            ? rho_c * ep * svp(T, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u : 0.0;
+                        SatT stT;
+                        if constexpr(FAST) stT = sat_t(T);
+                        const double q_Rain = qsat<FAST>(G, false, rho_c, ep, p_u, rep, T, stT);
+                        const double q_Ice  = (need(T) & 2) ? qsat<FAST>(G, true, rho_c, ep, p_u, rep, T, stT) : 0.0;
                         q_rain_now = q_Rain;
                         if(q_c_b > 0.0 && q_i_b > 0.0)
                             q_v_hyp = (q_c_b * q_Rain + q_i_b * q_Ice) / (q_c_b + q_i_b);
@@ -211,10 +233,10 @@ __global__ void __launch_bounds__(128) satadj_kernel(const SatArgs<S> a){
                         if(K.newton){
                             const double dT = 0.1;
                             const int nd = need(T);
-                            const double q_Rain_d = (nd & 1)
-                                ? rho_c * ep * svp(T + dT, G.C, G.L0, G.den, G.del_alf, G.del_bet) / p_u : 0.0;
-                            const double q_Ice_d  = (nd & 2)
-                                ? rho_c * ep * svp(T + dT, G.C_i, G.L0_i, G.den, G.del_alf_i, G.del_bet_i) / p_u : 0.0;
+                            SatT stD;
+                            if constexpr(FAST) stD = sat_t(T + dT);
+                            const double q_Rain_d = (nd & 1) ? qsat<FAST>(G, false, rho_c, ep, p_u, rep, T + dT, stD) : 0.0;
+                            const double q_Ice_d  = (nd & 2) ? qsat<FAST>(G, true, rho_c, ep, p_u, rep, T + dT, stD) : 0.0;
                             double q_hyp_d;
                             if(q_c_b > 0.0 && q_i_b > 0.0)
                                 q_hyp_d = (q_c_b * q_Rain_d + q_i_b * q_Ice_d) / (q_c_b + q_i_b);

@@ -192,9 +192,16 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
  * auxbar[3] (or NULL) is the adjoint of the step's projection outputs aux_u, aux_v, aux_w (the
  * stage-3 tendencies of u, v, w without the p_dyn gradient, which the next pressure solve reads;
  * RHS_Uran_Turb.cpp:1020-1022), and pbar (or NULL) receives the adjoint of the p_dyn the step
- * read, all [im][jm][km] FP64 device arrays. */
+ * read, all [im][jm][km] FP64 device arrays; heatbar (or NULL) receives the adjoint of the
+ * heating field of aturan_set_heating, a [jm][km] FP64 device array. */
 int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
-                          double* const* xbar, double* pbar);
+                          double* const* xbar, double* pbar, double* heatbar);
+
+/* A heating rate H(theta, phi) in K/s added to the temperature tendency at every interior level,
+ * rhs_t += H (L_atm 1e3 / u_0) / t_ref (no counterpart in the reference, whose heating enters as
+ * Q_rad in W/m^3, RHS_Uran_Turb.cpp:503-526). H: [jm][km] FP64, host or device (on_device);
+ * NULL removes the term (the default: the step is then the reference's, bit for bit). */
+int aturan_set_heating(aturan_ctx* ctx, const double* H, int on_device);
 
 /* Adjoint of the last taped ATURAN_PRESS_RB_SOR / RB_LINE pressure call (no counterpart in the
  * reference): given pbar, the adjoint of the p_dyn it produced (boundary rows included), writes
