@@ -1006,15 +1006,26 @@ static int xfer(aturan_ctx* ctx, int field, void* other, bool up, bool other_is_
     void* dev = field_ptr(ctx, field, &is64);
     const Grid& g = ctx->g;
     const size_t rows = (size_t)g.im * g.jm;
-    const cudaMemcpyKind kind = other_is_device ? cudaMemcpyDeviceToDevice : (up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost);
-    double* d64 = is64 ? reinterpret_cast<double*>(dev) : ctx->stage64;
+    // One contiguous copy of the caller's [im][jm][km] array into (out of) the staging field, and a
+    // kernel that changes the layout to the padded rows (and the type, for FP32 fields): one large
+    // DMA instead of im*jm row-sized ones. A device-side caller buffer is read (written) directly.
+    const size_t n = rows * g.km;
     if(up){
-        CK(cudaMemcpy2DAsync(d64, g.kp * 8, other, g.km * 8, g.km * 8, rows, kind, ctx->st));
-        if(!is64){ launch_f64_to_f32(ctx->stage64, reinterpret_cast<float*>(dev), g.fstride, ctx->st); CK_LAUNCH("f64->f32"); }
+        const double* src_c = reinterpret_cast<const double*>(other);
+        if(!other_is_device){
+            CK(cudaMemcpyAsync(ctx->stage64, other, n * 8, cudaMemcpyHostToDevice, ctx->st));
+            src_c = ctx->stage64;
+        }
+        if(is64) launch_pack_in_f64(src_c, reinterpret_cast<double*>(dev), g.km, g.kp, rows, ctx->st);
+        else     launch_pack_in_f32(src_c, reinterpret_cast<float*>(dev), g.km, g.kp, rows, ctx->st);
+        CK_LAUNCH("layout in");
         if(!other_is_device) CK(cudaStreamSynchronize(ctx->st));
     } else {
-        if(!is64){ launch_f32_to_f64(reinterpret_cast<const float*>(dev), ctx->stage64, g.fstride, ctx->st); CK_LAUNCH("f32->f64"); }
-        CK(cudaMemcpy2DAsync(other, g.km * 8, d64, g.kp * 8, g.km * 8, rows, kind, ctx->st));
+        double* tgt = other_is_device ? reinterpret_cast<double*>(other) : ctx->stage64;
+        if(is64) launch_pack_out_f64(reinterpret_cast<const double*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+        else     launch_pack_out_f32(reinterpret_cast<const float*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+        CK_LAUNCH("layout out");
+        if(!other_is_device) CK(cudaMemcpyAsync(other, ctx->stage64, n * 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
     }
     return ATURAN_OK;

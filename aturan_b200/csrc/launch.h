@@ -37,6 +37,10 @@ void launch_rb_colour(Grid g, double* P, const double* src, const RBW* w, int co
 
 // Layout conversions for the mixed-precision context (FP64 exchange <-> FP32 storage).
 void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st);
+void launch_pack_in_f64(const double* in, double* out, int km, int kp, size_t rows, cudaStream_t st);
+void launch_pack_in_f32(const double* in, float* out, int km, int kp, size_t rows, cudaStream_t st);
+void launch_pack_out_f64(const double* in, double* out, int km, int kp, size_t rows, cudaStream_t st);
+void launch_pack_out_f32(const float* in, double* out, int km, int kp, size_t rows, cudaStream_t st);
 void launch_f32_to_f64(const float* in, double* out, size_t n, cudaStream_t st);
 
 }  // namespace aturan

@@ -27,6 +27,39 @@ void launch_scale_copy_f32(const float* in, float* out, size_t n, double coeff, 
     scale_copy_f32_kernel<<<148 * 8, 256, 0, st>>>(in, out, n, coeff);
 }
 
+// Contiguous [im][jm][km] FP64 <-> padded [im][jm][kp] field of type T (the layout change and,
+// for FP32 fields, the conversion in one pass): one thread per element of a row's first km.
+template <typename T>
+__global__ void pack_in_kernel(const double* in, T* out, int km, int kp, size_t rows){
+    const size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= rows || k >= km) return;
+    out[r * kp + k] = (T)in[r * km + k];
+}
+template <typename T>
+__global__ void pack_out_kernel(const T* in, double* out, int km, int kp, size_t rows){
+    const size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= rows || k >= km) return;
+    out[r * km + k] = (double)in[r * kp + k];
+}
+static dim3 pack_grid(int km, size_t rows){
+    const unsigned y = (unsigned)(rows < 65535 ? rows : 65535);
+    return dim3((km + 127) / 128, y, (unsigned)((rows + y - 1) / y));
+}
+void launch_pack_in_f64(const double* in, double* out, int km, int kp, size_t rows, cudaStream_t st){
+    pack_in_kernel<double><<<pack_grid(km, rows), 128, 0, st>>>(in, out, km, kp, rows);
+}
+void launch_pack_in_f32(const double* in, float* out, int km, int kp, size_t rows, cudaStream_t st){
+    pack_in_kernel<float><<<pack_grid(km, rows), 128, 0, st>>>(in, out, km, kp, rows);
+}
+void launch_pack_out_f64(const double* in, double* out, int km, int kp, size_t rows, cudaStream_t st){
+    pack_out_kernel<double><<<pack_grid(km, rows), 128, 0, st>>>(in, out, km, kp, rows);
+}
+void launch_pack_out_f32(const float* in, double* out, int km, int kp, size_t rows, cudaStream_t st){
+    pack_out_kernel<float><<<pack_grid(km, rows), 128, 0, st>>>(in, out, km, kp, rows);
+}
+
 void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st){
     f64_to_f32_kernel<<<148 * 8, 256, 0, st>>>(in, out, n);
 }

@@ -381,7 +381,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers ----
     from aturan_b200 import fields as F
-    # what a CPU driver hands the drop-in every step (INTEGRATION.md's glue): the prognostic fields
+    # what a CPU driver hands the drop-in every step: the prognostic fields
     # and the pointwise RHS inputs its CPU modules (chemistry, precipitation, turbulence closure,
     # boundary conditions, filters) changed; the n-copies, p_dyn, p_hydro, p_bfollow and the
     # constant fields stay resident. Back: the new prognostic fields, p_dyn, p_hydro and the

@@ -3,8 +3,8 @@
  *
  * The reference has no plugin or FFI layer for this path: its call sites are member and friend
  * calls on one cUranusModel object. Each entry point below replaces one of those calls and says
- * which. A maintainer binds them from the reference's driver (planet/cUranusModel.cpp:Run) with
- * the glue shown in INTEGRATION.md, or from Python with ctypes (aturan_b200/_lib.py).
+ * which. A maintainer binds them from the reference's driver (planet/cUranusModel.cpp:Run) with a
+ * compile-time switch around those calls, or from Python with ctypes (aturan_b200/api.py).
  *
  * Conventions
  *   - Every function returns an int status: 0 = ATURAN_OK, negative = error (nothing was

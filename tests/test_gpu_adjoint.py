@@ -283,3 +283,43 @@ def test_config4_dry_heating_gradient():
         worst = max(worst, abs(fd - an) / max(abs(an), 1e-300))
     ctx.close()
     assert worst <= 1e-4, worst
+
+
+@pytest.mark.parametrize("rigid_lid", [1, 0])
+def test_pressure_adjoint_directional(rigid_lid):
+    """aturan_pressure_adjoint against central differences of the pressure call itself (aux ->
+    p_dyn: boundary rows, divergence, compatibility shift, solve, boundary passes), with the rigid
+    lid (aux_u = 0 on the radial boundary rows) and without it (cubic extrapolation)."""
+    p = P.default_params(21, 37, 73)
+    p.rigid_lid = rigid_lid
+    st = S.synthetic_state(p, seed=93)
+    ctx = api.Context(p)
+    ctx.upload_state(st)
+    ctx.tape(True)
+    aux0 = [torch.tensor(st[n], device="cuda") for n in ("aux_u", "aux_v", "aux_w")]
+    zero = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    out = torch.empty(p.shape, dtype=torch.float64, device="cuda")
+
+    def solve(aux):
+        torch.cuda.synchronize()
+        for n, a in zip(("aux_u", "aux_v", "aux_w"), aux):
+            ctx.upload_device(n, a.contiguous().data_ptr())
+        ctx.upload_device("p_dyn", zero.data_ptr())
+        ctx.pressure(P.PRESS_RB_LINE, omega=1.0, max_sweeps=200, tol=1e-11)
+        ctx.download_device("p_dyn", out.data_ptr())
+        return out.clone()
+
+    rng = np.random.default_rng(93)
+    pbar = torch.tensor(rng.standard_normal(p.shape), device="cuda")
+    pbar -= pbar.mean()                                 # the solve leaves p's constant free
+    d = [torch.tensor(rng.standard_normal(p.shape), device="cuda") * 1e-2 * float(a.abs().max()) for a in aux0]
+    h = 1e-2
+    fd = float(((solve([a + h * x for a, x in zip(aux0, d)]) - solve([a - h * x for a, x in zip(aux0, d)]))
+                * pbar).sum()) / (2 * h)
+    solve(aux0)                                         # tapes the call the adjoint reverses
+    abar = [torch.empty(p.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    ctx.pressure_adjoint(pbar.data_ptr(), [a.data_ptr() for a in abar], P.PRESS_RB_LINE, 1.0, 200, 1e-11)
+    ctx.close()
+    an = float(sum((a * x).sum() for a, x in zip(abar, d)))
+    assert abs(fd - an) <= 1e-6 * abs(an), (fd, an)
