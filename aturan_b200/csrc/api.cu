@@ -414,21 +414,16 @@ int run_rb(aturan_ctx* ctx, int sweeps, double omega){
 }
 
 // ---- RB_SOR: the shared solver's equation to a relative L2 residual (sor.cuh) ----
-template <typename T>
-void bc_passes(aturan_ctx* ctx, T* P){
-    const Grid g = ctx->g;
-    bc_r_kernel<T><<<dim3((g.km + 127) / 128, g.jm), 128, 0, ctx->st>>>(g, P);
-    bc_t_kernel<T><<<dim3((g.km + 127) / 128, g.im), 128, 0, ctx->st>>>(g, P);
-    bc_p_kernel<T><<<(g.im * g.jm + 255) / 256, 256, 0, ctx->st>>>(g, P);
-}
 
 // Residual of P against src: relative L2 norm (host sum of the block partials, fixed order).
 // TR: of the transposed operator.
 template <typename T, bool TR = false>
-int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr){
+int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr,
+                 bool fill32 = false){
     const Grid g = ctx->g;
     sor_colsum_kernel<T, TR><<<dim3((g.km - 1 + 31) / 32, g.jm - 2), dim3(32, 8), 0, ctx->st>>>(
-        g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0);
+        g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0,
+        fill32 ? ctx->r32 : nullptr, fill32 ? ctx->e32 : nullptr);
     CK_LAUNCH("residual");
     if(!rel) return ATURAN_OK;                                 // column sums only: no host round trip
     CK(cudaMemcpyAsync(ctx->host_part.data(), ctx->sor_part, 2 * ctx->sor_nblk * 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -564,19 +559,19 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
         // FP32 sweeps per refinement step: for line SOR 2 (measured at 41x181x361, warm: two
         // refinement steps of 2 reach 3e-8 against 6 sweeps with 3 per step, 0.53 vs 0.59 ms)
         const int inner = line ? 2 : 48;
-        rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
+        // Each FP64 residual also leaves r in FP32, e = 0 and the column sums of r: what the next
+        // correction solve starts from (one pass over p and src per refinement step).
+        rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
-            sor_resid32_kernel<<<dim3((g.km + 127) / 128, g.jm, g.im), 128, 0, ctx->st>>>(g, P, src, ctx->rbw, ctx->r32, ctx->e32);
-            nl++;
             for(int n = 0; n < inner && s < max_sweeps; n++, s++){
                 // the correction on the same cadence as the FP64 solve (once per `every` sweeps,
                 // counted over the whole solve): after the first one the column-uniform error is
                 // gone and a later refinement step's correction changes nothing (measured: same
-                // sweep count, 0.14 ms less at 41x181x361)
+                // sweep count, 0.14 ms less at 41x181x361); with e = 0 its column sums are r's
                 if(s % every == 0){
-                    rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc;
+                    if(n != 0){ rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc; nl++; }
                     rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
-                    nl += 5;
+                    nl += 4;
                 }
                 sor_sweep<float>(ctx, ctx->e32, ctx->r32, omega, line);
                 nl += 2;
@@ -584,7 +579,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
             sor_axpy_kernel<<<148 * 8, 256, 0, ctx->st>>>(fs, P, ctx->e32);
             CK_LAUNCH("SOR refinement");
             nl++;
-            rc = sor_residual<double>(ctx, P, src, false, &r, nullptr); if(rc) return rc; nl++;
+            rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true); if(rc) return rc; nl++;
         }
         status = r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
     }

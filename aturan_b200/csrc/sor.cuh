@@ -97,13 +97,15 @@ __device__ __forceinline__ double row_acc(const Grid& g, const T* P, size_t o, i
 }
 
 // Residual r = src - Lc p of the folded operator (or src - Lc^T p, TR): per (j,k) column its
-// y-weighted (TR: plain) sum over the interior levels, and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
+// y-weighted (TR: plain) sum over the interior levels (and, given r32/e32, r rounded to FP32 with
+// e = 0 on the interior for the mixed form's correction solve), and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
 // groups; the groups' column sums are added in group order and the block's norms in a fixed tree
 // order, so the result is deterministic. P and src of type T (double: FP64 solve; float: the
 // correction solve of the mixed form).
 template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, const T* src, const RBW* w,
-                                                         double* colR, double* part, int want_col){
+                                                         double* colR, double* part, int want_col,
+                                                         float* r32 = nullptr, float* e32 = nullptr){
     const int N = g.km - 1;
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int j = 1 + blockIdx.y;
@@ -118,6 +120,7 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
             const double lc = acc - diag * (double)P[o];
             const double s = (double)src[o];
             const double r = s - lc;
+            if(r32){ r32[o] = (float)r; e32[o] = 0.0f; }  // the mixed form's next correction solve
             R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
             rr += r * r;
             ss += s * s;
@@ -402,31 +405,6 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
     }
 }
 
-// The folded boundary passes for any T (same order as pdyn_bc_*).
-template <typename T>
-__global__ void bc_r_kernel(Grid g, T* P){
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if(k >= g.km) return;
-    P[gidx(g, 0, j, k)]        = (T)(C43 * (double)P[gidx(g, 1, j, k)] - C13 * (double)P[gidx(g, 2, j, k)]);
-    P[gidx(g, g.im - 1, j, k)] = (T)(C43 * (double)P[gidx(g, g.im - 2, j, k)] - C13 * (double)P[gidx(g, g.im - 3, j, k)]);
-}
-template <typename T>
-__global__ void bc_t_kernel(Grid g, T* P){
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if(k >= g.km) return;
-    P[gidx(g, i, 0, k)]        = (T)(C43 * (double)P[gidx(g, i, 1, k)] - C13 * (double)P[gidx(g, i, 2, k)]);
-    P[gidx(g, i, g.jm - 1, k)] = (T)(C43 * (double)P[gidx(g, i, g.jm - 2, k)] - C13 * (double)P[gidx(g, i, g.jm - 3, k)]);
-}
-template <typename T>
-__global__ void bc_p_kernel(Grid g, T* P){
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if(c >= g.im * g.jm) return;
-    const int i = c / g.jm, j = c - i * g.jm;
-    P[gidx(g, i, j, g.km - 1)] = P[gidx(g, i, j, 0)];
-}
-
 // Compatibility: per-block partial sums of y_i y_j src and y_i y_j over the interior (plain: of
 // src and 1, the transposed operator's left null vector being the constant).
 __global__ void __launch_bounds__(256) sor_ysum_kernel(Grid g, const double* src, double* part, int plain){
@@ -476,23 +454,8 @@ __global__ void sor_shift_kernel(Grid g, double* src, const double* shift_p){
     }
 }
 
-// Mixed form: r = src - Lc p in FP64, stored as FP32 for the correction solve; e cleared.
-__global__ void sor_resid32_kernel(Grid g, const double* P, const double* src, const RBW* w, float* r32, float* e32){
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    const int i = blockIdx.z;
-    if(k >= g.km) return;
-    const size_t o = gidx(g, i, j, k);
-    e32[o] = 0.0f;
-    if(i == 0 || i == g.im - 1 || j == 0 || j == g.jm - 1 || k == g.km - 1){ r32[o] = 0.0f; return; }
-    const RBW W = w[i * g.jm + j];
-    double diag;
-    const double acc = folded_acc<double>(g, P, o, i, j, k, W, &diag);
-    const double lc = acc - diag * P[o];
-    r32[o] = (float)(src[o] - lc);
-}
-
-// Mixed form: p += e over every cell (e carries its own folded boundary rows).
+// Mixed form: p += e over every cell (e is zero on the boundary rows and the seam column, which no
+// correction solve writes).
 __global__ void sor_axpy_kernel(size_t n, double* P, const float* e){
     for(size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
         P[t] += (double)e[t];
