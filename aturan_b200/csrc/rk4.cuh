@@ -223,6 +223,118 @@ __device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const Sc
     stage_update(a, scalar_field(n), o, r, scalar_kind(n), in.an);
 }
 
+// Everything the momentum and temperature tendencies of one cell read: the stencils of u, v, w,
+// t, the p_dyn and p_hydro neighbours (FP64), the accumulators and n-copies, two forcing values.
+template <typename C>
+struct MomIn {
+    R7<C> rU, rV, rW, rT;
+    double p_ip, p_im, p_jp, p_jm, p_ke, p_kw, ph_jp, ph_jm, ph_ke, ph_kw;
+    AccNc<C> anU, anV, anW, anT;
+    C f_tmf, f_qp;
+};
+
+template <typename S, typename C>
+__device__ __forceinline__ void load_momentum(MomIn<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb,
+                                              const RhsConst<C>& K){
+    const double* P = a.pdyn;
+    const double* PH = a.phydro;
+    in.p_ip = ld(P + nb.oip); in.p_im = ld(P + nb.oim); in.p_jp = ld(P + nb.ojp); in.p_jm = ld(P + nb.ojm);
+    in.p_ke = ld(P + nb.oke); in.p_kw = ld(P + nb.okw);
+    in.ph_jp = ld(PH + nb.ojp); in.ph_jm = ld(PH + nb.ojm); in.ph_ke = ld(PH + nb.oke); in.ph_kw = ld(PH + nb.okw);
+    in.rU = load7<S, C>(nb, ATURAN_U); in.rV = load7<S, C>(nb, ATURAN_V); in.rW = load7<S, C>(nb, ATURAN_W);
+    in.rT = load7<S, C>(nb, ATURAN_T);
+    in.anU = load_acc_nc(a, ATURAN_U, nb.o); in.anV = load_acc_nc(a, ATURAN_V, nb.o);
+    in.anW = load_acc_nc(a, ATURAN_W, nb.o); in.anT = load_acc_nc(a, ATURAN_T, nb.o);
+    const S* F = a.forc + nb.o;
+    in.f_tmf = (K.tmf != C(0.0)) ? (C)ld(F + (size_t)(ATURAN_THERMALMASSFLUX - ATURAN_NUE) * nb.fs) : C(0.0);
+    in.f_qp = (K.precip_coupling != C(0.0)) ? (C)ld(F + (size_t)(ATURAN_Q_PRECIP - ATURAN_NUE) * nb.fs) : C(0.0);
+}
+
+// The tendencies of u, v, w and t of one cell (RHS_Uran_Turb.cpp:117-175, :208-331, :382-391,
+// :528-557, :717-788) and the pressure-gradient terms aux needs (:1020-1022). j, k locate the
+// heating field's value.
+template <typename S, typename C>
+__device__ __forceinline__ void momentum_rhs(const StageArgs<S, C>& a, const MomIn<C>& in, const GeoIJ<C>& geo,
+                                             C nue_t, C nue_t_s, int j, int k, C& rhs_u, C& rhs_v, C& rhs_w,
+                                             C& rhs_t, C& dpdr_term, C& dpdthe_term, C& dpdphi_term){
+    const RhsConst<C>& K = a.k;
+    const C inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rmsinthe = geo.inv_rmsinthe;
+    const C inv_rm2sinthe = geo.inv_rm2sinthe, inv_rm2sinthe2 = geo.inv_rm2sinthe2;
+    const C costhe_inv_rm2sinthe = geo.costhe_inv_rm2sinthe, costhe = geo.costhe;
+    const C cotanthe = geo.cotanthe, two_inv_rm = geo.two_inv_rm;
+    // pressure gradients (:117, :146, :175), FP64 differences
+    const C dpdr   = (C)((in.p_ip - in.p_im) * (double)K.inv_2dr);
+    const C dpdthe = (C)((in.p_jp - in.p_jm) * (double)K.inv_2dthe);
+    const C dpdphi = (C)((in.p_ke - in.p_kw) * (double)K.inv_2dphi);
+
+    const D6<C> U = diff6(K, in.rU), V = diff6(K, in.rV), W = diff6(K, in.rW);
+    const C u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
+    const C v_invrm = v_ijk * inv_rm;
+    const C w_invrs = w_ijk * inv_rmsinthe;
+    // ---- momentum ----
+    {
+        const C sinthe_bf = geo.sinthe_bf;
+        const C Coriolis_rad = K.m2om * sinthe_bf * w_ijk;
+        const C Coriolis_the = K.m2om * costhe * w_ijk;
+        const C Coriolis_phi = K.p2om * (costhe * v_ijk + sinthe_bf * u_ijk);
+        const C transport_u = u_ijk * U.d1r + v_invrm * U.d1t + w_invrs * U.d1p
+            - C(0.0) * (v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
+        const C transport_v = u_ijk * V.d1r + v_invrm * V.d1t + w_invrs * V.d1p
+            + (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
+        const C transport_w = u_ijk * W.d1r + v_invrm * W.d1t + w_invrs * W.d1p
+            + (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
+        const C v_metric = geo.v_metric;
+        const C diffusion_u = U.d2r + C(2.0) * u_ijk * inv_rm2 + U.d2t * inv_rm2
+            + C(4.0) * U.d1r * inv_rm + U.d1t * costhe_inv_rm2sinthe
+            + U.d2p * inv_rm2sinthe2;
+        const C diffusion_v = V.d2r + V.d1r * two_inv_rm + V.d2t * inv_rm2
+            + V.d1t * costhe_inv_rm2sinthe - v_metric * v_ijk
+            + V.d2p * inv_rm2sinthe2
+            + C(2.0) * U.d1t * inv_rm2
+            - W.d1p * C(2.0) * costhe * inv_rm2sinthe2;
+        const C diffusion_w = W.d2r + W.d1r * two_inv_rm + W.d2t * inv_rm2
+            + W.d1t * costhe_inv_rm2sinthe - v_metric * w_ijk
+            + W.d2p * inv_rm2sinthe2
+            + C(2.0) * U.d1p * inv_rm2sinthe
+            + V.d1p * C(2.0) * costhe * inv_rm2sinthe2;
+        dpdr_term   = dpdr   * K.scale_p;
+        dpdthe_term = dpdthe * K.scale_p * inv_rm;
+        dpdphi_term = dpdphi * K.scale_p * inv_rmsinthe;
+        const C dphdthe_term = (C)((in.ph_jp - in.ph_jm) * (double)K.inv_2dthe) * inv_rm;
+        const C dphdphi_term = (C)((in.ph_ke - in.ph_kw) * (double)K.inv_2dphi) * inv_rmsinthe;
+        const C re_eff = K.re_eff;
+        rhs_u = - dpdr_term + C(0.0) - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
+                - K.cor_rad_f * Coriolis_rad
+                + K.cen_f * geo.cent_rad
+                - geo.sponge * u_ijk;
+        rhs_v = - dpdthe_term - dphdthe_term - transport_v + diffusion_v / re_eff + diffusion_v * nue_t
+                - K.cor_sc * Coriolis_the
+                + K.cen_f * geo.cent_the;
+        rhs_w = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
+                - K.cor_sc * Coriolis_phi;
+    }
+    // ---- temperature ----
+    {
+        const D6<C> T = diff6(K, in.rT);
+        C pressure_t = K.ce_sp * (u_ijk * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
+        if(K.cp_dyn && T.c > C(0.0)) pressure_t *= K.cp_mix / cp_lapse(K, a.cp_tab, T.c * K.t_ref);
+        const C transport_t = u_ijk * T.d1r + v_invrm * T.d1t + w_invrs * T.d1p;
+        const C diffusion_t = T.d2r + T.d1r * two_inv_rm + T.d2t * inv_rm2
+            + T.d1t * costhe_inv_rm2sinthe + T.d2p * inv_rm2sinthe2;
+        const C tmf = (K.tmf != C(0.0)) ? K.tmf * in.f_tmf : C(0.0);
+        C precip_t = C(0.0);
+        if(K.precip_coupling != C(0.0)){
+            precip_t = K.precip_coupling * in.f_qp * K.precip_L / K.precip_den;
+            if(!isfinite(precip_t)) precip_t = C(0.0);
+            else if(precip_t >  C(0.5)) precip_t =  C(0.5);
+            else if(precip_t < -C(0.5)) precip_t = -C(0.5);
+        }
+        rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
+                - tmf + C(0.0) + precip_t;
+        if(a.heat) rhs_t = rhs_t + K.heat_scale * (C)a.heat[(size_t)j * a.g.km + k];   // not in the reference
+    }
+}
+
 // ---- two cells per thread along k (the scalar launch's vectorised form) ----
 // Cells k0 and k0 + 1 (k0 even; km - 1 is even, so a pair never straddles the seam): the centre,
 // r and theta neighbours come as one 8-byte (FP32) or 16-byte (FP64) load each, the k neighbours
@@ -410,102 +522,22 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
 
     if constexpr(PART == 1){
     // ---- every load of the cell first ----
-    const double* P = a.pdyn;
-    const double* PH = a.phydro;
-    const double p_ip = ld(P + oip), p_im = ld(P + oim), p_jp = ld(P + ojp), p_jm = ld(P + ojm);
-    const double p_ke = ld(P + oke), p_kw = ld(P + okw);
-    const double ph_jp = ld(PH + ojp), ph_jm = ld(PH + ojm), ph_ke = ld(PH + oke), ph_kw = ld(PH + okw);
-    const R7<C> rU = load7<S, C>(nb, ATURAN_U), rV = load7<S, C>(nb, ATURAN_V), rW = load7<S, C>(nb, ATURAN_W);
-    const R7<C> rT = load7<S, C>(nb, ATURAN_T);
-    const AccNc<C> anU = load_acc_nc(a, ATURAN_U, o), anV = load_acc_nc(a, ATURAN_V, o);
-    const AccNc<C> anW = load_acc_nc(a, ATURAN_W, o), anT = load_acc_nc(a, ATURAN_T, o);
-    const C f_tmf = (K.tmf != C(0.0)) ? FORC(ATURAN_THERMALMASSFLUX) : C(0.0);
-    const C f_qp = (K.precip_coupling != C(0.0)) ? FORC(ATURAN_Q_PRECIP) : C(0.0);
-
-    // pressure gradients (:117, :146, :175), FP64 differences
-    const C dpdr   = (C)((p_ip - p_im) * (double)K.inv_2dr);
-    const C dpdthe = (C)((p_jp - p_jm) * (double)K.inv_2dthe);
-    const C dpdphi = (C)((p_ke - p_kw) * (double)K.inv_2dphi);
-
-    const D6<C> U = diff6(K, rU), V = diff6(K, rV), W = diff6(K, rW);
-    const C u_ijk = U.c, v_ijk = V.c, w_ijk = W.c;
-    const C v_invrm = v_ijk * inv_rm;
-    const C w_invrs = w_ijk * inv_rmsinthe;
-    // ---- momentum (:208-331, :382-391, :717-788) ----
-    {
-        const C sinthe_bf = geo.sinthe_bf;
-        const C Coriolis_rad = K.m2om * sinthe_bf * w_ijk;
-        const C Coriolis_the = K.m2om * costhe * w_ijk;
-        const C Coriolis_phi = K.p2om * (costhe * v_ijk + sinthe_bf * u_ijk);
-        const C transport_u = u_ijk * U.d1r + v_invrm * U.d1t + w_invrs * U.d1p
-            - C(0.0) * (v_ijk * v_ijk + w_ijk * w_ijk) * inv_rm;
-        const C transport_v = u_ijk * V.d1r + v_invrm * V.d1t + w_invrs * V.d1p
-            + (u_ijk * v_ijk - w_ijk * w_ijk * cotanthe) * inv_rm;
-        const C transport_w = u_ijk * W.d1r + v_invrm * W.d1t + w_invrs * W.d1p
-            + (w_ijk * u_ijk + v_ijk * w_ijk * cotanthe) * inv_rm;
-        const C v_metric = geo.v_metric;
-        const C diffusion_u = U.d2r + C(2.0) * u_ijk * inv_rm2 + U.d2t * inv_rm2
-            + C(4.0) * U.d1r * inv_rm + U.d1t * costhe_inv_rm2sinthe
-            + U.d2p * inv_rm2sinthe2;
-        const C diffusion_v = V.d2r + V.d1r * two_inv_rm + V.d2t * inv_rm2
-            + V.d1t * costhe_inv_rm2sinthe - v_metric * v_ijk
-            + V.d2p * inv_rm2sinthe2
-            + C(2.0) * U.d1t * inv_rm2
-            - W.d1p * C(2.0) * costhe * inv_rm2sinthe2;
-        const C diffusion_w = W.d2r + W.d1r * two_inv_rm + W.d2t * inv_rm2
-            + W.d1t * costhe_inv_rm2sinthe - v_metric * w_ijk
-            + W.d2p * inv_rm2sinthe2
-            + C(2.0) * U.d1p * inv_rm2sinthe
-            + V.d1p * C(2.0) * costhe * inv_rm2sinthe2;
-        const C dpdr_term   = dpdr   * K.scale_p;
-        const C dpdthe_term = dpdthe * K.scale_p * inv_rm;
-        const C dpdphi_term = dpdphi * K.scale_p * inv_rmsinthe;
-        const C dphdthe_term = (C)((ph_jp - ph_jm) * (double)K.inv_2dthe) * inv_rm;
-        const C dphdphi_term = (C)((ph_ke - ph_kw) * (double)K.inv_2dphi) * inv_rmsinthe;
-        const C re_eff = K.re_eff;
-        const C rhs_u = - dpdr_term + C(0.0) - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
-                        - K.cor_rad_f * Coriolis_rad
-                        + K.cen_f * geo.cent_rad
-                        - geo.sponge * u_ijk;
-        const C rhs_v = - dpdthe_term - dphdthe_term - transport_v + diffusion_v / re_eff + diffusion_v * nue_t
-                        - K.cor_sc * Coriolis_the
-                        + K.cen_f * geo.cent_the;
-        const C rhs_w = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
-                        - K.cor_sc * Coriolis_phi;
-        stage_update(a, ATURAN_U, o, rhs_u, 0, anU);
-        stage_update(a, ATURAN_V, o, rhs_v, 0, anV);
-        stage_update(a, ATURAN_W, o, rhs_w, 0, anW);
-        if(a.stage == 3){
-            a.proj[0 * fs + o] = (S)rhs_u;
-            a.proj[1 * fs + o] = (S)rhs_v;
-            a.proj[2 * fs + o] = (S)rhs_w;
-            a.proj[3 * fs + o] = (S)(rhs_u + dpdr_term);
-            a.proj[4 * fs + o] = (S)(rhs_v + dpdthe_term);
-            a.proj[5 * fs + o] = (S)(rhs_w + dpdphi_term);
-        }
+    MomIn<C> in;
+    load_momentum(in, a, nb, K);
+    C rhs_u, rhs_v, rhs_w, rhs_t, dpdr_term, dpdthe_term, dpdphi_term;
+    momentum_rhs(a, in, geo, nue_t, nue_t_s, j, k, rhs_u, rhs_v, rhs_w, rhs_t, dpdr_term, dpdthe_term, dpdphi_term);
+    stage_update(a, ATURAN_U, o, rhs_u, 0, in.anU);
+    stage_update(a, ATURAN_V, o, rhs_v, 0, in.anV);
+    stage_update(a, ATURAN_W, o, rhs_w, 0, in.anW);
+    if(a.stage == 3){
+        a.proj[0 * fs + o] = (S)rhs_u;
+        a.proj[1 * fs + o] = (S)rhs_v;
+        a.proj[2 * fs + o] = (S)rhs_w;
+        a.proj[3 * fs + o] = (S)(rhs_u + dpdr_term);
+        a.proj[4 * fs + o] = (S)(rhs_v + dpdthe_term);
+        a.proj[5 * fs + o] = (S)(rhs_w + dpdphi_term);
     }
-
-    // ---- temperature (:280-298, :329-334, :528-557) ----
-    {
-        const D6<C> T = diff6(K, rT);
-        C pressure_t = K.ce_sp * (u_ijk * dpdr + v_invrm * dpdthe + w_invrs * dpdphi);
-        if(K.cp_dyn && T.c > C(0.0)) pressure_t *= K.cp_mix / cp_lapse(K, a.cp_tab, T.c * K.t_ref);
-        const C transport_t = u_ijk * T.d1r + v_invrm * T.d1t + w_invrs * T.d1p;
-        const C diffusion_t = T.d2r + T.d1r * two_inv_rm + T.d2t * inv_rm2
-            + T.d1t * costhe_inv_rm2sinthe + T.d2p * inv_rm2sinthe2;
-        const C tmf = (K.tmf != C(0.0)) ? K.tmf * f_tmf : C(0.0);
-        C precip_t = C(0.0);
-        if(K.precip_coupling != C(0.0)){
-            precip_t = K.precip_coupling * f_qp * K.precip_L / K.precip_den;
-            if(!isfinite(precip_t)) precip_t = C(0.0);
-            else if(precip_t >  C(0.5)) precip_t =  C(0.5);
-            else if(precip_t < -C(0.5)) precip_t = -C(0.5);
-        }
-        C rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
-                  - tmf + C(0.0) + precip_t;
-        if(a.heat) rhs_t = rhs_t + K.heat_scale * (C)a.heat[(size_t)j * g.km + k];   // not in the reference
-        stage_update(a, ATURAN_T, o, rhs_t, 1, anT);
-    }
+    stage_update(a, ATURAN_T, o, rhs_t, 1, in.anT);
     }
 
     if constexpr(PART == 2){
