@@ -33,7 +33,9 @@ struct aturan_ctx {
     int mixed;                 // 0: FP64 storage, 1: FP32 storage
     size_t esz;                // bytes per stored element
     int device;
-    cudaStream_t st;
+    cudaStream_t st;           // every launch of the context, except:
+    cudaStream_t st2;          // the saturation adjustment inside aturan_step (lower priority)
+    cudaEvent_t ev_fork, ev_join;
     char* mem;                 // one device allocation for everything below
     size_t mem_bytes;
     // storage-type groups (each field fstride elements)
@@ -226,8 +228,9 @@ int validate(const aturan_params* p, std::string& why){
 // Brackets the launches of one kernel class: counts them and, with timing on, records a pair of
 // CUDA events on the context's stream around them.
 struct Region {
-    aturan_ctx* c; int kind; long n; int slot;
-    Region(aturan_ctx* c_, int kind_, long n_) : c(c_), kind(kind_), n(n_), slot(-1){
+    aturan_ctx* c; int kind; long n; int slot; cudaStream_t s;
+    Region(aturan_ctx* c_, int kind_, long n_, cudaStream_t s_ = nullptr)
+        : c(c_), kind(kind_), n(n_), slot(-1), s(s_ ? s_ : c_->st){
         if(!c->prof_timing) return;
         if(c->ev_used == c->evs.size()){
             aturan_ctx::EvPair e{kind, nullptr, nullptr};
@@ -236,11 +239,11 @@ struct Region {
         }
         slot = (int)c->ev_used++;
         c->evs[slot].kind = kind;
-        cudaEventRecord(c->evs[slot].a, c->st);
+        cudaEventRecord(c->evs[slot].a, s);
     }
     ~Region(){
         c->launches[kind] += n;
-        if(slot >= 0) cudaEventRecord(c->evs[slot].b, c->st);
+        if(slot >= 0) cudaEventRecord(c->evs[slot].b, s);
     }
 };
 
@@ -335,7 +338,7 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
 }
 
 template <typename S>
-int run_satadj(aturan_ctx* ctx, int mask, bool count){
+int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st){
     const size_t fs = ctx->g.fstride;
     S* state = reinterpret_cast<S*>(ctx->state);
     SatArgs<S> a;
@@ -349,8 +352,8 @@ int run_satadj(aturan_ctx* ctx, int mask, bool count){
     a.k = ctx->sc;
     a.gas_mask = mask;
     a.counters = count ? ctx->counters : nullptr;
-    Region reg(ctx, ATURAN_K_SATADJ, 1);
-    launch_satadj(a, ctx->st);
+    Region reg(ctx, ATURAN_K_SATADJ, 1, st);
+    launch_satadj(a, st);
     CK_LAUNCH("saturation adjustment");
     return ATURAN_OK;
 }
@@ -678,12 +681,24 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     for(int n = 0; n < 6; n++) add(nij * 8);                           // line factorisations (Lc, Lc^T)
     add(fs * 4); add(fs * 4);
     ctx->mem_bytes = bytes;
-    if(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess){
+    int prio_lo = 0, prio_hi = 0;                         // least and most urgent
+    if(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess){ cudaGetLastError(); prio_lo = prio_hi = 0; }
+    if(cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess){
         delete ctx; return ATURAN_E_CUDA;
+    }
+    if(cudaStreamCreateWithPriority(&ctx->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess){
+        cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_CUDA;
+    }
+    if(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess){
+        cudaGetLastError();
+        if(ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+        cudaStreamDestroy(ctx->st2); cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_CUDA;
     }
     if(cudaMalloc((void**)&ctx->mem, bytes) != cudaSuccess){
         cudaGetLastError();
-        cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_NOMEM;
+        cudaEventDestroy(ctx->ev_fork); cudaEventDestroy(ctx->ev_join);
+        cudaStreamDestroy(ctx->st2); cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_NOMEM;
     }
     char* cur = ctx->mem;
     ctx->state = carve<char>(cur, 19 * fs * e);
@@ -982,11 +997,15 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
 int aturan_ctx_destroy(aturan_ctx* ctx){
     if(!ctx) return ATURAN_E_INVALID;
     if(ctx->st) cudaStreamSynchronize(ctx->st);
+    if(ctx->st2) cudaStreamSynchronize(ctx->st2);
     if(ctx->gs_exec) cudaGraphExecDestroy(ctx->gs_exec);
     if(ctx->tape) cudaFree(ctx->tape);
     if(ctx->heat) cudaFree(ctx->heat);
     for(auto& e : ctx->evs){ cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if(ctx->mem) cudaFree(ctx->mem);
+    if(ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if(ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if(ctx->st2) cudaStreamDestroy(ctx->st2);
     if(ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return ATURAN_OK;
@@ -1239,7 +1258,8 @@ int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_nocon
     if(gas_mask & ~0xF) return fail(ctx, ATURAN_E_INVALID, "gas_mask has bits above 3");
     const bool count = n_adjusted || n_noconv;
     if(count) CK(cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), ctx->st));
-    int rc = ctx->mixed ? run_satadj<float>(ctx, gas_mask, count) : run_satadj<double>(ctx, gas_mask, count);
+    int rc = ctx->mixed ? run_satadj<float>(ctx, gas_mask, count, ctx->st)
+                         : run_satadj<double>(ctx, gas_mask, count, ctx->st);
     if(rc) return rc;
     if(count){
         unsigned long long h[2];
@@ -1251,16 +1271,20 @@ int aturan_satadj(aturan_ctx* ctx, int gas_mask, long* n_adjusted, long* n_nocon
     return ATURAN_OK;
 }
 
-int aturan_sync_ncopies(aturan_ctx* ctx){
-    if(!ctx) return ATURAN_E_INVALID;
+static int sync_ncopies(aturan_ctx* ctx, cudaStream_t st){
     const size_t fs = ctx->g.fstride, e = ctx->esz;
     char* s = (char*)ctx->state; char* n = (char*)ctx->ncopy;
-    Region reg(ctx, ATURAN_K_COPY, 0);
-    CK(cudaMemcpyAsync(n + ATURAN_CH4 * fs * e, s + ATURAN_CH4 * fs * e, 12 * fs * e, cudaMemcpyDeviceToDevice, ctx->st));
-    CK(cudaMemcpyAsync(n, s, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+    Region reg(ctx, ATURAN_K_COPY, 0, st);
+    CK(cudaMemcpyAsync(n + ATURAN_CH4 * fs * e, s + ATURAN_CH4 * fs * e, 12 * fs * e, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(n, s, fs * e, cudaMemcpyDeviceToDevice, st));
     if(ctx->p.nh4sh_sync)
-        CK(cudaMemcpyAsync(n + ATURAN_NH4SH * fs * e, s + ATURAN_NH4SH * fs * e, fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(n + ATURAN_NH4SH * fs * e, s + ATURAN_NH4SH * fs * e, fs * e, cudaMemcpyDeviceToDevice, st));
     return ATURAN_OK;
+}
+
+int aturan_sync_ncopies(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    return sync_ncopies(ctx, ctx->st);
 }
 
 int aturan_restore_ncopies(aturan_ctx* ctx, double coeff){
@@ -1334,14 +1358,24 @@ int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omeg
     return status;
 }
 
+// The reference's order is pressure, saturation adjustment, n-copy sync, RK4. The pressure solve
+// reads and writes p_dyn and the projection fields only; the adjustment and the sync read t,
+// p_stat, rho_mix and the species and write t, the species and their n-copies only. The two are
+// disjoint, so they run side by side with the same results as in order: the adjustment (one
+// large FP64-bound launch) on the low-priority side stream, the solve (a chain of small launches
+// and residual reads) on the main stream, whose blocks the scheduler places first. RK4 waits for
+// both.
 int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol){
     if(!ctx) return ATURAN_E_INVALID;
-    int rc = aturan_pressure(ctx, press_kind, omega, max_sweeps, tol, nullptr, nullptr);
-    if(rc < 0) return rc;
-    int rc2 = aturan_satadj(ctx, 0xF, nullptr, nullptr);
-    if(rc2) return rc2;
-    rc2 = aturan_sync_ncopies(ctx);
-    if(rc2) return rc2;
+    CK(cudaEventRecord(ctx->ev_fork, ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
+    int rc2 = ctx->mixed ? run_satadj<float>(ctx, 0xF, false, ctx->st2)
+                         : run_satadj<double>(ctx, 0xF, false, ctx->st2);
+    if(!rc2) rc2 = sync_ncopies(ctx, ctx->st2);
+    CK(cudaEventRecord(ctx->ev_join, ctx->st2));
+    const int rc = rc2 ? rc2 : aturan_pressure(ctx, press_kind, omega, max_sweeps, tol, nullptr, nullptr);
+    CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));
+    if(rc < 0 || rc2) return rc < 0 ? rc : rc2;
     rc2 = aturan_rk4_step(ctx);
     if(rc2) return rc2;
     return rc;

@@ -12,6 +12,21 @@ namespace aturan {
 // (rk_scalar_pair_kernel): 5 % faster than one cell per thread in FP64, 15 % in FP32.
 template <typename S> struct StageCfg { static constexpr int MINB1 = 4, PD = 1, MINB2 = 3; };
 template <> struct StageCfg<float> { static constexpr int MINB1 = 6, PD = 2, MINB2 = 4; };
+// The saturation adjustment has no shared memory of its own, so left to itself it runs with the
+// smallest shared-memory split of each SM's L1, and a kernel that needs shared memory (the pressure
+// solve's, beside it in aturan_step) cannot start on that SM until all its blocks have left.
+// Preferring the largest split lets the solve's blocks take each slot the adjustment frees.
+template <typename K>
+inline void prefer_max_shared(K* kernel){
+    if(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+        cudaGetLastError();                       // a hint: carry on without it
+}
+// Saturation adjustment: threads per block (one row segment of NT cells along k).
+template <typename S> struct SatCfg { static constexpr int NT = 128; };
+// Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
+template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
+template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
 }  // namespace aturan
 
 #define ATURAN_DEFINE_LAUNCHERS(S, C)                                                                     \
@@ -32,12 +47,16 @@ void launch_hydro(Grid g, const S* t, const S* ps, const S* v, const S* w, const
                   const double* rm_i, const double* cor_j, const double* pbaro, const double* pb0,         \
                   double* pbf, double* ph, HydroConst h, int advance, cudaStream_t st){                    \
     const int n = g.jm * g.km;                                                                            \
-    hydro_kernel<S><<<(n + 255) / 256, 256, 0, st>>>(g, t, ps, v, w, ref, rm_i, cor_j, pbaro, pb0, pbf,    \
-                                                    ph, h, advance);                                      \
+    constexpr int R = HydCfg<S>::ROWS;                                                                    \
+    hydro_kernel<S, R, HydCfg<S>::MINB><<<(n + 31) / 32, dim3(32, R), 0, st>>>(g, t, ps, v, w, ref, rm_i,   \
+                                                                  cor_j, pbaro, pb0, pbf, ph, h, advance); \
 }                                                                                                         \
 void launch_satadj(const SatArgs<S>& a, cudaStream_t st){                                                  \
-    dim3 grid((a.g.km + 127) / 128, a.g.jm, a.g.im);                                                      \
-    satadj_kernel<S><<<grid, 128, 0, st>>>(a);                                                            \
+    constexpr int NT = SatCfg<S>::NT;                                                                     \
+    static const bool carve = (prefer_max_shared(satadj_kernel<S, NT>), true);                            \
+    (void)carve;                                                                                          \
+    dim3 grid((a.g.km + NT - 1) / NT, a.g.jm, a.g.im);                                                    \
+    satadj_kernel<S, NT><<<grid, NT, 0, st>>>(a);                                                         \
 }                                                                                                         \
 void launch_gs_pre(Grid g, S* au, S* av, S* aw, const S* ru, const S* rv, const S* rw, const double* P,    \
                    const GSW* w, PressConst c, double* incr, cudaStream_t st){                             \

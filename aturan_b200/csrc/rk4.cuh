@@ -659,63 +659,121 @@ __global__ void __launch_bounds__(256) buoy_serial_kernel(Grid g, const S* t, co
 // ---- RungeKutta_Uran_Turb.cpp:62-177: per column (j, k) -- every column, the seam copy and the
 // pole rows included -- the trapezoid integral from the base of the buoyancy anomaly and the
 // metric + radial Coriolis force, plus p_baro minus what p_bfollow has taken up of B(t) - B0.
-// One thread per column, marching up i with coalesced rows along k; the inputs and outputs do not
-// alias (restrict), so the loads of later levels run ahead of the stores of earlier ones. ----
-template <typename S>
-__global__ void __launch_bounds__(256) hydro_kernel(Grid g, const S* __restrict__ t, const S* __restrict__ ps,
+//
+// A block owns 32 consecutive columns and walks up i in chunks of HYD_CH levels, in three
+// phases per chunk: (1) all 256 threads form the per-cell integrands (the divisions, the loads of
+// t, p_stat, v, w) for the chunk's cells into shared memory; (2) one warp, one lane per column,
+// runs the two running sums up the chunk in the reference's order (only the dependent adds are
+// serial) and leaves the prefix at each level in place; (3) all threads read p_baro, p_b0,
+// p_bfollow and write p_bfollow and p_hydro for the chunk. The arithmetic per cell and the
+// summation order are the reference's, so the FP64 form stays bit-equal to it. ----
+constexpr int HYD_CH = 48;          // levels per chunk (41 levels: one chunk)
+
+// ROWS threads per column in phases 1 and 3 (HYD_CH / ROWS levels each); MINB resident blocks.
+template <typename S, int ROWS, int MINB>
+__global__ void __launch_bounds__(32 * ROWS, MINB) hydro_kernel(Grid g, const S* __restrict__ t, const S* __restrict__ ps,
                                                     const S* __restrict__ v, const S* __restrict__ w,
                                                     const double* __restrict__ ref, const double* __restrict__ rm_i,
                                                     const double* __restrict__ cor_j, const double* __restrict__ pbaro,
                                                     const double* __restrict__ pb0, double* __restrict__ pbf,
                                                     double* __restrict__ ph, HydroConst h, int advance){
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if(c >= g.jm * g.km) return;
-    const int j = c / g.km, k = c - j * g.km;
+    constexpr int HYD_PER = HYD_CH / ROWS;
+    static_assert(HYD_CH % ROWS == 0, "a chunk splits evenly over the rows");
+    __shared__ double sm[HYD_CH][32], sb[HYD_CH][32];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int c = blockIdx.x * 32 + tx;
+    const bool col = c < g.jm * g.km;
+    const int j = col ? c / g.km : 0, k = col ? c - j * g.km : 0;
     const double cor_ = cor_j[j];
-    auto buoy = [&](int i) -> double {
-        const size_t o = gidx(g, i, j, k);
-        const double T = (double)__ldg(t + o);
+    auto buoy = [&](int i, double T, double p) -> double {
         if(!(T > 0.0)) return 0.0;
-        const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref) - ref[i];
+        const double b = h.g * p / (h.rR * T * h.t_ref) - ref[i];
         const double f = h.m_nd_rel_b * b / ref[i];
         return isfinite(f) ? f : 0.0;
     };
-    auto met0 = [&](int i) -> double {
-        const size_t o = gidx(g, i, j, k);
-        const double vv = (double)__ldg(v + o), ww = (double)__ldg(w + o);
-        return (vv * vv + ww * ww) / rm_i[i] + cor_ * ww;
-    };
-    if(h.follow_on){
-        double Pm = 0.0, Pb = 0.0;
-        double m_prev = met0(0), b_prev = buoy(0);
-#pragma unroll 4
-        for(int i = 0; i < g.im; i++){
-            if(i > 0){
-                const double m_i = met0(i), b_i = buoy(i);
-                Pm += 0.5 * (m_prev + m_i) * h.dr;
-                Pb += 0.5 * (b_prev + b_i) * h.dr;
-                m_prev = m_i; b_prev = b_i;
+    // running state of the serial lane (phase 2), carried across chunks
+    double Pm = 0.0, Pb = 0.0, m_prev = 0.0, b_prev = 0.0;
+    for(int i0 = 0; i0 < g.im; i0 += HYD_CH){
+        const int n = min(HYD_CH, g.im - i0);
+        // phase 1: integrands; every load of the thread's levels first
+        if(col){
+            S tv[HYD_PER], pv[HYD_PER], vv[HYD_PER], wv[HYD_PER];
+#pragma unroll
+            for(int q = 0; q < HYD_PER; q++){
+                const int r = ty + q * ROWS;
+                if(r < n){
+                    const size_t o = gidx(g, i0 + r, j, k);
+                    tv[q] = __ldg(t + o); pv[q] = __ldg(ps + o); vv[q] = __ldg(v + o); wv[q] = __ldg(w + o);
+                }
             }
-            const size_t o = gidx(g, i, j, k);
-            double bf = pbf[o];
-            if(advance){ bf += (Pb - pb0[o] - bf) / h.follow_tau; pbf[o] = bf; }
-            ph[o] = Pm + Pb + pbaro[o] - bf;
+#pragma unroll
+            for(int q = 0; q < HYD_PER; q++){
+                const int r = ty + q * ROWS;
+                if(r < n){
+                    const int i = i0 + r;
+                    const double V = (double)vv[q], W = (double)wv[q];
+                    if(h.follow_on){
+                        sm[r][tx] = (V * V + W * W) / rm_i[i] + cor_ * W;
+                        sb[r][tx] = buoy(i, (double)tv[q], (double)pv[q]);
+                    } else {
+                        // ATURAN_PBARO_FOLLOW=0: f_(i) = buoy(i) + (v^2 + w^2) / rm + cor_ w, :134-161
+                        sm[r][tx] = buoy(i, (double)tv[q], (double)pv[q]) + (V * V + W * W) / rm_i[i] + cor_ * W;
+                    }
+                }
+            }
         }
-    } else {
-        // ATURAN_PBARO_FOLLOW=0: f_(i) = buoy(i) + (v^2 + w^2) / rm + cor_ w, :134-161
-        auto f_ = [&](int i) -> double {
-            const size_t o = gidx(g, i, j, k);
-            const double vv = (double)__ldg(v + o), ww = (double)__ldg(w + o);
-            return buoy(i) + (vv * vv + ww * ww) / rm_i[i] + cor_ * ww;
-        };
-        double prev = 0.0, fp = f_(0);
-        ph[gidx(g, 0, j, k)] = 0.0 + pbaro[gidx(g, 0, j, k)];
-        for(int i = 1; i < g.im; i++){
-            const double fi = f_(i);
-            prev = prev + 0.5 * (fp + fi) * h.dr;
-            fp = fi;
-            ph[gidx(g, i, j, k)] = prev + pbaro[gidx(g, i, j, k)];
+        __syncthreads();
+        // phase 2: the running sums, in order, replaced in place by the prefix at each level
+        if(ty == 0 && col){
+            if(h.follow_on){
+                for(int r = 0; r < n; r++){
+                    const double m_i = sm[r][tx], b_i = sb[r][tx];
+                    if(i0 + r > 0){
+                        Pm += 0.5 * (m_prev + m_i) * h.dr;
+                        Pb += 0.5 * (b_prev + b_i) * h.dr;
+                    }
+                    m_prev = m_i; b_prev = b_i;
+                    sm[r][tx] = Pm; sb[r][tx] = Pb;
+                }
+            } else {
+                for(int r = 0; r < n; r++){
+                    const double f_i = sm[r][tx];
+                    if(i0 + r > 0) Pm = Pm + 0.5 * (m_prev + f_i) * h.dr;
+                    m_prev = f_i;
+                    sm[r][tx] = Pm;
+                }
+            }
         }
+        __syncthreads();
+        // phase 3: p_bfollow and p_hydro, loads first
+        if(col){
+            double bfv[HYD_PER], b0v[HYD_PER], pbv[HYD_PER];
+#pragma unroll
+            for(int q = 0; q < HYD_PER; q++){
+                const int r = ty + q * ROWS;
+                if(r < n){
+                    const size_t o = gidx(g, i0 + r, j, k);
+                    pbv[q] = pbaro[o];
+                    if(h.follow_on){ bfv[q] = pbf[o]; if(advance) b0v[q] = pb0[o]; }
+                }
+            }
+#pragma unroll
+            for(int q = 0; q < HYD_PER; q++){
+                const int r = ty + q * ROWS;
+                if(r < n){
+                    const size_t o = gidx(g, i0 + r, j, k);
+                    if(h.follow_on){
+                        const double pm = sm[r][tx], pb = sb[r][tx];
+                        double bf = bfv[q];
+                        if(advance){ bf += (pb - b0v[q] - bf) / h.follow_tau; pbf[o] = bf; }
+                        ph[o] = pm + pb + pbv[q] - bf;
+                    } else {
+                        ph[o] = sm[r][tx] + pbv[q];
+                    }
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -62,10 +62,11 @@ __device__ __forceinline__ double qsat(const GasConst& G, bool ice, double rho_c
     else return rho_c * ep * svp(T, C, L0, G.den, al, be) / p_u;
 }
 
-// 8 resident blocks per SM (64 registers, a few spilled): the kernel is bound by dependent FP64
-// exp/log chains, so more warps in flight beat the spill traffic (measured: 6 % faster than 4).
-template <typename S>
-__global__ void __launch_bounds__(128, 8) satadj_kernel(const SatArgs<S> a){
+// NT threads per block, 1024 / NT resident blocks per SM (64 registers, a few spilled): the kernel
+// is bound by dependent FP64 exp/log chains, so more warps in flight beat the spill traffic
+// (measured: 6 % faster than half as many).
+template <typename S, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> a){
     constexpr bool FAST = sizeof(S) == 4;            // the mixed form
     const Grid& g = a.g;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -276,7 +277,9 @@ __global__ void __launch_bounds__(128, 8) satadj_kernel(const SatArgs<S> a){
         }
         a.t[q] = (S)tt;
     }
-    // per-block counter reduction: integer adds, order-independent
+    // per-block counter reduction: integer adds, order-independent. Without counters (uniform
+    // over the block) each warp leaves as soon as its cells are done.
+    if(!a.counters) return;
     __shared__ unsigned s_adj, s_nc;
     if(threadIdx.x == 0){ s_adj = 0; s_nc = 0; }
     __syncthreads();

@@ -343,3 +343,27 @@ def test_restore_ncopies_is_restorevar():
     for n in F.PROGNOSTIC:
         assert np.array_equal(ctx.download(n + "n"), 0.5 * ctx.download(n)), n
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_step_side_by_side_equals_in_order(synth, precision):
+    """aturan_step runs the saturation adjustment and the n-copy sync on a second stream beside the
+    pressure solve. They touch disjoint fields, so two full-size steps must give the same bits as
+    the four calls in the reference's order (pressure, adjustment, sync, RK4)."""
+    _, st0 = synth
+    p = P.default_params(precision=precision)
+    names = F.PROGNOSTIC + ["p_dyn", "p_hydro"]
+    a, b = ctx_for(p), ctx_for(p)
+    a.upload_state(st0)
+    b.upload_state(st0)
+    for _ in range(2):
+        a.step(P.PRESS_RB_LINE, omega=1.0, max_sweeps=50, tol=1e-6)
+        b.pressure(P.PRESS_RB_LINE, omega=1.0, max_sweeps=50, tol=1e-6)
+        b.satadj(count=False)
+        b.sync_ncopies()
+        b.rk4_step()
+    ga, gb = a.download_state(names), b.download_state(names)
+    a.close()
+    b.close()
+    for n in names:
+        assert np.array_equal(ga[n], gb[n]), n
