@@ -198,6 +198,10 @@ RhsConst<C> make_rhs_const(const aturan_params& p){
         k.cp_rh2 = p.r_h2 / p.r_mix;
     }
     k.cp_h2_const = p.cp_h2;
+    k.inv_re_eff = 1.0 / k.re_eff; k.inv_re_pr = 1.0 / k.re_pr;
+    for(int n = 0; n < 5; n++) k.inv_sc_re[n] = 1.0 / k.sc_re[n];
+    k.inv_mue_mix = 1.0 / k.mue_mix; k.inv_u_0 = 1.0 / k.u_0; k.inv_precip_den = 1.0 / k.precip_den;
+    k.inv_cp_rsum = k.cp_rsum != 0.0 ? 1.0 / k.cp_rsum : 0.0;
     k.tke_max = 1000.0 / (p.u_0 * p.u_0);
     k.dis_min = 1.0e-10;
     k.t_min = p.t_min_K / p.t_ref;

@@ -59,6 +59,8 @@ struct RhsConst {
     T cp_rh2, cp_he_term, cp_ch4_term, cp_rsum, cp_h2_const;   // cp(T), CpH2.h:122-134
     T tke_max, dis_min, t_min, t_max, dt;
     T heat_scale;       // (L_atm * 1e3 / u_0) / t_ref: a heating rate in K/s as a tendency of t
+    // reciprocals of the divisors above, for the mixed form's multiplications (qdiv)
+    T inv_re_eff, inv_re_pr, inv_sc_re[5], inv_mue_mix, inv_u_0, inv_precip_den, inv_cp_rsum;
     int cp_dyn, cp_gas, cp_mode, turb_active;
 };
 

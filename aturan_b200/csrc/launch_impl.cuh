@@ -10,8 +10,12 @@ namespace aturan {
 // SM of the momentum launch (MINB1) and of the scalar launch (MINB2), and the scalar launch's
 // prefetch depth (PD fields ahead). The scalar launch takes two cells per thread
 // (rk_scalar_pair_kernel): 5 % faster than one cell per thread in FP64, 15 % in FP32.
-template <typename S> struct StageCfg { static constexpr int MINB1 = 4, PD = 1, MINB2 = 3; };
-template <> struct StageCfg<float> { static constexpr int MINB1 = 6, PD = 2, MINB2 = 4; };
+// AD > 0: the scalar launch stages its loads through a ring of AD shared-memory slots
+// (rk_scalar_async_kernel) at AMINB resident blocks per SM instead of the register ring. FP64:
+// 9 % faster than the register ring, whose 168 registers held 3 blocks per SM; FP32: 3-25 %
+// slower at every depth and occupancy tried, so the register ring stays.
+template <typename S> struct StageCfg { static constexpr int MINB1 = 4, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
+template <> struct StageCfg<float> { static constexpr int MINB1 = 6, PD = 1, MINB2 = 4, AD = 0, AMINB = 4; };
 // The saturation adjustment has no shared memory of its own, so left to itself it runs with the
 // smallest shared-memory split of each SM's L1, and a kernel that needs shared memory (the pressure
 // solve's, beside it in aturan_step) cannot start on that SM until all its blocks have left.
@@ -24,6 +28,20 @@ inline void prefer_max_shared(K* kernel){
 }
 // Saturation adjustment: threads per block (one row segment of NT cells along k).
 template <typename S> struct SatCfg { static constexpr int NT = 128; };
+template <typename S, typename C>
+void launch_scalars(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
+    if constexpr(StageCfg<S>::AD > 0){
+        constexpr int D = StageCfg<S>::AD;
+        auto kern = rk_scalar_async_kernel<S, C, D, StageCfg<S>::AMINB>;
+        const int sm = D * (int)sizeof(AsyncSlot<S>);
+        static const bool attr = (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) == cudaSuccess)
+                                 || (cudaGetLastError(), false);
+        (void)attr;
+        kern<<<grid2, dim3(32, 4), sm, st>>>(a);
+    } else {
+        rk_scalar_pair_kernel<S, C, StageCfg<S>::PD, StageCfg<S>::MINB2><<<grid2, dim3(32, 4), 0, st>>>(a);
+    }
+}
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
 template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
@@ -35,7 +53,7 @@ void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                   
     dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);                                        \
     rk_stage_kernel<S, C, 1, 0, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);                    \
     const dim3 grid2((g.km - 1 + 63) / 64, (g.jm - 2 + 3) / 4, g.im - 2);                                 \
-    rk_scalar_pair_kernel<S, C, StageCfg<S>::PD, StageCfg<S>::MINB2><<<grid2, dim3(32, 4), 0, st>>>(a);   \
+    launch_scalars(a, grid2, st);                                                                         \
 }                                                                                                         \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
                  double* part_w, int nblk, double* ref, int exact, cudaStream_t st){                       \

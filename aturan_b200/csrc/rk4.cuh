@@ -47,6 +47,13 @@ __device__ __forceinline__ S ld(const S* p){ return __ldg(p); }
 
 template <typename C>
 __device__ __forceinline__ C cmax(C a, C b){ return (a < b) ? b : a; }   // std::max
+// x / d: the reference's division in the FP64 form; in the mixed form x times the reciprocal of
+// the constant d formed once on the host (one rounding more, inside the form's tolerance, where an
+// FP32 division costs about ten instructions).
+template <typename C>
+__device__ __forceinline__ C qdiv(C x, C d, C inv_d){
+    if constexpr(sizeof(C) == 4) return x * inv_d; else return x / d;
+}
 template <typename C>
 __device__ __forceinline__ C cclamp(C v, C lo, C hi){ return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -63,7 +70,7 @@ __device__ __forceinline__ C cp_lapse(const RhsConst<C>& k, const C* tab, C T){
         const C a = __ldg(tab + i), b = __ldg(tab + i + 1);
         ch = a + f * (b - a);
     }
-    if(k.cp_gas) return (k.cp_rh2 * ch + k.cp_he_term + k.cp_ch4_term) / k.cp_rsum;
+    if(k.cp_gas) return qdiv(k.cp_rh2 * ch + k.cp_he_term + k.cp_ch4_term, k.cp_rsum, k.inv_cp_rsum);
     return k.cp_mix + k.cp_rh2 * (ch - k.cp_h2_const);   // cp_rh2 holds r_h2 / r_mix here
 }
 
@@ -138,7 +145,7 @@ __device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, si
         else if(kind == 3) y = cmax(y, a.k.dis_min);
         a.Y[off] = (S)y;
     } else {
-        C y = yn + a.k.dt * accv / C(6.0);
+        C y = yn + qdiv(a.k.dt * accv, C(6.0), C(1.0 / 6.0));
         if(kind == 1) y = cclamp(y, a.k.t_min, a.k.t_max);
         else if(kind == 2) y = cclamp(cmax(y, C(0.0)), C(0.0), a.k.tke_max);
         else if(kind == 3) y = cmax(y, a.k.dis_min);
@@ -190,7 +197,7 @@ __device__ __forceinline__ C scalar_rhs(const RhsConst<C>& K, const ScalarIn<C>&
         const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
         const C diffusion = Q.d2r + Q.d1r * geo.two_inv_rm + Q.d2t * geo.inv_rm2
             + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
-        C r = - transport + diffusion / K.sc_re[n / 3] + diffusion * nue_t_s;
+        C r = - transport + qdiv(diffusion, K.sc_re[n / 3], K.inv_sc_re[n / 3]) + diffusion * nue_t_s;
         if(q == ATURAN_H2S || q == ATURAN_NH3) r = r + K.chemical_reaction * in.f2;
         r = r + K.precip_coupling * in.f1;
         return r;
@@ -199,18 +206,18 @@ __device__ __forceinline__ C scalar_rhs(const RhsConst<C>& K, const ScalarIn<C>&
         const C transport = u_ijk * Q.d1r + v_invrm * Q.d1t + w_invrs * Q.d1p;
         const C diffusion = Q.d2r + Q.d1r * geo.two_inv_rm + Q.d2t * geo.inv_rm2
             + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
-        const C v_stokes = K.stokes_a * (K.rho_cond_nh4sh - in.f3) * K.g / K.mue_mix;
+        const C v_stokes = qdiv(K.stokes_a * (K.rho_cond_nh4sh - in.f3) * K.g, K.mue_mix, K.inv_mue_mix);
         return - transport + in.f1
-               + diffusion / K.sc_re[4] + diffusion * nue_t_s
+               + qdiv(diffusion, K.sc_re[4], K.inv_sc_re[4]) + diffusion * nue_t_s
                + K.chemical_reaction * in.f2
-               + (v_stokes / K.u_0) * Q.d1r;
+               + qdiv(v_stokes, K.u_0, K.inv_u_0) * Q.d1r;
     } else {
         // ---- k* and dis* (:989-1018) ----
         const C transport = u_ijk * Q.d1r + v_ijk * Q.d1t * geo.inv_rm + w_ijk * Q.d1p * geo.inv_rmsinthe;
         const C diffusion = Q.d2r + Q.d1r * C(2.0) * geo.inv_rm + Q.d2t * geo.inv_rm2
             + Q.d1t * geo.costhe_inv_rm2sinthe + Q.d2p * geo.inv_rm2sinthe2;
         const C sig = n == 13 ? C(0.85) : C(0.5);
-        return - transport + diffusion * (K.inv_re + nue_c / sig) + in.f1;
+        return - transport + diffusion * (K.inv_re + qdiv(nue_c, sig, n == 13 ? C(1.0 / 0.85) : C(2.0))) + in.f1;
     }
 }
 __host__ __device__ constexpr int scalar_kind(int n){ return n < 13 ? 0 : (n == 13 ? 2 : 3); }
@@ -303,14 +310,14 @@ __device__ __forceinline__ void momentum_rhs(const StageArgs<S, C>& a, const Mom
         const C dphdthe_term = (C)((in.ph_jp - in.ph_jm) * (double)K.inv_2dthe) * inv_rm;
         const C dphdphi_term = (C)((in.ph_ke - in.ph_kw) * (double)K.inv_2dphi) * inv_rmsinthe;
         const C re_eff = K.re_eff;
-        rhs_u = - dpdr_term + C(0.0) - transport_u + diffusion_u / re_eff + diffusion_u * nue_t
+        rhs_u = - dpdr_term + C(0.0) - transport_u + qdiv(diffusion_u, re_eff, K.inv_re_eff) + diffusion_u * nue_t
                 - K.cor_rad_f * Coriolis_rad
                 + K.cen_f * geo.cent_rad
                 - geo.sponge * u_ijk;
-        rhs_v = - dpdthe_term - dphdthe_term - transport_v + diffusion_v / re_eff + diffusion_v * nue_t
+        rhs_v = - dpdthe_term - dphdthe_term - transport_v + qdiv(diffusion_v, re_eff, K.inv_re_eff) + diffusion_v * nue_t
                 - K.cor_sc * Coriolis_the
                 + K.cen_f * geo.cent_the;
-        rhs_w = - dpdphi_term - dphdphi_term - transport_w + diffusion_w / re_eff + diffusion_w * nue_t
+        rhs_w = - dpdphi_term - dphdphi_term - transport_w + qdiv(diffusion_w, re_eff, K.inv_re_eff) + diffusion_w * nue_t
                 - K.cor_sc * Coriolis_phi;
     }
     // ---- temperature ----
@@ -324,12 +331,12 @@ __device__ __forceinline__ void momentum_rhs(const StageArgs<S, C>& a, const Mom
         const C tmf = (K.tmf != C(0.0)) ? K.tmf * in.f_tmf : C(0.0);
         C precip_t = C(0.0);
         if(K.precip_coupling != C(0.0)){
-            precip_t = K.precip_coupling * in.f_qp * K.precip_L / K.precip_den;
+            precip_t = qdiv(K.precip_coupling * in.f_qp * K.precip_L, K.precip_den, K.inv_precip_den);
             if(!isfinite(precip_t)) precip_t = C(0.0);
             else if(precip_t >  C(0.5)) precip_t =  C(0.5);
             else if(precip_t < -C(0.5)) precip_t = -C(0.5);
         }
-        rhs_t = + pressure_t - transport_t + diffusion_t / K.re_pr + diffusion_t * nue_t_s
+        rhs_t = + pressure_t - transport_t + qdiv(diffusion_t, K.re_pr, K.inv_re_pr) + diffusion_t * nue_t_s
                 - tmf + C(0.0) + precip_t;
         if(a.heat) rhs_t = rhs_t + K.heat_scale * (C)a.heat[(size_t)j * a.g.km + k];   // not in the reference
     }
@@ -413,7 +420,7 @@ __device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, int q, s
         if(kind == 2){ y0 = cclamp(y0, C(0.0), a.k.tke_max); y1 = cclamp(y1, C(0.0), a.k.tke_max); }
         else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
     } else {
-        y0 = n0.nc + a.k.dt * acc0 / C(6.0); y1 = n1.nc + a.k.dt * acc1 / C(6.0);
+        y0 = n0.nc + qdiv(a.k.dt * acc0, C(6.0), C(1.0 / 6.0)); y1 = n1.nc + qdiv(a.k.dt * acc1, C(6.0), C(1.0 / 6.0));
         if(kind == 1){ y0 = cclamp(y0, a.k.t_min, a.k.t_max); y1 = cclamp(y1, a.k.t_min, a.k.t_max); }
         else if(kind == 2){ y0 = cclamp(cmax(y0, C(0.0)), C(0.0), a.k.tke_max); y1 = cclamp(cmax(y1, C(0.0)), C(0.0), a.k.tke_max); }
         else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
@@ -452,7 +459,7 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_pair_kernel(const StageAr
     ld2<S, C>(a.X + (size_t)ATURAN_W * fs + o, w0, w1);
     auto nts = [&](C nue_c) -> C {
         const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
-        return nue_t / C(0.9);
+        return qdiv(nue_t, C(0.9), C(1.0 / 0.9));
     };
     const C nts0 = nts(nue0), nts1 = nts(nue1);
     const C vr0 = v0 * geo.inv_rm, vr1 = v1 * geo.inv_rm;
@@ -471,6 +478,142 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_pair_kernel(const StageAr
             stage_update2(a, scalar_field(n), o, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
         }
     }
+}
+
+// ---- the scalar part with its loads staged through shared memory by cp.async ----
+// The same cells, arithmetic and order as rk_scalar_pair_kernel; only the way the inputs arrive
+// differs. Each thread copies the inputs of its own pair for the next D fields into a ring of D
+// shared-memory slots with asynchronous copies (cp.async, L1-allocating, so the neighbours other
+// threads fetch are L1 hits), and waits for the oldest group only when it computes that field.
+// The loads in flight no longer hold registers, so the ring can be deeper than the register ring
+// of the plain kernel at more resident warps. A thread reads back only what it copied itself, and
+// refills a slot only after the stores that consumed it, so no barrier is needed.
+template <typename S>
+struct AsyncSlot {                       // one field's inputs for the 128 threads of a block
+    typename Pair<S>::T c[128], rp[128], rm[128], tp[128], tm[128], acc[128], nc[128], f1[128], f2[128], f3[128];
+    S pw[128], pe[128];
+};
+
+template <int N>
+__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem){
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" :: "r"(sa), "l"(gmem), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit(){ asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait(){ asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
+
+template <typename S, typename C>
+__device__ __forceinline__ void issue_scalar2(AsyncSlot<S>& sl, int t, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
+    constexpr int V = (int)sizeof(typename Pair<S>::T);
+    const int q = scalar_field(n);
+    const size_t f = (size_t)q * nb.fs, o = nb.o;
+    cp_async_n<V>(&sl.c[t], nb.X + f + o);
+    cp_async_n<V>(&sl.rp[t], nb.xip + f + nb.oip);
+    cp_async_n<V>(&sl.rm[t], nb.xim + f + nb.oim);
+    cp_async_n<V>(&sl.tp[t], nb.xjp + f + nb.ojp);
+    cp_async_n<V>(&sl.tm[t], nb.xjm + f + nb.ojm);
+    cp_async_n<(int)sizeof(S)>(&sl.pw[t], nb.X + f + nb.okw);
+    cp_async_n<(int)sizeof(S)>(&sl.pe[t], nb.X + f + nb.oke);
+    if(a.stage != 0) cp_async_n<V>(&sl.acc[t], a.acc + f + o);
+    cp_async_n<V>(&sl.nc[t], a.Nc + f + o);
+    const S* F = a.forc + o;
+    const size_t fs = nb.fs;
+    if(n < 12){
+        cp_async_n<V>(&sl.f1[t], F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs);
+        if(q == ATURAN_H2S) cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs);
+        if(q == ATURAN_NH3) cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs);
+    } else if(n == 12){
+        cp_async_n<V>(&sl.f1[t], F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f3[t], F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs);
+    } else {
+        cp_async_n<V>(&sl.f1[t], F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs);
+    }
+}
+
+// The slot read back into the register form load_scalar2 produces.
+template <typename S, typename C>
+__device__ __forceinline__ void take_scalar2(ScalarIn2<C>& in, const AsyncSlot<S>& sl, int t, const StageArgs<S, C>& a, int n){
+    const int q = scalar_field(n);
+    ScalarIn<C>& A = in.c0;
+    ScalarIn<C>& B = in.c1;
+    auto get = [&](const typename Pair<S>::T& v, C& x, C& y){ x = (C)v.x; y = (C)v.y; };
+    get(sl.c[t], A.v.c, B.v.c);
+    get(sl.rp[t], A.v.rp, B.v.rp);
+    get(sl.rm[t], A.v.rm, B.v.rm);
+    get(sl.tp[t], A.v.tp, B.v.tp);
+    get(sl.tm[t], A.v.tm, B.v.tm);
+    A.v.pw = (C)sl.pw[t];
+    B.v.pe = (C)sl.pe[t];
+    A.v.pe = B.v.c;
+    B.v.pw = A.v.c;
+    if(a.stage == 0){ A.an.acc = C(0.0); B.an.acc = C(0.0); }
+    else get(sl.acc[t], A.an.acc, B.an.acc);
+    get(sl.nc[t], A.an.nc, B.an.nc);
+    A.f2 = B.f2 = C(0.0); A.f3 = B.f3 = C(0.0);
+    get(sl.f1[t], A.f1, B.f1);
+    if(n == 12 || q == ATURAN_H2S || q == ATURAN_NH3) get(sl.f2[t], A.f2, B.f2);
+    if(n == 12) get(sl.f3[t], A.f3, B.f3);
+}
+
+template <typename S, typename C, int D, int MINB>
+__global__ void __launch_bounds__(128, MINB) rk_scalar_async_kernel(const StageArgs<S, C> a){
+    extern __shared__ __align__(16) unsigned char ring_raw[];
+    AsyncSlot<S>* ring = reinterpret_cast<AsyncSlot<S>*>(ring_raw);
+    const Grid& g = a.g;
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    const int k = 2 * (blockIdx.x * 32 + threadIdx.x);
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<C>& K = a.k;
+    Nbr<S> nb;
+    nb.fs  = g.fstride;
+    nb.o   = gidx(g, i, j, k);
+    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
+    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
+    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
+    nb.oke = nb.o - k + phi_wrap(k + 2, g.km);
+    nb.X   = a.X;
+    nb.xim = (i == 1) ? a.St : a.X;
+    nb.xip = (i == g.im - 2) ? a.St : a.X;
+    nb.xjm = (j == 1) ? a.St : a.X;
+    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
+    const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
+#pragma unroll
+    for(int n = 0; n < D; n++){
+        if(n < nfield) issue_scalar2(ring[n], t, a, nb, n);
+        cp_async_commit();
+    }
+    const size_t o = nb.o, fs = g.fstride;
+    const GeoIJ<C> geo = a.geo[i * g.jm + j];
+    C nue0, nue1, u0, u1, v0, v1, w0, w1;
+    ld2<S, C>(a.forc + (size_t)(ATURAN_NUE - ATURAN_NUE) * fs + o, nue0, nue1);
+    ld2<S, C>(a.X + (size_t)ATURAN_U * fs + o, u0, u1);
+    ld2<S, C>(a.X + (size_t)ATURAN_V * fs + o, v0, v1);
+    ld2<S, C>(a.X + (size_t)ATURAN_W * fs + o, w0, w1);
+    auto nts = [&](C nue_c) -> C {
+        const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
+        return qdiv(nue_t, C(0.9), C(1.0 / 0.9));
+    };
+    const C nts0 = nts(nue0), nts1 = nts(nue1);
+    const C vr0 = v0 * geo.inv_rm, vr1 = v1 * geo.inv_rm;
+    const C wr0 = w0 * geo.inv_rmsinthe, wr1 = w1 * geo.inv_rmsinthe;
+#pragma unroll
+    for(int n = 0; n < N_SCALARS; n++){
+        cp_async_wait<D - 1>();                      // field n's group has landed
+        if(n < nfield){
+            ScalarIn2<C> in;
+            take_scalar2(in, ring[n % D], t, a, n);
+            const C r0 = scalar_rhs(K, in.c0, n, geo, u0, v0, w0, vr0, wr0, nue0, nts0);
+            const C r1 = scalar_rhs(K, in.c1, n, geo, u1, v1, w1, vr1, wr1, nue1, nts1);
+            stage_update2(a, scalar_field(n), o, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
+        }
+        if(n + D < nfield) issue_scalar2(ring[n % D], t, a, nb, n + D);   // after the stores that used the slot
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
 }
 
 // Fused RHS evaluation and stage update of one cell. PART selects the equations: 1 momentum and
@@ -518,7 +661,7 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
 
     const C nue_c = FORC(ATURAN_NUE);
     const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
-    const C nue_t_s = nue_t / C(0.9);
+    const C nue_t_s = qdiv(nue_t, C(0.9), C(1.0 / 0.9));
 
     if constexpr(PART == 1){
     // ---- every load of the cell first ----
