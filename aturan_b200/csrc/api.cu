@@ -685,6 +685,11 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     for(int n = 0; n < 6; n++) add(nij * 8);                           // line factorisations (Lc, Lc^T)
     add(fs * 4); add(fs * 4);
     ctx->mem_bytes = bytes;
+    // the stage kernels address every buffer of the allocation by 32-bit element offsets
+    if(bytes / e >= (size_t)INT32_MAX){
+        std::fprintf(stderr, "aturan_ctx_create: grid too large (%zu elements of context memory, limit 2^31)\n", bytes / e);
+        delete ctx; return ATURAN_E_UNSUPPORTED;
+    }
     int prio_lo = 0, prio_hi = 0;                         // least and most urgent
     if(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess){ cudaGetLastError(); prio_lo = prio_hi = 0; }
     if(cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess){

@@ -12,10 +12,11 @@ namespace aturan {
 // (rk_scalar_pair_kernel): 5 % faster than one cell per thread in FP64, 15 % in FP32.
 // AD > 0: the scalar launch stages its loads through a ring of AD shared-memory slots
 // (rk_scalar_async_kernel) at AMINB resident blocks per SM instead of the register ring. FP64:
-// 9 % faster than the register ring, whose 168 registers held 3 blocks per SM; FP32: 3-25 %
-// slower at every depth and occupancy tried, so the register ring stays.
-template <typename S> struct StageCfg { static constexpr int MINB1 = 4, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
-template <> struct StageCfg<float> { static constexpr int MINB1 = 6, PD = 1, MINB2 = 4, AD = 0, AMINB = 4; };
+// 6-9 % faster than the register ring at 3 or 4 blocks per SM; FP32: 3-25 % slower at every
+// depth and occupancy tried, so the register ring stays, one field ahead at 6 blocks per SM
+// (80 registers; 9 % faster than 4 blocks with two fields ahead).
+template <typename S> struct StageCfg { static constexpr int MINB1 = 5, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
+template <> struct StageCfg<float> { static constexpr int MINB1 = 7, PD = 1, MINB2 = 6, AD = 0, AMINB = 4; };
 // The saturation adjustment has no shared memory of its own, so left to itself it runs with the
 // smallest shared-memory split of each SM's L1, and a kernel that needs shared memory (the pressure
 // solve's, beside it in aturan_step) cannot start on that SM until all its blocks have left.
@@ -51,7 +52,7 @@ template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
 void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                                             \
     const Grid& g = a.g;                                                                                  \
     dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);                                        \
-    rk_stage_kernel<S, C, 1, 0, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);                    \
+    rk_stage_kernel<S, C, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);                          \
     const dim3 grid2((g.km - 1 + 63) / 64, (g.jm - 2 + 3) / 4, g.im - 2);                                 \
     launch_scalars(a, grid2, st);                                                                         \
 }                                                                                                         \

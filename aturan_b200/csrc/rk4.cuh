@@ -100,6 +100,42 @@ __device__ __forceinline__ R7<C> load7(const Nbr<S>& n, int q){
     return r;
 }
 
+// The forward stage's addressing of one cell: offsets in elements from the stage input X -- of the
+// cell and its six stencil neighbours (a neighbour on a boundary row lies in the state St, reached
+// through the same base), of a field (fs), and of the accumulator, n-copy, forcing and stage-output
+// buffers (d*). Every buffer the stage touches is carved from the context's one allocation, which
+// the host keeps below 2^31 elements, so 32-bit offsets reach all of it: an address is one 32-bit
+// add and one wide multiply-add, and a thread holds 12 registers of addressing instead of seven
+// 64-bit offsets and five pointers (10 % faster stage in FP32: more resident blocks).
+struct Cell { int o, oim, oip, ojm, ojp, okw, oke, fs, dacc, dnc, dforc, dY; };
+
+// keast: the offset in k of the east neighbour (1 for one cell, 2 for a pair's second cell).
+template <typename S, typename C>
+__device__ __forceinline__ Cell make_cell(const StageArgs<S, C>& a, int i, int j, int k, int keast){
+    const Grid& g = a.g;
+    const int dSt = (int)(a.St - a.X);
+    const int JK = g.jm * g.kp;
+    Cell c;
+    c.fs  = (int)g.fstride;
+    c.o   = (int)gidx(g, i, j, k);
+    c.oim = c.o - JK + (i == 1 ? dSt : 0);       c.oip = c.o + JK + (i == g.im - 2 ? dSt : 0);
+    c.ojm = c.o - g.kp + (j == 1 ? dSt : 0);     c.ojp = c.o + g.kp + (j == g.jm - 2 ? dSt : 0);
+    c.okw = c.o - k + phi_wrap(k - 1, g.km);     c.oke = c.o - k + phi_wrap(k + keast, g.km);
+    c.dacc = (int)(a.acc - a.X); c.dnc = (int)(a.Nc - a.X); c.dforc = (int)(a.forc - a.X); c.dY = (int)(a.Y - a.X);
+    return c;
+}
+
+template <typename S, typename C>
+__device__ __forceinline__ R7<C> load7c(const S* X, const Cell& c, int q){
+    const int f = q * c.fs;
+    R7<C> r;
+    r.c  = (C)ld(X + (f + c.o));
+    r.rp = (C)ld(X + (f + c.oip)); r.rm = (C)ld(X + (f + c.oim));
+    r.tp = (C)ld(X + (f + c.ojp)); r.tm = (C)ld(X + (f + c.ojm));
+    r.pe = (C)ld(X + (f + c.oke)); r.pw = (C)ld(X + (f + c.okw));
+    return r;
+}
+
 // RHS_Uran_Turb.cpp:93-176: central first and second differences of one field.
 template <typename C>
 __device__ __forceinline__ D6<C> diff6(const RhsConst<C>& k, const R7<C>& v){
@@ -120,36 +156,36 @@ template <typename C>
 struct AccNc { C acc, nc; };
 
 template <typename S, typename C>
-__device__ __forceinline__ AccNc<C> load_acc_nc(const StageArgs<S, C>& a, int q, size_t o){
-    const size_t off = (size_t)q * a.g.fstride + o;
+__device__ __forceinline__ AccNc<C> load_acc_nc(const StageArgs<S, C>& a, const S* X, const Cell& c, int q){
+    const int off = q * c.fs + c.o;
     AccNc<C> v;
-    v.acc = (a.stage == 0) ? C(0.0) : (C)a.acc[off];
-    v.nc = (C)ld(a.Nc + off);
+    v.acc = (a.stage == 0) ? C(0.0) : (C)X[c.dacc + off];
+    v.nc = (C)ld(X + (c.dnc + off));
     return v;
 }
 
 // acc and next-stage / final update of one prognostic field (RungeKutta_Uran_Turb.cpp:291-403).
 // kind: 0 plain, 1 temperature (final clamp), 2 k* (clamp), 3 dis* (floor).
 template <typename S, typename C>
-__device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, int q, size_t o, C r, int kind,
+__device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, S* W, const Cell& c, int q, C r, int kind,
                                              const AccNc<C>& an){
-    const size_t off = (size_t)q * a.g.fstride + o;
+    const int off = q * c.fs + c.o;
     C accv;
     if(a.stage == 0) accv = a.wgt * r;
     else accv = an.acc + a.wgt * r;
     const C yn = an.nc;
     if(a.stage < 3){
-        a.acc[off] = (S)accv;
+        W[c.dacc + off] = (S)accv;
         C y = yn + a.c_in * r;
         if(kind == 2) y = cclamp(y, C(0.0), a.k.tke_max);
         else if(kind == 3) y = cmax(y, a.k.dis_min);
-        a.Y[off] = (S)y;
+        W[c.dY + off] = (S)y;
     } else {
         C y = yn + qdiv(a.k.dt * accv, C(6.0), C(1.0 / 6.0));
         if(kind == 1) y = cclamp(y, a.k.t_min, a.k.t_max);
         else if(kind == 2) y = cclamp(cmax(y, C(0.0)), C(0.0), a.k.tke_max);
         else if(kind == 3) y = cmax(y, a.k.dis_min);
-        a.Y[off] = (S)y;
+        W[c.dY + off] = (S)y;
     }
 }
 
@@ -165,26 +201,6 @@ __host__ __device__ constexpr int scalar_field(int n){
     return n < 12 ? ATURAN_CH4 + n : (n == 12 ? ATURAN_NH4SH : (n == 13 ? ATURAN_TKE : ATURAN_DIS));
 }
 
-template <typename S, typename C>
-__device__ __forceinline__ void load_scalar(ScalarIn<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
-    const int q = scalar_field(n);
-    const S* F = a.forc + nb.o;
-    const size_t fs = nb.fs;
-    in.v = load7<S, C>(nb, q);
-    in.an = load_acc_nc(a, q, nb.o);
-    in.f2 = C(0.0); in.f3 = C(0.0);
-    if(n < 12){
-        in.f1 = (C)ld(F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs);
-        if(q == ATURAN_H2S) in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs);
-        if(q == ATURAN_NH3) in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs);
-    } else if(n == 12){
-        in.f1 = (C)ld(F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs);
-        in.f2 = (C)ld(F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs);
-        in.f3 = (C)ld(F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs);
-    } else {
-        in.f1 = (C)ld(F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs);
-    }
-}
 
 // Tendency of scalar field n from its loaded inputs (:790-913, :989-1018).
 template <typename C>
@@ -222,13 +238,6 @@ __device__ __forceinline__ C scalar_rhs(const RhsConst<C>& K, const ScalarIn<C>&
 }
 __host__ __device__ constexpr int scalar_kind(int n){ return n < 13 ? 0 : (n == 13 ? 2 : 3); }
 
-template <typename S, typename C>
-__device__ __forceinline__ void scalar_update(const StageArgs<S, C>& a, const ScalarIn<C>& in, int n, size_t o,
-                                              const GeoIJ<C>& geo, C u_ijk, C v_ijk, C w_ijk, C v_invrm,
-                                              C w_invrs, C nue_c, C nue_t_s){
-    const C r = scalar_rhs(a.k, in, n, geo, u_ijk, v_ijk, w_ijk, v_invrm, w_invrs, nue_c, nue_t_s);
-    stage_update(a, scalar_field(n), o, r, scalar_kind(n), in.an);
-}
 
 // Everything the momentum and temperature tendencies of one cell read: the stencils of u, v, w,
 // t, the p_dyn and p_hydro neighbours (FP64), the accumulators and n-copies, two forcing values.
@@ -241,20 +250,21 @@ struct MomIn {
 };
 
 template <typename S, typename C>
-__device__ __forceinline__ void load_momentum(MomIn<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb,
+__device__ __forceinline__ void load_momentum(MomIn<C>& in, const StageArgs<S, C>& a, const S* X, const Cell& c,
                                               const RhsConst<C>& K){
-    const double* P = a.pdyn;
+    const double* P = a.pdyn;                   // FP64, no boundary substitution: offsets from the cell
     const double* PH = a.phydro;
-    in.p_ip = ld(P + nb.oip); in.p_im = ld(P + nb.oim); in.p_jp = ld(P + nb.ojp); in.p_jm = ld(P + nb.ojm);
-    in.p_ke = ld(P + nb.oke); in.p_kw = ld(P + nb.okw);
-    in.ph_jp = ld(PH + nb.ojp); in.ph_jm = ld(PH + nb.ojm); in.ph_ke = ld(PH + nb.oke); in.ph_kw = ld(PH + nb.okw);
-    in.rU = load7<S, C>(nb, ATURAN_U); in.rV = load7<S, C>(nb, ATURAN_V); in.rW = load7<S, C>(nb, ATURAN_W);
-    in.rT = load7<S, C>(nb, ATURAN_T);
-    in.anU = load_acc_nc(a, ATURAN_U, nb.o); in.anV = load_acc_nc(a, ATURAN_V, nb.o);
-    in.anW = load_acc_nc(a, ATURAN_W, nb.o); in.anT = load_acc_nc(a, ATURAN_T, nb.o);
-    const S* F = a.forc + nb.o;
-    in.f_tmf = (K.tmf != C(0.0)) ? (C)ld(F + (size_t)(ATURAN_THERMALMASSFLUX - ATURAN_NUE) * nb.fs) : C(0.0);
-    in.f_qp = (K.precip_coupling != C(0.0)) ? (C)ld(F + (size_t)(ATURAN_Q_PRECIP - ATURAN_NUE) * nb.fs) : C(0.0);
+    const int JK = a.g.jm * a.g.kp, kp = a.g.kp;
+    in.p_ip = ld(P + (c.o + JK)); in.p_im = ld(P + (c.o - JK)); in.p_jp = ld(P + (c.o + kp)); in.p_jm = ld(P + (c.o - kp));
+    in.p_ke = ld(P + c.oke); in.p_kw = ld(P + c.okw);
+    in.ph_jp = ld(PH + (c.o + kp)); in.ph_jm = ld(PH + (c.o - kp)); in.ph_ke = ld(PH + c.oke); in.ph_kw = ld(PH + c.okw);
+    in.rU = load7c<S, C>(X, c, ATURAN_U); in.rV = load7c<S, C>(X, c, ATURAN_V); in.rW = load7c<S, C>(X, c, ATURAN_W);
+    in.rT = load7c<S, C>(X, c, ATURAN_T);
+    in.anU = load_acc_nc(a, X, c, ATURAN_U); in.anV = load_acc_nc(a, X, c, ATURAN_V);
+    in.anW = load_acc_nc(a, X, c, ATURAN_W); in.anT = load_acc_nc(a, X, c, ATURAN_T);
+    const S* F = X + (c.dforc + c.o);
+    in.f_tmf = (K.tmf != C(0.0)) ? (C)ld(F + (ATURAN_THERMALMASSFLUX - ATURAN_NUE) * c.fs) : C(0.0);
+    in.f_qp = (K.precip_coupling != C(0.0)) ? (C)ld(F + (ATURAN_Q_PRECIP - ATURAN_NUE) * c.fs) : C(0.0);
 }
 
 // The tendencies of u, v, w and t of one cell (RHS_Uran_Turb.cpp:117-175, :208-331, :382-391,
@@ -372,50 +382,50 @@ template <typename C>
 struct ScalarIn2 { ScalarIn<C> c0, c1; };
 
 template <typename S, typename C>
-__device__ __forceinline__ void load_scalar2(ScalarIn2<C>& in, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
+__device__ __forceinline__ void load_scalar2(ScalarIn2<C>& in, const StageArgs<S, C>& a, const S* X, const Cell& c, int n){
     const int q = scalar_field(n);
-    const size_t f = (size_t)q * nb.fs, o = nb.o;
+    const int f = q * c.fs;
     ScalarIn<C>& A = in.c0;
     ScalarIn<C>& B = in.c1;
-    ld2<S, C>(nb.X + f + o, A.v.c, B.v.c);
-    ld2<S, C>(nb.xip + f + nb.oip, A.v.rp, B.v.rp);
-    ld2<S, C>(nb.xim + f + nb.oim, A.v.rm, B.v.rm);
-    ld2<S, C>(nb.xjp + f + nb.ojp, A.v.tp, B.v.tp);
-    ld2<S, C>(nb.xjm + f + nb.ojm, A.v.tm, B.v.tm);
-    A.v.pw = (C)ld(nb.X + f + nb.okw);            // k0 - 1
-    B.v.pe = (C)ld(nb.X + f + nb.oke);            // k0 + 2
+    ld2<S, C>(X + (f + c.o), A.v.c, B.v.c);
+    ld2<S, C>(X + (f + c.oip), A.v.rp, B.v.rp);
+    ld2<S, C>(X + (f + c.oim), A.v.rm, B.v.rm);
+    ld2<S, C>(X + (f + c.ojp), A.v.tp, B.v.tp);
+    ld2<S, C>(X + (f + c.ojm), A.v.tm, B.v.tm);
+    A.v.pw = (C)ld(X + (f + c.okw));            // k0 - 1
+    B.v.pe = (C)ld(X + (f + c.oke));            // k0 + 2
     A.v.pe = B.v.c;
     B.v.pw = A.v.c;
     if(a.stage == 0){ A.an.acc = C(0.0); B.an.acc = C(0.0); }
-    else ld2_rw<S, C>(a.acc + f + o, A.an.acc, B.an.acc);
-    ld2<S, C>(a.Nc + f + o, A.an.nc, B.an.nc);
-    const S* F = a.forc + o;
-    const size_t fs = nb.fs;
+    else ld2_rw<S, C>(X + (c.dacc + f + c.o), A.an.acc, B.an.acc);
+    ld2<S, C>(X + (c.dnc + f + c.o), A.an.nc, B.an.nc);
+    const S* F = X + (c.dforc + c.o);
+    const int fs = c.fs;
     A.f2 = B.f2 = C(0.0); A.f3 = B.f3 = C(0.0);
     if(n < 12){
-        ld2<S, C>(F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs, A.f1, B.f1);
-        if(q == ATURAN_H2S) ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs, A.f2, B.f2);
-        if(q == ATURAN_NH3) ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs, A.f2, B.f2);
+        ld2<S, C>(F + (ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs, A.f1, B.f1);
+        if(q == ATURAN_H2S) ld2<S, C>(F + (ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs, A.f2, B.f2);
+        if(q == ATURAN_NH3) ld2<S, C>(F + (ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs, A.f2, B.f2);
     } else if(n == 12){
-        ld2<S, C>(F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs, A.f1, B.f1);
-        ld2<S, C>(F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs, A.f2, B.f2);
-        ld2<S, C>(F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs, A.f3, B.f3);
+        ld2<S, C>(F + (ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs, A.f1, B.f1);
+        ld2<S, C>(F + (ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs, A.f2, B.f2);
+        ld2<S, C>(F + (ATURAN_RHO_MIX - ATURAN_NUE) * fs, A.f3, B.f3);
     } else {
-        ld2<S, C>(F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs, A.f1, B.f1);
+        ld2<S, C>(F + ((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs, A.f1, B.f1);
     }
 }
 
 // stage_update for the pair, with vector stores.
 template <typename S, typename C>
-__device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, int q, size_t o, C r0, C r1, int kind,
+__device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, S* W, const Cell& c, int q, C r0, C r1, int kind,
                                               const AccNc<C>& n0, const AccNc<C>& n1){
-    const size_t off = (size_t)q * a.g.fstride + o;
+    const int off = q * c.fs + c.o;
     C acc0, acc1;
     if(a.stage == 0){ acc0 = a.wgt * r0; acc1 = a.wgt * r1; }
     else { acc0 = n0.acc + a.wgt * r0; acc1 = n1.acc + a.wgt * r1; }
     C y0, y1;
     if(a.stage < 3){
-        st2<S, C>(a.acc + off, acc0, acc1);
+        st2<S, C>(W + (c.dacc + off), acc0, acc1);
         y0 = n0.nc + a.c_in * r0; y1 = n1.nc + a.c_in * r1;
         if(kind == 2){ y0 = cclamp(y0, C(0.0), a.k.tke_max); y1 = cclamp(y1, C(0.0), a.k.tke_max); }
         else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
@@ -425,7 +435,7 @@ __device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, int q, s
         else if(kind == 2){ y0 = cclamp(cmax(y0, C(0.0)), C(0.0), a.k.tke_max); y1 = cclamp(cmax(y1, C(0.0)), C(0.0), a.k.tke_max); }
         else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
     }
-    st2<S, C>(a.Y + off, y0, y1);
+    st2<S, C>(W + (c.dY + off), y0, y1);
 }
 
 // The scalar part of a stage (the fifteen scalar fields), two cells per thread; the same
@@ -439,24 +449,14 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_pair_kernel(const StageAr
     if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
     const RhsConst<C>& K = a.k;
     const GeoIJ<C> geo = a.geo[i * g.jm + j];
-    Nbr<S> nb;
-    nb.fs  = g.fstride;
-    nb.o   = gidx(g, i, j, k);
-    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
-    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
-    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
-    nb.oke = nb.o - k + phi_wrap(k + 2, g.km);
-    nb.X   = a.X;
-    nb.xim = (i == 1) ? a.St : a.X;
-    nb.xip = (i == g.im - 2) ? a.St : a.X;
-    nb.xjm = (j == 1) ? a.St : a.X;
-    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
-    const size_t o = nb.o, fs = g.fstride;
+    const S* X = a.X;
+    S* W = const_cast<S*>(a.X);                  // acc and Y, reached through the same base
+    const Cell c = make_cell(a, i, j, k, 2);
     C nue0, nue1, u0, u1, v0, v1, w0, w1;
-    ld2<S, C>(a.forc + (size_t)(ATURAN_NUE - ATURAN_NUE) * fs + o, nue0, nue1);
-    ld2<S, C>(a.X + (size_t)ATURAN_U * fs + o, u0, u1);
-    ld2<S, C>(a.X + (size_t)ATURAN_V * fs + o, v0, v1);
-    ld2<S, C>(a.X + (size_t)ATURAN_W * fs + o, w0, w1);
+    ld2<S, C>(X + (c.dforc + c.o), nue0, nue1);                 // ATURAN_NUE, the forcing group's first
+    ld2<S, C>(X + (ATURAN_U * c.fs + c.o), u0, u1);
+    ld2<S, C>(X + (ATURAN_V * c.fs + c.o), v0, v1);
+    ld2<S, C>(X + (ATURAN_W * c.fs + c.o), w0, w1);
     auto nts = [&](C nue_c) -> C {
         const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
         return qdiv(nue_t, C(0.9), C(1.0 / 0.9));
@@ -467,15 +467,15 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_pair_kernel(const StageAr
     const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
     ScalarIn2<C> ring[PD + 1];
 #pragma unroll
-    for(int n = 0; n < PD; n++) if(n < nfield) load_scalar2(ring[n], a, nb, n);
+    for(int n = 0; n < PD; n++) if(n < nfield) load_scalar2(ring[n], a, X, c, n);
 #pragma unroll
     for(int n = 0; n < N_SCALARS; n++){
-        if(n + PD < nfield) load_scalar2(ring[(n + PD) % (PD + 1)], a, nb, n + PD);
+        if(n + PD < nfield) load_scalar2(ring[(n + PD) % (PD + 1)], a, X, c, n + PD);
         if(n < nfield){
             const ScalarIn2<C>& in = ring[n % (PD + 1)];
             const C r0 = scalar_rhs(K, in.c0, n, geo, u0, v0, w0, vr0, wr0, nue0, nts0);
             const C r1 = scalar_rhs(K, in.c1, n, geo, u1, v1, w1, vr1, wr1, nue1, nts1);
-            stage_update2(a, scalar_field(n), o, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
+            stage_update2(a, W, c, scalar_field(n), r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
         }
     }
 }
@@ -504,31 +504,31 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait(){ asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
 
 template <typename S, typename C>
-__device__ __forceinline__ void issue_scalar2(AsyncSlot<S>& sl, int t, const StageArgs<S, C>& a, const Nbr<S>& nb, int n){
+__device__ __forceinline__ void issue_scalar2(AsyncSlot<S>& sl, int t, const StageArgs<S, C>& a, const S* X, const Cell& c, int n){
     constexpr int V = (int)sizeof(typename Pair<S>::T);
     const int q = scalar_field(n);
-    const size_t f = (size_t)q * nb.fs, o = nb.o;
-    cp_async_n<V>(&sl.c[t], nb.X + f + o);
-    cp_async_n<V>(&sl.rp[t], nb.xip + f + nb.oip);
-    cp_async_n<V>(&sl.rm[t], nb.xim + f + nb.oim);
-    cp_async_n<V>(&sl.tp[t], nb.xjp + f + nb.ojp);
-    cp_async_n<V>(&sl.tm[t], nb.xjm + f + nb.ojm);
-    cp_async_n<(int)sizeof(S)>(&sl.pw[t], nb.X + f + nb.okw);
-    cp_async_n<(int)sizeof(S)>(&sl.pe[t], nb.X + f + nb.oke);
-    if(a.stage != 0) cp_async_n<V>(&sl.acc[t], a.acc + f + o);
-    cp_async_n<V>(&sl.nc[t], a.Nc + f + o);
-    const S* F = a.forc + o;
-    const size_t fs = nb.fs;
+    const int f = q * c.fs;
+    cp_async_n<V>(&sl.c[t], X + (f + c.o));
+    cp_async_n<V>(&sl.rp[t], X + (f + c.oip));
+    cp_async_n<V>(&sl.rm[t], X + (f + c.oim));
+    cp_async_n<V>(&sl.tp[t], X + (f + c.ojp));
+    cp_async_n<V>(&sl.tm[t], X + (f + c.ojm));
+    cp_async_n<(int)sizeof(S)>(&sl.pw[t], X + (f + c.okw));
+    cp_async_n<(int)sizeof(S)>(&sl.pe[t], X + (f + c.oke));
+    if(a.stage != 0) cp_async_n<V>(&sl.acc[t], X + (c.dacc + f + c.o));
+    cp_async_n<V>(&sl.nc[t], X + (c.dnc + f + c.o));
+    const S* F = X + (c.dforc + c.o);
+    const int fs = c.fs;
     if(n < 12){
-        cp_async_n<V>(&sl.f1[t], F + (size_t)(ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs);
-        if(q == ATURAN_H2S) cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs);
-        if(q == ATURAN_NH3) cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f1[t], F + (ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs);
+        if(q == ATURAN_H2S) cp_async_n<V>(&sl.f2[t], F + (ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs);
+        if(q == ATURAN_NH3) cp_async_n<V>(&sl.f2[t], F + (ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs);
     } else if(n == 12){
-        cp_async_n<V>(&sl.f1[t], F + (size_t)(ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs);
-        cp_async_n<V>(&sl.f2[t], F + (size_t)(ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs);
-        cp_async_n<V>(&sl.f3[t], F + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f1[t], F + (ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f2[t], F + (ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f3[t], F + (ATURAN_RHO_MIX - ATURAN_NUE) * fs);
     } else {
-        cp_async_n<V>(&sl.f1[t], F + (size_t)((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs);
+        cp_async_n<V>(&sl.f1[t], F + ((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs);
     }
 }
 
@@ -568,31 +568,21 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_async_kernel(const StageA
     const int i = 1 + blockIdx.z;
     if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
     const RhsConst<C>& K = a.k;
-    Nbr<S> nb;
-    nb.fs  = g.fstride;
-    nb.o   = gidx(g, i, j, k);
-    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
-    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
-    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
-    nb.oke = nb.o - k + phi_wrap(k + 2, g.km);
-    nb.X   = a.X;
-    nb.xim = (i == 1) ? a.St : a.X;
-    nb.xip = (i == g.im - 2) ? a.St : a.X;
-    nb.xjm = (j == 1) ? a.St : a.X;
-    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
+    const S* X = a.X;
+    S* W = const_cast<S*>(a.X);
+    const Cell c = make_cell(a, i, j, k, 2);
     const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
 #pragma unroll
     for(int n = 0; n < D; n++){
-        if(n < nfield) issue_scalar2(ring[n], t, a, nb, n);
+        if(n < nfield) issue_scalar2(ring[n], t, a, X, c, n);
         cp_async_commit();
     }
-    const size_t o = nb.o, fs = g.fstride;
     const GeoIJ<C> geo = a.geo[i * g.jm + j];
     C nue0, nue1, u0, u1, v0, v1, w0, w1;
-    ld2<S, C>(a.forc + (size_t)(ATURAN_NUE - ATURAN_NUE) * fs + o, nue0, nue1);
-    ld2<S, C>(a.X + (size_t)ATURAN_U * fs + o, u0, u1);
-    ld2<S, C>(a.X + (size_t)ATURAN_V * fs + o, v0, v1);
-    ld2<S, C>(a.X + (size_t)ATURAN_W * fs + o, w0, w1);
+    ld2<S, C>(X + (c.dforc + c.o), nue0, nue1);
+    ld2<S, C>(X + (ATURAN_U * c.fs + c.o), u0, u1);
+    ld2<S, C>(X + (ATURAN_V * c.fs + c.o), v0, v1);
+    ld2<S, C>(X + (ATURAN_W * c.fs + c.o), w0, w1);
     auto nts = [&](C nue_c) -> C {
         const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
         return qdiv(nue_t, C(0.9), C(1.0 / 0.9));
@@ -608,27 +598,24 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_async_kernel(const StageA
             take_scalar2(in, ring[n % D], t, a, n);
             const C r0 = scalar_rhs(K, in.c0, n, geo, u0, v0, w0, vr0, wr0, nue0, nts0);
             const C r1 = scalar_rhs(K, in.c1, n, geo, u1, v1, w1, vr1, wr1, nue1, nts1);
-            stage_update2(a, scalar_field(n), o, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
+            stage_update2(a, W, c, scalar_field(n), r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
         }
-        if(n + D < nfield) issue_scalar2(ring[n % D], t, a, nb, n + D);   // after the stores that used the slot
+        if(n + D < nfield) issue_scalar2(ring[n % D], t, a, X, c, n + D);   // after the stores that used the slot
         cp_async_commit();
     }
     cp_async_wait<0>();
 }
 
-// Fused RHS evaluation and stage update of one cell. PART selects the equations: 1 momentum and
-// temperature (u, v, w, t and the projection fields), 2 the fifteen scalar fields (twelve
-// condensables, NH4SH, k*, dis*). The two parts read disjoint stencil fields and write disjoint
-// accumulator / stage-output fields, so they run as two launches of one stage with half the
-// live registers each.
+// The first launch of a stage: fused RHS evaluation and stage update of momentum and temperature
+// (u, v, w, t and, at the last stage, the projection fields) of one cell. The second launch
+// (rk_scalar_pair_kernel / rk_scalar_async_kernel) takes the fifteen scalar fields: the two read
+// disjoint stencil fields and write disjoint accumulator / stage-output fields, so they run as two
+// launches of one stage with half the live registers each.
 //
-// The kernel is bound by the latency of its loads, not by HBM bytes, so it is written to keep
-// many loads in flight per thread: a store to acc or Y could alias any later load as far as the
-// compiler knows, so no load is ever placed after a store in program order. Part 1 issues all
-// of its ~50 loads before its first store; part 2 walks its 15 fields with the inputs of the
-// next PD fields already loading while one field is computed and stored. MINB is the launch
-// bound on resident blocks per SM.
-template <typename S, typename C, int PART, int PD, int MINB>
+// The kernel is bound by the latency of its loads, so it keeps many loads in flight per thread:
+// a store to acc or Y could alias any later load as far as the compiler knows, so all ~50 loads
+// of the cell are issued before its first store. MINB is the launch bound on resident blocks per SM.
+template <typename S, typename C, int MINB>
 __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, C> a){
     const Grid& g = a.g;
     const int k = blockIdx.x * 32 + threadIdx.x;
@@ -637,71 +624,32 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
     if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
     const RhsConst<C>& K = a.k;
     const GeoIJ<C> geo = a.geo[i * g.jm + j];
+    const S* X = a.X;
+    S* W = const_cast<S*>(a.X);
+    const Cell c = make_cell(a, i, j, k, 1);
 
-    Nbr<S> nb;
-    nb.fs  = g.fstride;
-    nb.o   = gidx(g, i, j, k);
-    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
-    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
-    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
-    nb.oke = nb.o - k + phi_wrap(k + 1, g.km);
-    nb.X   = a.X;
-    nb.xim = (i == 1) ? a.St : a.X;
-    nb.xip = (i == g.im - 2) ? a.St : a.X;
-    nb.xjm = (j == 1) ? a.St : a.X;
-    nb.xjp = (j == g.jm - 2) ? a.St : a.X;
-    const size_t o = nb.o, fs = g.fstride;
-    const size_t oim = nb.oim, oip = nb.oip, ojm = nb.ojm, ojp = nb.ojp, okw = nb.okw, oke = nb.oke;
-#define FORC(id) ((C)ld(a.forc + (size_t)((id) - ATURAN_NUE) * fs + o))
-
-    const C inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rmsinthe = geo.inv_rmsinthe;
-    const C inv_rm2sinthe = geo.inv_rm2sinthe, inv_rm2sinthe2 = geo.inv_rm2sinthe2;
-    const C costhe_inv_rm2sinthe = geo.costhe_inv_rm2sinthe, costhe = geo.costhe;
-    const C cotanthe = geo.cotanthe, two_inv_rm = geo.two_inv_rm;
-
-    const C nue_c = FORC(ATURAN_NUE);
+    const C nue_c = (C)ld(X + (c.dforc + c.o));                 // ATURAN_NUE, the forcing group's first
     const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
     const C nue_t_s = qdiv(nue_t, C(0.9), C(1.0 / 0.9));
 
-    if constexpr(PART == 1){
-    // ---- every load of the cell first ----
     MomIn<C> in;
-    load_momentum(in, a, nb, K);
+    load_momentum(in, a, X, c, K);
     C rhs_u, rhs_v, rhs_w, rhs_t, dpdr_term, dpdthe_term, dpdphi_term;
     momentum_rhs(a, in, geo, nue_t, nue_t_s, j, k, rhs_u, rhs_v, rhs_w, rhs_t, dpdr_term, dpdthe_term, dpdphi_term);
-    stage_update(a, ATURAN_U, o, rhs_u, 0, in.anU);
-    stage_update(a, ATURAN_V, o, rhs_v, 0, in.anV);
-    stage_update(a, ATURAN_W, o, rhs_w, 0, in.anW);
+    stage_update(a, W, c, ATURAN_U, rhs_u, 0, in.anU);
+    stage_update(a, W, c, ATURAN_V, rhs_v, 0, in.anV);
+    stage_update(a, W, c, ATURAN_W, rhs_w, 0, in.anW);
     if(a.stage == 3){
-        a.proj[0 * fs + o] = (S)rhs_u;
-        a.proj[1 * fs + o] = (S)rhs_v;
-        a.proj[2 * fs + o] = (S)rhs_w;
-        a.proj[3 * fs + o] = (S)(rhs_u + dpdr_term);
-        a.proj[4 * fs + o] = (S)(rhs_v + dpdthe_term);
-        a.proj[5 * fs + o] = (S)(rhs_w + dpdphi_term);
+        S* Pj = a.proj + c.o;
+        const int fs = c.fs;
+        Pj[0 * fs] = (S)rhs_u;
+        Pj[1 * fs] = (S)rhs_v;
+        Pj[2 * fs] = (S)rhs_w;
+        Pj[3 * fs] = (S)(rhs_u + dpdr_term);
+        Pj[4 * fs] = (S)(rhs_v + dpdthe_term);
+        Pj[5 * fs] = (S)(rhs_w + dpdphi_term);
     }
-    stage_update(a, ATURAN_T, o, rhs_t, 1, in.anT);
-    }
-
-    if constexpr(PART == 2){
-    const C u_ijk = (C)ld(a.X + (size_t)ATURAN_U * fs + o);
-    const C v_ijk = (C)ld(a.X + (size_t)ATURAN_V * fs + o);
-    const C w_ijk = (C)ld(a.X + (size_t)ATURAN_W * fs + o);
-    const C v_invrm = v_ijk * inv_rm;
-    const C w_invrs = w_ijk * inv_rmsinthe;
-    const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
-    // ring of PD + 1 field inputs: fields n+1..n+PD load while field n is computed and stored
-    ScalarIn<C> ring[PD + 1];
-#pragma unroll
-    for(int n = 0; n < PD; n++) if(n < nfield) load_scalar(ring[n], a, nb, n);
-#pragma unroll
-    for(int n = 0; n < N_SCALARS; n++){
-        if(n + PD < nfield) load_scalar(ring[(n + PD) % (PD + 1)], a, nb, n + PD);
-        if(n < nfield)
-            scalar_update(a, ring[n % (PD + 1)], n, o, geo, u_ijk, v_ijk, w_ijk, v_invrm, w_invrs, nue_c, nue_t_s);
-    }
-    }
-#undef FORC
+    stage_update(a, W, c, ATURAN_T, rhs_t, 1, in.anT);
 }
 
 // ---- RungeKutta_Uran_Turb.cpp:18-37: per level, sin(theta)-weighted mean of g p / (r R T t_ref)
