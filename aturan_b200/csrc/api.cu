@@ -283,26 +283,37 @@ template <typename S> S* grp(void* base, int q, size_t fs){ return reinterpret_c
 template <typename S>
 bool taping(const aturan_ctx* ctx){ return std::is_same<S, double>::value && ctx->tape != nullptr; }
 
-template <typename S, typename C>
-int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
+// The RK4 prelude: the buoyancy level means and the hydrostatic integral from the state at the
+// start of the step (RungeKutta_Uran_Turb.cpp:18-177), on stream st.
+template <typename S>
+int rk4_prelude(aturan_ctx* ctx, cudaStream_t st){
     const Grid g = ctx->g;
     const size_t fs = g.fstride;
     S* state = reinterpret_cast<S*>(ctx->state);
-    {
     const int exact = ctx->mixed ? 0 : ctx->p.exact_reductions;   // the mixed form always sums in tree order
-    Region reg(ctx, ATURAN_K_HYDRO, exact ? 2 : 3);
+    Region reg(ctx, ATURAN_K_HYDRO, exact ? 2 : 3, st);
     launch_buoy(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), ctx->wsin, ctx->hc,
-                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, ctx->st);
+                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, st);
     CK_LAUNCH("buoyancy reference level");
+    launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
+                 grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
+                 ctx->phydro, ctx->hc, 1, st);
+    CK_LAUNCH("hydrostatic integral");
+    return ATURAN_OK;
+}
+
+// One RK4 step; prelude_done: rk4_prelude has already run for this step (aturan_step runs it on
+// the side stream, beside the pressure solve).
+template <typename S, typename C>
+int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* state = reinterpret_cast<S*>(ctx->state);
+    if(!prelude_done){ const int rc = rk4_prelude<S>(ctx, ctx->st); if(rc) return rc; }
     if(taping<S>(ctx)){
         CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->tX, state, ADJ_NF * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->tPd, ctx->pdyn, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
-    }
-    launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
-                 grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
-                 ctx->phydro, ctx->hc, 1, ctx->st);
-    CK_LAUNCH("hydrostatic integral");
     }
     StageArgs<S, C> a;
     a.g = g;
@@ -341,8 +352,9 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K){
     return ATURAN_OK;
 }
 
+// with_sync: also perform aturan_sync_ncopies' copies, fused (the values are in registers).
 template <typename S>
-int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st){
+int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st, bool with_sync = false){
     const size_t fs = ctx->g.fstride;
     S* state = reinterpret_cast<S*>(ctx->state);
     SatArgs<S> a;
@@ -356,6 +368,9 @@ int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st){
     a.k = ctx->sc;
     a.gas_mask = mask;
     a.counters = count ? ctx->counters : nullptr;
+    a.nc_off = (long long)(reinterpret_cast<S*>(ctx->ncopy) - state);
+    a.sync = with_sync ? (ctx->p.nh4sh_sync ? 2 : 1) : 0;
+    a.nh4sh = grp<S>(state, ATURAN_NH4SH, fs);
     Region reg(ctx, ATURAN_K_SATADJ, 1, st);
     launch_satadj(a, st);
     CK_LAUNCH("saturation adjustment");
@@ -469,14 +484,27 @@ int sor_correct(aturan_ctx* ctx, T* P){
     return ATURAN_OK;
 }
 
+// Dynamic shared memory of sor_line_kernel: the right-hand sides of LINE_COLS columns and the
+// row's three factor arrays, per level.
+inline size_t line_smem(const Grid& g){ return (size_t)(g.im - 2) * (LINE_COLS + 3) * sizeof(double); }
+
+// Allow sor_line_kernel above the default 48 KB of dynamic shared memory (once per instance).
+template <typename T, bool TR>
+bool line_smem_attr(){
+    static const bool ok = cudaFuncSetAttribute(sor_line_kernel<T, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                227 * 1024) == cudaSuccess || (cudaGetLastError(), false);
+    return ok;
+}
+
 // One relaxation sweep (both colours) of the folded operator (TR: its transpose): point
 // (line = false) or radial line.
 template <typename T, bool TR = false>
 void sor_sweep(aturan_ctx* ctx, T* E, const T* R, double omega, bool line){
     const Grid g = ctx->g;
+    if(line && line_smem(g) > 48 * 1024) line_smem_attr<T, TR>();
     for(int colour = 0; colour < 2; colour++){
         if(line)
-            sor_line_kernel<T, TR><<<dim3((g.km / 2 + 31) / 32, g.jm - 2), 256, (size_t)(g.im - 2) * 35 * sizeof(double), ctx->st>>>(
+            sor_line_kernel<T, TR><<<dim3((g.km / 2 + LINE_COLS - 1) / LINE_COLS, g.jm - 2), 256, line_smem(g), ctx->st>>>(
                 g, E, R, ctx->rbw, TR ? ctx->lluT_a : ctx->llu_a, TR ? ctx->lluT_cf : ctx->llu_cf,
                 TR ? ctx->lluT_idn : ctx->llu_idn, colour, omega);
         else
@@ -490,8 +518,8 @@ int sor_check_sizes(aturan_ctx* ctx, double omega, bool line){
     if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
     if(8 * ctx->sorc.J * (5 * ctx->sor_pm + 4) > 227 * 1024)
         return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 2900");
-    if(line && (g.im - 2) * 35 * (int)sizeof(double) > 49152)
-        return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 177");
+    if(line && line_smem(g) > 227 * 1024)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 435");
     return ATURAN_OK;
 }
 
@@ -1368,24 +1396,27 @@ int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omeg
 }
 
 // The reference's order is pressure, saturation adjustment, n-copy sync, RK4. The pressure solve
-// reads and writes p_dyn and the projection fields only; the adjustment and the sync read t,
-// p_stat, rho_mix and the species and write t, the species and their n-copies only. The two are
-// disjoint, so they run side by side with the same results as in order: the adjustment (one
-// large FP64-bound launch) on the low-priority side stream, the solve (a chain of small launches
-// and residual reads) on the main stream, whose blocks the scheduler places first. RK4 waits for
-// both.
+// reads and writes p_dyn and the projection fields only; the adjustment and the sync (fused into
+// the adjustment's launch here) read t, p_stat, rho_mix, the species and NH4SH and write t, the
+// species and their n-copies only; RK4's prelude
+// (level means, hydrostatic integral) reads t, p_stat, v, w and writes the level means, p_hydro and
+// p_bfollow only. So the solve on one side and adjustment, sync and prelude on the other are
+// disjoint, and they run side by side with the same results as in order: the latter (one large
+// FP64-bound launch, two small launches) on the low-priority side stream, the solve (a
+// chain of small launches and residual reads) on the main stream, whose blocks the scheduler
+// places first. The RK4 stages wait for both.
 int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol){
     if(!ctx) return ATURAN_E_INVALID;
     CK(cudaEventRecord(ctx->ev_fork, ctx->st));
     CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
-    int rc2 = ctx->mixed ? run_satadj<float>(ctx, 0xF, false, ctx->st2)
-                         : run_satadj<double>(ctx, 0xF, false, ctx->st2);
-    if(!rc2) rc2 = sync_ncopies(ctx, ctx->st2);
+    int rc2 = ctx->mixed ? run_satadj<float>(ctx, 0xF, false, ctx->st2, true)
+                         : run_satadj<double>(ctx, 0xF, false, ctx->st2, true);
+    if(!rc2) rc2 = ctx->mixed ? rk4_prelude<float>(ctx, ctx->st2) : rk4_prelude<double>(ctx, ctx->st2);
     CK(cudaEventRecord(ctx->ev_join, ctx->st2));
     const int rc = rc2 ? rc2 : aturan_pressure(ctx, press_kind, omega, max_sweeps, tol, nullptr, nullptr);
     CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));
     if(rc < 0 || rc2) return rc < 0 ? rc : rc2;
-    rc2 = aturan_rk4_step(ctx);
+    rc2 = ctx->mixed ? run_rk4<float, float>(ctx, ctx->k32, true) : run_rk4<double, double>(ctx, ctx->k64, true);
     if(rc2) return rc2;
     return rc;
 }

@@ -43,6 +43,12 @@ struct SatArgs {
     SatConst k;
     int gas_mask;
     unsigned long long* counters;   // [0] adjusted, [1] not converged (summed over gases)
+    // n-copy sync fused into the adjustment (aturan_step): when sync != 0, t, the twelve species and
+    // (sync == 2) NH4SH are also written to their start-of-step copies, nc_off elements from the
+    // fields, the values the adjustment leaves -- what the copy after it would write.
+    long long nc_off;
+    int sync;
+    S* nh4sh;
 };
 
 // The saturation vapour density rho ep svp(T) / p of the liquid (ice = false) or ice set.
@@ -82,7 +88,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
         if(K.local_rho){ const double r_ = (double)__ldg(a.rho_mix + q); rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : K.r_mix; }
         const double cp_mix = K.cp_mix, t_ref = K.t_ref;
         for(int gi = 0; gi < 4; gi++){
-            if(!(a.gas_mask & (1 << gi))) continue;
+            if(!(a.gas_mask & (1 << gi))){
+                if(a.sync){ S* f[3] = {a.spec[gi][0], a.spec[gi][1], a.spec[gi][2]};
+                            for(int n = 0; n < 3; n++) f[n][q + a.nc_off] = f[n][q]; }
+                continue;
+            }
             const GasConst& G = K.gas[gi];
             S* cP = a.spec[gi][0]; S* clP = a.spec[gi][1]; S* iP = a.spec[gi][2];
             double c = (double)cP[q], cloud = (double)clP[q], ice = (double)iP[q];
@@ -274,8 +284,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
             if(cloud <= 0.0) cloud = 0.0;
             if(ice <= 0.0) ice = 0.0;
             cP[q] = (S)c; clP[q] = (S)cloud; iP[q] = (S)ice;
+            if(a.sync){ cP[q + a.nc_off] = (S)c; clP[q + a.nc_off] = (S)cloud; iP[q + a.nc_off] = (S)ice; }
         }
         a.t[q] = (S)tt;
+        if(a.sync){
+            a.t[q + a.nc_off] = (S)tt;
+            if(a.sync == 2) a.nh4sh[q + a.nc_off] = a.nh4sh[q];
+        }
     }
     // per-block counter reduction: integer adds, order-independent. Without counters (uniform
     // over the block) each warp leaves as soon as its cells are done.

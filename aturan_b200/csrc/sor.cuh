@@ -335,72 +335,94 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
 // (the theta fold changes the diagonal on the first and last rows). TR relaxes Lc^T instead: the
 // transposed theta couplings and the host-factored transposed column tridiagonals.
 //
-// A block takes 32 columns of one colour in one row j. Its 8 warps form the right-hand sides of
-// all levels in parallel (coalesced along k, one level per warp at a time) into shared memory
-// [level][column] and stage the row's factors beside them; warp 0 then runs the 32 columns'
-// forward and back recurrences entirely on shared-memory latency, in place; all warps write the
-// relaxed columns back. Shared memory: (im - 2) * 35 doubles.
+// A block takes 64 columns of one colour in one row j (lane l: columns l and l + 32). Its 8 warps
+// form the right-hand sides of all levels in parallel (coalesced along k, one level of 32 columns
+// per warp at a time) into shared memory [level][column] and stage the row's factors beside them;
+// warp 0 then runs the recurrences of each lane's two columns interleaved (two independent
+// dependency chains per lane), entirely on shared-memory latency, in place; all warps write the
+// relaxed columns back. Shared memory: (im - 2) * (LINE_COLS + 3) doubles. With 64 columns the
+// default grid's 537 blocks are resident at once (one wave).
+constexpr int LINE_COLS = 64;
 template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
                                                        const double* lcf, const double* lidn, int colour, double omega){
     extern __shared__ double ds[];
     const int n = g.im - 2;
-    double* fa = ds + (size_t)n * 32;                  // the row's factors by level
+    double* fa = ds + (size_t)n * LINE_COLS;           // the row's factors by level
     double* fc = fa + n;
     double* fi = fc + n;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    const int k2 = blockIdx.x * 32 + lane;
     const int j = 1 + blockIdx.y;
-    const int k = 2 * k2 + ((j + colour) & 1);
-    const bool valid = k2 < g.km / 2 && k <= g.km - 2;
-    const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
     const size_t sj = g.kp;
     for(int i = threadIdx.x; i < n; i += blockDim.x){
         const size_t f = (size_t)(i + 1) * g.jm + j;
         fa[i] = la[f]; fc[i] = lcf[f]; fi[i] = lidn[f];
     }
+    int kk[2]; bool valid[2];
+#pragma unroll
+    for(int h = 0; h < 2; h++){
+        const int k2 = blockIdx.x * LINE_COLS + h * 32 + lane;
+        kk[h] = 2 * k2 + ((j + colour) & 1);
+        valid[h] = k2 < g.km / 2 && kk[h] <= g.km - 2;
+    }
 #pragma unroll 5
     for(int i = 1 + wp; i <= n; i += 8){
-        double d = 0.0;
-        if(valid){
-            const RBW W = w[i * g.jm + j];
-            const size_t o = gidx(g, i, j, k);
-            double h;
-            if constexpr(TR){                          // the transposed theta couplings (folded_accT)
-                h = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
-                if(j - 1 >= 1)        h += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
-                if(j + 1 <= g.jm - 2) h += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
-            } else {
-                const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
-                const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
-                h = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+        const RBW W = w[i * g.jm + j];
+#pragma unroll
+        for(int h = 0; h < 2; h++){
+            double d = 0.0;
+            if(valid[h]){
+                const int k = kk[h];
+                const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+                const size_t o = gidx(g, i, j, k);
+                double hsum;
+                if constexpr(TR){                      // the transposed theta couplings (folded_accT)
+                    hsum = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+                    if(j - 1 >= 1)        hsum += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
+                    if(j + 1 <= g.jm - 2) hsum += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
+                } else {
+                    const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
+                    const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
+                    hsum = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+                }
+                d = hsum - (double)R[o];
             }
-            d = h - (double)R[o];
+            ds[(i - 1) * LINE_COLS + h * 32 + lane] = d;
         }
-        ds[(i - 1) * 32 + lane] = d;
     }
     __syncthreads();
     if(wp == 0){
-        double yp = 0.0;
+        double* c0 = ds + lane;
+        double* c1 = ds + 32 + lane;
+        double y0 = 0.0, y1 = 0.0;
 #pragma unroll 4
         for(int i = 0; i < n; i++){
-            yp = (ds[i * 32 + lane] - fa[i] * yp) * fi[i];
-            ds[i * 32 + lane] = yp;
+            const double a_ = fa[i], r_ = fi[i];
+            y0 = (c0[i * LINE_COLS] - a_ * y0) * r_;
+            y1 = (c1[i * LINE_COLS] - a_ * y1) * r_;
+            c0[i * LINE_COLS] = y0;
+            c1[i * LINE_COLS] = y1;
         }
-        double x = ds[(n - 1) * 32 + lane];
+        double x0 = c0[(n - 1) * LINE_COLS], x1 = c1[(n - 1) * LINE_COLS];
 #pragma unroll 4
         for(int i = n - 2; i >= 0; i--){
-            x = ds[i * 32 + lane] - fc[i] * x;
-            ds[i * 32 + lane] = x;
+            const double c_ = fc[i];
+            x0 = c0[i * LINE_COLS] - c_ * x0;
+            x1 = c1[i * LINE_COLS] - c_ * x1;
+            c0[i * LINE_COLS] = x0;
+            c1[i * LINE_COLS] = x1;
         }
     }
     __syncthreads();
-    if(valid){
+#pragma unroll
+    for(int h = 0; h < 2; h++){
+        if(valid[h]){
 #pragma unroll 5
-        for(int i = 1 + wp; i <= n; i += 8){
-            const size_t o = gidx(g, i, j, k);
-            const double p0 = (double)P[o];
-            P[o] = (T)(p0 + omega * (ds[(i - 1) * 32 + lane] - p0));
+            for(int i = 1 + wp; i <= n; i += 8){
+                const size_t o = gidx(g, i, j, kk[h]);
+                const double p0 = (double)P[o];
+                P[o] = (T)(p0 + omega * (ds[(i - 1) * LINE_COLS + h * 32 + lane] - p0));
+            }
         }
     }
 }

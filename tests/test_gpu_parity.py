@@ -347,12 +347,13 @@ def test_restore_ncopies_is_restorevar():
 
 @pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
 def test_step_side_by_side_equals_in_order(synth, precision):
-    """aturan_step runs the saturation adjustment and the n-copy sync on a second stream beside the
-    pressure solve. They touch disjoint fields, so two full-size steps must give the same bits as
-    the four calls in the reference's order (pressure, adjustment, sync, RK4)."""
+    """aturan_step runs the saturation adjustment (with the n-copy sync fused into its launch) and
+    RK4's level means and hydrostatic integral on a second stream beside the pressure solve. They
+    touch disjoint fields, so two full-size steps must give the same bits, n-copies and hydrostatic
+    fields included, as the four calls in the reference's order (pressure, adjustment, sync, RK4)."""
     _, st0 = synth
     p = P.default_params(precision=precision)
-    names = F.PROGNOSTIC + ["p_dyn", "p_hydro"]
+    names = F.PROGNOSTIC + F.NCOPIES + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION
     a, b = ctx_for(p), ctx_for(p)
     a.upload_state(st0)
     b.upload_state(st0)
