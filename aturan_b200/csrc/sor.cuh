@@ -48,20 +48,28 @@ __device__ __forceinline__ double ywt(int n, int lo, int hi){ return (n == lo ||
 // row couples only to the other colour, so red-black SOR keeps its consistently-ordered rate
 // (with the lagged rows the radially structured modes converge at ~0.955 per sweep at omega 1.9
 // instead of ~0.9). Returns the off-diagonal sum; *diag receives the diagonal.
+// The weights a row reads, through the read-only path (the tables never change inside a launch).
+struct RBW4 { double num1, num2, num3, den; };
+__device__ __forceinline__ RBW4 ldw(const RBW* w){
+    RBW4 r; r.num1 = __ldg(&w->num1); r.num2 = __ldg(&w->num2); r.num3 = __ldg(&w->num3); r.den = __ldg(&w->den);
+    return r;
+}
+
 template <typename T>
 __device__ __forceinline__ double folded_acc(const Grid& g, const T* P, size_t o, int i, int j, int k,
-                                             const RBW& W, double* diag){
+                                             const RBW4& W, double* diag){
     const size_t si = (size_t)g.jm * g.kp, sj = g.kp;
     const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+    auto p = [&](size_t q){ return (double)__ldg(P + q); };
     double d = W.den;
     double aim, aip, ajm, ajp;
-    if(i == 1)        { d -= C43 * W.num1; aim = -C13 * (double)P[o + si]; } else aim = (double)P[o - si];
-    if(i == g.im - 2) { d -= C43 * W.num1; aip = -C13 * (double)P[o - si]; } else aip = (double)P[o + si];
-    if(j == 1)        { d -= C43 * W.num2; ajm = -C13 * (double)P[o + sj]; } else ajm = (double)P[o - sj];
-    if(j == g.jm - 2) { d -= C43 * W.num2; ajp = -C13 * (double)P[o - sj]; } else ajp = (double)P[o + sj];
+    if(i == 1)        { d -= C43 * W.num1; aim = -C13 * p(o + si); } else aim = p(o - si);
+    if(i == g.im - 2) { d -= C43 * W.num1; aip = -C13 * p(o - si); } else aip = p(o + si);
+    if(j == 1)        { d -= C43 * W.num2; ajm = -C13 * p(o + sj); } else ajm = p(o - sj);
+    if(j == g.jm - 2) { d -= C43 * W.num2; ajp = -C13 * p(o - sj); } else ajp = p(o + sj);
     *diag = d;
     return (aip + aim) * W.num1 + (ajp + ajm) * W.num2
-         + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+         + (p(o - k + ke) + p(o - k + kw)) * W.num3;
 }
 
 // The transposed folded operator (the pressure solve's adjoint): the gather of every row's
@@ -73,18 +81,19 @@ __device__ __forceinline__ double folded_accT(const Grid& g, const T* P, size_t 
                                               const RBW* w, double* diag){
     const size_t si = (size_t)g.jm * g.kp, sj = g.kp;
     const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
-    const RBW W = w[i * g.jm + j];
+    const RBW4 W = ldw(w + i * g.jm + j);
     double d = W.den;
     if(i == 1)        d -= C43 * W.num1;
     if(i == g.im - 2) d -= C43 * W.num1;
     if(j == 1)        d -= C43 * W.num2;
     if(j == g.jm - 2) d -= C43 * W.num2;
     *diag = d;
-    double acc = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
-    if(i - 1 >= 1)        acc += w[(i - 1) * g.jm + j].num1 * (i - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - si];
-    if(i + 1 <= g.im - 2) acc += w[(i + 1) * g.jm + j].num1 * (i + 1 == g.im - 2 ? 1.0 - C13 : 1.0) * (double)P[o + si];
-    if(j - 1 >= 1)        acc += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
-    if(j + 1 <= g.jm - 2) acc += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
+    auto p = [&](size_t q){ return (double)__ldg(P + q); };
+    double acc = (p(o - k + ke) + p(o - k + kw)) * W.num3;
+    if(i - 1 >= 1)        acc += __ldg(&w[(i - 1) * g.jm + j].num1) * (i - 1 == 1 ? 1.0 - C13 : 1.0) * p(o - si);
+    if(i + 1 <= g.im - 2) acc += __ldg(&w[(i + 1) * g.jm + j].num1) * (i + 1 == g.im - 2 ? 1.0 - C13 : 1.0) * p(o + si);
+    if(j - 1 >= 1)        acc += __ldg(&w[i * g.jm + j - 1].num2) * (j - 1 == 1 ? 1.0 - C13 : 1.0) * p(o - sj);
+    if(j + 1 <= g.jm - 2) acc += __ldg(&w[i * g.jm + j + 1].num2) * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * p(o + sj);
     return acc;
 }
 
@@ -93,7 +102,7 @@ template <bool TR, typename T>
 __device__ __forceinline__ double row_acc(const Grid& g, const T* P, size_t o, int i, int j, int k,
                                           const RBW* w, double* diag){
     if constexpr(TR) return folded_accT<T>(g, P, o, i, j, k, w, diag);
-    else return folded_acc<T>(g, P, o, i, j, k, w[i * g.jm + j], diag);
+    else return folded_acc<T>(g, P, o, i, j, k, ldw(w + i * g.jm + j), diag);
 }
 
 // Residual r = src - Lc p of the folded operator (or src - Lc^T p, TR): per (j,k) column its
@@ -117,8 +126,8 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
             const size_t o = gidx(g, i, j, k);
             double diag;
             const double acc = row_acc<TR, T>(g, P, o, i, j, k, w, &diag);
-            const double lc = acc - diag * (double)P[o];
-            const double s = (double)src[o];
+            const double lc = acc - diag * (double)__ldg(P + o);
+            const double s = (double)__ldg(src + o);
             const double r = s - lc;
             if(r32){ r32[o] = (float)r; e32[o] = 0.0f; }  // the mixed form's next correction solve
             R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
@@ -322,7 +331,7 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
     double diag;
     const double acc = row_acc<TR, T>(g, E, o, i, j, k, w, &diag);
     const double e0 = (double)E[o];
-    const double pn = (acc - (double)R[o]) / diag;
+    const double pn = (acc - (double)__ldg(R + o)) / diag;
     E[o] = (T)(e0 + omega * (pn - e0));
 }
 
@@ -354,6 +363,8 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const int j = 1 + blockIdx.y;
     const size_t sj = g.kp;
+    // phase 1 reads only the other colour's cells, which this launch does not write: read-only path
+    auto p = [&](size_t q){ return (double)__ldg(P + q); };
     for(int i = threadIdx.x; i < n; i += blockDim.x){
         const size_t f = (size_t)(i + 1) * g.jm + j;
         fa[i] = la[f]; fc[i] = lcf[f]; fi[i] = lidn[f];
@@ -367,7 +378,7 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
     }
 #pragma unroll 5
     for(int i = 1 + wp; i <= n; i += 8){
-        const RBW W = w[i * g.jm + j];
+        const RBW4 W = ldw(w + i * g.jm + j);
 #pragma unroll
         for(int h = 0; h < 2; h++){
             double d = 0.0;
@@ -377,15 +388,15 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
                 const size_t o = gidx(g, i, j, k);
                 double hsum;
                 if constexpr(TR){                      // the transposed theta couplings (folded_accT)
-                    hsum = ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
-                    if(j - 1 >= 1)        hsum += w[i * g.jm + j - 1].num2 * (j - 1 == 1 ? 1.0 - C13 : 1.0) * (double)P[o - sj];
-                    if(j + 1 <= g.jm - 2) hsum += w[i * g.jm + j + 1].num2 * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * (double)P[o + sj];
+                    hsum = (p(o - k + ke) + p(o - k + kw)) * W.num3;
+                    if(j - 1 >= 1)        hsum += __ldg(&w[i * g.jm + j - 1].num2) * (j - 1 == 1 ? 1.0 - C13 : 1.0) * p(o - sj);
+                    if(j + 1 <= g.jm - 2) hsum += __ldg(&w[i * g.jm + j + 1].num2) * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * p(o + sj);
                 } else {
-                    const double ajm = (j == 1)        ? -C13 * (double)P[o + sj] : (double)P[o - sj];
-                    const double ajp = (j == g.jm - 2) ? -C13 * (double)P[o - sj] : (double)P[o + sj];
-                    hsum = (ajp + ajm) * W.num2 + ((double)P[o - k + ke] + (double)P[o - k + kw]) * W.num3;
+                    const double ajm = (j == 1)        ? -C13 * p(o + sj) : p(o - sj);
+                    const double ajp = (j == g.jm - 2) ? -C13 * p(o - sj) : p(o + sj);
+                    hsum = (ajp + ajm) * W.num2 + (p(o - k + ke) + p(o - k + kw)) * W.num3;
                 }
-                d = hsum - (double)R[o];
+                d = hsum - (double)__ldg(R + o);
             }
             ds[(i - 1) * LINE_COLS + h * 32 + lane] = d;
         }
