@@ -59,6 +59,22 @@ struct SatArgs {
 struct SatT { double T, lg, inv; };
 __device__ __forceinline__ SatT sat_t(double T){ SatT r; r.T = T; r.lg = log(T); r.inv = 1.0 / T; return r; }
 
+// SatT at T + dT from SatT at T, for the Newton pass's finite difference (mixed form): with
+// x = dT / T, log(T + dT) = log T + log1p(x) and 1 / (T + dT) = (1 / T) / (1 + x), both by their
+// Taylor series through x^7 (truncation below x^8 / 8, i.e. below 1e-20 of the result for
+// x <= 2e-3, T >= 50 K at dT = 0.1); a full log and division above that.
+__device__ __forceinline__ SatT sat_t_next(const SatT& s, double dT){
+    const double x = dT * s.inv;
+    if(!(x <= 2.0e-3)) return sat_t(s.T + dT);
+    SatT r;
+    r.T = s.T + dT;
+    const double l1p = x * (1.0 + x * (-0.5 + x * (1.0 / 3.0 + x * (-0.25 + x * (0.2 + x * (-1.0 / 6.0 + x * (1.0 / 7.0)))))));
+    const double rcp = 1.0 + x * (-1.0 + x * (1.0 + x * (-1.0 + x * (1.0 + x * (-1.0 + x * (1.0 - x))))));
+    r.lg = s.lg + l1p;
+    r.inv = s.inv * rcp;
+    return r;
+}
+
 template <bool FAST>
 __device__ __forceinline__ double qsat(const GasConst& G, bool ice, double rho_c, double ep, double p_u,
                                        double rep, double T, const SatT& st){
@@ -87,6 +103,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
         double rho_c = K.r_mix;                               // rho_at, cUranusModel.h:526-531
         if(K.local_rho){ const double r_ = (double)__ldg(a.rho_mix + q); rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : K.r_mix; }
         const double cp_mix = K.cp_mix, t_ref = K.t_ref;
+        // latent heat to temperature: x / (cp_mix rho_c), a multiplication in the mixed form
+        const double inv_hc = FAST ? 1.0 / (cp_mix * rho_c) : 0.0;
+        auto per_hc = [&](double x) -> double {
+            if constexpr(FAST) return x * inv_hc; else return x / (cp_mix * rho_c);
+        };
+        // log T and 1/T at the entry temperature, shared by the gases while none changes T (mixed form)
+        SatT st_entry; st_entry.T = -1.0;
         for(int gi = 0; gi < 4; gi++){
             if(!(a.gas_mask & (1 << gi))){
                 if(a.sync){ S* f[3] = {a.spec[gi][0], a.spec[gi][1], a.spec[gi][2]};
@@ -137,7 +160,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                 const double ep = G.ep, lv = G.lv, ls = G.ls, tri = G.t_range_inv;
                 const double rep = FAST ? rho_c * ep / p_u : 0.0;
                 SatT st0;
-                if constexpr(FAST) st0 = sat_t(t_u);
+                if constexpr(FAST){
+                    if(t_u != st_entry.T) st_entry = sat_t(t_u);
+                    st0 = st_entry;
+                }
                 const double q_Rain_0 = qsat<FAST>(G, false, rho_c, ep, p_u, rep, t_u, st0);
                 bool go = q_Rain_0 > 0.0;                             // :422
                 if(go){
@@ -178,7 +204,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                         if(berg){
                             CND = 0.0; DEP = 1.0;
                             if(q_c_b > 0.0){
-                                T -= lv * q_c_b / (cp_mix * rho_c);
+                                T -= per_hc(lv * q_c_b);
                                 q_v_b += q_c_b;
                                 q_c_b = 0.0;
                             }
@@ -193,7 +219,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                                                      if(q_c_b + d_q_c < 0.0) d_q_c = -q_c_b; }
                             d_q_v = -(d_q_c + d_q_i);
                         }
-                        T     += (lv * d_q_c + ls * d_q_i) / (cp_mix * rho_c);
+                        T     += per_hc(lv * d_q_c + ls * d_q_i);
                         q_v_b += d_q_v;
                         q_c_b += d_q_c;
                         q_i_b += d_q_i;
@@ -247,7 +273,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                             const double dT = 0.1;
                             const int nd = need(T);
                             SatT stD;
-                            if constexpr(FAST) stD = sat_t(T + dT);
+                            if constexpr(FAST) stD = (T == stT.T) ? sat_t_next(stT, dT) : sat_t(T + dT);
                             const double q_Rain_d = (nd & 1) ? qsat<FAST>(G, false, rho_c, ep, p_u, rep, T + dT, stD) : 0.0;
                             const double q_Ice_d  = (nd & 2) ? qsat<FAST>(G, true, rho_c, ep, p_u, rep, T + dT, stD) : 0.0;
                             double q_hyp_d;
@@ -263,8 +289,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                             if(T <= t_00) CNDn = 0.0;
                             if(T >= t_0)  CNDn = 1.0;
                             if(berg)      CNDn = 0.0;
-                            const double Gf = (lv * CNDn + ls * (1.0 - CNDn)) / (cp_mix * rho_c)
-                                            * (q_hyp_d - q_v_hyp) / dT;
+                            double Gf;
+                            if constexpr(FAST) Gf = (lv * CNDn + ls * (1.0 - CNDn)) * inv_hc * (q_hyp_d - q_v_hyp) * (1.0 / dT);
+                            else Gf = (lv * CNDn + ls * (1.0 - CNDn)) / (cp_mix * rho_c) * (q_hyp_d - q_v_hyp) / dT;
                             const double Gp = (Gf < 0.0) ? 0.0 : Gf;          // std::max(G, 0.0)
                             double wn = 1.0 / (1.0 + Gp);
                             if(wn < 0.05) wn = 0.05;
