@@ -59,13 +59,14 @@ struct SatArgs {
 struct SatT { double T, lg, inv; };
 __device__ __forceinline__ SatT sat_t(double T){ SatT r; r.T = T; r.lg = log(T); r.inv = 1.0 / T; return r; }
 
-// SatT at T + dT from SatT at T, for the Newton pass's finite difference (mixed form): with
-// x = dT / T, log(T + dT) = log T + log1p(x) and 1 / (T + dT) = (1 / T) / (1 + x), both by their
-// Taylor series through x^7 (truncation below x^8 / 8, i.e. below 1e-20 of the result for
-// x <= 2e-3, T >= 50 K at dT = 0.1); a full log and division above that.
+// SatT at T + dT from SatT at T (mixed form): with x = dT / T, log(T + dT) = log T + log1p(x) and
+// 1 / (T + dT) = (1 / T) / (1 + x), both by their Taylor series through x^7 (truncation below
+// |x|^8 / 8, i.e. below 1e-20 of the result for |x| <= 2e-3); a full log and division above that.
+// Used for the Newton pass's finite difference (dT = 0.1, T >= 50 K) and for a pass's own T
+// when it lies within 0.2 % of the last full evaluation.
 __device__ __forceinline__ SatT sat_t_next(const SatT& s, double dT){
     const double x = dT * s.inv;
-    if(!(x <= 2.0e-3)) return sat_t(s.T + dT);
+    if(!(fabs(x) <= 2.0e-3)) return sat_t(s.T + dT);
     SatT r;
     r.T = s.T + dT;
     const double l1p = x * (1.0 + x * (-0.5 + x * (1.0 / 3.0 + x * (-0.25 + x * (0.2 + x * (-1.0 / 6.0 + x * (1.0 / 7.0)))))));
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                     // ---- :450-590, at most 15 passes ----
                     double q_v_b = c, q_c_b = cloud, q_i_b = ice;
                     double T = t_u, q_v_hyp = q_v_b;
+                    SatT st_full = st0;                 // the last full log / reciprocal (mixed form)
                     bool found = false, dry = false;
                     double q_rain_now = q_Rain_0;
                     for(int itr = 1; itr <= 15; itr++){
@@ -236,7 +238,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                             return (q_i_b == 0.0) ? 1 : 2;
                         };
                         SatT stT;
-                        if constexpr(FAST) stT = sat_t(T);
+                        if constexpr(FAST){
+                            const double dT0 = T - st_full.T;      // exact: T and st_full.T are close
+                            if(fabs(dT0) * st_full.inv <= 2.0e-3) stT = sat_t_next(st_full, dT0);
+                            else { stT = sat_t(T); st_full = stT; }
+                        }
                         const double q_Rain = qsat<FAST>(G, false, rho_c, ep, p_u, rep, T, stT);
                         const double q_Ice  = (need(T) & 2) ? qsat<FAST>(G, true, rho_c, ep, p_u, rep, T, stT) : 0.0;
                         q_rain_now = q_Rain;
