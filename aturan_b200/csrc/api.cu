@@ -438,14 +438,17 @@ int run_rb(aturan_ctx* ctx, int sweeps, double omega){
 // ---- RB_SOR: the shared solver's equation to a relative L2 residual (sor.cuh) ----
 
 // Residual of P against src: relative L2 norm (host sum of the block partials, fixed order).
-// TR: of the transposed operator.
+// TR: of the transposed operator. shift: apply the source's compatibility shift in this pass
+// (after sor_compat with apply = false).
 template <typename T, bool TR = false>
 int sor_residual(aturan_ctx* ctx, const T* P, const T* src, bool want_col, double* rel, double* abs_rr,
-                 bool fill32 = false){
+                 bool fill32 = false, const double* shift = nullptr){
     const Grid g = ctx->g;
+    double* src_w = nullptr;
+    if constexpr(std::is_same<T, double>::value) src_w = shift ? const_cast<double*>(src) : nullptr;
     sor_colsum_kernel<T, TR><<<dim3((g.km - 1 + 31) / 32, g.jm - 2), dim3(32, 8), 0, ctx->st>>>(
         g, P, src, ctx->rbw, ctx->sor_colR, ctx->sor_part, want_col ? 1 : 0,
-        fill32 ? ctx->r32 : nullptr, fill32 ? ctx->e32 : nullptr);
+        fill32 ? ctx->r32 : nullptr, fill32 ? ctx->e32 : nullptr, src_w, src_w ? shift : nullptr);
     CK_LAUNCH("residual");
     if(!rel) return ATURAN_OK;                                 // column sums only: no host round trip
     CK(cudaMemcpyAsync(ctx->host_part.data(), ctx->sor_part, 2 * ctx->sor_nblk * 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -532,23 +535,26 @@ inline int sor_correct_every(bool line){ return line ? 8 : 16; }
 
 // Remove src's component along the operator's left null vector (y_i y_j for Lc, the constant for
 // Lc^T) by a shift of the interior, all on the device.
-void sor_compat(aturan_ctx* ctx, double* src, bool transposed){
+const double* sor_compat(aturan_ctx* ctx, double* src, bool transposed, bool apply = true){
     const Grid& g = ctx->g;
     const int ny = ((g.jm - 2) * (g.km - 1) + 255) / 256;
+    // past the residual pass's block partials: the first residual reads it while writing those
+    double* shift = ctx->sor_part + 2 * ctx->sor_nblk;
     sor_ysum_kernel<<<ny, 256, 0, ctx->st>>>(g, src, ctx->sor_part, transposed ? 1 : 0);
-    sor_shift_finish_kernel<<<1, 256, 0, ctx->st>>>(ctx->sor_part, ny, ctx->sor_part + 2 * ny);
-    sor_shift_kernel<<<148 * 4, 256, 0, ctx->st>>>(g, src, ctx->sor_part + 2 * ny);
+    sor_shift_finish_kernel<<<1, 256, 0, ctx->st>>>(ctx->sor_part, ny, shift);
+    if(apply) sor_shift_kernel<<<148 * 4, 256, 0, ctx->st>>>(g, src, shift);
+    return shift;
 }
 
 // FP64 red-black solve of Lc P = src (TR: Lc^T P = src) on the interior from the given P, src
 // compatible. Returns ATURAN_OK at tol, ATURAN_NOT_CONVERGED at the cap; counts launches into nl.
 template <bool TR>
 int solve_fp64(aturan_ctx* ctx, double* P, const double* src, double omega, int max_sweeps, double tol, bool line,
-               int* sweeps_done, double* resid, long& nl){
+               int* sweeps_done, double* resid, long& nl, const double* shift = nullptr){
     const int check_every = sor_check_every(line), every = sor_correct_every(line);
     double r = 0.0;
     int s = 0;
-    int rc = sor_residual<double, TR>(ctx, P, src, true, &r, nullptr); if(rc) return rc; nl++;
+    int rc = sor_residual<double, TR>(ctx, P, src, true, &r, nullptr, false, shift); if(rc) return rc; nl++;
     while(s < max_sweeps && !(r <= tol)){
         if(s % every == 0){ rc = sor_correct<double, TR>(ctx, P); if(rc) return rc; nl += 4; }
         for(int n = 0; n < check_every && s < max_sweeps; n++, s++){ sor_sweep<double, TR>(ctx, P, src, omega, line); nl += 2; }
@@ -577,16 +583,17 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
         CK(cudaMemcpyAsync(ctx->tSrc, ctx->scratch, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
         ctx->tape_p_valid = true;
     }
-    sor_compat(ctx, ctx->scratch, false);
+    // the shift itself is applied by the first residual pass
+    const double* shift = sor_compat(ctx, ctx->scratch, false, false);
     CK_LAUNCH("SOR source");
-    nl += 6;
+    nl += 5;
     double* P = ctx->pdyn;
     const double* src = ctx->scratch;
     double r = 0.0;
     int s = 0;
     int status;
     if(!ctx->mixed){
-        status = solve_fp64<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl);
+        status = solve_fp64<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl, shift);
         if(status < 0) return status;
     } else {
         // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
@@ -596,7 +603,7 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
         const int inner = line ? 2 : 48;
         // Each FP64 residual also leaves r in FP32, e = 0 and the column sums of r: what the next
         // correction solve starts from (one pass over p and src per refinement step).
-        rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true); if(rc) return rc; nl++;
+        rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true, shift); if(rc) return rc; nl++;
         while(s < max_sweeps && !(r <= tol)){
             for(int n = 0; n < inner && s < max_sweeps; n++, s++){
                 // the correction on the same cadence as the FP64 solve (once per `every` sweeps,

@@ -110,16 +110,20 @@ __device__ __forceinline__ double row_acc(const Grid& g, const T* P, size_t o, i
 // e = 0 on the interior for the mixed form's correction solve), and per-block partial sums of r^2 and src^2. A block is 32 meridians x 8 level
 // groups; the groups' column sums are added in group order and the block's norms in a fixed tree
 // order, so the result is deterministic. P and src of type T (double: FP64 solve; float: the
-// correction solve of the mixed form).
+// correction solve of the mixed form). Given shift (the source's compatibility shift, FP64 only),
+// the pass first applies src -= shift to each interior cell it reads and writes the shifted value
+// back through src_w (the same array): sor_shift_kernel's work, folded into the solve's first pass.
 template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, const T* src, const RBW* w,
                                                          double* colR, double* part, int want_col,
-                                                         float* r32 = nullptr, float* e32 = nullptr){
+                                                         float* r32 = nullptr, float* e32 = nullptr,
+                                                         double* src_w = nullptr, const double* shift = nullptr){
     const int N = g.km - 1;
     const int k = blockIdx.x * 32 + threadIdx.x;
     const int j = 1 + blockIdx.y;
     const int grp = threadIdx.y;
     double R = 0.0, rr = 0.0, ss = 0.0;
+    const double sh = shift ? *shift : 0.0;
     if(k < N){
 #pragma unroll 5
         for(int i = 1 + grp; i < g.im - 1; i += 8){
@@ -127,7 +131,9 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
             double diag;
             const double acc = row_acc<TR, T>(g, P, o, i, j, k, w, &diag);
             const double lc = acc - diag * (double)__ldg(P + o);
-            const double s = (double)__ldg(src + o);
+            double s;
+            if(shift){ s = (double)src[o] - sh; src_w[o] = s; }      // the same subtraction as sor_shift_kernel
+            else s = (double)__ldg(src + o);
             const double r = s - lc;
             if(r32){ r32[o] = (float)r; e32[o] = 0.0f; }  // the mixed form's next correction solve
             R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
