@@ -488,8 +488,9 @@ int sor_correct(aturan_ctx* ctx, T* P){
 }
 
 // Dynamic shared memory of sor_line_kernel: the right-hand sides of LINE_COLS columns and the
-// row's three factor arrays, per level.
-inline size_t line_smem(const Grid& g){ return (size_t)(g.im - 2) * (LINE_COLS + 3) * sizeof(double); }
+// row's three factor arrays, per level, in the kernel's arithmetic type.
+template <typename T>
+inline size_t line_smem(const Grid& g){ return (size_t)(g.im - 2) * (LINE_COLS + 3) * sizeof(typename LineArith<T>::A); }
 
 // Allow sor_line_kernel above the default 48 KB of dynamic shared memory (once per instance).
 template <typename T, bool TR>
@@ -504,10 +505,10 @@ bool line_smem_attr(){
 template <typename T, bool TR = false>
 void sor_sweep(aturan_ctx* ctx, T* E, const T* R, double omega, bool line){
     const Grid g = ctx->g;
-    if(line && line_smem(g) > 48 * 1024) line_smem_attr<T, TR>();
+    if(line && line_smem<T>(g) > 48 * 1024) line_smem_attr<T, TR>();
     for(int colour = 0; colour < 2; colour++){
         if(line)
-            sor_line_kernel<T, TR><<<dim3((g.km / 2 + LINE_COLS - 1) / LINE_COLS, g.jm - 2), 256, line_smem(g), ctx->st>>>(
+            sor_line_kernel<T, TR><<<dim3((g.km / 2 + LINE_COLS - 1) / LINE_COLS, g.jm - 2), 256, line_smem<T>(g), ctx->st>>>(
                 g, E, R, ctx->rbw, TR ? ctx->lluT_a : ctx->llu_a, TR ? ctx->lluT_cf : ctx->llu_cf,
                 TR ? ctx->lluT_idn : ctx->llu_idn, colour, omega);
         else
@@ -521,7 +522,7 @@ int sor_check_sizes(aturan_ctx* ctx, double omega, bool line){
     if(!(omega > 0.0 && omega < 2.0)) return fail(ctx, ATURAN_E_INVALID, "omega must lie in (0, 2)");
     if(8 * ctx->sorc.J * (5 * ctx->sor_pm + 4) > 227 * 1024)
         return fail(ctx, ATURAN_E_UNSUPPORTED, "the column correction needs jm <= 2900");
-    if(line && line_smem(g) > 227 * 1024)
+    if(line && line_smem<double>(g) > 227 * 1024)
         return fail(ctx, ATURAN_E_UNSUPPORTED, "line relaxation needs im <= 435");
     return ATURAN_OK;
 }

@@ -358,22 +358,31 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
 // relaxed columns back. Shared memory: (im - 2) * (LINE_COLS + 3) doubles. With 64 columns the
 // default grid's 537 blocks are resident at once (one wave).
 constexpr int LINE_COLS = 64;
+// Arithmetic of the right-hand sides and recurrences: FP64 for the FP64 solve; FP32 for the
+// mixed form's FP32 correction solves (an FP64 recurrence step is ~4x the latency of an FP32 one
+// on this path's dependent chain, and the FP64 refinement around the correction solve fixes the
+// accuracy). LV: levels per warp per pass of phases 1 and 3, whose loads all come first; sized so
+// that 4 blocks of 256 threads (64 registers) stay resident without spills.
+template <typename T> struct LineArith { using A = double; static constexpr int LV = 3; };
+template <> struct LineArith<float> { using A = float; static constexpr int LV = 5; };
+
 template <typename T, bool TR = false>
-__global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
+__global__ void __launch_bounds__(256, 4) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
                                                        const double* lcf, const double* lidn, int colour, double omega){
-    extern __shared__ double ds[];
+    using A = typename LineArith<T>::A;
+    constexpr int LINE_LV = LineArith<T>::LV;
+    extern __shared__ __align__(16) unsigned char line_raw[];
+    A* ds = reinterpret_cast<A*>(line_raw);
     const int n = g.im - 2;
-    double* fa = ds + (size_t)n * LINE_COLS;           // the row's factors by level
-    double* fc = fa + n;
-    double* fi = fc + n;
+    A* fa = ds + (size_t)n * LINE_COLS;                // the row's factors by level
+    A* fc = fa + n;
+    A* fi = fc + n;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const int j = 1 + blockIdx.y;
     const size_t sj = g.kp;
-    // phase 1 reads only the other colour's cells, which this launch does not write: read-only path
-    auto p = [&](size_t q){ return (double)__ldg(P + q); };
     for(int i = threadIdx.x; i < n; i += blockDim.x){
         const size_t f = (size_t)(i + 1) * g.jm + j;
-        fa[i] = la[f]; fc[i] = lcf[f]; fi[i] = lidn[f];
+        fa[i] = (A)la[f]; fc[i] = (A)lcf[f]; fi[i] = (A)lidn[f];
     }
     int kk[2]; bool valid[2];
 #pragma unroll
@@ -382,48 +391,73 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
         kk[h] = 2 * k2 + ((j + colour) & 1);
         valid[h] = k2 < g.km / 2 && kk[h] <= g.km - 2;
     }
-#pragma unroll 5
-    for(int i = 1 + wp; i <= n; i += 8){
-        const RBW4 W = ldw(w + i * g.jm + j);
+    // phase 1: right-hand sides. It reads only the other colour's cells, which this launch does not
+    // write (read-only path); per pass, every load of the warp's LINE_LV levels comes first.
+    for(int i0 = 1 + wp; i0 <= n; i0 += 8 * LINE_LV){
 #pragma unroll
         for(int h = 0; h < 2; h++){
-            double d = 0.0;
-            if(valid[h]){
-                const int k = kk[h];
-                const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
-                const size_t o = gidx(g, i, j, k);
-                double hsum;
-                if constexpr(TR){                      // the transposed theta couplings (folded_accT)
-                    hsum = (p(o - k + ke) + p(o - k + kw)) * W.num3;
-                    if(j - 1 >= 1)        hsum += __ldg(&w[i * g.jm + j - 1].num2) * (j - 1 == 1 ? 1.0 - C13 : 1.0) * p(o - sj);
-                    if(j + 1 <= g.jm - 2) hsum += __ldg(&w[i * g.jm + j + 1].num2) * (j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * p(o + sj);
-                } else {
-                    const double ajm = (j == 1)        ? -C13 * p(o + sj) : p(o - sj);
-                    const double ajp = (j == g.jm - 2) ? -C13 * p(o - sj) : p(o + sj);
-                    hsum = (ajp + ajm) * W.num2 + (p(o - k + ke) + p(o - k + kw)) * W.num3;
+            T vjm[LINE_LV], vjp[LINE_LV], vke[LINE_LV], vkw[LINE_LV], vr[LINE_LV];
+            double n2[LINE_LV], n3[LINE_LV], n2m[LINE_LV], n2p[LINE_LV];
+            const int k = kk[h];
+            const int kw = phi_wrap(k - 1, g.km), ke = phi_wrap(k + 1, g.km);
+#pragma unroll
+            for(int q = 0; q < LINE_LV; q++){
+                const int i = i0 + 8 * q;
+                if(i <= n && valid[h]){
+                    const size_t o = gidx(g, i, j, k);
+                    vjm[q] = __ldg(P + (o - sj)); vjp[q] = __ldg(P + (o + sj));
+                    vke[q] = __ldg(P + (o - k + ke)); vkw[q] = __ldg(P + (o - k + kw));
+                    vr[q] = __ldg(R + o);
+                    n2[q] = __ldg(&w[i * g.jm + j].num2); n3[q] = __ldg(&w[i * g.jm + j].num3);
+                    if constexpr(TR){
+                        n2m[q] = (j - 1 >= 1) ? __ldg(&w[i * g.jm + j - 1].num2) : 0.0;
+                        n2p[q] = (j + 1 <= g.jm - 2) ? __ldg(&w[i * g.jm + j + 1].num2) : 0.0;
+                    }
                 }
-                d = hsum - (double)__ldg(R + o);
             }
-            ds[(i - 1) * LINE_COLS + h * 32 + lane] = d;
+#pragma unroll
+            for(int q = 0; q < LINE_LV; q++){
+                const int i = i0 + 8 * q;
+                if(i > n) break;
+                A d = A(0);
+                if(valid[h]){
+                    // at j = 1 and jm - 2 one theta neighbour is the boundary row, which lies in the
+                    // row itself through the theta fold: the other row (o + sj or o - sj) enters
+                    const A pjm = (A)vjm[q], pjp = (A)vjp[q];
+                    A hsum;
+                    if constexpr(TR){                  // the transposed theta couplings (folded_accT)
+                        hsum = ((A)vke[q] + (A)vkw[q]) * (A)n3[q];
+                        if(j - 1 >= 1)        hsum += (A)n2m[q] * (A)(j - 1 == 1 ? 1.0 - C13 : 1.0) * pjm;
+                        if(j + 1 <= g.jm - 2) hsum += (A)n2p[q] * (A)(j + 1 == g.jm - 2 ? 1.0 - C13 : 1.0) * pjp;
+                    } else {
+                        const A ajm = (j == 1)        ? (A)(-C13) * pjp : pjm;
+                        const A ajp = (j == g.jm - 2) ? (A)(-C13) * pjm : pjp;
+                        hsum = (ajp + ajm) * (A)n2[q] + ((A)vke[q] + (A)vkw[q]) * (A)n3[q];
+                    }
+                    d = hsum - (A)vr[q];
+                }
+                ds[(i - 1) * LINE_COLS + h * 32 + lane] = d;
+            }
         }
     }
     __syncthreads();
+    // phase 2: the host-factored Thomas recurrences, two independent chains per lane
     if(wp == 0){
-        double* c0 = ds + lane;
-        double* c1 = ds + 32 + lane;
-        double y0 = 0.0, y1 = 0.0;
+        A* c0 = ds + lane;
+        A* c1 = ds + 32 + lane;
+        A y0 = A(0), y1 = A(0);
 #pragma unroll 4
         for(int i = 0; i < n; i++){
-            const double a_ = fa[i], r_ = fi[i];
+            const A a_ = fa[i], r_ = fi[i];
             y0 = (c0[i * LINE_COLS] - a_ * y0) * r_;
             y1 = (c1[i * LINE_COLS] - a_ * y1) * r_;
             c0[i * LINE_COLS] = y0;
             c1[i * LINE_COLS] = y1;
         }
-        double x0 = c0[(n - 1) * LINE_COLS], x1 = c1[(n - 1) * LINE_COLS];
+        A x0 = c0[(n - 1) * LINE_COLS], x1 = c1[(n - 1) * LINE_COLS];
 #pragma unroll 4
         for(int i = n - 2; i >= 0; i--){
-            const double c_ = fc[i];
+            const A c_ = fc[i];
             x0 = c0[i * LINE_COLS] - c_ * x0;
             x1 = c1[i * LINE_COLS] - c_ * x1;
             c0[i * LINE_COLS] = x0;
@@ -431,14 +465,23 @@ __global__ void __launch_bounds__(256) sor_line_kernel(Grid g, T* P, const T* R,
         }
     }
     __syncthreads();
+    // phase 3: over-relax the columns in place, loads first
 #pragma unroll
     for(int h = 0; h < 2; h++){
-        if(valid[h]){
-#pragma unroll 5
-            for(int i = 1 + wp; i <= n; i += 8){
-                const size_t o = gidx(g, i, j, kk[h]);
-                const double p0 = (double)P[o];
-                P[o] = (T)(p0 + omega * (ds[(i - 1) * LINE_COLS + h * 32 + lane] - p0));
+        if(!valid[h]) continue;
+        for(int i0 = 1 + wp; i0 <= n; i0 += 8 * LINE_LV){
+            T pv[LINE_LV];
+#pragma unroll
+            for(int q = 0; q < LINE_LV; q++){
+                const int i = i0 + 8 * q;
+                if(i <= n) pv[q] = P[gidx(g, i, j, kk[h])];
+            }
+#pragma unroll
+            for(int q = 0; q < LINE_LV; q++){
+                const int i = i0 + 8 * q;
+                if(i > n) break;
+                const double p0 = (double)pv[q];
+                P[gidx(g, i, j, kk[h])] = (T)(p0 + omega * ((double)ds[(i - 1) * LINE_COLS + h * 32 + lane] - p0));
             }
         }
     }
