@@ -368,3 +368,33 @@ def test_step_side_by_side_equals_in_order(synth, precision):
     b.close()
     for n in names:
         assert np.array_equal(ga[n], gb[n]), n
+
+
+def test_grid_beyond_32bit_offsets_is_refused():
+    """The stage kernels address the context's allocation by 32-bit element offsets; a grid whose
+    context would exceed 2^31 elements is refused at creation, before any device allocation."""
+    from aturan_b200.api import AturanError, E_UNSUPPORTED
+    p = P.default_params(512, 2048, 2049)
+    with pytest.raises(AturanError) as e:
+        ctx_for(p)
+    assert e.value.code == E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("precision,shape", [(P.FP64, (100, 11, 17)), (P.MIXED, (190, 9, 17))])
+def test_line_deep_columns_match_oracle(oracle_lib, precision, shape):
+    """Columns deep enough that the line kernel's shared memory passes 48 KB (the opt-in path):
+    the solve still reaches the oracle's solution (FP64 solve, and FP32 sweeps in FP64 refinement)."""
+    p, st = sor_case(shape=shape, seed=35)
+    p.precision = precision
+    ctx = ctx_for(p)
+    ctx.upload_state(st)
+    rc, its, res = ctx.pressure(P.PRESS_RB_LINE, omega=1.0, max_sweeps=400, tol=1e-8)
+    g = ctx.download("p_dyn")
+    ctx.close()
+    st2 = S.copy_state(st)
+    rc2, its2, res2 = oracle_lib.pressure_line(p, st2, 1.0, 400, 1e-8)
+    assert rc == 0 and rc2 == 0 and res <= 1e-8
+    I = interior_of(p)
+    a = g[I] - g[I].mean()
+    b = st2["p_dyn"][I] - st2["p_dyn"][I].mean()
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
