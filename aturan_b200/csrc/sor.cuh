@@ -358,13 +358,13 @@ __global__ void __launch_bounds__(256) sor_colour_kernel(Grid g, T* E, const T* 
 // relaxed columns back. Shared memory: (im - 2) * (LINE_COLS + 3) doubles. With 64 columns the
 // default grid's 537 blocks are resident at once (one wave).
 constexpr int LINE_COLS = 64;
-// Arithmetic of the right-hand sides and recurrences: FP64 for the FP64 solve; FP32 for the
-// mixed form's FP32 correction solves (an FP64 recurrence step is ~4x the latency of an FP32 one
-// on this path's dependent chain, and the FP64 refinement around the correction solve fixes the
-// accuracy). LV: levels per warp per pass of phases 1 and 3, whose loads all come first; sized so
-// that 4 blocks of 256 threads (64 registers) stay resident without spills.
+// Arithmetic of the right-hand sides and recurrences: FP64 for both the FP64 solve and the mixed
+// form's FP32 correction solves (FP32 recurrences were no faster per solve and took more sweeps in
+// the first steps: the column tridiagonals are strongly anisotropic). LV: levels per warp per pass
+// of phases 1 and 3, whose loads all come first; sized so that 4 blocks of 256 threads (64
+// registers) stay resident without spills.
 template <typename T> struct LineArith { using A = double; static constexpr int LV = 3; };
-template <> struct LineArith<float> { using A = float; static constexpr int LV = 5; };
+template <> struct LineArith<float> { using A = double; static constexpr int LV = 5; };
 
 template <typename T, bool TR = false>
 __global__ void __launch_bounds__(256, 4) sor_line_kernel(Grid g, T* P, const T* R, const RBW* w, const double* la,
