@@ -52,6 +52,7 @@ struct aturan_ctx {
     double* stage64;           // one padded FP64 field, for conversions
     double* ref_level;         // im
     double *part_sum, *part_w; // im * nblk
+    BuoyScratch bx;            // the exact level means' scratch (FP64 context with exact_reductions)
     int nblk;
     double *wsin, *rm_i, *cor_j, *cp_tab64;
     void* geo;                 // GeoIJ<C>[im*jm]
@@ -293,7 +294,7 @@ int rk4_prelude(aturan_ctx* ctx, cudaStream_t st){
     const int exact = ctx->mixed ? 0 : ctx->p.exact_reductions;   // the mixed form always sums in tree order
     Region reg(ctx, ATURAN_K_HYDRO, exact ? 2 : 3, st);
     launch_buoy(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), ctx->wsin, ctx->hc,
-                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, st);
+                ctx->part_sum, ctx->part_w, ctx->nblk, ctx->ref_level, exact, ctx->bx, st);
     CK_LAUNCH("buoyancy reference level");
     launch_hydro(g, grp<S>(state, ATURAN_T, fs), reinterpret_cast<const S*>(ctx->pstat), grp<S>(state, ATURAN_V, fs),
                  grp<S>(state, ATURAN_W, fs), ctx->ref_level, ctx->rm_i, ctx->cor_j, ctx->pbaro, ctx->pb0, ctx->pbf,
@@ -709,6 +710,12 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     add(22 * fs * e); add(6 * fs * e); add(fs * e);
     for(int n = 0; n < 7; n++) add(fs * 8);                   // pdyn phydro pbaro pb0 pbf scratch stage64
     add(g.im * 8); add(2 * (size_t)g.im * ctx->nblk * 8);
+    // the exact level means (FP64 with exact_reductions): terms, chunk sums, binades, units
+    const bool bx_on = !ctx->mixed && p->exact_reductions;
+    const size_t ncell = (size_t)g.jm * g.km;
+    ctx->bx.nbx = (int)((ncell + BX_CH - 1) / BX_CH);
+    const size_t nbx_all = (size_t)g.im * ctx->bx.nbx;
+    if(bx_on){ add(2 * g.im * ncell * 8); add(3 * nbx_all * 8); add(2 * nbx_all * 4); add(4 * nbx_all * 8); }
     add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
@@ -760,6 +767,12 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->ref_level = carve<double>(cur, g.im);
     ctx->part_sum = carve<double>(cur, 2 * (size_t)g.im * ctx->nblk);
     ctx->part_w = ctx->part_sum + (size_t)g.im * ctx->nblk;
+    if(bx_on){
+        ctx->bx.terms = carve<double>(cur, 2 * g.im * ncell);
+        ctx->bx.bpart = carve<double>(cur, 3 * nbx_all);
+        ctx->bx.bexp = carve<int>(cur, 2 * nbx_all);
+        ctx->bx.bunits = carve<long long>(cur, 4 * nbx_all);
+    }
     ctx->wsin = carve<double>(cur, g.jm); ctx->rm_i = carve<double>(cur, g.im); ctx->cor_j = carve<double>(cur, g.jm);
     ctx->cp_tab64 = carve<double>(cur, CP_TABLE_N);
     ctx->geo = carve<char>(cur, nij * sgeo);

@@ -73,6 +73,16 @@ struct HydroConst {
     int follow_on;
 };
 
+// Scratch of the exact (reference-order) level means: the terms, per-chunk sums and flags, and the
+// per-chunk binades and units (rk4.cuh, buoy_terms_kernel to buoy_serial_pass_kernel).
+struct BuoyScratch {
+    double* terms;          // [im][2][jm*km]
+    double* bpart;          // [im][nbx][3]
+    int* bexp;              // [im][nbx][2]
+    long long* bunits;      // [im][nbx][4]
+    int nbx;                // chunks per level
+};
+
 constexpr int CP_TABLE_N = 2991;   // (1500 - 5) / 0.5 + 1, CpH2.h:66-75
 
 }  // namespace aturan

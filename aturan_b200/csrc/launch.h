@@ -13,7 +13,7 @@ struct GSW; struct RBW; struct PressConst;
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
 void launch_stage(const StageArgs<S, C>& a, cudaStream_t st);                                              \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
-                 double* part_w, int nblk, double* ref, int exact, cudaStream_t st);                       \
+                 double* part_w, int nblk, double* ref, int exact, const BuoyScratch& bx, cudaStream_t st);                       \
 void launch_hydro(Grid g, const S* t, const S* ps, const S* v, const S* w, const double* ref,              \
                   const double* rm_i, const double* cor_j, const double* pbaro, const double* pb0,         \
                   double* pbf, double* ph, HydroConst h, int advance, cudaStream_t st);                    \

@@ -57,8 +57,14 @@ void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                   
     launch_scalars(a, grid2, st);                                                                         \
 }                                                                                                         \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
-                 double* part_w, int nblk, double* ref, int exact, cudaStream_t st){                       \
-    if(exact){ buoy_serial_kernel<S><<<g.im, 256, 0, st>>>(g, t, ps, wsin, h, ref); return; } \
+                 double* part_w, int nblk, double* ref, int exact, const BuoyScratch& bx, cudaStream_t st){ \
+    if(exact){                                                                                            \
+        buoy_terms_kernel<S><<<dim3(bx.nbx, g.im), BX_CH, 0, st>>>(g, t, ps, wsin, h, bx.terms, bx.bpart, bx.nbx); \
+        buoy_predict_kernel<<<g.im, 256, 0, st>>>(bx.nbx, bx.bpart, bx.bexp);                               \
+        buoy_units_kernel<<<dim3(bx.nbx, g.im), BX_CH, 0, st>>>(g, bx.nbx, bx.terms, bx.bexp, bx.bunits);  \
+        buoy_serial_pass_kernel<<<g.im, 32, 0, st>>>(g, bx.nbx, bx.terms, bx.bexp, bx.bunits, ref);         \
+        return;                                                                                           \
+    }                                                                                                     \
     buoy_partial_kernel<S><<<dim3(nblk, g.im), 256, 0, st>>>(g, t, ps, wsin, h, part_sum, part_w, nblk); \
     buoy_finish_kernel<<<(g.im + 63) / 64, 64, 0, st>>>(g.im, nblk, part_sum, part_w, ref);               \
 }                                                                                                         \

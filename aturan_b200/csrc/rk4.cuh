@@ -18,6 +18,7 @@
 // FP64 instantiation is compiled without FMA contraction and keeps the reference's operand order
 // in every expression, so it reproduces the CPU's IEEE results.
 #pragma once
+#include <climits>
 #include "common.cuh"
 
 namespace aturan {
@@ -692,59 +693,236 @@ static __global__ void buoy_finish_kernel(int im, int nblk, const double* part_s
     ref[lev] = (w > 0.0) ? s / w : 0.0;
 }
 
-// Exact form: the reference's serial j-then-k order, bit-equal to the reference. A floating-point
-// running sum cannot be reassociated, so its dependent add chain (two adds per valid cell) is the
-// floor; everything else is taken off it. One block per level: warps 1..7 load t and p_stat
-// (coalesced along k), form w b and the validity of a chunk of 224 consecutive cells into shared
-// memory while lane 0 of warp 0 adds the previous chunk in order (double buffer, one barrier per
-// chunk).
+// Exact form: the reference's serial j-then-k running sums, bit-equal to the reference, computed
+// in parallel. The terms are w b >= 0 (w the sin(theta) weight, 0 for a skipped cell), so the
+// running sum s never decreases. While s stays in one binade [2^e, 2^(e+1)) every representable
+// value there is an integer multiple of u = 2^(e-52), and fl(s + x) = s + u round(x / u) with
+// ties to the even multiple -- integer arithmetic, exact, in which only the ties depend on s (on
+// the parity of s / u). So a chunk of BX_CH terms whose running sum provably stays in one binade
+// acts on s as "add I_p units", p the parity of s / u at the chunk's start, and the chunk's two
+// integers I_0, I_1 can be formed independently of every other chunk.
+//   pass 1 (buoy_terms_kernel, one block per chunk): the terms, into a scratch array, and each
+//     chunk's sum in any order (an approximate prefix is all pass 2 needs of them);
+//   pass 2 (buoy_predict_kernel, one block per level): the approximate prefix of the chunk sums
+//     predicts the binade each chunk's running sum stays in, if one;
+//   pass 3 (buoy_units_kernel, one block per chunk): (I_0, I_1) of every predicted chunk, by an
+//     ordered tree over its terms' own actions;
+//   pass 4 (buoy_serial_pass_kernel, one warp per level): the chunks in order, each applied in O(1)
+//     when s lies in the predicted binade and the result stays below its top, and term by term
+//     otherwise (the first chunks, where s is small, and the ~9 where s crosses a power of two).
+// Every O(1) step is checked exactly, so the prediction only decides speed. A level with a
+// negative term (not monotone) runs all its chunks term by term.
+// Both sums (w b and w) go this way; the mean is s / w as in the reference.
+constexpr int BX_CH = 256;
+
 template <typename S>
-__global__ void __launch_bounds__(256) buoy_serial_kernel(Grid g, const S* t, const S* ps, const double* wsin,
-                                                          HydroConst h, double* ref){
-    constexpr int CH = 224;                              // producers: threads 32..255
-    __shared__ double sb[2][CH], sw[2][CH];
-    const int lev = blockIdx.x;
+__global__ void __launch_bounds__(BX_CH) buoy_terms_kernel(Grid g, const S* t, const S* ps, const double* wsin,
+                                                          HydroConst h, double* terms, double* bpart, int nbx){
+    const int lev = blockIdx.y;
     const int ncell = g.jm * g.km;
-    const int nchunk = (ncell + CH - 1) / CH;
-    double s = 0.0, w = 0.0;
-    auto produce = [&](int chunk, int buf){
-        const int q = threadIdx.x - 32;
-        const int c = chunk * CH + q;
-        double bv = 0.0, wv = 0.0;                       // wv = 0 marks a skipped cell
-        if(c < ncell){
-            const int j = c / g.km, k = c - j * g.km;
-            const size_t o = gidx(g, lev, j, k);
-            const double T = (double)__ldg(t + o);
-            if(T > 0.0){
-                const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
-                if(isfinite(b)){ const double wg = wsin[j]; bv = wg * b; wv = wg; }
-            }
+    const int c = blockIdx.x * BX_CH + threadIdx.x;
+    double bv = 0.0, wv = 0.0;                         // wv = 0 marks a skipped cell
+    if(c < ncell){
+        const int j = c / g.km, k = c - j * g.km;
+        const size_t o = gidx(g, lev, j, k);
+        const double T = (double)__ldg(t + o);
+        if(T > 0.0){
+            const double b = h.g * (double)__ldg(ps + o) / (h.rR * T * h.t_ref);
+            if(isfinite(b)){ const double wg = wsin[j]; bv = wg * b; wv = wg; }
         }
-        sb[buf][q] = bv; sw[buf][q] = wv;
-    };
-    if(threadIdx.x >= 32) produce(0, 0);
+        double* xb = terms + (size_t)lev * 2 * ncell;
+        xb[c] = bv; xb[ncell + c] = wv;
+    }
+    __shared__ double sb[BX_CH], sw[BX_CH];
+    __shared__ int neg;
+    if(threadIdx.x == 0) neg = 0;
+    sb[threadIdx.x] = bv; sw[threadIdx.x] = wv;
     __syncthreads();
-    for(int chunk = 0; chunk < nchunk; chunk++){
-        const int buf = chunk & 1;
-        if(threadIdx.x >= 32){
-            if(chunk + 1 < nchunk) produce(chunk + 1, buf ^ 1);
-        } else if(threadIdx.x == 0){
-            // Skipped cells hold +0.0 in both arrays, and adding +0.0 leaves a sum of
-            // non-negative terms unchanged, so the chain can run without a branch; unrolled so
-            // the shared-memory loads run ahead of the two dependent add chains.
-            const int n = min(CH, ncell - chunk * CH);
-            const double* pb = sb[buf];
-            const double* pw = sw[buf];
-            if(n == CH){
-#pragma unroll 32
-                for(int q = 0; q < CH; q++){ s += pb[q]; w += pw[q]; }
-            } else {
-                for(int q = 0; q < n; q++){ s += pb[q]; w += pw[q]; }
-            }
+    if(bv < 0.0) neg = 1;
+    for(int st = BX_CH / 2; st > 0; st >>= 1){
+        if(threadIdx.x < st){ sb[threadIdx.x] += sb[threadIdx.x + st]; sw[threadIdx.x] += sw[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0){
+        double* q = bpart + 3 * ((size_t)lev * nbx + blockIdx.x);
+        q[0] = sb[0]; q[1] = sw[0]; q[2] = neg ? 1.0 : 0.0;
+    }
+}
+
+// pass 2: the approximate prefix of the chunk sums (a block scan over tiles of 256 chunks) and the
+// predicted binade of each chunk's running sum (INT_MIN: not predicted to stay in one binade, or
+// the level has a negative term), one block per level.
+static __global__ void __launch_bounds__(256) buoy_predict_kernel(int nbx, const double* bpart, int* bexp){
+    const int lev = blockIdx.x;
+    const double* bp = bpart + 3 * (size_t)lev * nbx;
+    int* E = bexp + 2 * (size_t)lev * nbx;
+    __shared__ double scb[256], scw[256];
+    __shared__ int negl;
+    if(threadIdx.x == 0) negl = 0;
+    __syncthreads();
+    for(int b = threadIdx.x; b < nbx; b += 256) if(bp[3 * b + 2] != 0.0) negl = 1;
+    __syncthreads();
+    double carry_b = 0.0, carry_w = 0.0;
+    for(int b0 = 0; b0 < nbx; b0 += 256){
+        const int b = b0 + threadIdx.x;
+        const double vb = (b < nbx) ? bp[3 * b] : 0.0, vw = (b < nbx) ? bp[3 * b + 1] : 0.0;
+        scb[threadIdx.x] = vb; scw[threadIdx.x] = vw;
+        __syncthreads();
+        for(int off = 1; off < 256; off <<= 1){
+            const double tb = threadIdx.x >= off ? scb[threadIdx.x - off] : 0.0;
+            const double tw = threadIdx.x >= off ? scw[threadIdx.x - off] : 0.0;
+            __syncthreads();
+            scb[threadIdx.x] += tb; scw[threadIdx.x] += tw;
+            __syncthreads();
+        }
+        if(b < nbx){
+            const double pb_end = carry_b + scb[threadIdx.x], pw_end = carry_w + scw[threadIdx.x];
+            const double eb_lo = (pb_end - vb) * (1.0 - 1e-9), eb_hi = pb_end * (1.0 + 1e-9);
+            const double ew_lo = (pw_end - vw) * (1.0 - 1e-9), ew_hi = pw_end * (1.0 + 1e-9);
+            // binades whose unit and scale are normal powers of two: -970 <= e <= 1000
+            auto pred = [&](double lo, double hi) -> int {
+                if(negl || !(lo > 0.0)) return INT_MIN;
+                const int e = ilogb(lo);
+                return (e == ilogb(hi) && e >= -970 && e <= 1000) ? e : INT_MIN;
+            };
+            E[2 * b] = pred(eb_lo, eb_hi); E[2 * b + 1] = pred(ew_lo, ew_hi);
+        }
+        carry_b += scb[255]; carry_w += scw[255];
+        __syncthreads();
+    }
+}
+
+// 2^n as a double for normal n (-1022 <= n <= 1023): the exponent field alone; x * pow2(n) is then
+// exact for x and the product normal.
+__device__ __forceinline__ double pow2(int n){ return __longlong_as_double((long long)(1023 + n) << 52); }
+
+// A term's action on the units of a running sum in binade e, for an even (r.x) and odd (r.y)
+// parity of s / u at the term: round(x / u) with ties to the even total.
+__device__ __forceinline__ longlong2 term_units(double x, int e){
+    const double q = x * pow2(52 - e);                 // exact: a power-of-two scaling, q < 2^53
+    const double m = floor(q);
+    const double f = q - m;                            // exact
+    const long long mi = (long long)m;
+    longlong2 r;
+    if(f < 0.5)      { r.x = r.y = mi; }
+    else if(f > 0.5) { r.x = r.y = mi + 1; }
+    else             { r.x = mi + (mi & 1); r.y = mi + ((1 + mi) & 1); }      // the tie: to even
+    return r;
+}
+// A then B, as actions on (parity -> units): C(p) = A(p) + B((p + A(p)) mod 2).
+__device__ __forceinline__ longlong2 units_then(longlong2 A, longlong2 B){
+    longlong2 C;
+    C.x = A.x + ((A.x & 1) ? B.y : B.x);
+    C.y = A.y + (((1 + A.y) & 1) ? B.y : B.x);
+    return C;
+}
+
+// pass 3: each chunk's action (units for an even and an odd start) in its predicted binade, by an
+// ordered tree over its terms, one block per chunk; the same for the weights.
+static __global__ void __launch_bounds__(BX_CH) buoy_units_kernel(Grid g, int nbx, const double* terms, const int* bexp,
+                                                                  long long* bunits){
+    const int lev = blockIdx.y, b = blockIdx.x;
+    const int ncell = g.jm * g.km;
+    const int c = b * BX_CH + threadIdx.x;
+    const int* E = bexp + 2 * ((size_t)lev * nbx + b);
+    const double* xb = terms + (size_t)lev * 2 * ncell;
+    __shared__ longlong2 ub[BX_CH], uw[BX_CH];
+    const int eb = E[0], ew = E[1];
+    const longlong2 zero = make_longlong2(0, 0);
+    ub[threadIdx.x] = (eb != INT_MIN && c < ncell) ? term_units(xb[c], eb) : zero;
+    uw[threadIdx.x] = (ew != INT_MIN && c < ncell) ? term_units(xb[ncell + c], ew) : zero;
+    __syncthreads();
+    for(int st = 1; st < BX_CH; st <<= 1){               // ordered: (t, t + st) into t
+        if((threadIdx.x & (2 * st - 1)) == 0){
+            ub[threadIdx.x] = units_then(ub[threadIdx.x], ub[threadIdx.x + st]);
+            uw[threadIdx.x] = units_then(uw[threadIdx.x], uw[threadIdx.x + st]);
         }
         __syncthreads();
     }
-    if(threadIdx.x == 0) ref[lev] = (w > 0.0) ? s / w : 0.0;
+    if(threadIdx.x == 0){
+        long long* U = bunits + 4 * ((size_t)lev * nbx + b);
+        U[0] = ub[0].x; U[1] = ub[0].y; U[2] = uw[0].x; U[3] = uw[0].y;
+    }
+}
+
+// pass 4: the chunks in order, one warp per level. Lane 0 applies a chunk in O(1) when s lies in
+// its predicted binade and the result stays below the binade's top; otherwise the warp stages the
+// chunk's terms in shared memory and lane 0 adds them one by one. Between O(1) chunks of one binade
+// the running sum stays an integer count of units (si), so the dependent chain is one integer add.
+struct RunSum {
+    double s;        // the running sum, when !in_units
+    long long si;    // s / 2^(e-52), when in_units
+    int e;
+    bool in_units;
+};
+__device__ __forceinline__ void run_to_double(RunSum& r){
+    if(r.in_units){ r.s = (double)r.si * pow2(r.e - 52); r.in_units = false; }    // exact
+}
+__device__ __forceinline__ bool chunk_fast(RunSum& r, int e, const long long* I){
+    if(e == INT_MIN){ run_to_double(r); return false; }
+    if(!(r.in_units && r.e == e)){
+        run_to_double(r);
+        const double lo = pow2(e);
+        if(!(r.s >= lo && r.s < 2.0 * lo)) return false;
+        r.si = (long long)(r.s * pow2(52 - e));        // exact integer
+        r.e = e;
+        r.in_units = true;
+    }
+    const long long ni = r.si + I[r.si & 1];
+    if(ni >= (1LL << 53)){ run_to_double(r); return false; }
+    r.si = ni;
+    return true;
+}
+
+static __global__ void __launch_bounds__(32) buoy_serial_pass_kernel(Grid g, int nbx, const double* terms, const int* bexp,
+                                                                     const long long* bunits, double* ref){
+    constexpr int TILE = 256;                          // chunks whose binades and units are staged at once
+    const int lev = blockIdx.x, lane = threadIdx.x;
+    const int ncell = g.jm * g.km;
+    const double* xb = terms + (size_t)lev * 2 * ncell;
+    const double* xw = xb + ncell;
+    const int* E = bexp + 2 * (size_t)lev * nbx;
+    const long long* U = bunits + 4 * (size_t)lev * nbx;
+    __shared__ int se[2 * TILE];
+    __shared__ long long su[4 * TILE];
+    __shared__ double st[BX_CH];
+    RunSum rs{0.0, 0, 0, false}, rw{0.0, 0, 0, false};   // lane 0's
+    for(int b0 = 0; b0 < nbx; b0 += TILE){
+        const int nt = min(TILE, nbx - b0);
+        for(int q = lane; q < 2 * nt; q += 32) se[q] = E[2 * b0 + q];
+        for(int q = lane; q < 4 * nt; q += 32) su[q] = U[4 * (size_t)b0 + q];
+        __syncwarp();
+        for(int bt = 0; bt < nt; bt++){
+            const int b = b0 + bt;
+            const int n = min(BX_CH, ncell - b * BX_CH);
+            int ok = 0;
+            if(lane == 0){                             // the two chains' O(1) steps side by side
+                const bool okb = chunk_fast(rs, se[2 * bt], su + 4 * bt);
+                const bool okw = chunk_fast(rw, se[2 * bt + 1], su + 4 * bt + 2);
+                ok = (okb ? 1 : 0) | (okw ? 2 : 0);
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            for(int which = 0; which < 2; which++){
+                if(ok & (1 << which)) continue;
+                RunSum& r = which ? rw : rs;           // in double form after a failed O(1) step
+                const double* x = (which ? xw : xb) + (size_t)b * BX_CH;
+                for(int c = lane; c < n; c += 32) st[c] = x[c];
+                __syncwarp();
+                if(lane == 0){
+                    double acc = r.s;
+#pragma unroll 8
+                    for(int c = 0; c < n; c++) acc += st[c];
+                    r.s = acc;
+                }
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+    }
+    if(lane == 0){
+        run_to_double(rs); run_to_double(rw);
+        ref[lev] = (rw.s > 0.0) ? rs.s / rw.s : 0.0;
+    }
 }
 
 // ---- RungeKutta_Uran_Turb.cpp:62-177: per column (j, k) -- every column, the seam copy and the
