@@ -879,22 +879,36 @@ static __global__ void __launch_bounds__(32) buoy_serial_pass_kernel(Grid g, int
     constexpr int TILE = 256;                          // chunks whose binades and units are staged at once
     const int lev = blockIdx.x, lane = threadIdx.x;
     const int ncell = g.jm * g.km;
-    const double* xb = terms + (size_t)lev * 2 * ncell;
-    const double* xw = xb + ncell;
+    const double* xs[2] = {terms + (size_t)lev * 2 * ncell, terms + (size_t)lev * 2 * ncell + ncell};
     const int* E = bexp + 2 * (size_t)lev * nbx;
     const long long* U = bunits + 4 * (size_t)lev * nbx;
     __shared__ int se[2 * TILE];
     __shared__ long long su[4 * TILE];
-    __shared__ double st[BX_CH];
+    // the terms of chunks taken term by term, [chunk parity][chain]: a chunk predicted to need it
+    // is copied in (cp.async) while the chunk before it is applied
+    __shared__ double stg[2][2][BX_CH];
     RunSum rs{0.0, 0, 0, false}, rw{0.0, 0, 0, false};   // lane 0's
     for(int b0 = 0; b0 < nbx; b0 += TILE){
         const int nt = min(TILE, nbx - b0);
         for(int q = lane; q < 2 * nt; q += 32) se[q] = E[2 * b0 + q];
         for(int q = lane; q < 4 * nt; q += 32) su[q] = U[4 * (size_t)b0 + q];
         __syncwarp();
+        int staged = 0;                                // chains whose chunk bt is copied in: bit c
         for(int bt = 0; bt < nt; bt++){
             const int b = b0 + bt;
             const int n = min(BX_CH, ncell - b * BX_CH);
+            // copy in the next chunk's terms for each chain predicted to take it term by term
+            int next = 0;
+            if(bt + 1 < nt){
+                const int b1 = b + 1, n1 = min(BX_CH, ncell - b1 * BX_CH);
+                for(int c = 0; c < 2; c++){
+                    if(se[2 * (bt + 1) + c] != INT_MIN) continue;
+                    next |= 1 << c;
+                    const double* x = xs[c] + (size_t)b1 * BX_CH;
+                    for(int q = lane; q < n1; q += 32) cp_async_n<8>(&stg[b1 & 1][c][q], x + q);
+                }
+            }
+            cp_async_commit();                         // one group per chunk, possibly empty
             int ok = 0;
             if(lane == 0){                             // the two chains' O(1) steps side by side
                 const bool okb = chunk_fast(rs, se[2 * bt], su + 4 * bt);
@@ -902,21 +916,30 @@ static __global__ void __launch_bounds__(32) buoy_serial_pass_kernel(Grid g, int
                 ok = (okb ? 1 : 0) | (okw ? 2 : 0);
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);
-            for(int which = 0; which < 2; which++){
-                if(ok & (1 << which)) continue;
-                RunSum& r = which ? rw : rs;           // in double form after a failed O(1) step
-                const double* x = (which ? xw : xb) + (size_t)b * BX_CH;
-                for(int c = lane; c < n; c += 32) st[c] = x[c];
+            if((ok & 3) != 3){
+                cp_async_wait<1>();                    // chunk b's copies (all but the newest group)
+                for(int c = 0; c < 2; c++){
+                    if((ok & (1 << c)) || (staged & (1 << c))) continue;
+                    const double* x = xs[c] + (size_t)b * BX_CH;     // not predicted: copy now
+                    for(int q = lane; q < n; q += 32) stg[b & 1][c][q] = x[q];
+                }
                 __syncwarp();
                 if(lane == 0){
-                    double acc = r.s;
+                    for(int c = 0; c < 2; c++){
+                        if(ok & (1 << c)) continue;
+                        RunSum& r = c ? rw : rs;       // in double form after a failed O(1) step
+                        const double* t = stg[b & 1][c];
+                        double acc = r.s;
 #pragma unroll 8
-                    for(int c = 0; c < n; c++) acc += st[c];
-                    r.s = acc;
+                        for(int q = 0; q < n; q++) acc += t[q];
+                        r.s = acc;
+                    }
                 }
                 __syncwarp();
             }
+            staged = next;
         }
+        cp_async_wait<0>();
         __syncwarp();
     }
     if(lane == 0){
