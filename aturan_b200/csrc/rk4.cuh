@@ -916,27 +916,26 @@ static __global__ void __launch_bounds__(32) buoy_serial_pass_kernel(Grid g, int
                 ok = (okb ? 1 : 0) | (okw ? 2 : 0);
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);
-            if((ok & 3) != 3){
-                cp_async_wait<1>();                    // chunk b's copies (all but the newest group)
-                for(int c = 0; c < 2; c++){
-                    if((ok & (1 << c)) || (staged & (1 << c))) continue;
-                    const double* x = xs[c] + (size_t)b * BX_CH;     // not predicted: copy now
+            // the chains that failed their O(1) step, term by term (RunSum in double form); the
+            // two chains are named, not selected through a reference, so they stay in registers
+            auto by_terms = [&](RunSum& r, int c){
+                if(!(staged & (1 << c))){               // not predicted: copy now
+                    const double* x = xs[c] + (size_t)b * BX_CH;
                     for(int q = lane; q < n; q += 32) stg[b & 1][c][q] = x[q];
                 }
                 __syncwarp();
                 if(lane == 0){
-                    for(int c = 0; c < 2; c++){
-                        if(ok & (1 << c)) continue;
-                        RunSum& r = c ? rw : rs;       // in double form after a failed O(1) step
-                        const double* t = stg[b & 1][c];
-                        double acc = r.s;
+                    const double* t = stg[b & 1][c];
+                    double acc = r.s;
 #pragma unroll 8
-                        for(int q = 0; q < n; q++) acc += t[q];
-                        r.s = acc;
-                    }
+                    for(int q = 0; q < n; q++) acc += t[q];
+                    r.s = acc;
                 }
                 __syncwarp();
-            }
+            };
+            if((ok & 3) != 3) cp_async_wait<1>();     // chunk b's copies (all but the newest group)
+            if(!(ok & 1)) by_terms(rs, 0);
+            if(!(ok & 2)) by_terms(rw, 1);
             staged = next;
         }
         cp_async_wait<0>();
