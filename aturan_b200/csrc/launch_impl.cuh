@@ -15,8 +15,12 @@ namespace aturan {
 // 6-9 % faster than the register ring at 3 or 4 blocks per SM; FP32: 3-25 % slower at every
 // depth and occupancy tried, so the register ring stays, one field ahead at 6 blocks per SM
 // (80 registers; 9 % faster than 4 blocks with two fields ahead).
-template <typename S> struct StageCfg { static constexpr int MINB1 = 5, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
-template <> struct StageCfg<float> { static constexpr int MINB1 = 7, PD = 1, MINB2 = 6, AD = 0, AMINB = 4; };
+// MP > 0: the momentum launch takes two cells per thread (rk_stage_pair_kernel) at MP resident
+// blocks per SM instead of one cell per thread at MINB1. FP32: 128 registers at 4 blocks per SM,
+// a 1.5 % faster stage than one cell per thread at 7 (3 blocks per SM: 2 % slower). FP64: the
+// pair form spills at 3-5 blocks per SM, so it keeps one cell per thread.
+template <typename S> struct StageCfg { static constexpr int MINB1 = 5, MP = 0, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
+template <> struct StageCfg<float> { static constexpr int MINB1 = 7, MP = 4, PD = 1, MINB2 = 6, AD = 0, AMINB = 4; };
 // The saturation adjustment has no shared memory of its own, so left to itself it runs with the
 // smallest shared-memory split of each SM's L1, and a kernel that needs shared memory (the pressure
 // solve's, beside it in aturan_step) cannot start on that SM until all its blocks have left.
@@ -43,6 +47,16 @@ void launch_scalars(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
         rk_scalar_pair_kernel<S, C, StageCfg<S>::PD, StageCfg<S>::MINB2><<<grid2, dim3(32, 4), 0, st>>>(a);
     }
 }
+template <typename S, typename C>
+void launch_momentum(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
+    if constexpr(StageCfg<S>::MP > 0){
+        rk_stage_pair_kernel<S, C, StageCfg<S>::MP><<<grid2, dim3(32, 4), 0, st>>>(a);
+    } else {
+        const Grid& g = a.g;
+        const dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);
+        rk_stage_kernel<S, C, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);
+    }
+}
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
 template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
@@ -51,9 +65,8 @@ template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
 #define ATURAN_DEFINE_LAUNCHERS(S, C)                                                                     \
 void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                                             \
     const Grid& g = a.g;                                                                                  \
-    dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);                                        \
-    rk_stage_kernel<S, C, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);                          \
     const dim3 grid2((g.km - 1 + 63) / 64, (g.jm - 2 + 3) / 4, g.im - 2);                                 \
+    launch_momentum(a, grid2, st);                                                                        \
     launch_scalars(a, grid2, st);                                                                         \
 }                                                                                                         \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \

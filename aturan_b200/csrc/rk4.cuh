@@ -653,6 +653,103 @@ __global__ void __launch_bounds__(128, MINB) rk_stage_kernel(const StageArgs<S, 
     stage_update(a, W, c, ATURAN_T, rhs_t, 1, in.anT);
 }
 
+// The seven stencil values of one field at the pair k0, k0 + 1 (as load_scalar2 forms them).
+template <typename S, typename C>
+__device__ __forceinline__ void load7c2(const S* X, const Cell& c, int q, R7<C>& A, R7<C>& B){
+    const int f = q * c.fs;
+    ld2<S, C>(X + (f + c.o), A.c, B.c);
+    ld2<S, C>(X + (f + c.oip), A.rp, B.rp);
+    ld2<S, C>(X + (f + c.oim), A.rm, B.rm);
+    ld2<S, C>(X + (f + c.ojp), A.tp, B.tp);
+    ld2<S, C>(X + (f + c.ojm), A.tm, B.tm);
+    A.pw = (C)ld(X + (f + c.okw));
+    B.pe = (C)ld(X + (f + c.oke));
+    A.pe = B.c;
+    B.pw = A.c;
+}
+
+template <typename S, typename C>
+__device__ __forceinline__ void load_acc_nc2(const StageArgs<S, C>& a, const S* X, const Cell& c, int q, AccNc<C>& A, AccNc<C>& B){
+    const int off = q * c.fs + c.o;
+    if(a.stage == 0){ A.acc = C(0.0); B.acc = C(0.0); }
+    else ld2_rw<S, C>(X + (c.dacc + off), A.acc, B.acc);
+    ld2<S, C>(X + (c.dnc + off), A.nc, B.nc);
+}
+
+// load_momentum for the pair: the same values, by 8-byte (FP32) or 16-byte (FP64 / pressure) loads
+// where the two cells' values are adjacent.
+template <typename S, typename C>
+__device__ __forceinline__ void load_momentum2(MomIn<C>& A, MomIn<C>& B, const StageArgs<S, C>& a, const S* X,
+                                               const Cell& c, const RhsConst<C>& K){
+    const double* P = a.pdyn;
+    const double* PH = a.phydro;
+    const int JK = a.g.jm * a.g.kp, kp = a.g.kp;
+    auto ldd2 = [](const double* p, double& x, double& y){
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p)); x = v.x; y = v.y;
+    };
+    ldd2(P + (c.o + JK), A.p_ip, B.p_ip); ldd2(P + (c.o - JK), A.p_im, B.p_im);
+    ldd2(P + (c.o + kp), A.p_jp, B.p_jp); ldd2(P + (c.o - kp), A.p_jm, B.p_jm);
+    ldd2(P + c.o, B.p_kw, A.p_ke);                      // p(k0) is k0 + 1's west, p(k0 + 1) k0's east
+    A.p_kw = ld(P + c.okw); B.p_ke = ld(P + c.oke);
+    ldd2(PH + (c.o + kp), A.ph_jp, B.ph_jp); ldd2(PH + (c.o - kp), A.ph_jm, B.ph_jm);
+    ldd2(PH + c.o, B.ph_kw, A.ph_ke);
+    A.ph_kw = ld(PH + c.okw); B.ph_ke = ld(PH + c.oke);
+    load7c2<S, C>(X, c, ATURAN_U, A.rU, B.rU); load7c2<S, C>(X, c, ATURAN_V, A.rV, B.rV);
+    load7c2<S, C>(X, c, ATURAN_W, A.rW, B.rW); load7c2<S, C>(X, c, ATURAN_T, A.rT, B.rT);
+    load_acc_nc2(a, X, c, ATURAN_U, A.anU, B.anU); load_acc_nc2(a, X, c, ATURAN_V, A.anV, B.anV);
+    load_acc_nc2(a, X, c, ATURAN_W, A.anW, B.anW); load_acc_nc2(a, X, c, ATURAN_T, A.anT, B.anT);
+    const S* F = X + (c.dforc + c.o);
+    if(K.tmf != C(0.0)) ld2<S, C>(F + (ATURAN_THERMALMASSFLUX - ATURAN_NUE) * c.fs, A.f_tmf, B.f_tmf);
+    else A.f_tmf = B.f_tmf = C(0.0);
+    if(K.precip_coupling != C(0.0)) ld2<S, C>(F + (ATURAN_Q_PRECIP - ATURAN_NUE) * c.fs, A.f_qp, B.f_qp);
+    else A.f_qp = B.f_qp = C(0.0);
+}
+
+// rk_stage_kernel with two cells per thread along k (k0 even; km - 1 is even, so a pair never
+// straddles the seam): the same arithmetic per cell, in the same order, with about half the load
+// and store instructions and address arithmetic per cell. Grid as the scalar launch's.
+template <typename S, typename C, int MINB>
+__global__ void __launch_bounds__(128, MINB) rk_stage_pair_kernel(const StageArgs<S, C> a){
+    const Grid& g = a.g;
+    const int k = 2 * (blockIdx.x * 32 + threadIdx.x);
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<C>& K = a.k;
+    const GeoIJ<C> geo = a.geo[i * g.jm + j];
+    const S* X = a.X;
+    S* W = const_cast<S*>(a.X);
+    const Cell c = make_cell(a, i, j, k, 2);
+
+    C nue0, nue1;
+    ld2<S, C>(X + (c.dforc + c.o), nue0, nue1);                 // ATURAN_NUE, the forcing group's first
+    auto nts = [&](C nue_c) -> C {
+        return (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
+    };
+    const C nue_t0 = nts(nue0), nue_t1 = nts(nue1);
+    const C nue_t_s0 = qdiv(nue_t0, C(0.9), C(1.0 / 0.9)), nue_t_s1 = qdiv(nue_t1, C(0.9), C(1.0 / 0.9));
+
+    MomIn<C> A, B;
+    load_momentum2(A, B, a, X, c, K);
+    C ru0, rv0, rw0, rt0, pr0, pt0, pp0, ru1, rv1, rw1, rt1, pr1, pt1, pp1;
+    momentum_rhs(a, A, geo, nue_t0, nue_t_s0, j, k, ru0, rv0, rw0, rt0, pr0, pt0, pp0);
+    momentum_rhs(a, B, geo, nue_t1, nue_t_s1, j, k + 1, ru1, rv1, rw1, rt1, pr1, pt1, pp1);
+    stage_update2(a, W, c, ATURAN_U, ru0, ru1, 0, A.anU, B.anU);
+    stage_update2(a, W, c, ATURAN_V, rv0, rv1, 0, A.anV, B.anV);
+    stage_update2(a, W, c, ATURAN_W, rw0, rw1, 0, A.anW, B.anW);
+    if(a.stage == 3){
+        S* Pj = a.proj + c.o;
+        const int fs = c.fs;
+        st2<S, C>(Pj + 0 * fs, ru0, ru1);
+        st2<S, C>(Pj + 1 * fs, rv0, rv1);
+        st2<S, C>(Pj + 2 * fs, rw0, rw1);
+        st2<S, C>(Pj + 3 * fs, ru0 + pr0, ru1 + pr1);
+        st2<S, C>(Pj + 4 * fs, rv0 + pt0, rv1 + pt1);
+        st2<S, C>(Pj + 5 * fs, rw0 + pp0, rw1 + pp1);
+    }
+    stage_update2(a, W, c, ATURAN_T, rt0, rt1, 1, A.anT, B.anT);
+}
+
 // ---- RungeKutta_Uran_Turb.cpp:18-37: per level, sin(theta)-weighted mean of g p / (r R T t_ref)
 // over every cell with T > 0 and a finite value. Fast form: each block reduces a contiguous
 // chunk of one level in a fixed tree order into partials[level][block]; a second kernel adds a
