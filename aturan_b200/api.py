@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 from . import fields as F
-from .params import Params, default_params
+from .params import Params, PostParams, default_params, default_post_params
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
@@ -61,11 +61,14 @@ SIGNATURES = {
     "aturan_profile_read": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "aturan_buoy_ref_level_static": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p], ctypes.c_int),
+    "aturan_post_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_post_step": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 STATIC_MAX_IM, STATIC_MAX_JM = 512, 4096
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post"]
+NSPECIES = 13
 
 _LIB = None
 
@@ -98,6 +101,13 @@ def library_default_params():
     rc = load_library().aturan_params_default(ctypes.byref(p))
     assert rc == 0
     return p
+
+
+def library_default_post_params():
+    pp = PostParams()
+    rc = load_library().aturan_post_params_default(ctypes.byref(pp))
+    assert rc == 0
+    return pp
 
 
 class Context:
@@ -173,6 +183,20 @@ class Context:
     def restore_ncopies(self, coeff=1.0):
         """aturan_restore_ncopies: the reference's restoreVar(coeff) after a step."""
         self._check(self.L.aturan_restore_ncopies(self.h, float(coeff)), "restore_ncopies")
+
+    def post_step(self, pp=None, sums=False):
+        """aturan_post_step: the filters, boundary passes and species clamp that follow the RK4 step
+        (cUranusModel.cpp:1218-1248), with pp's knobs (default: the reference's defaults). With
+        sums=True returns this call's clipped sum and count per species (synchronizes)."""
+        pp = default_post_params() if pp is None else pp
+        if not sums:
+            self._check(self.L.aturan_post_step(self.h, ctypes.byref(pp), None, None), "post_step")
+            return None
+        added = np.zeros(NSPECIES)
+        cells = np.zeros(NSPECIES, dtype=np.int64)
+        self._check(self.L.aturan_post_step(self.h, ctypes.byref(pp), added.ctypes.data, cells.ctypes.data),
+                    "post_step")
+        return added, cells
 
     def tape(self, on=True):
         """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""

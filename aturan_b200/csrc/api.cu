@@ -5,6 +5,7 @@
 // operand order (sources cited per table) and uploaded once, so the device reads the CPU's
 // values rather than recomputing them.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -22,6 +23,7 @@
 #include "pressure.cuh"
 #include "sor.cuh"
 #include "adjoint.cuh"
+#include "post.cuh"
 
 using namespace aturan;
 
@@ -637,6 +639,66 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
 }
 
 }  // namespace
+
+// The passes after RK4 on the context's fields (aturan_post_step).
+template <typename S>
+int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells){
+    const Grid& g = ctx->g;
+    const size_t fs = g.fstride;
+    S* X = reinterpret_cast<S*>(ctx->state);
+    S* Fo = reinterpret_cast<S*>(ctx->forc);
+    auto fld = [&](int id) -> S* { return id < ATURAN_NPROG ? X + (size_t)id * fs : Fo + (size_t)(id - ATURAN_NUE) * fs; };
+    static const int RAD[POST_NRAD] = { ATURAN_T, ATURAN_U, ATURAN_V, ATURAN_W,       // BC_Uran.cpp:21-41
+        ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+        ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+        ATURAN_NH4SH, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH,
+        ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX };
+    static const int THX[POST_NTHX] = { ATURAN_T, ATURAN_U,                             // BC_Uran.cpp:43-59
+        ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+        ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+        ATURAN_NH4SH, ATURAN_THERMALMASSFLUX };
+    static const int THZ[POST_NTHZ] = { ATURAN_V, ATURAN_W, ATURAN_MASSFLUX_H2S,         // BC_Uran.cpp:61-71
+        ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH };
+    static const int SP[POST_NSP] = { ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,      // BC_Uran.h:83-89
+        ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+        ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_NH4SH };
+    PostArgs<S> a;
+    a.g = g;
+    for(int n = 0; n < POST_NRAD; n++) a.rad[n] = fld(RAD[n]);
+    for(int n = 0; n < POST_NTHX; n++) a.thx[n] = fld(THX[n]);
+    for(int n = 0; n < POST_NTHZ; n++) a.thz[n] = fld(THZ[n]);
+    for(int n = 0; n < POST_NSP; n++) a.sp[n] = fld(SP[n]);
+    a.u = fld(ATURAN_U); a.v = fld(ATURAN_V); a.w = fld(ATURAN_W);
+    a.radius_form = pp->radius_form; a.bottom_form = pp->bottom_form; a.pole_form = pp->pole_form;
+    a.lid_u = pp->lid_u; a.top_taper = pp->top_taper; a.lid_vw = pp->lid_vw;
+    a.positive = pp->radius_positive; a.phi_periodic = pp->phi_periodic;
+    PostPlan pl;
+    pl.damp_t_horiz = pp->damp_t_horiz; pl.damp_t_vert = pp->damp_t_vert; pl.vel_shapiro = pp->vel_shapiro;
+    pl.damp_t_j = pp->damp_t_j; pl.species_clamp = pp->species_clamp;
+    // the clamp's partial sums borrow the pressure source's scratch (free between calls)
+    pl.nb = (int)std::min<size_t>(148 * 4, (fs - 2 * POST_NSP) / (2 * POST_NSP));
+    pl.part = ctx->scratch;
+    pl.out = ctx->scratch + (size_t)2 * POST_NSP * pl.nb;
+    int nl;
+    {
+        Region reg(ctx, ATURAN_K_POST, 0);
+        nl = launch_post(a, pl, fld(ATURAN_T), ctx->st);
+        reg.n = nl;
+        CK_LAUNCH("post step");
+    }
+    if(clamp_added || clamp_cells){
+        double h[2 * POST_NSP] = {0.0};
+        if(pp->species_clamp){
+            CK(cudaMemcpyAsync(h, pl.out, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+        }
+        for(int n = 0; n < POST_NSP; n++){
+            if(clamp_added) clamp_added[n] = h[n];
+            if(clamp_cells) clamp_cells[n] = (long)h[POST_NSP + n];
+        }
+    }
+    return ATURAN_OK;
+}
 
 extern "C" {
 
@@ -1440,6 +1502,37 @@ int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, d
     rc2 = ctx->mixed ? run_rk4<float, float>(ctx, ctx->k32, true) : run_rk4<double, double>(ctx, ctx->k64, true);
     if(rc2) return rc2;
     return rc;
+}
+
+// ---- the passes after RK4 (cUranusModel.cpp:1218-1248) ----
+int aturan_post_params_default(aturan_post_params* pp){
+    if(!pp) return ATURAN_E_INVALID;
+    std::memset(pp, 0, sizeof *pp);
+    pp->abi_version = ATURAN_ABI_VERSION;
+    pp->damp_t_j = 0;              // cUranusModel.cpp:1216-1217, !geo_balance() with GEO_BALANCE's default 1
+    pp->radius_form = 0;           // cUranusModel.h:406
+    pp->bottom_form = 0;           // cUranusModel.h:409
+    pp->pole_form = 0;             // cUranusModel.h:405
+    pp->lid_u = 1;                 // BC_LID_U defaults to BC_RIGID_LID, cUranusModel.h:403
+    pp->top_taper = 0;             // cUranusModel.h:404
+    pp->lid_vw = 2;                // BC_Uran.h:155, with geo_balance()
+    pp->radius_positive = 1;       // BC_Uran.h:92
+    pp->phi_periodic = 1;          // cUranusModel.h:412
+    pp->species_clamp = 1;         // BC_Uran.h:111
+    pp->damp_t_horiz = 1.0;        // cUranusModel.cpp:1214-1215
+    pp->damp_t_vert = 0.0;         // cUranusModel.cpp:1204-1205
+    pp->vel_shapiro = 0.0;         // cUranusModel.cpp:1229-1230, with geo_balance()
+    return ATURAN_OK;
+}
+
+int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells){
+    if(!ctx || !pp) return ATURAN_E_INVALID;
+    if(pp->abi_version != ATURAN_ABI_VERSION) return ATURAN_E_INVALID;
+    const Grid& g = ctx->g;
+    // the passes read four planes in from each end (BCForm's cubic); the k filter holds a row in
+    // 48 KB of shared memory
+    if(g.im < 4 || g.jm < 4 || g.km < 4 || g.km > 6144 || g.im > 65535 || g.jm > 65535) return ATURAN_E_UNSUPPORTED;
+    return ctx->mixed ? run_post<float>(ctx, pp, clamp_added, clamp_cells) : run_post<double>(ctx, pp, clamp_added, clamp_cells);
 }
 
 int aturan_profile(aturan_ctx* ctx, int enable){

@@ -8,7 +8,8 @@ namespace aturan {
 
 template <typename S, typename C> struct StageArgs;
 template <typename S> struct SatArgs;
-struct GSW; struct RBW; struct PressConst;
+template <typename S> struct PostArgs;
+struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
 void launch_stage(const StageArgs<S, C>& a, cudaStream_t st);                                              \
@@ -23,7 +24,8 @@ void launch_gs_pre(Grid g, S* au, S* av, S* aw, const S* ru, const S* rv, const 
 void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S* av, const S* aw,         \
                      const GSW* w, PressConst c, int s, cudaStream_t st);                                   \
 void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
-                    const RBW* w, PressConst c, double* src, cudaStream_t st);
+                    const RBW* w, PressConst c, double* src, cudaStream_t st);                             \
+int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)

@@ -4,6 +4,7 @@
 #include "rk4.cuh"
 #include "satadj.cuh"
 #include "pressure.cuh"
+#include "post.cuh"
 
 namespace aturan {
 // Stage launch configuration per storage type, measured on B200 at 41x181x361: resident blocks per
@@ -56,6 +57,33 @@ void launch_momentum(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
         const dim3 grid((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);
         rk_stage_kernel<S, C, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);
     }
+}
+// The passes after RK4 in the reference's order; returns the number of launches.
+template <typename S>
+int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st){
+    const Grid& g = a.g;
+    const dim3 cols_k((g.km + 127) / 128);
+    int n = 0;
+    auto filt = [&](S* x, bool ai, bool aj, bool ak, double strength){
+        const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
+        if(ak){ post_filter_k_kernel<S><<<g.im * g.jm, 128, g.km * sizeof(double), st>>>(g, x, coeff, a.phi_periodic && g.km > 2); n++; }
+        if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, coeff); n++; }
+        if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, coeff); n++; }
+    };
+    if(pl.damp_t_horiz != 0.0) filt(t, false, pl.damp_t_j != 0, true, pl.damp_t_horiz);
+    if(pl.damp_t_vert != 0.0) filt(t, true, false, false, pl.damp_t_vert);
+    if(pl.vel_shapiro != 0.0){ filt(a.u, true, true, true, pl.vel_shapiro); filt(a.v, true, true, true, pl.vel_shapiro);
+                               filt(a.w, true, true, true, pl.vel_shapiro); }
+    post_bc_radius_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(a);
+    post_bc_theta_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(a);
+    post_bc_phi_kernel<S><<<(g.im * g.jm + 127) / 128, 128, 0, st>>>(a);
+    n += 3;
+    if(pl.species_clamp){
+        post_clamp_kernel<S><<<dim3(pl.nb, POST_NSP), POST_CLAMP_NT, 0, st>>>(a, pl.part);
+        post_clamp_finish_kernel<<<1, 32, 0, st>>>(pl.part, pl.nb, pl.out);
+        n += 2;
+    }
+    return n;
 }
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
@@ -115,4 +143,7 @@ void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_
     prep_seam_kernel<S><<<(g.im * g.jm + 255) / 256, 256, 0, st>>>(g, au, av, aw, ru, rv, rw);            \
     rb_src_kernel<S><<<dim3((g.km - 1 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(                   \
         g, au, av, aw, w, c, src);                                                                        \
+}                                                                                                         \
+int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st){                          \
+    return launch_post_impl<S>(a, pl, t, st);                                                             \
 }

@@ -1,0 +1,233 @@
+// The passes that follow RungeKuttaUran in one iteration (planet/cUranusModel.cpp:1218-1248): the
+// 1-2-1 filters of lib/Utils.cpp:224-317 (damp_wiggles), the boundary passes of
+// BoundaryConditions.h:152-518 as BC_Uran.h:140-173 runs them for Uranus (margin 0, Neumann
+// default, no turbulence fields, no pole fill rows), the species floor of the radial planes and
+// the species clamp (BC_Uran.h:91-128).
+//
+// All of it is streaming work on a few planes of the state, bound by HBM. The filters update a
+// field in place: along k one block holds a row in shared memory; along j and i one thread walks
+// a column, keeping the old values of the cell and its lower neighbour in registers, so every old
+// value is read before it is overwritten, as the reference's copy of the field guarantees. The
+// boundary passes are column-local (radius: per (j,k), theta: per (i,k), phi: per (i,j)), so a
+// thread applies every step of its column in the reference's order, and one launch per pass
+// keeps the reference's order between passes. Arithmetic is FP64 on the stored values (FP32
+// storage in the mixed form is widened, computed in FP64 and rounded back).
+#pragma once
+#include "common.cuh"
+#include "pressure.cuh"
+
+namespace aturan {
+
+// Field tables: the reference's lists (BC_Uran.cpp:21-88) restricted to the fields the context
+// holds. The phi list equals the radius list on those fields.
+constexpr int POST_NRAD = 22, POST_NTHX = 16, POST_NTHZ = 6, POST_NSP = 13;
+
+// Which filter passes run and the clamp's scratch: part holds 2 nb doubles per species, out 2 x 13.
+struct PostPlan {
+    double damp_t_horiz, damp_t_vert, vel_shapiro;
+    int damp_t_j, species_clamp, nb;
+    double *part, *out;
+};
+
+template <typename S>
+struct PostArgs {
+    Grid g;
+    S* rad[POST_NRAD];           // radius and phi passes; rad[1] is u
+    S* thx[POST_NTHX];           // theta pass, extrapolated to the poles
+    S* thz[POST_NTHZ];           // theta pass, zeroed at the poles (v, w first)
+    S* sp[POST_NSP];             // species: floor and clamp, in BC_Uran.h:83-89's order
+    S *u, *v, *w;
+    int radius_form, bottom_form, pole_form, lid_u, top_taper, lid_vw, positive, phi_periodic;
+};
+
+// BCForm::apply with the model default NEUMANN (BoundaryConditions.h, cUranusModel.h:397)
+__device__ __forceinline__ double post_form(int form, double a, double b, double c){
+    const int f = (form == 0) ? 2 : form;
+    if(f == 1) return a;
+    if(f == 2) return C43 * a - C13 * b;
+    return c - 3.0 * b + 3.0 * a;
+}
+__device__ __forceinline__ double post_max0(double x){ return (0.0 < x) ? x : 0.0; }   // std::max(0.0, x)
+
+// ---- damp_wiggles (lib/Utils.cpp:224-317), one axis per launch ----
+
+// Along k: one block per (i, j) row, the row's old values in shared memory. With the periodic
+// seam the ring is k = 0..km-2 and k = km-1 takes the new k = 0; otherwise k wraps over all km.
+template <typename S>
+__global__ void __launch_bounds__(128) post_filter_k_kernel(Grid g, S* x, double coeff, int seam){
+    extern __shared__ double row[];
+    const size_t o = (size_t)blockIdx.x * g.kp;
+    const int km = g.km;
+    for(int k = threadIdx.x; k < km; k += blockDim.x) row[k] = (double)x[o + k];
+    __syncthreads();
+    const int k_end = seam ? km - 1 : km;
+    for(int k = threadIdx.x; k < k_end; k += blockDim.x){
+        const int km1 = seam ? (k == 0 ? km - 2 : k - 1) : (k - 1 + km) % km;
+        const int kp1 = seam ? (k == km - 2 ? 0 : k + 1) : (k + 1) % km;
+        const double c = row[k];
+        const S y = (S)(c + coeff * (row[km1] - 2.0 * c + row[kp1]));
+        x[o + k] = y;
+        if(seam && k == 0) x[o + km - 1] = y;
+    }
+}
+
+// Along a column of n cells at stride st from x0 (j: clamped at the poles; i: at the ends).
+template <typename S>
+__device__ __forceinline__ void post_walk(S* x0, size_t st, int n, double coeff){
+    double pm = (double)x0[0], c = pm;
+    for(int q = 0; q < n; q++){
+        const double nx = (q + 1 < n) ? (double)x0[(size_t)(q + 1) * st] : c;
+        x0[(size_t)q * st] = (S)(c + coeff * (pm - 2.0 * c + nx));
+        pm = c;
+        c = nx;
+    }
+}
+template <typename S>
+__global__ void __launch_bounds__(128) post_filter_j_kernel(Grid g, S* x, double coeff){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if(k >= g.km) return;
+    post_walk(x + gidx(g, i, 0, k), (size_t)g.kp, g.jm, coeff);
+}
+template <typename S>
+__global__ void __launch_bounds__(128) post_filter_i_kernel(Grid g, S* x, double coeff){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if(k >= g.km) return;
+    post_walk(x + gidx(g, 0, j, k), (size_t)g.jm * g.kp, g.im, coeff);
+}
+
+// ---- bcRadius (BoundaryConditions.h:152-286), floorRadialSpecies and the lid v, w (BC_Uran.h:91-170) ----
+template <typename S>
+__global__ void __launch_bounds__(128) post_bc_radius_kernel(PostArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if(k >= g.km) return;
+    const int im = g.im;
+    const size_t pl = (size_t)g.jm * g.kp, o = gidx(g, 0, j, k);
+    auto at = [&](S* F, int i) -> S& { return F[o + (size_t)i * pl]; };
+#pragma unroll 1
+    for(int n = 0; n < POST_NRAD; n++){
+        S* F = a.rad[n];
+        const int fb = (a.bottom_form != 0 && n != 1) ? a.bottom_form : a.radius_form;
+        at(F, 0) = (S)post_form(fb, (double)at(F, 1), (double)at(F, 2), (double)at(F, 3));
+        at(F, im - 1) = (S)post_form(a.radius_form, (double)at(F, im - 2), (double)at(F, im - 3), (double)at(F, im - 4));
+    }
+    if(a.lid_u != 0){ at(a.u, 0) = (S)0.0; at(a.u, im - 1) = (S)0.0; }
+    if(a.top_taper != 0){
+        const int l = im - 1;
+        at(a.v, l) = (S)0.0;
+        at(a.w, l) = (S)0.0;
+        if(a.top_taper == 2){
+            at(a.v, l - 1) = (S)((1.0 / 3.0) * (double)at(a.v, l - 3));
+            at(a.w, l - 1) = (S)((1.0 / 3.0) * (double)at(a.w, l - 3));
+            at(a.v, l - 2) = (S)((2.0 / 3.0) * (double)at(a.v, l - 3));
+            at(a.w, l - 2) = (S)((2.0 / 3.0) * (double)at(a.w, l - 3));
+        } else {
+            at(a.v, l - 1) = (S)((double)at(a.v, l - 1) * (1.0 / 3.0));
+            at(a.w, l - 1) = (S)((double)at(a.w, l - 1) * (1.0 / 3.0));
+            at(a.v, l - 2) = (S)((double)at(a.v, l - 2) * (2.0 / 3.0));
+            at(a.w, l - 2) = (S)((double)at(a.w, l - 2) * (2.0 / 3.0));
+        }
+    }
+    if(a.positive != 0){
+#pragma unroll 1
+        for(int n = 0; n < POST_NSP; n++){
+            S* F = a.sp[n];
+            if((double)at(F, 0) < 0.0) at(F, 0) = (S)((a.positive == 2) ? post_max0((double)at(F, 1)) : 0.0);
+            if((double)at(F, im - 1) < 0.0) at(F, im - 1) = (S)((a.positive == 2) ? post_max0((double)at(F, im - 2)) : 0.0);
+        }
+    }
+    if(a.lid_vw == 2 || a.lid_vw == 3){
+        const int A = im - 2, B = im - 3, Cc = im - 4, l = im - 1;
+        if(a.lid_vw == 2){
+            at(a.v, l) = (S)(2.0 * (double)at(a.v, A) - (double)at(a.v, B));
+            at(a.w, l) = (S)(2.0 * (double)at(a.w, A) - (double)at(a.w, B));
+        } else {
+            at(a.v, l) = (S)((double)at(a.v, Cc) - 3.0 * (double)at(a.v, B) + 3.0 * (double)at(a.v, A));
+            at(a.w, l) = (S)((double)at(a.w, Cc) - 3.0 * (double)at(a.w, B) + 3.0 * (double)at(a.w, A));
+        }
+    }
+}
+
+// ---- bcTheta (BoundaryConditions.h:293-391) ----
+template <typename S>
+__global__ void __launch_bounds__(128) post_bc_theta_kernel(PostArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if(k >= g.km) return;
+    const int jm = g.jm;
+    const size_t kp = (size_t)g.kp, o = gidx(g, i, 0, k);
+    auto at = [&](S* F, int j) -> S& { return F[o + (size_t)j * kp]; };
+#pragma unroll 1
+    for(int n = 0; n < POST_NTHZ; n++){ at(a.thz[n], 0) = (S)0.0; at(a.thz[n], jm - 1) = (S)0.0; }
+#pragma unroll 1
+    for(int n = 0; n < POST_NTHX; n++){
+        S* F = a.thx[n];
+        at(F, 0) = (S)post_form(a.pole_form, (double)at(F, 1), (double)at(F, 2), (double)at(F, 3));
+        at(F, jm - 1) = (S)post_form(a.pole_form, (double)at(F, jm - 2), (double)at(F, jm - 3), (double)at(F, jm - 4));
+    }
+}
+
+// ---- bcPhi (BoundaryConditions.h:398-455, without the seam damping) ----
+template <typename S>
+__global__ void __launch_bounds__(128) post_bc_phi_kernel(PostArgs<S> a){
+    const Grid& g = a.g;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;      // row (i, j)
+    if(r >= g.im * g.jm) return;
+    const size_t o = (size_t)r * g.kp;
+    const int km = g.km;
+#pragma unroll 1
+    for(int n = 0; n < POST_NRAD; n++){
+        S* F = a.rad[n] + o;
+        if(a.phi_periodic) F[km - 1] = F[0];
+        else {
+            const double lo = C43 * (double)F[1] - C13 * (double)F[2];
+            const double hi = C43 * (double)F[km - 2] - C13 * (double)F[km - 3];
+            const S y = (S)(0.5 * (lo + hi));
+            F[0] = y;
+            F[km - 1] = y;
+        }
+    }
+}
+
+// ---- clampNegativeSpecies (BC_Uran.h:110-128) ----
+// Block (b, n) clamps a grid-stride share of species n's stored cells and writes its clipped sum
+// and count (as doubles, exact for any count below 2^53) to part[2 (n nb + b)] in a fixed tree
+// order; post_clamp_finish_kernel adds a species' nb partials in block order. Deterministic run
+// to run; the reference's OpenMP reduction order differs, so the sum agrees to its rounding.
+constexpr int POST_CLAMP_NT = 256;
+template <typename S>
+__global__ void __launch_bounds__(POST_CLAMP_NT) post_clamp_kernel(PostArgs<S> a, double* part){
+    const Grid& g = a.g;
+    const int n = blockIdx.y, nb = gridDim.x;
+    S* F = a.sp[n];
+    const size_t N = (size_t)g.im * g.jm * g.km;
+    double s = 0.0, c = 0.0;
+    for(size_t e = (size_t)blockIdx.x * POST_CLAMP_NT + threadIdx.x; e < N; e += (size_t)nb * POST_CLAMP_NT){
+        const size_t r = e / (size_t)g.km;
+        const size_t o = r * g.kp + (e - r * g.km);
+        const double x = (double)F[o];
+        if(!(x >= 0.0)){                           // catches a NaN too
+            if(isfinite(x)){ s -= x; c += 1.0; }
+            F[o] = (S)0.0;
+        }
+    }
+    __shared__ double ss[POST_CLAMP_NT], sc[POST_CLAMP_NT];
+    ss[threadIdx.x] = s; sc[threadIdx.x] = c;
+    __syncthreads();
+    for(int st = POST_CLAMP_NT / 2; st > 0; st >>= 1){
+        if((int)threadIdx.x < st){ ss[threadIdx.x] += ss[threadIdx.x + st]; sc[threadIdx.x] += sc[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0){ part[2 * ((size_t)n * nb + blockIdx.x)] = ss[0]; part[2 * ((size_t)n * nb + blockIdx.x) + 1] = sc[0]; }
+}
+
+static __global__ void post_clamp_finish_kernel(const double* part, int nb, double* out){
+    const int n = threadIdx.x;
+    if(n >= POST_NSP) return;
+    double s = 0.0, c = 0.0;
+    for(int b = 0; b < nb; b++){ s += part[2 * ((size_t)n * nb + b)]; c += part[2 * ((size_t)n * nb + b) + 1]; }
+    out[n] = s;
+    out[POST_NSP + n] = c;
+}
+
+}  // namespace aturan

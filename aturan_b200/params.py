@@ -144,3 +144,39 @@ def params_from_ref(ref):
             G.del_alf_i = ref.scalar(f"del_alf_{g}_ice")
             G.del_bet_i = ref.scalar(f"del_bet_{g}_ice")
     return p
+
+
+class PostParams(ctypes.Structure):
+    """aturan_post_params: the knobs of the passes after RungeKuttaUran (cUranusModel.cpp:1218-1248)."""
+    _fields_ = ([(n, ctypes.c_int32) for n in (
+        "abi_version", "damp_t_j", "radius_form", "bottom_form", "pole_form", "lid_u", "top_taper",
+        "lid_vw", "radius_positive", "phi_periodic", "species_clamp")]
+        + [("reserved_i", ctypes.c_int32 * 5)]
+        + [(n, ctypes.c_double) for n in ("damp_t_horiz", "damp_t_vert", "vel_shapiro")]
+        + [("reserved_d", ctypes.c_double * 5)])
+
+    def copy(self):
+        c = PostParams()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(self), ctypes.sizeof(self))
+        return c
+
+
+def default_post_params(geo_balance=True):
+    """The values the reference's ATURAN_* knobs take with the environment unset (ATURAN_GEO_BALANCE
+    defaults to 1, cUranusModel.h:1467-1469); geo_balance=False gives those of GEO_BALANCE=0."""
+    pp = PostParams()
+    pp.abi_version = ABI_VERSION
+    pp.damp_t_j = 0 if geo_balance else 1             # cUranusModel.cpp:1216-1217
+    pp.radius_form = 0                                # cUranusModel.h:406
+    pp.bottom_form = 0                                # cUranusModel.h:409
+    pp.pole_form = 0                                  # cUranusModel.h:405
+    pp.lid_u = 1                                      # BC_LID_U = BC_RIGID_LID, cUranusModel.h:403
+    pp.top_taper = 0                                  # cUranusModel.h:404
+    pp.lid_vw = 2 if geo_balance else 0               # BC_Uran.h:155
+    pp.radius_positive = 1                            # BC_Uran.h:92
+    pp.phi_periodic = 1                               # cUranusModel.h:412
+    pp.species_clamp = 1                              # BC_Uran.h:111
+    pp.damp_t_horiz = 1.0                             # cUranusModel.cpp:1214-1215
+    pp.damp_t_vert = 0.0                              # cUranusModel.cpp:1204-1205
+    pp.vel_shapiro = 0.0 if geo_balance else 1.0      # cUranusModel.cpp:1229-1230
+    return pp

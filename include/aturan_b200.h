@@ -266,6 +266,53 @@ int aturan_restore_ncopies(aturan_ctx* ctx, double coeff);
  * the n-copy sync and the RK4 step. */
 int aturan_step(aturan_ctx* ctx, int press_kind, double omega, int max_sweeps, double tol);
 
+/* The knobs of the part of an iteration that follows RungeKuttaUran (cUranusModel.cpp:1218-1248):
+ * the t filter, the velocity filter, the three boundary passes (BC_Uran.h:140-173 over
+ * BoundaryConditions.h:152-518) and the species clamp. The reference reads each from an
+ * ATURAN_* environment variable once per process; the caller resolves them.
+ * aturan_post_params_default gives the values they take with the environment unset. A form is
+ * BCForm's (BoundaryConditions.h): 0 the model default (Neumann), 1 copy, 2 Neumann
+ * c43 a - c13 b, anything else the cubic c - 3 b + 3 a. */
+typedef struct aturan_post_params {
+    int32_t abi_version;      /* = ATURAN_ABI_VERSION */
+    int32_t damp_t_j;         /* ATURAN_DAMP_T_J: the t filter's latitude pass (default !GEO_BALANCE = 0) */
+    int32_t radius_form;      /* ATURAN_BC_RADIUS_COPY (0): i = 0 and im-1 of the radius list */
+    int32_t bottom_form;      /* ATURAN_BC_BOTTOM_FORM (0 = radius_form): i = 0 of every field but u */
+    int32_t pole_form;        /* ATURAN_BC_POLE_COPY (0): j = 0 and jm-1 of the theta list */
+    int32_t lid_u;            /* ATURAN_BC_LID_U (= ATURAN_BC_RIGID_LID = 1): u = 0 on i = 0, im-1 */
+    int32_t top_taper;        /* ATURAN_BC_TOP_TAPER (0; 1 or 2): v, w toward zero at the top */
+    int32_t lid_vw;           /* ATURAN_BC_LID_VW (2 with GEO_BALANCE): v, w at im-1; 2 linear, 3 cubic */
+    int32_t radius_positive;  /* ATURAN_BC_RADIUS_POSITIVE (1): species floor on i = 0, im-1; 2 copy */
+    int32_t phi_periodic;     /* ATURAN_BC_PHI_PERIODIC (1): k = km-1 copies k = 0; 0 = averaged ends */
+    int32_t species_clamp;    /* ATURAN_SPECIES_CLAMP (1): negative and NaN species values -> 0 */
+    int32_t reserved_i[5];
+    double damp_t_horiz;      /* ATURAN_DAMP_T_HORIZ (1.0): strength of the t filter's horizontal passes */
+    double damp_t_vert;       /* ATURAN_DAMP_T_VERT (0.0): strength of its radial pass */
+    double vel_shapiro;       /* ATURAN_VEL_SHAPIRO (0.0 with GEO_BALANCE): 1-2-1 pass on u, v, w */
+    double reserved_d[5];
+} aturan_post_params;
+
+#define ATURAN_NSPECIES 13    /* h2o, h2o_cloud, h2o_ice, h2s.., nh3.., ch4.., nh4sh (BC_Uran.h:83-89) */
+
+int aturan_post_params_default(aturan_post_params* pp);
+
+/* What cUranusModel.cpp:1218-1248 does to the state after RungeKuttaUran, in its order:
+ *   damp_wiggles(t, along k [and j]) with damp_t_horiz, damp_wiggles(t, along i) with damp_t_vert
+ *   (lib/Utils.cpp:224-317), damp_wiggles(u / v / w, along k, j, i) with vel_shapiro, then
+ *   BC_Uran::bcRadius (with floorRadialSpecies and the lid v, w), bcTheta, bcPhi, and
+ *   clampNegativeSpecies (BC_Uran.h:91-128).
+ * The boundary passes apply to the fields of the reference's lists (BC_Uran.cpp) that the
+ * context holds: t, u, v, w, the twelve condensables, nh4sh, massflux_h2s/nh3/nh4sh,
+ * fluxlim_nh4sh and thermalmassflux. The other listed arrays (chrom, the j_/jT_/w_ and difflux
+ * fluxes, the force and heat diagnostics) are not held; a driver applies the passes to those on
+ * the host. clamp_added / clamp_cells (may be NULL; ATURAN_NSPECIES entries each, in the order
+ * above) receive this call's clipped sum and count per species, what the reference adds to its
+ * cumulative clamp_added / clamp_cells; passing them synchronizes the stream.
+ * Not implemented (the reference's defaults leave them off; the host keeps them): BC_T_LID_PIN,
+ * BC_SEAM_DAMP, VEL_SHAPIRO_ORDER=4, the turbulence fields' floors (bc_turb_active is false for
+ * Uranus) and pole fill rows (bc_pole_open_rows is 0 for Uranus). */
+int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
@@ -275,6 +322,7 @@ enum aturan_kernel_kind {
     ATURAN_K_HYDRO,          /* buoyancy reference level + hydrostatic column integral */
     ATURAN_K_COPY,           /* n-copy sync and layout conversions */
     ATURAN_K_ADJOINT,        /* the RK4 step's adjoint (aturan_rk4_adjoint) */
+    ATURAN_K_POST,           /* filters, boundary passes and species clamp (aturan_post_step) */
     ATURAN_K_NKINDS
 };
 

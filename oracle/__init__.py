@@ -69,6 +69,7 @@ class Oracle:
             ("oracle_cp_lapse", [P, ctypes.c_double], ctypes.c_double),
             ("oracle_rhs_cell", [P, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             ("oracle_set_threads", [ctypes.c_int], None),
+            ("oracle_post_step", [P, vp, P, vp, vp], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -169,3 +170,11 @@ class Oracle:
         out = np.zeros(22)
         assert self.L.oracle_rhs_cell(self._p(p), field_ptrs(state), i, j, k, out.ctypes.data) == 0
         return out
+
+    def post_step(self, p, state, pp):
+        """The passes after RK4 (filters, boundary passes, species clamp) on the state in place;
+        returns this call's clipped sums and counts per species."""
+        added, cells = np.zeros(13), np.zeros(13, dtype=np.int64)
+        assert self.L.oracle_post_step(self._p(p), field_ptrs(state), self._p(pp), added.ctypes.data,
+                                       cells.ctypes.data) == 0
+        return added, cells

@@ -1624,3 +1624,183 @@ int oracle_step(const aturan_params* p, double* const* f, int press_kind, double
     oracle_sync_ncopies(p, f);
     return oracle_rk4(p, f, ref_out);
 }
+
+/* ---- after RungeKuttaUran: filters, boundary passes, species clamp (cUranusModel.cpp:1218-1248) ---- */
+
+/* The reference's boundary lists (BC_Uran.cpp:21-88) restricted to the fields the library holds. */
+static const int POST_RADIUS[] = { ATURAN_T, ATURAN_U, ATURAN_V, ATURAN_W,
+    ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+    ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+    ATURAN_NH4SH, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH,
+    ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX };
+static const int POST_THETA_EXTRAP[] = { ATURAN_T, ATURAN_U,
+    ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+    ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+    ATURAN_NH4SH, ATURAN_THERMALMASSFLUX };
+static const int POST_THETA_ZERO[] = { ATURAN_V, ATURAN_W, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3,
+    ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH };
+/* BC_Uran.h:83-89 (species_fields), the order of the clamp's per-species sums */
+static const int POST_SPECIES[ATURAN_NSPECIES] = { ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+    ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+    ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_NH4SH };
+#define NELEM(a) ((int)(sizeof(a) / sizeof((a)[0])))
+
+/* BoundaryConditions.h (BCForm::apply) with the model default NEUMANN (cUranusModel.h:397) */
+static double bc_form(int form, double a, double b, double c){
+    const int f = (form == 0) ? 2 : form;
+    if(f == 1) return a;
+    if(f == 2) return C43 * a - C13 * b;
+    return c - 3.0 * b + 3.0 * a;
+}
+
+/* lib/Utils.cpp:224-317, damp_wiggles without a surface (i_surface = nullptr): the 1-2-1 pass
+ * along k (periodic ring of km-1 meridians when seam, with k = km-1 the copy of k = 0), then j
+ * (clamped at the poles), then i (clamped at the ends), each from a copy of the field. */
+static void post_damp(const aturan_params* p, double* x, int along_i, int along_j, int along_k,
+                      double strength, int seam_periodic, double* tmp){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const size_t N = (size_t)im * jm * km;
+    const double coeff = strength * 0.25;
+    if(along_k){
+        memcpy(tmp, x, sizeof(double) * N);
+        const int seam = seam_periodic && km > 2;
+        const int k_end = seam ? km - 1 : km;
+        for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++){
+            for(int k = 0; k < k_end; k++){
+                const int km1 = seam ? (k == 0 ? km - 2 : k - 1) : (k - 1 + km) % km;
+                const int kp1 = seam ? (k == km - 2 ? 0 : k + 1) : (k + 1) % km;
+                const double c = tmp[IDX(i,j,k)];
+                x[IDX(i,j,k)] = c + coeff * (tmp[IDX(i,j,km1)] - 2.0 * c + tmp[IDX(i,j,kp1)]);
+            }
+            if(seam) x[IDX(i,j,km-1)] = x[IDX(i,j,0)];
+        }
+    }
+    if(along_j){
+        memcpy(tmp, x, sizeof(double) * N);
+        for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++){
+            const int jm1 = j - 1 < 0 ? 0 : j - 1, jp1 = j + 1 > jm - 1 ? jm - 1 : j + 1;
+            for(int k = 0; k < km; k++){
+                const double c = tmp[IDX(i,j,k)];
+                x[IDX(i,j,k)] = c + coeff * (tmp[IDX(i,jm1,k)] - 2.0 * c + tmp[IDX(i,jp1,k)]);
+            }
+        }
+    }
+    if(along_i){
+        memcpy(tmp, x, sizeof(double) * N);
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++) for(int i = 0; i < im; i++){
+            const int im1 = i - 1 < 0 ? 0 : i - 1, ip1 = i + 1 > im - 1 ? im - 1 : i + 1;
+            const double c = tmp[IDX(i,j,k)];
+            x[IDX(i,j,k)] = c + coeff * (tmp[IDX(im1,j,k)] - 2.0 * c + tmp[IDX(ip1,j,k)]);
+        }
+    }
+}
+
+static double post_max0(double x){ return (0.0 < x) ? x : 0.0; }   /* std::max(0.0, x) */
+
+int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post_params* pp,
+                     double* clamp_added, long* clamp_cells){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const size_t N = (size_t)im * jm * km;
+    double* tmp = (double*)malloc(sizeof(double) * N);
+    if(!tmp) return -1;
+    /* cUranusModel.cpp:1218-1221: the t filter, horizontal passes then the radial one */
+    if(pp->damp_t_horiz != 0.0) post_damp(p, f[ATURAN_T], 0, pp->damp_t_j, 1, pp->damp_t_horiz, pp->phi_periodic, tmp);
+    if(pp->damp_t_vert != 0.0) post_damp(p, f[ATURAN_T], 1, 0, 0, pp->damp_t_vert, pp->phi_periodic, tmp);
+    /* :1236-1240: the velocity filter, u then v then w, each along k, j, i */
+    if(pp->vel_shapiro != 0.0)
+        for(int q = ATURAN_U; q <= ATURAN_W; q++) post_damp(p, f[q], 1, 1, 1, pp->vel_shapiro, pp->phi_periodic, tmp);
+    free(tmp);
+
+    /* BoundaryConditions.h:152-286 (bcRadius; margin 0, no turbulence fields, no lid pin) */
+    for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){
+        for(int n = 0; n < NELEM(POST_RADIUS); n++){
+            double* F = f[POST_RADIUS[n]];
+            const int fb = (pp->bottom_form != 0 && POST_RADIUS[n] != ATURAN_U) ? pp->bottom_form : pp->radius_form;
+            F[IDX(0,j,k)] = bc_form(fb, F[IDX(1,j,k)], F[IDX(2,j,k)], F[IDX(3,j,k)]);
+            F[IDX(im-1,j,k)] = bc_form(pp->radius_form, F[IDX(im-2,j,k)], F[IDX(im-3,j,k)], F[IDX(im-4,j,k)]);
+        }
+    }
+    if(pp->lid_u != 0)
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){ f[ATURAN_U][IDX(0,j,k)] = 0.0; f[ATURAN_U][IDX(im-1,j,k)] = 0.0; }
+    if(pp->top_taper != 0){
+        double* v = f[ATURAN_V]; double* w = f[ATURAN_W];
+        const int l = im - 1;
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){
+            v[IDX(l,j,k)] = 0.0;
+            w[IDX(l,j,k)] = 0.0;
+            if(pp->top_taper == 2){
+                v[IDX(l-1,j,k)] = (1.0 / 3.0) * v[IDX(l-3,j,k)];
+                w[IDX(l-1,j,k)] = (1.0 / 3.0) * w[IDX(l-3,j,k)];
+                v[IDX(l-2,j,k)] = (2.0 / 3.0) * v[IDX(l-3,j,k)];
+                w[IDX(l-2,j,k)] = (2.0 / 3.0) * w[IDX(l-3,j,k)];
+            } else {
+                v[IDX(l-1,j,k)] *= (1.0 / 3.0);
+                w[IDX(l-1,j,k)] *= (1.0 / 3.0);
+                v[IDX(l-2,j,k)] *= (2.0 / 3.0);
+                w[IDX(l-2,j,k)] *= (2.0 / 3.0);
+            }
+        }
+    }
+    /* BC_Uran.h:91-108, floorRadialSpecies */
+    if(pp->radius_positive != 0)
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++)
+            for(int n = 0; n < ATURAN_NSPECIES; n++){
+                double* F = f[POST_SPECIES[n]];
+                if(F[IDX(0,j,k)] < 0.0) F[IDX(0,j,k)] = (pp->radius_positive == 2) ? post_max0(F[IDX(1,j,k)]) : 0.0;
+                if(F[IDX(im-1,j,k)] < 0.0) F[IDX(im-1,j,k)] = (pp->radius_positive == 2) ? post_max0(F[IDX(im-2,j,k)]) : 0.0;
+            }
+    /* BC_Uran.h:155-170, the lid value of v, w */
+    if(pp->lid_vw == 2 || pp->lid_vw == 3){
+        double* v = f[ATURAN_V]; double* w = f[ATURAN_W];
+        const int a = im - 2, b = im - 3, c = im - 4, l = im - 1;
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){
+            if(pp->lid_vw == 2){
+                v[IDX(l,j,k)] = 2.0 * v[IDX(a,j,k)] - v[IDX(b,j,k)];
+                w[IDX(l,j,k)] = 2.0 * w[IDX(a,j,k)] - w[IDX(b,j,k)];
+            } else {
+                v[IDX(l,j,k)] = v[IDX(c,j,k)] - 3.0 * v[IDX(b,j,k)] + 3.0 * v[IDX(a,j,k)];
+                w[IDX(l,j,k)] = w[IDX(c,j,k)] - 3.0 * w[IDX(b,j,k)] + 3.0 * w[IDX(a,j,k)];
+            }
+        }
+    }
+    /* BoundaryConditions.h:293-391 (bcTheta; no pole fill rows for Uranus) */
+    for(int k = 0; k < km; k++) for(int i = 0; i < im; i++){
+        for(int n = 0; n < NELEM(POST_THETA_ZERO); n++){
+            double* F = f[POST_THETA_ZERO[n]];
+            F[IDX(i,0,k)] = 0.0;
+            F[IDX(i,jm-1,k)] = 0.0;
+        }
+        for(int n = 0; n < NELEM(POST_THETA_EXTRAP); n++){
+            double* F = f[POST_THETA_EXTRAP[n]];
+            F[IDX(i,0,k)] = bc_form(pp->pole_form, F[IDX(i,1,k)], F[IDX(i,2,k)], F[IDX(i,3,k)]);
+            F[IDX(i,jm-1,k)] = bc_form(pp->pole_form, F[IDX(i,jm-2,k)], F[IDX(i,jm-3,k)], F[IDX(i,jm-4,k)]);
+        }
+    }
+    /* BoundaryConditions.h:398-518 (bcPhi without the seam damping); its list equals the radius
+     * list on the fields held */
+    for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++)
+        for(int n = 0; n < NELEM(POST_RADIUS); n++){
+            double* F = f[POST_RADIUS[n]];
+            if(pp->phi_periodic) F[IDX(i,j,km-1)] = F[IDX(i,j,0)];
+            else {
+                const double lo = C43 * F[IDX(i,j,1)] - C13 * F[IDX(i,j,2)];
+                const double hi = C43 * F[IDX(i,j,km-2)] - C13 * F[IDX(i,j,km-3)];
+                F[IDX(i,j,0)] = F[IDX(i,j,km-1)] = 0.5 * (lo + hi);
+            }
+        }
+    /* BC_Uran.h:110-128, clampNegativeSpecies: this call's clipped sum and count per species */
+    for(int n = 0; n < ATURAN_NSPECIES; n++){
+        double a = 0.0; long c = 0;
+        if(pp->species_clamp){
+            double* F = f[POST_SPECIES[n]];
+            for(size_t q = 0; q < N; q++)
+                if(!(F[q] >= 0.0)){
+                    if(isfinite(F[q])){ a -= F[q]; c++; }
+                    F[q] = 0.0;
+                }
+        }
+        if(clamp_added) clamp_added[n] = a;
+        if(clamp_cells) clamp_cells[n] = c;
+    }
+    return 0;
+}

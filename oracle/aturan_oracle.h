@@ -46,6 +46,9 @@ int oracle_sync_ncopies(const aturan_params* p, double* const* f);
 int oracle_step(const aturan_params* p, double* const* f, int press_kind, double omega,
                 int max_sweeps, double tol, double* ref_level_out);
 void oracle_set_threads(int n);
+/* cUranusModel.cpp:1218-1248 after RK4: filters, boundary passes, species clamp */
+int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post_params* pp,
+                     double* clamp_added, long* clamp_cells);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,8 @@ class Ref:
         L.ref_pressure_shared.argtypes = [ctypes.c_int]
         L.ref_satadj.argtypes = [ctypes.c_int]
         L.ref_hydro.argtypes = [ctypes.c_int]
+        L.ref_damp_wiggles.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.ref_clamp_species.argtypes = [vp, vp]
         L.ref_set_quiet(1 if quiet else 0)
         self.L = L
         self.path = path
@@ -140,3 +142,25 @@ class Ref:
 
     def sync_ncopies(self):
         assert self.L.ref_sync_ncopies() == 0
+
+    def geo_balance(self):
+        return bool(self.L.ref_geo_balance())
+
+    def post_step(self, pp):
+        """cUranusModel.cpp:1218-1248 on the loaded state: the t and velocity filters with pp's
+        axes and strengths (the values the model's own knobs take must be passed), then bcRadius,
+        bcTheta, bcPhi and clampNegativeSpecies with the reference's own knobs. Returns this call's
+        clipped sums and counts per species."""
+        L = self.L
+        if pp.damp_t_horiz != 0.0:
+            assert L.ref_damp_wiggles(b"t", 0, int(pp.damp_t_j), 1, float(pp.damp_t_horiz)) == 0
+        if pp.damp_t_vert != 0.0:
+            assert L.ref_damp_wiggles(b"t", 1, 0, 0, float(pp.damp_t_vert)) == 0
+        if pp.vel_shapiro != 0.0:
+            for n in (b"u", b"v", b"w"):
+                assert L.ref_damp_wiggles(n, 1, 1, 1, float(pp.vel_shapiro)) == 0
+        assert L.ref_bc_radius() == 0 and L.ref_bc_theta() == 0 and L.ref_bc_phi() == 0
+        added, cells = np.zeros(13), np.zeros(13, dtype=np.int64)
+        n = L.ref_clamp_species(added.ctypes.data, cells.ctypes.data)
+        assert n in (0, 13), n
+        return added, cells

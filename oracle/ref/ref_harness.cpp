@@ -55,6 +55,7 @@
 #include "PressureSolver.h"
 #include "SaturationAdjustmentUran.h"
 #include "ChemistryUran.h"
+#include "BC_Uran.h"
 #undef private
 
 namespace {
@@ -312,5 +313,29 @@ int ref_sync_ncopies(){
 }
 
 int ref_restore_var(){ g_model->restoreVar(1.0); return 0; }
+
+// The calls cUranusModel.cpp:1218-1248 makes after RungeKuttaUran, each exposed alone so that a
+// test composes them in the model's order. The boundary passes and the clamp read their knobs
+// from the reference's own ATURAN_* environment variables (once per process); the filter takes
+// its axes and strength as the model's call site passes them.
+int ref_damp_wiggles(const char* name, int along_i, int along_j, int along_k, double strength){
+    Array* a = field(name);
+    if(!a || !a->x) return -1;
+    AtomUtils::damp_wiggles(*a, nullptr, along_i != 0, along_j != 0, along_k != 0, strength);
+    return 0;
+}
+int ref_bc_radius(){ BC_Uran(*g_model).bcRadius(); return 0; }
+int ref_bc_theta(){ BC_Uran(*g_model).bcTheta(); return 0; }
+int ref_bc_phi(){ BC_Uran(*g_model).bcPhi(); return 0; }
+// clampNegativeSpecies with its cumulative sums reset first, so they hold this call's.
+int ref_clamp_species(double* added, long* cells){
+    cUranusModel& m = *g_model;
+    m.clamp_added.clear();
+    m.clamp_cells.clear();
+    m.clampNegativeSpecies();
+    for(size_t n = 0; n < m.clamp_added.size(); n++){ added[n] = m.clamp_added[n]; cells[n] = m.clamp_cells[n]; }
+    return (int)m.clamp_added.size();
+}
+int ref_geo_balance(){ return cUranusModel::geo_balance() ? 1 : 0; }
 
 }  // extern "C"

@@ -7,6 +7,7 @@ oracle restatement must reproduce every digest bit for bit (tests/test_golden.py
 it on machines without the reference tree.
 
     python tests/golden/make_golden.py          # needs oracle/_ref (make -C oracle ref)
+    python tests/golden/make_golden.py post_step   # (re)make the named cases, keep the others
 """
 import hashlib
 import json
@@ -26,6 +27,11 @@ CASES = {
     "pressure_gs": dict(seed=103, outputs=["p_dyn", "aux_u", "aux_v", "aux_w"]),
     "pressure_rb3": dict(seed=104, outputs=["p_dyn"] + F.PROJECTION),
     "step_gs": dict(seed=105, outputs=F.PROGNOSTIC + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION),
+    # the passes after RK4 with the default knobs, on post_case.post_state(state, seed + 1)
+    "post_step": dict(seed=106, outputs=["t", "u", "v", "w", "h2o", "h2o_cloud", "h2o_ice", "h2s", "h2s_cloud",
+                                         "h2s_ice", "nh3", "nh3_cloud", "nh3_ice", "ch4", "ch4_cloud", "ch4_ice",
+                                         "nh4sh", "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh",
+                                         "thermalmassflux"]),
 }
 NSAMPLE = 32
 
@@ -53,9 +59,16 @@ def run_case(name, runner):
     return rec
 
 
+def post_input(p, st, seed):
+    from tests.post_case import post_state
+    return post_state(st, p, seed + 1)
+
+
 def ref_runner(name, p, st):
     from oracle.ref import Ref
     ref = Ref.get_instance()
+    if name == "post_step":
+        st = post_input(p, st, CASES[name]["seed"])
     ref.load(st)
     if name == "satadj4":
         for g in range(4):
@@ -72,22 +85,27 @@ def ref_runner(name, p, st):
             ref.satadj(g)
         ref.sync_ncopies()
         ref.rk4()
+    elif name == "post_step":
+        ref.post_step(P.default_post_params())
     out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
     if "buoy_ref_level" in CASES[name]["outputs"]:
         out["buoy_ref_level"] = ref.get("buoy_ref_level")
     return out
 
 
-def main():
+def main(only=()):
+    path = os.path.join(HERE, "golden.json")
     golden = {"note": "SHA-256 of FP64 outputs of the compiled reference on seeded synthetic states; "
                       "made by tests/golden/make_golden.py",
               "numpy": np.__version__, "cases": {}}
-    for name in CASES:
+    if only and os.path.exists(path):
+        golden["cases"] = json.load(open(path))["cases"]
+    for name in (only or CASES):
         golden["cases"][name] = run_case(name, ref_runner)
         print("done", name, flush=True)
-    with open(os.path.join(HERE, "golden.json"), "w") as fh:
+    with open(path, "w") as fh:
         json.dump(golden, fh, indent=1)
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -46,6 +46,22 @@ def test_library_defaults_equal_python_defaults():
     assert bytes(a) == bytes(b)
 
 
+def test_post_params_layout_and_defaults(tmp_path):
+    """aturan_post_params: the header's layout, and the library's defaults (the reference's knobs
+    with the environment unset) equal the Python mirror's."""
+    src = tmp_path / "pp.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu %zu\\n", sizeof(aturan_post_params),'
+                   ' offsetof(aturan_post_params, damp_t_horiz), offsetof(aturan_post_params, vel_shapiro));'
+                   ' return 0; }\n')
+    exe = tmp_path / "pp"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_h, off_v = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.PostParams)
+    assert off_h == P.PostParams.damp_t_horiz.offset and off_v == P.PostParams.vel_shapiro.offset
+    assert bytes(api.library_default_post_params()) == bytes(P.default_post_params())
+
+
 def test_no_cpu_fallback_without_gpu():
     import torch
     if torch.cuda.is_available():

@@ -28,6 +28,10 @@ def oracle_runner(O, name, p, st):
         O.pressure_rb(p, st, 3)
     elif name == "step_gs":
         lev = O.step(p, st, P.PRESS_GS_LEX)
+    elif name == "post_step":
+        from tests.golden.make_golden import post_input
+        st = post_input(p, st, CASES[name]["seed"])
+        O.post_step(p, st, P.default_post_params())
     out = dict(st)
     if lev is not None:
         out["buoy_ref_level"] = lev

@@ -106,3 +106,39 @@ def test_full_step(ref_model, oracle_lib, base_state):
     oracle_lib.step(p, st, P.PRESS_GS_LEX)
     names = F.PROGNOSTIC + F.NCOPIES + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION
     assert_same(ref_model.state(names), st, names)
+
+
+def test_post_step(ref_model, oracle_lib, base_state):
+    """The passes after RK4 with the reference's default knobs (cUranusModel.cpp:1218-1248): t
+    filter, boundary passes (with the species floor and the lid v, w) and the species clamp; every
+    written value identical, the clamp's counts equal and its sums equal up to the order of the
+    reference's OpenMP reduction."""
+    from tests.post_case import KNOB_SETS, POST_FIELDS, post_state
+    p = P.default_params()
+    st = post_state(S.perturb(base_state, p, seed=41), p, seed=42)
+    pp = KNOB_SETS["defaults"][1]()
+    assert bool(pp.lid_vw == 2) == ref_model.geo_balance()
+    ref_model.load(st)
+    ra, rc = ref_model.post_step(pp)
+    oa, oc = oracle_lib.post_step(p, st, pp)
+    assert_same(ref_model.state(POST_FIELDS), st, POST_FIELDS)
+    assert np.array_equal(rc, oc) and rc.sum() > 0
+    assert np.allclose(ra, oa, rtol=1e-12, atol=0.0)
+
+
+@pytest.mark.parametrize("knobs", ["no_geo_balance_forms", "cubic_lid_open_phi"])
+def test_post_step_knob_sets(knobs):
+    """Other knob values (forms, taper, lid, floor, filters, an open phi seam): the reference reads
+    them from its environment once per process, so each set runs in a child process with that
+    environment; the child requires bit equality as above."""
+    import os
+    import subprocess
+    import sys
+    from oracle import ref
+    from tests.post_case import KNOB_SETS
+    if not ref.available():
+        pytest.skip("compiled reference (oracle/_ref) not present")
+    env = dict(os.environ, **KNOB_SETS[knobs][0])
+    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_post_knobs_child.py")
+    r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
