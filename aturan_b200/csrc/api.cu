@@ -676,7 +676,8 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
     pl.damp_t_horiz = pp->damp_t_horiz; pl.damp_t_vert = pp->damp_t_vert; pl.vel_shapiro = pp->vel_shapiro;
     pl.damp_t_j = pp->damp_t_j; pl.species_clamp = pp->species_clamp;
     // the clamp's partial sums borrow the pressure source's scratch (free between calls)
-    pl.nb = (int)std::min<size_t>(148 * 4, (fs - 2 * POST_NSP) / (2 * POST_NSP));
+    // one wave: 8 resident blocks of 256 threads on each of 148 SMs, shared by the 13 species
+    pl.nb = (int)std::min<size_t>(148 * 8 / POST_NSP, (fs - 2 * POST_NSP) / (2 * POST_NSP));
     pl.part = ctx->scratch;
     pl.out = ctx->scratch + (size_t)2 * POST_NSP * pl.nb;
     int nl;
@@ -1528,10 +1529,6 @@ int aturan_post_params_default(aturan_post_params* pp){
 int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells){
     if(!ctx || !pp) return ATURAN_E_INVALID;
     if(pp->abi_version != ATURAN_ABI_VERSION) return ATURAN_E_INVALID;
-    const Grid& g = ctx->g;
-    // the passes read four planes in from each end (BCForm's cubic); the k filter holds a row in
-    // 48 KB of shared memory
-    if(g.im < 4 || g.jm < 4 || g.km < 4 || g.km > 6144 || g.im > 65535 || g.jm > 65535) return ATURAN_E_UNSUPPORTED;
     return ctx->mixed ? run_post<float>(ctx, pp, clamp_added, clamp_cells) : run_post<double>(ctx, pp, clamp_added, clamp_cells);
 }
 

@@ -66,7 +66,14 @@ int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_
     int n = 0;
     auto filt = [&](S* x, bool ai, bool aj, bool ak, double strength){
         const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
-        if(ak){ post_filter_k_kernel<S><<<g.im * g.jm, 128, g.km * sizeof(double), st>>>(g, x, coeff, a.phi_periodic && g.km > 2); n++; }
+        if(ak){
+            const int sm = g.km * (int)sizeof(double);
+            static const bool big = (cudaFuncSetAttribute(post_filter_k_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          8192 * (int)sizeof(double)) == cudaSuccess) || (cudaGetLastError(), false);
+            (void)big;                                   // rows longer than 6144 need the opt-in size
+            post_filter_k_kernel<S><<<g.im * g.jm, 128, sm, st>>>(g, x, coeff, a.phi_periodic && g.km > 2);
+            n++;
+        }
         if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, coeff); n++; }
         if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, coeff); n++; }
     };
@@ -74,13 +81,13 @@ int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_
     if(pl.damp_t_vert != 0.0) filt(t, true, false, false, pl.damp_t_vert);
     if(pl.vel_shapiro != 0.0){ filt(a.u, true, true, true, pl.vel_shapiro); filt(a.v, true, true, true, pl.vel_shapiro);
                                filt(a.w, true, true, true, pl.vel_shapiro); }
-    post_bc_radius_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(a);
-    post_bc_theta_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(a);
-    post_bc_phi_kernel<S><<<(g.im * g.jm + 127) / 128, 128, 0, st>>>(a);
+    post_bc_radius_kernel<S><<<dim3(cols_k.x, g.jm, POST_NRAD), 128, 0, st>>>(a);
+    post_bc_theta_kernel<S><<<dim3(cols_k.x, g.im, POST_NTHZ + POST_NTHX), 128, 0, st>>>(a);
+    post_bc_phi_kernel<S><<<dim3((g.im * g.jm + 127) / 128, POST_NRAD), 128, 0, st>>>(a);
     n += 3;
     if(pl.species_clamp){
         post_clamp_kernel<S><<<dim3(pl.nb, POST_NSP), POST_CLAMP_NT, 0, st>>>(a, pl.part);
-        post_clamp_finish_kernel<<<1, 32, 0, st>>>(pl.part, pl.nb, pl.out);
+        post_clamp_finish_kernel<<<POST_NSP, POST_CLAMP_NT, 0, st>>>(pl.part, pl.nb, pl.out);
         n += 2;
     }
     return n;

@@ -96,119 +96,134 @@ __global__ void __launch_bounds__(128) post_filter_i_kernel(Grid g, S* x, double
 }
 
 // ---- bcRadius (BoundaryConditions.h:152-286), floorRadialSpecies and the lid v, w (BC_Uran.h:91-170) ----
+// One thread per (j, k) column of one field (blockIdx.z = the field's place in rad): the field's
+// two end values, then what the reference does afterwards to that same column -- u = 0 at the
+// ends (lid_u), the top taper and the lid form of v and w, the species floor. Every later step
+// reads and writes only its own field's column, so the fields run side by side.
 template <typename S>
 __global__ void __launch_bounds__(128) post_bc_radius_kernel(PostArgs<S> a){
     const Grid& g = a.g;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, n = blockIdx.z;
     if(k >= g.km) return;
     const int im = g.im;
-    const size_t pl = (size_t)g.jm * g.kp, o = gidx(g, 0, j, k);
-    auto at = [&](S* F, int i) -> S& { return F[o + (size_t)i * pl]; };
-#pragma unroll 1
-    for(int n = 0; n < POST_NRAD; n++){
-        S* F = a.rad[n];
-        const int fb = (a.bottom_form != 0 && n != 1) ? a.bottom_form : a.radius_form;
-        at(F, 0) = (S)post_form(fb, (double)at(F, 1), (double)at(F, 2), (double)at(F, 3));
-        at(F, im - 1) = (S)post_form(a.radius_form, (double)at(F, im - 2), (double)at(F, im - 3), (double)at(F, im - 4));
-    }
-    if(a.lid_u != 0){ at(a.u, 0) = (S)0.0; at(a.u, im - 1) = (S)0.0; }
-    if(a.top_taper != 0){
+    const size_t pl = (size_t)g.jm * g.kp;
+    S* F = a.rad[n] + gidx(g, 0, j, k);
+    auto at = [&](int i) -> S& { return F[(size_t)i * pl]; };
+    const int fb = (a.bottom_form != 0 && n != 1) ? a.bottom_form : a.radius_form;
+    // in the reference's order, through memory (the planes overlap when im < 5)
+    at(0) = (S)post_form(fb, (double)at(1), (double)at(2), (double)at(3));
+    at(im - 1) = (S)post_form(a.radius_form, (double)at(im - 2), (double)at(im - 3), (double)at(im - 4));
+    if(n == 1 && a.lid_u != 0){ at(0) = (S)0.0; at(im - 1) = (S)0.0; }
+    if(n == 2 || n == 3){                         // v, w
         const int l = im - 1;
-        at(a.v, l) = (S)0.0;
-        at(a.w, l) = (S)0.0;
-        if(a.top_taper == 2){
-            at(a.v, l - 1) = (S)((1.0 / 3.0) * (double)at(a.v, l - 3));
-            at(a.w, l - 1) = (S)((1.0 / 3.0) * (double)at(a.w, l - 3));
-            at(a.v, l - 2) = (S)((2.0 / 3.0) * (double)at(a.v, l - 3));
-            at(a.w, l - 2) = (S)((2.0 / 3.0) * (double)at(a.w, l - 3));
-        } else {
-            at(a.v, l - 1) = (S)((double)at(a.v, l - 1) * (1.0 / 3.0));
-            at(a.w, l - 1) = (S)((double)at(a.w, l - 1) * (1.0 / 3.0));
-            at(a.v, l - 2) = (S)((double)at(a.v, l - 2) * (2.0 / 3.0));
-            at(a.w, l - 2) = (S)((double)at(a.w, l - 2) * (2.0 / 3.0));
+        if(a.top_taper != 0){
+            at(l) = (S)0.0;
+            if(a.top_taper == 2){
+                at(l - 1) = (S)((1.0 / 3.0) * (double)at(l - 3));
+                at(l - 2) = (S)((2.0 / 3.0) * (double)at(l - 3));
+            } else {
+                at(l - 1) = (S)((double)at(l - 1) * (1.0 / 3.0));
+                at(l - 2) = (S)((double)at(l - 2) * (2.0 / 3.0));
+            }
         }
-    }
-    if(a.positive != 0){
-#pragma unroll 1
-        for(int n = 0; n < POST_NSP; n++){
-            S* F = a.sp[n];
-            if((double)at(F, 0) < 0.0) at(F, 0) = (S)((a.positive == 2) ? post_max0((double)at(F, 1)) : 0.0);
-            if((double)at(F, im - 1) < 0.0) at(F, im - 1) = (S)((a.positive == 2) ? post_max0((double)at(F, im - 2)) : 0.0);
-        }
-    }
-    if(a.lid_vw == 2 || a.lid_vw == 3){
-        const int A = im - 2, B = im - 3, Cc = im - 4, l = im - 1;
-        if(a.lid_vw == 2){
-            at(a.v, l) = (S)(2.0 * (double)at(a.v, A) - (double)at(a.v, B));
-            at(a.w, l) = (S)(2.0 * (double)at(a.w, A) - (double)at(a.w, B));
-        } else {
-            at(a.v, l) = (S)((double)at(a.v, Cc) - 3.0 * (double)at(a.v, B) + 3.0 * (double)at(a.v, A));
-            at(a.w, l) = (S)((double)at(a.w, Cc) - 3.0 * (double)at(a.w, B) + 3.0 * (double)at(a.w, A));
-        }
+        if(a.lid_vw == 2)
+            at(l) = (S)(2.0 * (double)at(l - 1) - (double)at(l - 2));
+        else if(a.lid_vw == 3)
+            at(l) = (S)((double)at(l - 3) - 3.0 * (double)at(l - 2) + 3.0 * (double)at(l - 1));
+    } else if(n >= 4 && n <= 16 && a.positive != 0){          // the twelve condensables and nh4sh
+        if((double)at(0) < 0.0) at(0) = (S)((a.positive == 2) ? post_max0((double)at(1)) : 0.0);
+        if((double)at(im - 1) < 0.0) at(im - 1) = (S)((a.positive == 2) ? post_max0((double)at(im - 2)) : 0.0);
     }
 }
 
-// ---- bcTheta (BoundaryConditions.h:293-391) ----
+// ---- bcTheta (BoundaryConditions.h:293-391): one thread per (i, k) column of one field; fields
+// 0..POST_NTHZ-1 are zeroed at the poles, the others extrapolated. ----
 template <typename S>
 __global__ void __launch_bounds__(128) post_bc_theta_kernel(PostArgs<S> a){
     const Grid& g = a.g;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y, n = blockIdx.z;
     if(k >= g.km) return;
     const int jm = g.jm;
     const size_t kp = (size_t)g.kp, o = gidx(g, i, 0, k);
-    auto at = [&](S* F, int j) -> S& { return F[o + (size_t)j * kp]; };
-#pragma unroll 1
-    for(int n = 0; n < POST_NTHZ; n++){ at(a.thz[n], 0) = (S)0.0; at(a.thz[n], jm - 1) = (S)0.0; }
-#pragma unroll 1
-    for(int n = 0; n < POST_NTHX; n++){
-        S* F = a.thx[n];
-        at(F, 0) = (S)post_form(a.pole_form, (double)at(F, 1), (double)at(F, 2), (double)at(F, 3));
-        at(F, jm - 1) = (S)post_form(a.pole_form, (double)at(F, jm - 2), (double)at(F, jm - 3), (double)at(F, jm - 4));
+    if(n < POST_NTHZ){
+        S* F = a.thz[n] + o;
+        F[0] = (S)0.0;
+        F[(size_t)(jm - 1) * kp] = (S)0.0;
+        return;
     }
+    S* F = a.thx[n - POST_NTHZ] + o;
+    auto at = [&](int j) -> S& { return F[(size_t)j * kp]; };
+    at(0) = (S)post_form(a.pole_form, (double)at(1), (double)at(2), (double)at(3));     // in order (jm < 5 overlaps)
+    at(jm - 1) = (S)post_form(a.pole_form, (double)at(jm - 2), (double)at(jm - 3), (double)at(jm - 4));
 }
 
-// ---- bcPhi (BoundaryConditions.h:398-455, without the seam damping) ----
+// ---- bcPhi (BoundaryConditions.h:398-455, without the seam damping): one thread per (i, j) row
+// of one field ----
 template <typename S>
 __global__ void __launch_bounds__(128) post_bc_phi_kernel(PostArgs<S> a){
     const Grid& g = a.g;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;      // row (i, j)
     if(r >= g.im * g.jm) return;
-    const size_t o = (size_t)r * g.kp;
     const int km = g.km;
-#pragma unroll 1
-    for(int n = 0; n < POST_NRAD; n++){
-        S* F = a.rad[n] + o;
-        if(a.phi_periodic) F[km - 1] = F[0];
-        else {
-            const double lo = C43 * (double)F[1] - C13 * (double)F[2];
-            const double hi = C43 * (double)F[km - 2] - C13 * (double)F[km - 3];
-            const S y = (S)(0.5 * (lo + hi));
-            F[0] = y;
-            F[km - 1] = y;
-        }
+    S* F = a.rad[blockIdx.y] + (size_t)r * g.kp;
+    if(a.phi_periodic) F[km - 1] = F[0];
+    else {
+        const double lo = C43 * (double)F[1] - C13 * (double)F[2];
+        const double hi = C43 * (double)F[km - 2] - C13 * (double)F[km - 3];
+        const S y = (S)(0.5 * (lo + hi));
+        F[0] = y;
+        F[km - 1] = y;
     }
 }
 
 // ---- clampNegativeSpecies (BC_Uran.h:110-128) ----
-// Block (b, n) clamps a grid-stride share of species n's stored cells and writes its clipped sum
-// and count (as doubles, exact for any count below 2^53) to part[2 (n nb + b)] in a fixed tree
-// order; post_clamp_finish_kernel adds a species' nb partials in block order. Deterministic run
-// to run; the reference's OpenMP reduction order differs, so the sum agrees to its rounding.
+// Block (b, n) clamps a block-stride share of species n's padded field, read as 16-byte vectors
+// (a vector never straddles a row: the row pitch is a multiple of 32 values), four vectors in
+// flight per thread; values in the row padding are skipped. It writes its clipped sum and count
+// (as doubles, exact for any count below 2^53) to part[2 (n nb + b)] in a fixed tree order, and
+// post_clamp_finish_kernel adds a species' nb partials in a fixed order. Deterministic run to
+// run; the reference's OpenMP reduction order differs, so the sum agrees to its rounding.
 constexpr int POST_CLAMP_NT = 256;
+template <typename S> struct Vec16;
+template <> struct Vec16<float>  { using T = float4;  static constexpr int N = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int N = 2; };
+
+template <typename S>
+__device__ __forceinline__ void post_clamp_one(S* R, int k, int km, double x, double& s, double& c){
+    if(k < km && !(x >= 0.0)){                     // catches a NaN too
+        if(isfinite(x)){ s -= x; c += 1.0; }
+        R[k] = (S)0.0;
+    }
+}
+
 template <typename S>
 __global__ void __launch_bounds__(POST_CLAMP_NT) post_clamp_kernel(PostArgs<S> a, double* part){
+    using V = typename Vec16<S>::T;
+    constexpr int NV = Vec16<S>::N, U = 4;
     const Grid& g = a.g;
     const int n = blockIdx.y, nb = gridDim.x;
     S* F = a.sp[n];
-    const size_t N = (size_t)g.im * g.jm * g.km;
+    const int vpr = g.kp / NV;                                    // vectors per row
+    const long long nvec = (long long)g.im * g.jm * vpr;
+    const long long step = (long long)nb * POST_CLAMP_NT;
     double s = 0.0, c = 0.0;
-    for(size_t e = (size_t)blockIdx.x * POST_CLAMP_NT + threadIdx.x; e < N; e += (size_t)nb * POST_CLAMP_NT){
-        const size_t r = e / (size_t)g.km;
-        const size_t o = r * g.kp + (e - r * g.km);
-        const double x = (double)F[o];
-        if(!(x >= 0.0)){                           // catches a NaN too
-            if(isfinite(x)){ s -= x; c += 1.0; }
-            F[o] = (S)0.0;
+    for(long long q0 = (long long)blockIdx.x * POST_CLAMP_NT + threadIdx.x; q0 < nvec; q0 += U * step){
+        V v[U];
+#pragma unroll
+        for(int u = 0; u < U; u++){
+            const long long q = q0 + u * step;
+            if(q < nvec) v[u] = reinterpret_cast<const V*>(F)[q];
+        }
+#pragma unroll
+        for(int u = 0; u < U; u++){
+            const long long q = q0 + u * step;
+            if(q >= nvec) break;
+            const long long r = q / vpr;
+            const int k0 = (int)(q - r * vpr) * NV;
+            S* R = F + r * g.kp;
+            const S* e = reinterpret_cast<const S*>(&v[u]);
+#pragma unroll
+            for(int m = 0; m < NV; m++) post_clamp_one(R, k0 + m, g.km, (double)e[m], s, c);
         }
     }
     __shared__ double ss[POST_CLAMP_NT], sc[POST_CLAMP_NT];
@@ -221,13 +236,19 @@ __global__ void __launch_bounds__(POST_CLAMP_NT) post_clamp_kernel(PostArgs<S> a
     if(threadIdx.x == 0){ part[2 * ((size_t)n * nb + blockIdx.x)] = ss[0]; part[2 * ((size_t)n * nb + blockIdx.x) + 1] = sc[0]; }
 }
 
-static __global__ void post_clamp_finish_kernel(const double* part, int nb, double* out){
-    const int n = threadIdx.x;
-    if(n >= POST_NSP) return;
+// One block per species: thread t adds partials t, t + 256, ... in order, then a fixed tree.
+static __global__ void __launch_bounds__(POST_CLAMP_NT) post_clamp_finish_kernel(const double* part, int nb, double* out){
+    const int n = blockIdx.x;
     double s = 0.0, c = 0.0;
-    for(int b = 0; b < nb; b++){ s += part[2 * ((size_t)n * nb + b)]; c += part[2 * ((size_t)n * nb + b) + 1]; }
-    out[n] = s;
-    out[POST_NSP + n] = c;
+    for(int b = threadIdx.x; b < nb; b += POST_CLAMP_NT){ s += part[2 * ((size_t)n * nb + b)]; c += part[2 * ((size_t)n * nb + b) + 1]; }
+    __shared__ double ss[POST_CLAMP_NT], sc[POST_CLAMP_NT];
+    ss[threadIdx.x] = s; sc[threadIdx.x] = c;
+    __syncthreads();
+    for(int st = POST_CLAMP_NT / 2; st > 0; st >>= 1){
+        if((int)threadIdx.x < st){ ss[threadIdx.x] += ss[threadIdx.x + st]; sc[threadIdx.x] += sc[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if(threadIdx.x == 0){ out[n] = ss[0]; out[POST_NSP + n] = sc[0]; }
 }
 
 }  // namespace aturan

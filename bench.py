@@ -223,6 +223,73 @@ def algorithmic_stage_bytes(precision):
     return total / 4 * N_CELLS
 
 
+def post_step_bytes(p, pp, e):
+    """Algorithmic bytes of one aturan_post_step with knobs pp and storage e bytes per value: every
+    value the passes must read or write once (the padding never counts)."""
+    im, jm, km = p.im, p.jm, p.km
+    N = im * jm * km
+    b = 0
+    if pp.damp_t_horiz != 0.0:
+        b += 2 * N                                   # t along k (and j): read and write
+        if pp.damp_t_j:
+            b += 2 * N
+    if pp.damp_t_vert != 0.0:
+        b += 2 * N
+    if pp.vel_shapiro != 0.0:
+        b += 3 * 3 * 2 * N                           # u, v, w along k, j, i
+    nrad, nthx, nthz, nsp = 22, 16, 6, 13
+    b += nrad * 6 * jm * km                          # radius: planes 1, 2, im-2, im-3 read, 0 and im-1 written
+    b += (nthx * 6 + nthz * 2) * im * km             # theta: rows 1, 2, jm-2, jm-3 read, 0 and jm-1 written
+    b += nrad * 2 * im * jm                          # phi: k = 0 read, k = km-1 written
+    if pp.species_clamp:
+        b += nsp * N                                 # every species value read (writes: the clipped few)
+    return b * e
+
+
+def post_step_timing(api, P, S, torch, precision, calls=20):
+    """aturan_post_step with the reference's default knobs at 41x181x361: device time per call (CUDA
+    events on the context's stream, mean over `calls` after 3 warm-up calls), its algorithmic bytes
+    and GB/s, and the compiled reference's same passes on the host cores when it is present."""
+    prec = P.MIXED if precision == "mixed" else P.FP64
+    p = P.default_params(precision=prec)
+    pp = P.default_post_params()
+    ctx = api.Context(p)
+    ctx.upload_state(S.synthetic_state(p, seed=20261205))
+    s = torch.cuda.ExternalStream(ctx.stream)
+    for _ in range(3):
+        ctx.post_step(pp)
+    ctx.synchronize()
+    ctx.profile(False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(calls):
+        ctx.post_step(pp)
+    e1.record(s)
+    e1.synchronize()
+    launches = ctx.profile_read()["post"][0] // calls
+    ctx.close()
+    ms = e0.elapsed_time(e1) / calls
+    alg = post_step_bytes(p, pp, 4 if precision == "mixed" else 8)
+    peak, peak_kind = peaks()
+    out = {"ms": ms, "launches": launches, "alg_bytes": alg, "achieved_gbs": alg / (ms / 1e3) / 1e9,
+           "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_source": f"{peak_kind} hbm_gbs",
+           "what": "t filter along k, radius/theta/phi boundary passes with the species floor and lid v, w, "
+                   "species clamp (the reference's default knobs), 41x181x361; 20 calls, state > L2"}
+    try:
+        from oracle import ref as R
+        if R.available():
+            m = R.Ref.get_instance()
+            m.post_step(pp)
+            t0 = time.perf_counter()
+            for _ in range(5):
+                m.post_step(pp)
+            out["cpu_reference_ms"] = (time.perf_counter() - t0) / 5 * 1e3
+            out["cpu_reference_cores"] = os.cpu_count()
+    except Exception as ex:               # reported, never silently replaced
+        out["cpu_reference_ms"] = f"{type(ex).__name__}: {ex}"
+    return out
+
+
 def cpu_reference_step_time(nsteps, press, budget_s=120.0):
     """Time the reference's own step on the host cores after one untimed warm-up step; at most
     nsteps steps and no more than fit in budget_s. Returns (seconds/step, kind, cores, note, n)."""
@@ -303,6 +370,8 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="only the warm-up and the K timed steps (for ncu); prints a short line")
     ap.add_argument("--grid", default="41x181x361", help="IxJxK of the shell (profiling cases)")
+    ap.add_argument("--post-step", action="store_true",
+                    help="only the passes after RK4 (aturan_post_step): prints the post_step object")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -321,6 +390,11 @@ def main():
         torch.cuda.set_device(0)
 
     from aturan_b200 import api, params as P, replicas, state as S
+    if args.post_step:
+        if rank == 0:
+            print(json.dumps({"post_step": post_step_timing(api, P, S, torch, args.precision),
+                              "precision": args.precision}), flush=True)
+        return
     prec = P.MIXED if args.precision == "mixed" else P.FP64
     gi, gj, gk = (int(x) for x in args.grid.lower().split("x"))
     p = P.default_params(gi, gj, gk, precision=prec)
@@ -431,6 +505,13 @@ def main():
         except Exception as ex:          # reported, never silently replaced
             adjoint = {"error": f"{type(ex).__name__}: {ex}"}
 
+    post = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            post = post_step_timing(api, P, S, torch, args.precision)
+        except Exception as ex:          # reported, never silently replaced
+            post = {"error": f"{type(ex).__name__}: {ex}"}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -465,6 +546,7 @@ def main():
                     "d2h_bytes_per_step": len(out_names) * fbytes, "steps": E},
             "clocks": clk,
             "adjoint": adjoint,
+            "post_step": post,
             "cpu_baseline": cpu,
         }
         if accuracy is not None:

@@ -27,8 +27,8 @@ def post_state(st, p, seed):
         scale = max(float(np.abs(a).max()), 1e-12)
         m = rng.random(shape) < 0.01
         a[m] = -scale * rng.random(int(m.sum()))
-    s["h2o"][5, 7, 11] = np.nan
-    s["nh3_ice"][0, 3, 4] = np.nan
+    s["h2o"][p.im // 2, p.jm // 2, p.km // 2] = np.nan
+    s["nh3_ice"][0, p.jm // 3, p.km // 4] = np.nan
     return s
 
 

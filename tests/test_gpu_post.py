@@ -33,7 +33,7 @@ def run_gpu(p, st, pp):
     return out, added, cells
 
 
-@pytest.mark.parametrize("shape", [(41, 181, 361), (9, 13, 17)])
+@pytest.mark.parametrize("shape", [(41, 181, 361), (9, 13, 17), (5, 5, 5)])
 @pytest.mark.parametrize("knobs", list(KNOB_SETS))
 def test_post_step_fp64_matches_oracle(oracle_lib, knobs, shape):
     p = P.default_params(*shape)
