@@ -14,9 +14,9 @@ FLUXES = ["massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "th
 POST_FIELDS = ["t", "u", "v", "w"] + SPECIES + FLUXES
 
 
-def post_state(st, p, seed):
+def post_state(st, p, seed, nan=True):
     """st with seeded fluxes, negative species values in ~1 % of the cells (boundary planes
-    included) and one NaN, so the floor and the clamp have work."""
+    included) and (nan=True) two NaNs, so the floor and the clamp have work."""
     rng = np.random.default_rng(seed)
     s = {n: np.array(a, dtype=np.float64, copy=True) for n, a in st.items()}
     shape = (p.im, p.jm, p.km)
@@ -27,8 +27,9 @@ def post_state(st, p, seed):
         scale = max(float(np.abs(a).max()), 1e-12)
         m = rng.random(shape) < 0.01
         a[m] = -scale * rng.random(int(m.sum()))
-    s["h2o"][p.im // 2, p.jm // 2, p.km // 2] = np.nan
-    s["nh3_ice"][0, p.jm // 3, p.km // 4] = np.nan
+    if nan:
+        s["h2o"][p.im // 2, p.jm // 2, p.km // 2] = np.nan
+        s["nh3_ice"][0, p.jm // 3, p.km // 4] = np.nan
     return s
 
 

@@ -82,6 +82,35 @@ def test_post_step_mixed_within_fp32_rounding(oracle_lib, knobs):
     assert np.allclose(ga, oa, rtol=1e-5, atol=0.0), (ga, oa)
 
 
+def test_iteration_sequence_matches_oracle(oracle_lib):
+    """Two iterations of a driver's sequence -- aturan_step (GS pressure), aturan_post_step,
+    aturan_restore_ncopies -- against the oracle's same calls, FP64, on the config-3 grid. Every
+    prognostic field and n-copy, boundary planes included, within 1e-10 of its maximum: the
+    saturation adjustment's last-bit exp/log differences (the one-step bar, 1e-11) carried
+    through two iterations and the post passes."""
+    from aturan_b200 import fields as F
+    from aturan_b200.api import Context
+    p = P.default_params(41, 91, 181)
+    st = post_state(S.synthetic_state(p, seed=61), p, seed=62, nan=False)
+    pp = P.default_post_params()
+    ctx = Context(p)
+    ctx.upload_state(st)
+    for _ in range(2):
+        ctx.step(P.PRESS_GS_LEX)
+        ctx.post_step(pp)
+        ctx.restore_ncopies(1.0)
+        oracle_lib.step(p, st, P.PRESS_GS_LEX)
+        oracle_lib.post_step(p, st, pp)
+        for n in F.PROGNOSTIC:                     # restoreVar(1.0)
+            st[n + "n"] = st[n].copy()
+    names = F.PROGNOSTIC + F.NCOPIES + ["p_dyn"]
+    g = ctx.download_state(names)
+    ctx.close()
+    for n in names:
+        scale = max(float(np.abs(st[n]).max()), 1e-300)
+        assert np.abs(g[n] - st[n]).max() <= 1e-10 * scale, (n, np.abs(g[n] - st[n]).max() / scale)
+
+
 def test_post_step_rejects_bad_version():
     from aturan_b200.api import AturanError, Context, E_INVALID
     p = P.default_params(9, 13, 17)
