@@ -358,7 +358,7 @@ def run_reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -612,6 +612,18 @@ def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
         out[f"step{n}"] = errs
         out[f"step{n}_p99.99"] = p9999
         out[f"step{n}_rel_l2"] = l2
+        if n == 10:
+            # the FP64 step with tree-ordered level sums against the bit-exact one: two FP64 paths
+            # that differ by rounding only (~1e-13 in the level means), so what separates them
+            # after 10 steps is the reference algorithm's own sensitivity (threshold tests)
+            tre, trq = {}, {}
+            for f in ("t", "u", "v", "w", "p_dyn"):
+                a, b = c64t.download(f)[I], c64.download(f)[I]
+                s_ = np.abs(b).max()
+                d = np.abs(a - b) / (s_ if s_ > 0 else 1.0)
+                tre[f] = float(d.max())
+                trq[f] = float(np.quantile(d, 0.9999))
+            out["fp64_tree_vs_fp64_step10"] = {"max": tre, "p99.99": trq}
     c64.close()
     c32.close()
     c64t.close()
