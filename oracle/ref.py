@@ -67,8 +67,9 @@ class Ref:
         L.ref_pressure_shared.argtypes = [ctypes.c_int]
         L.ref_satadj.argtypes = [ctypes.c_int]
         L.ref_hydro.argtypes = [ctypes.c_int]
-        L.ref_damp_wiggles.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
-        L.ref_clamp_species.argtypes = [vp, vp]
+        if hasattr(L, "ref_damp_wiggles"):       # a harness built before the post-step entry points lacks them
+            L.ref_damp_wiggles.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+            L.ref_clamp_species.argtypes = [vp, vp]
         L.ref_set_quiet(1 if quiet else 0)
         self.L = L
         self.path = path
