@@ -67,11 +67,14 @@ int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_
     auto filt = [&](S* x, bool ai, bool aj, bool ak, double strength){
         const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
         if(ak){
-            const int sm = g.km * (int)sizeof(double);
+            // four rows (warps) per block while they fit the default 48 KB, else one row per block
+            // with the opt-in size (rows of up to 8192 values)
+            const int R = 4 * g.km * (int)sizeof(double) <= 48 * 1024 ? 4 : 1;
+            const int sm = R * g.km * (int)sizeof(double), rows = g.im * g.jm;
             static const bool big = (cudaFuncSetAttribute(post_filter_k_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                           8192 * (int)sizeof(double)) == cudaSuccess) || (cudaGetLastError(), false);
-            (void)big;                                   // rows longer than 6144 need the opt-in size
-            post_filter_k_kernel<S><<<g.im * g.jm, 128, sm, st>>>(g, x, coeff, a.phi_periodic && g.km > 2);
+            (void)big;
+            post_filter_k_kernel<S><<<(rows + R - 1) / R, dim3(32, R), sm, st>>>(g, x, coeff, a.phi_periodic && g.km > 2, rows);
             n++;
         }
         if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, coeff); n++; }

@@ -51,17 +51,21 @@ __device__ __forceinline__ double post_max0(double x){ return (0.0 < x) ? x : 0.
 
 // ---- damp_wiggles (lib/Utils.cpp:224-317), one axis per launch ----
 
-// Along k: one block per (i, j) row, the row's old values in shared memory. With the periodic
-// seam the ring is k = 0..km-2 and k = km-1 takes the new k = 0; otherwise k wraps over all km.
+// Along k: one warp per (i, j) row (blockDim.y rows per block), the row's old values in the warp's
+// own slice of shared memory, ~km/32 loads in flight per lane. With the periodic seam the ring is
+// k = 0..km-2 and k = km-1 takes the new k = 0; otherwise k wraps over all km.
 template <typename S>
-__global__ void __launch_bounds__(128) post_filter_k_kernel(Grid g, S* x, double coeff, int seam){
-    extern __shared__ double row[];
-    const size_t o = (size_t)blockIdx.x * g.kp;
+__global__ void __launch_bounds__(128) post_filter_k_kernel(Grid g, S* x, double coeff, int seam, int rows){
+    extern __shared__ double sm[];
+    const int r = blockIdx.x * blockDim.y + threadIdx.y;
+    if(r >= rows) return;                          // a whole warp: only warp-level syncs below
     const int km = g.km;
-    for(int k = threadIdx.x; k < km; k += blockDim.x) row[k] = (double)x[o + k];
-    __syncthreads();
+    double* row = sm + (size_t)threadIdx.y * km;
+    const size_t o = (size_t)r * g.kp;
+    for(int k = threadIdx.x; k < km; k += 32) row[k] = (double)x[o + k];
+    __syncwarp();
     const int k_end = seam ? km - 1 : km;
-    for(int k = threadIdx.x; k < k_end; k += blockDim.x){
+    for(int k = threadIdx.x; k < k_end; k += 32){
         const int km1 = seam ? (k == 0 ? km - 2 : k - 1) : (k - 1 + km) % km;
         const int kp1 = seam ? (k == km - 2 ? 0 : k + 1) : (k + 1) % km;
         const double c = row[k];
@@ -110,10 +114,29 @@ __global__ void __launch_bounds__(128) post_bc_radius_kernel(PostArgs<S> a){
     S* F = a.rad[n] + gidx(g, 0, j, k);
     auto at = [&](int i) -> S& { return F[(size_t)i * pl]; };
     const int fb = (a.bottom_form != 0 && n != 1) ? a.bottom_form : a.radius_form;
-    // in the reference's order, through memory (the planes overlap when im < 5)
-    at(0) = (S)post_form(fb, (double)at(1), (double)at(2), (double)at(3));
-    at(im - 1) = (S)post_form(a.radius_form, (double)at(im - 2), (double)at(im - 3), (double)at(im - 4));
-    if(n == 1 && a.lid_u != 0){ at(0) = (S)0.0; at(im - 1) = (S)0.0; }
+    const bool species = n >= 4 && n <= 16;        // the twelve condensables and nh4sh
+    if(im >= 8){
+        // planes 1..3 and im-4..im-2 are disjoint from each other and from 0 and im-1: every
+        // value is loaded up front (the third plane only for the cubic form), one round trip
+        auto cubic = [](int f){ return f != 0 && f != 1 && f != 2; };
+        const double b1 = (double)at(1), b2 = (double)at(2), b3 = cubic(fb) ? (double)at(3) : 0.0;
+        const double t1 = (double)at(im - 2), t2 = (double)at(im - 3);
+        const double t3 = cubic(a.radius_form) ? (double)at(im - 4) : 0.0;
+        S y0 = (S)post_form(fb, b1, b2, b3), yl = (S)post_form(a.radius_form, t1, t2, t3);
+        if(n == 1 && a.lid_u != 0){ y0 = (S)0.0; yl = (S)0.0; }
+        if(species && a.positive != 0){          // the floor reads planes 1 and im-2, unchanged
+            if((double)y0 < 0.0) y0 = (S)((a.positive == 2) ? post_max0(b1) : 0.0);
+            if((double)yl < 0.0) yl = (S)((a.positive == 2) ? post_max0(t1) : 0.0);
+        }
+        at(0) = y0;
+        at(im - 1) = yl;
+        if(n != 2 && n != 3) return;
+    } else {
+        // in the reference's order, through memory (the planes overlap when im < 8)
+        at(0) = (S)post_form(fb, (double)at(1), (double)at(2), (double)at(3));
+        at(im - 1) = (S)post_form(a.radius_form, (double)at(im - 2), (double)at(im - 3), (double)at(im - 4));
+        if(n == 1 && a.lid_u != 0){ at(0) = (S)0.0; at(im - 1) = (S)0.0; }
+    }
     if(n == 2 || n == 3){                         // v, w
         const int l = im - 1;
         if(a.top_taper != 0){
@@ -130,7 +153,7 @@ __global__ void __launch_bounds__(128) post_bc_radius_kernel(PostArgs<S> a){
             at(l) = (S)(2.0 * (double)at(l - 1) - (double)at(l - 2));
         else if(a.lid_vw == 3)
             at(l) = (S)((double)at(l - 3) - 3.0 * (double)at(l - 2) + 3.0 * (double)at(l - 1));
-    } else if(n >= 4 && n <= 16 && a.positive != 0){          // the twelve condensables and nh4sh
+    } else if(species && a.positive != 0){
         if((double)at(0) < 0.0) at(0) = (S)((a.positive == 2) ? post_max0((double)at(1)) : 0.0);
         if((double)at(im - 1) < 0.0) at(im - 1) = (S)((a.positive == 2) ? post_max0((double)at(im - 2)) : 0.0);
     }
