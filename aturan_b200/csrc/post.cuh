@@ -5,12 +5,12 @@
 // the species clamp (BC_Uran.h:91-128).
 //
 // All of it is streaming work on a few planes of the state, bound by HBM. The filters update a
-// field in place: along k one block holds a row in shared memory; along j and i one thread walks
+// field in place: along k one warp holds a row in shared memory; along j and i one thread walks
 // a column, keeping the old values of the cell and its lower neighbour in registers, so every old
 // value is read before it is overwritten, as the reference's copy of the field guarantees. The
-// boundary passes are column-local (radius: per (j,k), theta: per (i,k), phi: per (i,j)), so a
-// thread applies every step of its column in the reference's order, and one launch per pass
-// keeps the reference's order between passes. Arithmetic is FP64 on the stored values (FP32
+// boundary passes are column-local (radius: per (j,k), theta: per (i,k), phi: per (i,j)) and
+// field-local, so a thread applies every step of one field's column in the reference's order,
+// and one launch per pass keeps the reference's order between passes. Arithmetic is FP64 on the stored values (FP32
 // storage in the mixed form is widened, computed in FP64 and rounded back).
 #pragma once
 #include "common.cuh"
@@ -32,10 +32,10 @@ struct PostPlan {
 template <typename S>
 struct PostArgs {
     Grid g;
-    S* rad[POST_NRAD];           // radius and phi passes; rad[1] is u
+    S* rad[POST_NRAD];           // radius and phi passes: t, u, v, w, the species (4..16), the fluxes
     S* thx[POST_NTHX];           // theta pass, extrapolated to the poles
     S* thz[POST_NTHZ];           // theta pass, zeroed at the poles (v, w first)
-    S* sp[POST_NSP];             // species: floor and clamp, in BC_Uran.h:83-89's order
+    S* sp[POST_NSP];             // species for the clamp, in BC_Uran.h:83-89's order
     S *u, *v, *w;
     int radius_form, bottom_form, pole_form, lid_u, top_taper, lid_vw, positive, phi_periodic;
 };
