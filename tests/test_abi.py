@@ -80,3 +80,6 @@ def test_invalid_parameters_rejected():
     p = P.default_params(km=18)              # km-1 odd: colours would not alternate across the seam
     assert L.aturan_ctx_create(ctypes.byref(p), ctypes.byref(h)) == api.E_UNSUPPORTED
     assert L.aturan_ctx_create(None, ctypes.byref(h)) == api.E_INVALID
+    pp = P.default_post_params()
+    assert L.aturan_post_step(None, ctypes.byref(pp), None, None) == api.E_INVALID
+    assert L.aturan_post_params_default(None) == api.E_INVALID
