@@ -70,6 +70,7 @@ class Oracle:
             ("oracle_rhs_cell", [P, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             ("oracle_set_threads", [ctypes.c_int], None),
             ("oracle_post_step", [P, vp, P, vp, vp], ctypes.c_int),
+            ("oracle_mca", [P, vp], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -178,3 +179,7 @@ class Oracle:
         assert self.L.oracle_post_step(self._p(p), field_ptrs(state), self._p(pp), added.ctypes.data,
                                        cells.ctypes.data) == 0
         return added, cells
+
+    def mca(self, p, state):
+        """The moist convective adjustment (default knobs) on the state in place."""
+        assert self.L.oracle_mca(self._p(p), field_ptrs(state)) == 0

@@ -1804,3 +1804,276 @@ int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post
     }
     return 0;
 }
+
+/* ---- MoistConvectiveAdjustment<cUranusModel>::run (ConvectiveAdjustment.h:402-849) ----
+ * With the reference's default knobs: MCA_LEDOUX 1, MCA_LOADING 1, MCA_RELAX 1, MCA_SMOOTH 0
+ * (cUranusModel.h:572), MCA_PASSES 64, MCA_PHASE off (SATADJ_BERGERON = 2, cUranusModel.h:586),
+ * MCA_INTERIOR 1 (:566), no SeaMount; the gas list and the NH4SH tracer of
+ * cUranusModel.cpp:1276-1290. Columns are independent, so they run in parallel. */
+#define MCA_NG 4
+
+static double mca_mx(double a, double b){ return (a < b) ? b : a; }            /* std::max(a, b) */
+
+static double* g_cp_H[3];   /* CpH2.h:66-75: the table's running integral, H[0] = cp[0] T_LO */
+static const double* cp_H_table(int mode){
+    if(g_cp_H[mode]) return g_cp_H[mode];
+    const double* t = cp_table(mode);
+    double* H = (double*)malloc(sizeof(double) * g_cp_n);
+    H[0] = t[0] * CP_T_LO;
+    for(int i = 1; i < g_cp_n; i++) H[i] = H[i-1] + 0.5 * CP_DT * (t[i] + t[i-1]);
+    g_cp_H[mode] = H;
+    return H;
+}
+
+/* CpH2.h:94-101 */
+static double mca_enth_h2(const aturan_params* p, double T){
+    if(p->cp_h2_mode <= 0) return p->cp_h2 * T;
+    const double* t = cp_table(p->cp_h2_mode);
+    const double* H = cp_H_table(p->cp_h2_mode);
+    const int n = g_cp_n;
+    if(T <= CP_T_LO) return t[0] * T;
+    if(T >= CP_T_HI) return H[n-1] + t[n-1] * (T - CP_T_HI);
+    const double x = (T - CP_T_LO) / CP_DT;
+    int i = (int)x; if(i > n - 2) i = n - 2;
+    const double fr = x - i;
+    return H[i] + CP_DT * fr * (t[i] + 0.5 * fr * (t[i+1] - t[i]));
+}
+
+/* CpH2.h:135-142 (Lapse::enth) */
+static double mca_enth(const aturan_params* p, double T){
+    if(!p->cp_dyn) return p->cp_mix * T;
+    const double hh = mca_enth_h2(p, T);
+    if(p->cp_gas) return (p->r_h2 * hh + (p->r_he * p->cp_he + p->r_ch4 * p->cp_ch4) * T) / (p->r_h2 + p->r_he + p->r_ch4);
+    return (p->cp_mix - (p->r_h2 / p->r_mix) * p->cp_h2) * T + (p->r_h2 / p->r_mix) * hh;
+}
+
+/* CpH2.h:146-157 (enth_inv: Newton from T0) */
+static double mca_enth_inv(const aturan_params* p, double h, double T0){
+    if(!p->cp_dyn) return h / p->cp_mix;
+    double T = (T0 > 0.0) ? T0 : h / p->cp_mix;
+    for(int it = 0; it < 30; it++){
+        const double f = mca_enth(p, T) - h, c = oracle_cp_lapse(p, T);
+        const double dT = f / c;
+        T -= dT; if(T < 1.0) T = 1.0;
+        if(fabs(dT) < 1.0e-10 * T) break;
+    }
+    return T;
+}
+
+typedef struct {
+    const aturan_params* p;
+    const aturan_gas* G[MCA_NG];
+    double L_tr;                       /* the NH4SH tracer's heat (ep 0, condensed) */
+} mca_ctx;
+
+/* ConvectiveAdjustment.h:437-450 with the phase split off */
+static double mca_qsat(const aturan_gas* s, double T, double pr){
+    const double E = (T >= s->t_0) ? svp(T, s->C, s->L0, s->R, s->del_alf, s->del_bet)
+                                   : svp(T, s->C_i, s->L0_i, s->R, s->del_alf_i, s->del_bet_i);
+    const double q = s->ep * E / pr;
+    return isfinite(q) ? q : 0.0;
+}
+static double mca_lat(const aturan_gas* s, double T){ return T >= s->t_0 ? s->lv : s->ls; }
+
+static double mca_fof(const mca_ctx* M, double TT, double hL, const double* qt, double pr, double z){
+    double f = mca_enth(M->p, TT) + M->p->g * z - hL;
+    for(int g = 0; g < MCA_NG; g++) f -= mca_lat(M->G[g], TT) * mca_mx(0.0, qt[g] - mca_qsat(M->G[g], TT, pr));
+    return f;
+}
+
+/* :455-488, the equilibrium of (hL, qt) at (p, z) */
+static int mca_equil(const mca_ctx* M, double hL, const double* qt, double pr, double z, double* T, double* cond){
+    const aturan_params* p = M->p;
+    const double cp = p->cp_mix, grav = p->g, tol_T = 1.0e-10;
+    const double T_lo = p->cp_dyn ? mca_enth_inv(p, hL - grav * z, 0.0) : (hL - grav * z) / cp;
+    if(!(T_lo > 0.0) || !(pr > 0.0)) return 0;
+    int any = 0;
+    for(int g = 0; g < MCA_NG; g++) if(qt[g] > mca_qsat(M->G[g], T_lo, pr)){ any = 1; break; }
+    if(!any){ *T = T_lo; for(int g = 0; g < MCA_NG; g++) cond[g] = 0.0; return 1; }
+    double span = 0.0;
+    for(int g = 0; g < MCA_NG; g++) span += mca_mx(M->G[g]->lv, M->G[g]->ls) * mca_mx(0.0, qt[g]);
+    double a = T_lo, b = p->cp_dyn ? mca_enth_inv(p, mca_enth(p, T_lo) + span, T_lo) + 1.0e-9 : T_lo + span / cp + 1.0e-9;
+    double fa = mca_fof(M, a, hL, qt, pr, z), fb = mca_fof(M, b, hL, qt, pr, z);
+    int side = 0;
+    for(int it = 0; it < 60 && b - a > tol_T; it++){
+        double c = (fb - fa != 0.0) ? b - fb * (b - a) / (fb - fa) : 0.5 * (a + b);
+        if(!(c > a && c < b)) c = 0.5 * (a + b);
+        const double fc = mca_fof(M, c, hL, qt, pr, z);
+        if(fc < 0.0){ a = c; fa = fc; if(side == -1) fb *= 0.5; side = -1; }
+        else        { b = c; fb = fc; if(side == +1) fa *= 0.5; side = +1; }
+        if(fabs(fc) <= cp * tol_T){ a = b = c; break; }
+    }
+    *T = b;
+    for(int g = 0; g < MCA_NG; g++) cond[g] = mca_mx(0.0, qt[g] - mca_qsat(M->G[g], *T, pr));
+    return 1;
+}
+
+typedef struct {
+    int im;
+    double *T, *p, *z, *rho, *w, *hL, *qt, *qv, *qc, *qi, *qr, *Teq, *ceq;
+    char *touched, *eq_ok, *cen_u, *cen_m;
+} mca_col;
+
+static double mca_trE(const mca_ctx* M, const mca_col* C, int i){ double e = 0.0; e += M->L_tr * C->qr[i]; return e; }
+
+/* :613-624, Ledoux virtual temperature with condensate loading */
+static double mca_tv(const mca_ctx* M, const mca_col* C, double TT, const double* v_, const double* cnd, int i_tr){
+    double f = 1.0;
+    for(int g = 0; g < MCA_NG; g++){ f += v_[g] * (1.0 / M->G[g]->ep - 1.0); f -= cnd[g]; }
+    f -= C->qr[i_tr];                       /* NH4SH: ep 0, condensed */
+    return TT * f;
+}
+
+/* :627-644 */
+static int mca_unstable(const mca_ctx* M, mca_col* C, int a, int b, int* held, int* moist){
+    const double tol_K = 1.0e-7;
+    double Tp, pc[MCA_NG], pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
+    if(!mca_equil(M, C->hL[a] + mca_trE(M, C, a), &C->qt[a * MCA_NG], C->p[b], C->z[b], &Tp, pc)) return 0;
+    if(!C->eq_ok[b]){
+        if(!mca_equil(M, C->hL[b] + mca_trE(M, C, b), &C->qt[b * MCA_NG], C->p[b], C->z[b], &C->Teq[b], &C->ceq[b * MCA_NG])) return 0;
+        C->eq_ok[b] = 1;
+    }
+    const double Tb = C->Teq[b];
+    for(int g = 0; g < MCA_NG; g++) ec[g] = C->ceq[b * MCA_NG + g];
+    int wet = 0;
+    for(int g = 0; g < MCA_NG; g++){ pv[g] = C->qt[a * MCA_NG + g] - pc[g]; if(pc[g] > 0.0) wet = 1; ev[g] = C->qt[b * MCA_NG + g] - ec[g]; }
+    const double dTv = mca_tv(M, C, Tp, pv, pc, a) - mca_tv(M, C, Tb, ev, ec, b);
+    if(held) *held = (Tp - Tb > tol_K) && !(dTv > tol_K);
+    if(moist) *moist = wet;
+    return dTv > tol_K;
+}
+
+/* :645-661, cell q to equilibrium from hL / qt */
+static int mca_settle(const mca_ctx* M, mca_col* C, int q){
+    double TT, pc[MCA_NG];
+    if(!mca_equil(M, C->hL[q] + mca_trE(M, C, q), &C->qt[q * MCA_NG], C->p[q], C->z[q], &TT, pc)) return 0;
+    C->T[q] = TT;
+    C->Teq[q] = TT; C->eq_ok[q] = 1;
+    for(int g = 0; g < MCA_NG; g++){
+        const int x = q * MCA_NG + g;
+        C->ceq[x] = pc[g];
+        C->qv[x] = C->qt[x] - pc[g];
+        if(TT >= M->G[g]->t_0){ C->qc[x] = pc[g]; C->qi[x] = 0.0; } else { C->qi[x] = pc[g]; C->qc[x] = 0.0; }
+    }
+    C->touched[q] = 1;
+    return 1;
+}
+
+/* one column (j, k): :555-826 with MCA_SMOOTH 0 and MCA_RELAX 1 */
+static void mca_column(const mca_ctx* M, mca_col* C, double* const* f, int j, int k){
+    const aturan_params* p = M->p;
+    const int im = p->im, jm = p->jm, km = p->km;
+    static const int FV[MCA_NG] = { ATURAN_H2O, ATURAN_NH3, ATURAN_H2S, ATURAN_CH4 };
+    const int i0 = 1, i1 = im - 2;                          /* MCA_INTERIOR, no SeaMount */
+    if(i1 - i0 < 1) return;
+    const float hz = (float)(p->L_atm / (im - 1));          /* cUranusModel.h:1205-1208, km per level */
+    int ok = 1;
+    for(int i = i0; i <= i1 && ok; i++){
+        C->T[i] = f[ATURAN_T][IDX(i,j,k)] * p->t_ref;
+        C->p[i] = f[ATURAN_P_STAT][IDX(i,j,k)];
+        C->z[i] = (double)((float)i * hz) * 1.0e3;
+        double rr = p->r_mix;                               /* rho_at, cUranusModel.h:526-531 */
+        if(p->local_rho){ const double r_ = f[ATURAN_RHO_MIX][IDX(i,j,k)]; rr = (r_ > 0.0 && isfinite(r_)) ? r_ : p->r_mix; }
+        C->rho[i] = rr;
+        if(!(C->T[i] > 0.0) || !(C->p[i] > 0.0) || !(C->rho[i] > 0.0) || !isfinite(C->T[i] + C->p[i] + C->rho[i])) ok = 0;
+    }
+    if(!ok) return;
+    for(int i = i0; i <= i1 && ok; i++){
+        const double lo = (i > i0) ? 0.5 * (C->z[i-1] + C->z[i]) : C->z[i0];
+        const double hi = (i < i1) ? 0.5 * (C->z[i] + C->z[i+1]) : C->z[i1];
+        C->w[i] = C->rho[i] * (hi - lo);
+        if(!(C->w[i] > 0.0)) ok = 0;
+        double h = mca_enth(p, C->T[i]) + p->g * C->z[i];
+        for(int g = 0; g < MCA_NG; g++){
+            const int x = i * MCA_NG + g;
+            C->qv[x] = mca_mx(0.0, f[FV[g]][IDX(i,j,k)]) / C->rho[i];
+            C->qc[x] = mca_mx(0.0, f[FV[g] + 1][IDX(i,j,k)]) / C->rho[i];
+            C->qi[x] = mca_mx(0.0, f[FV[g] + 2][IDX(i,j,k)]) / C->rho[i];
+            C->qt[x] = C->qv[x] + C->qc[x] + C->qi[x];
+            h -= M->G[g]->lv * C->qc[x] + M->G[g]->ls * C->qi[x];
+        }
+        C->qr[i] = f[ATURAN_NH4SH][IDX(i,j,k)] / C->rho[i];
+        h -= M->L_tr * C->qr[i];
+        C->hL[i] = h;
+    }
+    if(!ok) return;
+    memset(C->touched, 0, im); memset(C->eq_ok, 0, im);
+    for(int i = i0; i < i1; i++){
+        int held = 0, moist = 0;
+        C->cen_u[i] = (char)mca_unstable(M, C, i, i + 1, &held, &moist);
+        C->cen_m[i] = (char)moist;
+    }
+    int passes = 0, changed = 1, fail = 0;
+    long layers = 0;
+    while(changed && passes < 64 && !fail){
+        changed = 0; passes++;
+        int i = i0;
+        while(i < i1 && !fail){
+            int moist = 0, uns;
+            if(passes == 1 && !C->touched[i] && !C->touched[i + 1]){ uns = C->cen_u[i]; moist = C->cen_m[i]; }
+            else uns = mca_unstable(M, C, i, i + 1, NULL, &moist);
+            if(!uns){ i++; continue; }
+            int a = i, b = i + 1;
+            for(;;){
+                double sw = 0.0, sh = 0.0, sq[MCA_NG] = {0.0, 0.0, 0.0, 0.0}, sr = 0.0;
+                for(int q = a; q <= b; q++){
+                    sw += C->w[q]; sh += C->w[q] * C->hL[q];
+                    for(int g = 0; g < MCA_NG; g++) sq[g] += C->w[q] * C->qt[q * MCA_NG + g];
+                    sr += C->w[q] * C->qr[q];
+                }
+                for(int q = a; q <= b; q++){
+                    C->hL[q] = sh / sw;
+                    for(int g = 0; g < MCA_NG; g++) C->qt[q * MCA_NG + g] = sq[g] / sw;
+                    C->qr[q] = sr / sw;
+                    if(!mca_settle(M, C, q)){ fail = 1; break; }
+                }
+                if(fail) break;
+                int ext = 0;
+                if(a > i0 && mca_unstable(M, C, a - 1, a, NULL, NULL)){ a--; ext = 1; }
+                if(b < i1 && mca_unstable(M, C, b, b + 1, NULL, NULL)){ b++; ext = 1; }
+                if(!ext) break;
+            }
+            layers += b - a + 1;
+            changed = 1;
+            i = b;
+        }
+    }
+    if(fail || layers == 0) return;                         /* nothing written */
+    for(int q = i0; q <= i1; q++){
+        if(!C->touched[q]) continue;
+        f[ATURAN_T][IDX(q,j,k)] = C->T[q] / p->t_ref;
+        for(int g = 0; g < MCA_NG; g++){
+            const int x = q * MCA_NG + g;
+            f[FV[g]][IDX(q,j,k)]     = C->qv[x] * C->rho[q];
+            f[FV[g] + 1][IDX(q,j,k)] = C->qc[x] * C->rho[q];
+            f[FV[g] + 2][IDX(q,j,k)] = C->qi[x] * C->rho[q];
+        }
+        f[ATURAN_NH4SH][IDX(q,j,k)] = C->qr[q] * C->rho[q];
+    }
+}
+
+int oracle_mca(const aturan_params* p, double* const* f){
+    mca_ctx M;
+    M.p = p;
+    M.G[0] = &p->gas[0]; M.G[1] = &p->gas[2]; M.G[2] = &p->gas[1]; M.G[3] = &p->gas[3];   /* H2O NH3 H2S CH4 */
+    M.L_tr = p->nh4sh_sync ? 4705.0 * log(10.0) * 8314.46 / 51.1114 : 0.0;             /* ChemistryUran.h:132 */
+    if(p->cp_h2_mode > 0){ cp_table(p->cp_h2_mode); cp_H_table(p->cp_h2_mode); }      /* built before the threads */
+    const int im = p->im, jm = p->jm, km = p->km;
+    #pragma omp parallel
+    {
+        mca_col C;
+        C.im = im;
+        double* buf = (double*)malloc(sizeof(double) * (size_t)im * (9 + 6 * MCA_NG));
+        char* cb = (char*)malloc((size_t)im * 4);
+        double* q = buf;
+        C.T = q; q += im; C.p = q; q += im; C.z = q; q += im; C.rho = q; q += im; C.w = q; q += im;
+        C.hL = q; q += im; C.qr = q; q += im; C.Teq = q; q += im; q += im;
+        C.qt = q; q += im * MCA_NG; C.qv = q; q += im * MCA_NG; C.qc = q; q += im * MCA_NG;
+        C.qi = q; q += im * MCA_NG; C.ceq = q; q += im * MCA_NG;
+        C.touched = cb; C.eq_ok = cb + im; C.cen_u = cb + 2 * im; C.cen_m = cb + 3 * im;
+        #pragma omp for collapse(2) schedule(dynamic, 8)
+        for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++) mca_column(&M, &C, f, j, k);
+        free(buf); free(cb);
+    }
+    return 0;
+}

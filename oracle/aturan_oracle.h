@@ -47,6 +47,9 @@ int oracle_step(const aturan_params* p, double* const* f, int press_kind, double
                 int max_sweeps, double tol, double* ref_level_out);
 void oracle_set_threads(int n);
 /* cUranusModel.cpp:1218-1248 after RK4: filters, boundary passes, species clamp */
+/* ConvectiveAdjustment.h:402-849 with the reference's default knobs, the gas list of
+ * cUranusModel.cpp:1276-1290 */
+int oracle_mca(const aturan_params* p, double* const* f);
 int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post_params* pp,
                      double* clamp_added, long* clamp_cells);
 

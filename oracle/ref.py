@@ -165,3 +165,7 @@ class Ref:
         n = L.ref_clamp_species(added.ctypes.data, cells.ctypes.data)
         assert n in (0, 13), n
         return added, cells
+
+    def mca(self):
+        """MoistConvectiveAdjustment as the model's loop calls it (cUranusModel.cpp:1276-1292)."""
+        assert self.L.ref_mca() == 0

@@ -56,6 +56,7 @@
 #include "SaturationAdjustmentUran.h"
 #include "ChemistryUran.h"
 #include "BC_Uran.h"
+#include "ConvectiveAdjustmentUran.h"
 #undef private
 
 namespace {
@@ -337,5 +338,33 @@ int ref_clamp_species(double* added, long* cells){
     return (int)m.clamp_added.size();
 }
 int ref_geo_balance(){ return cUranusModel::geo_balance() ? 1 : 0; }
+
+// The moist convective adjustment as cUranusModel.cpp:1276-1292 calls it: the same gas list
+// (H2O, NH3, H2S with its liquid set for both phases, CH4), NH4SH as a condensed tracer carrying
+// its formation heat when the NH4SH equilibrium is on, and chrom when ATURAN_CHROM is set.
+int ref_mca(){
+    Quiet q_;
+    cUranusModel& m = *g_model;
+    typedef MoistConvectiveAdjustmentUran::Gas Gas_;
+    typedef MoistConvectiveAdjustmentUran::Tracer Tr_;
+    std::vector<Gas_> gases = {
+        { "H2O", &m.h2o, &m.h2o_cloud, &m.h2o_ice, m.ep_h2o, m.lv_h2o, m.ls_h2o, m.t_0_h2o,
+          m.C_h2o, m.L0_h2o, m.R_h2o, m.del_alf_h2o, m.del_bet_h2o,
+          m.C_h2o_ice, m.L0_h2o_ice, m.del_alf_h2o_ice, m.del_bet_h2o_ice, m.t_00_h2o },
+        { "NH3", &m.nh3, &m.nh3_cloud, &m.nh3_ice, m.ep_nh3, m.lv_nh3, m.ls_nh3, m.t_0_nh3,
+          m.C_nh3, m.L0_nh3, m.R_nh3, m.del_alf_nh3, m.del_bet_nh3,
+          m.C_nh3_ice, m.L0_nh3_ice, m.del_alf_nh3_ice, m.del_bet_nh3_ice, m.t_00_nh3 },
+        { "H2S", &m.h2s, &m.h2s_cloud, &m.h2s_ice, m.ep_h2s, m.lv_h2s, m.ls_h2s, m.t_0_h2s,
+          m.C_h2s, m.L0_h2s, m.R_h2s, m.del_alf_h2s, m.del_bet_h2s,
+          m.C_h2s, m.L0_h2s, m.del_alf_h2s, m.del_bet_h2s, m.t_00_h2s },
+        { "CH4", &m.ch4, &m.ch4_cloud, &m.ch4_ice, m.ep_ch4, m.lv_ch4, m.ls_ch4, m.t_0_ch4,
+          m.C_ch4, m.L0_ch4, m.R_ch4, m.del_alf_ch4, m.del_bet_ch4,
+          m.C_ch4_ice, m.L0_ch4_ice, m.del_alf_ch4_ice, m.del_bet_ch4_ice, m.t_00_ch4 } };
+    const double L_nh4sh = ChemistryUran::nh4sh_eq() ? ChemistryUran::nh4sh_formation_heat() : 0.0;
+    std::vector<Tr_> tracers = { { "NH4SH", &m.nh4sh, 0.0, true, L_nh4sh } };
+    if(cUranusModel::chrom_on()) tracers.push_back({ "chrom", &m.chrom, 0.0, false, 0.0 });
+    MoistConvectiveAdjustmentUran(m, gases, tracers).run();
+    return 0;
+}
 
 }  // extern "C"

@@ -27,6 +27,8 @@ CASES = {
     "pressure_gs": dict(seed=103, outputs=["p_dyn", "aux_u", "aux_v", "aux_w"]),
     "pressure_rb3": dict(seed=104, outputs=["p_dyn"] + F.PROJECTION),
     "step_gs": dict(seed=105, outputs=F.PROGNOSTIC + ["p_dyn", "p_hydro", "p_bfollow"] + F.PROJECTION),
+    # the moist convective adjustment with the default knobs
+    "mca": dict(seed=107, outputs=["t", "nh4sh"] + [n for g in F.GASES for n in F.GAS_FIELDS[g]]),
     # the passes after RK4 with the default knobs, on post_case.post_state(state, seed + 1)
     "post_step": dict(seed=106, outputs=["t", "u", "v", "w", "h2o", "h2o_cloud", "h2o_ice", "h2s", "h2s_cloud",
                                          "h2s_ice", "nh3", "nh3_cloud", "nh3_ice", "ch4", "ch4_cloud", "ch4_ice",
@@ -87,6 +89,8 @@ def ref_runner(name, p, st):
         ref.rk4()
     elif name == "post_step":
         ref.post_step(P.default_post_params())
+    elif name == "mca":
+        ref.mca()
     out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
     if "buoy_ref_level" in CASES[name]["outputs"]:
         out["buoy_ref_level"] = ref.get("buoy_ref_level")

@@ -28,6 +28,8 @@ def oracle_runner(O, name, p, st):
         O.pressure_rb(p, st, 3)
     elif name == "step_gs":
         lev = O.step(p, st, P.PRESS_GS_LEX)
+    elif name == "mca":
+        O.mca(p, st)
     elif name == "post_step":
         from tests.golden.make_golden import post_input
         st = post_input(p, st, CASES[name]["seed"])

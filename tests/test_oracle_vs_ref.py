@@ -142,3 +142,19 @@ def test_post_step_knob_sets(knobs):
     child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_post_knobs_child.py")
     r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_mca(ref_model, oracle_lib, base_state, source):
+    """The moist convective adjustment (ConvectiveAdjustment.h:402-849) as the model's loop calls
+    it, default knobs: every value it writes (t, the twelve condensables, nh4sh) identical. Both
+    states have most columns unstable somewhere, so segments form, mix, settle and grow."""
+    p = P.default_params()
+    st = S.perturb(base_state, p, seed=71) if source == "reference_init" else S.synthetic_state(p, seed=72)
+    names = ["t", "nh4sh"] + [n for g in F.GASES for n in F.GAS_FIELDS[g]]
+    before = {n: st[n].copy() for n in names}
+    ref_model.load(st)
+    ref_model.mca()
+    oracle_lib.mca(p, st)
+    assert_same(ref_model.state(names), st, names)
+    assert np.count_nonzero(st["t"] != before["t"]) > 100000
