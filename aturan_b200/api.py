@@ -63,11 +63,12 @@ SIGNATURES = {
                                       ctypes.c_void_p], ctypes.c_int),
     "aturan_post_params_default": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_post_step": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_mca": ([ctypes.c_void_p], ctypes.c_int),
 }
 
 STATIC_MAX_IM, STATIC_MAX_JM = 512, 4096
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca"]
 NSPECIES = 13
 
 _LIB = None
@@ -197,6 +198,10 @@ class Context:
         self._check(self.L.aturan_post_step(self.h, ctypes.byref(pp), added.ctypes.data, cells.ctypes.data),
                     "post_step")
         return added, cells
+
+    def mca(self):
+        """aturan_mca: the moist convective adjustment (ConvectiveAdjustment.h:402-849), default knobs."""
+        self._check(self.L.aturan_mca(self.h), "mca")
 
     def tape(self, on=True):
         """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""

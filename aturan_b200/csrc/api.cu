@@ -24,6 +24,7 @@
 #include "sor.cuh"
 #include "adjoint.cuh"
 #include "post.cuh"
+#include "mca.cuh"
 
 using namespace aturan;
 
@@ -81,6 +82,7 @@ struct aturan_ctx {
     bool tape_p_valid;         // a taped RB_SOR / RB_LINE pressure call has run since the tape was switched on
     double* ahacc;             // the T tendencies' adjoint summed over the stages (heating gradient)
     double* heat;              // aturan_set_heating: [jm][km] K/s, or null
+    double* mca_H;             // aturan_mca: the cp table's running integral, made at the first call
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -1122,6 +1124,7 @@ int aturan_ctx_destroy(aturan_ctx* ctx){
     if(ctx->gs_exec) cudaGraphExecDestroy(ctx->gs_exec);
     if(ctx->tape) cudaFree(ctx->tape);
     if(ctx->heat) cudaFree(ctx->heat);
+    if(ctx->mca_H) cudaFree(ctx->mca_H);
     for(auto& e : ctx->evs){ cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if(ctx->mem) cudaFree(ctx->mem);
     if(ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
@@ -1523,6 +1526,42 @@ int aturan_post_params_default(aturan_post_params* pp){
     pp->damp_t_horiz = 1.0;        // cUranusModel.cpp:1214-1215
     pp->damp_t_vert = 0.0;         // cUranusModel.cpp:1204-1205
     pp->vel_shapiro = 0.0;         // cUranusModel.cpp:1229-1230, with geo_balance()
+    return ATURAN_OK;
+}
+
+int aturan_mca(aturan_ctx* ctx){
+    if(!ctx) return ATURAN_E_INVALID;
+    const Grid& g = ctx->g;
+    if(ctx->mixed || g.im > MCA_MAXI) return ATURAN_E_UNSUPPORTED;
+    const aturan_params& p = ctx->p;
+    const bool first = ctx->mca_H == nullptr;
+    if(first && cudaMalloc((void**)&ctx->mca_H, CP_TABLE_N * sizeof(double)) != cudaSuccess){
+        cudaGetLastError(); ctx->mca_H = nullptr; return ATURAN_E_NOMEM;
+    }
+    McaArgs a;
+    a.g = g;
+    const int order[MCA_NG] = { 0, 2, 1, 3 };                  // H2O, NH3, H2S, CH4 from the params' H2O, H2S, NH3, CH4
+    const int fv[MCA_NG] = { ATURAN_H2O, ATURAN_NH3, ATURAN_H2S, ATURAN_CH4 };
+    double* X = reinterpret_cast<double*>(ctx->state);
+    const size_t fs = g.fstride;
+    for(int n = 0; n < MCA_NG; n++){
+        const aturan_gas& s = p.gas[order[n]];
+        a.G[n] = McaGas{ s.ep, s.lv, s.ls, s.t_0, s.C, s.L0, s.R, s.del_alf, s.del_bet, s.C_i, s.L0_i, s.del_alf_i, s.del_bet_i };
+        for(int c = 0; c < 3; c++) a.sp[n][c] = X + (size_t)(fv[n] + c) * fs;
+    }
+    a.L_tr = p.nh4sh_sync ? 4705.0 * std::log(10.0) * 8314.46 / 51.1114 : 0.0;   // ChemistryUran.h:132
+    a.t_ref = p.t_ref; a.grav = p.g; a.cp_mix = p.cp_mix; a.r_mix = p.r_mix; a.cp_h2 = p.cp_h2;
+    a.r_h2 = p.r_h2; a.r_he = p.r_he; a.r_ch4 = p.r_ch4; a.cp_he = p.cp_he; a.cp_ch4 = p.cp_ch4;
+    a.hz = (float)(p.L_atm / (g.im - 1));                      // cUranusModel.h:1205-1208
+    a.cp_dyn = p.cp_dyn; a.cp_mode = p.cp_h2_mode; a.cp_gas = p.cp_gas; a.local_rho = p.local_rho;
+    a.cp_tab = ctx->cp_tab64; a.H_tab = ctx->mca_H;
+    a.t = X + (size_t)ATURAN_T * fs;
+    a.nh4sh = X + (size_t)ATURAN_NH4SH * fs;
+    a.ps = reinterpret_cast<const double*>(ctx->pstat);
+    a.rho = reinterpret_cast<const double*>(ctx->forc) + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs;
+    Region reg(ctx, ATURAN_K_MCA, first ? 2 : 1);
+    launch_mca(a, ctx->mca_H, first, ctx->st);
+    CK_LAUNCH("moist convective adjustment");
     return ATURAN_OK;
 }
 

@@ -9,6 +9,7 @@
 #include "rk4.cuh"
 #include "satadj.cuh"
 #include "pressure.cuh"
+#include "mca.cuh"
 #include "launch.h"
 #include "launch_impl.cuh"
 
@@ -21,6 +22,11 @@ __global__ void scale_copy_f64_kernel(const double* in, double* out, size_t n, d
 }
 void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff, cudaStream_t st){
     scale_copy_f64_kernel<<<148 * 8, 256, 0, st>>>(in, out, n, coeff);
+}
+
+void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st){
+    if(build_H) mca_H_kernel<<<1, 32, 0, st>>>(a.cp_tab, H);
+    mca_kernel<<<dim3((a.g.km + 63) / 64, a.g.jm), 64, 0, st>>>(a);
 }
 
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st){

@@ -31,6 +31,10 @@ ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)
 #undef ATURAN_DECLARE_LAUNCHERS
 
+// The moist convective adjustment (FP64 contexts); build_H first forms the cp table's integral in H.
+struct McaArgs;
+void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st);
+
 // FP64-only kernels (p_dyn is FP64 in both precisions).
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st);
 void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff, cudaStream_t st);

@@ -290,6 +290,43 @@ def post_step_timing(api, P, S, torch, precision, calls=20):
     return out
 
 
+def mca_timing(api, P, S, torch, reps=3):
+    """aturan_mca (FP64, default knobs) at 41x181x361 on a seeded synthetic state in which most
+    columns are unstable: device time of one call on the freshly uploaded state (CUDA events on the
+    context's stream, median of `reps`, after one warm-up call), and the compiled reference's same
+    call on the host cores when it is present."""
+    p = P.default_params()
+    st = S.synthetic_state(p, seed=72)
+    ctx = api.Context(p)
+    s = torch.cuda.ExternalStream(ctx.stream)
+    ms = []
+    for r in range(reps + 1):
+        ctx.upload_state(st)
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.mca()
+        e1.record(s)
+        e1.synchronize()
+        if r > 0:
+            ms.append(e0.elapsed_time(e1))
+    ctx.close()
+    out = {"ms": statistics.median(ms), "columns": p.jm * p.km,
+           "what": "moist convective adjustment, FP64, 41x181x361, synthetic state (seed 72), one call per upload"}
+    try:
+        from oracle import ref as R
+        if R.available():
+            m = R.Ref.get_instance()
+            m.load(st)
+            t0 = time.perf_counter()
+            m.mca()
+            out["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference_cores"] = os.cpu_count()
+    except Exception as ex:               # reported, never silently replaced
+        out["cpu_reference_ms"] = f"{type(ex).__name__}: {ex}"
+    return out
+
+
 def cpu_reference_step_time(nsteps, press, budget_s=120.0):
     """Time the reference's own step on the host cores after one untimed warm-up step; at most
     nsteps steps and no more than fit in budget_s. Returns (seconds/step, kind, cores, note, n)."""
@@ -372,6 +409,8 @@ def main():
     ap.add_argument("--grid", default="41x181x361", help="IxJxK of the shell (profiling cases)")
     ap.add_argument("--post-step", action="store_true",
                     help="only the passes after RK4 (aturan_post_step): prints the post_step object")
+    ap.add_argument("--mca", action="store_true",
+                    help="only the moist convective adjustment (aturan_mca): prints the mca object")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -390,6 +429,10 @@ def main():
         torch.cuda.set_device(0)
 
     from aturan_b200 import api, params as P, replicas, state as S
+    if args.mca:
+        if rank == 0:
+            print(json.dumps({"mca": mca_timing(api, P, S, torch)}), flush=True)
+        return
     if args.post_step:
         if rank == 0:
             print(json.dumps({"post_step": post_step_timing(api, P, S, torch, args.precision),

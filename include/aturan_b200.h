@@ -313,6 +313,15 @@ int aturan_post_params_default(aturan_post_params* pp);
  * Uranus) and pole fill rows (bc_pole_open_rows is 0 for Uranus). */
 int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells);
 
+/* MoistConvectiveAdjustment<cUranusModel>::run (planet/ConvectiveAdjustment.h:402-849) as the
+ * model's loop calls it (cUranusModel.cpp:1272-1292, every iteration by default), with the
+ * reference's default knobs (MCA_LEDOUX 1, MCA_LOADING 1, MCA_RELAX 1, MCA_SMOOTH 0, MCA_PASSES 64,
+ * no phase split, interior levels): per (j, k) column, the unstable pairs' segments mixed to their
+ * mass-weighted liquid-water static energy and total mixing ratios and settled to equilibrium;
+ * t, the twelve condensables and nh4sh written where touched. FP64 contexts with im <= 64; other
+ * contexts return ATURAN_E_UNSUPPORTED. The first call allocates 24 KB on the device. */
+int aturan_mca(aturan_ctx* ctx);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
@@ -323,6 +332,7 @@ enum aturan_kernel_kind {
     ATURAN_K_COPY,           /* n-copy sync and layout conversions */
     ATURAN_K_ADJOINT,        /* the RK4 step's adjoint (aturan_rk4_adjoint) */
     ATURAN_K_POST,           /* filters, boundary passes and species clamp (aturan_post_step) */
+    ATURAN_K_MCA,            /* moist convective adjustment (aturan_mca) */
     ATURAN_K_NKINDS
 };
 
