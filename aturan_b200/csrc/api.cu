@@ -572,6 +572,46 @@ int solve_fp64(aturan_ctx* ctx, double* P, const double* src, double omega, int 
     return r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
 }
 
+// The mixed form of the same solve: FP64 iterative refinement around FP32 correction solves,
+// r = src - Lc p in FP64, Lc e = r by FP32 sweeps (with the column-uniform correction), p += e in
+// FP64. Given shift, the first residual pass applies the source's compatibility shift.
+template <bool TR>
+int solve_mixed(aturan_ctx* ctx, double* P, const double* src, double omega, int max_sweeps, double tol, bool line,
+                int* sweeps_done, double* resid, long& nl, const double* shift = nullptr){
+    const size_t fs = ctx->g.fstride;
+    const int every = sor_correct_every(line);
+    // FP32 sweeps per refinement step: for line SOR 2 (measured at 41x181x361, warm: two
+    // refinement steps of 2 reach 3e-8 against 6 sweeps with 3 per step, 0.53 vs 0.59 ms)
+    const int inner = line ? 2 : 48;
+    double r = 0.0;
+    int s = 0;
+    // Each FP64 residual also leaves r in FP32, e = 0 and the column sums of r: what the next
+    // correction solve starts from (one pass over p and src per refinement step).
+    int rc = sor_residual<double, TR>(ctx, P, src, true, &r, nullptr, true, shift); if(rc) return rc; nl++;
+    while(s < max_sweeps && !(r <= tol)){
+        for(int n = 0; n < inner && s < max_sweeps; n++, s++){
+            // the correction on the same cadence as the FP64 solve (once per `every` sweeps,
+            // counted over the whole solve): after the first one the column-uniform error is
+            // gone and a later refinement step's correction changes nothing (measured: same
+            // sweep count, 0.14 ms less at 41x181x361); with e = 0 its column sums are r's
+            if(s % every == 0){
+                if(n != 0){ rc = sor_residual<float, TR>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc; nl++; }
+                rc = sor_correct<float, TR>(ctx, ctx->e32); if(rc) return rc;
+                nl += 4;
+            }
+            sor_sweep<float, TR>(ctx, ctx->e32, ctx->r32, omega, line);
+            nl += 2;
+        }
+        sor_axpy_kernel<<<148 * 8, 256, 0, ctx->st>>>(fs, P, ctx->e32);
+        CK_LAUNCH("SOR refinement");
+        nl++;
+        rc = sor_residual<double, TR>(ctx, P, src, true, &r, nullptr, true); if(rc) return rc; nl++;
+    }
+    if(sweeps_done) *sweeps_done = s;
+    if(resid) *resid = r;
+    return r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
+}
+
 template <typename S>
 int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line, int* sweeps_done, double* resid){
     const Grid g = ctx->g;
@@ -579,7 +619,6 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     S* proj = reinterpret_cast<S*>(ctx->proj);
     int rc = sor_check_sizes(ctx, omega, line); if(rc) return rc;
     if(max_sweeps < 1) max_sweeps = 1;
-    const int every = sor_correct_every(line);
     long nl = 0;
     Region reg(ctx, ATURAN_K_RB, 0);
     launch_rb_prep(g, grp<S>(proj, 3, fs), grp<S>(proj, 4, fs), grp<S>(proj, 5, fs),
@@ -598,39 +637,9 @@ int run_sor(aturan_ctx* ctx, double omega, int max_sweeps, double tol, bool line
     double r = 0.0;
     int s = 0;
     int status;
-    if(!ctx->mixed){
-        status = solve_fp64<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl, shift);
-        if(status < 0) return status;
-    } else {
-        // FP64 iterative refinement around FP32 correction solves: r = src - Lc p in FP64,
-        // Lc e = r by FP32 sweeps (with the column-uniform correction), p += e in FP64.
-        // FP32 sweeps per refinement step: for line SOR 2 (measured at 41x181x361, warm: two
-        // refinement steps of 2 reach 3e-8 against 6 sweeps with 3 per step, 0.53 vs 0.59 ms)
-        const int inner = line ? 2 : 48;
-        // Each FP64 residual also leaves r in FP32, e = 0 and the column sums of r: what the next
-        // correction solve starts from (one pass over p and src per refinement step).
-        rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true, shift); if(rc) return rc; nl++;
-        while(s < max_sweeps && !(r <= tol)){
-            for(int n = 0; n < inner && s < max_sweeps; n++, s++){
-                // the correction on the same cadence as the FP64 solve (once per `every` sweeps,
-                // counted over the whole solve): after the first one the column-uniform error is
-                // gone and a later refinement step's correction changes nothing (measured: same
-                // sweep count, 0.14 ms less at 41x181x361); with e = 0 its column sums are r's
-                if(s % every == 0){
-                    if(n != 0){ rc = sor_residual<float>(ctx, ctx->e32, ctx->r32, true, nullptr, nullptr); if(rc) return rc; nl++; }
-                    rc = sor_correct<float>(ctx, ctx->e32); if(rc) return rc;
-                    nl += 4;
-                }
-                sor_sweep<float>(ctx, ctx->e32, ctx->r32, omega, line);
-                nl += 2;
-            }
-            sor_axpy_kernel<<<148 * 8, 256, 0, ctx->st>>>(fs, P, ctx->e32);
-            CK_LAUNCH("SOR refinement");
-            nl++;
-            rc = sor_residual<double>(ctx, P, src, true, &r, nullptr, true); if(rc) return rc; nl++;
-        }
-        status = r <= tol ? ATURAN_OK : ATURAN_NOT_CONVERGED;
-    }
+    status = ctx->mixed ? solve_mixed<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl, shift)
+                        : solve_fp64<false>(ctx, P, src, omega, max_sweeps, tol, line, &s, &r, nl, shift);
+    if(status < 0) return status;
     launch_pdyn_bcs(g, P, ctx->st);                            // the boundary rows of the solution
     CK_LAUNCH("SOR boundary rows");
     nl += 3;
@@ -1470,9 +1479,13 @@ int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omeg
     nl += 3;
     int s = 0;
     double r = 0.0;
-    const int status = transposed
-        ? solve_fp64<true>(ctx, ctx->stage64, ctx->scratch, omega, max_sweeps, tol, line, &s, &r, nl)
-        : solve_fp64<false>(ctx, ctx->stage64, ctx->scratch, omega, max_sweeps, tol, line, &s, &r, nl);
+    double* X = ctx->stage64;
+    const double* B = ctx->scratch;
+    const int status = ctx->mixed
+        ? (transposed ? solve_mixed<true>(ctx, X, B, omega, max_sweeps, tol, line, &s, &r, nl)
+                      : solve_mixed<false>(ctx, X, B, omega, max_sweeps, tol, line, &s, &r, nl))
+        : (transposed ? solve_fp64<true>(ctx, X, B, omega, max_sweeps, tol, line, &s, &r, nl)
+                      : solve_fp64<false>(ctx, X, B, omega, max_sweeps, tol, line, &s, &r, nl));
     if(status < 0) return status;
     CK(cudaMemcpy2DAsync(x, g.km * 8, ctx->stage64, g.kp * 8, g.km * 8, rows, cudaMemcpyDeviceToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));

@@ -211,3 +211,98 @@ def perturb(base, p, seed=20261203, forcing_noise=True):
 
 def copy_state(s):
     return {n: a.copy() for n, a in s.items()}
+
+
+# ---- the isolated Poisson solve's input: a smoothed random velocity field and its divergence ----
+
+def _box3(a):
+    """One pass of the 3x3x3 box filter over (r, theta, phi) on the km-1 distinct meridians:
+    periodic in phi, the end rows repeated in r and theta (a clamped stencil). Separable: the
+    mean of three neighbours along each axis in turn."""
+    a = (np.roll(a, 1, axis=2) + a + np.roll(a, -1, axis=2)) / 3.0
+    for ax in (0, 1):
+        n = a.shape[ax]
+        lo = np.take(a, np.r_[0, 0:n - 1], axis=ax)
+        hi = np.take(a, np.r_[1:n, n - 1], axis=ax)
+        a = (lo + a + hi) / 3.0
+    return a
+
+
+def poisson_velocity(p, seed=20261205, passes=3):
+    """(u, v, w): iid N(0, 1) values on every cell of the shell (km-1 distinct meridians, k = km-1
+    the seam copy of k = 0), smoothed by `passes` passes of the 3x3x3 box filter."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(3):
+        a = rng.standard_normal((p.im, p.jm, p.km - 1))
+        for _ in range(passes):
+            a = _box3(a)
+        out.append(_seam(np.ascontiguousarray(np.concatenate([a, a[:, :, :1]], axis=2))))
+    return tuple(out)
+
+
+def poisson_source(p, u, v, w):
+    """The shared solver's pressure source for aux = (u, v, w), FP64 on the host: the boundary rows
+    that prepareProjectionBoundaries sets (Pressure_Uran.cpp:30-146: the lid's aux_u = 0, or the
+    cubic extrapolation without the rigid lid; cubic radial ends of v, w; cubic polar rows of u
+    with v = w = 0 there; the seam copy), then the centred divergence
+    du/dr + dv/dtheta / rm + dw/dphi / (rm sin theta) (PressureSolver.h:448-459, no obstacle) and
+    its clamp at den * p_dyn_cap with the non-finite guard (:481-487) on the interior. Returns the
+    source on [im][jm][km], zero outside the interior. Same operations in the same order as the
+    C code, so the values are the same bits as the oracle's."""
+    import math
+    im, jm, km = p.im, p.jm, p.km
+    au, av, aw = (np.array(x, dtype=np.float64, copy=True) for x in (u, v, w))
+    J, K = slice(1, jm - 1), slice(0, km - 1)
+
+    def cub0(X):
+        return X[3, J, K] - 3.0 * X[2, J, K] + 3.0 * X[1, J, K]
+
+    def cub1(X):
+        return X[im - 4, J, K] - 3.0 * X[im - 3, J, K] + 3.0 * X[im - 2, J, K]
+    if p.rigid_lid:
+        au[0, J, K] = 0.0
+        au[im - 1, J, K] = 0.0
+    else:
+        au[0, J, K], au[im - 1, J, K] = cub0(au), cub1(au)
+    for X in (av, aw):
+        X[0, J, K], X[im - 1, J, K] = cub0(X), cub1(X)
+    Ii = slice(1, im - 1)
+    au[Ii, 0, K] = au[Ii, 3, K] - 3.0 * au[Ii, 2, K] + 3.0 * au[Ii, 1, K]
+    au[Ii, jm - 1, K] = au[Ii, jm - 4, K] - 3.0 * au[Ii, jm - 3, K] + 3.0 * au[Ii, jm - 2, K]
+    for X in (av, aw):
+        X[Ii, 0, K] = 0.0
+        X[Ii, jm - 1, K] = 0.0
+    for X in (au, av, aw):
+        _seam(X)
+    rad, the = coords(p)
+    st = np.array([max(math.sin(t), p.sinthe_min) for t in the])
+    st[st == 0.0] = 1.0e-5
+    R_km = p.metric_R_km
+    rm = rad + (R_km / p.L_atm - 1.0) if R_km > 0.0 else rad.copy()
+    inv_dr2, inv_dthe2, inv_dphi2 = 1.0 / (p.dr * p.dr), 1.0 / (p.dthe * p.dthe), 1.0 / (p.dphi * p.dphi)
+    inv_2dr, inv_2dthe, inv_2dphi = 1.0 / (2.0 * p.dr), 1.0 / (2.0 * p.dthe), 1.0 / (2.0 * p.dphi)
+    rm2 = (rm * rm)[:, None]
+    inv_rm2 = 1.0 / rm2
+    inv_rm2sinthe2 = inv_rm2 / (st * st)[None, :]
+    num1 = 1.0 * inv_dr2
+    num2 = inv_rm2 * inv_dthe2
+    num3 = inv_rm2sinthe2 * inv_dphi2
+    den = 2.0 * num1 + 2.0 * num2 + 2.0 * num3                       # (im, jm)
+    inv_rm = (1.0 / rm)[:, None]
+    inv_rmsinthe = 1.0 / (rm[:, None] * st[None, :])
+    k = np.arange(km - 1)
+    ke = np.where(k + 1 >= km - 1, k + 1 - (km - 1), k + 1)
+    kw = np.where(k - 1 < 0, k - 1 + (km - 1), k - 1)
+    Jj = slice(1, jm - 1)
+    du = (au[2:, Jj, :km - 1] - au[:-2, Jj, :km - 1]) * inv_2dr
+    dv = (av[Ii, 2:, :km - 1] - av[Ii, :-2, :km - 1]) * inv_2dthe
+    dw = (aw[Ii, Jj][:, :, ke] - aw[Ii, Jj][:, :, kw]) * inv_2dphi
+    with np.errstate(invalid="ignore", over="ignore"):
+        div = du * 1.0 + dv * inv_rm[Ii, :, None] + dw * inv_rmsinthe[Ii, Jj, None]
+    smax = (den[Ii, Jj] * p.p_dyn_cap)[:, :, None]
+    div = np.where(np.isfinite(div), div, 0.0)
+    div = np.where(div > smax, smax, np.where(div < -smax, -smax, div))
+    src = np.zeros((im, jm, km))
+    src[Ii, Jj, :km - 1] = div
+    return src

@@ -327,6 +327,75 @@ def mca_timing(api, P, S, torch, reps=3):
     return out
 
 
+POISSON_OMEGAS = (1.0, 1.5, 1.6, 1.7, 1.8, 1.9)
+
+
+def poisson_timing(api, P, S, torch, tol=1e-8, omegas=POISSON_OMEGAS):
+    """The isolated Poisson solve at 41x181x361: the source is the shared solver's divergence
+    (with its boundary rows and clamp) of a seeded N(0, 1) velocity field smoothed by 3 passes of a
+    3x3x3 box filter (aturan_b200.state.poisson_velocity / poisson_source, FP64); Lc x = src from
+    x = 0 to a relative L2 residual of `tol` through aturan_pressure_solve, for point red-black SOR
+    and radial-line red-black SOR at every omega, in an FP64 context (FP64 sweeps) and in a mixed
+    context (FP32 sweeps inside FP64 iterative refinement; the same FP64 source and solution).
+    Per case: the status, sweeps, the achieved residual, device time (CUDA events on the context's
+    stream around the synchronous call) and the sweeps' algorithmic bytes (p read, src read, p
+    written per sweep: 3 words per stored cell) against the HBM peak. The iterate and the source
+    (43 MB in FP64) fit in L2, so that fraction can pass 1."""
+    p = P.default_params()
+    u, v, w = S.poisson_velocity(p, seed=20261205)
+    src = S.poisson_source(p, u, v, w)
+    bd = torch.tensor(src, device="cuda")
+    xd = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+    peak, peak_kind = peaks()
+    N = p.im * p.jm * p.km
+    out = {"what": "Lc x = div(smoothed N(0,1) velocity) at 41x181x361 from x = 0 to a relative residual of "
+                   f"{tol:g}; aturan_pressure_solve; FP64 context = FP64 sweeps, mixed context = FP32 sweeps "
+                   "in FP64 refinement", "tol": tol, "cases": [], "peak_source": f"{peak_kind} hbm_gbs"}
+    solves = {}
+    for prec_name, prec in (("fp64", P.FP64), ("mixed", P.MIXED)):
+        ctx = api.Context(P.default_params(precision=prec))
+        s = torch.cuda.ExternalStream(ctx.stream)
+        for kind_name, kind, cap in (("rb_sor", P.PRESS_RB_SOR, 6000), ("rb_line", P.PRESS_RB_LINE, 400)):
+            for om in omegas:
+                for rep in range(2):               # the first call warms the kernels up
+                    xd.zero_()
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(s)
+                    rc, sweeps, res = ctx.pressure_solve(bd.data_ptr(), xd.data_ptr(), kind, False, om, cap, tol)
+                    e1.record(s)
+                    e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                word = 8 if prec_name == "fp64" else 4
+                alg = 3 * word * N * sweeps
+                out["cases"].append({"kind": kind_name, "precision": prec_name, "omega": om,
+                                     "converged": rc == 0, "sweeps": sweeps, "resid": res, "ms": ms,
+                                     "sweep_alg_gbs": alg / (ms / 1e3) / 1e9,
+                                     "sweep_frac": alg / (ms / 1e3) / 1e9 / peak})
+                if rc == 0 and om in (1.0, 1.8):
+                    solves[(prec_name, kind_name, om)] = xd.clone()
+        ctx.close()
+    # the mixed solution against the FP64 one (interior, up to the free constant of the
+    # all-Neumann problem), for the fastest case of each kind
+    I = (slice(1, p.im - 1), slice(1, p.jm - 1), slice(0, p.km - 1))
+    agree = {}
+    for kind_name, om in (("rb_sor", 1.8), ("rb_line", 1.0)):
+        a, b = solves.get(("mixed", kind_name, om)), solves.get(("fp64", kind_name, om))
+        if a is not None and b is not None:
+            d = (a - b)[I]
+            d = d - d.mean()
+            bb = b[I] - b[I].mean()
+            agree[f"{kind_name}_omega{om}"] = float(d.abs().max() / bb.abs().max())
+    out["mixed_vs_fp64_solution"] = agree
+    best = {}
+    for c in out["cases"]:
+        key = f"{c['kind']}_{c['precision']}"
+        if c["converged"] and (key not in best or c["ms"] < best[key]["ms"]):
+            best[key] = {"omega": c["omega"], "sweeps": c["sweeps"], "ms": c["ms"]}
+    out["best"] = best
+    return out
+
+
 def cpu_reference_step_time(nsteps, press, budget_s=120.0):
     """Time the reference's own step on the host cores after one untimed warm-up step; at most
     nsteps steps and no more than fit in budget_s. Returns (seconds/step, kind, cores, note, n)."""
@@ -411,6 +480,8 @@ def main():
                     help="only the passes after RK4 (aturan_post_step): prints the post_step object")
     ap.add_argument("--mca", action="store_true",
                     help="only the moist convective adjustment (aturan_mca): prints the mca object")
+    ap.add_argument("--poisson", action="store_true",
+                    help="only the isolated Poisson solve (omega sweep, FP64 and mixed): prints the poisson object")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -432,6 +503,10 @@ def main():
     if args.mca:
         if rank == 0:
             print(json.dumps({"mca": mca_timing(api, P, S, torch)}), flush=True)
+        return
+    if args.poisson:
+        if rank == 0:
+            print(json.dumps({"poisson": poisson_timing(api, P, S, torch)}), flush=True)
         return
     if args.post_step:
         if rank == 0:
@@ -555,6 +630,13 @@ def main():
         except Exception as ex:          # reported, never silently replaced
             post = {"error": f"{type(ex).__name__}: {ex}"}
 
+    poisson = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            poisson = poisson_timing(api, P, S, torch)
+        except Exception as ex:          # reported, never silently replaced
+            poisson = {"error": f"{type(ex).__name__}: {ex}"}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -590,6 +672,7 @@ def main():
             "clocks": clk,
             "adjoint": adjoint,
             "post_step": post,
+            "poisson": poisson,
             "cpu_baseline": cpu,
         }
         if accuracy is not None:

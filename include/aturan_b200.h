@@ -239,8 +239,10 @@ int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, dou
  *   transposed = 1: Lc^T x = b, b first made zero-mean (Lc^T's left null vector is the constant);
  *     x is defined up to a multiple of y_i y_j. For compatible s and g,
  *     <solve(s), g> = <s, solve^T(g)>: the adjoint of the pressure solve.
- * kind is ATURAN_PRESS_RB_SOR or ATURAN_PRESS_RB_LINE (as aturan_pressure, FP64 arithmetic in
- * either context precision); ATURAN_NOT_CONVERGED at the cap. Synchronous. */
+ * kind is ATURAN_PRESS_RB_SOR or ATURAN_PRESS_RB_LINE, in the context's precision as
+ * aturan_pressure: FP64 relaxation in an FP64 context; in a mixed context FP32 correction solves
+ * inside FP64 iterative refinement (residual, its norm and x += e in FP64; b and x stay FP64).
+ * ATURAN_NOT_CONVERGED at the cap. Synchronous. */
 int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omega, int max_sweeps, double tol,
                           const double* b, double* x, int* sweeps_done, double* resid);
 

@@ -108,3 +108,29 @@ def test_adjoint_solve_dot_product(oracle_lib, line):
     gc = g[I] - g[I].mean()
     lhs, rhs = float((x[I] * gc).sum()), float((sc * lam[I]).sum())
     assert abs(lhs - rhs) <= 1e-8 * abs(lhs), (lhs, rhs)
+
+
+@pytest.mark.parametrize("shape,rigid", [((12, 20, 33), 1), ((41, 91, 181), 1), ((9, 13, 17), 0)])
+def test_poisson_source_is_the_shared_solvers(oracle_lib, shape, rigid):
+    """The isolated Poisson solve's right-hand side (aturan_b200.state.poisson_source: the
+    divergence of PressureSolver.h:448-487 after prepareProjectionBoundaries) is the oracle's
+    pressure source, which is pinned to the compiled reference, bit for bit."""
+    from aturan_b200 import fields as F
+    p = P.default_params(*shape)
+    p.rigid_lid = rigid
+    u, v, w = S.poisson_velocity(p, seed=5)
+    src = S.poisson_source(p, u, v, w)
+    st = {n: np.zeros(p.shape) for n in F.PROJECTION}
+    st["aux_u"], st["aux_v"], st["aux_w"] = u.copy(), v.copy(), w.copy()
+    assert np.array_equal(src, oracle_lib.pressure_source(p, st))
+
+
+def test_poisson_velocity_is_smoothed_and_periodic():
+    p = P.default_params(12, 20, 33)
+    u, v, w = S.poisson_velocity(p, seed=7)
+    for a in (u, v, w):
+        assert a.shape == p.shape and np.array_equal(a[..., -1], a[..., 0])
+        # 3 passes of a 3x3x3 mean shrink unit-variance noise well below 1
+        assert 0.02 < a.std() < 0.3
+    u2, _, _ = S.poisson_velocity(p, seed=7)
+    assert np.array_equal(u, u2)
