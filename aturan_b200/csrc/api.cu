@@ -71,6 +71,7 @@ struct aturan_ctx {
     double *mluT_a, *mluT_cf, *mluT_idn;         // the same for the transposed operator
     double *lluT_a, *lluT_cf, *lluT_idn;
     float *r32, *e32;
+    float* tlo;                // mixed form: the low parts of t and of tn (two FP32 fields; common.cuh), else null
     int sor_nblk;
     int sor_pm;                // Fourier modes per block of the column correction's tridiagonal solves
     std::vector<double> host_part;
@@ -285,6 +286,14 @@ void* field_ptr(aturan_ctx* c, int id, bool* is64){
 
 template <typename S> S* grp(void* base, int q, size_t fs){ return reinterpret_cast<S*>(base) + (size_t)q * fs; }
 
+// The low part of the mixed form's temperature pair for field id t or tn, else null.
+float* t_lo_of(aturan_ctx* c, int id){
+    if(!c->tlo) return nullptr;
+    if(id == ATURAN_T) return c->tlo;
+    if(id == ATURAN_TN) return c->tlo + c->g.fstride;
+    return nullptr;
+}
+
 template <typename S>
 bool taping(const aturan_ctx* ctx){ return std::is_same<S, double>::value && ctx->tape != nullptr; }
 
@@ -333,6 +342,8 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
     a.cp_tab = reinterpret_cast<const C*>(ctx->cp_tab);
     a.heat = ctx->heat;
     a.k = K;
+    a.tlo = ctx->tlo;
+    a.tnlo = ctx->tlo ? ctx->tlo + fs : nullptr;
     S* y0 = reinterpret_cast<S*>(ctx->ybuf[0]);
     S* y1 = reinterpret_cast<S*>(ctx->ybuf[1]);
     const double dt = ctx->p.dt;
@@ -376,6 +387,8 @@ int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st, bool with
     a.nc_off = (long long)(reinterpret_cast<S*>(ctx->ncopy) - state);
     a.sync = with_sync ? (ctx->p.nh4sh_sync ? 2 : 1) : 0;
     a.nh4sh = grp<S>(state, ATURAN_NH4SH, fs);
+    a.tlo = ctx->tlo;
+    a.tnlo = ctx->tlo ? ctx->tlo + fs : nullptr;
     Region reg(ctx, ATURAN_K_SATADJ, 1, st);
     launch_satadj(a, st);
     CK_LAUNCH("saturation adjustment");
@@ -680,6 +693,7 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
     for(int n = 0; n < POST_NTHZ; n++) a.thz[n] = fld(THZ[n]);
     for(int n = 0; n < POST_NSP; n++) a.sp[n] = fld(SP[n]);
     a.u = fld(ATURAN_U); a.v = fld(ATURAN_V); a.w = fld(ATURAN_W);
+    a.tlo = ctx->tlo;
     a.radius_form = pp->radius_form; a.bottom_form = pp->bottom_form; a.pole_form = pp->pole_form;
     a.lid_u = pp->lid_u; a.top_taper = pp->top_taper; a.lid_vw = pp->lid_vw;
     a.positive = pp->radius_positive; a.phi_periodic = pp->phi_periodic;
@@ -694,7 +708,7 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
     int nl;
     {
         Region reg(ctx, ATURAN_K_POST, 0);
-        nl = launch_post(a, pl, fld(ATURAN_T), ctx->st);
+        nl = launch_post(a, pl, fld(ATURAN_T), ctx->tlo, ctx->st);
         reg.n = nl;
         CK_LAUNCH("post step");
     }
@@ -801,6 +815,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     for(int n = 0; n < 6; n++) add((size_t)(sNM + 1) * sJ * 8);        // mode factorisations (Lc, Lc^T)
     for(int n = 0; n < 6; n++) add(nij * 8);                           // line factorisations (Lc, Lc^T)
     add(fs * 4); add(fs * 4);
+    if(ctx->mixed) add(2 * fs * 4);                                    // the temperature pair's low parts
     ctx->mem_bytes = bytes;
     // the stage kernels address every buffer of the allocation by 32-bit element offsets
     if(bytes / e >= (size_t)INT32_MAX){
@@ -867,6 +882,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->mluT_idn = carve<double>(cur, (size_t)(sNM + 1) * sJ);
     ctx->lluT_a = carve<double>(cur, nij); ctx->lluT_cf = carve<double>(cur, nij); ctx->lluT_idn = carve<double>(cur, nij);
     ctx->r32 = carve<float>(cur, fs); ctx->e32 = carve<float>(cur, fs);
+    ctx->tlo = ctx->mixed ? carve<float>(cur, 2 * fs) : nullptr;
     ctx->host_part.resize(2 * ctx->sor_nblk);
 
     // zero everything once: padding columns and unused planes read as 0, never as garbage
@@ -1163,14 +1179,18 @@ static int xfer(aturan_ctx* ctx, int field, void* other, bool up, bool other_is_
             CK(cudaMemcpyAsync(ctx->stage64, other, n * 8, cudaMemcpyHostToDevice, ctx->st));
             src_c = ctx->stage64;
         }
-        if(is64) launch_pack_in_f64(src_c, reinterpret_cast<double*>(dev), g.km, g.kp, rows, ctx->st);
-        else     launch_pack_in_f32(src_c, reinterpret_cast<float*>(dev), g.km, g.kp, rows, ctx->st);
+        float* lo = t_lo_of(ctx, field);
+        if(is64)    launch_pack_in_f64(src_c, reinterpret_cast<double*>(dev), g.km, g.kp, rows, ctx->st);
+        else if(lo) launch_pack_in_pair(src_c, reinterpret_cast<float*>(dev), lo, g.km, g.kp, rows, ctx->st);
+        else        launch_pack_in_f32(src_c, reinterpret_cast<float*>(dev), g.km, g.kp, rows, ctx->st);
         CK_LAUNCH("layout in");
         if(!other_is_device) CK(cudaStreamSynchronize(ctx->st));
     } else {
         double* tgt = other_is_device ? reinterpret_cast<double*>(other) : ctx->stage64;
-        if(is64) launch_pack_out_f64(reinterpret_cast<const double*>(dev), tgt, g.km, g.kp, rows, ctx->st);
-        else     launch_pack_out_f32(reinterpret_cast<const float*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+        const float* lo = t_lo_of(ctx, field);
+        if(is64)    launch_pack_out_f64(reinterpret_cast<const double*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+        else if(lo) launch_pack_out_pair(reinterpret_cast<const float*>(dev), lo, tgt, g.km, g.kp, rows, ctx->st);
+        else        launch_pack_out_f32(reinterpret_cast<const float*>(dev), tgt, g.km, g.kp, rows, ctx->st);
         CK_LAUNCH("layout out");
         if(!other_is_device) CK(cudaMemcpyAsync(other, ctx->stage64, n * 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
@@ -1412,6 +1432,7 @@ static int sync_ncopies(aturan_ctx* ctx, cudaStream_t st){
     CK(cudaMemcpyAsync(n, s, fs * e, cudaMemcpyDeviceToDevice, st));
     if(ctx->p.nh4sh_sync)
         CK(cudaMemcpyAsync(n + ATURAN_NH4SH * fs * e, s + ATURAN_NH4SH * fs * e, fs * e, cudaMemcpyDeviceToDevice, st));
+    if(ctx->tlo) CK(cudaMemcpyAsync(ctx->tlo + fs, ctx->tlo, fs * 4, cudaMemcpyDeviceToDevice, st));
     return ATURAN_OK;
 }
 
@@ -1426,8 +1447,14 @@ int aturan_restore_ncopies(aturan_ctx* ctx, double coeff){
     Region reg(ctx, ATURAN_K_COPY, coeff == 1.0 ? 0 : 1);
     if(coeff == 1.0){                                     // 1.0 * x == x: a copy
         CK(cudaMemcpyAsync(ctx->ncopy, ctx->state, 19 * fs * e, cudaMemcpyDeviceToDevice, ctx->st));
+        if(ctx->tlo) CK(cudaMemcpyAsync(ctx->tlo + fs, ctx->tlo, fs * 4, cudaMemcpyDeviceToDevice, ctx->st));
     } else {
-        if(ctx->mixed) launch_scale_copy_f32(reinterpret_cast<const float*>(ctx->state), reinterpret_cast<float*>(ctx->ncopy), 19 * fs, coeff, ctx->st);
+        if(ctx->mixed){
+            launch_scale_copy_f32(reinterpret_cast<const float*>(ctx->state), reinterpret_cast<float*>(ctx->ncopy), 19 * fs, coeff, ctx->st);
+            // tn = coeff * (hi + lo) in FP64, split again
+            launch_scale_copy_pair(reinterpret_cast<const float*>(ctx->state), ctx->tlo,
+                                   reinterpret_cast<float*>(ctx->ncopy), ctx->tlo + fs, fs, coeff, ctx->st);
+        }
         else launch_scale_copy_f64(reinterpret_cast<const double*>(ctx->state), reinterpret_cast<double*>(ctx->ncopy), 19 * fs, coeff, ctx->st);
         CK_LAUNCH("restore n-copies");
     }

@@ -85,4 +85,24 @@ struct BuoyScratch {
 
 constexpr int CP_TABLE_N = 2991;   // (1500 - 5) / 0.5 + 1, CpH2.h:66-75
 
+// The mixed form carries the temperature (t and its start-of-step copy tn) as an FP32 pair: the
+// stored FP32 value hi, which every stencil reads, and lo = the FP32-rounded remainder T - hi, so
+// that T = hi + lo to about 2^-48 relative. The kernels that write T (the RK4 final update, the
+// saturation adjustment, the passes after RK4, the layout kernels) form it in FP64 from hi + lo
+// and store both halves. Without lo the FP32 rounding of T (~6e-8) moves the adjustment's
+// relative 1e-3 stopping test (SaturationAdjustment.h:250-251) to another pass in some cells of
+// the CH4 band, a jump of ~1e-5 in T there. lo is null in an FP64 context (and ignored).
+template <typename S>
+__device__ __forceinline__ double t_ld(const S* hi, const float* lo, size_t q){
+    double v = (double)hi[q];
+    if(lo) v += (double)lo[q];
+    return v;
+}
+template <typename S>
+__device__ __forceinline__ void t_st(S* hi, float* lo, size_t q, double v){
+    const S h = (S)v;
+    hi[q] = h;
+    if(lo) lo[q] = (float)(v - (double)h);
+}
+
 }  // namespace aturan

@@ -25,7 +25,7 @@ void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S
                      const GSW* w, PressConst c, int s, cudaStream_t st);                                   \
 void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
                     const RBW* w, PressConst c, double* src, cudaStream_t st);                             \
-int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st);
+int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)
@@ -48,5 +48,9 @@ void launch_pack_in_f32(const double* in, float* out, int km, int kp, size_t row
 void launch_pack_out_f64(const double* in, double* out, int km, int kp, size_t rows, cudaStream_t st);
 void launch_pack_out_f32(const float* in, double* out, int km, int kp, size_t rows, cudaStream_t st);
 void launch_f32_to_f64(const float* in, double* out, size_t n, cudaStream_t st);
+// The mixed form's temperature pair (common.cuh): FP64 exchange <-> (hi, lo) FP32 storage.
+void launch_pack_in_pair(const double* in, float* hi, float* lo, int km, int kp, size_t rows, cudaStream_t st);
+void launch_pack_out_pair(const float* hi, const float* lo, double* out, int km, int kp, size_t rows, cudaStream_t st);
+void launch_scale_copy_pair(const float* hi, const float* lo, float* ohi, float* olo, size_t n, double coeff, cudaStream_t st);
 
 }  // namespace aturan

@@ -60,11 +60,12 @@ void launch_momentum(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
 }
 // The passes after RK4 in the reference's order; returns the number of launches.
 template <typename S>
-int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st){
+int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st){
     const Grid& g = a.g;
     const dim3 cols_k((g.km + 127) / 128);
     int n = 0;
-    auto filt = [&](S* x, bool ai, bool aj, bool ak, double strength){
+    // lo: the low part of the mixed form's temperature pair when x is t (common.cuh), else null
+    auto filt = [&](S* x, float* lo, bool ai, bool aj, bool ak, double strength){
         const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
         if(ak){
             // four rows (warps) per block while they fit the default 48 KB, else one row per block
@@ -74,16 +75,16 @@ int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_
             static const bool big = (cudaFuncSetAttribute(post_filter_k_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                           8192 * (int)sizeof(double)) == cudaSuccess) || (cudaGetLastError(), false);
             (void)big;
-            post_filter_k_kernel<S><<<(rows + R - 1) / R, dim3(32, R), sm, st>>>(g, x, coeff, a.phi_periodic && g.km > 2, rows);
+            post_filter_k_kernel<S><<<(rows + R - 1) / R, dim3(32, R), sm, st>>>(g, x, lo, coeff, a.phi_periodic && g.km > 2, rows);
             n++;
         }
-        if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, coeff); n++; }
-        if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, coeff); n++; }
+        if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, lo, coeff); n++; }
+        if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, lo, coeff); n++; }
     };
-    if(pl.damp_t_horiz != 0.0) filt(t, false, pl.damp_t_j != 0, true, pl.damp_t_horiz);
-    if(pl.damp_t_vert != 0.0) filt(t, true, false, false, pl.damp_t_vert);
-    if(pl.vel_shapiro != 0.0){ filt(a.u, true, true, true, pl.vel_shapiro); filt(a.v, true, true, true, pl.vel_shapiro);
-                               filt(a.w, true, true, true, pl.vel_shapiro); }
+    if(pl.damp_t_horiz != 0.0) filt(t, tlo, false, pl.damp_t_j != 0, true, pl.damp_t_horiz);
+    if(pl.damp_t_vert != 0.0) filt(t, tlo, true, false, false, pl.damp_t_vert);
+    if(pl.vel_shapiro != 0.0){ filt(a.u, nullptr, true, true, true, pl.vel_shapiro); filt(a.v, nullptr, true, true, true, pl.vel_shapiro);
+                               filt(a.w, nullptr, true, true, true, pl.vel_shapiro); }
     post_bc_radius_kernel<S><<<dim3(cols_k.x, g.jm, POST_NRAD), 128, 0, st>>>(a);
     post_bc_theta_kernel<S><<<dim3(cols_k.x, g.im, POST_NTHZ + POST_NTHX), 128, 0, st>>>(a);
     post_bc_phi_kernel<S><<<dim3((g.im * g.jm + 127) / 128, POST_NRAD), 128, 0, st>>>(a);
@@ -154,6 +155,6 @@ void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_
     rb_src_kernel<S><<<dim3((g.km - 1 + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(                   \
         g, au, av, aw, w, c, src);                                                                        \
 }                                                                                                         \
-int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, cudaStream_t st){                          \
-    return launch_post_impl<S>(a, pl, t, st);                                                             \
+int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st){              \
+    return launch_post_impl<S>(a, pl, t, tlo, st);                                                        \
 }

@@ -60,6 +60,33 @@ void launch_pack_out_f32(const float* in, double* out, int km, int kp, size_t ro
     pack_out_kernel<float><<<pack_grid(km, rows), 128, 0, st>>>(in, out, km, kp, rows);
 }
 
+// The temperature pair (common.cuh): FP64 in, hi = (float)x and lo = (float)(x - hi) out, and back.
+__global__ void pack_in_pair_kernel(const double* in, float* hi, float* lo, int km, int kp, size_t rows){
+    const size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= rows || k >= km) return;
+    t_st(hi, lo, r * kp + k, in[r * km + k]);
+}
+__global__ void pack_out_pair_kernel(const float* hi, const float* lo, double* out, int km, int kp, size_t rows){
+    const size_t r = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= rows || k >= km) return;
+    out[r * km + k] = t_ld(hi, lo, r * kp + k);
+}
+void launch_pack_in_pair(const double* in, float* hi, float* lo, int km, int kp, size_t rows, cudaStream_t st){
+    pack_in_pair_kernel<<<pack_grid(km, rows), 128, 0, st>>>(in, hi, lo, km, kp, rows);
+}
+void launch_pack_out_pair(const float* hi, const float* lo, double* out, int km, int kp, size_t rows, cudaStream_t st){
+    pack_out_pair_kernel<<<pack_grid(km, rows), 128, 0, st>>>(hi, lo, out, km, kp, rows);
+}
+__global__ void scale_copy_pair_kernel(const float* hi, const float* lo, float* ohi, float* olo, size_t n, double coeff){
+    for(size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        t_st(ohi, olo, t, coeff * t_ld(hi, lo, t));
+}
+void launch_scale_copy_pair(const float* hi, const float* lo, float* ohi, float* olo, size_t n, double coeff, cudaStream_t st){
+    scale_copy_pair_kernel<<<148 * 8, 256, 0, st>>>(hi, lo, ohi, olo, n, coeff);
+}
+
 void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st){
     f64_to_f32_kernel<<<148 * 8, 256, 0, st>>>(in, out, n);
 }

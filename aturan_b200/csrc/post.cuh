@@ -37,6 +37,7 @@ struct PostArgs {
     S* thz[POST_NTHZ];           // theta pass, zeroed at the poles (v, w first)
     S* sp[POST_NSP];             // species for the clamp, in BC_Uran.h:83-89's order
     S *u, *v, *w;
+    float* tlo;                  // the mixed form's temperature pair (common.cuh): t's low part, else null
     int radius_form, bottom_form, pole_form, lid_u, top_taper, lid_vw, positive, phi_periodic;
 };
 
@@ -53,50 +54,53 @@ __device__ __forceinline__ double post_max0(double x){ return (0.0 < x) ? x : 0.
 
 // Along k: one warp per (i, j) row (blockDim.y rows per block), the row's old values in the warp's
 // own slice of shared memory, ~km/32 loads in flight per lane. With the periodic seam the ring is
-// k = 0..km-2 and k = km-1 takes the new k = 0; otherwise k wraps over all km.
+// k = 0..km-2 and k = km-1 takes the new k = 0; otherwise k wraps over all km. lo: the low part of
+// the mixed form's temperature pair when x is its t (common.cuh), else null.
 template <typename S>
-__global__ void __launch_bounds__(128) post_filter_k_kernel(Grid g, S* x, double coeff, int seam, int rows){
+__global__ void __launch_bounds__(128) post_filter_k_kernel(Grid g, S* x, float* lo, double coeff, int seam, int rows){
     extern __shared__ double sm[];
     const int r = blockIdx.x * blockDim.y + threadIdx.y;
     if(r >= rows) return;                          // a whole warp: only warp-level syncs below
     const int km = g.km;
     double* row = sm + (size_t)threadIdx.y * km;
     const size_t o = (size_t)r * g.kp;
-    for(int k = threadIdx.x; k < km; k += 32) row[k] = (double)x[o + k];
+    for(int k = threadIdx.x; k < km; k += 32) row[k] = t_ld(x, lo, o + k);
     __syncwarp();
     const int k_end = seam ? km - 1 : km;
     for(int k = threadIdx.x; k < k_end; k += 32){
         const int km1 = seam ? (k == 0 ? km - 2 : k - 1) : (k - 1 + km) % km;
         const int kp1 = seam ? (k == km - 2 ? 0 : k + 1) : (k + 1) % km;
         const double c = row[k];
-        const S y = (S)(c + coeff * (row[km1] - 2.0 * c + row[kp1]));
-        x[o + k] = y;
-        if(seam && k == 0) x[o + km - 1] = y;
+        const double y = c + coeff * (row[km1] - 2.0 * c + row[kp1]);
+        t_st(x, lo, o + k, y);
+        if(seam && k == 0) t_st(x, lo, o + km - 1, y);
     }
 }
 
 // Along a column of n cells at stride st from x0 (j: clamped at the poles; i: at the ends).
 template <typename S>
-__device__ __forceinline__ void post_walk(S* x0, size_t st, int n, double coeff){
-    double pm = (double)x0[0], c = pm;
+__device__ __forceinline__ void post_walk(S* x0, float* lo0, size_t st, int n, double coeff){
+    double pm = t_ld(x0, lo0, 0), c = pm;
     for(int q = 0; q < n; q++){
-        const double nx = (q + 1 < n) ? (double)x0[(size_t)(q + 1) * st] : c;
-        x0[(size_t)q * st] = (S)(c + coeff * (pm - 2.0 * c + nx));
+        const double nx = (q + 1 < n) ? t_ld(x0, lo0, (size_t)(q + 1) * st) : c;
+        t_st(x0, lo0, (size_t)q * st, c + coeff * (pm - 2.0 * c + nx));
         pm = c;
         c = nx;
     }
 }
 template <typename S>
-__global__ void __launch_bounds__(128) post_filter_j_kernel(Grid g, S* x, double coeff){
+__global__ void __launch_bounds__(128) post_filter_j_kernel(Grid g, S* x, float* lo, double coeff){
     const int k = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
     if(k >= g.km) return;
-    post_walk(x + gidx(g, i, 0, k), (size_t)g.kp, g.jm, coeff);
+    const size_t o = gidx(g, i, 0, k);
+    post_walk(x + o, lo ? lo + o : nullptr, (size_t)g.kp, g.jm, coeff);
 }
 template <typename S>
-__global__ void __launch_bounds__(128) post_filter_i_kernel(Grid g, S* x, double coeff){
+__global__ void __launch_bounds__(128) post_filter_i_kernel(Grid g, S* x, float* lo, double coeff){
     const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
     if(k >= g.km) return;
-    post_walk(x + gidx(g, 0, j, k), (size_t)g.jm * g.kp, g.im, coeff);
+    const size_t o = gidx(g, 0, j, k);
+    post_walk(x + o, lo ? lo + o : nullptr, (size_t)g.jm * g.kp, g.im, coeff);
 }
 
 // ---- bcRadius (BoundaryConditions.h:152-286), floorRadialSpecies and the lid v, w (BC_Uran.h:91-170) ----
@@ -114,6 +118,13 @@ __global__ void __launch_bounds__(128) post_bc_radius_kernel(PostArgs<S> a){
     S* F = a.rad[n] + gidx(g, 0, j, k);
     auto at = [&](int i) -> S& { return F[(size_t)i * pl]; };
     const int fb = (a.bottom_form != 0 && n != 1) ? a.bottom_form : a.radius_form;
+    if(n == 0 && a.tlo){                            // t as the mixed form's pair: its two end values, in order
+        float* L = a.tlo + gidx(g, 0, j, k);
+        auto get = [&](int i) -> double { return t_ld(F, L, (size_t)i * pl); };
+        t_st(F, L, 0, post_form(fb, get(1), get(2), get(3)));
+        t_st(F, L, (size_t)(im - 1) * pl, post_form(a.radius_form, get(im - 2), get(im - 3), get(im - 4)));
+        return;
+    }
     const bool species = n >= 4 && n <= 16;        // the twelve condensables and nh4sh
     if(im >= 8){
         // planes 1..3 and im-4..im-2 are disjoint from each other and from 0 and im-1: every
@@ -175,6 +186,13 @@ __global__ void __launch_bounds__(128) post_bc_theta_kernel(PostArgs<S> a){
         return;
     }
     S* F = a.thx[n - POST_NTHZ] + o;
+    if(n == POST_NTHZ && a.tlo){                    // t as the mixed form's pair
+        float* L = a.tlo + o;
+        auto get = [&](int j) -> double { return t_ld(F, L, (size_t)j * kp); };
+        t_st(F, L, 0, post_form(a.pole_form, get(1), get(2), get(3)));
+        t_st(F, L, (size_t)(jm - 1) * kp, post_form(a.pole_form, get(jm - 2), get(jm - 3), get(jm - 4)));
+        return;
+    }
     auto at = [&](int j) -> S& { return F[(size_t)j * kp]; };
     at(0) = (S)post_form(a.pole_form, (double)at(1), (double)at(2), (double)at(3));     // in order (jm < 5 overlaps)
     at(jm - 1) = (S)post_form(a.pole_form, (double)at(jm - 2), (double)at(jm - 3), (double)at(jm - 4));
@@ -189,6 +207,16 @@ __global__ void __launch_bounds__(128) post_bc_phi_kernel(PostArgs<S> a){
     if(r >= g.im * g.jm) return;
     const int km = g.km;
     S* F = a.rad[blockIdx.y] + (size_t)r * g.kp;
+    if(blockIdx.y == 0 && a.tlo){                   // t as the mixed form's pair
+        float* L = a.tlo + (size_t)r * g.kp;
+        if(a.phi_periodic){ F[km - 1] = F[0]; L[km - 1] = L[0]; }
+        else {
+            const double y = 0.5 * ((C43 * t_ld(F, L, 1) - C13 * t_ld(F, L, 2)) + (C43 * t_ld(F, L, km - 2) - C13 * t_ld(F, L, km - 3)));
+            t_st(F, L, 0, y);
+            t_st(F, L, km - 1, y);
+        }
+        return;
+    }
     if(a.phi_periodic) F[km - 1] = F[0];
     else {
         const double lo = C43 * (double)F[1] - C13 * (double)F[2];

@@ -41,6 +41,10 @@ struct StageArgs {
     RhsConst<C> k;
     C c_in, wgt;
     int stage;
+    // the mixed form's temperature pair (common.cuh): the low parts of t (written by stage 3) and of
+    // tn (read by stage 3); null in an FP64 context
+    float* tlo;
+    const float* tnlo;
 };
 
 template <typename S>
@@ -182,6 +186,16 @@ __device__ __forceinline__ void stage_update(const StageArgs<S, C>& a, S* W, con
         else if(kind == 3) y = cmax(y, a.k.dis_min);
         W[c.dY + off] = (S)y;
     } else {
+        if constexpr(sizeof(S) == 4){
+            if(kind == 1 && a.tlo){           // the temperature pair: y_n + dt acc / 6 in FP64
+                const double inc = (double)qdiv(a.k.dt * accv, C(6.0), C(1.0 / 6.0));
+                const double y = cclamp((double)yn + (double)a.tnlo[c.o] + inc, (double)a.k.t_min, (double)a.k.t_max);
+                const S h = (S)y;
+                W[c.dY + off] = h;
+                a.tlo[c.o] = (float)(y - (double)h);
+                return;
+            }
+        }
         C y = yn + qdiv(a.k.dt * accv, C(6.0), C(1.0 / 6.0));
         if(kind == 1) y = cclamp(y, a.k.t_min, a.k.t_max);
         else if(kind == 2) y = cclamp(cmax(y, C(0.0)), C(0.0), a.k.tke_max);
@@ -431,6 +445,18 @@ __device__ __forceinline__ void stage_update2(const StageArgs<S, C>& a, S* W, co
         if(kind == 2){ y0 = cclamp(y0, C(0.0), a.k.tke_max); y1 = cclamp(y1, C(0.0), a.k.tke_max); }
         else if(kind == 3){ y0 = cmax(y0, a.k.dis_min); y1 = cmax(y1, a.k.dis_min); }
     } else {
+        if constexpr(sizeof(S) == 4){
+            if(kind == 1 && a.tlo){           // the temperature pair: y_n + dt acc / 6 in FP64
+                const float2 ln = *reinterpret_cast<const float2*>(a.tnlo + c.o);
+                const double tmin = (double)a.k.t_min, tmax = (double)a.k.t_max;
+                const double z0 = cclamp((double)n0.nc + (double)ln.x + (double)qdiv(a.k.dt * acc0, C(6.0), C(1.0 / 6.0)), tmin, tmax);
+                const double z1 = cclamp((double)n1.nc + (double)ln.y + (double)qdiv(a.k.dt * acc1, C(6.0), C(1.0 / 6.0)), tmin, tmax);
+                const S h0 = (S)z0, h1 = (S)z1;
+                st2<S, C>(W + (c.dY + off), (C)h0, (C)h1);
+                *reinterpret_cast<float2*>(a.tlo + c.o) = make_float2((float)(z0 - (double)h0), (float)(z1 - (double)h1));
+                return;
+            }
+        }
         y0 = n0.nc + qdiv(a.k.dt * acc0, C(6.0), C(1.0 / 6.0)); y1 = n1.nc + qdiv(a.k.dt * acc1, C(6.0), C(1.0 / 6.0));
         if(kind == 1){ y0 = cclamp(y0, a.k.t_min, a.k.t_max); y1 = cclamp(y1, a.k.t_min, a.k.t_max); }
         else if(kind == 2){ y0 = cclamp(cmax(y0, C(0.0)), C(0.0), a.k.tke_max); y1 = cclamp(cmax(y1, C(0.0)), C(0.0), a.k.tke_max); }

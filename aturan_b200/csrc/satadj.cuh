@@ -49,6 +49,10 @@ struct SatArgs {
     long long nc_off;
     int sync;
     S* nh4sh;
+    // the mixed form's temperature pair (common.cuh): the low parts of t and of its n-copy; null in
+    // an FP64 context
+    float* tlo;
+    float* tnlo;
 };
 
 // The saturation vapour density rho ep svp(T) / p of the liquid (ice = false) or ice set.
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
     if(k < g.km){
         const size_t q = gidx(g, i, j, k);
         const SatConst& K = a.k;
-        double tt = (double)a.t[q];
+        double tt = t_ld(a.t, a.tlo, q);
         const double p_u = (double)__ldg(a.ps + q);
         double rho_c = K.r_mix;                               // rho_at, cUranusModel.h:526-531
         if(K.local_rho){ const double r_ = (double)__ldg(a.rho_mix + q); rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : K.r_mix; }
@@ -319,9 +323,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
             cP[q] = (S)c; clP[q] = (S)cloud; iP[q] = (S)ice;
             if(a.sync){ cP[q + a.nc_off] = (S)c; clP[q + a.nc_off] = (S)cloud; iP[q + a.nc_off] = (S)ice; }
         }
-        a.t[q] = (S)tt;
+        t_st(a.t, a.tlo, q, tt);
         if(a.sync){
-            a.t[q + a.nc_off] = (S)tt;
+            t_st(a.t + a.nc_off, a.tnlo, q, tt);
             if(a.sync == 2) a.nh4sh[q + a.nc_off] = a.nh4sh[q];
         }
     }
