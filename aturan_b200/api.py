@@ -38,6 +38,10 @@ SIGNATURES = {
     "aturan_upload_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "aturan_download_device": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "aturan_download_buoy_ref": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_upload_many": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "aturan_download_many": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int],
+                             ctypes.c_int),
+    "aturan_pressure_last": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_rk4_step": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_tape": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "aturan_restore_ncopies": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
@@ -66,7 +70,7 @@ SIGNATURES = {
     "aturan_mca": ([ctypes.c_void_p], ctypes.c_int),
 }
 
-STATIC_MAX_IM, STATIC_MAX_JM = 512, 4096
+STATIC_MAX_IM, STATIC_MAX_JM, STATIC_MAX_LEVEL_CELLS = 512, 4096, 1 << 30
 
 KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca"]
 NSPECIES = 13
@@ -245,6 +249,27 @@ class Context:
                                                       ctypes.c_void_p(int(x_ptr)), ctypes.byref(s), ctypes.byref(r)),
                          "pressure_solve")
         return rc, s.value, r.value
+
+    def upload_many(self, names, ptrs, on_device=False):
+        """aturan_upload_many: field names and host (or device) pointers of FP64 [i][j][k] arrays."""
+        n = len(names)
+        ids = (ctypes.c_int * n)(*[F.ID[x] for x in names])
+        ps = (ctypes.c_void_p * n)(*[ctypes.c_void_p(int(x)) for x in ptrs])
+        self._check(self.L.aturan_upload_many(self.h, n, ids, ps, 1 if on_device else 0), "upload_many")
+
+    def download_many(self, names, ptrs, on_device=False):
+        """aturan_download_many into host (or device) pointers of FP64 [i][j][k] arrays."""
+        n = len(names)
+        ids = (ctypes.c_int * n)(*[F.ID[x] for x in names])
+        ps = (ctypes.c_void_p * n)(*[ctypes.c_void_p(int(x)) for x in ptrs])
+        self._check(self.L.aturan_download_many(self.h, n, ids, ps, 1 if on_device else 0), "download_many")
+
+    def pressure_last(self):
+        """aturan_pressure_last: (sweeps, residual) of the last pressure solve."""
+        s = ctypes.c_int()
+        r = ctypes.c_double()
+        self._check(self.L.aturan_pressure_last(self.h, ctypes.byref(s), ctypes.byref(r)), "pressure_last")
+        return s.value, r.value
 
     def pressure(self, kind=0, omega=1.0, max_sweeps=1, tol=0.0):
         s = ctypes.c_int()

@@ -39,6 +39,7 @@ struct aturan_ctx {
     cudaStream_t st;           // every launch of the context, except:
     cudaStream_t st2;          // the saturation adjustment inside aturan_step (lower priority)
     cudaEvent_t ev_fork, ev_join;
+    cudaEvent_t ev_xcopy[2], ev_xpack[2];   // the batched transfers' staging ring (aturan_upload_many)
     char* mem;                 // one device allocation for everything below
     size_t mem_bytes;
     // storage-type groups (each field fstride elements)
@@ -72,6 +73,8 @@ struct aturan_ctx {
     double *lluT_a, *lluT_cf, *lluT_idn;
     float *r32, *e32;
     float* tlo;                // mixed form: the low parts of t and of tn (two FP32 fields; common.cuh), else null
+    int last_sweeps;           // the last aturan_pressure's sweeps and residual (aturan_pressure_last)
+    double last_resid;
     int sor_nblk;
     int sor_pm;                // Fourier modes per block of the column correction's tridiagonal solves
     std::vector<double> host_part;
@@ -830,16 +833,19 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     if(cudaStreamCreateWithPriority(&ctx->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess){
         cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_CUDA;
     }
-    if(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-       cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess){
-        cudaGetLastError();
-        if(ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-        cudaStreamDestroy(ctx->st2); cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_CUDA;
+    {
+        cudaEvent_t* evs[6] = {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_xcopy[0], &ctx->ev_xcopy[1],
+                               &ctx->ev_xpack[0], &ctx->ev_xpack[1]};
+        for(cudaEvent_t* e : evs){
+            if(cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess){
+                cudaGetLastError();
+                aturan_ctx_destroy(ctx); return ATURAN_E_CUDA;
+            }
+        }
     }
     if(cudaMalloc((void**)&ctx->mem, bytes) != cudaSuccess){
         cudaGetLastError();
-        cudaEventDestroy(ctx->ev_fork); cudaEventDestroy(ctx->ev_join);
-        cudaStreamDestroy(ctx->st2); cudaStreamDestroy(ctx->st); delete ctx; return ATURAN_E_NOMEM;
+        aturan_ctx_destroy(ctx); return ATURAN_E_NOMEM;
     }
     char* cur = ctx->mem;
     ctx->state = carve<char>(cur, 19 * fs * e);
@@ -1154,6 +1160,10 @@ int aturan_ctx_destroy(aturan_ctx* ctx){
     if(ctx->mem) cudaFree(ctx->mem);
     if(ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if(ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    for(int b = 0; b < 2; b++){
+        if(ctx->ev_xcopy[b]) cudaEventDestroy(ctx->ev_xcopy[b]);
+        if(ctx->ev_xpack[b]) cudaEventDestroy(ctx->ev_xpack[b]);
+    }
     if(ctx->st2) cudaStreamDestroy(ctx->st2);
     if(ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -1198,8 +1208,80 @@ static int xfer(aturan_ctx* ctx, int field, void* other, bool up, bool other_is_
     return ATURAN_OK;
 }
 
+// Several fields in one call. With host buffers the DMA copies run on the side stream and the
+// layout kernels on the main one, through two staging fields (stage64 and scratch, both free
+// between calls) used in turn: field q's copy overlaps field q-1's layout kernel, and the call
+// waits once, at the end, instead of once per field. Device buffers need no staging: the layout
+// kernels run back to back on the main stream.
+static int xfer_many(aturan_ctx* ctx, int n, const int* fields, void* const* ptrs, bool up, bool on_device){
+    if(!ctx || n < 0 || (n > 0 && (!fields || !ptrs))) return ATURAN_E_INVALID;
+    for(int q = 0; q < n; q++){
+        if(fields[q] < 0 || fields[q] >= ATURAN_NFIELDS) return fail(ctx, ATURAN_E_INVALID, "field id out of range");
+        if(!ptrs[q]) return fail(ctx, ATURAN_E_INVALID, "null buffer");
+    }
+    const Grid& g = ctx->g;
+    const size_t rows = (size_t)g.im * g.jm, nval = rows * g.km;
+    auto pack = [&](int field, const double* src, double* tgt) -> int {
+        bool is64;
+        void* dev = field_ptr(ctx, field, &is64);
+        float* lo = t_lo_of(ctx, field);
+        if(src){
+            if(is64)    launch_pack_in_f64(src, reinterpret_cast<double*>(dev), g.km, g.kp, rows, ctx->st);
+            else if(lo) launch_pack_in_pair(src, reinterpret_cast<float*>(dev), lo, g.km, g.kp, rows, ctx->st);
+            else        launch_pack_in_f32(src, reinterpret_cast<float*>(dev), g.km, g.kp, rows, ctx->st);
+        } else {
+            if(is64)    launch_pack_out_f64(reinterpret_cast<const double*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+            else if(lo) launch_pack_out_pair(reinterpret_cast<const float*>(dev), lo, tgt, g.km, g.kp, rows, ctx->st);
+            else        launch_pack_out_f32(reinterpret_cast<const float*>(dev), tgt, g.km, g.kp, rows, ctx->st);
+        }
+        CK_LAUNCH(src ? "layout in" : "layout out");
+        return ATURAN_OK;
+    };
+    if(on_device){
+        for(int q = 0; q < n; q++){
+            const int rc = up ? pack(fields[q], reinterpret_cast<const double*>(ptrs[q]), nullptr)
+                              : pack(fields[q], nullptr, reinterpret_cast<double*>(ptrs[q]));
+            if(rc) return rc;
+        }
+        if(!up) CK(cudaStreamSynchronize(ctx->st));
+        return ATURAN_OK;
+    }
+    double* buf[2] = {ctx->stage64, ctx->scratch};
+    // the staging fields are free only once the work already queued on the main stream is done
+    CK(cudaEventRecord(ctx->ev_fork, ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
+    for(int q = 0; q < n; q++){
+        const int b = q & 1;
+        if(up){
+            if(q >= 2) CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_xpack[b], 0));     // field q-2's layout has read buf[b]
+            CK(cudaMemcpyAsync(buf[b], ptrs[q], nval * 8, cudaMemcpyHostToDevice, ctx->st2));
+            CK(cudaEventRecord(ctx->ev_xcopy[b], ctx->st2));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->ev_xcopy[b], 0));
+            const int rc = pack(fields[q], buf[b], nullptr); if(rc) return rc;
+            CK(cudaEventRecord(ctx->ev_xpack[b], ctx->st));
+        } else {
+            if(q >= 2) CK(cudaStreamWaitEvent(ctx->st, ctx->ev_xcopy[b], 0));      // field q-2's copy has read buf[b]
+            const int rc = pack(fields[q], nullptr, buf[b]); if(rc) return rc;
+            CK(cudaEventRecord(ctx->ev_xpack[b], ctx->st));
+            CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_xpack[b], 0));
+            CK(cudaMemcpyAsync(ptrs[q], buf[b], nval * 8, cudaMemcpyDeviceToHost, ctx->st2));
+            CK(cudaEventRecord(ctx->ev_xcopy[b], ctx->st2));
+        }
+    }
+    CK(cudaEventRecord(ctx->ev_join, ctx->st2));
+    CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));
+    CK(cudaStreamSynchronize(ctx->st));
+    return ATURAN_OK;
+}
+
 int aturan_upload(aturan_ctx* ctx, int field, const double* host){ return xfer(ctx, field, (void*)host, true, false); }
 int aturan_download(aturan_ctx* ctx, int field, double* host){ return xfer(ctx, field, host, false, false); }
+int aturan_upload_many(aturan_ctx* ctx, int n, const int* fields, const double* const* src, int on_device){
+    return xfer_many(ctx, n, fields, const_cast<void* const*>(reinterpret_cast<const void* const*>(src)), true, on_device != 0);
+}
+int aturan_download_many(aturan_ctx* ctx, int n, const int* fields, double* const* dst, int on_device){
+    return xfer_many(ctx, n, fields, reinterpret_cast<void* const*>(dst), false, on_device != 0);
+}
 int aturan_upload_device(aturan_ctx* ctx, int field, const double* dev){ return xfer(ctx, field, (void*)dev, true, true); }
 int aturan_download_device(aturan_ctx* ctx, int field, double* dev){ return xfer(ctx, field, dev, false, true); }
 
@@ -1466,22 +1548,41 @@ int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, dou
     if(!ctx) return ATURAN_E_INVALID;
     if(sweeps_done) *sweeps_done = 0;
     if(resid) *resid = 0.0;
-    int rc;
+    ctx->last_sweeps = 0;
+    ctx->last_resid = 0.0;
+    int rc, s = 0;
+    double r = 0.0;
     switch(kind){
     case ATURAN_PRESS_GS_LEX:
         rc = ctx->mixed ? run_gs<float>(ctx) : run_gs<double>(ctx);
-        if(!rc && sweeps_done) *sweeps_done = 1;
-        return rc;
+        if(!rc) s = 1;
+        break;
     case ATURAN_PRESS_RB_SHARED:
         rc = ctx->mixed ? run_rb<float>(ctx, max_sweeps, 1.0) : run_rb<double>(ctx, max_sweeps, 1.0);
-        if(!rc && sweeps_done) *sweeps_done = max_sweeps < 1 ? 1 : max_sweeps;
-        return rc;
+        if(!rc) s = max_sweeps < 1 ? 1 : max_sweeps;
+        break;
     case ATURAN_PRESS_RB_SOR:
     case ATURAN_PRESS_RB_LINE:
-        return ctx->mixed ? run_sor<float>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, sweeps_done, resid)
-                          : run_sor<double>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, sweeps_done, resid);
+        rc = ctx->mixed ? run_sor<float>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, &s, &r)
+                        : run_sor<double>(ctx, omega, max_sweeps, tol, kind == ATURAN_PRESS_RB_LINE, &s, &r);
+        break;
+    default:
+        return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
     }
-    return fail(ctx, ATURAN_E_INVALID, "unknown pressure kind");
+    if(rc >= 0){
+        ctx->last_sweeps = s;
+        ctx->last_resid = r;
+        if(sweeps_done) *sweeps_done = s;
+        if(resid) *resid = r;
+    }
+    return rc;
+}
+
+int aturan_pressure_last(aturan_ctx* ctx, int* sweeps_done, double* resid){
+    if(!ctx) return ATURAN_E_INVALID;
+    if(sweeps_done) *sweeps_done = ctx->last_sweeps;
+    if(resid) *resid = ctx->last_resid;
+    return ATURAN_OK;
 }
 
 int aturan_pressure_solve(aturan_ctx* ctx, int kind, int transposed, double omega, int max_sweeps, double tol,

@@ -19,6 +19,7 @@ same workload; under torchrun only rank 0 runs it.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -52,9 +53,10 @@ def peaks():
 
 
 class ClockSampler:
-    """SM clocks and throttle reasons sampled every ~2 ms through NVML while the timed region runs
-    (nvidia-smi's 100 ms period would see a few-millisecond region once or not at all); falls
-    back to nvidia-smi when NVML is not importable. Reads only."""
+    """SM clocks and throttle reasons polled through NVML back to back (a 2 ms sleep between polls)
+    while the timed region runs; each poll takes three NVML queries, so a region of a few tens of
+    milliseconds sees only a few samples (`samples` in the result says how many). Falls back to
+    nvidia-smi (100 ms period) when NVML is not importable. Reads only."""
     REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
                ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
@@ -221,6 +223,44 @@ def algorithmic_stage_bytes(precision):
         else:          # FP32 storage except the FP64 pressure pair read by every stage
             total += (w - 2) * 4 + 2 * 8
     return total / 4 * N_CELLS
+
+
+def step_alg_bytes(precision, press, sweeps, N=N_CELLS):
+    """Algorithmic bytes of one full step (every value each kernel must read or write once, per
+    stored cell; FP32 words of 4 B in the mixed form except the FP64 pressure family):
+      RK4 stages   the stage words above (81 + 119 + 119 + 106 per cell)
+      prelude      level means (t, p_stat) and hydrostatic integral (t, p_stat, v, w; p_baro, p_b0,
+                   p_bfollow read, p_hydro and p_bfollow written: FP64)
+      satadj+sync  t, p_stat, rho_mix, 12 species read; t, 12 species written; their 13 n-copies and
+                   nh4sh's (read and written) by the fused sync; the mixed form adds the temperature
+                   pair's low parts (t read and written, tn written)
+      pressure     RB_LINE / RB_SOR: aux_u, v, w read and the FP64 source written; per sweep p and the
+                   source read, p written (FP32 correction sweeps in the mixed form); per residual check
+                   p and the source read (the mixed form also writes r and e in FP32); per column
+                   correction p read and written; the mixed form's refinement p += e. GS_LEX: the
+                   source (5 words) and one sweep (3 words)
+    sweeps: the pressure sweeps of each timed step (aturan_pressure_last)."""
+    mixed = precision == "mixed"
+    e = 4 if mixed else 8
+    rk = sum(((w - 2) * 4 + 2 * 8) if mixed else w * 8 for w in STAGE_WORDS)
+    prelude = 6 * e + 5 * 8
+    sat = 43 * e + (3 * 4 if mixed else 0)
+    S = statistics.mean(sweeps) if sweeps else 0.0
+    if press in ("line", "sor"):
+        every = 8 if press == "line" else 16
+        corr = math.ceil(S / every) if S else 0
+        if mixed:
+            inner = 2 if press == "line" else 48
+            refine = math.ceil(S / inner) if S else 0
+            pres = (3 * e + 8) + S * 3 * 4 + (refine + 1) * (2 * 8 + 2 * 4) + refine * (4 + 2 * 8) + corr * 2 * 4
+        else:
+            checks = (S + 1) if press == "line" else (math.ceil(S / 16) + 1)
+            pres = (3 * e + 8) + S * 3 * 8 + checks * 2 * 8 + corr * 2 * 8
+    else:
+        pres = 5 * 8 + 3 * 8 * max(S, 1.0)
+    out = {"rk4": rk * N, "prelude": prelude * N, "satadj_sync": sat * N, "pressure": pres * N}
+    out["total"] = sum(out.values())
+    return out
 
 
 def post_step_bytes(p, pp, e):
@@ -454,7 +494,10 @@ def run_reference_arm(args, rank, world):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "dynamical-core full step (pressure + 4 SatAdj + n-copy sync + RK4), 41x181x361, "
                                "FP64 on the host cores",
-                   "grid": [41, 181, 361], "cells": N_CELLS, "pressure": args.press},
+                   "grid": [41, 181, 361], "cells": N_CELLS,
+                   # the solve the reference ran: it has no solve to a residual, so every pressure kind
+                   # other than the shared red-black sweep times its default lexicographic GS sweep
+                   "pressure": "rb" if args.press == "rb" else "gs"},
         "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind, "sample": note},
         "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -565,14 +608,23 @@ def main():
 
     # ---- per-kernel device times of the same steps (event-bracketed pass) ----
     ctx.profile(timing=True)
+    sweeps = []
     for _ in range(K):
         step()
+        sweeps.append(ctx.pressure_last()[0])      # the step's pressure sweeps (a host-side value)
     prof = ctx.profile_read()
     n_stage, ms_stage = prof["rk_stage"]
     avg_stage_ms = ms_stage / max(n_stage, 1)
     alg = algorithmic_stage_bytes(args.precision)
     peak, peak_kind = peaks()
     achieved = alg / (avg_stage_ms / 1e3) / 1e9
+    step_alg = step_alg_bytes(args.precision, args.press, sweeps)
+    step_roof = {"achieved": step_alg["total"] / (ms_max / K / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": step_alg["total"] / (ms_max / K / 1e3) / 1e9 / peak, "alg_bytes_per_step": step_alg,
+                 "sweeps_per_step": statistics.mean(sweeps) if sweeps else None,
+                 "what": "every kernel of the step: the algorithmic bytes of the RK4 stages, the level means "
+                         "and hydrostatic integral, the saturation adjustment with its fused n-copy sync, and "
+                         "the pressure solve with its actual sweep count, divided by ms_per_step"}
     traffic = None
     tp = os.path.join(ROOT, "profiles", f"rk_stage_{args.precision}_traffic.json")
     if os.path.exists(tp):
@@ -592,15 +644,15 @@ def main():
     out_names = F.PROGNOSTIC + ["p_dyn", "p_hydro"] + F.PROJECTION
     pinned = {n: torch.from_numpy(np.ascontiguousarray(st[n])).pin_memory() for n in in_names}
     outs = {n: torch.empty(p.shape, dtype=torch.float64).pin_memory() for n in out_names}
+    in_ptrs = [pinned[n].data_ptr() for n in in_names]
+    out_ptrs = [outs[n].data_ptr() for n in out_names]
     barrier()
     E = max(1, args.e2e_steps)
     t0 = time.perf_counter()
     for _ in range(E):
-        for n in in_names:
-            ctx.L.aturan_upload(ctx.h, F.ID[n], pinned[n].data_ptr())
+        ctx.upload_many(in_names, in_ptrs)          # aturan_upload_many: one wait for all fields
         step()
-        for n in out_names:
-            ctx.L.aturan_download(ctx.h, F.ID[n], outs[n].data_ptr())
+        ctx.download_many(out_names, out_ptrs)      # aturan_download_many
     e2e_s = time.perf_counter() - t0
     e2e_value = replicas.throughput(N_CELLS, E, world, replicas.max_over_ranks(e2e_s, dist, device="cuda"))
     fbytes = p.im * p.jm * p.km * 8
@@ -662,7 +714,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": STAGE_KERNELS[args.precision], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs", "avg_launch_ms": avg_stage_ms,
-                         "alg_bytes_per_launch": alg},
+                         "alg_bytes_per_launch": alg, "step": step_roof},
             "kernels_ms_per_step": {k: v[1] / K for k, v in prof.items()},
             "kernels_ms_note": "device time per kind from events on the stream each kind runs on; the "
                                "saturation adjustment and the n-copy sync run on a second stream beside the "

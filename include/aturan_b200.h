@@ -156,13 +156,22 @@ const char* aturan_last_error(const aturan_ctx* ctx);   /* NULL: the last error 
                                                           without a context, on this thread */
 
 /* Copy one field between host memory (contiguous FP64 [i][j][k], im*jm*km values) and the
- * device. Upload is asynchronous on the context's stream from pinned memory, synchronous from
- * pageable memory; download returns when the data is on the host. */
+ * device. Both return when the host buffer may be reused (upload) or holds the data (download).
+ * In a mixed context t and tn are stored as the FP32 pair hi + lo (FP64 to ~2^-48), so they come
+ * back as uploaded; every other FP32 field comes back rounded to FP32. */
 int aturan_upload(aturan_ctx* ctx, int field, const double* host);
 int aturan_download(aturan_ctx* ctx, int field, double* host);
-/* As upload/download for a field on a device pointer (contiguous [i][j][k] FP64). */
+/* As upload/download for a field on a device pointer (contiguous [i][j][k] FP64). The upload is
+ * asynchronous on the context's stream. */
 int aturan_upload_device(aturan_ctx* ctx, int field, const double* dev);
 int aturan_download_device(aturan_ctx* ctx, int field, double* dev);
+/* n fields in one call: fields[q] from src[q] (to dst[q]); host buffers (pinned for overlap), or
+ * device buffers with on_device = 1. The host copies of field q overlap the on-device layout
+ * change of field q-1, and the call waits once instead of once per field (what a driver that
+ * exchanges the fields its CPU modules touch each iteration uses). Same return conditions as the
+ * one-field calls, except that a device upload is asynchronous. */
+int aturan_upload_many(aturan_ctx* ctx, int n, const int* fields, const double* const* src, int on_device);
+int aturan_download_many(aturan_ctx* ctx, int n, const int* fields, double* const* dst, int on_device);
 /* buoy_ref_level[im] of the last RK4 step (cUranusModel.h:1431). */
 int aturan_download_buoy_ref(aturan_ctx* ctx, double* host_im);
 
@@ -228,6 +237,12 @@ int aturan_pressure_adjoint(aturan_ctx* ctx, int kind, double omega, int max_swe
  * sweeps_done and resid (relative L2 residual at exit; RB_SOR only, else 0) may be NULL. */
 int aturan_pressure(aturan_ctx* ctx, int kind, double omega, int max_sweeps, double tol,
                     int* sweeps_done, double* resid);
+
+/* The sweeps and the residual of the context's last pressure solve, whether aturan_pressure or
+ * aturan_step ran it (aturan_step has no out-parameters); 0 and 0.0 before any. No counterpart in
+ * the reference, which prints no solver diagnostics for its single sweep. Either pointer may be
+ * NULL. */
+int aturan_pressure_last(aturan_ctx* ctx, int* sweeps_done, double* resid);
 
 /* Solve the pressure equation's folded operator, or its transpose, on caller buffers: the linear
  * solve inside ATURAN_PRESS_RB_SOR / RB_LINE, and with transposed = 1 the adjoint of that solve
@@ -348,20 +363,23 @@ int aturan_profile_read(aturan_ctx* ctx, double* ms, long* launches, int nkinds)
 /* The buoyancy reference level of RungeKutta_Uran_Turb.cpp:18-37 computed without allocating any
  * device memory; no counterpart in the reference, which has no device. It is for callers that may
  * not allocate: an application whose memory pool owns the whole GPU and hands this library only
- * the buffers it holds, or code issuing work while a stream is being captured into a CUDA graph
- * (where cudaMalloc is not allowed). t and p_stat are the caller's device arrays, contiguous FP64
- * [i][j][k] with k fastest (im*jm*km values); ref_out receives im doubles on the device.
- * The scratch (block partial sums and the sin(theta) weights) is a fixed array inside the library
- * image, so every GPU that loads the library holds 288 KiB until the process exits; it bounds the
- * grid to im <= ATURAN_STATIC_MAX_IM and jm <= ATURAN_STATIC_MAX_JM, larger grids are rejected with
- * ATURAN_E_INVALID (message in aturan_last_error(NULL)). The first call on a device looks the
- * array's address up (cudaGetSymbolAddress) with that device current; make it before any stream
- * capture. The call is asynchronous on `stream` (a cudaStream_t, NULL for the legacy default
- * stream). All calls on a device share the array: calls whose kernels may overlap on the GPU (on
- * unordered streams) race and must not be issued. The result equals aturan_rk4_step's level means
- * with exact_reductions = 0 (the same tree order). */
+ * the buffers it holds, or a plugin run under a fixed device-memory budget. t and p_stat are the
+ * caller's device arrays, contiguous FP64 [i][j][k] with k fastest (im*jm*km values); ref_out
+ * receives im doubles on the device.
+ * The scratch (block partial sums and the sin(theta) weights, both written by the call's own
+ * kernels) is a fixed array inside the library image, so every GPU that loads the library holds
+ * 288 KiB until the process exits; it bounds the grid to im <= ATURAN_STATIC_MAX_IM,
+ * jm <= ATURAN_STATIC_MAX_JM and jm * km <= ATURAN_STATIC_MAX_LEVEL_CELLS; larger grids are
+ * rejected with ATURAN_E_INVALID (message in aturan_last_error(NULL)). The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress) with that device current; make it before any
+ * stream capture. The call is asynchronous on `stream` (a cudaStream_t, NULL for the legacy default
+ * stream). All calls on a device share the array and each overwrites what it reads: calls whose
+ * kernels may overlap on the GPU (on unordered streams) race and must not be issued. The result
+ * agrees with aturan_rk4_step's level means with exact_reductions = 0 (the same tree order) to
+ * rounding: the weights' sin is the device's here, the host's there. */
 #define ATURAN_STATIC_MAX_IM 512
 #define ATURAN_STATIC_MAX_JM 4096
+#define ATURAN_STATIC_MAX_LEVEL_CELLS 1073741824
 int aturan_buoy_ref_level_static(const aturan_params* p, const double* t, const double* p_stat,
                                  double* ref_out, void* stream);
 

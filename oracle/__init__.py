@@ -22,12 +22,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 
+def reference_tree():
+    """Where the reference's sources lie: $ATURAN_REF, else the REF default of oracle/Makefile."""
+    env = os.environ.get("ATURAN_REF")
+    if env:
+        return env
+    with open(os.path.join(HERE, "Makefile")) as fh:
+        for line in fh:
+            if line.startswith("REF") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
 def build(quiet=True):
     """Compile liboracle.so (and, when the reference tree is present, oracle/_ref)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.check_call(["make", "-C", HERE, "liboracle.so"], stdout=out)
-    if os.path.isdir("/root/reference/planet"):
-        subprocess.check_call(["make", "-C", HERE, "-j8", "ref"], stdout=out)
+    ref = reference_tree()
+    if ref and os.path.isdir(os.path.join(ref, "planet")):
+        subprocess.check_call(["make", "-C", HERE, "-j8", "ref", f"REF={ref}"], stdout=out)
 
 
 def field_ptrs(state):

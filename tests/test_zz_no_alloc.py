@@ -1,11 +1,12 @@
 """The entry point that allocates nothing: aturan_buoy_ref_level_static.
 
 It serves callers that may not allocate device memory -- an application whose memory pool owns
-the GPU and hands the library only its own buffers, or work issued while a stream is captured
-into a CUDA graph -- by keeping its scratch in a fixed array inside the library. These tests call
-it through the C ABI on device buffers the test owns and compare it with the level means that
-aturan_rk4_step computes through a context (same tree order), on two calls in a row: the second
-call finds the scratch holding the first call's contents and must give the same answer.
+the GPU and hands the library only its own buffers, or a plugin run under a fixed device-memory
+budget -- by keeping its scratch in a fixed array inside the library. These tests call it through
+the C ABI on device buffers the test owns and compare it with the level means that
+aturan_rk4_step computes through a context (same tree order; the sin(theta) weights are the
+device's there and the host's here, so the two agree to rounding), on two calls in a row: the
+second call finds the scratch holding the first call's contents and must give the same answer.
 
 The file is named to be collected last, so a run that stops at the first failure has run every
 other test; it passes alone in a fresh process and after the others.
@@ -26,6 +27,12 @@ def test_static_entry_point_rejects_grids_beyond_its_scratch():
     rc = L.aturan_buoy_ref_level_static(ctypes.byref(p), dummy, dummy, dummy, None)
     assert rc == api.E_INVALID
     assert b"static scratch" in L.aturan_last_error(None)
+    # a level whose cells a 32-bit index cannot count
+    p = P.default_params()
+    p.jm, p.km = 4096, 300000
+    rc = L.aturan_buoy_ref_level_static(ctypes.byref(p), dummy, dummy, dummy, None)
+    assert rc == api.E_INVALID
+    assert b"level size" in L.aturan_last_error(None)
 
 
 @pytest.mark.gpu
