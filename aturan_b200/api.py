@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 from . import fields as F
-from .params import Params, PostParams, default_params, default_post_params
+from .params import ChemParams, Params, PostParams, default_chem_params, default_params, default_post_params
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
@@ -68,11 +68,16 @@ SIGNATURES = {
     "aturan_post_params_default": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_post_step": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_mca": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_chem_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_chemistry": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+                         ctypes.c_int),
 }
+
+CHEM_NH4SH_EQ, CHEM_FORCING = 1, 2
 
 STATIC_MAX_IM, STATIC_MAX_JM, STATIC_MAX_LEVEL_CELLS = 512, 4096, 1 << 30
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca", "chem"]
 NSPECIES = 13
 
 _LIB = None
@@ -113,6 +118,13 @@ def library_default_post_params():
     rc = load_library().aturan_post_params_default(ctypes.byref(pp))
     assert rc == 0
     return pp
+
+
+def library_default_chem_params():
+    cp = ChemParams()
+    rc = load_library().aturan_chem_params_default(ctypes.byref(cp))
+    assert rc == 0
+    return cp
 
 
 class Context:
@@ -206,6 +218,19 @@ class Context:
     def mca(self):
         """aturan_mca: the moist convective adjustment (ConvectiveAdjustment.h:402-849), default knobs."""
         self._check(self.L.aturan_mca(self.h), "mca")
+
+    def chemistry(self, what=CHEM_NH4SH_EQ | CHEM_FORCING, cp=None, counts=False):
+        """aturan_chemistry: the NH4SH equilibrium (cUranusModel.cpp:1034) and/or the chemistry
+        forcing (cUranusModel.cpp:1074-1087) with cp's constants (default: the reference's). With
+        counts=True returns (cells that formed NH4SH, cells that decomposed it) (synchronizes)."""
+        cp = default_chem_params() if cp is None else cp
+        if not counts:
+            self._check(self.L.aturan_chemistry(self.h, ctypes.byref(cp), int(what), None, None), "chemistry")
+            return None
+        nf, nd = ctypes.c_long(), ctypes.c_long()
+        self._check(self.L.aturan_chemistry(self.h, ctypes.byref(cp), int(what), ctypes.byref(nf),
+                                            ctypes.byref(nd)), "chemistry")
+        return nf.value, nd.value
 
     def tape(self, on=True):
         """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""

@@ -24,6 +24,7 @@
 #include "sor.cuh"
 #include "adjoint.cuh"
 #include "post.cuh"
+#include "chem.cuh"
 #include "mca.cuh"
 
 using namespace aturan;
@@ -49,6 +50,7 @@ struct aturan_ctx {
     void* acc;                 // 19
     void* forc;                // 22 pointwise RHS inputs
     void* proj;                // rhs_u, rhs_v, rhs_w, aux_u, aux_v, aux_w
+    void* chem;                // difflux_h2s, difflux_nh3, difflux_nh4sh
     void* pstat;               // p_stat
     // FP64 always
     double *pdyn, *phydro, *pbaro, *pb0, *pbf;
@@ -87,6 +89,7 @@ struct aturan_ctx {
     double* ahacc;             // the T tendencies' adjoint summed over the stages (heating gradient)
     double* heat;              // aturan_set_heating: [jm][km] K/s, or null
     double* mca_H;             // aturan_mca: the cp table's running integral, made at the first call
+    double* chem_tab;          // aturan_chemistry: radius, metric radius (im), sin, cos of the colatitude (jm)
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -275,6 +278,7 @@ void* field_ptr(aturan_ctx* c, int id, bool* is64){
     if(id >= ATURAN_TN && id < ATURAN_TN + ATURAN_NPROG) return (char*)c->ncopy + (size_t)(id - ATURAN_TN) * fs * e;
     if(id >= ATURAN_NUE && id <= ATURAN_DIS_SOURCE) return (char*)c->forc + (size_t)(id - ATURAN_NUE) * fs * e;
     if(id >= ATURAN_RHS_U && id <= ATURAN_AUX_W) return (char*)c->proj + (size_t)(id - ATURAN_RHS_U) * fs * e;
+    if(id >= ATURAN_DIFFLUX_H2S && id <= ATURAN_DIFFLUX_NH4SH) return (char*)c->chem + (size_t)(id - ATURAN_DIFFLUX_H2S) * fs * e;
     if(id == ATURAN_P_STAT) return c->pstat;
     *is64 = true;
     switch(id){
@@ -674,18 +678,25 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
     const size_t fs = g.fstride;
     S* X = reinterpret_cast<S*>(ctx->state);
     S* Fo = reinterpret_cast<S*>(ctx->forc);
-    auto fld = [&](int id) -> S* { return id < ATURAN_NPROG ? X + (size_t)id * fs : Fo + (size_t)(id - ATURAN_NUE) * fs; };
+    S* Ch = reinterpret_cast<S*>(ctx->chem);
+    auto fld = [&](int id) -> S* {
+        if(id >= ATURAN_DIFFLUX_H2S) return Ch + (size_t)(id - ATURAN_DIFFLUX_H2S) * fs;
+        return id < ATURAN_NPROG ? X + (size_t)id * fs : Fo + (size_t)(id - ATURAN_NUE) * fs;
+    };
+    // the phi pass takes the first POST_NPHI: all but difflux_nh4sh (BC_Uran.cpp:73-88)
     static const int RAD[POST_NRAD] = { ATURAN_T, ATURAN_U, ATURAN_V, ATURAN_W,       // BC_Uran.cpp:21-41
         ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
         ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
         ATURAN_NH4SH, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH,
-        ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX };
+        ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX, ATURAN_DIFFLUX_H2S, ATURAN_DIFFLUX_NH3,
+        ATURAN_DIFFLUX_NH4SH };
     static const int THX[POST_NTHX] = { ATURAN_T, ATURAN_U,                             // BC_Uran.cpp:43-59
         ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
         ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
         ATURAN_NH4SH, ATURAN_THERMALMASSFLUX };
     static const int THZ[POST_NTHZ] = { ATURAN_V, ATURAN_W, ATURAN_MASSFLUX_H2S,         // BC_Uran.cpp:61-71
-        ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH };
+        ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH, ATURAN_DIFFLUX_H2S,
+        ATURAN_DIFFLUX_NH3, ATURAN_DIFFLUX_NH4SH };
     static const int SP[POST_NSP] = { ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,      // BC_Uran.h:83-89
         ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
         ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_NH4SH };
@@ -726,6 +737,50 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
             if(clamp_cells) clamp_cells[n] = (long)h[POST_NSP + n];
         }
     }
+    return ATURAN_OK;
+}
+
+// The chemistry on the context's fields (aturan_chemistry).
+template <typename S>
+int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what){
+    const Grid& g = ctx->g;
+    const size_t fs = g.fstride;
+    const aturan_params& p = ctx->p;
+    S* X = reinterpret_cast<S*>(ctx->state);
+    S* Fo = reinterpret_cast<S*>(ctx->forc);
+    S* Ch = reinterpret_cast<S*>(ctx->chem);
+    auto fo = [&](int id) -> S* { return Fo + (size_t)(id - ATURAN_NUE) * fs; };
+    ChemArgs<S> a;
+    a.g = g;
+    a.t = X + (size_t)ATURAN_T * fs; a.nh3 = X + (size_t)ATURAN_NH3 * fs;
+    a.h2s = X + (size_t)ATURAN_H2S * fs; a.nh4sh = X + (size_t)ATURAN_NH4SH * fs;
+    a.tlo = ctx->tlo;
+    a.u = X + (size_t)ATURAN_U * fs; a.v = X + (size_t)ATURAN_V * fs; a.w = X + (size_t)ATURAN_W * fs;
+    a.ps = reinterpret_cast<const S*>(ctx->pstat);
+    a.rho_mix = fo(ATURAN_RHO_MIX); a.tmf = fo(ATURAN_THERMALMASSFLUX);
+    a.mf_h2s = fo(ATURAN_MASSFLUX_H2S); a.mf_nh3 = fo(ATURAN_MASSFLUX_NH3); a.mf_nh4sh = fo(ATURAN_MASSFLUX_NH4SH);
+    a.fl = fo(ATURAN_FLUXLIM_NH4SH);
+    a.df_h2s = Ch; a.df_nh3 = Ch + fs; a.df_nh4sh = Ch + 2 * fs;
+    a.tab.rad = ctx->chem_tab; a.tab.rmm = ctx->chem_tab + g.im;
+    a.tab.sin = ctx->chem_tab + 2 * g.im; a.tab.cos = ctx->chem_tab + 2 * g.im + g.jm;
+    ChemConst& c = a.c;
+    c.t_ref = p.t_ref; c.R_mix = p.R_mix; c.r_mix = p.r_mix; c.cp_mix = p.cp_mix;
+    c.L_f = 4705.0 * std::log(10.0) * 8314.46 / 51.1114;                    // ChemistryUran.h:132
+    c.m_nh3 = cp->m_nh3; c.m_h2s = cp->m_h2s; c.m_nh4sh = cp->m_nh4sh;
+    const double nu_mix = p.mue_mix / p.r_mix;                                // ChemistryUran.h:303-309
+    c.D_nh3 = nu_mix / p.sc_nh3; c.D_h2s = nu_mix / p.sc_h2s;
+    c.DT_nh3 = nu_mix / p.sc_nh3; c.DT_h2s = nu_mix / p.sc_h2s;
+    c.D_nh4sh = cp->D_nh4sh; c.DT_nh4sh = cp->DT_nh4sh; c.c_mix = cp->c_mix;
+    c.cp_nh3 = cp->cp_nh3; c.cp_h2s = cp->cp_h2s; c.cp_nh4sh = cp->cp_nh4sh;
+    c.k_nh3 = cp->k_nh3; c.k_h2s = cp->k_h2s; c.k_nh4sh = cp->k_nh4sh;
+    c.dr = p.dr; c.dthe = p.dthe; c.dphi = p.dphi;
+    c.dsign = cp->difflux_plus ? 1.0 : -1.0;                                  // ChemistryUran.h:64-65
+    c.sinthe_min = p.sinthe_min; c.floor = cp->polar_floor;
+    c.per = cp->phi_periodic != 0;
+    a.counts = ctx->counters + 4;
+    Region reg(ctx, ATURAN_K_CHEM, 0);
+    reg.n = launch_chem(a, what, ctx->st);
+    CK_LAUNCH("chemistry");
     return ATURAN_OK;
 }
 
@@ -798,7 +853,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     size_t bytes = 0;
     auto add = [&](size_t n){ bytes += round_up(n, 256); };
     add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e);
-    add(22 * fs * e); add(6 * fs * e); add(fs * e);
+    add(22 * fs * e); add(6 * fs * e); add(3 * fs * e); add(fs * e);
     for(int n = 0; n < 7; n++) add(fs * 8);                   // pdyn phydro pbaro pb0 pbf scratch stage64
     add(g.im * 8); add(2 * (size_t)g.im * ctx->nblk * 8);
     // the exact level means (FP64 with exact_reductions): terms, chunk sums, binades, units
@@ -808,6 +863,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     const size_t nbx_all = (size_t)g.im * ctx->bx.nbx;
     if(bx_on){ add(2 * g.im * ncell * 8); add(3 * nbx_all * 8); add(2 * nbx_all * 4); add(4 * nbx_all * 8); }
     add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
+    add((size_t)(2 * g.im + 2 * g.jm) * 8);
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
     ctx->sor_nblk = ((sN + 31) / 32) * sJ;
@@ -855,6 +911,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->acc = carve<char>(cur, 19 * fs * e);
     ctx->forc = carve<char>(cur, 22 * fs * e);
     ctx->proj = carve<char>(cur, 6 * fs * e);
+    ctx->chem = carve<char>(cur, 3 * fs * e);
     ctx->pstat = carve<char>(cur, fs * e);
     ctx->pdyn = carve<double>(cur, fs); ctx->phydro = carve<double>(cur, fs);
     ctx->pbaro = carve<double>(cur, fs); ctx->pb0 = carve<double>(cur, fs); ctx->pbf = carve<double>(cur, fs);
@@ -870,6 +927,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     }
     ctx->wsin = carve<double>(cur, g.jm); ctx->rm_i = carve<double>(cur, g.im); ctx->cor_j = carve<double>(cur, g.jm);
     ctx->cp_tab64 = carve<double>(cur, CP_TABLE_N);
+    ctx->chem_tab = carve<double>(cur, 2 * (size_t)g.im + 2 * (size_t)g.jm);
     ctx->geo = carve<char>(cur, nij * sgeo);
     ctx->cp_tab = carve<char>(cur, CP_TABLE_N * e);
     ctx->gsw = carve<GSW>(cur, nij); ctx->rbw = carve<RBW>(cur, nij);
@@ -1104,6 +1162,10 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     bad |= up(ctx->rm_i, rm_i.data(), g.im * 8);
     bad |= up(ctx->cor_j, cor_j.data(), g.jm * 8);
     bad |= up(ctx->cp_tab64, cp64.data(), CP_TABLE_N * 8);
+    std::vector<double> chem_tab(2 * (size_t)g.im + 2 * (size_t)g.jm);
+    for(int i = 0; i < g.im; i++){ chem_tab[i] = rad[i]; chem_tab[g.im + i] = rm_i[i]; }
+    for(int j = 0; j < g.jm; j++){ chem_tab[2 * g.im + j] = std::sin(the[j]); chem_tab[2 * g.im + g.jm + j] = std::cos(the[j]); }
+    bad |= up(ctx->chem_tab, chem_tab.data(), chem_tab.size() * 8);
     bad |= up(ctx->gsw, gsw.data(), nij * sizeof(GSW));
     bad |= up(ctx->rbw, rbw.data(), nij * sizeof(RBW));
     bad |= up(ctx->sor_ct, sct.data(), sct.size() * 8);
@@ -1703,6 +1765,43 @@ int aturan_mca(aturan_ctx* ctx){
     Region reg(ctx, ATURAN_K_MCA, first ? 2 : 1);
     launch_mca(a, ctx->mca_H, first, ctx->st);
     CK_LAUNCH("moist convective adjustment");
+    return ATURAN_OK;
+}
+
+int aturan_chem_params_default(aturan_chem_params* cp){
+    if(!cp) return ATURAN_E_INVALID;
+    std::memset(cp, 0, sizeof(*cp));
+    cp->abi_version = ATURAN_ABI_VERSION;
+    cp->nh4sh_eq = 1; cp->difflux_plus = 1; cp->difflux_laplacian = 1; cp->phi_periodic = 1;
+    cp->m_nh3 = 17.03052; cp->m_h2s = 34.08088; cp->m_nh4sh = 51.1114;       // cUranusModel.h:997-999
+    // ThermalPropertiesUran's sum of the species' molar densities c_x = r_x / m_x
+    cp->c_mix = 0x1.12b14645f7a58p+0;
+    cp->D_nh4sh = 1.45e-9; cp->DT_nh4sh = 1.45e-9;                           // cUranusModel.h:1135-1140
+    cp->cp_nh3 = 2.19e3; cp->cp_h2s = 2.24e3; cp->cp_nh4sh = 2.00e3;         // :1085-1087
+    cp->k_nh3 = 0.02102; cp->k_h2s = 0.013; cp->k_nh4sh = 0.02102;          // :1076-1078
+    cp->polar_floor = 0.4;                                                   // ATPhys.h:104-107
+    return ATURAN_OK;
+}
+
+int aturan_chemistry(aturan_ctx* ctx, const aturan_chem_params* cp, int what, long* n_formed, long* n_decomposed){
+    if(!ctx || !cp) return ATURAN_E_INVALID;
+    if(cp->abi_version != ATURAN_ABI_VERSION) return fail(ctx, ATURAN_E_INVALID, "abi_version mismatch");
+    if(what & ~(ATURAN_CHEM_NH4SH_EQ | ATURAN_CHEM_FORCING)) return fail(ctx, ATURAN_E_INVALID, "unknown chemistry part");
+    if(cp->nh4sh_eq != 1) return fail(ctx, ATURAN_E_UNSUPPORTED, "only the NH4SH equilibrium form (nh4sh_eq = 1) is implemented");
+    if(cp->difflux_laplacian != 1) return fail(ctx, ATURAN_E_UNSUPPORTED, "only difflux_laplacian = 1 is implemented");
+    const bool count = (what & ATURAN_CHEM_NH4SH_EQ) && (n_formed || n_decomposed);
+    if(count) CK(cudaMemsetAsync(ctx->counters + 4, 0, 2 * sizeof(unsigned long long), ctx->st));
+    const int rc = ctx->mixed ? run_chem<float>(ctx, cp, what) : run_chem<double>(ctx, cp, what);
+    if(rc) return rc;
+    if(n_formed) *n_formed = 0;
+    if(n_decomposed) *n_decomposed = 0;
+    if(count){
+        unsigned long long h[2];
+        CK(cudaMemcpyAsync(h, ctx->counters + 4, sizeof h, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if(n_formed) *n_formed = (long)h[0];
+        if(n_decomposed) *n_decomposed = (long)h[1];
+    }
     return ATURAN_OK;
 }
 

@@ -1,0 +1,260 @@
+// The chemistry of the iteration loop in its equilibrium form (planet/ChemistryUran.h,
+// FluxLimiter.h): the NH4SH equilibrium (EquilibriumNH4SH("loop"), cUranusModel.cpp:1034) and the
+// chemistry forcing (DiffMassFluxUran, ChemMassRateUran, FluxLimiterNH4SH and the 1-2-1 filters
+// between them, cUranusModel.cpp:1074-1087).
+//
+// The equilibrium is cell-local: one thread per cell brackets and bisects the cell's
+// K_p(T) condition (at most 82 evaluations of pow). The forcing is two 7-point stencil passes
+// over the interior (the diffusive tendencies and the thermal mass flux; then the mass rates and
+// the Superbee limiter) with the filters of post.cuh between and after them; every pass streams a
+// few planes of the state and is bound by HBM. Arithmetic is FP64 on the stored values (FP32
+// storage in the mixed form is widened, computed in FP64 and rounded back), in the reference's
+// operand order; the per-level and per-latitude factors (radius, metric radius, sin and cos of
+// the colatitude) come from a host table made with the host's libm, so the FP64 forcing equals
+// the CPU's bit for bit.
+#pragma once
+#include "common.cuh"
+
+namespace aturan {
+
+struct ChemConst {
+    double t_ref, R_mix, r_mix, cp_mix, L_f;          // equilibrium
+    double m_nh3, m_h2s, m_nh4sh;
+    double D_nh3, D_h2s, DT_nh3, DT_h2s, D_nh4sh, DT_nh4sh, c_mix;
+    double cp_nh3, cp_h2s, cp_nh4sh, k_nh3, k_h2s, k_nh4sh;
+    double dr, dthe, dphi, dsign;
+    double sinthe_min, floor;                         // the model's polar metric floor; ATPhys's divisor floor
+    int per;                                          // the periodic phi seam
+};
+
+// Host table made with the host's libm: radius, metric radius (im each), sin and cos of the
+// colatitude (jm each).
+struct ChemTab {
+    const double *rad, *rmm, *sin, *cos;
+};
+
+template <typename S>
+struct ChemArgs {
+    Grid g;
+    S *t, *nh3, *h2s, *nh4sh;
+    float* tlo;                                       // the mixed form's temperature pair, else null
+    const S *u, *v, *w, *ps;
+    S *rho_mix, *tmf, *mf_h2s, *mf_nh3, *mf_nh4sh, *fl, *df_h2s, *df_nh3, *df_nh4sh;
+    ChemTab tab;
+    ChemConst c;
+    unsigned long long* counts;                       // [formed, decomposed]
+};
+
+__device__ __forceinline__ double chem_max(double a, double b){ return (a < b) ? b : a; }   // std::max
+__device__ __forceinline__ double chem_min(double a, double b){ return (b < a) ? b : a; }   // std::min
+
+// ChemistryUran.h:144 and :154-156
+__device__ __forceinline__ double nh4sh_kp(double T){
+    const double atm = 101325.0;
+    return pow(10.0, 14.82 - 4705.0 / T) * atm * atm;
+}
+__device__ __forceinline__ double nh4sh_f(double x, double T0, double heat, double a, double b){
+    const double T = T0 + heat * x, RT = 8314.46 * T;
+    return (a - x) * (b - x) * RT * RT - nh4sh_kp(T);
+}
+
+// ChemistryUran.h:140-177 per cell, :210-275 over every cell; counts formed / decomposed cells.
+template <typename S>
+__global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
+    int formed = 0, decomposed = 0;
+    if(k < g.km){
+        const ChemConst& c = a.c;
+        const size_t q = gidx(g, i, j, k);
+        const double T0 = t_ld(a.t, a.tlo, q) * c.t_ref;
+        if(T0 > 0.0){
+            double rho = (double)a.ps[q] * 1e5 / (c.R_mix * T0);
+            if(!(rho > 0.0) || !isfinite(rho)) rho = c.r_mix;
+            const double n3 = (double)a.nh3[q], hs = (double)a.h2s[q], ns = (double)a.nh4sh[q];
+            const double A = chem_max(0.0, n3) / c.m_nh3;
+            const double B = chem_max(0.0, hs) / c.m_h2s;
+            const double Sx = chem_max(0.0, ns) / c.m_nh4sh;
+            const double heat = c.L_f * c.m_nh4sh / (c.cp_mix * rho);
+            const double f0 = nh4sh_f(0.0, T0, heat, A, B);
+            double lo = 0.0, hi = 0.0;
+            bool go = true;
+            if(f0 > 0.0){ lo = 0.0; hi = chem_min(A, B); }
+            else if(Sx > 0.0){
+                if(nh4sh_f(-Sx, T0, heat, A, B) <= 0.0){ lo = hi = -Sx; }
+                else { lo = -Sx; hi = 0.0; }
+            } else go = false;
+            if(go){
+                if(hi > lo){
+                    const double stop = 1.0e-15 * chem_max(A, chem_max(B, Sx));
+                    for(int it = 0; it < 80; it++){
+                        const double xm = 0.5 * (lo + hi);
+                        if(nh4sh_f(xm, T0, heat, A, B) > 0.0) lo = xm; else hi = xm;
+                        if(hi - lo <= stop) break;
+                    }
+                }
+                const double x = (f0 > 0.0) ? lo : hi;
+                if(x != 0.0){
+                    a.nh3[q] = (S)chem_max(0.0, n3 - c.m_nh3 * x);
+                    a.h2s[q] = (S)chem_max(0.0, hs - c.m_h2s * x);
+                    a.nh4sh[q] = (S)chem_max(0.0, ns + c.m_nh4sh * x);
+                    const double dT = heat * x;
+                    t_st(a.t, a.tlo, q, (T0 + dT) / c.t_ref);
+                    if(x > 0.0) formed = 1; else decomposed = 1;
+                }
+            }
+        }
+    }
+    // counts: a warp sum, one atomic per warp
+    formed = __reduce_add_sync(0xffffffffu, formed);
+    decomposed = __reduce_add_sync(0xffffffffu, decomposed);
+    if((threadIdx.x & 31) == 0 && (formed | decomposed)){
+        if(formed) atomicAdd(a.counts, (unsigned long long)formed);
+        if(decomposed) atomicAdd(a.counts + 1, (unsigned long long)decomposed);
+    }
+}
+
+// ChemistryUran.h:601-686 without SeaMount cells: the central first differences of x at (i, j, k)
+template <typename S>
+__device__ __forceinline__ void chem_d1(const S* x, size_t q, size_t pl, size_t kp, int dkw, int dke,
+                                        const ChemConst& c, double& dr_, double& dt_, double& dp_){
+    dr_ = ((double)x[q + pl] - (double)x[q - pl]) / (2.0 * c.dr);
+    dt_ = ((double)x[q + kp] - (double)x[q - kp]) / (2.0 * c.dthe);
+    dp_ = ((double)x[q + dke] - (double)x[q - dkw]) / (2.0 * c.dphi);
+}
+// ChemistryUran.h:576-598 (exp_rm = 1: coord_stretching is false)
+template <typename S>
+__device__ __forceinline__ double chem_lap(const S* x, size_t q, size_t pl, size_t kp, int dkw, int dke,
+                                           double rm, double rmsinthe, double costhe, const ChemConst& c){
+    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
+    const double v = (double)x[q];
+    const double xip = (double)x[q + pl], xim = (double)x[q - pl];
+    const double xjp = (double)x[q + kp], xjm = (double)x[q - kp];
+    const double xkp = (double)x[q + dke], xkm = (double)x[q - dkw];
+    const double d2cdr2 = (xip - 2.0 * v + xim) / (c.dr * c.dr) * exp_2_rm;
+    const double d2cdthe2 = (xjp - 2.0 * v + xjm) / (c.dthe * c.dthe);
+    const double d2cdphi2 = (xkp - 2.0 * v + xkm) / (c.dphi * c.dphi);
+    const double dcdr = (xip - xim) / (2.0 * c.dr) * exp_rm;
+    const double dcdthe = (xjp - xjm) / (2.0 * c.dthe);
+    return d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) + costhe / (rm * rmsinthe) * dcdthe
+         + d2cdphi2 / (rmsinthe * rmsinthe);
+}
+
+// The phi neighbours' offsets k-1 and k+1 of k in a row: round the ring of km-1 meridians with the
+// periodic seam, else the plain neighbours (k runs over 1..km-2 then).
+__device__ __forceinline__ void chem_kn(int k, int km, int per, int& dkw, int& dke){
+    dkw = per ? k - phi_wrap(k - 1, km) : 1;
+    dke = per ? phi_wrap(k + 1, km) - k : 1;
+}
+
+// rho_mix on every cell (ChemistryUran.h:312-320); on the interior the thermal mass flux and the
+// diffusive tendencies difflux_x = D_x lap(c_x) (passes 1 and 2, ChemistryUran.h:322-419, with
+// j_* formed at the cell where pass 2 reads them).
+template <typename S>
+__global__ void __launch_bounds__(128) chem_diff_kernel(ChemArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
+    if(k >= g.km) return;
+    const ChemConst& c = a.c;
+    const size_t q = gidx(g, i, j, k);
+    const double t0 = t_ld(a.t, a.tlo, q);
+    a.rho_mix[q] = (S)((double)a.ps[q] * 1e5 / (c.R_mix * t0 * c.t_ref));
+    const int k_first = c.per ? 0 : 1;
+    if(i < 1 || i > g.im - 2 || j < 1 || j > g.jm - 2 || k < k_first || k > g.km - 2) return;
+    const size_t pl = (size_t)g.jm * g.kp, kp = (size_t)g.kp;
+    int dkw, dke;
+    chem_kn(k, g.km, c.per, dkw, dke);
+    // pass 1's metric: the raw radius and max(sinthe_min, |sin|)
+    const double rm = a.tab.rad[i];
+    const double rmsinthe = rm * chem_max(c.sinthe_min, fabs(a.tab.sin[j]));
+    double dtdr, dtdthe, dtdphi;
+    if(a.tlo){
+        const double tip = t_ld(a.t, a.tlo, q + pl), tim = t_ld(a.t, a.tlo, q - pl);
+        const double tjp = t_ld(a.t, a.tlo, q + kp), tjm = t_ld(a.t, a.tlo, q - kp);
+        const double tkp = t_ld(a.t, a.tlo, q + dke), tkm = t_ld(a.t, a.tlo, q - dkw);
+        dtdr = (tip - tim) / (2.0 * c.dr);
+        dtdthe = (tjp - tjm) / (2.0 * c.dthe);
+        dtdphi = (tkp - tkm) / (2.0 * c.dphi);
+    } else chem_d1(a.t, q, pl, kp, dkw, dke, c, dtdr, dtdthe, dtdphi);
+    double hr, ht, hp, nr, nt, np, sr, stt, sp;
+    chem_d1(a.h2s, q, pl, kp, dkw, dke, c, hr, ht, hp);
+    chem_d1(a.nh3, q, pl, kp, dkw, dke, c, nr, nt, np);
+    chem_d1(a.nh4sh, q, pl, kp, dkw, dke, c, sr, stt, sp);
+    const double jT_nh3 = c.DT_nh3 / t0 * dtdr;
+    const double jT_h2s = c.DT_h2s / t0 * dtdr;
+    const double jT_nh4sh = c.DT_nh4sh / t0 * dtdr;
+    const double d_nh3 = nr + fabs(nt) / rm + np / rmsinthe;
+    const double d_h2s = hr + fabs(ht) / rm + hp / rmsinthe;
+    const double d_nh4sh = sr + fabs(stt) / rm + sp / rmsinthe;
+    const double j_nh3 = c.c_mix / c.r_mix * (c.m_nh3 * c.D_nh3 * d_nh3 - jT_nh3);
+    const double j_h2s = c.c_mix / c.r_mix * (c.m_h2s * c.D_h2s * d_h2s - jT_h2s);
+    const double j_nh4sh = c.c_mix / c.r_mix * (c.m_nh4sh * c.D_nh4sh * d_nh4sh - jT_nh4sh);
+    const double w0 = 0.0;                            // w_nh3, w_h2s, w_nh4sh in the equilibrium form
+    a.tmf[q] = (S)((j_nh3 * c.cp_nh3 + j_h2s * c.cp_h2s + j_nh4sh * c.cp_nh4sh)
+                   * (dtdr + fabs(dtdthe) / rm + dtdphi / rmsinthe)
+                   + t0 * (w0 * c.k_nh3 + w0 * c.k_h2s + w0 * c.k_nh4sh));
+    // the Laplacian's metric: the metric radius and max(sin, floor)
+    const double rml = a.tab.rmm[i];
+    const double rmsl = rml * chem_max(a.tab.sin[j], c.floor);
+    const double cl = a.tab.cos[j];
+    a.df_h2s[q] = (S)(c.D_h2s * chem_lap(a.h2s, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
+    a.df_nh3[q] = (S)(c.D_nh3 * chem_lap(a.nh3, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
+    a.df_nh4sh[q] = (S)(c.D_nh4sh * chem_lap(a.nh4sh, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
+}
+
+// FluxLimiter.h:68-70
+__device__ __forceinline__ double chem_superbee(double r){
+    return chem_max(0.0, chem_max(chem_min(2.0 * r, 1.0), chem_min(r, 2.0)));
+}
+
+// On the interior: massflux_x = w_x + sign difflux_x with w_x = 0 (ChemistryUran.h:38-110) and
+// the Superbee correction fluxlim_nh4sh (FluxLimiter.h:89-186).
+template <typename S>
+__global__ void __launch_bounds__(128) chem_limit_kernel(ChemArgs<S> a){
+    const Grid& g = a.g;
+    const ChemConst& c = a.c;
+    const int k_first = c.per ? 0 : 1;
+    const int k = k_first + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, i = 1 + blockIdx.z;
+    if(k > g.km - 2) return;
+    const size_t o = gidx(g, i, j, k), pl = (size_t)g.jm * g.kp, kp = (size_t)g.kp;
+    a.mf_h2s[o] = (S)(0.0 + c.dsign * (double)a.df_h2s[o]);
+    a.mf_nh3[o] = (S)(0.0 + c.dsign * (double)a.df_nh3[o]);
+    a.mf_nh4sh[o] = (S)(0.0 + c.dsign * (double)a.df_nh4sh[o]);
+    const S* x = a.nh4sh;
+    int dkw, dke;
+    chem_kn(k, g.km, c.per, dkw, dke);
+    const double q = (double)x[o], q_rp = (double)x[o + pl], q_rm = (double)x[o - pl];
+    const double q_tp = (double)x[o + kp], q_tm = (double)x[o - kp];
+    const double q_pp = (double)x[o + dke], q_pm = (double)x[o - dkw];
+    const double uu = (double)a.u[o], vv = (double)a.v[o], ww = (double)a.w[o];
+    const double rm = a.tab.rmm[i];
+    const double sinthe = chem_max(c.floor, fabs(a.tab.sin[j]));
+    const double inv_rm = 1.0 / rm, inv_rmsinthe = 1.0 / (rm * sinthe);
+    const double eps = 1.0e-12;
+    double corr = 0.0;
+    {
+        const double df = q_rp - q, db = q - q_rm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        const double r = (uu >= 0.0) ? db / denom : ((i + 2 < g.im ? (double)x[o + 2 * pl] : q_rp) - q_rp) / denom;
+        corr += (1.0 - chem_superbee(r)) * fabs(uu) * (df - db) / (2.0 * c.dr);
+    }
+    {
+        const double df = q_tp - q, db = q - q_tm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        const double q_far = (j + 2 < g.jm) ? (double)x[o + 2 * kp] : (C43 * q_tp - C13 * q);
+        const double r = (vv >= 0.0) ? db / denom : (q_far - q_tp) / denom;
+        corr += (1.0 - chem_superbee(r)) * fabs(vv) * inv_rm * (df - db) / (2.0 * c.dthe);
+    }
+    {
+        const double df = q_pp - q, db = q - q_pm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        double q2;
+        if(c.per) q2 = (double)x[o - k + phi_wrap(k + 2, g.km)];
+        else q2 = (k + 2 < g.km) ? (double)x[o + 2] : q_pp;
+        const double r = (ww >= 0.0) ? db / denom : (q2 - q_pp) / denom;
+        corr += (1.0 - chem_superbee(r)) * fabs(ww) * inv_rmsinthe * (df - db) / (2.0 * c.dphi);
+    }
+    a.fl[o] = (S)corr;
+}
+
+}  // namespace aturan

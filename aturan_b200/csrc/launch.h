@@ -9,6 +9,7 @@ namespace aturan {
 template <typename S, typename C> struct StageArgs;
 template <typename S> struct SatArgs;
 template <typename S> struct PostArgs;
+template <typename S> struct ChemArgs;
 struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
@@ -25,7 +26,8 @@ void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S
                      const GSW* w, PressConst c, int s, cudaStream_t st);                                   \
 void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
                     const RBW* w, PressConst c, double* src, cudaStream_t st);                             \
-int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);
+int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);               \
+int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)

@@ -5,6 +5,7 @@
 #include "satadj.cuh"
 #include "pressure.cuh"
 #include "post.cuh"
+#include "chem.cuh"
 
 namespace aturan {
 // Stage launch configuration per storage type, measured on B200 at 41x181x361: resident blocks per
@@ -58,28 +59,38 @@ void launch_momentum(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
         rk_stage_kernel<S, C, StageCfg<S>::MINB1><<<grid, dim3(32, 4), 0, st>>>(a);
     }
 }
+// damp_wiggles (lib/Utils.cpp:224-317) on x along the axes selected, k then j then i; lo: the low
+// part of the mixed form's temperature pair when x is t (common.cuh), else null. Returns the
+// number of launches.
+template <typename S>
+int launch_filter(const Grid& g, S* x, float* lo, bool ai, bool aj, bool ak, double strength, int phi_periodic,
+                  cudaStream_t st){
+    const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
+    const dim3 cols_k((g.km + 127) / 128);
+    int n = 0;
+    if(ak){
+        // four rows (warps) per block while they fit the default 48 KB, else one row per block
+        // with the opt-in size (rows of up to 8192 values)
+        const int R = 4 * g.km * (int)sizeof(double) <= 48 * 1024 ? 4 : 1;
+        const int sm = R * g.km * (int)sizeof(double), rows = g.im * g.jm;
+        static const bool big = (cudaFuncSetAttribute(post_filter_k_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      8192 * (int)sizeof(double)) == cudaSuccess) || (cudaGetLastError(), false);
+        (void)big;
+        post_filter_k_kernel<S><<<(rows + R - 1) / R, dim3(32, R), sm, st>>>(g, x, lo, coeff, phi_periodic && g.km > 2, rows);
+        n++;
+    }
+    if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, lo, coeff); n++; }
+    if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, lo, coeff); n++; }
+    return n;
+}
 // The passes after RK4 in the reference's order; returns the number of launches.
 template <typename S>
 int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st){
     const Grid& g = a.g;
     const dim3 cols_k((g.km + 127) / 128);
     int n = 0;
-    // lo: the low part of the mixed form's temperature pair when x is t (common.cuh), else null
     auto filt = [&](S* x, float* lo, bool ai, bool aj, bool ak, double strength){
-        const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
-        if(ak){
-            // four rows (warps) per block while they fit the default 48 KB, else one row per block
-            // with the opt-in size (rows of up to 8192 values)
-            const int R = 4 * g.km * (int)sizeof(double) <= 48 * 1024 ? 4 : 1;
-            const int sm = R * g.km * (int)sizeof(double), rows = g.im * g.jm;
-            static const bool big = (cudaFuncSetAttribute(post_filter_k_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                          8192 * (int)sizeof(double)) == cudaSuccess) || (cudaGetLastError(), false);
-            (void)big;
-            post_filter_k_kernel<S><<<(rows + R - 1) / R, dim3(32, R), sm, st>>>(g, x, lo, coeff, a.phi_periodic && g.km > 2, rows);
-            n++;
-        }
-        if(aj){ post_filter_j_kernel<S><<<dim3(cols_k.x, g.im), 128, 0, st>>>(g, x, lo, coeff); n++; }
-        if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, lo, coeff); n++; }
+        n += launch_filter<S>(g, x, lo, ai, aj, ak, strength, a.phi_periodic, st);
     };
     if(pl.damp_t_horiz != 0.0) filt(t, tlo, false, pl.damp_t_j != 0, true, pl.damp_t_horiz);
     if(pl.damp_t_vert != 0.0) filt(t, tlo, true, false, false, pl.damp_t_vert);
@@ -87,12 +98,33 @@ int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo,
                                filt(a.w, nullptr, true, true, true, pl.vel_shapiro); }
     post_bc_radius_kernel<S><<<dim3(cols_k.x, g.jm, POST_NRAD), 128, 0, st>>>(a);
     post_bc_theta_kernel<S><<<dim3(cols_k.x, g.im, POST_NTHZ + POST_NTHX), 128, 0, st>>>(a);
-    post_bc_phi_kernel<S><<<dim3((g.im * g.jm + 127) / 128, POST_NRAD), 128, 0, st>>>(a);
+    post_bc_phi_kernel<S><<<dim3((g.im * g.jm + 127) / 128, POST_NPHI), 128, 0, st>>>(a);
     n += 3;
     if(pl.species_clamp){
         post_clamp_kernel<S><<<dim3(pl.nb, POST_NSP), POST_CLAMP_NT, 0, st>>>(a, pl.part);
         post_clamp_finish_kernel<<<POST_NSP, POST_CLAMP_NT, 0, st>>>(pl.part, pl.nb, pl.out);
         n += 2;
+    }
+    return n;
+}
+// The chemistry (chem.cuh): NH4SH_EQ (1) then FORCING (2) as selected in `what`; returns the
+// number of launches.
+template <typename S>
+int launch_chem_impl(const ChemArgs<S>& a, int what, cudaStream_t st){
+    const Grid& g = a.g;
+    const dim3 cols((g.km + 127) / 128, g.jm, g.im);
+    int n = 0;
+    if(what & 1){ nh4sh_eq_kernel<S><<<cols, 128, 0, st>>>(a); n++; }
+    if(what & 2){
+        chem_diff_kernel<S><<<cols, 128, 0, st>>>(a);
+        n++;
+        S* f1[4] = {a.df_h2s, a.df_nh3, a.df_nh4sh, a.tmf};
+        for(S* x : f1) n += launch_filter<S>(g, x, nullptr, true, true, true, 1.0, a.c.per, st);
+        const int kn = g.km - 1 - (a.c.per ? 0 : 1);
+        chem_limit_kernel<S><<<dim3((kn + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(a);
+        n++;
+        S* f2[4] = {a.mf_h2s, a.mf_nh3, a.mf_nh4sh, a.fl};
+        for(S* x : f2) n += launch_filter<S>(g, x, nullptr, true, true, true, 1.0, a.c.per, st);
     }
     return n;
 }
@@ -157,4 +189,7 @@ void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_
 }                                                                                                         \
 int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st){              \
     return launch_post_impl<S>(a, pl, t, tlo, st);                                                        \
+}                                                                                                         \
+int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st){                                         \
+    return launch_chem_impl<S>(a, what, st);                                                              \
 }

@@ -19,8 +19,8 @@
 namespace aturan {
 
 // Field tables: the reference's lists (BC_Uran.cpp:21-88) restricted to the fields the context
-// holds. The phi list equals the radius list on those fields.
-constexpr int POST_NRAD = 22, POST_NTHX = 16, POST_NTHZ = 6, POST_NSP = 13;
+// holds. The phi list is the radius list's first POST_NPHI fields: all but difflux_nh4sh.
+constexpr int POST_NRAD = 25, POST_NPHI = 24, POST_NTHX = 16, POST_NTHZ = 9, POST_NSP = 13;
 
 // Which filter passes run and the clamp's scratch: part holds 2 nb doubles per species, out 2 x 13.
 struct PostPlan {
@@ -32,7 +32,7 @@ struct PostPlan {
 template <typename S>
 struct PostArgs {
     Grid g;
-    S* rad[POST_NRAD];           // radius and phi passes: t, u, v, w, the species (4..16), the fluxes
+    S* rad[POST_NRAD];           // radius and phi passes: t, u, v, w, the species (4..16), the fluxes, difflux
     S* thx[POST_NTHX];           // theta pass, extrapolated to the poles
     S* thz[POST_NTHZ];           // theta pass, zeroed at the poles (v, w first)
     S* sp[POST_NSP];             // species for the clamp, in BC_Uran.h:83-89's order

@@ -26,8 +26,10 @@ FORCING = [
 ]
 HYDRO = ["p_baro", "p_b0", "p_bfollow"]
 PROJECTION = ["rhs_u", "rhs_v", "rhs_w", "aux_u", "aux_v", "aux_w"]
+# The chemistry's diffusive tendencies (cUranusModel.h:1401-1403), persistent between iterations.
+CHEM_STATE = ["difflux_h2s", "difflux_nh3", "difflux_nh4sh"]
 
-NAMES = PROGNOSTIC + NCOPIES + PRESSURE + FORCING + HYDRO + PROJECTION
+NAMES = PROGNOSTIC + NCOPIES + PRESSURE + FORCING + HYDRO + PROJECTION + CHEM_STATE
 NFIELDS = len(NAMES)
 ID = {n: i for i, n in enumerate(NAMES)}
 NPROG = len(PROGNOSTIC)
@@ -40,6 +42,6 @@ GAS_FIELDS = {g: (g, g + "_cloud", g + "_ice") for g in GASES}
 # Fields every path reads or writes; what a full step touches.
 STATE_FIELDS = NAMES
 
-assert NFIELDS == 72, NFIELDS
+assert NFIELDS == 75, NFIELDS
 assert ID["tn"] == 19 and ID["p_dyn"] == 38 and ID["nue"] == 41
-assert ID["p_baro"] == 63 and ID["rhs_u"] == 66
+assert ID["p_baro"] == 63 and ID["rhs_u"] == 66 and ID["difflux_h2s"] == 72

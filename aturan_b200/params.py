@@ -180,3 +180,44 @@ def default_post_params(geo_balance=True):
     pp.damp_t_vert = 0.0                              # cUranusModel.cpp:1204-1205
     pp.vel_shapiro = 0.0 if geo_balance else 1.0      # cUranusModel.cpp:1229-1230
     return pp
+
+
+# aturan_chem_params' doubles in their order, and the reference's values (cUranusModel.h:997-999,
+# 1076-1087, 1135-1140; c_mix as ThermalPropertiesUran sums it; ATPhys.h:104's polar floor)
+CHEM_SCALARS = ("m_nh3", "m_h2s", "m_nh4sh", "c_mix", "D_nh4sh", "DT_nh4sh", "cp_nh3", "cp_h2s",
+                "cp_nh4sh", "k_nh3", "k_h2s", "k_nh4sh", "polar_floor")
+CHEM_DEFAULTS = dict(m_nh3=17.03052, m_h2s=34.08088, m_nh4sh=51.1114, c_mix=float.fromhex("0x1.12b14645f7a58p+0"),
+                     D_nh4sh=1.45e-9, DT_nh4sh=1.45e-9, cp_nh3=2.19e3, cp_h2s=2.24e3, cp_nh4sh=2.00e3,
+                     k_nh3=0.02102, k_h2s=0.013, k_nh4sh=0.02102, polar_floor=0.4)
+
+
+class ChemParams(ctypes.Structure):
+    """aturan_chem_params: the chemistry's constants and knobs (planet/ChemistryUran.h)."""
+    _fields_ = ([(n, ctypes.c_int32) for n in (
+        "abi_version", "nh4sh_eq", "difflux_plus", "difflux_laplacian", "phi_periodic")]
+        + [("reserved_i", ctypes.c_int32 * 3)]
+        + [(n, ctypes.c_double) for n in CHEM_SCALARS]
+        + [("reserved_d", ctypes.c_double * 5)])
+
+
+def default_chem_params():
+    """The reference's values with its ATURAN_* knobs unset."""
+    cp = ChemParams()
+    cp.abi_version = ABI_VERSION
+    cp.nh4sh_eq = 1                                   # ChemistryUran.h:134-137
+    cp.difflux_plus = 1                               # ChemistryUran.h:64-65
+    cp.difflux_laplacian = 1                          # ChemistryUran.h:292-293
+    cp.phi_periodic = 1                               # cUranusModel.h:412
+    for n, v in CHEM_DEFAULTS.items():
+        setattr(cp, n, v)
+    return cp
+
+
+def chem_params_from_ref(ref):
+    """The chemistry params read from the initialised reference model."""
+    cp = default_chem_params()
+    for n in CHEM_SCALARS:
+        setattr(cp, n, ref.chem_scalar(n))
+    cp.nh4sh_eq = int(ref.chem_scalar("nh4sh_eq"))
+    cp.phi_periodic = int(ref.chem_scalar("phi_periodic"))
+    return cp

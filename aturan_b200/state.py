@@ -157,6 +157,9 @@ def synthetic_state(p, seed=20261203, condensate=True):
         s[q + "n"] = s[q].copy()
     for q in ("un", "vn", "wn"):
         s[q] = s[q] * (1.0 + 1.0e-6 * rng.normal(size=shape))
+    # drawn last, so that every field above keeps the values it had before these were held
+    for nm in F.CHEM_STATE:
+        s[nm] = 1.0e-9 * rng.normal(size=shape)
 
     out = {}
     for n in F.NAMES:

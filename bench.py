@@ -277,10 +277,10 @@ def post_step_bytes(p, pp, e):
         b += 2 * N
     if pp.vel_shapiro != 0.0:
         b += 3 * 3 * 2 * N                           # u, v, w along k, j, i
-    nrad, nthx, nthz, nsp = 22, 16, 6, 13
+    nrad, nphi, nthx, nthz, nsp = 25, 24, 16, 9, 13
     b += nrad * 6 * jm * km                          # radius: planes 1, 2, im-2, im-3 read, 0 and im-1 written
     b += (nthx * 6 + nthz * 2) * im * km             # theta: rows 1, 2, jm-2, jm-3 read, 0 and jm-1 written
-    b += nrad * 2 * im * jm                          # phi: k = 0 read, k = km-1 written
+    b += nphi * 2 * im * jm                          # phi: k = 0 read, k = km-1 written
     if pp.species_clamp:
         b += nsp * N                                 # every species value read (writes: the clipped few)
     return b * e
@@ -324,6 +324,68 @@ def post_step_timing(api, P, S, torch, precision, calls=20):
             for _ in range(5):
                 m.post_step(pp)
             out["cpu_reference_ms"] = (time.perf_counter() - t0) / 5 * 1e3
+            out["cpu_reference_cores"] = os.cpu_count()
+    except Exception as ex:               # reported, never silently replaced
+        out["cpu_reference_ms"] = f"{type(ex).__name__}: {ex}"
+    return out
+
+
+def chem_bytes(p, e, changed, tpair):
+    """Algorithmic bytes of one aturan_chemistry(NH4SH_EQ | FORCING) with storage e bytes per value:
+    the equilibrium reads t, p_stat, nh3, h2s, nh4sh once and writes t, nh3, h2s, nh4sh in the
+    `changed` cells; the forcing reads t, p_stat, the three species, u, v, w once and writes
+    rho_mix, thermalmassflux, difflux_* (3), massflux_* (3) and fluxlim_nh4sh once, and each of the
+    eight filtered fields is read and written once more by its filter (the three axes fused, the
+    minimum). tpair: t carries a second FP32 word (the mixed form's pair)."""
+    N = p.im * p.jm * p.km
+    tw = 4 if tpair else 0
+    eq = N * (5 * e + tw) + changed * (4 * e + tw)
+    forcing = N * (8 * e + tw) + N * 9 * e + 8 * 2 * N * e
+    return eq + forcing
+
+
+def chem_timing(api, P, S, torch, precision, calls=10):
+    """aturan_chemistry (NH4SH equilibrium and forcing, the reference's knobs) at 41x181x361: device
+    time per call (CUDA events on the context's stream, mean over `calls` on a freshly uploaded
+    state each, after one warm-up call), its algorithmic bytes and GB/s, and the compiled
+    reference's same calls on the host cores when it is present."""
+    prec = P.MIXED if precision == "mixed" else P.FP64
+    p = P.default_params(precision=prec)
+    st = S.synthetic_state(p, seed=20261207)
+    ctx = api.Context(p)
+    s = torch.cuda.ExternalStream(ctx.stream)
+    ctx.upload_state(st)
+    nf, nd = ctx.chemistry(counts=True)
+    ms = []
+    for _ in range(calls):
+        ctx.upload_state(st)
+        ctx.synchronize()
+        ctx.profile(False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.chemistry()
+        e1.record(s)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = ctx.profile_read()["chem"][0]
+    ctx.close()
+    m = statistics.median(ms)
+    alg = chem_bytes(p, 4 if precision == "mixed" else 8, nf + nd, precision == "mixed")
+    peak, peak_kind = peaks()
+    out = {"ms": m, "launches": launches, "alg_bytes": alg, "achieved_gbs": alg / (m / 1e3) / 1e9,
+           "frac": alg / (m / 1e3) / 1e9 / peak, "peak_source": f"{peak_kind} hbm_gbs",
+           "cells_formed": nf, "cells_decomposed": nd,
+           "what": "NH4SH equilibrium + chemistry forcing (rho_mix, thermal mass flux, D lap(c), filters, mass "
+                   f"rates, Superbee limiter, filters), {precision}, 41x181x361, synthetic state; median of {calls}"}
+    try:
+        from oracle import ref as R
+        if R.available():
+            m_ = R.Ref.get_instance()
+            m_.load(st)
+            t0 = time.perf_counter()
+            m_.chem_eq()
+            m_.chem_forcing()
+            out["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference_cores"] = os.cpu_count()
     except Exception as ex:               # reported, never silently replaced
         out["cpu_reference_ms"] = f"{type(ex).__name__}: {ex}"
@@ -682,6 +744,13 @@ def main():
         except Exception as ex:          # reported, never silently replaced
             post = {"error": f"{type(ex).__name__}: {ex}"}
 
+    chem = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            chem = chem_timing(api, P, S, torch, args.precision)
+        except Exception as ex:          # reported, never silently replaced
+            chem = {"error": f"{type(ex).__name__}: {ex}"}
+
     poisson = None
     if rank == 0 and not args.no_adjoint:
         try:
@@ -724,6 +793,7 @@ def main():
             "clocks": clk,
             "adjoint": adjoint,
             "post_step": post,
+            "chemistry": chem,
             "poisson": poisson,
             "cpu_baseline": cpu,
         }

@@ -74,6 +74,9 @@ enum aturan_field {
     /* projection fields: last RK stage's tendencies and aux = rhs + grad p_dyn */
     ATURAN_RHS_U, ATURAN_RHS_V, ATURAN_RHS_W,
     ATURAN_AUX_U, ATURAN_AUX_V, ATURAN_AUX_W,                   /* 66..71 */
+    /* the chemistry's diffusive tendencies D lap(c) (cUranusModel.h:1401-1403): persistent state
+     * whose boundary rows the boundary passes set and whose neighbours the chemistry's filters read */
+    ATURAN_DIFFLUX_H2S, ATURAN_DIFFLUX_NH3, ATURAN_DIFFLUX_NH4SH, /* 72..74 */
     ATURAN_NFIELDS
 };
 
@@ -320,9 +323,9 @@ int aturan_post_params_default(aturan_post_params* pp);
  *   clampNegativeSpecies (BC_Uran.h:91-128).
  * The boundary passes apply to the fields of the reference's lists (BC_Uran.cpp) that the
  * context holds: t, u, v, w, the twelve condensables, nh4sh, massflux_h2s/nh3/nh4sh,
- * fluxlim_nh4sh and thermalmassflux. The other listed arrays (chrom, the j_/jT_/w_ and difflux
- * fluxes, the force and heat diagnostics) are not held; a driver applies the passes to those on
- * the host. clamp_added / clamp_cells (may be NULL; ATURAN_NSPECIES entries each, in the order
+ * fluxlim_nh4sh, thermalmassflux and difflux_h2s/nh3/nh4sh. The other listed arrays (chrom, the
+ * j_/jT_/w_ fluxes, the force and heat diagnostics) are not held; a driver applies the passes to
+ * those on the host. clamp_added / clamp_cells (may be NULL; ATURAN_NSPECIES entries each, in the order
  * above) receive this call's clipped sum and count per species, what the reference adds to its
  * cumulative clamp_added / clamp_cells; passing them synchronizes the stream.
  * Not implemented (the reference's defaults leave them off; the host keeps them): BC_T_LID_PIN,
@@ -339,6 +342,47 @@ int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clam
  * contexts return ATURAN_E_UNSUPPORTED. The first call allocates 24 KB on the device. */
 int aturan_mca(aturan_ctx* ctx);
 
+/* The chemistry of the iteration loop (planet/ChemistryUran.h, FluxLimiter.h) as the model calls
+ * it (cUranusModel.cpp:1034 and 1074-1087) with the reference's default knobs. Constants the
+ * params struct does not carry come from aturan_params (r_mix, R_mix, cp_mix, mue_mix, sc_h2s,
+ * sc_nh3, sinthe_min, metric_R_km, t_ref). */
+typedef struct aturan_chem_params {
+    int32_t abi_version;          /* = ATURAN_ABI_VERSION */
+    int32_t nh4sh_eq;             /* ATURAN_NH4SH_EQ (ChemistryUran.h:143): only 1 (the default) */
+    int32_t difflux_plus;         /* ATURAN_CHEM_DIFFLUX_PLUS: 1 (default) massflux = +difflux, 0: minus */
+    int32_t difflux_laplacian;    /* ATURAN_CHEM_DIFFLUX_LAPLACIAN: only 1 (the default) */
+    int32_t phi_periodic;         /* ATURAN_BC_PHI_PERIODIC (ATPhys.h:125): 1 (default) or 0 */
+    int32_t reserved_i[3];
+    double m_nh3, m_h2s, m_nh4sh;      /* molar masses [kg/kmol] (cUranusModel.h:997-999) */
+    double c_mix;                      /* mixture molar density [kmol/m3] (ThermalPropertiesUran) */
+    double D_nh4sh, DT_nh4sh;          /* NH4SH diffusion coefficients (cUranusModel.h:1135-1140) */
+    double cp_nh3, cp_h2s, cp_nh4sh;   /* [J/(kg K)] (cUranusModel.h:1085-1087) */
+    double k_nh3, k_h2s, k_nh4sh;      /* [W/(m K)] (cUranusModel.h:1076-1078) */
+    double polar_floor;                /* ATPhys::polar_divisor_floor (ATPhys.h:104): 0.4 */
+    double reserved_d[5];
+} aturan_chem_params;
+
+/* Fill the reference's defaults. */
+int aturan_chem_params_default(aturan_chem_params* cp);
+
+#define ATURAN_CHEM_NH4SH_EQ 1    /* ChemistryUran::EquilibriumNH4SH("loop") (ChemistryUran.h:222-280) */
+#define ATURAN_CHEM_FORCING 2     /* DiffMassFluxUran, the 1-2-1 filters, ChemMassRateUran,
+                                     FluxLimiterNH4SH, the filters (cUranusModel.cpp:1074-1087) */
+
+/* Run the parts of the chemistry selected in `what` (a mask of the two flags above; NH4SH_EQ runs
+ * first when both are set, as the loop orders them: it follows the saturation adjustment and
+ * precedes the precipitation, FORCING follows the n-copy sync).
+ * NH4SH_EQ: every cell to the NH3 + H2S <-> NH4SH(s) equilibrium of K_p(T) (Lewis 1969), solved
+ * with T by bisection; writes nh3, h2s, nh4sh and t where x != 0; n_formed / n_decomposed (may be
+ * NULL; passing either synchronizes the stream) receive the cells that formed / decomposed NH4SH.
+ * FORCING: rho_mix (every cell), thermalmassflux, difflux_h2s/nh3/nh4sh = D lap(c), the filters
+ * on those four, massflux_* = w_* + sign difflux_* with w_* = 0 (equilibrium form), the Superbee
+ * limiter's fluxlim_nh4sh, the filters on those four. The interior rows are written, the
+ * boundary rows of the persistent fields are read as the last boundary passes left them.
+ * Knob values other than those supported return ATURAN_E_UNSUPPORTED. */
+int aturan_chemistry(aturan_ctx* ctx, const aturan_chem_params* cp, int what, long* n_formed,
+                     long* n_decomposed);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
@@ -350,6 +394,7 @@ enum aturan_kernel_kind {
     ATURAN_K_ADJOINT,        /* the RK4 step's adjoint (aturan_rk4_adjoint) */
     ATURAN_K_POST,           /* filters, boundary passes and species clamp (aturan_post_step) */
     ATURAN_K_MCA,            /* moist convective adjustment (aturan_mca) */
+    ATURAN_K_CHEM,           /* NH4SH equilibrium and chemistry forcing (aturan_chemistry) */
     ATURAN_K_NKINDS
 };
 

@@ -84,6 +84,8 @@ class Oracle:
             ("oracle_set_threads", [ctypes.c_int], None),
             ("oracle_post_step", [P, vp, P, vp, vp], ctypes.c_int),
             ("oracle_mca", [P, vp], ctypes.c_int),
+            ("oracle_nh4sh_eq", [P, P, vp, vp], ctypes.c_int),
+            ("oracle_chem_forcing", [P, P, vp], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -196,3 +198,14 @@ class Oracle:
     def mca(self, p, state):
         """The moist convective adjustment (default knobs) on the state in place."""
         assert self.L.oracle_mca(self._p(p), field_ptrs(state)) == 0
+
+    def nh4sh_eq(self, p, cp, state):
+        """EquilibriumNH4SH("loop") on the state in place; returns (cells formed, cells decomposed)."""
+        c = np.zeros(2, dtype=np.int64)
+        assert self.L.oracle_nh4sh_eq(self._p(p), self._p(cp), field_ptrs(state), c.ctypes.data) == 0
+        return int(c[0]), int(c[1])
+
+    def chem_forcing(self, p, cp, state):
+        """The chemistry forcing sequence (rho_mix, thermalmassflux, difflux_*, massflux_*,
+        fluxlim_nh4sh) on the state in place."""
+        assert self.L.oracle_chem_forcing(self._p(p), self._p(cp), field_ptrs(state)) == 0

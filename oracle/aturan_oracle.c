@@ -1632,13 +1632,15 @@ static const int POST_RADIUS[] = { ATURAN_T, ATURAN_U, ATURAN_V, ATURAN_W,
     ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
     ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
     ATURAN_NH4SH, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3, ATURAN_MASSFLUX_NH4SH,
-    ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX };
+    ATURAN_FLUXLIM_NH4SH, ATURAN_THERMALMASSFLUX, ATURAN_DIFFLUX_H2S, ATURAN_DIFFLUX_NH3, ATURAN_DIFFLUX_NH4SH };
+/* BC_Uran.cpp:73-88: the phi list is the radius list without difflux_nh4sh (the last entry above) */
+#define POST_NPHI (NELEM(POST_RADIUS) - 1)
 static const int POST_THETA_EXTRAP[] = { ATURAN_T, ATURAN_U,
     ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE, ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
     ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
     ATURAN_NH4SH, ATURAN_THERMALMASSFLUX };
 static const int POST_THETA_ZERO[] = { ATURAN_V, ATURAN_W, ATURAN_MASSFLUX_H2S, ATURAN_MASSFLUX_NH3,
-    ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH };
+    ATURAN_MASSFLUX_NH4SH, ATURAN_FLUXLIM_NH4SH, ATURAN_DIFFLUX_H2S, ATURAN_DIFFLUX_NH3, ATURAN_DIFFLUX_NH4SH };
 /* BC_Uran.h:83-89 (species_fields), the order of the clamp's per-species sums */
 static const int POST_SPECIES[ATURAN_NSPECIES] = { ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
     ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE, ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
@@ -1776,10 +1778,10 @@ int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post
             F[IDX(i,jm-1,k)] = bc_form(pp->pole_form, F[IDX(i,jm-2,k)], F[IDX(i,jm-3,k)], F[IDX(i,jm-4,k)]);
         }
     }
-    /* BoundaryConditions.h:398-518 (bcPhi without the seam damping); its list equals the radius
-     * list on the fields held */
+    /* BoundaryConditions.h:398-518 (bcPhi without the seam damping); its list is the radius list
+     * without difflux_nh4sh on the fields held */
     for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++)
-        for(int n = 0; n < NELEM(POST_RADIUS); n++){
+        for(int n = 0; n < POST_NPHI; n++){
             double* F = f[POST_RADIUS[n]];
             if(pp->phi_periodic) F[IDX(i,j,km-1)] = F[IDX(i,j,0)];
             else {
@@ -2075,5 +2077,209 @@ int oracle_mca(const aturan_params* p, double* const* f){
         for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++) mca_column(&M, &C, f, j, k);
         free(buf); free(cb);
     }
+    return 0;
+}
+
+/* ---- ChemistryUran (planet/ChemistryUran.h) and FluxLimiter<cUranusModel>::nh4sh (FluxLimiter.h),
+ * the equilibrium form with the reference's default knobs ---- */
+
+static double stdmin(double a, double b){ return (b < a) ? b : a; }            /* std::min(a, b) */
+
+/* ChemistryUran.h:132, the van't Hoff enthalpy of K_p [J/kg] */
+static double nh4sh_formation_heat(void){ return 4705.0 * log(10.0) * 8314.46 / 51.1114; }
+/* ChemistryUran.h:144, Lewis (1969) [Pa^2] */
+static double nh4sh_kp(double T){ const double atm = 101325.0; return pow(10.0, 14.82 - 4705.0 / T) * atm * atm; }
+/* ChemistryUran.h:154-156 */
+static double nh4sh_f(double x, double T0, double heat, double a, double b){
+    const double T = T0 + heat * x, RT = 8314.46 * T;
+    return (a - x) * (b - x) * RT * RT - nh4sh_kp(T);
+}
+
+/* ChemistryUran.h:140-177, equilibrateNH4SHCell: x [kmol/m3] formed (> 0) or decomposed (< 0) */
+static double nh4sh_cell(const aturan_params* p, const aturan_chem_params* cp, double* const* f, size_t q){
+    const double L_f = nh4sh_formation_heat();
+    const double T0 = f[ATURAN_T][q] * p->t_ref;
+    if(!(T0 > 0.0)) return 0.0;
+    double rho = f[ATURAN_P_STAT][q] * 1e5 / (p->R_mix * T0);
+    if(!(rho > 0.0) || !isfinite(rho)) rho = p->r_mix;
+    const double a = stdmax(0.0, f[ATURAN_NH3][q]) / cp->m_nh3;
+    const double b = stdmax(0.0, f[ATURAN_H2S][q]) / cp->m_h2s;
+    const double s = stdmax(0.0, f[ATURAN_NH4SH][q]) / cp->m_nh4sh;
+    const double heat = L_f * cp->m_nh4sh / (p->cp_mix * rho);
+    const double f0 = nh4sh_f(0.0, T0, heat, a, b);
+    double lo, hi;
+    if(f0 > 0.0){ lo = 0.0; hi = stdmin(a, b); }
+    else if(s > 0.0){
+        if(nh4sh_f(-s, T0, heat, a, b) <= 0.0){ lo = hi = -s; }
+        else { lo = -s; hi = 0.0; }
+    } else return 0.0;
+    if(hi > lo) for(int it = 0; it < 80; it++){
+        const double xm = 0.5 * (lo + hi);
+        if(nh4sh_f(xm, T0, heat, a, b) > 0.0) lo = xm; else hi = xm;
+        if(hi - lo <= 1.0e-15 * stdmax(a, stdmax(b, s))) break;
+    }
+    const double x = (f0 > 0.0) ? lo : hi;
+    if(x == 0.0) return 0.0;
+    f[ATURAN_NH3][q] = stdmax(0.0, f[ATURAN_NH3][q] - cp->m_nh3 * x);
+    f[ATURAN_H2S][q] = stdmax(0.0, f[ATURAN_H2S][q] - cp->m_h2s * x);
+    f[ATURAN_NH4SH][q] = stdmax(0.0, f[ATURAN_NH4SH][q] + cp->m_nh4sh * x);
+    const double dT = heat * x;
+    f[ATURAN_T][q] = (T0 + dT) / p->t_ref;
+    return x;
+}
+
+/* ChemistryUran.h:210-275, EquilibriumNH4SH("loop"): every cell in place (no SeaMount cells);
+ * counts[0] / counts[1] = cells that formed / decomposed NH4SH. */
+int oracle_nh4sh_eq(const aturan_params* p, const aturan_chem_params* cp, double* const* f, long* counts){
+    const size_t N = (size_t)p->im * p->jm * p->km;
+    long nf = 0, nd = 0;
+    #pragma omp parallel for reduction(+:nf, nd) schedule(static)
+    for(size_t q = 0; q < N; q++){
+        const double x = nh4sh_cell(p, cp, f, q);
+        if(x > 0.0) nf++;
+        else if(x < 0.0) nd++;
+    }
+    if(counts){ counts[0] = nf; counts[1] = nd; }
+    return 0;
+}
+
+/* ChemistryUran.h:601-686, derivative_1_order without SeaMount cells: the central differences */
+static void chem_d1(const aturan_params* p, const double* c, int i, int j, int k, int per,
+                    double* dr_, double* dthe_, double* dphi_){
+    const int jm = p->jm, km = p->km;
+    const int kw = per ? phi_wrap(k - 1, km) : k - 1, ke = per ? phi_wrap(k + 1, km) : k + 1;
+    *dr_ = (c[IDX(i+1,j,k)] - c[IDX(i-1,j,k)]) / (2.0 * p->dr);
+    *dthe_ = (c[IDX(i,j+1,k)] - c[IDX(i,j-1,k)]) / (2.0 * p->dthe);
+    *dphi_ = (c[IDX(i,j,ke)] - c[IDX(i,j,kw)]) / (2.0 * p->dphi);
+}
+
+/* ChemistryUran.h:576-598, laplacian_spherical (coord_stretching false: exp_rm = 1) */
+static double chem_laplacian(const aturan_params* p, const aturan_chem_params* cp, const double* c,
+                             const double* rad, const double* the, int i, int j, int k, int per){
+    const int jm = p->jm, km = p->km;
+    const double rm = metric_radius(p, rad[i]);
+    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
+    const double sinthe = sin(the[j]), costhe = cos(the[j]);
+    const double rmsinthe = rm * stdmax(sinthe, cp->polar_floor);
+    const double x = c[IDX(i,j,k)];
+    const double d2cdr2 = (c[IDX(i+1,j,k)] - 2.0 * x + c[IDX(i-1,j,k)]) / (p->dr * p->dr) * exp_2_rm;
+    const double d2cdthe2 = (c[IDX(i,j+1,k)] - 2.0 * x + c[IDX(i,j-1,k)]) / (p->dthe * p->dthe);
+    const int kw = per ? phi_wrap(k - 1, km) : k - 1, ke = per ? phi_wrap(k + 1, km) : k + 1;
+    const double d2cdphi2 = (c[IDX(i,j,ke)] - 2.0 * x + c[IDX(i,j,kw)]) / (p->dphi * p->dphi);
+    const double dcdr = (c[IDX(i+1,j,k)] - c[IDX(i-1,j,k)]) / (2.0 * p->dr) * exp_rm;
+    const double dcdthe = (c[IDX(i,j+1,k)] - c[IDX(i,j-1,k)]) / (2.0 * p->dthe);
+    return d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) + costhe / (rm * rmsinthe) * dcdthe
+         + d2cdphi2 / (rmsinthe * rmsinthe);
+}
+
+/* FluxLimiter.h:68-70 */
+static double superbee(double r){ return stdmax(0.0, stdmax(stdmin(2.0 * r, 1.0), stdmin(r, 2.0))); }
+
+/* cUranusModel.cpp:1074-1087: DiffMassFluxUran (ChemistryUran.h:277-427), damp_wiggles on
+ * difflux_h2s/nh3/nh4sh and thermalmassflux, ChemMassRateUran (:38-110; w_* = 0 in the
+ * equilibrium form), FluxLimiter<cUranusModel>::nh4sh (FluxLimiter.h:89-186), damp_wiggles on
+ * massflux_h2s/nh3/nh4sh and fluxlim_nh4sh. The interior rows are written; the boundary rows of
+ * the persistent fields are read as they are. */
+int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, double* const* f){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const size_t N = (size_t)im * jm * km;
+    const int per = cp->phi_periodic != 0, k_first = per ? 0 : 1;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    double* tmp = (double*)malloc(sizeof(double) * N);
+    if(!rad || !the || !tmp){ free(rad); free(the); free(tmp); return -1; }
+    oracle_coords(p, rad, the);
+    const double nu_mix = p->mue_mix / p->r_mix;
+    const double D_nh3 = nu_mix / p->sc_nh3, D_h2s = nu_mix / p->sc_h2s;
+    const double DT_nh3 = nu_mix / p->sc_nh3, DT_h2s = nu_mix / p->sc_h2s;
+    const double dsign = cp->difflux_plus ? 1.0 : -1.0;
+    const double* t = f[ATURAN_T];
+    const double *nh3 = f[ATURAN_NH3], *h2s = f[ATURAN_H2S], *nh4sh = f[ATURAN_NH4SH];
+    /* ChemistryUran.h:312-320, the local density */
+    #pragma omp parallel for schedule(static)
+    for(size_t q = 0; q < N; q++) f[ATURAN_RHO_MIX][q] = f[ATURAN_P_STAT][q] * 1e5 / (p->R_mix * t[q] * p->t_ref);
+    /* passes 1 and 2 (ChemistryUran.h:322-419): j_* at the cell, thermalmassflux and difflux_* */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int k = k_first; k < km - 1; k++) for(int j = 1; j < jm - 1; j++) for(int i = 1; i < im - 1; i++){
+        const size_t q = IDX(i,j,k);
+        const double rm = rad[i];
+        const double sinthe = stdmax(p->sinthe_min, fabs(sin(the[j])));
+        const double rmsinthe = rm * sinthe;
+        double dtdr, dtdthe, dtdphi, a_r, a_t, a_p, b_r, b_t, b_p, c_r, c_t, c_p;
+        chem_d1(p, t, i, j, k, per, &dtdr, &dtdthe, &dtdphi);
+        chem_d1(p, h2s, i, j, k, per, &a_r, &a_t, &a_p);
+        chem_d1(p, nh3, i, j, k, per, &b_r, &b_t, &b_p);
+        chem_d1(p, nh4sh, i, j, k, per, &c_r, &c_t, &c_p);
+        const double jT_nh3 = DT_nh3 / t[q] * dtdr;
+        const double jT_h2s = DT_h2s / t[q] * dtdr;
+        const double jT_nh4sh = cp->DT_nh4sh / t[q] * dtdr;
+        const double d_nh3 = b_r + fabs(b_t) / rm + b_p / rmsinthe;
+        const double d_h2s = a_r + fabs(a_t) / rm + a_p / rmsinthe;
+        const double d_nh4sh = c_r + fabs(c_t) / rm + c_p / rmsinthe;
+        const double j_nh3 = cp->c_mix / p->r_mix * (cp->m_nh3 * D_nh3 * d_nh3 - jT_nh3);
+        const double j_h2s = cp->c_mix / p->r_mix * (cp->m_h2s * D_h2s * d_h2s - jT_h2s);
+        const double j_nh4sh = cp->c_mix / p->r_mix * (cp->m_nh4sh * cp->D_nh4sh * d_nh4sh - jT_nh4sh);
+        f[ATURAN_DIFFLUX_H2S][q] = D_h2s * chem_laplacian(p, cp, h2s, rad, the, i, j, k, per);
+        f[ATURAN_DIFFLUX_NH3][q] = D_nh3 * chem_laplacian(p, cp, nh3, rad, the, i, j, k, per);
+        f[ATURAN_DIFFLUX_NH4SH][q] = cp->D_nh4sh * chem_laplacian(p, cp, nh4sh, rad, the, i, j, k, per);
+        const double w0 = 0.0;   /* w_nh3, w_h2s, w_nh4sh */
+        f[ATURAN_THERMALMASSFLUX][q] = (j_nh3 * cp->cp_nh3 + j_h2s * cp->cp_h2s + j_nh4sh * cp->cp_nh4sh)
+            * (dtdr + fabs(dtdthe) / rm + dtdphi / rmsinthe)
+            + t[q] * (w0 * cp->k_nh3 + w0 * cp->k_h2s + w0 * cp->k_nh4sh);
+    }
+    post_damp(p, f[ATURAN_DIFFLUX_H2S], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_DIFFLUX_NH3], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_DIFFLUX_NH4SH], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_THERMALMASSFLUX], 1, 1, 1, 1.0, per, tmp);
+    /* ChemMassRateUran: massflux = w + sign difflux, w = 0 */
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int k = k_first; k < km - 1; k++) for(int j = 1; j < jm - 1; j++) for(int i = 1; i < im - 1; i++){
+        const size_t q = IDX(i,j,k);
+        f[ATURAN_MASSFLUX_H2S][q] = 0.0 + dsign * f[ATURAN_DIFFLUX_H2S][q];
+        f[ATURAN_MASSFLUX_NH3][q] = 0.0 + dsign * f[ATURAN_DIFFLUX_NH3][q];
+        f[ATURAN_MASSFLUX_NH4SH][q] = 0.0 + dsign * f[ATURAN_DIFFLUX_NH4SH][q];
+    }
+    /* the Superbee limiter */
+    const double eps = 1.0e-12;
+    const double* u = f[ATURAN_U]; const double* v = f[ATURAN_V]; const double* w = f[ATURAN_W];
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int k = k_first; k < km - 1; k++) for(int j = 1; j < jm - 1; j++) for(int i = 1; i < im - 1; i++){
+        const size_t o = IDX(i,j,k);
+        const double q = nh4sh[o], q_rp = nh4sh[IDX(i+1,j,k)], q_rm = nh4sh[IDX(i-1,j,k)];
+        const double q_tp = nh4sh[IDX(i,j+1,k)], q_tm = nh4sh[IDX(i,j-1,k)];
+        const int kp1 = per ? phi_wrap(k + 1, km) : k + 1, km1 = per ? phi_wrap(k - 1, km) : k - 1;
+        const double q_pp = nh4sh[IDX(i,j,kp1)], q_pm = nh4sh[IDX(i,j,km1)];
+        const double uu = u[o], vv = v[o], ww = w[o];
+        const double rm = metric_radius(p, rad[i]);
+        const double sinthe = stdmax(cp->polar_floor, fabs(sin(the[j])));
+        const double inv_rm = 1.0 / rm, inv_rmsinthe = 1.0 / (rm * sinthe);
+        double corr = 0.0;
+        {
+            const double df = q_rp - q, db = q - q_rm;
+            const double denom = df + (df >= 0.0 ? eps : -eps);
+            const double r = (uu >= 0.0) ? db / denom : ((i + 2 < im ? nh4sh[IDX(i+2,j,k)] : q_rp) - q_rp) / denom;
+            corr += (1.0 - superbee(r)) * fabs(uu) * (df - db) / (2.0 * p->dr);
+        }
+        {
+            const double df = q_tp - q, db = q - q_tm;
+            const double denom = df + (df >= 0.0 ? eps : -eps);
+            const double q_far = (j + 2 < jm) ? nh4sh[IDX(i,j+2,k)] : (C43 * q_tp - C13 * q);
+            const double r = (vv >= 0.0) ? db / denom : (q_far - q_tp) / denom;
+            corr += (1.0 - superbee(r)) * fabs(vv) * inv_rm * (df - db) / (2.0 * p->dthe);
+        }
+        {
+            const double df = q_pp - q, db = q - q_pm;
+            const double denom = df + (df >= 0.0 ? eps : -eps);
+            const double q2 = per ? nh4sh[IDX(i,j,phi_wrap(k + 2, km))] : (k + 2 < km ? nh4sh[IDX(i,j,k+2)] : q_pp);
+            const double r = (ww >= 0.0) ? db / denom : (q2 - q_pp) / denom;
+            corr += (1.0 - superbee(r)) * fabs(ww) * inv_rmsinthe * (df - db) / (2.0 * p->dphi);
+        }
+        f[ATURAN_FLUXLIM_NH4SH][o] = corr;
+    }
+    post_damp(p, f[ATURAN_MASSFLUX_H2S], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_MASSFLUX_NH3], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_MASSFLUX_NH4SH], 1, 1, 1, 1.0, per, tmp);
+    post_damp(p, f[ATURAN_FLUXLIM_NH4SH], 1, 1, 1, 1.0, per, tmp);
+    free(rad); free(the); free(tmp);
     return 0;
 }

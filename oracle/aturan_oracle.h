@@ -52,6 +52,10 @@ void oracle_set_threads(int n);
 int oracle_mca(const aturan_params* p, double* const* f);
 int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post_params* pp,
                      double* clamp_added, long* clamp_cells);
+/* ChemistryUran.h:210-275, EquilibriumNH4SH("loop"); counts[2] = cells formed, decomposed */
+int oracle_nh4sh_eq(const aturan_params* p, const aturan_chem_params* cp, double* const* f, long* counts);
+/* cUranusModel.cpp:1074-1087: DiffMassFluxUran, filters, ChemMassRateUran, FluxLimiterNH4SH, filters */
+int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, double* const* f);
 
 #ifdef __cplusplus
 }

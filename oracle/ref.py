@@ -70,6 +70,8 @@ class Ref:
         if hasattr(L, "ref_damp_wiggles"):       # a harness built before the post-step entry points lacks them
             L.ref_damp_wiggles.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
             L.ref_clamp_species.argtypes = [vp, vp]
+        if hasattr(L, "ref_chem_scalar"):
+            L.ref_chem_scalar.argtypes = [ctypes.c_char_p, vp]
         L.ref_set_quiet(1 if quiet else 0)
         self.L = L
         self.path = path
@@ -169,3 +171,17 @@ class Ref:
     def mca(self):
         """MoistConvectiveAdjustment as the model's loop calls it (cUranusModel.cpp:1276-1292)."""
         assert self.L.ref_mca() == 0
+
+    def chem_eq(self):
+        """ChemistryUran::EquilibriumNH4SH("loop") (cUranusModel.cpp:1034)."""
+        assert self.L.ref_chem_eq() == 0
+
+    def chem_forcing(self):
+        """DiffMassFluxUran, the filters, ChemMassRateUran, FluxLimiterNH4SH and the filters
+        (cUranusModel.cpp:1074-1087)."""
+        assert self.L.ref_chem_forcing() == 0
+
+    def chem_scalar(self, name):
+        d = ctypes.c_double()
+        assert self.L.ref_chem_scalar(name.encode(), ctypes.byref(d)) == 0, name
+        return d.value

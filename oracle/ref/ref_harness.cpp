@@ -109,6 +109,7 @@ Array* field(const char* name){
         {"massflux_h2s", &m.massflux_h2s}, {"massflux_nh3", &m.massflux_nh3},
         {"massflux_nh4sh", &m.massflux_nh4sh}, {"fluxlim_nh4sh", &m.fluxlim_nh4sh},
         {"rho_mix", &m.rho_mix}, {"tke_source", &m.tke_source}, {"dis_source", &m.dis_source},
+        {"difflux_h2s", &m.difflux_h2s}, {"difflux_nh3", &m.difflux_nh3}, {"difflux_nh4sh", &m.difflux_nh4sh},
         {"rhs_t", &m.rhs_t}, {"rhs_u", &m.rhs_u}, {"rhs_v", &m.rhs_v}, {"rhs_w", &m.rhs_w},
         {"rhs_ch4", &m.rhs_ch4}, {"rhs_tke", &m.rhs_tke}, {"rhs_dis", &m.rhs_dis},
         {"rhs_nh4sh", &m.rhs_nh4sh},
@@ -365,6 +366,44 @@ int ref_mca(){
     if(cUranusModel::chrom_on()) tracers.push_back({ "chrom", &m.chrom, 0.0, false, 0.0 });
     MoistConvectiveAdjustmentUran(m, gases, tracers).run();
     return 0;
+}
+
+
+// The chemistry as the loop calls it: EquilibriumNH4SH("loop") after the saturation adjustments
+// (cUranusModel.cpp:1034) and the forcing sequence of :1074-1087, filters included.
+int ref_chem_eq(){ Quiet q_; ChemistryUran(*g_model).EquilibriumNH4SH("loop"); return 0; }
+int ref_chem_forcing(){
+    Quiet q_;
+    cUranusModel& m = *g_model;
+    ChemistryUran(m).DiffMassFluxUran();
+    AtomUtils::damp_wiggles(m.difflux_h2s,     nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.difflux_nh3,     nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.difflux_nh4sh,   nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.thermalmassflux, nullptr, true, true, true);
+    ChemistryUran(m).ChemMassRateUran();
+    ChemistryUran(m).FluxLimiterNH4SH();
+    AtomUtils::damp_wiggles(m.massflux_h2s,   nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.massflux_nh3,   nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.massflux_nh4sh, nullptr, true, true, true);
+    AtomUtils::damp_wiggles(m.fluxlim_nh4sh,  nullptr, true, true, true);
+    return 0;
+}
+// The chemistry's constants and resolved knobs.
+int ref_chem_scalar(const char* name, double* out){
+    cUranusModel& m = *g_model;
+    struct E { const char* n; double v; };
+    const E tab[] = {
+        {"m_nh3", m.m_nh3}, {"m_h2s", m.m_h2s}, {"m_nh4sh", m.m_nh4sh}, {"c_mix", m.c_mix},
+        {"D_nh4sh", m.D_nh4sh}, {"DT_nh4sh", m.DT_nh4sh},
+        {"cp_nh3", m.cp_nh3}, {"cp_h2s", m.cp_h2s}, {"cp_nh4sh", m.cp_nh4sh},
+        {"k_nh3", m.k_nh3}, {"k_h2s", m.k_h2s}, {"k_nh4sh", m.k_nh4sh},
+        {"polar_floor", ATPhys::polar_divisor_floor<cUranusModel>()},
+        {"nh4sh_eq", ChemistryUran::nh4sh_eq() ? 1.0 : 0.0},
+        {"phi_periodic", ATPhys::phi_periodic<cUranusModel>() ? 1.0 : 0.0},
+        {"coord_stretching", m.coord_stretching ? 1.0 : 0.0},
+    };
+    for(const E& e : tab) if(std::strcmp(e.n, name) == 0){ *out = e.v; return 0; }
+    return -1;
 }
 
 }  // extern "C"

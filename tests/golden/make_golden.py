@@ -34,6 +34,10 @@ CASES = {
                                          "h2s_ice", "nh3", "nh3_cloud", "nh3_ice", "ch4", "ch4_cloud", "ch4_ice",
                                          "nh4sh", "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh",
                                          "thermalmassflux"]),
+    # the chemistry (equilibrium form, default knobs) on chem_case.chem_state(state, seed + 1)
+    "chem_eq": dict(seed=108, outputs=["t", "nh3", "h2s", "nh4sh"]),
+    "chem_forcing": dict(seed=109, outputs=["rho_mix", "difflux_h2s", "difflux_nh3", "difflux_nh4sh", "massflux_h2s",
+                                            "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "thermalmassflux"]),
 }
 NSAMPLE = 32
 
@@ -66,11 +70,18 @@ def post_input(p, st, seed):
     return post_state(st, p, seed + 1)
 
 
+def chem_input(p, st, seed):
+    from tests.chem_case import chem_state
+    return chem_state(st, p, seed + 1)
+
+
 def ref_runner(name, p, st):
     from oracle.ref import Ref
     ref = Ref.get_instance()
     if name == "post_step":
         st = post_input(p, st, CASES[name]["seed"])
+    if name.startswith("chem_"):
+        st = chem_input(p, st, CASES[name]["seed"])
     ref.load(st)
     if name == "satadj4":
         for g in range(4):
@@ -91,6 +102,10 @@ def ref_runner(name, p, st):
         ref.post_step(P.default_post_params())
     elif name == "mca":
         ref.mca()
+    elif name == "chem_eq":
+        ref.chem_eq()
+    elif name == "chem_forcing":
+        ref.chem_forcing()
     out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
     if "buoy_ref_level" in CASES[name]["outputs"]:
         out["buoy_ref_level"] = ref.get("buoy_ref_level")

@@ -11,7 +11,7 @@ SPECIES = ["h2o", "h2o_cloud", "h2o_ice", "h2s", "h2s_cloud", "h2s_ice", "nh3", 
            "nh3_ice", "ch4", "ch4_cloud", "ch4_ice", "nh4sh"]
 FLUXES = ["massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "thermalmassflux"]
 # every field the passes write
-POST_FIELDS = ["t", "u", "v", "w"] + SPECIES + FLUXES
+POST_FIELDS = ["t", "u", "v", "w"] + SPECIES + FLUXES + F.CHEM_STATE
 
 
 def post_state(st, p, seed, nan=True):
@@ -30,6 +30,8 @@ def post_state(st, p, seed, nan=True):
     if nan:
         s["h2o"][p.im // 2, p.jm // 2, p.km // 2] = np.nan
         s["nh3_ice"][0, p.jm // 3, p.km // 4] = np.nan
+    for n in F.CHEM_STATE:                     # drawn last: the draws above keep their values
+        s[n] = rng.normal(0.0, 1e-9, shape)
     return s
 
 

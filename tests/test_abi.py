@@ -62,6 +62,22 @@ def test_post_params_layout_and_defaults(tmp_path):
     assert bytes(api.library_default_post_params()) == bytes(P.default_post_params())
 
 
+def test_chem_params_layout_and_defaults(tmp_path):
+    """aturan_chem_params: the header's layout, and the library's defaults (the reference's
+    constants and knobs) equal the Python mirror's."""
+    src = tmp_path / "cp.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu %zu\\n", sizeof(aturan_chem_params),'
+                   ' offsetof(aturan_chem_params, m_nh3), offsetof(aturan_chem_params, polar_floor));'
+                   ' return 0; }\n')
+    exe = tmp_path / "cp"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_m, off_f = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.ChemParams)
+    assert off_m == P.ChemParams.m_nh3.offset and off_f == P.ChemParams.polar_floor.offset
+    assert bytes(api.library_default_chem_params()) == bytes(P.default_chem_params())
+
+
 def test_no_cpu_fallback_without_gpu():
     import torch
     if torch.cuda.is_available():

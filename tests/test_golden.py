@@ -34,6 +34,13 @@ def oracle_runner(O, name, p, st):
         from tests.golden.make_golden import post_input
         st = post_input(p, st, CASES[name]["seed"])
         O.post_step(p, st, P.default_post_params())
+    elif name.startswith("chem_"):
+        from tests.golden.make_golden import chem_input
+        st = chem_input(p, st, CASES[name]["seed"])
+        if name == "chem_eq":
+            O.nh4sh_eq(p, P.default_chem_params(), st)
+        else:
+            O.chem_forcing(p, P.default_chem_params(), st)
     out = dict(st)
     if lev is not None:
         out["buoy_ref_level"] = lev

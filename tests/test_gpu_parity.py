@@ -372,17 +372,29 @@ def test_step_side_by_side_equals_in_order(synth, precision):
         assert np.array_equal(ga[n], gb[n]), n
 
 
-def test_mixed_step_error_against_fp64(synth):
-    """The mixed form (FP32 state and stencils; FP64 Poisson residual, norm and refinement, FP64
-    saturation adjustment) against the FP64 path, which matches the FP64 oracle to 1e-11, over full
-    steps at 41x181x361 (RB_LINE to 1e-6, the reference's restoreVar between steps). The stated
-    bound: relative error <= 1e-5 in T and u after 10 steps, norm-wise (||d||_2 / ||fp64||_2) and
-    over 99.99 % of cells (|d| / max |fp64|). The maximum is held to 1e-4 only: in a few cells per
-    million the adjustment's relative stopping test (1e-3) passes one pass earlier or later for the
-    FP32-rounded state, a jump of one Newton pass. After one step u, v, w, T and p_dyn are within
-    1e-5 of max |fp64| in every cell."""
-    _, st0 = synth
-    I = interior_of(P.default_params())
+# Measured maxima and norm-wise errors of the condensates after 200 mixed steps (seed 99, the
+# bench's state) with about 3x headroom: (max |d| / max |fp64|, ||d||_2 / ||fp64||_2)
+MIXED_200_BOUNDS = {
+    "t": (3e-5, 1e-7), "u": (1e-5, 1e-5),
+    "ch4_cloud": (1e-2, 1e-3), "ch4_ice": (3e-3, 5e-5), "h2o_cloud": (1e-6, 1e-6), "h2o_ice": (3e-5, 1e-5),
+    "h2s_cloud": (1e-6, 1e-6), "h2s_ice": (5e-3, 1e-4), "nh3_cloud": (0.5, 3e-2), "nh3_ice": (3e-3, 5e-5),
+    "nh4sh": (3e-6, 1e-6),
+}
+
+
+def test_mixed_step_error_against_fp64():
+    """The mixed form (FP32 state and stencils with T carried as an FP32 pair; FP64 Poisson
+    residual, norm and refinement, FP64 saturation adjustment) against the FP64 path, which matches
+    the FP64 oracle to 1e-11, over full steps at 41x181x361 from the bench's state (RB_LINE to 1e-6,
+    the reference's restoreVar between steps). The stated bar, in the max norm over the interior:
+    |d| / max |fp64| <= 1e-5 in T and u after 10 steps; after one step u, v, w, T and p_dyn are
+    within 1e-5 everywhere. After 200 steps each condensate stays within the bounds above: in a few
+    cells per million the adjustment's relative stopping test (1e-3) passes one pass earlier or
+    later for the FP32-rounded vapour and condensate, a jump of one Newton pass in that cell, which
+    the norm-wise error shows to be isolated."""
+    p0 = P.default_params()
+    st0 = S.synthetic_state(p0, seed=99)
+    I = interior_of(p0)
     ctxs = {}
     for prec in (P.FP64, P.MIXED):
         ctxs[prec] = ctx_for(P.default_params(precision=prec))
@@ -392,20 +404,24 @@ def test_mixed_step_error_against_fp64(synth):
         a = ctxs[P.MIXED].download(f)[I].astype(np.float64)
         b = ctxs[P.FP64].download(f)[I]
         d = np.abs(a - b) / np.abs(b).max()
-        return d.max(), np.quantile(d, 0.9999), np.linalg.norm(a - b) / np.linalg.norm(b)
+        return d.max(), np.linalg.norm(a - b) / np.linalg.norm(b)
 
     try:
-        for n in range(1, 11):
+        for n in range(1, 201):
             for c in ctxs.values():
                 c.step(P.PRESS_RB_LINE, omega=1.0, max_sweeps=50, tol=1e-6)
                 c.restore_ncopies(1.0)
             if n == 1:
                 for f in ("u", "v", "w", "t", "p_dyn"):
                     mx = errs(f)[0]
-                    assert mx <= 1e-5, (f, mx)
-        for f in ("t", "u"):
-            mx, q, l2 = errs(f)
-            assert l2 <= 1e-5 and q <= 1e-5 and mx <= 1e-4, (f, mx, q, l2)
+                    assert mx <= 1e-5, (n, f, mx)
+            if n == 10:
+                for f in ("t", "u"):
+                    mx = errs(f)[0]
+                    assert mx <= 1e-5, (n, f, mx)
+        for f, (bmax, bl2) in MIXED_200_BOUNDS.items():
+            mx, l2 = errs(f)
+            assert mx <= bmax and l2 <= bl2, (f, mx, l2)
     finally:
         for c in ctxs.values():
             c.close()

@@ -158,3 +158,43 @@ def test_mca(ref_model, oracle_lib, base_state, source):
     oracle_lib.mca(p, st)
     assert_same(ref_model.state(names), st, names)
     assert np.count_nonzero(st["t"] != before["t"]) > 100000
+
+
+def test_chem_params_are_the_references(ref_model):
+    cp, cr = P.default_chem_params(), P.chem_params_from_ref(ref_model)
+    for name, _ in P.ChemParams._fields_:
+        if name in ("reserved_i", "reserved_d"):
+            continue
+        assert getattr(cp, name) == getattr(cr, name), name
+    assert ref_model.chem_scalar("coord_stretching") == 0.0
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_nh4sh_equilibrium(ref_model, oracle_lib, base_state, source):
+    """EquilibriumNH4SH("loop") (ChemistryUran.h:210-275): t, nh3, h2s, nh4sh identical in every
+    cell; NH4SH both forms and decomposes in many cells."""
+    from tests.chem_case import EQ_OUT, chem_state
+    p, cp = P.default_params(), P.default_chem_params()
+    base = S.perturb(base_state, p, seed=81) if source == "reference_init" else S.synthetic_state(p, seed=82)
+    st = chem_state(base, p, seed=83)
+    ref_model.load(st)
+    ref_model.chem_eq()
+    nf, nd = oracle_lib.nh4sh_eq(p, cp, st)
+    assert_same(ref_model.state(EQ_OUT), st, EQ_OUT)
+    assert nf > 10000 and nd > 10000, (nf, nd)
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_chem_forcing(ref_model, oracle_lib, base_state, source):
+    """DiffMassFluxUran, the filters, ChemMassRateUran, FluxLimiterNH4SH and the filters
+    (cUranusModel.cpp:1074-1087), on persistent fields whose boundary rows hold seeded values:
+    every value written identical."""
+    from tests.chem_case import FORCING_OUT, chem_state
+    p, cp = P.default_params(), P.default_chem_params()
+    base = S.perturb(base_state, p, seed=84) if source == "reference_init" else S.synthetic_state(p, seed=85)
+    st = chem_state(base, p, seed=86)
+    ref_model.load(st)
+    ref_model.chem_forcing()
+    oracle_lib.chem_forcing(p, cp, st)
+    assert_same(ref_model.state(FORCING_OUT), st, FORCING_OUT)
+    assert np.count_nonzero(st["fluxlim_nh4sh"]) > 100000
