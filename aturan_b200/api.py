@@ -17,7 +17,8 @@ import os
 import numpy as np
 
 from . import fields as F
-from .params import ChemParams, Params, PostParams, default_chem_params, default_params, default_post_params
+from .params import (ChemParams, Params, PostParams, TurbParams, default_chem_params, default_params,
+                     default_post_params, default_turb_params)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
@@ -71,13 +72,15 @@ SIGNATURES = {
     "aturan_chem_params_default": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_chemistry": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),
+    "aturan_turb_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_turbulence": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 CHEM_NH4SH_EQ, CHEM_FORCING = 1, 2
 
 STATIC_MAX_IM, STATIC_MAX_JM, STATIC_MAX_LEVEL_CELLS = 512, 4096, 1 << 30
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca", "chem"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca", "chem", "turb"]
 NSPECIES = 13
 
 _LIB = None
@@ -125,6 +128,13 @@ def library_default_chem_params():
     rc = load_library().aturan_chem_params_default(ctypes.byref(cp))
     assert rc == 0
     return cp
+
+
+def library_default_turb_params():
+    tp = TurbParams()
+    rc = load_library().aturan_turb_params_default(ctypes.byref(tp))
+    assert rc == 0
+    return tp
 
 
 class Context:
@@ -218,6 +228,12 @@ class Context:
     def mca(self):
         """aturan_mca: the moist convective adjustment (ConvectiveAdjustment.h:402-849), default knobs."""
         self._check(self.L.aturan_mca(self.h), "mca")
+
+    def turbulence(self, tp=None):
+        """aturan_turbulence: the k-omega SST closure (Turbulence<cUranusModel>::run,
+        cUranusModel.cpp:1270) with tp's knobs (default: the reference's)."""
+        tp = default_turb_params() if tp is None else tp
+        self._check(self.L.aturan_turbulence(self.h, ctypes.byref(tp)), "turbulence")
 
     def chemistry(self, what=CHEM_NH4SH_EQ | CHEM_FORCING, cp=None, counts=False):
         """aturan_chemistry: the NH4SH equilibrium (cUranusModel.cpp:1034) and/or the chemistry

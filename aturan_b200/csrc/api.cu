@@ -25,6 +25,7 @@
 #include "adjoint.cuh"
 #include "post.cuh"
 #include "chem.cuh"
+#include "turb.cuh"
 #include "mca.cuh"
 
 using namespace aturan;
@@ -50,7 +51,7 @@ struct aturan_ctx {
     void* acc;                 // 19
     void* forc;                // 22 pointwise RHS inputs
     void* proj;                // rhs_u, rhs_v, rhs_w, aux_u, aux_v, aux_w
-    void* chem;                // difflux_h2s, difflux_nh3, difflux_nh4sh
+    void* chem;                // difflux_h2s, difflux_nh3, difflux_nh4sh, prod
     void* pstat;               // p_stat
     // FP64 always
     double *pdyn, *phydro, *pbaro, *pb0, *pbf;
@@ -278,7 +279,7 @@ void* field_ptr(aturan_ctx* c, int id, bool* is64){
     if(id >= ATURAN_TN && id < ATURAN_TN + ATURAN_NPROG) return (char*)c->ncopy + (size_t)(id - ATURAN_TN) * fs * e;
     if(id >= ATURAN_NUE && id <= ATURAN_DIS_SOURCE) return (char*)c->forc + (size_t)(id - ATURAN_NUE) * fs * e;
     if(id >= ATURAN_RHS_U && id <= ATURAN_AUX_W) return (char*)c->proj + (size_t)(id - ATURAN_RHS_U) * fs * e;
-    if(id >= ATURAN_DIFFLUX_H2S && id <= ATURAN_DIFFLUX_NH4SH) return (char*)c->chem + (size_t)(id - ATURAN_DIFFLUX_H2S) * fs * e;
+    if(id >= ATURAN_DIFFLUX_H2S && id <= ATURAN_PROD) return (char*)c->chem + (size_t)(id - ATURAN_DIFFLUX_H2S) * fs * e;
     if(id == ATURAN_P_STAT) return c->pstat;
     *is64 = true;
     switch(id){
@@ -784,6 +785,41 @@ int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what){
     return ATURAN_OK;
 }
 
+// The turbulence closure on the context's fields (aturan_turbulence).
+template <typename S>
+int run_turb(aturan_ctx* ctx, const aturan_turb_params* tp){
+    const Grid& g = ctx->g;
+    const size_t fs = g.fstride;
+    const aturan_params& p = ctx->p;
+    S* X = reinterpret_cast<S*>(ctx->state);
+    S* Nc = reinterpret_cast<S*>(ctx->ncopy);
+    S* Fo = reinterpret_cast<S*>(ctx->forc);
+    S* Ch = reinterpret_cast<S*>(ctx->chem);
+    TurbArgs<S> a;
+    a.g = g;
+    a.tke = X + (size_t)ATURAN_TKE * fs; a.dis = X + (size_t)ATURAN_DIS * fs;
+    a.tken = Nc + (size_t)ATURAN_TKE * fs; a.disn = Nc + (size_t)ATURAN_DIS * fs;
+    a.nue = Fo + (size_t)(ATURAN_NUE - ATURAN_NUE) * fs;
+    a.tks = Fo + (size_t)(ATURAN_TKE_SOURCE - ATURAN_NUE) * fs;
+    a.dss = Fo + (size_t)(ATURAN_DIS_SOURCE - ATURAN_NUE) * fs;
+    a.prod = Ch + (size_t)(ATURAN_PROD - ATURAN_DIFFLUX_H2S) * fs;
+    a.u = X + (size_t)ATURAN_U * fs; a.v = X + (size_t)ATURAN_V * fs; a.w = X + (size_t)ATURAN_W * fs;
+    a.rmm = ctx->chem_tab + g.im; a.sin = ctx->chem_tab + 2 * g.im; a.cos = ctx->chem_tab + 2 * g.im + g.jm;
+    TurbConst& c = a.c;
+    const double L_m = p.L_atm * 1.0e3;                                       // Turbulence.h:266-269
+    c.dis_min = 1.0e-10;                                                      // :195
+    c.nue_max = tp->nue_max / (p.u_0 * L_m);
+    c.k_bg_nd = tp->k_bg / (p.u_0 * p.u_0);                                   // :622-628
+    c.nue_air_nd = tp->nue_air / (p.u_0 * L_m);
+    c.y_star = 1.0e20 / L_m;                                                  // free_wall_dist(), :147
+    c.dr = p.dr; c.dthe = p.dthe; c.dphi = p.dphi;
+    c.curv = tp->curv != 0; c.per = tp->phi_periodic != 0;
+    Region reg(ctx, ATURAN_K_TURB, 0);
+    reg.n = launch_turb(a, ctx->st);
+    CK_LAUNCH("turbulence closure");
+    return ATURAN_OK;
+}
+
 extern "C" {
 
 int aturan_params_default(aturan_params* p){
@@ -853,7 +889,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     size_t bytes = 0;
     auto add = [&](size_t n){ bytes += round_up(n, 256); };
     add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e); add(19 * fs * e);
-    add(22 * fs * e); add(6 * fs * e); add(3 * fs * e); add(fs * e);
+    add(22 * fs * e); add(6 * fs * e); add(4 * fs * e); add(fs * e);
     for(int n = 0; n < 7; n++) add(fs * 8);                   // pdyn phydro pbaro pb0 pbf scratch stage64
     add(g.im * 8); add(2 * (size_t)g.im * ctx->nblk * 8);
     // the exact level means (FP64 with exact_reductions): terms, chunk sums, binades, units
@@ -911,7 +947,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->acc = carve<char>(cur, 19 * fs * e);
     ctx->forc = carve<char>(cur, 22 * fs * e);
     ctx->proj = carve<char>(cur, 6 * fs * e);
-    ctx->chem = carve<char>(cur, 3 * fs * e);
+    ctx->chem = carve<char>(cur, 4 * fs * e);
     ctx->pstat = carve<char>(cur, fs * e);
     ctx->pdyn = carve<double>(cur, fs); ctx->phydro = carve<double>(cur, fs);
     ctx->pbaro = carve<double>(cur, fs); ctx->pb0 = carve<double>(cur, fs); ctx->pbf = carve<double>(cur, fs);
@@ -1803,6 +1839,29 @@ int aturan_chemistry(aturan_ctx* ctx, const aturan_chem_params* cp, int what, lo
         if(n_decomposed) *n_decomposed = (long)h[1];
     }
     return ATURAN_OK;
+}
+
+int aturan_turb_params_default(aturan_turb_params* tp){
+    if(!tp) return ATURAN_E_INVALID;
+    std::memset(tp, 0, sizeof(*tp));
+    tp->abi_version = ATURAN_ABI_VERSION;
+    tp->model = 2;                                   // k_omega_SST (the configured turb_model)
+    tp->turb_free = 1; tp->clamp_pass = 1; tp->curv = 1;
+    tp->buoy = 0;                                    // cUranusModel.h:411
+    tp->abl_taper = 0; tp->phi_periodic = 1;
+    tp->nue_max = 1.0e5; tp->k_bg = 1.0;             // Turbulence.h:123-126, :156-159
+    tp->nue_air = 1.8e-5;                            // the constructor's nue_gas
+    return ATURAN_OK;
+}
+
+int aturan_turbulence(aturan_ctx* ctx, const aturan_turb_params* tp){
+    if(!ctx || !tp) return ATURAN_E_INVALID;
+    if(tp->abi_version != ATURAN_ABI_VERSION) return fail(ctx, ATURAN_E_INVALID, "abi_version mismatch");
+    if(tp->model != 2) return fail(ctx, ATURAN_E_UNSUPPORTED, "only the k-omega SST closure (model 2) is implemented");
+    if(tp->turb_free != 1 || tp->clamp_pass != 1 || tp->buoy != 0 || tp->abl_taper != 0)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "only turb_free = 1, clamp_pass = 1, buoy = 0, abl_taper = 0 are implemented");
+    if(ctx->g.im < 3 || ctx->g.jm < 3) return fail(ctx, ATURAN_E_INVALID, "grid too small");
+    return ctx->mixed ? run_turb<float>(ctx, tp) : run_turb<double>(ctx, tp);
 }
 
 int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells){

@@ -10,6 +10,7 @@ template <typename S, typename C> struct StageArgs;
 template <typename S> struct SatArgs;
 template <typename S> struct PostArgs;
 template <typename S> struct ChemArgs;
+template <typename S> struct TurbArgs;
 struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
@@ -27,7 +28,8 @@ void launch_gs_plane(Grid g, double* P, const double* incr, const S* au, const S
 void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_lid,                       \
                     const RBW* w, PressConst c, double* src, cudaStream_t st);                             \
 int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);               \
-int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st);
+int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st);                                         \
+int launch_turb(const TurbArgs<S>& a, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)

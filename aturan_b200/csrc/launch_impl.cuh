@@ -6,6 +6,7 @@
 #include "pressure.cuh"
 #include "post.cuh"
 #include "chem.cuh"
+#include "turb.cuh"
 
 namespace aturan {
 // Stage launch configuration per storage type, measured on B200 at 41x181x361: resident blocks per
@@ -128,6 +129,17 @@ int launch_chem_impl(const ChemArgs<S>& a, int what, cudaStream_t st){
     }
     return n;
 }
+// The turbulence closure (turb.cuh); returns the number of launches.
+template <typename S>
+int launch_turb_impl(const TurbArgs<S>& a, cudaStream_t st){
+    const Grid& g = a.g;
+    const int kn = g.km - 1 - (a.c.per ? 0 : 1);
+    turb_sources_kernel<S><<<dim3((kn + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(a);
+    turb_column_kernel<S><<<dim3((g.km + 127) / 128, g.jm), 128, 0, st>>>(a);
+    const long nedge = (a.c.per ? (long)(g.im - 1) * (g.jm - 2) : 0) + (long)(g.jm - 2) * g.km + (long)g.im * g.km;
+    turb_edges_kernel<S><<<(unsigned)((nedge + 127) / 128), 128, 0, st>>>(a);
+    return 3;
+}
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
 template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
@@ -192,4 +204,7 @@ int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cuda
 }                                                                                                         \
 int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st){                                         \
     return launch_chem_impl<S>(a, what, st);                                                              \
+}                                                                                                         \
+int launch_turb(const TurbArgs<S>& a, cudaStream_t st){                                                   \
+    return launch_turb_impl<S>(a, st);                                                                    \
 }

@@ -28,8 +28,10 @@ HYDRO = ["p_baro", "p_b0", "p_bfollow"]
 PROJECTION = ["rhs_u", "rhs_v", "rhs_w", "aux_u", "aux_v", "aux_w"]
 # The chemistry's diffusive tendencies (cUranusModel.h:1401-1403), persistent between iterations.
 CHEM_STATE = ["difflux_h2s", "difflux_nh3", "difflux_nh4sh"]
+# The turbulence closure's shear production (cUranusModel.h:358), a diagnostic it writes.
+TURB_DIAG = ["prod"]
 
-NAMES = PROGNOSTIC + NCOPIES + PRESSURE + FORCING + HYDRO + PROJECTION + CHEM_STATE
+NAMES = PROGNOSTIC + NCOPIES + PRESSURE + FORCING + HYDRO + PROJECTION + CHEM_STATE + TURB_DIAG
 NFIELDS = len(NAMES)
 ID = {n: i for i, n in enumerate(NAMES)}
 NPROG = len(PROGNOSTIC)
@@ -42,6 +44,6 @@ GAS_FIELDS = {g: (g, g + "_cloud", g + "_ice") for g in GASES}
 # Fields every path reads or writes; what a full step touches.
 STATE_FIELDS = NAMES
 
-assert NFIELDS == 75, NFIELDS
+assert NFIELDS == 76, NFIELDS
 assert ID["tn"] == 19 and ID["p_dyn"] == 38 and ID["nue"] == 41
 assert ID["p_baro"] == 63 and ID["rhs_u"] == 66 and ID["difflux_h2s"] == 72

@@ -221,3 +221,42 @@ def chem_params_from_ref(ref):
     cp.nh4sh_eq = int(ref.chem_scalar("nh4sh_eq"))
     cp.phi_periodic = int(ref.chem_scalar("phi_periodic"))
     return cp
+
+
+class TurbParams(ctypes.Structure):
+    """aturan_turb_params: the turbulence closure's knobs (planet/Turbulence.h)."""
+    _fields_ = ([(n, ctypes.c_int32) for n in (
+        "abi_version", "model", "turb_free", "clamp_pass", "curv", "buoy", "abl_taper", "phi_periodic")]
+        + [(n, ctypes.c_double) for n in ("nue_max", "k_bg", "nue_air")]
+        + [("reserved_d", ctypes.c_double * 5)])
+
+
+TURB_K_OMEGA_SST = 2
+
+
+def default_turb_params():
+    """The reference's values with its ATURAN_* knobs unset (Turbulence.h:123-180, the constructor's
+    nue_gas, Uranus's turb_default_buoy 0, turb_model k_omega_SST)."""
+    tp = TurbParams()
+    tp.abi_version = ABI_VERSION
+    tp.model = TURB_K_OMEGA_SST
+    tp.turb_free = 1
+    tp.clamp_pass = 1
+    tp.curv = 1
+    tp.buoy = 0
+    tp.abl_taper = 0
+    tp.phi_periodic = 1
+    tp.nue_max = 1.0e5
+    tp.k_bg = 1.0
+    tp.nue_air = 1.8e-5
+    return tp
+
+
+def turb_params_from_ref(ref):
+    """The turbulence knobs read from the initialised reference model."""
+    tp = default_turb_params()
+    for n in ("model", "turb_free", "clamp_pass", "curv", "buoy", "abl_taper", "phi_periodic"):
+        setattr(tp, n, int(ref.turb_scalar(n)))
+    tp.nue_max = ref.turb_scalar("nue_max")
+    tp.k_bg = ref.turb_scalar("k_bg")
+    return tp

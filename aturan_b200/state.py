@@ -160,6 +160,7 @@ def synthetic_state(p, seed=20261203, condensate=True):
     # drawn last, so that every field above keeps the values it had before these were held
     for nm in F.CHEM_STATE:
         s[nm] = 1.0e-9 * rng.normal(size=shape)
+    s["prod"] = np.abs(1.0e-4 * rng.normal(size=shape))
 
     out = {}
     for n in F.NAMES:

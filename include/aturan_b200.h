@@ -77,6 +77,8 @@ enum aturan_field {
     /* the chemistry's diffusive tendencies D lap(c) (cUranusModel.h:1401-1403): persistent state
      * whose boundary rows the boundary passes set and whose neighbours the chemistry's filters read */
     ATURAN_DIFFLUX_H2S, ATURAN_DIFFLUX_NH3, ATURAN_DIFFLUX_NH4SH, /* 72..74 */
+    /* the turbulence closure's shear production P_k (cUranusModel.h:358), a diagnostic */
+    ATURAN_PROD,                                                /* 75 */
     ATURAN_NFIELDS
 };
 
@@ -383,6 +385,34 @@ int aturan_chem_params_default(aturan_chem_params* cp);
 int aturan_chemistry(aturan_ctx* ctx, const aturan_chem_params* cp, int what, long* n_formed,
                      long* n_decomposed);
 
+/* The turbulence closure (planet/Turbulence.h, Turbulence<cUranusModel>::run, :307-331) as the
+ * model's loop calls it (cUranusModel.cpp:1270, every iteration when the closure is on, which is
+ * the default) with the reference's default knobs. */
+typedef struct aturan_turb_params {
+    int32_t abi_version;         /* = ATURAN_ABI_VERSION */
+    int32_t model;               /* ATURAN_TURB_MODEL: 2 = k_omega_SST (the default; the only one implemented) */
+    int32_t turb_free;           /* ATURAN_TURB_FREE (Turbulence.h:141): only 1 (the default) */
+    int32_t clamp_pass;          /* ATURAN_TURB_CLAMP_PASS (:175): only 1 (the default) */
+    int32_t curv;                /* ATURAN_TURB_CURV: 1 (default) the curvature terms of the velocity gradient */
+    int32_t buoy;                /* ATURAN_TURB_BUOY: only 0 (Uranus's default) */
+    int32_t abl_taper;           /* ATURAN_ABL_TAPER: only 0 (the default) */
+    int32_t phi_periodic;        /* ATURAN_BC_PHI_PERIODIC: 1 (default) or 0 */
+    double nue_max;              /* ATURAN_NUE_MAX [m2/s] (:123): 1e5 */
+    double k_bg;                 /* ATURAN_TURB_K_BG [m2/s2] (:156): 1 */
+    double nue_air;              /* the gas's kinematic viscosity [m2/s] (constructor default): 1.8e-5 */
+    double reserved_d[5];
+} aturan_turb_params;
+
+/* Fill the reference's defaults. */
+int aturan_turb_params_default(aturan_turb_params* tp);
+
+/* compute_sources (clamp pass, SST production, eddy viscosity and sources, floors and caps on the
+ * interior), apply_wall_bc (zero-gradient copy at i = 0), clamp_nue, seam_copy and
+ * fill_lid_corners (lid and pole rows copied from their neighbours): tke, dis, nue, prod,
+ * tke_source, dis_source written, tken and disn copied at the seam and the edges. Knob values
+ * other than those supported return ATURAN_E_UNSUPPORTED. */
+int aturan_turbulence(aturan_ctx* ctx, const aturan_turb_params* tp);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
@@ -395,6 +425,7 @@ enum aturan_kernel_kind {
     ATURAN_K_POST,           /* filters, boundary passes and species clamp (aturan_post_step) */
     ATURAN_K_MCA,            /* moist convective adjustment (aturan_mca) */
     ATURAN_K_CHEM,           /* NH4SH equilibrium and chemistry forcing (aturan_chemistry) */
+    ATURAN_K_TURB,           /* turbulence closure (aturan_turbulence) */
     ATURAN_K_NKINDS
 };
 

@@ -86,6 +86,7 @@ class Oracle:
             ("oracle_mca", [P, vp], ctypes.c_int),
             ("oracle_nh4sh_eq", [P, P, vp, vp], ctypes.c_int),
             ("oracle_chem_forcing", [P, P, vp], ctypes.c_int),
+            ("oracle_turbulence", [P, P, vp], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -209,3 +210,7 @@ class Oracle:
         """The chemistry forcing sequence (rho_mix, thermalmassflux, difflux_*, massflux_*,
         fluxlim_nh4sh) on the state in place."""
         assert self.L.oracle_chem_forcing(self._p(p), self._p(cp), field_ptrs(state)) == 0
+
+    def turbulence(self, p, tp, state):
+        """Turbulence<cUranusModel>::run (k-omega SST, default knobs) on the state in place."""
+        assert self.L.oracle_turbulence(self._p(p), self._p(tp), field_ptrs(state)) == 0

@@ -2283,3 +2283,159 @@ int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, do
     free(rad); free(the); free(tmp);
     return 0;
 }
+
+/* ---- Turbulence<cUranusModel>::run (planet/Turbulence.h:307-331), k-omega SST with the
+ * reference's default knobs: TURB_FREE 1, TURB_CLAMP_PASS 1, no land cells, no buoyancy term,
+ * no ABL taper, no obstacle (surface_index 0), the closure's fields not in the model's own
+ * boundary lists (bc_turb_active false) ---- */
+
+static double clamp3d(double x, double lo, double hi){ return (x < lo) ? lo : ((x > hi) ? hi : x); }   /* Turbulence.h:207-209 */
+static double turb_blend(double inner, double outer, double F1){ return F1 * inner + (1.0 - F1) * outer; }   /* :203-205 */
+
+int oracle_turbulence(const aturan_params* p, const aturan_turb_params* tp, double* const* f){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const int per = tp->phi_periodic != 0, k_first = per ? 0 : 1;
+    double* rad = (double*)malloc(sizeof(double) * im);
+    double* the = (double*)malloc(sizeof(double) * jm);
+    if(!rad || !the){ free(rad); free(the); return -1; }
+    oracle_coords(p, rad, the);
+    double *tke = f[ATURAN_TKE], *dis = f[ATURAN_DIS], *nue = f[ATURAN_NUE], *prod = f[ATURAN_PROD];
+    double *tks = f[ATURAN_TKE_SOURCE], *dss = f[ATURAN_DIS_SOURCE];
+    const double *u = f[ATURAN_U], *v = f[ATURAN_V], *w = f[ATURAN_W];
+    const double dis_min = 1.0e-10;                                   /* :195 */
+    const double L_m = p->L_atm * 1.0e3;                              /* L_atm_m(), :268 */
+    const double nue_max = tp->nue_max / (p->u_0 * L_m);
+    const double k_bg_nd = tp->k_bg / (p->u_0 * p->u_0);              /* k_bg_of with TURB_FREE, :622-628 */
+    /* compute_sources, :614-883; the clamp pass before the loop (:645-650) */
+    for(int j = 1; j < jm - 1; j++) for(int k = k_first; k < km - 1; k++) for(int i = 1; i < im - 1; i++){
+        const size_t q = IDX(i,j,k);
+        tke[q] = stdmax(0.0, tke[q]);
+        dis[q] = stdmax(dis_min, dis[q]);
+    }
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int j = 1; j < jm - 1; j++) for(int k = k_first; k < km - 1; k++){
+        const int kw = per ? phi_wrap(k - 1, km) : k - 1, ke = per ? phi_wrap(k + 1, km) : k + 1;
+        for(int i = 1; i < im - 1; i++){
+            const size_t q = IDX(i,j,k);
+            const double rm = metric_radius(p, rad[i]);
+            const double exp_rm = 1.0;                                /* coord_stretching false */
+            double sinthe = sin(the[j]);
+            if(sinthe == 0.0) sinthe = 1.0e-5;
+            const double costhe = cos(the[j]);
+            const double cotanthe = costhe / sinthe;
+            const double inv_rm = 1.0 / rm;
+            const double rmsinthe = rm * sinthe;
+            const double inv_2dr = 1.0 / (2.0 * p->dr);
+            const double inv_2dthe = 1.0 / (2.0 * p->dthe);
+            const double inv_2dphi = 1.0 / (2.0 * p->dphi);
+            const double inv_rm2dthe = inv_2dthe / rm;
+            const double inv_rmsinthe2dphi = inv_2dphi / rmsinthe;
+            const double dudr = (u[IDX(i+1,j,k)] - u[IDX(i-1,j,k)]) * inv_2dr * exp_rm;
+            const double dvdr = (v[IDX(i+1,j,k)] - v[IDX(i-1,j,k)]) * inv_2dr * exp_rm;
+            const double dwdr = (w[IDX(i+1,j,k)] - w[IDX(i-1,j,k)]) * inv_2dr * exp_rm;
+            const double dudthe = (u[IDX(i,j+1,k)] - u[IDX(i,j-1,k)]) * inv_rm2dthe;
+            const double dvdthe = (v[IDX(i,j+1,k)] - v[IDX(i,j-1,k)]) * inv_rm2dthe;
+            const double dwdthe = (w[IDX(i,j+1,k)] - w[IDX(i,j-1,k)]) * inv_rm2dthe;
+            const double dudphi = (u[IDX(i,j,ke)] - u[IDX(i,j,kw)]) * inv_rmsinthe2dphi;
+            const double dvdphi = (v[IDX(i,j,ke)] - v[IDX(i,j,kw)]) * inv_rmsinthe2dphi;
+            const double dwdphi = (w[IDX(i,j,ke)] - w[IDX(i,j,kw)]) * inv_rmsinthe2dphi;
+            const double dtkedr = (tke[IDX(i+1,j,k)] - tke[IDX(i-1,j,k)]) * inv_2dr * exp_rm;
+            const double ddisdr = (dis[IDX(i+1,j,k)] - dis[IDX(i-1,j,k)]) * inv_2dr * exp_rm;
+            /* the production tensor, :697-760 */
+            double cnue;
+            {
+                const double dis_here = stdmax(dis[q], dis_min);
+                const double tke_here = stdmax(tke[q], 0.0);
+                cnue = tke_here / dis_here;
+                cnue = stdmin(cnue, nue_max);
+            }
+            const int curv = tp->curv != 0;
+            const double u_r = curv ? u[q] * inv_rm : 0.0;
+            const double v_r = curv ? v[q] * inv_rm : 0.0;
+            const double w_r = curv ? w[q] * inv_rm : 0.0;
+            const double v_cot_r = v_r * cotanthe;
+            const double w_cot_r = w_r * cotanthe;
+            const double g_rr = dudr, g_rt = dudthe - v_r, g_rp = dudphi - w_r;
+            const double g_tr = dvdr, g_tt = dvdthe + u_r, g_tp = dvdphi - w_cot_r;
+            const double g_pr = dwdr, g_pt = dwdthe, g_pp = dwdphi + u_r + v_cot_r;
+            const double der = 0.66667 * (g_rr + g_tt + g_pp);
+            const double tk = tke[q];
+            prod[q] = stdmax(0.0,
+                  (cnue * (2.0 * g_rr - der) - 0.66667 * tk) * g_rr
+                + (cnue * (g_rt + g_tr)) * g_rt
+                + (cnue * (g_rp + g_pr)) * g_rp
+                + (cnue * (2.0 * g_tt - der) - 0.66667 * tk) * g_tt
+                + (cnue * (g_tr + g_rt)) * g_tr
+                + (cnue * (g_tp + g_pt)) * g_tp
+                + (cnue * (2.0 * g_pp - der) - 0.66667 * tk) * g_pp
+                + (cnue * (g_pr + g_rp)) * g_pr
+                + (cnue * (g_pt + g_tp)) * g_pt);
+            const double W12 = g_rt - g_tr, W13 = g_rp - g_pr, W23 = g_tp - g_pt;
+            const double Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
+            /* compute_k_omega_SST, :1020-1100, with no land cells and no wall */
+            const double a1 = 0.31, bet_star = 0.09, bet1 = 0.0333, bet2 = 0.0368;
+            const double gam1 = 0.413, gam2 = 0.2, sig_w2 = 1.168;
+            const double nue_air_nd = tp->nue_air / (p->u_0 * L_m);
+            const double y_phys = 1.0e20;                             /* free_wall_dist(), :147 */
+            const double y_star = y_phys / L_m;
+            const double rms = rm * sinthe;
+            const double dtkedthe_neu = (tke[IDX(i,j+1,k)] - tke[IDX(i,j-1,k)]) / (rm * 2.0 * p->dthe);
+            const double ddisdthe_neu = (dis[IDX(i,j+1,k)] - dis[IDX(i,j-1,k)]) / (rm * 2.0 * p->dthe);
+            const double dtkedphi_neu = (tke[IDX(i,j,ke)] - tke[IDX(i,j,kw)]) / (rms * 2.0 * p->dphi);
+            const double ddisdphi_neu = (dis[IDX(i,j,ke)] - dis[IDX(i,j,kw)]) / (rms * 2.0 * p->dphi);
+            const double grad_dot = dtkedr * ddisdr + dtkedthe_neu * ddisdthe_neu + dtkedphi_neu * ddisdphi_neu;
+            const double CD_kw = stdmax(2.0 * sig_w2 / stdmax(dis[q], 1.0e-20) * grad_dot, 1.0e-20);
+            const double dis_safe = stdmax(dis[q], 1.0e-20);
+            const double arg1 = stdmin(
+                stdmax(sqrt(tk) / (bet_star * dis_safe * y_star), 500.0 * nue_air_nd / (y_star * y_star * dis_safe)),
+                4.0 * sig_w2 * tk / (CD_kw * y_star * y_star));
+            const double arg2 = stdmax(2.0 * sqrt(tk) / (bet_star * dis_safe * y_star),
+                                       500.0 * nue_air_nd / (y_star * y_star * dis_safe));
+            const double F1 = tanh(pow(arg1, 4));
+            const double F2 = tanh(pow(arg2, 2));
+            nue[q] = a1 * tk / stdmax(a1 * dis_safe, Omega * F2);
+            const double tke_safe = stdmax(tk, 1.0e-20);
+            const double P_k = stdmin(prod[q], 20.0 * bet_star * tke_safe * dis_safe);
+            const double Y_k = bet_star * tke_safe * dis_safe;
+            const double P_w = turb_blend(gam1, gam2, F1) * P_k * dis_safe / tke_safe;
+            const double Y_w = turb_blend(bet1, bet2, F1) * dis_safe * dis_safe;
+            const double D_w = 2.0 * (1.0 - F1) * sig_w2 / dis_safe * grad_dot;
+            tks[q] = P_k - Y_k;
+            dss[q] = P_w - Y_w + D_w;
+        }
+    }
+    /* the floor and the caps after the loop (:862-869, clamp_out :631-643) */
+    for(int j = 1; j < jm - 1; j++) for(int k = k_first; k < km - 1; k++) for(int i = 1; i < im - 1; i++){
+        const size_t q = IDX(i,j,k);
+        tke[q] = stdmax(k_bg_nd, tke[q]);
+        dis[q] = stdmax(dis_min, dis[q]);
+        nue[q] = clamp3d(nue[q], 0.0, nue_max);
+        const double dis_src_max = 20.0 * dis[q] * dis[q];
+        dss[q] = clamp3d(dss[q], -dis_src_max, dis_src_max);
+        const double tke_src_max = 20.0 * tke[q] * dis[q];
+        tks[q] = clamp3d(tks[q], -tke_src_max, tke_src_max);
+    }
+    /* apply_wall_bc with TURB_FREE (:383-424): the zero-gradient copy at i = 0 in every column */
+    for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){
+        tke[IDX(0,j,k)] = tke[IDX(1,j,k)];
+        dis[IDX(0,j,k)] = dis[IDX(1,j,k)];
+        nue[IDX(0,j,k)] = nue[IDX(1,j,k)];
+    }
+    /* clamp_nue without the taper (:565-589) */
+    for(size_t q = 0; q < (size_t)im * jm * km; q++) nue[q] = clamp3d(nue[q], 0.0, nue_max) * 1.0;
+    /* seam_copy (:543-562) and fill_lid_corners for a model without the closure's fields in its own
+     * boundary lists (:511-540): the lid row from im-2, then the pole rows from 1 and jm-2 */
+    double* arr[8] = { tke, dis, f[ATURAN_TKEN], f[ATURAN_DISN], nue, prod, tks, dss };
+    if(per)
+        for(int i = 0; i < im; i++) for(int j = 0; j < jm; j++)
+            for(int n = 0; n < 8; n++) arr[n][IDX(i,j,km-1)] = arr[n][IDX(i,j,0)];
+    for(int j = 1; j < jm - 1; j++) for(int k = 0; k < km; k++)
+        for(int n = 0; n < 8; n++) arr[n][IDX(im-1,j,k)] = arr[n][IDX(im-2,j,k)];
+    for(int i = 0; i < im; i++) for(int k = 0; k < km; k++)
+        for(int n = 0; n < 8; n++){
+            arr[n][IDX(i,0,k)] = arr[n][IDX(i,1,k)];
+            arr[n][IDX(i,jm-1,k)] = arr[n][IDX(i,jm-2,k)];
+        }
+    free(rad); free(the);
+    return 0;
+}

@@ -56,6 +56,8 @@ int oracle_post_step(const aturan_params* p, double* const* f, const aturan_post
 int oracle_nh4sh_eq(const aturan_params* p, const aturan_chem_params* cp, double* const* f, long* counts);
 /* cUranusModel.cpp:1074-1087: DiffMassFluxUran, filters, ChemMassRateUran, FluxLimiterNH4SH, filters */
 int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, double* const* f);
+/* Turbulence.h:307-331, Turbulence<cUranusModel>::run with the default knobs (k-omega SST) */
+int oracle_turbulence(const aturan_params* p, const aturan_turb_params* tp, double* const* f);
 
 #ifdef __cplusplus
 }

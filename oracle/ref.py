@@ -72,6 +72,8 @@ class Ref:
             L.ref_clamp_species.argtypes = [vp, vp]
         if hasattr(L, "ref_chem_scalar"):
             L.ref_chem_scalar.argtypes = [ctypes.c_char_p, vp]
+        if hasattr(L, "ref_turb_scalar"):
+            L.ref_turb_scalar.argtypes = [ctypes.c_char_p, vp]
         L.ref_set_quiet(1 if quiet else 0)
         self.L = L
         self.path = path
@@ -184,4 +186,13 @@ class Ref:
     def chem_scalar(self, name):
         d = ctypes.c_double()
         assert self.L.ref_chem_scalar(name.encode(), ctypes.byref(d)) == 0, name
+        return d.value
+
+    def turbulence(self):
+        """Turbulence<cUranusModel>::run (cUranusModel.cpp:1270)."""
+        assert self.L.ref_turbulence() == 0
+
+    def turb_scalar(self, name):
+        d = ctypes.c_double()
+        assert self.L.ref_turb_scalar(name.encode(), ctypes.byref(d)) == 0, name
         return d.value

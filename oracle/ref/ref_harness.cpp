@@ -55,6 +55,7 @@
 #include "PressureSolver.h"
 #include "SaturationAdjustmentUran.h"
 #include "ChemistryUran.h"
+#include "TurbulenceUran.h"
 #include "BC_Uran.h"
 #include "ConvectiveAdjustmentUran.h"
 #undef private
@@ -110,6 +111,7 @@ Array* field(const char* name){
         {"massflux_nh4sh", &m.massflux_nh4sh}, {"fluxlim_nh4sh", &m.fluxlim_nh4sh},
         {"rho_mix", &m.rho_mix}, {"tke_source", &m.tke_source}, {"dis_source", &m.dis_source},
         {"difflux_h2s", &m.difflux_h2s}, {"difflux_nh3", &m.difflux_nh3}, {"difflux_nh4sh", &m.difflux_nh4sh},
+        {"prod", &m.prod},
         {"rhs_t", &m.rhs_t}, {"rhs_u", &m.rhs_u}, {"rhs_v", &m.rhs_v}, {"rhs_w", &m.rhs_w},
         {"rhs_ch4", &m.rhs_ch4}, {"rhs_tke", &m.rhs_tke}, {"rhs_dis", &m.rhs_dis},
         {"rhs_nh4sh", &m.rhs_nh4sh},
@@ -401,6 +403,32 @@ int ref_chem_scalar(const char* name, double* out){
         {"nh4sh_eq", ChemistryUran::nh4sh_eq() ? 1.0 : 0.0},
         {"phi_periodic", ATPhys::phi_periodic<cUranusModel>() ? 1.0 : 0.0},
         {"coord_stretching", m.coord_stretching ? 1.0 : 0.0},
+    };
+    for(const E& e : tab) if(std::strcmp(e.n, name) == 0){ *out = e.v; return 0; }
+    return -1;
+}
+
+
+// The turbulence closure as the loop calls it (cUranusModel.cpp:1270), and its resolved knobs.
+int ref_turbulence(){ Quiet q_; TurbulenceUran(*g_model).run(); return 0; }
+int ref_turb_scalar(const char* name, double* out){
+    cUranusModel& m = *g_model;
+    const std::string tm = m.turb_model;
+    const char* curv_e = getenv("ATURAN_TURB_CURV");
+    const char* buoy_e = getenv("ATURAN_TURB_BUOY");
+    struct E { const char* n; double v; };
+    const E tab[] = {
+        {"active", m.turb_active ? 1.0 : 0.0},
+        {"model", tm == "k_epsilon" ? 0.0 : (tm == "k_omega" ? 1.0 : 2.0)},
+        {"turb_free", (double)TurbulenceUran::turb_free()},
+        {"clamp_pass", (double)TurbulenceUran::turb_clamp_pass()},
+        {"curv", (!curv_e || atoi(curv_e) != 0) ? 1.0 : 0.0},
+        {"buoy", buoy_e ? (double)atoi(buoy_e) : (double)cUranusModel::turb_default_buoy()},
+        {"abl_taper", (double)TurbulenceUran::abl_taper()},
+        {"phi_periodic", ATPhys::phi_periodic<cUranusModel>() ? 1.0 : 0.0},
+        {"nue_max", TurbulenceUran::nue_max_phys()},
+        {"k_bg", TurbulenceUran::turb_k_bg()},
+        {"bc_turb_active", m.bc_turb_active() ? 1.0 : 0.0},
     };
     for(const E& e : tab) if(std::strcmp(e.n, name) == 0){ *out = e.v; return 0; }
     return -1;

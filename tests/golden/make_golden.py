@@ -38,6 +38,8 @@ CASES = {
     "chem_eq": dict(seed=108, outputs=["t", "nh3", "h2s", "nh4sh"]),
     "chem_forcing": dict(seed=109, outputs=["rho_mix", "difflux_h2s", "difflux_nh3", "difflux_nh4sh", "massflux_h2s",
                                             "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "thermalmassflux"]),
+    # the turbulence closure (k-omega SST, default knobs) on turb_case.turb_state(state, seed + 1)
+    "turbulence": dict(seed=110, outputs=["tke", "dis", "nue", "prod", "tke_source", "dis_source", "tken", "disn"]),
 }
 NSAMPLE = 32
 
@@ -75,6 +77,11 @@ def chem_input(p, st, seed):
     return chem_state(st, p, seed + 1)
 
 
+def turb_input(p, st, seed):
+    from tests.turb_case import turb_state
+    return turb_state(st, p, seed + 1)
+
+
 def ref_runner(name, p, st):
     from oracle.ref import Ref
     ref = Ref.get_instance()
@@ -82,6 +89,8 @@ def ref_runner(name, p, st):
         st = post_input(p, st, CASES[name]["seed"])
     if name.startswith("chem_"):
         st = chem_input(p, st, CASES[name]["seed"])
+    if name == "turbulence":
+        st = turb_input(p, st, CASES[name]["seed"])
     ref.load(st)
     if name == "satadj4":
         for g in range(4):
@@ -106,6 +115,8 @@ def ref_runner(name, p, st):
         ref.chem_eq()
     elif name == "chem_forcing":
         ref.chem_forcing()
+    elif name == "turbulence":
+        ref.turbulence()
     out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
     if "buoy_ref_level" in CASES[name]["outputs"]:
         out["buoy_ref_level"] = ref.get("buoy_ref_level")

@@ -78,6 +78,21 @@ def test_chem_params_layout_and_defaults(tmp_path):
     assert bytes(api.library_default_chem_params()) == bytes(P.default_chem_params())
 
 
+def test_turb_params_layout_and_defaults(tmp_path):
+    """aturan_turb_params: the header's layout, and the library's defaults equal the Python mirror's."""
+    src = tmp_path / "tp.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu %zu\\n", sizeof(aturan_turb_params),'
+                   ' offsetof(aturan_turb_params, nue_max), offsetof(aturan_turb_params, nue_air));'
+                   ' return 0; }\n')
+    exe = tmp_path / "tp"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_m, off_a = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.TurbParams)
+    assert off_m == P.TurbParams.nue_max.offset and off_a == P.TurbParams.nue_air.offset
+    assert bytes(api.library_default_turb_params()) == bytes(P.default_turb_params())
+
+
 def test_no_cpu_fallback_without_gpu():
     import torch
     if torch.cuda.is_available():

@@ -41,6 +41,10 @@ def oracle_runner(O, name, p, st):
             O.nh4sh_eq(p, P.default_chem_params(), st)
         else:
             O.chem_forcing(p, P.default_chem_params(), st)
+    elif name == "turbulence":
+        from tests.golden.make_golden import turb_input
+        st = turb_input(p, st, CASES[name]["seed"])
+        O.turbulence(p, P.default_turb_params(), st)
     out = dict(st)
     if lev is not None:
         out["buoy_ref_level"] = lev

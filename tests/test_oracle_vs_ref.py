@@ -198,3 +198,27 @@ def test_chem_forcing(ref_model, oracle_lib, base_state, source):
     oracle_lib.chem_forcing(p, cp, st)
     assert_same(ref_model.state(FORCING_OUT), st, FORCING_OUT)
     assert np.count_nonzero(st["fluxlim_nh4sh"]) > 100000
+
+
+def test_turb_params_are_the_references(ref_model):
+    tp, tr = P.default_turb_params(), P.turb_params_from_ref(ref_model)
+    for name, _ in P.TurbParams._fields_:
+        if name == "reserved_d":
+            continue
+        assert getattr(tp, name) == getattr(tr, name), name
+    assert ref_model.turb_scalar("active") == 1.0 and ref_model.turb_scalar("bc_turb_active") == 0.0
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_turbulence(ref_model, oracle_lib, base_state, source):
+    """Turbulence<cUranusModel>::run (k-omega SST, default knobs): every value it writes (tke, dis,
+    nue, prod, tke_source, dis_source, and tken, disn at the seam and the edges) identical."""
+    from tests.turb_case import TURB_OUT, turb_state
+    p, tp = P.default_params(), P.default_turb_params()
+    base = S.perturb(base_state, p, seed=91) if source == "reference_init" else S.synthetic_state(p, seed=92)
+    st = turb_state(base, p, seed=93)
+    ref_model.load(st)
+    ref_model.turbulence()
+    oracle_lib.turbulence(p, tp, st)
+    assert_same(ref_model.state(TURB_OUT), st, TURB_OUT)
+    assert np.count_nonzero(st["prod"] > 0) > 100000
