@@ -17,8 +17,8 @@ import os
 import numpy as np
 
 from . import fields as F
-from .params import (ChemParams, Params, PostParams, TurbParams, default_chem_params, default_params,
-                     default_post_params, default_turb_params)
+from .params import (ChemParams, Params, PostParams, PrecipParams, TurbParams, default_chem_params, default_params,
+                     default_post_params, default_precip_params, default_turb_params)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
@@ -74,13 +74,15 @@ SIGNATURES = {
                          ctypes.c_int),
     "aturan_turb_params_default": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_turbulence": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_precip_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_precipitation": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 CHEM_NH4SH_EQ, CHEM_FORCING = 1, 2
 
 STATIC_MAX_IM, STATIC_MAX_JM, STATIC_MAX_LEVEL_CELLS = 512, 4096, 1 << 30
 
-KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca", "chem", "turb"]
+KERNEL_KINDS = ["rk_stage", "satadj", "gs", "rb", "hydro", "copy", "adjoint", "post", "mca", "chem", "turb", "precip"]
 NSPECIES = 13
 
 _LIB = None
@@ -135,6 +137,13 @@ def library_default_turb_params():
     rc = load_library().aturan_turb_params_default(ctypes.byref(tp))
     assert rc == 0
     return tp
+
+
+def library_default_precip_params():
+    pp = PrecipParams()
+    rc = load_library().aturan_precip_params_default(ctypes.byref(pp))
+    assert rc == 0
+    return pp
 
 
 class Context:
@@ -228,6 +237,13 @@ class Context:
     def mca(self):
         """aturan_mca: the moist convective adjustment (ConvectiveAdjustment.h:402-849), default knobs."""
         self._check(self.L.aturan_mca(self.h), "mca")
+
+    def precipitation(self, pp=None):
+        """aturan_precipitation: the three-category scheme of H2O, NH3, CH4 and H2S
+        (Precipitation<cUranusModel>::run, cUranusModel.cpp:1037) with pp's knobs (default: the
+        reference's)."""
+        pp = default_precip_params() if pp is None else pp
+        self._check(self.L.aturan_precipitation(self.h, ctypes.byref(pp)), "precipitation")
 
     def turbulence(self, tp=None):
         """aturan_turbulence: the k-omega SST closure (Turbulence<cUranusModel>::run,

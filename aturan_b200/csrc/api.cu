@@ -26,6 +26,7 @@
 #include "post.cuh"
 #include "chem.cuh"
 #include "turb.cuh"
+#include "precip.cuh"
 #include "mca.cuh"
 
 using namespace aturan;
@@ -91,6 +92,7 @@ struct aturan_ctx {
     double* heat;              // aturan_set_heating: [jm][km] K/s, or null
     double* mca_H;             // aturan_mca: the cp table's running integral, made at the first call
     double* chem_tab;          // aturan_chemistry: radius, metric radius (im), sin, cos of the colatitude (jm)
+    double* dz_tab;            // aturan_precipitation: layer thickness [m] per level (the float layer heights)
     // host-side constants
     RhsConst<double> k64;
     RhsConst<float> k32;
@@ -820,6 +822,45 @@ int run_turb(aturan_ctx* ctx, const aturan_turb_params* tp){
     return ATURAN_OK;
 }
 
+// The precipitation on the context's fields (aturan_precipitation).
+template <typename S>
+int run_precip(aturan_ctx* ctx, const aturan_precip_params* pp){
+    const Grid& g = ctx->g;
+    const size_t fs = g.fstride;
+    const aturan_params& p = ctx->p;
+    S* X = reinterpret_cast<S*>(ctx->state);
+    S* Fo = reinterpret_cast<S*>(ctx->forc);
+    auto fo = [&](int id) -> S* { return Fo + (size_t)(id - ATURAN_NUE) * fs; };
+    PrecipArgs<S> a;
+    a.g = g;
+    a.t = X + (size_t)ATURAN_T * fs;
+    a.tlo = ctx->tlo;
+    a.ps = reinterpret_cast<const S*>(ctx->pstat);
+    a.rho = fo(ATURAN_RHO_MIX);
+    a.Q = fo(ATURAN_Q_PRECIP);
+    // the reference's species order H2O, NH3, CH4, H2S (Precipitation.h:214-262, cUranusModel.h:280-297)
+    const int vap[4] = { ATURAN_H2O, ATURAN_NH3, ATURAN_CH4, ATURAN_H2S };
+    const int src[4] = { ATURAN_S_PRECIP_H2O, ATURAN_S_PRECIP_NH3, ATURAN_S_PRECIP_CH4, ATURAN_S_PRECIP_H2S };
+    const int gas[4] = { 0, 2, 3, 1 };                           // the params' order is H2O, H2S, NH3, CH4
+    for(int n = 0; n < 4; n++){
+        for(int c = 0; c < 3; c++){
+            a.sp[n][c] = X + (size_t)(vap[n] + c) * fs;
+            a.ss[n][c] = fo(src[n] + c);
+        }
+        const aturan_gas& G = p.gas[gas[n]];
+        a.gas[n] = PrecipGas{ G.C, G.L0, 1e-3 * G.R, G.del_alf, G.del_bet, G.ep, G.lv, G.ls - G.lv, G.t_0, G.t_00 };
+    }
+    a.dz = ctx->dz_tab;
+    a.rs = pp->rate_scale;
+    a.nd = (p.L_atm * 1.0e3) / p.u_0;                                         // Precipitation.h:420
+    a.r_mix = p.r_mix; a.t_ref = p.t_ref;
+    a.coupling = pp->coupling != 0; a.h2s = pp->h2s != 0; a.local_rho = p.local_rho != 0;
+    Region reg(ctx, ATURAN_K_PRECIP, 0);
+    reg.n = launch_precip(a, ctx->st);
+    CK_LAUNCH("precipitation");
+    return ATURAN_OK;
+}
+
 extern "C" {
 
 int aturan_params_default(aturan_params* p){
@@ -899,7 +940,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     const size_t nbx_all = (size_t)g.im * ctx->bx.nbx;
     if(bx_on){ add(2 * g.im * ncell * 8); add(3 * nbx_all * 8); add(2 * nbx_all * 4); add(4 * nbx_all * 8); }
     add(g.jm * 8); add(g.im * 8); add(g.jm * 8); add(CP_TABLE_N * 8);
-    add((size_t)(2 * g.im + 2 * g.jm) * 8);
+    add((size_t)(2 * g.im + 2 * g.jm) * 8); add((size_t)g.im * 8);
     add(nij * sgeo); add(CP_TABLE_N * e); add(nij * sizeof(GSW)); add(nij * sizeof(RBW)); add(64);
     const int sJ = g.jm - 2, sN = g.km - 1, sNM = sN / 2;
     ctx->sor_nblk = ((sN + 31) / 32) * sJ;
@@ -964,6 +1005,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     ctx->wsin = carve<double>(cur, g.jm); ctx->rm_i = carve<double>(cur, g.im); ctx->cor_j = carve<double>(cur, g.jm);
     ctx->cp_tab64 = carve<double>(cur, CP_TABLE_N);
     ctx->chem_tab = carve<double>(cur, 2 * (size_t)g.im + 2 * (size_t)g.jm);
+    ctx->dz_tab = carve<double>(cur, g.im);
     ctx->geo = carve<char>(cur, nij * sgeo);
     ctx->cp_tab = carve<char>(cur, CP_TABLE_N * e);
     ctx->gsw = carve<GSW>(cur, nij); ctx->rbw = carve<RBW>(cur, nij);
@@ -1202,6 +1244,17 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     for(int i = 0; i < g.im; i++){ chem_tab[i] = rad[i]; chem_tab[g.im + i] = rm_i[i]; }
     for(int j = 0; j < g.jm; j++){ chem_tab[2 * g.im + j] = std::sin(the[j]); chem_tab[2 * g.im + g.jm + j] = std::cos(the[j]); }
     bad |= up(ctx->chem_tab, chem_tab.data(), chem_tab.size() * 8);
+    // cUranusModel.h:1199-1210 and :372-375: heights i * h in float, h = L_atm / (im-1) rounded
+    // to float, the thickness as the float difference in metres (0 for the lid level)
+    std::vector<double> dz_tab(g.im, 0.0);
+    {
+        const float h = (float)(p->L_atm / (g.im - 1));
+        for(int i = 0; i + 1 < g.im; i++){
+            const float hi = (float)(i + 1) * h, lo = (float)i * h;
+            dz_tab[i] = (double)(hi - lo) * 1.0e3;
+        }
+    }
+    bad |= up(ctx->dz_tab, dz_tab.data(), dz_tab.size() * 8);
     bad |= up(ctx->gsw, gsw.data(), nij * sizeof(GSW));
     bad |= up(ctx->rbw, rbw.data(), nij * sizeof(RBW));
     bad |= up(ctx->sor_ct, sct.data(), sct.size() * 8);
@@ -1862,6 +1915,21 @@ int aturan_turbulence(aturan_ctx* ctx, const aturan_turb_params* tp){
         return fail(ctx, ATURAN_E_UNSUPPORTED, "only turb_free = 1, clamp_pass = 1, buoy = 0, abl_taper = 0 are implemented");
     if(ctx->g.im < 3 || ctx->g.jm < 3) return fail(ctx, ATURAN_E_INVALID, "grid too small");
     return ctx->mixed ? run_turb<float>(ctx, tp) : run_turb<double>(ctx, tp);
+}
+
+int aturan_precip_params_default(aturan_precip_params* pp){
+    if(!pp) return ATURAN_E_INVALID;
+    std::memset(pp, 0, sizeof(*pp));
+    pp->abi_version = ATURAN_ABI_VERSION;
+    pp->coupling = 1; pp->h2s = 1;                   // Precipitation.h:164-167, cUranusModel.h:276-279
+    pp->rate_scale = 0.00071;                        // cUranusModel.h:610
+    return ATURAN_OK;
+}
+
+int aturan_precipitation(aturan_ctx* ctx, const aturan_precip_params* pp){
+    if(!ctx || !pp) return ATURAN_E_INVALID;
+    if(pp->abi_version != ATURAN_ABI_VERSION) return fail(ctx, ATURAN_E_INVALID, "abi_version mismatch");
+    return ctx->mixed ? run_precip<float>(ctx, pp) : run_precip<double>(ctx, pp);
 }
 
 int aturan_post_step(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added, long* clamp_cells){

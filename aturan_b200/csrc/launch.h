@@ -11,6 +11,7 @@ template <typename S> struct SatArgs;
 template <typename S> struct PostArgs;
 template <typename S> struct ChemArgs;
 template <typename S> struct TurbArgs;
+template <typename S> struct PrecipArgs;
 struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
@@ -29,7 +30,8 @@ void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_
                     const RBW* w, PressConst c, double* src, cudaStream_t st);                             \
 int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);               \
 int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st);                                         \
-int launch_turb(const TurbArgs<S>& a, cudaStream_t st);
+int launch_turb(const TurbArgs<S>& a, cudaStream_t st);                                                   \
+int launch_precip(const PrecipArgs<S>& a, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)

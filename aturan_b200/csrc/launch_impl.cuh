@@ -7,6 +7,7 @@
 #include "post.cuh"
 #include "chem.cuh"
 #include "turb.cuh"
+#include "precip.cuh"
 
 namespace aturan {
 // Stage launch configuration per storage type, measured on B200 at 41x181x361: resident blocks per
@@ -140,6 +141,12 @@ int launch_turb_impl(const TurbArgs<S>& a, cudaStream_t st){
     turb_edges_kernel<S><<<(unsigned)((nedge + 127) / 128), 128, 0, st>>>(a);
     return 3;
 }
+// The precipitation (precip.cuh): one thread per column; returns the number of launches.
+template <typename S>
+int launch_precip_impl(const PrecipArgs<S>& a, cudaStream_t st){
+    precip_kernel<S><<<dim3((a.g.km + 127) / 128, a.g.jm), 128, 0, st>>>(a);
+    return 1;
+}
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
 template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
@@ -207,4 +214,7 @@ int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st){               
 }                                                                                                         \
 int launch_turb(const TurbArgs<S>& a, cudaStream_t st){                                                   \
     return launch_turb_impl<S>(a, st);                                                                    \
+}                                                                                                         \
+int launch_precip(const PrecipArgs<S>& a, cudaStream_t st){                                               \
+    return launch_precip_impl<S>(a, st);                                                                  \
 }

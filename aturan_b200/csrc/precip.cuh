@@ -1,0 +1,135 @@
+// The precipitation microphysics (planet/Precipitation.h, Precipitation<cUranusModel>::run,
+// :192-277, and its column solver, :280-446) for H2O, NH3, CH4 and then H2S
+// (cUranusModel.h:280-297), no land cells.
+//
+// One thread per (j, k) column walks the levels top down (the scheme is a downward sweep: each
+// level's collection and phase-change terms read the fluxes the level above produced) and runs the
+// four species side by side, their rain / snow / graupel fluxes in registers. Per cell it writes
+// Q_precip once, as the reference's sum over the species in its order (H2O, NH3, CH4, H2S), and
+// the twelve S_precip_* (or, with the coupling off, the condensate fields in place); the lid row
+// and every S field the call does not fill are written with the zeros the reference's first pass
+// puts there, so nothing is launched besides this kernel. The fluxes themselves, the NH4SH settling
+// flux and the surface maps are diagnostics and are not stored. Adjacent threads take adjacent k,
+// so every load and store of a level is coalesced; the work is per-cell FP64 arithmetic with an
+// exp and a log per species and level (two pow where rain falls) on ~16 values read and ~13
+// written.
+#pragma once
+#include "common.cuh"
+
+namespace aturan {
+
+struct PrecipGas {
+    double C, L0, den, del_alf, del_bet;   // liquid saturation set, den = 1e-3 R
+    double ep, lv, Lf, t_frz, t_low;
+};
+
+template <typename S>
+struct PrecipArgs {
+    Grid g;
+    const S *t, *ps, *rho;
+    const float* tlo;                    // the mixed form's temperature pair, else null
+    S* Q;
+    S* sp[4][3];                         // vapour, cloud, ice of H2O, NH3, CH4, H2S
+    S* ss[4][3];                         // S_precip_<gas>, _cloud, _ice
+    PrecipGas gas[4];
+    const double* dz;                    // layer thickness [m] per level (the float layer heights)
+    double rs, nd, r_mix, t_ref;
+    int coupling, h2s, local_rho;
+};
+
+__device__ __forceinline__ double pr_max(double a, double b){ return (a < b) ? b : a; }   // std::max
+__device__ __forceinline__ double pr_min(double a, double b){ return (b < a) ? b : a; }   // std::min
+
+template <typename S>
+__global__ void __launch_bounds__(128) precip_kernel(PrecipArgs<S> a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if(k >= g.km) return;
+    const size_t pl = (size_t)g.jm * g.kp;
+    const size_t o = gidx(g, 0, j, k);
+    // Precipitation.h:89-131 and :286-302
+    const double c_c_au = 2.0e-8, c_i_au = 5.0e-8, q_c_crit = 5.0e-4, c_ac = 1.0e-7, c_rim = 1.0e-8;
+    const double z_csg = 2.5e-8, a_ev = 2.76e-3, c_melt_K = 0.2, c_frz_K = 0.2, P_ref = 1.0e-4;
+    const double v_fall = 2.0, P_max_flux = 1.0e-4, dep_frac = 1.0, ratio_cap = 5.0;
+    const double rs = a.rs;
+    double Pr[4] = {0.0, 0.0, 0.0, 0.0}, Ps[4] = {0.0, 0.0, 0.0, 0.0}, Pg[4] = {0.0, 0.0, 0.0, 0.0};
+    {   // the lid row: zeroed by the first pass, never reached by the sweep
+        const size_t q = o + (size_t)(g.im - 1) * pl;
+        a.Q[q] = (S)0.0;
+#pragma unroll
+        for(int n = 0; n < 4; n++)
+#pragma unroll
+            for(int c = 0; c < 3; c++) a.ss[n][c][q] = (S)0.0;
+    }
+    for(int i = g.im - 2; i >= 0; i--){
+        const size_t q = o + (size_t)i * pl;
+        const double T = t_ld(a.t, a.tlo, q) * a.t_ref;
+        const double p_u = (double)a.ps[q];
+        double rho = a.r_mix;                                  // rho_at, cUranusModel.h:526-531
+        if(a.local_rho){ const double r = (double)a.rho[q]; rho = (r > 0.0 && isfinite(r)) ? r : a.r_mix; }
+        const double dz = pr_max(0.0, a.dz[i]);
+        double Qc = 0.0;                                       // zeroed by the first pass
+#pragma unroll
+        for(int n = 0; n < 4; n++){
+            const bool on = n < 3 || a.h2s;
+            if(!on || dz <= 0.0){                              // dz <= 0: the fluxes pass through
+                a.ss[n][0][q] = (S)0.0; a.ss[n][1][q] = (S)0.0; a.ss[n][2][q] = (S)0.0;
+                continue;
+            }
+            const PrecipGas& s = a.gas[n];
+            const double q_v = pr_max(0.0, (double)a.sp[n][0][q]);
+            const double q_c = pr_max(0.0, (double)a.sp[n][1][q]);
+            const double q_i = pr_max(0.0, (double)a.sp[n][2][q]);
+            const double E_r = exp(s.C + (-s.L0 / T + s.del_alf * log(T) + s.del_bet * T) / s.den);   // ATPhys.h:49-52
+            const double q_sat = (p_u > E_r) ? rho * s.ep * E_r / p_u : q_v;
+            const double F_r_in = Pr[n], F_s_in = Ps[n], F_g_in = Pg[n];
+            const double Rain = pr_min(ratio_cap, F_r_in / P_ref);
+            const double Snow = pr_min(ratio_cap, F_s_in / P_ref);
+            const double Graupel = pr_min(ratio_cap, F_g_in / P_ref);
+            const double Rain_79 = (Rain > 0.0) ? pow(Rain, 7.0 / 9.0) : 0.0;
+            const double Rain_49 = (Rain > 0.0) ? pow(Rain, 4.0 / 9.0) : 0.0;
+            const bool warm = (T >= s.t_frz);
+            const double S_c_au = (warm && q_c > q_c_crit) ? (rs * c_c_au) * (q_c - q_c_crit) : 0.0;
+            const double S_i_au = (!warm && T >= s.t_low) ? (rs * c_i_au) * q_i : 0.0;
+            const double S_ac = warm ? (rs * c_ac) * q_c * Rain_79 : 0.0;
+            const double S_s_rim = !warm ? (rs * c_rim) * q_c * Snow : 0.0;
+            const double S_g_rim = !warm ? (rs * c_rim) * q_c * Graupel : 0.0;
+            const double S_csg = (!warm && q_c > q_c_crit) ? (rs * z_csg) * q_c * Snow : 0.0;
+            const double f_melt = warm ? pr_min(1.0, c_melt_K * (T - s.t_frz)) : 0.0;
+            const double f_frz = warm ? 0.0 : pr_min(1.0, c_frz_K * (s.t_frz - T));
+            const double F_s_melt = f_melt * F_s_in;
+            const double F_g_melt = f_melt * F_g_in;
+            const double F_r_frz = f_frz * F_r_in;
+            const double F_r_avail = pr_max(0.0, F_r_in - F_r_frz + F_s_melt + F_g_melt + (S_c_au + S_ac) * dz);
+            const double S_ev_raw = (warm && Rain > 0.0 && q_v < q_sat) ? a_ev * (q_sat - q_v) * Rain_49 : 0.0;
+            const double F_ev_sat = pr_max(0.0, q_sat - q_v) * v_fall;
+            const double F_ev = pr_min(pr_min(S_ev_raw * dz, F_r_avail), F_ev_sat);
+            const double S_ev = F_ev / dz;
+            Qc += s.Lf * (S_s_rim + S_g_rim + S_csg)
+                + s.Lf * (F_r_frz - F_s_melt - F_g_melt) / dz
+                - s.lv * F_ev / dz;
+            const double tau = dz / v_fall;
+            const double d_c = pr_min(dep_frac * q_c, (S_c_au + S_ac + S_s_rim + S_g_rim + S_csg) * tau);
+            const double d_i = pr_min(dep_frac * q_i, S_i_au * tau);
+            if(a.coupling){
+                a.ss[n][1][q] = (S)(-pr_max(0.0, d_c) / tau * a.nd);
+                a.ss[n][2][q] = (S)(-pr_max(0.0, d_i) / tau * a.nd);
+                a.ss[n][0][q] = (S)(+S_ev * a.nd);
+            } else {
+                a.sp[n][1][q] = (S)(q_c - pr_max(0.0, d_c));
+                a.sp[n][2][q] = (S)(q_i - pr_max(0.0, d_i));
+                a.sp[n][0][q] = (S)(q_v + S_ev * tau);
+                a.ss[n][0][q] = (S)0.0; a.ss[n][1][q] = (S)0.0; a.ss[n][2][q] = (S)0.0;
+            }
+            const double F_r = F_r_in - F_r_frz + F_s_melt + F_g_melt - F_ev + (S_c_au + S_ac) * dz;
+            const double F_s = F_s_in - F_s_melt + (S_i_au + S_s_rim - S_csg) * dz;
+            const double F_g = F_g_in - F_g_melt + F_r_frz + (S_g_rim + S_csg) * dz;
+            Pr[n] = pr_min(P_max_flux, pr_max(0.0, F_r));
+            Ps[n] = pr_min(P_max_flux, pr_max(0.0, F_s));
+            Pg[n] = pr_min(P_max_flux, pr_max(0.0, F_g));
+        }
+        a.Q[q] = (S)Qc;
+    }
+}
+
+}  // namespace aturan

@@ -260,3 +260,31 @@ def turb_params_from_ref(ref):
     tp.nue_max = ref.turb_scalar("nue_max")
     tp.k_bg = ref.turb_scalar("k_bg")
     return tp
+
+
+class PrecipParams(ctypes.Structure):
+    """aturan_precip_params: the precipitation's knobs (planet/Precipitation.h)."""
+    _fields_ = ([(n, ctypes.c_int32) for n in ("abi_version", "coupling", "h2s")]
+                + [("reserved_i", ctypes.c_int32 * 5)]
+                + [("rate_scale", ctypes.c_double)]
+                + [("reserved_d", ctypes.c_double * 7)])
+
+
+def default_precip_params():
+    """The reference's values with its ATURAN_* knobs unset (Precipitation.h:164-167,
+    cUranusModel.h:276-279 and :610)."""
+    pp = PrecipParams()
+    pp.abi_version = ABI_VERSION
+    pp.coupling = 1
+    pp.h2s = 1
+    pp.rate_scale = 0.00071
+    return pp
+
+
+def precip_params_from_ref(ref):
+    """The precipitation knobs read from the initialised reference model."""
+    pp = default_precip_params()
+    pp.coupling = int(ref.precip_scalar("coupling"))
+    pp.h2s = int(ref.precip_scalar("h2s"))
+    pp.rate_scale = ref.precip_scalar("rate_scale")
+    return pp

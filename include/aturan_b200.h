@@ -413,6 +413,33 @@ int aturan_turb_params_default(aturan_turb_params* tp);
  * other than those supported return ATURAN_E_UNSUPPORTED. */
 int aturan_turbulence(aturan_ctx* ctx, const aturan_turb_params* tp);
 
+/* The precipitation microphysics (planet/Precipitation.h, Precipitation<cUranusModel>::run,
+ * :192-277, and its column solver, :280-446) as the model's loop calls it (cUranusModel.cpp:1037,
+ * after the NH4SH equilibrium and
+ * before the n-copy sync, on by default): per (j, k) column, top down, the three-category
+ * (rain / snow / graupel) scheme of each condensable in the order H2O, NH3, CH4 and then H2S
+ * (cUranusModel.h:280-297). */
+typedef struct aturan_precip_params {
+    int32_t abi_version;         /* = ATURAN_ABI_VERSION */
+    int32_t coupling;            /* ATURAN_PRECIP_COUPLING (Precipitation.h:164): 1 (default) the depletion
+                                    as rates in S_precip_*; 0 written into the condensate fields */
+    int32_t h2s;                 /* ATURAN_PRECIP_H2S (cUranusModel.h:276): 1 (default) H2S runs too */
+    int32_t reserved_i[5];
+    double rate_scale;           /* ATURAN_PRECIP_SCALE: the factor on the five rate coefficients,
+                                    Uranus's default 0.00071 (cUranusModel.h:610) */
+    double reserved_d[7];
+} aturan_precip_params;
+
+/* Fill the reference's defaults. */
+int aturan_precip_params_default(aturan_precip_params* pp);
+
+/* Q_precip and the twelve S_precip_* zeroed, then every column of every species: Q_precip gains
+ * each species' latent heating; with coupling, S_precip_<gas>, _cloud, _ice receive the vapour
+ * source and the cloud and ice depletion rates (nondimensional); without it the vapour, cloud and
+ * ice fields are updated in place. The precipitation fluxes themselves (P_rain, ..., the NH4SH
+ * settling flux and the surface maps) are the reference's diagnostics and are not kept. */
+int aturan_precipitation(aturan_ctx* ctx, const aturan_precip_params* pp);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */
@@ -426,6 +453,7 @@ enum aturan_kernel_kind {
     ATURAN_K_MCA,            /* moist convective adjustment (aturan_mca) */
     ATURAN_K_CHEM,           /* NH4SH equilibrium and chemistry forcing (aturan_chemistry) */
     ATURAN_K_TURB,           /* turbulence closure (aturan_turbulence) */
+    ATURAN_K_PRECIP,         /* precipitation microphysics (aturan_precipitation) */
     ATURAN_K_NKINDS
 };
 

@@ -87,6 +87,7 @@ class Oracle:
             ("oracle_nh4sh_eq", [P, P, vp, vp], ctypes.c_int),
             ("oracle_chem_forcing", [P, P, vp], ctypes.c_int),
             ("oracle_turbulence", [P, P, vp], ctypes.c_int),
+            ("oracle_precipitation", [P, P, vp], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -214,3 +215,7 @@ class Oracle:
     def turbulence(self, p, tp, state):
         """Turbulence<cUranusModel>::run (k-omega SST, default knobs) on the state in place."""
         assert self.L.oracle_turbulence(self._p(p), self._p(tp), field_ptrs(state)) == 0
+
+    def precipitation(self, p, pp, state):
+        """Precipitation<cUranusModel>::run (H2O, NH3, CH4, H2S) on the state in place."""
+        assert self.L.oracle_precipitation(self._p(p), self._p(pp), field_ptrs(state)) == 0

@@ -2439,3 +2439,116 @@ int oracle_turbulence(const aturan_params* p, const aturan_turb_params* tp, doub
     free(rad); free(the);
     return 0;
 }
+
+/* ---- Precipitation<cUranusModel>::run (planet/Precipitation.h:192-277) and its column solver
+ * (:280-446) for H2O, NH3, CH4 and H2S (cUranusModel.h:280-297), no land cells. The fluxes
+ * P_rain, P_snow, P_graupel of a column are carried down the column in locals; they, the NH4SH
+ * settling flux and the surface maps are diagnostics the hot path does not keep. ---- */
+
+/* cUranusModel.h:1199-1210 and :372-375: float layer heights i * (L_atm / (im-1)), thickness in m */
+static double precip_dz(const aturan_params* p, int i){
+    if(i < 0 || i > p->im - 2) return 0.0;
+    const float h = (float)(p->L_atm / (p->im - 1));
+    const float hi = (float)(i + 1) * h, lo = (float)i * h;
+    return (double)(hi - lo) * 1.0e3;
+}
+
+/* one species, every column (Precipitation.h:281-446) */
+static void precip_column(const aturan_params* p, const aturan_precip_params* pp, double* const* f,
+                          const aturan_gas* s, int fv, int fc, int fi, int sv, int sc, int si){
+    const int im = p->im, jm = p->jm, km = p->km;
+    const double c_c_au = 2.0e-8, c_i_au = 5.0e-8, q_c_crit = 5.0e-4, c_ac = 1.0e-7, c_rim = 1.0e-8;
+    const double z_csg = 2.5e-8, a_ev = 2.76e-3, c_melt_K = 0.2, c_frz_K = 0.2, P_ref = 1.0e-4;
+    const double v_fall = 2.0;
+    const double t_ref = p->t_ref;
+    const double Lf = s->ls - s->lv;
+    const double P_max_flux = 1.0e-4, dep_frac = 1.0, ratio_cap = 5.0;
+    const double rs = pp->rate_scale;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for(int j = 0; j < jm; j++) for(int k = 0; k < km; k++){
+        double Pr = 0.0, Ps = 0.0, Pg = 0.0;                    /* the fluxes at i + 1 */
+        for(int i = im - 2; i >= 0; i--){
+            const size_t q = IDX(i,j,k);
+            const double T = f[ATURAN_T][q] * t_ref;
+            const double p_u = f[ATURAN_P_STAT][q];
+            const double q_v = stdmax(0.0, f[fv][q]);
+            const double q_c = stdmax(0.0, f[fc][q]);
+            const double q_i = stdmax(0.0, f[fi][q]);
+            const double E_r = svp(T, s->C, s->L0, s->R, s->del_alf, s->del_bet);
+            double rho = p->r_mix;                                 /* rho_at, cUranusModel.h:526-531 */
+            if(p->local_rho){ const double r = f[ATURAN_RHO_MIX][q]; rho = (r > 0.0 && isfinite(r)) ? r : p->r_mix; }
+            const double q_sat = (p_u > E_r) ? rho * s->ep * E_r / p_u : q_v;
+            const double dz = stdmax(0.0, precip_dz(p, i));
+            if(dz <= 0.0) continue;                                /* the fluxes pass through */
+            const double F_r_in = Pr, F_s_in = Ps, F_g_in = Pg;
+            const double Rain = stdmin(ratio_cap, F_r_in / P_ref);
+            const double Snow = stdmin(ratio_cap, F_s_in / P_ref);
+            const double Graupel = stdmin(ratio_cap, F_g_in / P_ref);
+            const double Rain_79 = (Rain > 0.0) ? pow(Rain, 7.0 / 9.0) : 0.0;
+            const double Rain_49 = (Rain > 0.0) ? pow(Rain, 4.0 / 9.0) : 0.0;
+            const int warm = (T >= s->t_0);
+            const double S_c_au = (warm && q_c > q_c_crit) ? (rs * c_c_au) * (q_c - q_c_crit) : 0.0;
+            const double S_i_au = (!warm && T >= s->t_00) ? (rs * c_i_au) * q_i : 0.0;
+            const double S_ac = warm ? (rs * c_ac) * q_c * Rain_79 : 0.0;
+            const double S_s_rim = !warm ? (rs * c_rim) * q_c * Snow : 0.0;
+            const double S_g_rim = !warm ? (rs * c_rim) * q_c * Graupel : 0.0;
+            const double S_csg = (!warm && q_c > q_c_crit) ? (rs * z_csg) * q_c * Snow : 0.0;
+            const double f_melt = warm ? stdmin(1.0, c_melt_K * (T - s->t_0)) : 0.0;
+            const double f_frz = warm ? 0.0 : stdmin(1.0, c_frz_K * (s->t_0 - T));
+            const double F_s_melt = f_melt * F_s_in;
+            const double F_g_melt = f_melt * F_g_in;
+            const double F_r_frz = f_frz * F_r_in;
+            const double F_r_avail = stdmax(0.0, F_r_in - F_r_frz + F_s_melt + F_g_melt + (S_c_au + S_ac) * dz);
+            const double S_ev_raw = (warm && Rain > 0.0 && q_v < q_sat) ? a_ev * (q_sat - q_v) * Rain_49 : 0.0;
+            const double F_ev_sat = stdmax(0.0, q_sat - q_v) * v_fall;
+            const double F_ev = stdmin(stdmin(S_ev_raw * dz, F_r_avail), F_ev_sat);
+            const double S_ev = F_ev / dz;
+            f[ATURAN_Q_PRECIP][q] += Lf * (S_s_rim + S_g_rim + S_csg)
+                                   + Lf * (F_r_frz - F_s_melt - F_g_melt) / dz
+                                   - s->lv * F_ev / dz;
+            const double tau = dz / v_fall;
+            const double d_c = stdmin(dep_frac * q_c, (S_c_au + S_ac + S_s_rim + S_g_rim + S_csg) * tau);
+            const double d_i = stdmin(dep_frac * q_i, S_i_au * tau);
+            if(pp->coupling){
+                const double nd = (p->L_atm * 1.0e3) / p->u_0;
+                f[sc][q] = -stdmax(0.0, d_c) / tau * nd;
+                f[si][q] = -stdmax(0.0, d_i) / tau * nd;
+                f[sv][q] = +S_ev * nd;
+            } else {
+                f[fc][q] = q_c - stdmax(0.0, d_c);
+                f[fi][q] = q_i - stdmax(0.0, d_i);
+                f[fv][q] = q_v + S_ev * tau;
+            }
+            const double F_r = F_r_in - F_r_frz + F_s_melt + F_g_melt - F_ev + (S_c_au + S_ac) * dz;
+            const double F_s = F_s_in - F_s_melt + (S_i_au + S_s_rim - S_csg) * dz;
+            const double F_g = F_g_in - F_g_melt + F_r_frz + (S_g_rim + S_csg) * dz;
+            Pr = stdmin(P_max_flux, stdmax(0.0, F_r));
+            Ps = stdmin(P_max_flux, stdmax(0.0, F_s));
+            Pg = stdmin(P_max_flux, stdmax(0.0, F_g));
+        }
+    }
+}
+
+int oracle_precipitation(const aturan_params* p, const aturan_precip_params* pp, double* const* f){
+    const size_t N = (size_t)p->im * p->jm * p->km;
+    /* Precipitation.h:199-212 */
+    static const int zero_me[] = { ATURAN_Q_PRECIP, ATURAN_S_PRECIP_H2O, ATURAN_S_PRECIP_H2O_CLOUD,
+        ATURAN_S_PRECIP_H2O_ICE, ATURAN_S_PRECIP_NH3, ATURAN_S_PRECIP_NH3_CLOUD, ATURAN_S_PRECIP_NH3_ICE,
+        ATURAN_S_PRECIP_CH4, ATURAN_S_PRECIP_CH4_CLOUD, ATURAN_S_PRECIP_CH4_ICE };
+    for(int n = 0; n < 10; n++) memset(f[zero_me[n]], 0, sizeof(double) * N);
+    /* the params' gas order is H2O, H2S, NH3, CH4 */
+    precip_column(p, pp, f, &p->gas[0], ATURAN_H2O, ATURAN_H2O_CLOUD, ATURAN_H2O_ICE,
+                  ATURAN_S_PRECIP_H2O, ATURAN_S_PRECIP_H2O_CLOUD, ATURAN_S_PRECIP_H2O_ICE);
+    precip_column(p, pp, f, &p->gas[2], ATURAN_NH3, ATURAN_NH3_CLOUD, ATURAN_NH3_ICE,
+                  ATURAN_S_PRECIP_NH3, ATURAN_S_PRECIP_NH3_CLOUD, ATURAN_S_PRECIP_NH3_ICE);
+    precip_column(p, pp, f, &p->gas[3], ATURAN_CH4, ATURAN_CH4_CLOUD, ATURAN_CH4_ICE,
+                  ATURAN_S_PRECIP_CH4, ATURAN_S_PRECIP_CH4_CLOUD, ATURAN_S_PRECIP_CH4_ICE);
+    /* cUranusModel.h:280-297, precip_extra_species */
+    memset(f[ATURAN_S_PRECIP_H2S], 0, sizeof(double) * N);
+    memset(f[ATURAN_S_PRECIP_H2S_CLOUD], 0, sizeof(double) * N);
+    memset(f[ATURAN_S_PRECIP_H2S_ICE], 0, sizeof(double) * N);
+    if(pp->h2s)
+        precip_column(p, pp, f, &p->gas[1], ATURAN_H2S, ATURAN_H2S_CLOUD, ATURAN_H2S_ICE,
+                      ATURAN_S_PRECIP_H2S, ATURAN_S_PRECIP_H2S_CLOUD, ATURAN_S_PRECIP_H2S_ICE);
+    return 0;
+}

@@ -58,6 +58,8 @@ int oracle_nh4sh_eq(const aturan_params* p, const aturan_chem_params* cp, double
 int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, double* const* f);
 /* Turbulence.h:307-331, Turbulence<cUranusModel>::run with the default knobs (k-omega SST) */
 int oracle_turbulence(const aturan_params* p, const aturan_turb_params* tp, double* const* f);
+/* Precipitation.h:192-446 for H2O, NH3, CH4, H2S (cUranusModel.h:280-297) */
+int oracle_precipitation(const aturan_params* p, const aturan_precip_params* pp, double* const* f);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,8 @@ class Ref:
             L.ref_chem_scalar.argtypes = [ctypes.c_char_p, vp]
         if hasattr(L, "ref_turb_scalar"):
             L.ref_turb_scalar.argtypes = [ctypes.c_char_p, vp]
+        if hasattr(L, "ref_precip_scalar"):
+            L.ref_precip_scalar.argtypes = [ctypes.c_char_p, vp]
         L.ref_set_quiet(1 if quiet else 0)
         self.L = L
         self.path = path
@@ -195,4 +197,13 @@ class Ref:
     def turb_scalar(self, name):
         d = ctypes.c_double()
         assert self.L.ref_turb_scalar(name.encode(), ctypes.byref(d)) == 0, name
+        return d.value
+
+    def precipitation(self):
+        """Precipitation<cUranusModel>::run (cUranusModel.cpp:1037)."""
+        assert self.L.ref_precipitation() == 0
+
+    def precip_scalar(self, name):
+        d = ctypes.c_double()
+        assert self.L.ref_precip_scalar(name.encode(), ctypes.byref(d)) == 0, name
         return d.value

@@ -56,6 +56,7 @@
 #include "SaturationAdjustmentUran.h"
 #include "ChemistryUran.h"
 #include "TurbulenceUran.h"
+#include "PrecipitationUran.h"
 #include "BC_Uran.h"
 #include "ConvectiveAdjustmentUran.h"
 #undef private
@@ -429,6 +430,20 @@ int ref_turb_scalar(const char* name, double* out){
         {"nue_max", TurbulenceUran::nue_max_phys()},
         {"k_bg", TurbulenceUran::turb_k_bg()},
         {"bc_turb_active", m.bc_turb_active() ? 1.0 : 0.0},
+    };
+    for(const E& e : tab) if(std::strcmp(e.n, name) == 0){ *out = e.v; return 0; }
+    return -1;
+}
+
+
+// The precipitation as the loop calls it (cUranusModel.cpp:1037), and its resolved knobs.
+int ref_precipitation(){ Quiet q_; PrecipitationUran(*g_model).run(); return 0; }
+int ref_precip_scalar(const char* name, double* out){
+    struct E { const char* n; double v; };
+    const E tab[] = {
+        {"coupling", PrecipitationUran::coupling_on() ? 1.0 : 0.0},
+        {"h2s", cUranusModel::precip_h2s_on() ? 1.0 : 0.0},
+        {"rate_scale", PrecipitationUran::rate_scale()},
     };
     for(const E& e : tab) if(std::strcmp(e.n, name) == 0){ *out = e.v; return 0; }
     return -1;

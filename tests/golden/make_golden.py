@@ -40,6 +40,11 @@ CASES = {
                                             "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "thermalmassflux"]),
     # the turbulence closure (k-omega SST, default knobs) on turb_case.turb_state(state, seed + 1)
     "turbulence": dict(seed=110, outputs=["tke", "dis", "nue", "prod", "tke_source", "dis_source", "tken", "disn"]),
+    # the precipitation (default knobs) on precip_case.precip_state(state, seed + 1)
+    "precipitation": dict(seed=111, outputs=["Q_precip", "S_precip_ch4", "S_precip_ch4_cloud", "S_precip_ch4_ice",
+                                             "S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice",
+                                             "S_precip_h2s", "S_precip_h2s_cloud", "S_precip_h2s_ice",
+                                             "S_precip_nh3", "S_precip_nh3_cloud", "S_precip_nh3_ice"]),
 }
 NSAMPLE = 32
 
@@ -82,6 +87,11 @@ def turb_input(p, st, seed):
     return turb_state(st, p, seed + 1)
 
 
+def precip_input(p, st, seed):
+    from tests.precip_case import precip_state
+    return precip_state(st, p, seed + 1)
+
+
 def ref_runner(name, p, st):
     from oracle.ref import Ref
     ref = Ref.get_instance()
@@ -91,6 +101,8 @@ def ref_runner(name, p, st):
         st = chem_input(p, st, CASES[name]["seed"])
     if name == "turbulence":
         st = turb_input(p, st, CASES[name]["seed"])
+    if name == "precipitation":
+        st = precip_input(p, st, CASES[name]["seed"])
     ref.load(st)
     if name == "satadj4":
         for g in range(4):
@@ -117,6 +129,8 @@ def ref_runner(name, p, st):
         ref.chem_forcing()
     elif name == "turbulence":
         ref.turbulence()
+    elif name == "precipitation":
+        ref.precipitation()
     out = ref.state([n for n in CASES[name]["outputs"] if n != "buoy_ref_level"])
     if "buoy_ref_level" in CASES[name]["outputs"]:
         out["buoy_ref_level"] = ref.get("buoy_ref_level")

@@ -93,6 +93,19 @@ def test_turb_params_layout_and_defaults(tmp_path):
     assert bytes(api.library_default_turb_params()) == bytes(P.default_turb_params())
 
 
+def test_precip_params_layout_and_defaults(tmp_path):
+    """aturan_precip_params: the header's layout, and the library's defaults equal the Python mirror's."""
+    src = tmp_path / "pr.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu\\n", sizeof(aturan_precip_params),'
+                   ' offsetof(aturan_precip_params, rate_scale)); return 0; }\n')
+    exe = tmp_path / "pr"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_r = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.PrecipParams) and off_r == P.PrecipParams.rate_scale.offset
+    assert bytes(api.library_default_precip_params()) == bytes(P.default_precip_params())
+
+
 def test_no_cpu_fallback_without_gpu():
     import torch
     if torch.cuda.is_available():

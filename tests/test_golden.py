@@ -45,6 +45,10 @@ def oracle_runner(O, name, p, st):
         from tests.golden.make_golden import turb_input
         st = turb_input(p, st, CASES[name]["seed"])
         O.turbulence(p, P.default_turb_params(), st)
+    elif name == "precipitation":
+        from tests.golden.make_golden import precip_input
+        st = precip_input(p, st, CASES[name]["seed"])
+        O.precipitation(p, P.default_precip_params(), st)
     out = dict(st)
     if lev is not None:
         out["buoy_ref_level"] = lev

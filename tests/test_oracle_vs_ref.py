@@ -222,3 +222,48 @@ def test_turbulence(ref_model, oracle_lib, base_state, source):
     oracle_lib.turbulence(p, tp, st)
     assert_same(ref_model.state(TURB_OUT), st, TURB_OUT)
     assert np.count_nonzero(st["prod"] > 0) > 100000
+
+
+def test_precip_params_are_the_references(ref_model):
+    pp, pr = P.default_precip_params(), P.precip_params_from_ref(ref_model)
+    for name in ("coupling", "h2s", "rate_scale"):
+        assert getattr(pp, name) == getattr(pr, name), name
+
+
+@pytest.mark.parametrize("source", ["reference_init", "synthetic"])
+def test_precipitation(ref_model, oracle_lib, base_state, source):
+    """Precipitation<cUranusModel>::run (H2O, NH3, CH4, H2S, default knobs): Q_precip and the twelve
+    S_precip_* identical in every cell; at least two species precipitate in many cells (H2O, whose
+    ice-autoconversion band lies above the domain's temperatures, does not)."""
+    from tests.precip_case import PRECIP_OUT, precip_state
+    p, pp = P.default_params(), P.default_precip_params()
+    base = S.perturb(base_state, p, seed=95) if source == "reference_init" else S.synthetic_state(p, seed=96)
+    st = precip_state(base, p, seed=97)
+    ref_model.load(st)
+    ref_model.precipitation()
+    oracle_lib.precipitation(p, pp, st)
+    assert_same(ref_model.state(PRECIP_OUT), st, PRECIP_OUT)
+    active = [g for g in ("h2o", "nh3", "ch4", "h2s")
+              if np.count_nonzero(st["S_precip_" + g + "_cloud"]) + np.count_nonzero(st["S_precip_" + g + "_ice"]) > 1000]
+    assert len(active) >= 2, active
+    assert np.count_nonzero(st["Q_precip"]) > 1000
+
+
+@pytest.mark.parametrize("knobs", ["chem_minus_open_phi", "turb_no_curv_open_phi", "precip_uncoupled", "precip_no_h2s"])
+def test_physics_knob_sets(knobs):
+    """Other knob values of the chemistry (massflux = -difflux, the open phi seam), the turbulence
+    closure (no curvature terms, the open seam) and the precipitation (the depletion written into the
+    condensate fields; no H2S and another rate scale), each in a child process with that environment;
+    the child requires bit equality of every written value."""
+    import os
+    import subprocess
+    import sys
+    from oracle import ref
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _physics_knobs_child import KNOB_SETS
+    if not ref.available():
+        pytest.skip("compiled reference (oracle/_ref) not present")
+    env = dict(os.environ, **KNOB_SETS[knobs][0])
+    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_physics_knobs_child.py")
+    r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
