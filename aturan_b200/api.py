@@ -17,8 +17,9 @@ import os
 import numpy as np
 
 from . import fields as F
-from .params import (ChemParams, Params, PostParams, PrecipParams, TurbParams, default_chem_params, default_params,
-                     default_post_params, default_precip_params, default_turb_params)
+from .params import (ChemParams, IterParams, Params, PostParams, PrecipParams, TurbParams, default_chem_params,
+                     default_iter_params, default_params, default_post_params, default_precip_params,
+                     default_turb_params)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaturan_b200.so")
@@ -76,6 +77,8 @@ SIGNATURES = {
     "aturan_turbulence": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_precip_params_default": ([ctypes.c_void_p], ctypes.c_int),
     "aturan_precipitation": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "aturan_iter_params_default": ([ctypes.c_void_p], ctypes.c_int),
+    "aturan_iteration": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
 }
 
 CHEM_NH4SH_EQ, CHEM_FORCING = 1, 2
@@ -144,6 +147,13 @@ def library_default_precip_params():
     rc = load_library().aturan_precip_params_default(ctypes.byref(pp))
     assert rc == 0
     return pp
+
+
+def library_default_iter_params():
+    ip = IterParams()
+    rc = load_library().aturan_iter_params_default(ctypes.byref(ip))
+    assert rc == 0
+    return ip
 
 
 class Context:
@@ -237,6 +247,12 @@ class Context:
     def mca(self):
         """aturan_mca: the moist convective adjustment (ConvectiveAdjustment.h:402-849), default knobs."""
         self._check(self.L.aturan_mca(self.h), "mca")
+
+    def iteration(self, iter_n, ip=None):
+        """aturan_iteration: iteration number iter_n (from 1) of the model's loop
+        (cUranusModel.cpp:952-1296) with ip's knobs (default: the reference's)."""
+        ip = default_iter_params() if ip is None else ip
+        self._check(self.L.aturan_iteration(self.h, ctypes.byref(ip), int(iter_n)), "iteration")
 
     def precipitation(self, pp=None):
         """aturan_precipitation: the three-category scheme of H2O, NH3, CH4 and H2S

@@ -745,7 +745,8 @@ int run_post(aturan_ctx* ctx, const aturan_post_params* pp, double* clamp_added,
 
 // The chemistry on the context's fields (aturan_chemistry).
 template <typename S>
-int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what){
+int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what, cudaStream_t st = nullptr){
+    if(!st) st = ctx->st;
     const Grid& g = ctx->g;
     const size_t fs = g.fstride;
     const aturan_params& p = ctx->p;
@@ -781,8 +782,8 @@ int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what){
     c.sinthe_min = p.sinthe_min; c.floor = cp->polar_floor;
     c.per = cp->phi_periodic != 0;
     a.counts = ctx->counters + 4;
-    Region reg(ctx, ATURAN_K_CHEM, 0);
-    reg.n = launch_chem(a, what, ctx->st);
+    Region reg(ctx, ATURAN_K_CHEM, 0, st);
+    reg.n = launch_chem(a, what, st);
     CK_LAUNCH("chemistry");
     return ATURAN_OK;
 }
@@ -824,7 +825,8 @@ int run_turb(aturan_ctx* ctx, const aturan_turb_params* tp){
 
 // The precipitation on the context's fields (aturan_precipitation).
 template <typename S>
-int run_precip(aturan_ctx* ctx, const aturan_precip_params* pp){
+int run_precip(aturan_ctx* ctx, const aturan_precip_params* pp, cudaStream_t st = nullptr){
+    if(!st) st = ctx->st;
     const Grid& g = ctx->g;
     const size_t fs = g.fstride;
     const aturan_params& p = ctx->p;
@@ -855,8 +857,8 @@ int run_precip(aturan_ctx* ctx, const aturan_precip_params* pp){
     a.nd = (p.L_atm * 1.0e3) / p.u_0;                                         // Precipitation.h:420
     a.r_mix = p.r_mix; a.t_ref = p.t_ref;
     a.coupling = pp->coupling != 0; a.h2s = pp->h2s != 0; a.local_rho = p.local_rho != 0;
-    Region reg(ctx, ATURAN_K_PRECIP, 0);
-    reg.n = launch_precip(a, ctx->st);
+    Region reg(ctx, ATURAN_K_PRECIP, 0, st);
+    reg.n = launch_precip(a, st);
     CK_LAUNCH("precipitation");
     return ATURAN_OK;
 }
@@ -1892,6 +1894,90 @@ int aturan_chemistry(aturan_ctx* ctx, const aturan_chem_params* cp, int what, lo
         if(n_decomposed) *n_decomposed = (long)h[1];
     }
     return ATURAN_OK;
+}
+
+int aturan_iter_params_default(aturan_iter_params* ip){
+    if(!ip) return ATURAN_E_INVALID;
+    std::memset(ip, 0, sizeof(*ip));
+    ip->abi_version = ATURAN_ABI_VERSION;
+    ip->press_kind = ATURAN_PRESS_GS_LEX; ip->max_sweeps = 1;   // PressureSolverUran (cUranusModel.cpp:970-972)
+    ip->chemistry = 1; ip->precipitation = 1;                    // NH4SH_EQ, ATURAN_PRECIP (:105-108)
+    ip->turbulence = 1; ip->mca_stride = 1;                      // turb_active (:482), ATURAN_MCA (:131-134)
+    ip->omega = 1.0; ip->tol = 0.0;
+    ip->damp_p_horiz = 0.0;                                      // :979-980 with GEO_BALANCE
+    aturan_post_params_default(&ip->post);
+    aturan_chem_params_default(&ip->chem);
+    aturan_turb_params_default(&ip->turb);
+    aturan_precip_params_default(&ip->precip);
+    return ATURAN_OK;
+}
+
+int aturan_iteration(aturan_ctx* ctx, const aturan_iter_params* ip, int iter_n){
+    if(!ctx || !ip) return ATURAN_E_INVALID;
+    if(ip->abi_version != ATURAN_ABI_VERSION || ip->post.abi_version != ATURAN_ABI_VERSION ||
+       ip->chem.abi_version != ATURAN_ABI_VERSION || ip->turb.abi_version != ATURAN_ABI_VERSION ||
+       ip->precip.abi_version != ATURAN_ABI_VERSION) return fail(ctx, ATURAN_E_INVALID, "abi_version mismatch");
+    if(iter_n < 1) return fail(ctx, ATURAN_E_INVALID, "iter_n counts from 1");
+    // every knob checked before the first launch
+    if(ip->chemistry && (ip->chem.nh4sh_eq != 1 || ip->chem.difflux_laplacian != 1))
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "chemistry: only nh4sh_eq = 1 and difflux_laplacian = 1 are implemented");
+    if(ip->turbulence && (ip->turb.model != 2 || ip->turb.turb_free != 1 || ip->turb.clamp_pass != 1 ||
+                          ip->turb.buoy != 0 || ip->turb.abl_taper != 0))
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "turbulence: only the default knobs are implemented");
+    const bool mca = ip->mca_stride > 0 && iter_n % ip->mca_stride == 0;
+    if(ip->mca_stride > 0 && (ctx->mixed || ctx->g.im > MCA_MAXI))
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "moist convective adjustment: FP64 contexts with im <= 64 only");
+    int rc;
+    if(iter_n % 2 == 0){
+        // the saturation adjustment and what follows it up to the chemistry forcing touch no field
+        // of the pressure solve and its filter: they run on the second stream beside it
+        CK(cudaEventRecord(ctx->ev_fork, ctx->st));
+        CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
+        int rc2 = ctx->mixed ? run_satadj<float>(ctx, 0xF, false, ctx->st2) : run_satadj<double>(ctx, 0xF, false, ctx->st2);
+        if(!rc2 && ip->chemistry)
+            rc2 = ctx->mixed ? run_chem<float>(ctx, &ip->chem, ATURAN_CHEM_NH4SH_EQ, ctx->st2)
+                             : run_chem<double>(ctx, &ip->chem, ATURAN_CHEM_NH4SH_EQ, ctx->st2);
+        if(!rc2 && ip->precipitation)
+            rc2 = ctx->mixed ? run_precip<float>(ctx, &ip->precip, ctx->st2) : run_precip<double>(ctx, &ip->precip, ctx->st2);
+        if(!rc2) rc2 = sync_ncopies(ctx, ctx->st2);
+        if(!rc2 && ip->chemistry)
+            rc2 = ctx->mixed ? run_chem<float>(ctx, &ip->chem, ATURAN_CHEM_FORCING, ctx->st2)
+                             : run_chem<double>(ctx, &ip->chem, ATURAN_CHEM_FORCING, ctx->st2);
+        if(!rc2) rc2 = ctx->mixed ? rk4_prelude<float>(ctx, ctx->st2) : rk4_prelude<double>(ctx, ctx->st2);
+        CK(cudaEventRecord(ctx->ev_join, ctx->st2));
+        rc = rc2 ? rc2 : aturan_pressure(ctx, ip->press_kind, ip->omega, ip->max_sweeps, ip->tol, nullptr, nullptr);
+        if(rc >= 0 && !rc2){
+            // cUranusModel.cpp:974-986, the p_dyn filter (FP64 in both precisions)
+            Region reg(ctx, ATURAN_K_POST, 0);
+            const int per = ip->post.phi_periodic;
+            if(ip->damp_p_horiz == 1.0) reg.n += launch_filter_f64(ctx->g, ctx->pdyn, true, true, true, 1.0, per, ctx->st);
+            else {
+                if(ip->damp_p_horiz != 0.0) reg.n += launch_filter_f64(ctx->g, ctx->pdyn, false, true, true, ip->damp_p_horiz, per, ctx->st);
+                reg.n += launch_filter_f64(ctx->g, ctx->pdyn, true, false, false, 1.0, per, ctx->st);
+            }
+            CK_LAUNCH("p_dyn filter");
+        }
+        CK(cudaStreamWaitEvent(ctx->st, ctx->ev_join, 0));
+        if(rc < 0 || rc2) return rc < 0 ? rc : rc2;
+        rc2 = ctx->mixed ? run_rk4<float, float>(ctx, ctx->k32, true) : run_rk4<double, double>(ctx, ctx->k64, true);
+        if(rc2) return rc2;
+    } else {
+        rc = aturan_rk4_step(ctx);
+        if(rc) return rc;
+    }
+    int r = ctx->mixed ? run_post<float>(ctx, &ip->post, nullptr, nullptr) : run_post<double>(ctx, &ip->post, nullptr, nullptr);
+    if(r) return r;
+    r = aturan_restore_ncopies(ctx, 1.0);                      // cUranusModel.cpp:1264
+    if(r) return r;
+    if(ip->turbulence){
+        r = ctx->mixed ? run_turb<float>(ctx, &ip->turb) : run_turb<double>(ctx, &ip->turb);
+        if(r) return r;
+    }
+    if(mca){
+        r = aturan_mca(ctx);
+        if(r) return r;
+    }
+    return rc;
 }
 
 int aturan_turb_params_default(aturan_turb_params* tp){

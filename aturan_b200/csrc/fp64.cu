@@ -29,6 +29,10 @@ void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st){
     mca_kernel<<<dim3((a.g.km + 63) / 64, a.g.jm), 64, 0, st>>>(a);
 }
 
+int launch_filter_f64(const Grid& g, double* x, bool ai, bool aj, bool ak, double strength, int phi_periodic, cudaStream_t st){
+    return launch_filter<double>(g, x, nullptr, ai, aj, ak, strength, phi_periodic, st);
+}
+
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st){
     pdyn_bc_r_kernel<<<dim3((g.km + 127) / 128, g.jm), 128, 0, st>>>(g, P);
     pdyn_bc_t_kernel<<<dim3((g.km + 127) / 128, g.im), 128, 0, st>>>(g, P);

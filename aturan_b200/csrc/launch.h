@@ -43,6 +43,8 @@ void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st);
 
 // FP64-only kernels (p_dyn is FP64 in both precisions).
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st);
+// damp_wiggles on an FP64 field (p_dyn) in either precision; returns the launches.
+int launch_filter_f64(const Grid& g, double* x, bool ai, bool aj, bool ak, double strength, int phi_periodic, cudaStream_t st);
 void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff, cudaStream_t st);
 void launch_scale_copy_f32(const float* in, float* out, size_t n, double coeff, cudaStream_t st);
 void launch_rb_colour(Grid g, double* P, const double* src, const RBW* w, int colour, double omega, cudaStream_t st);

@@ -288,3 +288,35 @@ def precip_params_from_ref(ref):
     pp.h2s = int(ref.precip_scalar("h2s"))
     pp.rate_scale = ref.precip_scalar("rate_scale")
     return pp
+
+
+class IterParams(ctypes.Structure):
+    """aturan_iter_params: one iteration of the model's loop (cUranusModel.cpp:952-1296)."""
+    _fields_ = ([(n, ctypes.c_int32) for n in (
+        "abi_version", "press_kind", "max_sweeps", "chemistry", "precipitation", "turbulence", "mca_stride")]
+        + [("reserved_i", ctypes.c_int32 * 5)]
+        + [(n, ctypes.c_double) for n in ("omega", "tol", "damp_p_horiz")]
+        + [("reserved_d", ctypes.c_double * 5)]
+        + [("post", PostParams), ("chem", ChemParams), ("turb", TurbParams), ("precip", PrecipParams)])
+
+
+def default_iter_params(geo_balance=True):
+    """The reference's loop with its ATURAN_* knobs unset: PressureSolverUran's sweep, the radial
+    p_dyn filter only (DAMP_P_HORIZ 0 with GEO_BALANCE, cUranusModel.cpp:979-980), chemistry,
+    precipitation, turbulence and the MCA every iteration on."""
+    ip = IterParams()
+    ip.abi_version = ABI_VERSION
+    ip.press_kind = PRESS_GS_LEX
+    ip.max_sweeps = 1
+    ip.chemistry = 1
+    ip.precipitation = 1
+    ip.turbulence = 1
+    ip.mca_stride = 1
+    ip.omega = 1.0
+    ip.tol = 0.0
+    ip.damp_p_horiz = 0.0 if geo_balance else 1.0
+    ip.post = default_post_params(geo_balance)
+    ip.chem = default_chem_params()
+    ip.turb = default_turb_params()
+    ip.precip = default_precip_params()
+    return ip

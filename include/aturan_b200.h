@@ -440,6 +440,41 @@ int aturan_precip_params_default(aturan_precip_params* pp);
  * settling flux and the surface maps) are the reference's diagnostics and are not kept. */
 int aturan_precipitation(aturan_ctx* ctx, const aturan_precip_params* pp);
 
+/* One iteration of the model's loop (cUranusModel.cpp:952-1296) with the reference's default
+ * knobs, all on the device. Even iter_n (the loop's `iter_n % 2 == 0` branch): the pressure solve,
+ * the p_dyn filter (:975-984), the four saturation adjustments, the NH4SH equilibrium, the
+ * precipitation, the n-copy sync, the chemistry forcing; every iteration: the RK4 step, the passes
+ * after it (aturan_post_step), restoreVar(1.0), the turbulence closure, the moist convective
+ * adjustment every mca_stride-th iteration. The diagnostics of the loop (forces, latent heat,
+ * radiation with its default RAD_COUPLING 0, the budgets and reports) change no field the step
+ * reads and are not run. */
+typedef struct aturan_iter_params {
+    int32_t abi_version;         /* = ATURAN_ABI_VERSION */
+    int32_t press_kind;          /* enum aturan_pressure_kind; GS_LEX = PressureSolverUran (the default) */
+    int32_t max_sweeps;          /* as aturan_pressure */
+    int32_t chemistry;           /* 1 (default): aturan_chemistry's two parts on even iterations */
+    int32_t precipitation;       /* ATURAN_PRECIP (cUranusModel.cpp:105-108): 1 (default) */
+    int32_t turbulence;          /* turb_active (cUranusModel.cpp:482): 1 (default) */
+    int32_t mca_stride;          /* ATURAN_MCA (cUranusModel.cpp:131-134): 1 (default); 0 = off */
+    int32_t reserved_i[5];
+    double omega, tol;           /* as aturan_pressure (RB_SOR / RB_LINE) */
+    double damp_p_horiz;         /* ATURAN_DAMP_P_HORIZ (:979-980): 0 (default with GEO_BALANCE) = the radial
+                                    pass of the p_dyn filter only; 1 = all three axes; else horizontal
+                                    passes of that strength, then the radial one */
+    double reserved_d[5];
+    aturan_post_params post;
+    aturan_chem_params chem;
+    aturan_turb_params turb;
+    aturan_precip_params precip;
+} aturan_iter_params;
+
+/* Fill the reference's defaults. */
+int aturan_iter_params_default(aturan_iter_params* ip);
+
+/* One iteration number iter_n (1-based, as the reference counts) of the loop above. Parts whose
+ * knob values are not implemented return ATURAN_E_UNSUPPORTED before any launch. */
+int aturan_iteration(aturan_ctx* ctx, const aturan_iter_params* ip, int iter_n);
+
 /* Kernel classes for the per-class launch counts and timings below. */
 enum aturan_kernel_kind {
     ATURAN_K_RK_STAGE = 0,   /* fused RHS + RK4 stage update */

@@ -88,6 +88,7 @@ class Oracle:
             ("oracle_chem_forcing", [P, P, vp], ctypes.c_int),
             ("oracle_turbulence", [P, P, vp], ctypes.c_int),
             ("oracle_precipitation", [P, P, vp], ctypes.c_int),
+            ("oracle_iteration", [P, P, vp, ctypes.c_int], ctypes.c_int),
         ):
             f = getattr(L, fn)
             f.argtypes = args
@@ -219,3 +220,7 @@ class Oracle:
     def precipitation(self, p, pp, state):
         """Precipitation<cUranusModel>::run (H2O, NH3, CH4, H2S) on the state in place."""
         assert self.L.oracle_precipitation(self._p(p), self._p(pp), field_ptrs(state)) == 0
+
+    def iteration(self, p, ip, state, iter_n):
+        """One iteration (number iter_n, from 1) of the model's loop on the state in place."""
+        assert self.L.oracle_iteration(self._p(p), self._p(ip), field_ptrs(state), int(iter_n)) == 0

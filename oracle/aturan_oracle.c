@@ -2552,3 +2552,47 @@ int oracle_precipitation(const aturan_params* p, const aturan_precip_params* pp,
                       ATURAN_S_PRECIP_H2S, ATURAN_S_PRECIP_H2S_CLOUD, ATURAN_S_PRECIP_H2S_ICE);
     return 0;
 }
+
+/* ---- one iteration of cUranusModel::Run's loop (cUranusModel.cpp:952-1296) with the default
+ * knobs, composed of the functions above in the loop's order ---- */
+int oracle_iteration(const aturan_params* p, const aturan_iter_params* ip, double* const* f, int iter_n){
+    const size_t N = (size_t)p->im * p->jm * p->km;
+    if(iter_n % 2 == 0){
+        /* :967-973 */
+        if(ip->press_kind == ATURAN_PRESS_GS_LEX) oracle_pressure_gs(p, f);
+        else if(ip->press_kind == ATURAN_PRESS_RB_SHARED) oracle_pressure_rb(p, f, ip->max_sweeps);
+        else if(ip->press_kind == ATURAN_PRESS_RB_LINE){ int s; double r; oracle_pressure_line(p, f, ip->omega, ip->max_sweeps, ip->tol, &s, &r); }
+        else { int s; double r; oracle_pressure_sor(p, f, ip->omega, ip->max_sweeps, ip->tol, 16, &s, &r); }
+        /* :975-984, the p_dyn filter */
+        double* tmp = (double*)malloc(sizeof(double) * N);
+        if(!tmp) return -1;
+        const int per = ip->post.phi_periodic;
+        if(ip->damp_p_horiz == 1.0) post_damp(p, f[ATURAN_P_DYN], 1, 1, 1, 1.0, per, tmp);
+        else {
+            if(ip->damp_p_horiz != 0.0) post_damp(p, f[ATURAN_P_DYN], 0, 1, 1, ip->damp_p_horiz, per, tmp);
+            post_damp(p, f[ATURAN_P_DYN], 1, 0, 0, 1.0, per, tmp);
+        }
+        free(tmp);
+        /* :997-1030, H2O, H2S, NH3, CH4 */
+        for(int g = 0; g < 4; g++) oracle_satadj(p, f, g, NULL, NULL);
+        /* :1034, :1037 */
+        if(ip->chemistry) oracle_nh4sh_eq(p, &ip->chem, f, NULL);
+        if(ip->precipitation) oracle_precipitation(p, &ip->precip, f);
+        /* :1049-1073 */
+        oracle_sync_ncopies(p, f);
+        /* :1074-1087 */
+        if(ip->chemistry) oracle_chem_forcing(p, &ip->chem, f);
+    }
+    /* :1123 */
+    double ref[1024];
+    if(p->im > 1024) return -1;
+    oracle_rk4(p, f, ref);
+    /* :1199-1248 */
+    oracle_post_step(p, f, &ip->post, NULL, NULL);
+    /* :1264, restoreVar(1.0) */
+    for(int q = 0; q < ATURAN_NPROG; q++) memcpy(f[ATURAN_TN + q], f[q], sizeof(double) * N);
+    /* :1270-1296 */
+    if(ip->turbulence) oracle_turbulence(p, &ip->turb, f);
+    if(ip->mca_stride > 0 && iter_n % ip->mca_stride == 0) oracle_mca(p, f);
+    return 0;
+}

@@ -60,6 +60,8 @@ int oracle_chem_forcing(const aturan_params* p, const aturan_chem_params* cp, do
 int oracle_turbulence(const aturan_params* p, const aturan_turb_params* tp, double* const* f);
 /* Precipitation.h:192-446 for H2O, NH3, CH4, H2S (cUranusModel.h:280-297) */
 int oracle_precipitation(const aturan_params* p, const aturan_precip_params* pp, double* const* f);
+/* cUranusModel.cpp:952-1296, one iteration (iter_n counted from 1) with the default knobs */
+int oracle_iteration(const aturan_params* p, const aturan_iter_params* ip, double* const* f, int iter_n);
 
 #ifdef __cplusplus
 }

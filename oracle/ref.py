@@ -49,7 +49,7 @@ _SINGLETON = None
 class Ref:
     """The reference model, initialised once per process (Run() with nm = 0)."""
 
-    def __init__(self, outdir="/tmp/aturan_ref_out", quiet=True):
+    def __init__(self, outdir="/tmp/aturan_ref_out", quiet=True, loop_iterations=0):
         path = lib_path()
         if path is None:
             raise RuntimeError("compiled reference not found under oracle/_ref")
@@ -83,7 +83,12 @@ class Ref:
         L.ref_dims(ctypes.byref(im), ctypes.byref(jm), ctypes.byref(km))
         self.shape = (im.value, jm.value, km.value)
         os.makedirs(outdir, exist_ok=True)
-        assert L.ref_create(outdir.encode()) == 0
+        if loop_iterations > 0:
+            # Run() with that many iterations of the model's own loop after its initialisation
+            L.ref_create_loop.argtypes = [ctypes.c_char_p, ctypes.c_int]
+            assert L.ref_create_loop(outdir.encode(), int(loop_iterations)) == 0
+        else:
+            assert L.ref_create(outdir.encode()) == 0
 
     @classmethod
     def get_instance(cls):

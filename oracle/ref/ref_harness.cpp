@@ -156,6 +156,20 @@ int ref_create(const char* outdir){
     return 0;
 }
 
+// The same, then nm iterations of the model's own loop (planet/cUranusModel.cpp:952-1396) inside
+// Run(); checkpoint is set past nm so that the loop writes no files and prints no reports.
+int ref_create_loop(const char* outdir, int nm){
+    if(g_model) return -1;
+    Quiet q_;
+    g_model = new cUranusModel();
+    g_model->nm = nm;
+    g_model->checkpoint = nm + 1000000;
+    g_model->paraview_flag = false;
+    g_model->output_path = std::string(outdir ? outdir : "/tmp/aturan_ref_out") + "/";
+    g_model->Run();
+    return 0;
+}
+
 int ref_get(const char* name, double* out){
     Array* a = field(name);
     if(!a || !a->x) return -1;

@@ -106,6 +106,22 @@ def test_precip_params_layout_and_defaults(tmp_path):
     assert bytes(api.library_default_precip_params()) == bytes(P.default_precip_params())
 
 
+def test_iter_params_layout_and_defaults(tmp_path):
+    """aturan_iter_params: the header's layout (nested structs included), and the library's defaults
+    equal the Python mirror's."""
+    src = tmp_path / "ip.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "aturan_b200.h"\n'
+                   'int main(void){ printf("%zu %zu %zu %zu\\n", sizeof(aturan_iter_params),'
+                   ' offsetof(aturan_iter_params, omega), offsetof(aturan_iter_params, chem),'
+                   ' offsetof(aturan_iter_params, precip)); return 0; }\n')
+    exe = tmp_path / "ip"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, off_o, off_c, off_p = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == ctypes.sizeof(P.IterParams)
+    assert (off_o, off_c, off_p) == (P.IterParams.omega.offset, P.IterParams.chem.offset, P.IterParams.precip.offset)
+    assert bytes(api.library_default_iter_params()) == bytes(P.default_iter_params())
+
+
 def test_no_cpu_fallback_without_gpu():
     import torch
     if torch.cuda.is_available():

@@ -113,18 +113,27 @@ def test_chemistry_both_parts_in_order(oracle_lib):
         assert d <= 1e-10, (n, d)
 
 
-def test_chemistry_mixed_matches_oracle(oracle_lib):
+@pytest.mark.parametrize("what", [EQ, FORCING])
+def test_chemistry_mixed_matches_oracle(oracle_lib, what):
+    """Each part alone on the same FP32-rounded inputs as the oracle. (Run back to back, the
+    equilibrium's FP32-rounded NH4SH would feed the Superbee limiter, whose ratio of neighbour
+    differences is ill-conditioned where NH4SH is nearly uniform: its output differs there by a few
+    per cent of its maximum between an FP32 and an FP64 NH4SH, a property of the limiter, not of
+    the arithmetic.)"""
     p32 = P.default_params(precision=P.MIXED)
     p, cp = P.default_params(), P.default_chem_params()
     st = chem_state(S.synthetic_state(p, seed=69), p, seed=70)
-    g, (gf, gd) = run_gpu(p32, st, EQ | FORCING, cp, EQ_OUT + FORCING_OUT)
+    names = EQ_OUT if what == EQ else FORCING_OUT
+    g, (gf, gd) = run_gpu(p32, st, what, cp, names)
     s = rounded32(st)
-    of, od = oracle_lib.nh4sh_eq(p, cp, s)
-    oracle_lib.chem_forcing(p, cp, s)
-    for n in EQ_OUT + FORCING_OUT:
+    if what == EQ:
+        of, od = oracle_lib.nh4sh_eq(p, cp, s)
+        assert abs(gf - of) <= of // 100 and abs(gd - od) <= od // 100, (gf, of, gd, od)
+    else:
+        oracle_lib.chem_forcing(p, cp, s)
+    for n in names:
         d = np.abs(g[n] - s[n]).max() / np.abs(s[n]).max()
         assert d <= 1e-5, (n, d)
-    assert abs(gf - of) <= of // 100 and abs(gd - od) <= od // 100, (gf, of, gd, od)
 
 
 def test_chemistry_rejects_unsupported_knobs():

@@ -267,3 +267,27 @@ def test_physics_knob_sets(knobs):
     child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_physics_knobs_child.py")
     r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def test_reference_loop(ref_model, oracle_lib, base_state, tmp_path):
+    """The reference's own loop: Run() with 4 iterations after its initialisation (in a child
+    process, a fresh model) against the oracle's iteration applied 4 times to the initialised state
+    (iterations 1 and 3 odd: RK4 onward; 2 and 4 even: the full sequence). Every field the loop
+    carries is identical, which pins the iteration's composition and order as well as its parts."""
+    import os
+    import subprocess
+    import sys
+    p, ip = P.default_params(), P.default_iter_params()
+    n = 4
+    out = tmp_path / "loop.npz"
+    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_loop_child.py")
+    r = subprocess.run([sys.executable, child, str(n), str(out)], capture_output=True, text=True, timeout=1800)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+    got = dict(np.load(out))
+    st = {k: np.array(v, copy=True) for k, v in base_state.items()}
+    for it in range(1, n + 1):
+        oracle_lib.iteration(p, ip, st, it)
+    names = [m for m in F.NAMES if m not in F.PROJECTION]
+    bad = {m: int(np.count_nonzero(got[m] != st[m])) for m in names if not np.array_equal(got[m], st[m])}
+    assert not bad, bad
+    assert not np.array_equal(got["t"], base_state["t"])
