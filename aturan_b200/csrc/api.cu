@@ -91,6 +91,7 @@ struct aturan_ctx {
     double* ahacc;             // the T tendencies' adjoint summed over the stages (heating gradient)
     double* heat;              // aturan_set_heating: [jm][km] K/s, or null
     double* mca_H;             // aturan_mca: the cp table's running integral, made at the first call
+    bool mca_H_ready;          // mca_H holds the integral (its kernel has launched)
     double* chem_tab;          // aturan_chemistry: radius, metric radius (im), sin, cos of the colatitude (jm)
     double* dz_tab;            // aturan_precipitation: layer thickness [m] per level (the float layer heights)
     // host-side constants
@@ -860,6 +861,54 @@ int run_precip(aturan_ctx* ctx, const aturan_precip_params* pp, cudaStream_t st 
     Region reg(ctx, ATURAN_K_PRECIP, 0, st);
     reg.n = launch_precip(a, st);
     CK_LAUNCH("precipitation");
+    return ATURAN_OK;
+}
+
+// The moist convective adjustment on the context's fields (aturan_mca).
+template <typename S>
+int run_mca(aturan_ctx* ctx){
+    const Grid& g = ctx->g;
+    const aturan_params& p = ctx->p;
+    if(mca_warp_bytes(g.im) > MCA_SMEM_MAX) return fail(ctx, ATURAN_E_UNSUPPORTED, "column too deep for the shared memory");
+    int nl = 0;
+    if(!ctx->mca_H_ready){
+        // the cp table's running integral, formed once; ready only once its kernel has launched
+        if(!ctx->mca_H && cudaMalloc((void**)&ctx->mca_H, CP_TABLE_N * sizeof(double)) != cudaSuccess){
+            cudaGetLastError(); ctx->mca_H = nullptr; return fail(ctx, ATURAN_E_NOMEM, "mca: cp integral");
+        }
+        launch_mca_H(ctx->cp_tab64, ctx->mca_H, ctx->st);
+        CK_LAUNCH("moist convective adjustment: cp integral");
+        ctx->mca_H_ready = true;
+        nl++;
+    }
+    McaArgs<S> a;
+    a.g = g;
+    McaConst& c = a.c;
+    const int order[MCA_NG] = { 0, 2, 1, 3 };                  // H2O, NH3, H2S, CH4 from the params' H2O, H2S, NH3, CH4
+    const int fv[MCA_NG] = { ATURAN_H2O, ATURAN_NH3, ATURAN_H2S, ATURAN_CH4 };
+    S* X = reinterpret_cast<S*>(ctx->state);
+    const size_t fs = g.fstride;
+    for(int n = 0; n < MCA_NG; n++){
+        const aturan_gas& s = p.gas[order[n]];
+        c.G[n] = McaGas{ s.ep, s.lv, s.ls, s.t_0, s.C, s.L0, s.R, s.del_alf, s.del_bet, s.C_i, s.L0_i, s.del_alf_i, s.del_bet_i };
+        for(int q = 0; q < 3; q++) a.sp[n][q] = X + (size_t)(fv[n] + q) * fs;
+    }
+    c.L_tr = p.nh4sh_sync ? 4705.0 * std::log(10.0) * 8314.46 / 51.1114 : 0.0;   // ChemistryUran.h:132
+    c.t_ref = p.t_ref; c.grav = p.g; c.cp_mix = p.cp_mix; c.r_mix = p.r_mix; c.cp_h2 = p.cp_h2;
+    c.r_h2 = p.r_h2; c.r_he = p.r_he; c.r_ch4 = p.r_ch4; c.cp_he = p.cp_he; c.cp_ch4 = p.cp_ch4;
+    c.hz = (float)(p.L_atm / (g.im - 1));                      // cUranusModel.h:1205-1208
+    c.cp_dyn = p.cp_dyn; c.cp_mode = p.cp_h2_mode; c.cp_gas = p.cp_gas; c.local_rho = p.local_rho;
+    c.cp_tab = ctx->cp_tab64; c.H_tab = ctx->mca_H;
+    a.t = X + (size_t)ATURAN_T * fs;
+    a.tlo = ctx->tlo;
+    a.nh4sh = X + (size_t)ATURAN_NH4SH * fs;
+    a.ps = reinterpret_cast<const S*>(ctx->pstat);
+    a.rho = reinterpret_cast<const S*>(ctx->forc) + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs;
+    Region reg(ctx, ATURAN_K_MCA, 0);
+    const int n = launch_mca(a, ctx->st);
+    if(n < 0) return fail(ctx, ATURAN_E_UNSUPPORTED, "mca: the column's shared memory");
+    reg.n = nl + n;
+    CK_LAUNCH("moist convective adjustment");
     return ATURAN_OK;
 }
 
@@ -1825,38 +1874,7 @@ int aturan_post_params_default(aturan_post_params* pp){
 
 int aturan_mca(aturan_ctx* ctx){
     if(!ctx) return ATURAN_E_INVALID;
-    const Grid& g = ctx->g;
-    if(ctx->mixed || g.im > MCA_MAXI) return ATURAN_E_UNSUPPORTED;
-    const aturan_params& p = ctx->p;
-    const bool first = ctx->mca_H == nullptr;
-    if(first && cudaMalloc((void**)&ctx->mca_H, CP_TABLE_N * sizeof(double)) != cudaSuccess){
-        cudaGetLastError(); ctx->mca_H = nullptr; return ATURAN_E_NOMEM;
-    }
-    McaArgs a;
-    a.g = g;
-    const int order[MCA_NG] = { 0, 2, 1, 3 };                  // H2O, NH3, H2S, CH4 from the params' H2O, H2S, NH3, CH4
-    const int fv[MCA_NG] = { ATURAN_H2O, ATURAN_NH3, ATURAN_H2S, ATURAN_CH4 };
-    double* X = reinterpret_cast<double*>(ctx->state);
-    const size_t fs = g.fstride;
-    for(int n = 0; n < MCA_NG; n++){
-        const aturan_gas& s = p.gas[order[n]];
-        a.G[n] = McaGas{ s.ep, s.lv, s.ls, s.t_0, s.C, s.L0, s.R, s.del_alf, s.del_bet, s.C_i, s.L0_i, s.del_alf_i, s.del_bet_i };
-        for(int c = 0; c < 3; c++) a.sp[n][c] = X + (size_t)(fv[n] + c) * fs;
-    }
-    a.L_tr = p.nh4sh_sync ? 4705.0 * std::log(10.0) * 8314.46 / 51.1114 : 0.0;   // ChemistryUran.h:132
-    a.t_ref = p.t_ref; a.grav = p.g; a.cp_mix = p.cp_mix; a.r_mix = p.r_mix; a.cp_h2 = p.cp_h2;
-    a.r_h2 = p.r_h2; a.r_he = p.r_he; a.r_ch4 = p.r_ch4; a.cp_he = p.cp_he; a.cp_ch4 = p.cp_ch4;
-    a.hz = (float)(p.L_atm / (g.im - 1));                      // cUranusModel.h:1205-1208
-    a.cp_dyn = p.cp_dyn; a.cp_mode = p.cp_h2_mode; a.cp_gas = p.cp_gas; a.local_rho = p.local_rho;
-    a.cp_tab = ctx->cp_tab64; a.H_tab = ctx->mca_H;
-    a.t = X + (size_t)ATURAN_T * fs;
-    a.nh4sh = X + (size_t)ATURAN_NH4SH * fs;
-    a.ps = reinterpret_cast<const double*>(ctx->pstat);
-    a.rho = reinterpret_cast<const double*>(ctx->forc) + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs;
-    Region reg(ctx, ATURAN_K_MCA, first ? 2 : 1);
-    launch_mca(a, ctx->mca_H, first, ctx->st);
-    CK_LAUNCH("moist convective adjustment");
-    return ATURAN_OK;
+    return ctx->mixed ? run_mca<float>(ctx) : run_mca<double>(ctx);
 }
 
 int aturan_chem_params_default(aturan_chem_params* cp){
@@ -1925,8 +1943,8 @@ int aturan_iteration(aturan_ctx* ctx, const aturan_iter_params* ip, int iter_n){
                           ip->turb.buoy != 0 || ip->turb.abl_taper != 0))
         return fail(ctx, ATURAN_E_UNSUPPORTED, "turbulence: only the default knobs are implemented");
     const bool mca = ip->mca_stride > 0 && iter_n % ip->mca_stride == 0;
-    if(ip->mca_stride > 0 && (ctx->mixed || ctx->g.im > MCA_MAXI))
-        return fail(ctx, ATURAN_E_UNSUPPORTED, "moist convective adjustment: FP64 contexts with im <= 64 only");
+    if(ip->mca_stride > 0 && mca_warp_bytes(ctx->g.im) > MCA_SMEM_MAX)
+        return fail(ctx, ATURAN_E_UNSUPPORTED, "moist convective adjustment: column too deep for the shared memory");
     int rc;
     if(iter_n % 2 == 0){
         // the saturation adjustment and what follows it up to the chemistry forcing touch no field

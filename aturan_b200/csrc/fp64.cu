@@ -24,9 +24,8 @@ void launch_scale_copy_f64(const double* in, double* out, size_t n, double coeff
     scale_copy_f64_kernel<<<148 * 8, 256, 0, st>>>(in, out, n, coeff);
 }
 
-void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st){
-    if(build_H) mca_H_kernel<<<1, 32, 0, st>>>(a.cp_tab, H);
-    mca_kernel<<<dim3((a.g.km + 63) / 64, a.g.jm), 64, 0, st>>>(a);
+void launch_mca_H(const double* cp_tab, double* H, cudaStream_t st){
+    mca_H_kernel<<<1, 32, 0, st>>>(cp_tab, H);
 }
 
 int launch_filter_f64(const Grid& g, double* x, bool ai, bool aj, bool ak, double strength, int phi_periodic, cudaStream_t st){

@@ -12,6 +12,7 @@ template <typename S> struct PostArgs;
 template <typename S> struct ChemArgs;
 template <typename S> struct TurbArgs;
 template <typename S> struct PrecipArgs;
+template <typename S> struct McaArgs;
 struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
@@ -31,15 +32,15 @@ void launch_rb_prep(Grid g, S* au, S* av, S* aw, S* ru, S* rv, S* rw, int rigid_
 int launch_post(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st);               \
 int launch_chem(const ChemArgs<S>& a, int what, cudaStream_t st);                                         \
 int launch_turb(const TurbArgs<S>& a, cudaStream_t st);                                                   \
-int launch_precip(const PrecipArgs<S>& a, cudaStream_t st);
+int launch_precip(const PrecipArgs<S>& a, cudaStream_t st);                                               \
+int launch_mca(const McaArgs<S>& a, cudaStream_t st);
 
 ATURAN_DECLARE_LAUNCHERS(double, double)
 ATURAN_DECLARE_LAUNCHERS(float, float)
 #undef ATURAN_DECLARE_LAUNCHERS
 
-// The moist convective adjustment (FP64 contexts); build_H first forms the cp table's integral in H.
-struct McaArgs;
-void launch_mca(const McaArgs& a, double* H, bool build_H, cudaStream_t st);
+// The moist convective adjustment's cp-table integral (CpH2.h:66-75), formed once per context.
+void launch_mca_H(const double* cp_tab, double* H, cudaStream_t st);
 
 // FP64-only kernels (p_dyn is FP64 in both precisions).
 void launch_pdyn_bcs(Grid g, double* P, cudaStream_t st);

@@ -8,6 +8,7 @@
 #include "chem.cuh"
 #include "turb.cuh"
 #include "precip.cuh"
+#include "mca.cuh"
 
 namespace aturan {
 // Stage launch configuration per storage type, measured on B200 at 41x181x361: resident blocks per
@@ -147,6 +148,25 @@ int launch_precip_impl(const PrecipArgs<S>& a, cudaStream_t st){
     precip_kernel<S><<<dim3((a.g.km + 127) / 128, a.g.jm), 128, 0, st>>>(a);
     return 1;
 }
+// The moist convective adjustment (mca.cuh): one warp per column, W warps per block, W = 4 halved
+// until the block's slices fit the shared memory; returns the launches, or -1 if one column's slice
+// does not fit.
+template <typename S>
+int launch_mca_impl(const McaArgs<S>& a, cudaStream_t st){
+    const size_t per = mca_warp_bytes(a.g.im);
+    int W = 4;
+    while(W > 1 && (size_t)W * per > MCA_SMEM_MAX) W /= 2;
+    if((size_t)W * per > MCA_SMEM_MAX) return -1;
+    const size_t sm = (size_t)W * per;
+    if(sm > 48 * 1024 &&
+       cudaFuncSetAttribute(mca_warp_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess){
+        cudaGetLastError();
+        return -1;
+    }
+    const long cols = (long)a.g.jm * a.g.km;
+    mca_warp_kernel<S><<<(unsigned)((cols + W - 1) / W), dim3(32, W), sm, st>>>(a);
+    return 1;
+}
 // Hydrostatic integral: threads per column (ROWS) and resident blocks per SM (MINB), measured.
 template <typename S> struct HydCfg { static constexpr int ROWS = 8, MINB = 2; };
 template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
@@ -217,4 +237,7 @@ int launch_turb(const TurbArgs<S>& a, cudaStream_t st){                         
 }                                                                                                         \
 int launch_precip(const PrecipArgs<S>& a, cudaStream_t st){                                               \
     return launch_precip_impl<S>(a, st);                                                                  \
+}                                                                                                         \
+int launch_mca(const McaArgs<S>& a, cudaStream_t st){                                                     \
+    return launch_mca_impl<S>(a, st);                                                                     \
 }

@@ -5,37 +5,54 @@
 // list H2O, NH3, H2S (its liquid set for both phases), CH4 and the NH4SH tracer of
 // cUranusModel.cpp:1276-1290.
 //
-// Every (j, k) column is independent: one thread per column, FP64, the column's state (at most
-// MCA_MAXI levels) in the thread's local memory. Every loop is bounded: 60 regula-falsi steps,
-// 30 Newton steps of the enthalpy inverse, 64 sweeps, and a segment grows by one level per step
-// within the column.
+// Every (j, k) column is independent. One warp takes one column and keeps its state in its own
+// slice of shared memory (16 values and 4 flags per level): the lanes load, convert and write back
+// the levels in parallel, and run in parallel everything of a sweep that does not depend on what
+// the sweep has done before it:
+//   * at the start of each sweep every pair test (i, i+1) is evaluated, one pair per lane; while
+//     the sweep walks up the column a pair is re-tested (by lane 0) only if one of its two cells
+//     has been mixed in this sweep, which is exactly when its inputs differ from the start's (the
+//     reference's first sweep makes the same reuse with its cached test of untouched pairs);
+//   * a segment's mass-weighted means are summed by lane 0 in the reference's order, and each of
+//     its cells is then brought to equilibrium by its own lane;
+//   * the two growth tests of a segment (below and above) run on lanes 0 and 1.
+// Each test solves a cell's equilibrium by Illinois regula falsi, so the arithmetic is FP64
+// whatever the storage (FP32 storage in the mixed form is widened, T read as its FP32 pair).
+// Every loop is bounded: 60 regula-falsi steps, 30 Newton steps of the enthalpy inverse, 64
+// sweeps, and a segment grows by one level per step within the column.
 #pragma once
 #include "common.cuh"
 
 namespace aturan {
 
-constexpr int MCA_MAXI = 64, MCA_NG = 4;
+constexpr int MCA_NG = 4;
 constexpr double CP_T_LO_D = 5.0, CP_T_HI_D = 1500.0, CP_DT_D = 0.5;   // CpH2.h:13
 
 struct McaGas { double ep, lv, ls, t_0, C, L0, R, del_alf, del_bet, C_i, L0_i, del_alf_i, del_bet_i; };
 
-struct McaArgs {
-    Grid g;
+struct McaConst {
     McaGas G[MCA_NG];                // H2O, NH3, H2S, CH4
     double L_tr, t_ref, grav, cp_mix, r_mix, cp_h2, r_h2, r_he, r_ch4, cp_he, cp_ch4;
     float hz;                        // level spacing [km] as the model stores it (float)
     int cp_dyn, cp_mode, cp_gas, local_rho;
     const double *cp_tab, *H_tab;    // H2 cp table and its running integral (CpH2.h:66-75)
-    double* t;
-    double* sp[MCA_NG][3];           // vapour, cloud, ice
-    double* nh4sh;
-    const double *ps, *rho;
+};
+
+template <typename S>
+struct McaArgs {
+    Grid g;
+    McaConst c;
+    S* t;
+    float* tlo;                      // the mixed form's temperature pair (common.cuh), else null
+    S* sp[MCA_NG][3];                // vapour, cloud, ice
+    S* nh4sh;
+    const S *ps, *rho;
 };
 
 __device__ __forceinline__ double mca_mx(double a, double b){ return (a < b) ? b : a; }   // std::max
 
 // CpH2.h:88-101, 122-157
-static __device__ double mca_cp_h2(const McaArgs& A, double T){
+static __device__ double mca_cp_h2(const McaConst& A, double T){
     if(A.cp_mode <= 0) return A.cp_h2;
     const double Tc = T < CP_T_LO_D ? CP_T_LO_D : T;
     const double x = ((Tc > CP_T_HI_D ? CP_T_HI_D : Tc) - CP_T_LO_D) / CP_DT_D;
@@ -43,7 +60,7 @@ static __device__ double mca_cp_h2(const McaArgs& A, double T){
     const double f = x - i;
     return A.cp_tab[i] + f * (A.cp_tab[i + 1] - A.cp_tab[i]);
 }
-static __device__ double mca_enth_h2(const McaArgs& A, double T){
+static __device__ double mca_enth_h2(const McaConst& A, double T){
     if(A.cp_mode <= 0) return A.cp_h2 * T;
     const int n = CP_TABLE_N;
     if(T <= CP_T_LO_D) return A.cp_tab[0] * T;
@@ -53,19 +70,19 @@ static __device__ double mca_enth_h2(const McaArgs& A, double T){
     const double f = x - i;
     return A.H_tab[i] + CP_DT_D * f * (A.cp_tab[i] + 0.5 * f * (A.cp_tab[i + 1] - A.cp_tab[i]));
 }
-static __device__ double mca_cp(const McaArgs& A, double T){
+static __device__ double mca_cp(const McaConst& A, double T){
     if(!A.cp_dyn) return A.cp_mix;
     const double ch = mca_cp_h2(A, T);
     if(A.cp_gas) return (A.r_h2 * ch + A.r_he * A.cp_he + A.r_ch4 * A.cp_ch4) / (A.r_h2 + A.r_he + A.r_ch4);
     return A.cp_mix + (A.r_h2 / A.r_mix) * (ch - A.cp_h2);
 }
-static __device__ double mca_enth(const McaArgs& A, double T){
+static __device__ double mca_enth(const McaConst& A, double T){
     if(!A.cp_dyn) return A.cp_mix * T;
     const double hh = mca_enth_h2(A, T);
     if(A.cp_gas) return (A.r_h2 * hh + (A.r_he * A.cp_he + A.r_ch4 * A.cp_ch4) * T) / (A.r_h2 + A.r_he + A.r_ch4);
     return (A.cp_mix - (A.r_h2 / A.r_mix) * A.cp_h2) * T + (A.r_h2 / A.r_mix) * hh;
 }
-static __device__ double mca_enth_inv(const McaArgs& A, double h, double T0){
+static __device__ double mca_enth_inv(const McaConst& A, double h, double T0){
     if(!A.cp_dyn) return h / A.cp_mix;
     double T = (T0 > 0.0) ? T0 : h / A.cp_mix;
     for(int it = 0; it < 30; it++){
@@ -86,14 +103,14 @@ __device__ __forceinline__ double mca_qsat(const McaGas& s, double T, double pr)
 }
 __device__ __forceinline__ double mca_lat(const McaGas& s, double T){ return T >= s.t_0 ? s.lv : s.ls; }
 
-static __device__ double mca_fof(const McaArgs& A, double TT, double hL, const double* qt, double pr, double z){
+static __device__ double mca_fof(const McaConst& A, double TT, double hL, const double* qt, double pr, double z){
     double f = mca_enth(A, TT) + A.grav * z - hL;
     for(int g = 0; g < MCA_NG; g++) f -= mca_lat(A.G[g], TT) * mca_mx(0.0, qt[g] - mca_qsat(A.G[g], TT, pr));
     return f;
 }
 
 // :455-488, the equilibrium of (hL, qt) at (p, z): Illinois regula falsi on the energy balance
-static __device__ bool mca_equil(const McaArgs& A, double hL, const double* qt, double pr, double z, double& T, double* cond){
+static __device__ bool mca_equil(const McaConst& A, double hL, const double* qt, double pr, double z, double& T, double* cond){
     const double cp = A.cp_mix, tol_T = 1.0e-10;
     const double T_lo = A.cp_dyn ? mca_enth_inv(A, hL - A.grav * z, 0.0) : (hL - A.grav * z) / cp;
     if(!(T_lo > 0.0) || !(pr > 0.0)) return false;
@@ -118,80 +135,99 @@ static __device__ bool mca_equil(const McaArgs& A, double hL, const double* qt, 
     return true;
 }
 
-// One column's state (levels i0..i1 used).
+// One column's state in its warp's slice of shared memory (levels 0..im-1, i0..i1 used).
 struct McaCol {
-    double T[MCA_MAXI], p[MCA_MAXI], z[MCA_MAXI], rho[MCA_MAXI], w[MCA_MAXI], hL[MCA_MAXI], qr[MCA_MAXI], Teq[MCA_MAXI];
-    double qt[MCA_MAXI * MCA_NG], qv[MCA_MAXI * MCA_NG], qc[MCA_MAXI * MCA_NG], qi[MCA_MAXI * MCA_NG], ceq[MCA_MAXI * MCA_NG];
-    bool touched[MCA_MAXI], eq_ok[MCA_MAXI], cen_u[MCA_MAXI], cen_m[MCA_MAXI];
+    double *T, *p, *z, *rho, *w, *hL, *qr, *Teq;   // im each
+    double *qt, *ceq;                              // im * MCA_NG each
+    unsigned char *touched, *eq_ok, *mod, *U;      // im each: mixed ever, equilibrium cached,
+                                                   // mixed in this sweep, the pair test of the sweep's start
 };
+// Bytes of one warp's slice for a column of im levels; a block's slices share at most MCA_SMEM_MAX.
+constexpr size_t MCA_SMEM_MAX = 227 * 1024;
+__host__ __device__ inline size_t mca_warp_bytes(int im){
+    return (size_t)(16 * im) * sizeof(double) + (((size_t)4 * im + 7) / 8) * 8;
+}
+__device__ inline McaCol mca_col(char* base, int im){
+    McaCol C;
+    double* d = reinterpret_cast<double*>(base);
+    C.T = d; C.p = d + im; C.z = d + 2 * im; C.rho = d + 3 * im; C.w = d + 4 * im; C.hL = d + 5 * im;
+    C.qr = d + 6 * im; C.Teq = d + 7 * im; C.qt = d + 8 * im; C.ceq = d + 12 * im;
+    unsigned char* f = reinterpret_cast<unsigned char*>(d + 16 * im);
+    C.touched = f; C.eq_ok = f + im; C.mod = f + 2 * im; C.U = f + 3 * im;
+    return C;
+}
 
-__device__ __forceinline__ double mca_trE(const McaArgs& A, const McaCol& C, int i){ double e = 0.0; e += A.L_tr * C.qr[i]; return e; }
+__device__ __forceinline__ double mca_trE(const McaConst& A, const McaCol& C, int i){ double e = 0.0; e += A.L_tr * C.qr[i]; return e; }
 
 // :613-624, Ledoux virtual temperature with condensate loading; NH4SH is a condensed tracer
-static __device__ double mca_tv(const McaArgs& A, const McaCol& C, double TT, const double* v_, const double* cnd, int i_tr){
+static __device__ double mca_tv(const McaConst& A, const McaCol& C, double TT, const double* v_, const double* cnd, int i_tr){
     double f = 1.0;
     for(int g = 0; g < MCA_NG; g++){ f += v_[g] * (1.0 / A.G[g].ep - 1.0); f -= cnd[g]; }
     f -= C.qr[i_tr];
     return TT * f;
 }
 
-// :627-644
-static __device__ bool mca_unstable(const McaArgs& A, McaCol& C, int a, int b, bool* held, bool* moist){
+// :627-644: is the pair (a, b = a+1) unstable? Caches b's equilibrium (written by this lane only:
+// each cell is the upper cell of one pair).
+static __device__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
     const double tol_K = 1.0e-7;
     double Tp, pc[MCA_NG], pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
     if(!mca_equil(A, C.hL[a] + mca_trE(A, C, a), &C.qt[a * MCA_NG], C.p[b], C.z[b], Tp, pc)) return false;
     if(!C.eq_ok[b]){
         if(!mca_equil(A, C.hL[b] + mca_trE(A, C, b), &C.qt[b * MCA_NG], C.p[b], C.z[b], C.Teq[b], &C.ceq[b * MCA_NG])) return false;
-        C.eq_ok[b] = true;
+        C.eq_ok[b] = 1;
     }
     const double Tb = C.Teq[b];
     for(int g = 0; g < MCA_NG; g++) ec[g] = C.ceq[b * MCA_NG + g];
-    bool wet = false;
-    for(int g = 0; g < MCA_NG; g++){ pv[g] = C.qt[a * MCA_NG + g] - pc[g]; if(pc[g] > 0.0) wet = true; ev[g] = C.qt[b * MCA_NG + g] - ec[g]; }
+    for(int g = 0; g < MCA_NG; g++){ pv[g] = C.qt[a * MCA_NG + g] - pc[g]; ev[g] = C.qt[b * MCA_NG + g] - ec[g]; }
     const double dTv = mca_tv(A, C, Tp, pv, pc, a) - mca_tv(A, C, Tb, ev, ec, b);
-    if(held) *held = (Tp - Tb > tol_K) && !(dTv > tol_K);
-    if(moist) *moist = wet;
     return dTv > tol_K;
 }
 
-// :645-661, cell q to equilibrium from hL / qt
-static __device__ bool mca_settle(const McaArgs& A, McaCol& C, int q){
+// :645-661, cell q to equilibrium from hL / qt; the vapour and the condensate's phase split are
+// rebuilt from qt, ceq and T at write-back (qv = qt - ceq; ceq is liquid at T >= t_0, else ice)
+static __device__ bool mca_settle(const McaConst& A, McaCol& C, int q){
     double TT, pc[MCA_NG];
     if(!mca_equil(A, C.hL[q] + mca_trE(A, C, q), &C.qt[q * MCA_NG], C.p[q], C.z[q], TT, pc)) return false;
     C.T[q] = TT;
-    C.Teq[q] = TT; C.eq_ok[q] = true;
-    for(int g = 0; g < MCA_NG; g++){
-        const int x = q * MCA_NG + g;
-        C.ceq[x] = pc[g];
-        C.qv[x] = C.qt[x] - pc[g];
-        if(TT >= A.G[g].t_0){ C.qc[x] = pc[g]; C.qi[x] = 0.0; } else { C.qi[x] = pc[g]; C.qc[x] = 0.0; }
-    }
-    C.touched[q] = true;
+    C.Teq[q] = TT; C.eq_ok[q] = 1;
+    for(int g = 0; g < MCA_NG; g++) C.ceq[q * MCA_NG + g] = pc[g];
+    C.touched[q] = 1;
     return true;
 }
 
-// One thread per (j, k) column, k over all km stored meridians as the reference loops.
-static __global__ void __launch_bounds__(64) mca_kernel(const McaArgs A){
-    const Grid& g = A.g;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
-    if(k >= g.km) return;
+// One warp per (j, k) column (blockDim = (32, W)), k over all km stored meridians as the reference
+// loops; the warp's slice of dynamic shared memory holds the column.
+template <typename S>
+__global__ void __launch_bounds__(128) mca_warp_kernel(McaArgs<S> a){
+    extern __shared__ __align__(16) char mca_smem[];
+    const Grid& g = a.g;
+    const McaConst& A = a.c;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x;
+    const long col = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    if(col >= (long)g.jm * g.km) return;                     // a whole warp
+    const int j = (int)(col / g.km), k = (int)(col % g.km);
     const int im = g.im, i0 = 1, i1 = im - 2;
     if(i1 - i0 < 1) return;
-    McaCol C;
+    McaCol C = mca_col(mca_smem + threadIdx.y * mca_warp_bytes(im), im);
+    const size_t pl = (size_t)g.jm * g.kp, o0 = gidx(g, 0, j, k);
+
     bool ok = true;
-    for(int i = i0; i <= i1 && ok; i++){
-        const size_t o = gidx(g, i, j, k);
-        C.T[i] = A.t[o] * A.t_ref;
-        C.p[i] = A.ps[o];
+    for(int i = i0 + lane; i <= i1; i += 32){
+        const size_t o = o0 + (size_t)i * pl;
+        C.T[i] = t_ld(a.t, a.tlo, o) * A.t_ref;
+        C.p[i] = (double)a.ps[o];
         C.z[i] = (double)((float)i * A.hz) * 1.0e3;
         double rr = A.r_mix;                                // rho_at, cUranusModel.h:526-531
-        if(A.local_rho){ const double r_ = A.rho[o]; rr = (r_ > 0.0 && isfinite(r_)) ? r_ : A.r_mix; }
+        if(A.local_rho){ const double r_ = (double)a.rho[o]; rr = (r_ > 0.0 && isfinite(r_)) ? r_ : A.r_mix; }
         C.rho[i] = rr;
         if(!(C.T[i] > 0.0) || !(C.p[i] > 0.0) || !(C.rho[i] > 0.0) || !isfinite(C.T[i] + C.p[i] + C.rho[i])) ok = false;
     }
-    if(!ok) return;
-    for(int i = i0; i <= i1 && ok; i++){
-        const size_t o = gidx(g, i, j, k);
+    if(!__all_sync(FULL, ok)) return;
+    __syncwarp();
+    for(int i = i0 + lane; i <= i1; i += 32){
+        const size_t o = o0 + (size_t)i * pl;
         const double lo = (i > i0) ? 0.5 * (C.z[i - 1] + C.z[i]) : C.z[i0];
         const double hi = (i < i1) ? 0.5 * (C.z[i] + C.z[i + 1]) : C.z[i1];
         C.w[i] = C.rho[i] * (hi - lo);
@@ -199,71 +235,100 @@ static __global__ void __launch_bounds__(64) mca_kernel(const McaArgs A){
         double h = mca_enth(A, C.T[i]) + A.grav * C.z[i];
         for(int q = 0; q < MCA_NG; q++){
             const int x = i * MCA_NG + q;
-            C.qv[x] = mca_mx(0.0, A.sp[q][0][o]) / C.rho[i];
-            C.qc[x] = mca_mx(0.0, A.sp[q][1][o]) / C.rho[i];
-            C.qi[x] = mca_mx(0.0, A.sp[q][2][o]) / C.rho[i];
-            C.qt[x] = C.qv[x] + C.qc[x] + C.qi[x];
-            h -= A.G[q].lv * C.qc[x] + A.G[q].ls * C.qi[x];
+            const double qv = mca_mx(0.0, (double)a.sp[q][0][o]) / C.rho[i];
+            const double qc = mca_mx(0.0, (double)a.sp[q][1][o]) / C.rho[i];
+            const double qi = mca_mx(0.0, (double)a.sp[q][2][o]) / C.rho[i];
+            C.qt[x] = qv + qc + qi;
+            h -= A.G[q].lv * qc + A.G[q].ls * qi;
         }
-        C.qr[i] = A.nh4sh[o] / C.rho[i];
+        C.qr[i] = (double)a.nh4sh[o] / C.rho[i];
         h -= A.L_tr * C.qr[i];
         C.hL[i] = h;
     }
-    if(!ok) return;
-    for(int i = 0; i < im; i++){ C.touched[i] = false; C.eq_ok[i] = false; }
-    for(int i = i0; i < i1; i++){
-        bool held = false, moist = false;
-        C.cen_u[i] = mca_unstable(A, C, i, i + 1, &held, &moist);
-        C.cen_m[i] = moist;
-    }
+    for(int i = lane; i < im; i += 32){ C.touched[i] = 0; C.eq_ok[i] = 0; }
+    if(!__all_sync(FULL, ok)) return;
+    __syncwarp();
+
     int passes = 0;
     bool changed = true, fail = false;
     long layers = 0;
     while(changed && passes < 64 && !fail){
         changed = false; passes++;
+        // every pair's test at the start of the sweep, one pair per lane
+        for(int i = i0 + lane; i < i1; i += 32) C.U[i] = mca_unstable(A, C, i, i + 1) ? 1 : 0;
+        for(int i = lane; i < im; i += 32) C.mod[i] = 0;
+        __syncwarp();
         int i = i0;
         while(i < i1 && !fail){
-            bool moist = false, uns;
-            if(passes == 1 && !C.touched[i] && !C.touched[i + 1]){ uns = C.cen_u[i]; moist = C.cen_m[i]; }
-            else uns = mca_unstable(A, C, i, i + 1, nullptr, &moist);
-            if(!uns){ i++; continue; }
-            int a = i, b = i + 1;
-            for(;;){
-                double sw = 0.0, sh = 0.0, sq[MCA_NG] = {0.0, 0.0, 0.0, 0.0}, sr = 0.0;
-                for(int q = a; q <= b; q++){
-                    sw += C.w[q]; sh += C.w[q] * C.hL[q];
-                    for(int s = 0; s < MCA_NG; s++) sq[s] += C.w[q] * C.qt[q * MCA_NG + s];
-                    sr += C.w[q] * C.qr[q];
-                }
-                for(int q = a; q <= b; q++){
-                    C.hL[q] = sh / sw;
-                    for(int s = 0; s < MCA_NG; s++) C.qt[q * MCA_NG + s] = sq[s] / sw;
-                    C.qr[q] = sr / sw;
-                    if(!mca_settle(A, C, q)){ fail = true; break; }
-                }
-                if(fail) break;
-                bool ext = false;
-                if(a > i0 && mca_unstable(A, C, a - 1, a, nullptr, nullptr)){ a--; ext = true; }
-                if(b < i1 && mca_unstable(A, C, b, b + 1, nullptr, nullptr)){ b++; ext = true; }
-                if(!ext) break;
+            bool uns;
+            if(!C.mod[i] && !C.mod[i + 1]) uns = C.U[i] != 0;
+            else {
+                int u = 0;
+                if(lane == 0) u = mca_unstable(A, C, i, i + 1) ? 1 : 0;
+                u = __shfl_sync(FULL, u, 0);
+                uns = u != 0;
+                __syncwarp();
             }
-            layers += b - a + 1;
+            if(!uns){ i++; continue; }
+            int lo = i, hi = i + 1;
+            for(;;){
+                // the segment's mass-weighted means, summed in the reference's order
+                double m_h = 0.0, m_q[MCA_NG], m_r = 0.0;
+                if(lane == 0){
+                    double sw = 0.0, sh = 0.0, sq[MCA_NG] = {0.0, 0.0, 0.0, 0.0}, sr = 0.0;
+                    for(int q = lo; q <= hi; q++){
+                        sw += C.w[q]; sh += C.w[q] * C.hL[q];
+                        for(int s = 0; s < MCA_NG; s++) sq[s] += C.w[q] * C.qt[q * MCA_NG + s];
+                        sr += C.w[q] * C.qr[q];
+                    }
+                    m_h = sh / sw;
+                    for(int s = 0; s < MCA_NG; s++) m_q[s] = sq[s] / sw;
+                    m_r = sr / sw;
+                }
+                m_h = __shfl_sync(FULL, m_h, 0);
+                for(int s = 0; s < MCA_NG; s++) m_q[s] = __shfl_sync(FULL, lane == 0 ? m_q[s] : 0.0, 0);
+                m_r = __shfl_sync(FULL, m_r, 0);
+                bool sok = true;
+                for(int q = lo + lane; q <= hi; q += 32){
+                    C.hL[q] = m_h;
+                    for(int s = 0; s < MCA_NG; s++) C.qt[q * MCA_NG + s] = m_q[s];
+                    C.qr[q] = m_r;
+                    C.mod[q] = 1;
+                    if(!mca_settle(A, C, q)) sok = false;
+                }
+                fail = !__all_sync(FULL, sok);
+                __syncwarp();
+                if(fail) break;
+                // the two growth tests, below on lane 0 and above on lane 1
+                int gr = 0;
+                if(lane == 0 && lo > i0) gr = mca_unstable(A, C, lo - 1, lo) ? 1 : 0;
+                if(lane == 1 && hi < i1) gr = mca_unstable(A, C, hi, hi + 1) ? 2 : 0;
+                gr = __reduce_or_sync(FULL, (unsigned)gr);
+                __syncwarp();
+                if(gr & 1) lo--;
+                if(gr & 2) hi++;
+                if(!gr) break;
+            }
+            layers += hi - lo + 1;
             changed = true;
-            i = b;
+            i = hi;
         }
     }
     if(fail || layers == 0) return;                        // nothing written: the column keeps its state
-    for(int q = i0; q <= i1; q++){
+    for(int q = i0 + lane; q <= i1; q += 32){
         if(!C.touched[q]) continue;
-        const size_t o = gidx(g, q, j, k);
-        A.t[o] = C.T[q] / A.t_ref;
+        const size_t o = o0 + (size_t)q * pl;
+        t_st(a.t, a.tlo, o, C.T[q] / A.t_ref);
         for(int s = 0; s < MCA_NG; s++){
             const int x = q * MCA_NG + s;
-            A.sp[s][0][o] = C.qv[x] * C.rho[q];
-            A.sp[s][1][o] = C.qc[x] * C.rho[q];
-            A.sp[s][2][o] = C.qi[x] * C.rho[q];
+            const double ce = C.ceq[x];
+            const double qv = C.qt[x] - ce;
+            const bool liq = C.T[q] >= A.G[s].t_0;
+            a.sp[s][0][o] = (S)(qv * C.rho[q]);
+            a.sp[s][1][o] = (S)((liq ? ce : 0.0) * C.rho[q]);
+            a.sp[s][2][o] = (S)((liq ? 0.0 : ce) * C.rho[q]);
         }
-        A.nh4sh[o] = C.qr[q] * C.rho[q];
+        a.nh4sh[o] = (S)(C.qr[q] * C.rho[q]);
     }
 }
 
