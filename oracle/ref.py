@@ -49,8 +49,8 @@ _SINGLETON = None
 class Ref:
     """The reference model, initialised once per process (Run() with nm = 0)."""
 
-    def __init__(self, outdir="/tmp/aturan_ref_out", quiet=True, loop_iterations=0):
-        path = lib_path()
+    def __init__(self, outdir="/tmp/aturan_ref_out", quiet=True, loop_iterations=0, path=None):
+        path = path or lib_path()
         if path is None:
             raise RuntimeError("compiled reference not found under oracle/_ref")
         L = ctypes.CDLL(path)

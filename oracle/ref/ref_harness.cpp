@@ -136,6 +136,9 @@ std::vector<double>* vec(const char* name){
 
 extern "C" {
 
+// The model, for the driver glue compiled beside this harness (b200_glue.cpp).
+void* ref_model_ptr(){ return g_model; }
+
 int ref_dims(int* im, int* jm, int* km){
     *im = cUranusModel::im; *jm = cUranusModel::jm; *km = cUranusModel::km;
     return 0;
