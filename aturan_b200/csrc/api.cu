@@ -783,6 +783,7 @@ int run_chem(aturan_ctx* ctx, const aturan_chem_params* cp, int what, cudaStream
     c.sinthe_min = p.sinthe_min; c.floor = cp->polar_floor;
     c.per = cp->phi_periodic != 0;
     a.counts = ctx->counters + 4;
+    a.scratch = reinterpret_cast<S*>(ctx->ybuf[0]);           // free outside the RK4 step
     Region reg(ctx, ATURAN_K_CHEM, 0, st);
     reg.n = launch_chem(a, what, st);
     CK_LAUNCH("chemistry");

@@ -3,15 +3,16 @@
 // chemistry forcing (DiffMassFluxUran, ChemMassRateUran, FluxLimiterNH4SH and the 1-2-1 filters
 // between them, cUranusModel.cpp:1074-1087).
 //
-// The equilibrium is cell-local: one thread per cell brackets and bisects the cell's
-// K_p(T) condition (at most 82 evaluations of pow). The forcing is two 7-point stencil passes
-// over the interior (the diffusive tendencies and the thermal mass flux; then the mass rates and
-// the Superbee limiter) with the filters of post.cuh between and after them; every pass streams a
-// few planes of the state and is bound by HBM. Arithmetic is FP64 on the stored values (FP32
-// storage in the mixed form is widened, computed in FP64 and rounded back), in the reference's
-// operand order; the per-level and per-latitude factors (radius, metric radius, sin and cos of
-// the colatitude) come from a host table made with the host's libm, so the FP64 forcing equals
-// the CPU's bit for bit.
+// The equilibrium is cell-local: one thread per cell brackets the cell's K_p(T) condition as the
+// reference does and finds the root by safeguarded Newton (a few evaluations of K_p). The forcing
+// is two 7-point stencil passes over the interior (the diffusive tendencies and the thermal mass
+// flux; then the mass rates and the Superbee limiter) with the filters between and after them;
+// every pass streams a few planes of the state and is bound by HBM; each filter is one fused pass
+// over the three axes (post.cuh, post_filter3_kernel) and a copy back. Arithmetic is FP64 on the
+// stored values (FP32 storage in the mixed form is widened, computed in FP64 and rounded back), in
+// the reference's operand order; the per-level and per-latitude factors (radius, metric radius,
+// sin and cos of the colatitude) come from a host table made with the host's libm, so the FP64
+// forcing equals the CPU's bit for bit.
 #pragma once
 #include "common.cuh"
 
@@ -43,22 +44,56 @@ struct ChemArgs {
     ChemTab tab;
     ChemConst c;
     unsigned long long* counts;                       // [formed, decomposed]
+    S* scratch;                                       // one field the fused filters write before the copy back
 };
 
 __device__ __forceinline__ double chem_max(double a, double b){ return (a < b) ? b : a; }   // std::max
 __device__ __forceinline__ double chem_min(double a, double b){ return (b < a) ? b : a; }   // std::min
 
-// ChemistryUran.h:144 and :154-156
+// ChemistryUran.h:144 and :154-156: K_p(T) [Pa^2] (Lewis 1969) and the cell's equilibrium condition
+// f(x) = (a - x)(b - x)(R* T)^2 - K_p(T), T = T0 + heat x, with its derivative in x.
 __device__ __forceinline__ double nh4sh_kp(double T){
     const double atm = 101325.0;
-    return pow(10.0, 14.82 - 4705.0 / T) * atm * atm;
+    return exp10(14.82 - 4705.0 / T) * atm * atm;
 }
 __device__ __forceinline__ double nh4sh_f(double x, double T0, double heat, double a, double b){
     const double T = T0 + heat * x, RT = 8314.46 * T;
     return (a - x) * (b - x) * RT * RT - nh4sh_kp(T);
 }
+__device__ __forceinline__ double nh4sh_df(double x, double T0, double heat, double a, double b, double& f){
+    const double R = 8314.46, T = T0 + heat * x, RT = R * T;
+    const double P = (a - x) * (b - x), K = nh4sh_kp(T);
+    f = P * RT * RT - K;
+    return (2.0 * x - a - b) * RT * RT + P * 2.0 * R * RT * heat - K * 2.302585092994046 * 4705.0 / (T * T) * heat;
+}
+
+// The root of f in the bracket [lo, hi] (f(lo) > 0 >= f(hi)), as the reference's bisection finds it
+// to hi - lo <= stop. Safeguarded Newton from x0: a step that leaves the bracket is replaced by
+// the bracket's midpoint, every iterate narrows the bracket by its sign, at most 60 iterations.
+// The reference's bisection (ChemistryUran.h:163-168) returns the bracket end on the side it
+// started from (lo when forming, hi when decomposing); this returns the last iterate clamped into
+// the final bracket, within the same tolerance of the root.
+__device__ __forceinline__ double nh4sh_root(double lo, double hi, double x0, double stop, double T0, double heat,
+                                            double a, double b){
+    double x = (x0 > lo && x0 < hi) ? x0 : 0.5 * (lo + hi);
+    for(int it = 0; it < 60; it++){
+        double f;
+        const double d = nh4sh_df(x, T0, heat, a, b, f);
+        if(f > 0.0) lo = x; else hi = x;
+        if(hi - lo <= stop) break;
+        double xn = (d != 0.0 && isfinite(d)) ? x - f / d : 0.5 * (lo + hi);
+        if(!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        if(fabs(xn - x) <= 0.25 * stop){ x = xn; break; }
+        x = xn;
+    }
+    return fmin(fmax(x, lo), hi);
+}
 
 // ChemistryUran.h:140-177 per cell, :210-275 over every cell; counts formed / decomposed cells.
+// The branches, the brackets and the applied change are the reference's; inside a bracket the
+// root comes from safeguarded Newton (nh4sh_root) started at the fixed-T equilibrium (the
+// closed form of ChemistryUran.h:199-208) instead of 50-80 bisection steps, each an evaluation of
+// K_p: the same root to the bisection's stopping width.
 template <typename S>
 __global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
     const Grid& g = a.g;
@@ -77,31 +112,27 @@ __global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
             const double Sx = chem_max(0.0, ns) / c.m_nh4sh;
             const double heat = c.L_f * c.m_nh4sh / (c.cp_mix * rho);
             const double f0 = nh4sh_f(0.0, T0, heat, A, B);
-            double lo = 0.0, hi = 0.0;
+            const double stop = 1.0e-15 * chem_max(A, chem_max(B, Sx));
+            double x = 0.0;
             bool go = true;
-            if(f0 > 0.0){ lo = 0.0; hi = chem_min(A, B); }
-            else if(Sx > 0.0){
-                if(nh4sh_f(-Sx, T0, heat, A, B) <= 0.0){ lo = hi = -Sx; }
-                else { lo = -Sx; hi = 0.0; }
+            if(f0 > 0.0){
+                // the fixed-T root, ChemistryUran.h:199-208's cancellation-free form
+                const double RT = 8314.46 * T0;
+                const double K = nh4sh_kp(T0) / (RT * RT), d = A - B;
+                const double x0 = (A * B > K) ? 2.0 * (A * B - K) / ((A + B) + sqrt(d * d + 4.0 * K)) : 0.0;
+                const double hi = chem_min(A, B);
+                x = (hi > 0.0) ? nh4sh_root(0.0, hi, x0, stop, T0, heat, A, B) : 0.0;
+            } else if(Sx > 0.0){
+                if(nh4sh_f(-Sx, T0, heat, A, B) <= 0.0) x = -Sx;
+                else x = nh4sh_root(-Sx, 0.0, -0.5 * Sx, stop, T0, heat, A, B);
             } else go = false;
-            if(go){
-                if(hi > lo){
-                    const double stop = 1.0e-15 * chem_max(A, chem_max(B, Sx));
-                    for(int it = 0; it < 80; it++){
-                        const double xm = 0.5 * (lo + hi);
-                        if(nh4sh_f(xm, T0, heat, A, B) > 0.0) lo = xm; else hi = xm;
-                        if(hi - lo <= stop) break;
-                    }
-                }
-                const double x = (f0 > 0.0) ? lo : hi;
-                if(x != 0.0){
-                    a.nh3[q] = (S)chem_max(0.0, n3 - c.m_nh3 * x);
-                    a.h2s[q] = (S)chem_max(0.0, hs - c.m_h2s * x);
-                    a.nh4sh[q] = (S)chem_max(0.0, ns + c.m_nh4sh * x);
-                    const double dT = heat * x;
-                    t_st(a.t, a.tlo, q, (T0 + dT) / c.t_ref);
-                    if(x > 0.0) formed = 1; else decomposed = 1;
-                }
+            if(go && x != 0.0){
+                a.nh3[q] = (S)chem_max(0.0, n3 - c.m_nh3 * x);
+                a.h2s[q] = (S)chem_max(0.0, hs - c.m_h2s * x);
+                a.nh4sh[q] = (S)chem_max(0.0, ns + c.m_nh4sh * x);
+                const double dT = heat * x;
+                t_st(a.t, a.tlo, q, (T0 + dT) / c.t_ref);
+                if(x > 0.0) formed = 1; else decomposed = 1;
             }
         }
     }

@@ -86,6 +86,16 @@ int launch_filter(const Grid& g, S* x, float* lo, bool ai, bool aj, bool ak, dou
     if(ai){ post_filter_i_kernel<S><<<dim3(cols_k.x, g.jm), 128, 0, st>>>(g, x, lo, coeff); n++; }
     return n;
 }
+// damp_wiggles on x along all three axes in one fused pass into the scratch field y, copied back
+// over x (post_filter3_kernel); returns the launches.
+template <typename S>
+int launch_filter3(const Grid& g, S* x, S* y, double strength, int phi_periodic, cudaStream_t st){
+    const double coeff = strength * 0.25;                 // lib/Utils.cpp:232
+    const dim3 grid((g.km + FT_K - 1) / FT_K, (g.jm + FT_J - 1) / FT_J, (g.im + FT_I - 1) / FT_I);
+    post_filter3_kernel<S><<<grid, dim3(32, 8), 0, st>>>(g, x, y, coeff, phi_periodic && g.km > 2);
+    cudaMemcpyAsync(x, y, g.fstride * sizeof(S), cudaMemcpyDeviceToDevice, st);
+    return 1;
+}
 // The passes after RK4 in the reference's order; returns the number of launches.
 template <typename S>
 int launch_post_impl(const PostArgs<S>& a, const PostPlan& pl, S* t, float* tlo, cudaStream_t st){
@@ -122,12 +132,12 @@ int launch_chem_impl(const ChemArgs<S>& a, int what, cudaStream_t st){
         chem_diff_kernel<S><<<cols, 128, 0, st>>>(a);
         n++;
         S* f1[4] = {a.df_h2s, a.df_nh3, a.df_nh4sh, a.tmf};
-        for(S* x : f1) n += launch_filter<S>(g, x, nullptr, true, true, true, 1.0, a.c.per, st);
+        for(S* x : f1) n += launch_filter3<S>(g, x, a.scratch, 1.0, a.c.per, st);
         const int kn = g.km - 1 - (a.c.per ? 0 : 1);
         chem_limit_kernel<S><<<dim3((kn + 127) / 128, g.jm - 2, g.im - 2), 128, 0, st>>>(a);
         n++;
         S* f2[4] = {a.mf_h2s, a.mf_nh3, a.mf_nh4sh, a.fl};
-        for(S* x : f2) n += launch_filter<S>(g, x, nullptr, true, true, true, 1.0, a.c.per, st);
+        for(S* x : f2) n += launch_filter3<S>(g, x, a.scratch, 1.0, a.c.per, st);
     }
     return n;
 }
@@ -145,7 +155,7 @@ int launch_turb_impl(const TurbArgs<S>& a, cudaStream_t st){
 // The precipitation (precip.cuh): one thread per column; returns the number of launches.
 template <typename S>
 int launch_precip_impl(const PrecipArgs<S>& a, cudaStream_t st){
-    precip_kernel<S><<<dim3((a.g.km + 127) / 128, a.g.jm), 128, 0, st>>>(a);
+    precip_kernel<S><<<dim3((a.g.km + 31) / 32, a.g.jm), dim3(32, 4), 0, st>>>(a);
     return 1;
 }
 // The moist convective adjustment (mca.cuh): one warp per column, W warps per block, W = 4 halved

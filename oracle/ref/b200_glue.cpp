@@ -182,12 +182,18 @@ int glue_run(int n, int precision){
     if(!m || n < 0) return ATURAN_E_INVALID;
     const aturan_params p = b200_params(*m, precision);
     aturan_ctx* ctx = nullptr;
+    std::fprintf(stderr, "glue_run: creating the context\n");
     int rc = aturan_ctx_create(&p, &ctx);
     if(rc) return rc;
     const aturan_iter_params ip = b200_iter_params(*m);
+    std::fprintf(stderr, "glue_run: uploading\n");
     rc = b200_transfer(ctx, *m, true);
-    for(int it = 1; !rc && it <= n; it++) rc = aturan_iteration(ctx, &ip, it);
+    for(int it = 1; !rc && it <= n; it++){
+        std::fprintf(stderr, "glue_run: iteration %d\n", it);
+        rc = aturan_iteration(ctx, &ip, it);
+    }
     if(!rc) rc = aturan_sync(ctx);
+    std::fprintf(stderr, "glue_run: downloading (rc %d)\n", rc);
     if(!rc) rc = b200_transfer(ctx, *m, false);
     if(rc) std::fprintf(stderr, "glue_run: %s\n", aturan_last_error(ctx));
     aturan_ctx_destroy(ctx);

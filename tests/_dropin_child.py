@@ -3,9 +3,12 @@ reference with the driver glue, oracle/_ref/libaturan_ref_glue.so) runs N iterat
 the GPU through libaturan_b200 (glue_run: upload, aturan_iteration x N, download into the model's
 fields); the oracle runs the same N iterations on the same initialised state. Prints one JSON line
 of per-field agreement and exits 0."""
+import faulthandler
 import json
 import os
 import sys
+
+faulthandler.enable()
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
@@ -19,7 +22,9 @@ GLUE = os.path.join(ROOT, "oracle", "_ref", "libaturan_ref_glue.so")
 
 
 def main(n, precision):
+    print("loading the reference with the glue", file=sys.stderr, flush=True)
     r = ref.Ref(path=GLUE)
+    print("reference initialised", file=sys.stderr, flush=True)
     names = [m for m in F.NAMES if m not in F.PROJECTION]
     st = r.state(names)
     p = P.params_from_ref(r)
