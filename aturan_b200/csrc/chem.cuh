@@ -3,8 +3,9 @@
 // chemistry forcing (DiffMassFluxUran, ChemMassRateUran, FluxLimiterNH4SH and the 1-2-1 filters
 // between them, cUranusModel.cpp:1074-1087).
 //
-// The equilibrium is cell-local: one thread per cell brackets the cell's K_p(T) condition as the
-// reference does and finds the root by safeguarded Newton (a few evaluations of K_p). The forcing
+// The equilibrium is cell-local: one thread per cell brackets the cell's K_p(T) condition and
+// bisects it as the reference does, evaluating K_p only at the midpoints near the root that a
+// Newton estimate locates (nh4sh_bisect: the reference's midpoints and result). The forcing
 // is two 7-point stencil passes over the interior (the diffusive tendencies and the thermal mass
 // flux; then the mass rates and the Superbee limiter) with the filters between and after them;
 // every pass streams a few planes of the state and is bound by HBM; each filter is one fused pass
@@ -51,10 +52,11 @@ __device__ __forceinline__ double chem_max(double a, double b){ return (a < b) ?
 __device__ __forceinline__ double chem_min(double a, double b){ return (b < a) ? b : a; }   // std::min
 
 // ChemistryUran.h:144 and :154-156: K_p(T) [Pa^2] (Lewis 1969) and the cell's equilibrium condition
-// f(x) = (a - x)(b - x)(R* T)^2 - K_p(T), T = T0 + heat x, with its derivative in x.
+// f(x) = (a - x)(b - x)(R* T)^2 - K_p(T), T = T0 + heat x, as the reference evaluates it; and f
+// with its derivative in x for the Newton estimate of the root (K_p by exp10 there).
 __device__ __forceinline__ double nh4sh_kp(double T){
     const double atm = 101325.0;
-    return exp10(14.82 - 4705.0 / T) * atm * atm;
+    return pow(10.0, 14.82 - 4705.0 / T) * atm * atm;
 }
 __device__ __forceinline__ double nh4sh_f(double x, double T0, double heat, double a, double b){
     const double T = T0 + heat * x, RT = 8314.46 * T;
@@ -62,38 +64,58 @@ __device__ __forceinline__ double nh4sh_f(double x, double T0, double heat, doub
 }
 __device__ __forceinline__ double nh4sh_df(double x, double T0, double heat, double a, double b, double& f){
     const double R = 8314.46, T = T0 + heat * x, RT = R * T;
-    const double P = (a - x) * (b - x), K = nh4sh_kp(T);
+    const double P = (a - x) * (b - x), K = exp10(14.82 - 4705.0 / T) * 101325.0 * 101325.0;
     f = P * RT * RT - K;
     return (2.0 * x - a - b) * RT * RT + P * 2.0 * R * RT * heat - K * 2.302585092994046 * 4705.0 / (T * T) * heat;
 }
 
-// The root of f in the bracket [lo, hi] (f(lo) > 0 >= f(hi)), as the reference's bisection finds it
-// to hi - lo <= stop. Safeguarded Newton from x0: a step that leaves the bracket is replaced by
-// the bracket's midpoint, every iterate narrows the bracket by its sign, at most 60 iterations.
-// The reference's bisection (ChemistryUran.h:163-168) returns the bracket end on the side it
-// started from (lo when forming, hi when decomposing); this returns the last iterate clamped into
-// the final bracket, within the same tolerance of the root.
-__device__ __forceinline__ double nh4sh_root(double lo, double hi, double x0, double stop, double T0, double heat,
-                                            double a, double b){
-    double x = (x0 > lo && x0 < hi) ? x0 : 0.5 * (lo + hi);
-    for(int it = 0; it < 60; it++){
-        double f;
-        const double d = nh4sh_df(x, T0, heat, a, b, f);
-        if(f > 0.0) lo = x; else hi = x;
-        if(hi - lo <= stop) break;
-        double xn = (d != 0.0 && isfinite(d)) ? x - f / d : 0.5 * (lo + hi);
-        if(!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
-        if(fabs(xn - x) <= 0.25 * stop){ x = xn; break; }
-        x = xn;
+// The reference's bisection of f on [lo, hi] (f(lo) > 0 >= f(hi); ChemistryUran.h:163-168), with
+// the same midpoints and the same result, evaluating f only where its sign is in question. f is
+// decreasing on the bracket (the formation heat moves T by millikelvin, against (a-x)(b-x) going
+// from ab to 0), so at a midpoint farther than `band` from the root r its sign is that of r - xm;
+// r comes from safeguarded Newton (a step that leaves the bracket is replaced by its midpoint),
+// and f itself is evaluated, as the reference does, at the ~10 midpoints inside the band instead
+// of at all ~50. The final bracket is checked with f at both ends; a bracket that does not hold
+// (no single root, or Newton astray) is bisected again with f at every midpoint.
+__device__ __forceinline__ void nh4sh_bisect(double& lo, double& hi, double stop, double T0, double heat,
+                                             double a, double b, double x0){
+    const double lo0 = lo, hi0 = hi;
+    // Newton estimate of the root
+    double r = (x0 > lo && x0 < hi) ? x0 : 0.5 * (lo + hi);
+    {
+        double l = lo, h = hi;
+        for(int it = 0; it < 60; it++){
+            double f;
+            const double d = nh4sh_df(r, T0, heat, a, b, f);
+            if(f > 0.0) l = r; else h = r;
+            double rn = (d != 0.0 && isfinite(d)) ? r - f / d : 0.5 * (l + h);
+            if(!(rn > l && rn < h)) rn = 0.5 * (l + h);
+            const bool done = fabs(rn - r) <= 1.0e-3 * stop || h - l <= 1.0e-3 * stop;
+            r = rn;
+            if(done) break;
+        }
     }
-    return fmin(fmax(x, lo), hi);
+    const double band = 1.0e3 * stop;
+    for(int it = 0; it < 80; it++){
+        const double xm = 0.5 * (lo + hi);
+        bool pos;
+        if(xm < r - band) pos = true;
+        else if(xm > r + band) pos = false;
+        else pos = nh4sh_f(xm, T0, heat, a, b) > 0.0;
+        if(pos) lo = xm; else hi = xm;
+        if(hi - lo <= stop) break;
+    }
+    if(hi > lo && (nh4sh_f(lo, T0, heat, a, b) > 0.0) && !(nh4sh_f(hi, T0, heat, a, b) > 0.0)) return;
+    if(!(hi > lo)) return;
+    lo = lo0; hi = hi0;                                       // the plain bisection
+    for(int it = 0; it < 80; it++){
+        const double xm = 0.5 * (lo + hi);
+        if(nh4sh_f(xm, T0, heat, a, b) > 0.0) lo = xm; else hi = xm;
+        if(hi - lo <= stop) break;
+    }
 }
 
 // ChemistryUran.h:140-177 per cell, :210-275 over every cell; counts formed / decomposed cells.
-// The branches, the brackets and the applied change are the reference's; inside a bracket the
-// root comes from safeguarded Newton (nh4sh_root) started at the fixed-T equilibrium (the
-// closed form of ChemistryUran.h:199-208) instead of 50-80 bisection steps, each an evaluation of
-// K_p: the same root to the bisection's stopping width.
 template <typename S>
 __global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
     const Grid& g = a.g;
@@ -112,27 +134,29 @@ __global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
             const double Sx = chem_max(0.0, ns) / c.m_nh4sh;
             const double heat = c.L_f * c.m_nh4sh / (c.cp_mix * rho);
             const double f0 = nh4sh_f(0.0, T0, heat, A, B);
-            const double stop = 1.0e-15 * chem_max(A, chem_max(B, Sx));
-            double x = 0.0;
+            double lo = 0.0, hi = 0.0, x0 = 0.0;
             bool go = true;
             if(f0 > 0.0){
-                // the fixed-T root, ChemistryUran.h:199-208's cancellation-free form
+                lo = 0.0; hi = chem_min(A, B);
+                // the fixed-T root (ChemistryUran.h:199-208's cancellation-free form) starts Newton
                 const double RT = 8314.46 * T0;
                 const double K = nh4sh_kp(T0) / (RT * RT), d = A - B;
-                const double x0 = (A * B > K) ? 2.0 * (A * B - K) / ((A + B) + sqrt(d * d + 4.0 * K)) : 0.0;
-                const double hi = chem_min(A, B);
-                x = (hi > 0.0) ? nh4sh_root(0.0, hi, x0, stop, T0, heat, A, B) : 0.0;
+                x0 = (A * B > K) ? 2.0 * (A * B - K) / ((A + B) + sqrt(d * d + 4.0 * K)) : 0.0;
             } else if(Sx > 0.0){
-                if(nh4sh_f(-Sx, T0, heat, A, B) <= 0.0) x = -Sx;
-                else x = nh4sh_root(-Sx, 0.0, -0.5 * Sx, stop, T0, heat, A, B);
+                if(nh4sh_f(-Sx, T0, heat, A, B) <= 0.0){ lo = hi = -Sx; }
+                else { lo = -Sx; hi = 0.0; x0 = -0.5 * Sx; }
             } else go = false;
-            if(go && x != 0.0){
-                a.nh3[q] = (S)chem_max(0.0, n3 - c.m_nh3 * x);
-                a.h2s[q] = (S)chem_max(0.0, hs - c.m_h2s * x);
-                a.nh4sh[q] = (S)chem_max(0.0, ns + c.m_nh4sh * x);
-                const double dT = heat * x;
-                t_st(a.t, a.tlo, q, (T0 + dT) / c.t_ref);
-                if(x > 0.0) formed = 1; else decomposed = 1;
+            if(go){
+                if(hi > lo) nh4sh_bisect(lo, hi, 1.0e-15 * chem_max(A, chem_max(B, Sx)), T0, heat, A, B, x0);
+                const double x = (f0 > 0.0) ? lo : hi;
+                if(x != 0.0){
+                    a.nh3[q] = (S)chem_max(0.0, n3 - c.m_nh3 * x);
+                    a.h2s[q] = (S)chem_max(0.0, hs - c.m_h2s * x);
+                    a.nh4sh[q] = (S)chem_max(0.0, ns + c.m_nh4sh * x);
+                    const double dT = heat * x;
+                    t_st(a.t, a.tlo, q, (T0 + dT) / c.t_ref);
+                    if(x > 0.0) formed = 1; else decomposed = 1;
+                }
             }
         }
     }

@@ -17,7 +17,10 @@
 //     its cells is then brought to equilibrium by its own lane;
 //   * the two growth tests of a segment (below and above) run on lanes 0 and 1.
 // Each test solves a cell's equilibrium by Illinois regula falsi, so the arithmetic is FP64
-// whatever the storage (FP32 storage in the mixed form is widened, T read as its FP32 pair).
+// whatever the storage (FP32 storage in the mixed form is widened, T read as its FP32 pair). The
+// solve, the test, the settle, the energy balance and the enthalpy inverse are out-of-line
+// functions: inlined at each call site the kernel's code outgrew the instruction cache and most
+// issue slots went unused for want of an instruction.
 // Every loop is bounded: 60 regula-falsi steps, 30 Newton steps of the enthalpy inverse, 64
 // sweeps, and a segment grows by one level per step within the column.
 #pragma once
@@ -82,7 +85,7 @@ static __device__ double mca_enth(const McaConst& A, double T){
     if(A.cp_gas) return (A.r_h2 * hh + (A.r_he * A.cp_he + A.r_ch4 * A.cp_ch4) * T) / (A.r_h2 + A.r_he + A.r_ch4);
     return (A.cp_mix - (A.r_h2 / A.r_mix) * A.cp_h2) * T + (A.r_h2 / A.r_mix) * hh;
 }
-static __device__ double mca_enth_inv(const McaConst& A, double h, double T0){
+static __device__ __noinline__ double mca_enth_inv(const McaConst& A, double h, double T0){
     if(!A.cp_dyn) return h / A.cp_mix;
     double T = (T0 > 0.0) ? T0 : h / A.cp_mix;
     for(int it = 0; it < 30; it++){
@@ -94,28 +97,31 @@ static __device__ double mca_enth_inv(const McaConst& A, double h, double T0){
     return T;
 }
 
-// ATPhys.h:49-53 (the saturation pressure) and ConvectiveAdjustment.h:437-453 without the phase split
-__device__ __forceinline__ double mca_qsat(const McaGas& s, double T, double pr){
-    const double E = (T >= s.t_0) ? exp(s.C + (-s.L0 / T + s.del_alf * log(T) + s.del_bet * T) / (1e-3 * s.R))
-                                  : exp(s.C_i + (-s.L0_i / T + s.del_alf_i * log(T) + s.del_bet_i * T) / (1e-3 * s.R));
+// ATPhys.h:49-53 (the saturation pressure) and ConvectiveAdjustment.h:437-453 without the phase
+// split; lg = log(T), the same value for every gas at one T, formed once by the caller
+__device__ __forceinline__ double mca_qsat(const McaGas& s, double T, double lg, double pr){
+    const double E = (T >= s.t_0) ? exp(s.C + (-s.L0 / T + s.del_alf * lg + s.del_bet * T) / (1e-3 * s.R))
+                                  : exp(s.C_i + (-s.L0_i / T + s.del_alf_i * lg + s.del_bet_i * T) / (1e-3 * s.R));
     const double q = s.ep * E / pr;
     return isfinite(q) ? q : 0.0;
 }
 __device__ __forceinline__ double mca_lat(const McaGas& s, double T){ return T >= s.t_0 ? s.lv : s.ls; }
 
-static __device__ double mca_fof(const McaConst& A, double TT, double hL, const double* qt, double pr, double z){
+static __device__ __noinline__ double mca_fof(const McaConst& A, double TT, double hL, const double* qt, double pr, double z){
     double f = mca_enth(A, TT) + A.grav * z - hL;
-    for(int g = 0; g < MCA_NG; g++) f -= mca_lat(A.G[g], TT) * mca_mx(0.0, qt[g] - mca_qsat(A.G[g], TT, pr));
+    const double lg = log(TT);
+    for(int g = 0; g < MCA_NG; g++) f -= mca_lat(A.G[g], TT) * mca_mx(0.0, qt[g] - mca_qsat(A.G[g], TT, lg, pr));
     return f;
 }
 
 // :455-488, the equilibrium of (hL, qt) at (p, z): Illinois regula falsi on the energy balance
-static __device__ bool mca_equil(const McaConst& A, double hL, const double* qt, double pr, double z, double& T, double* cond){
+static __device__ __noinline__ bool mca_equil(const McaConst& A, double hL, const double* qt, double pr, double z, double& T, double* cond){
     const double cp = A.cp_mix, tol_T = 1.0e-10;
     const double T_lo = A.cp_dyn ? mca_enth_inv(A, hL - A.grav * z, 0.0) : (hL - A.grav * z) / cp;
     if(!(T_lo > 0.0) || !(pr > 0.0)) return false;
     bool any = false;
-    for(int g = 0; g < MCA_NG; g++) if(qt[g] > mca_qsat(A.G[g], T_lo, pr)){ any = true; break; }
+    const double lg_lo = log(T_lo);
+    for(int g = 0; g < MCA_NG; g++) if(qt[g] > mca_qsat(A.G[g], T_lo, lg_lo, pr)){ any = true; break; }
     if(!any){ T = T_lo; for(int g = 0; g < MCA_NG; g++) cond[g] = 0.0; return true; }
     double span = 0.0;
     for(int g = 0; g < MCA_NG; g++) span += mca_mx(A.G[g].lv, A.G[g].ls) * mca_mx(0.0, qt[g]);
@@ -131,7 +137,8 @@ static __device__ bool mca_equil(const McaConst& A, double hL, const double* qt,
         if(fabs(fc) <= cp * tol_T){ a = b = c; break; }
     }
     T = b;
-    for(int g = 0; g < MCA_NG; g++) cond[g] = mca_mx(0.0, qt[g] - mca_qsat(A.G[g], T, pr));
+    const double lg_b = log(T);
+    for(int g = 0; g < MCA_NG; g++) cond[g] = mca_mx(0.0, qt[g] - mca_qsat(A.G[g], T, lg_b, pr));
     return true;
 }
 
@@ -169,7 +176,7 @@ static __device__ double mca_tv(const McaConst& A, const McaCol& C, double TT, c
 
 // :627-644: is the pair (a, b = a+1) unstable? Caches b's equilibrium (written by this lane only:
 // each cell is the upper cell of one pair).
-static __device__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
+static __device__ __noinline__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
     const double tol_K = 1.0e-7;
     double Tp, pc[MCA_NG], pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
     if(!mca_equil(A, C.hL[a] + mca_trE(A, C, a), &C.qt[a * MCA_NG], C.p[b], C.z[b], Tp, pc)) return false;
@@ -186,7 +193,7 @@ static __device__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
 
 // :645-661, cell q to equilibrium from hL / qt; the vapour and the condensate's phase split are
 // rebuilt from qt, ceq and T at write-back (qv = qt - ceq; ceq is liquid at T >= t_0, else ice)
-static __device__ bool mca_settle(const McaConst& A, McaCol& C, int q){
+static __device__ __noinline__ bool mca_settle(const McaConst& A, McaCol& C, int q){
     double TT, pc[MCA_NG];
     if(!mca_equil(A, C.hL[q] + mca_trE(A, C, q), &C.qt[q * MCA_NG], C.p[q], C.z[q], TT, pc)) return false;
     C.T[q] = TT;

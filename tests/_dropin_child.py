@@ -26,7 +26,7 @@ def main(n, precision):
     r = ref.Ref(path=GLUE)
     print("reference initialised", file=sys.stderr, flush=True)
     names = [m for m in F.NAMES if m not in F.PROJECTION]
-    st = r.state(names)
+    st = r.state(F.NAMES)                    # every field the oracle's iteration reads or writes
     p = P.params_from_ref(r)
     ip = P.default_iter_params()
     rc = r.L.glue_run(int(n), int(precision))
