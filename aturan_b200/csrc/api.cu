@@ -355,7 +355,6 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
     a.k = K;
     a.tlo = ctx->tlo;
     a.tnlo = ctx->tlo ? ctx->tlo + fs : nullptr;
-    a.err = ctx->counters + 7;
     S* y0 = reinterpret_cast<S*>(ctx->ybuf[0]);
     S* y1 = reinterpret_cast<S*>(ctx->ybuf[1]);
     const double dt = ctx->p.dt;
@@ -2072,15 +2071,6 @@ int aturan_profile_read(aturan_ctx* ctx, double* ms, long* launches, int nkinds)
 int aturan_sync(aturan_ctx* ctx){
     if(!ctx) return ATURAN_E_INVALID;
     CK(cudaStreamSynchronize(ctx->st));
-    // counters[7]: bounded waits on a bulk copy that gave up (the RK4 scalar launch); the fields
-    // that launch wrote since the last check are then not to be trusted
-    unsigned long long lost = 0;
-    CK(cudaMemcpy(&lost, ctx->counters + 7, sizeof lost, cudaMemcpyDeviceToHost));
-    if(lost){
-        CK(cudaMemset(ctx->counters + 7, 0, sizeof lost));
-        return fail(ctx, ATURAN_E_CUDA, "RK4 scalar launch: " + std::to_string(lost) +
-                    " bounded bulk-copy wait(s) gave up; the step's scalar fields are invalid");
-    }
     return ATURAN_OK;
 }
 

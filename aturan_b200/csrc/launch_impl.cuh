@@ -24,10 +24,8 @@ namespace aturan {
 // blocks per SM instead of one cell per thread at MINB1. FP32: 128 registers at 4 blocks per SM,
 // a 1.5 % faster stage than one cell per thread at 7 (3 blocks per SM: 2 % slower). FP64: the
 // pair form spills at 3-5 blocks per SM, so it keeps one cell per thread.
-// BULK > 0 (FP32 storage): the scalar launch stages its inputs with bulk copies through a ring of
-// BULK slots (rk_scalar_bulk_kernel) at BMINB resident blocks per SM.
-template <typename S> struct StageCfg { static constexpr int MINB1 = 5, MP = 0, PD = 1, MINB2 = 3, AD = 2, AMINB = 3, BULK = 0, BMINB = 0; };
-template <> struct StageCfg<float> { static constexpr int MINB1 = 7, MP = 4, PD = 1, MINB2 = 6, AD = 0, AMINB = 4, BULK = 3, BMINB = 4; };
+template <typename S> struct StageCfg { static constexpr int MINB1 = 5, MP = 0, PD = 1, MINB2 = 3, AD = 2, AMINB = 3; };
+template <> struct StageCfg<float> { static constexpr int MINB1 = 7, MP = 4, PD = 1, MINB2 = 6, AD = 0, AMINB = 4; };
 // The saturation adjustment has no shared memory of its own, so left to itself it runs with the
 // smallest shared-memory split of each SM's L1, and a kernel that needs shared memory (the pressure
 // solve's, beside it in aturan_step) cannot start on that SM until all its blocks have left.
@@ -42,15 +40,7 @@ inline void prefer_max_shared(K* kernel){
 template <typename S> struct SatCfg { static constexpr int NT = 128; };
 template <typename S, typename C>
 void launch_scalars(const StageArgs<S, C>& a, dim3 grid2, cudaStream_t st){
-    if constexpr(sizeof(S) == 4 && StageCfg<S>::BULK > 0){
-        constexpr int D = StageCfg<S>::BULK;
-        auto kern = rk_scalar_bulk_kernel<C, StageCfg<S>::BMINB, D>;
-        const int sm = D * (int)sizeof(BulkSlot) + D * 8;
-        static const bool attr = (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) == cudaSuccess)
-                                 || (cudaGetLastError(), false);
-        (void)attr;
-        kern<<<grid2, dim3(32, 4), sm, st>>>(a);
-    } else if constexpr(StageCfg<S>::AD > 0){
+    if constexpr(StageCfg<S>::AD > 0){
         constexpr int D = StageCfg<S>::AD;
         auto kern = rk_scalar_async_kernel<S, C, D, StageCfg<S>::AMINB>;
         const int sm = D * (int)sizeof(AsyncSlot<S>);

@@ -45,7 +45,6 @@ struct StageArgs {
     // tn (read by stage 3); null in an FP64 context
     float* tlo;
     const float* tnlo;
-    unsigned long long* err;   // counts bounded waits that gave up (rk_scalar_bulk_kernel)
 };
 
 template <typename S>
@@ -632,182 +631,6 @@ __global__ void __launch_bounds__(128, MINB) rk_scalar_async_kernel(const StageA
         cp_async_commit();
     }
     cp_async_wait<0>();
-}
-
-// ---- the scalar part with its inputs staged by the bulk-copy engine (cp.async.bulk) ----
-// The same cells, arithmetic and order as rk_scalar_pair_kernel. A block's tile is one i plane,
-// four j rows (one per warp) and 64 k (two cells per thread); for each scalar field one thread
-// brings the rows the tile reads -- the field's own plane j0-1 .. j0+4 and planes i-1, i+1 at
-// j0 .. j0+3, and the tile's accumulator, n-copy and forcing rows -- into a slot of a D-deep ring
-// in shared memory with 256-byte bulk copies (each row's 64 values, 16-byte aligned at both ends)
-// that complete on the slot's mbarrier. The block computes field n while the copies of fields
-// n+1 .. n+D-1 are in flight; after all threads are done with a slot (a block barrier) it is
-// refilled with field n+D. Boundary rows come from the state, as make_cell addresses them; the k
-// neighbours outside the tile's 64 values (k0-1, k0+64, and the periodic seam) are loaded directly.
-// Every wait on an mbarrier is bounded: past the limit the kernel records it in *err and goes on,
-// and before exiting it waits (bounded again) for every copy it issued.
-constexpr int BULK_K = 64, BULK_J = 4;
-struct BulkSlot {
-    float xc[BULK_J + 2][BULK_K];        // the field's own plane, rows j0-1 .. j0+4
-    float xm[BULK_J][BULK_K], xp[BULK_J][BULK_K];
-    float acc[BULK_J][BULK_K], nc[BULK_J][BULK_K], f1[BULK_J][BULK_K], f2[BULK_J][BULK_K], f3[BULK_J][BULK_K];
-};
-
-__device__ __forceinline__ unsigned smem_u32(const void* p){ return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count){
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes){
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity){
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// The wait of one slot's phase, bounded (about a second at the longest); false if it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity){
-    for(long it = 0; it < (1L << 24); it++) if(mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar){
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-
-// The rows of scalar field n for the tile at (i, j0, k0): f(dst, src) for each, in one order for
-// the byte count and the copies. kp is a multiple of 32 and k0 of 64, so a row holds 64 or (the
-// last tile of a row with kp = 64 m + 32) 32 values from k0 on: the copy takes what the row holds
-// (256 or 128 bytes), never the next row's, and the values the tile reads lie below km <= kp.
-template <typename S, typename C, typename Fn>
-__device__ __forceinline__ void bulk_rows(BulkSlot& sl, const StageArgs<S, C>& a, int n, int i, int j0, int k0, Fn f){
-    const Grid& g = a.g;
-    const size_t fs = g.fstride;
-    const int q = scalar_field(n);
-    const S* X = a.X + (size_t)q * fs;
-    const S* St = a.St + (size_t)q * fs;
-    for(int jj = 0; jj < BULK_J + 2; jj++){
-        const int jr = j0 - 1 + jj;
-        if(jr > g.jm - 1) break;
-        f(&sl.xc[jj][0], ((jr == 0 || jr == g.jm - 1) ? St : X) + gidx(g, i, jr, k0));
-    }
-    const S* F = a.forc + gidx(g, i, 0, k0);
-    for(int jj = 0; jj < BULK_J; jj++){
-        const int jr = j0 + jj;
-        if(jr > g.jm - 2) break;
-        const size_t row = (size_t)jr * g.kp;
-        f(&sl.xm[jj][0], (i - 1 == 0 ? St : X) + gidx(g, i - 1, jr, k0));
-        f(&sl.xp[jj][0], (i + 1 == g.im - 1 ? St : X) + gidx(g, i + 1, jr, k0));
-        if(a.stage != 0) f(&sl.acc[jj][0], a.acc + (size_t)q * fs + gidx(g, i, jr, k0));
-        f(&sl.nc[jj][0], a.Nc + (size_t)q * fs + gidx(g, i, jr, k0));
-        if(n < 12){
-            f(&sl.f1[jj][0], F + (ATURAN_S_PRECIP_CH4 + n - ATURAN_NUE) * fs + row);
-            if(q == ATURAN_H2S) f(&sl.f2[jj][0], F + (ATURAN_MASSFLUX_H2S - ATURAN_NUE) * fs + row);
-            if(q == ATURAN_NH3) f(&sl.f2[jj][0], F + (ATURAN_MASSFLUX_NH3 - ATURAN_NUE) * fs + row);
-        } else if(n == 12){
-            f(&sl.f1[jj][0], F + (ATURAN_FLUXLIM_NH4SH - ATURAN_NUE) * fs + row);
-            f(&sl.f2[jj][0], F + (ATURAN_MASSFLUX_NH4SH - ATURAN_NUE) * fs + row);
-            f(&sl.f3[jj][0], F + (ATURAN_RHO_MIX - ATURAN_NUE) * fs + row);
-        } else {
-            f(&sl.f1[jj][0], F + ((n == 13 ? ATURAN_TKE_SOURCE : ATURAN_DIS_SOURCE) - ATURAN_NUE) * fs + row);
-        }
-    }
-}
-template <typename S, typename C>
-__device__ __forceinline__ void bulk_issue(BulkSlot& sl, unsigned long long* bar, const StageArgs<S, C>& a, int n,
-                                           int i, int j0, int k0){
-    const unsigned row = (unsigned)min(BULK_K, a.g.kp - k0) * (unsigned)sizeof(float);
-    unsigned bytes = 0;
-    bulk_rows(sl, a, n, i, j0, k0, [&](float*, const S*){ bytes += row; });
-    mbar_expect_tx(bar, bytes);
-    bulk_rows(sl, a, n, i, j0, k0, [&](float* dst, const S* src){ bulk_g2s(dst, src, row, bar); });
-}
-
-template <typename C, int MINB, int D>
-__global__ void __launch_bounds__(128, MINB) rk_scalar_bulk_kernel(const StageArgs<float, C> a){
-    using S = float;
-    extern __shared__ __align__(128) unsigned char bulk_raw[];
-    BulkSlot* ring = reinterpret_cast<BulkSlot*>(bulk_raw);
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(bulk_raw + D * sizeof(BulkSlot));
-    const Grid& g = a.g;
-    const int tx = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tx;
-    const int k0 = blockIdx.x * BULK_K, j0 = 1 + blockIdx.y * BULK_J, i = 1 + blockIdx.z;
-    const int k = k0 + 2 * tx, j = j0 + ty;
-    const bool act = k <= g.km - 2 && j <= g.jm - 2;
-    const RhsConst<C>& K = a.k;
-    const int nfield = K.turb_active ? N_SCALARS : N_SCALARS - 2;
-    if(t == 0){
-        for(int s = 0; s < D; s++) mbar_init(&full[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-    if(t == 0) for(int n = 0; n < D && n < nfield; n++) bulk_issue(ring[n], &full[n], a, n, i, j0, k0);
-    const S* X = a.X;
-    S* W = const_cast<S*>(a.X);
-    Cell c{};
-    GeoIJ<C> geo{};
-    C nue0 = C(0), nue1 = C(0), u0 = C(0), u1 = C(0), v0 = C(0), v1 = C(0), w0 = C(0), w1 = C(0);
-    C nts0 = C(0), nts1 = C(0), vr0 = C(0), vr1 = C(0), wr0 = C(0), wr1 = C(0);
-    if(act){
-        geo = a.geo[i * g.jm + j];
-        c = make_cell(a, i, j, k, 2);
-        ld2<S, C>(X + (c.dforc + c.o), nue0, nue1);
-        ld2<S, C>(X + (ATURAN_U * c.fs + c.o), u0, u1);
-        ld2<S, C>(X + (ATURAN_V * c.fs + c.o), v0, v1);
-        ld2<S, C>(X + (ATURAN_W * c.fs + c.o), w0, w1);
-        auto nts = [&](C nue_c) -> C {
-            const C nue_t = (K.turb_coupling != C(0.0) && isfinite(nue_c)) ? K.turb_coupling * cmax(C(0.0), nue_c) : C(0.0);
-            return qdiv(nue_t, C(0.9), C(1.0 / 0.9));
-        };
-        nts0 = nts(nue0); nts1 = nts(nue1);
-        vr0 = v0 * geo.inv_rm; vr1 = v1 * geo.inv_rm;
-        wr0 = w0 * geo.inv_rmsinthe; wr1 = w1 * geo.inv_rmsinthe;
-    }
-    const int kk = 2 * tx;
-    bool lost = false;
-    for(int n = 0; n < nfield; n++){
-        const int s = n % D;
-        if(!mbar_wait_bounded(&full[s], (unsigned)((n / D) & 1))){
-            lost = true;
-            if(t == 0 && a.err) atomicAdd(a.err, 1ull);
-        }
-        if(act){
-            const BulkSlot& sl = ring[s];
-            const int q = scalar_field(n);
-            const int f = q * c.fs;
-            ScalarIn2<C> in;
-            ScalarIn<C>& A = in.c0;
-            ScalarIn<C>& B = in.c1;
-            A.v.c = (C)sl.xc[ty + 1][kk];     B.v.c = (C)sl.xc[ty + 1][kk + 1];
-            A.v.tp = (C)sl.xc[ty + 2][kk];    B.v.tp = (C)sl.xc[ty + 2][kk + 1];
-            A.v.tm = (C)sl.xc[ty][kk];        B.v.tm = (C)sl.xc[ty][kk + 1];
-            A.v.rp = (C)sl.xp[ty][kk];        B.v.rp = (C)sl.xp[ty][kk + 1];
-            A.v.rm = (C)sl.xm[ty][kk];        B.v.rm = (C)sl.xm[ty][kk + 1];
-            A.v.pw = (tx > 0) ? (C)sl.xc[ty + 1][kk - 1] : (C)ld(X + (f + c.okw));
-            B.v.pe = (tx < 31 && k + 2 <= g.km - 2) ? (C)sl.xc[ty + 1][kk + 2] : (C)ld(X + (f + c.oke));
-            A.v.pe = B.v.c;
-            B.v.pw = A.v.c;
-            if(a.stage == 0){ A.an.acc = C(0.0); B.an.acc = C(0.0); }
-            else { A.an.acc = (C)sl.acc[ty][kk]; B.an.acc = (C)sl.acc[ty][kk + 1]; }
-            A.an.nc = (C)sl.nc[ty][kk]; B.an.nc = (C)sl.nc[ty][kk + 1];
-            A.f1 = (C)sl.f1[ty][kk]; B.f1 = (C)sl.f1[ty][kk + 1];
-            A.f2 = B.f2 = C(0.0); A.f3 = B.f3 = C(0.0);
-            if(n == 12 || q == ATURAN_H2S || q == ATURAN_NH3){ A.f2 = (C)sl.f2[ty][kk]; B.f2 = (C)sl.f2[ty][kk + 1]; }
-            if(n == 12){ A.f3 = (C)sl.f3[ty][kk]; B.f3 = (C)sl.f3[ty][kk + 1]; }
-            const C r0 = scalar_rhs(K, in.c0, n, geo, u0, v0, w0, vr0, wr0, nue0, nts0);
-            const C r1 = scalar_rhs(K, in.c1, n, geo, u1, v1, w1, vr1, wr1, nue1, nts1);
-            stage_update2(a, W, c, q, r0, r1, scalar_kind(n), in.c0.an, in.c1.an);
-        }
-        __syncthreads();                                   // every thread is done with slot s
-        if(t == 0 && n + D < nfield){
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            bulk_issue(ring[s], &full[s], a, n + D, i, j0, k0);
-        }
-    }
-    // each slot's last phase once more, bounded, if a wait gave up: no copy in flight at exit
-    if(lost)
-        for(int n = nfield - 1; n >= 0 && n >= nfield - D; n--) mbar_wait_bounded(&full[n % D], (unsigned)((n / D) & 1));
 }
 
 // The first launch of a stage: fused RHS evaluation and stage update of momentum and temperature
