@@ -6,21 +6,24 @@
 // cUranusModel.cpp:1276-1290.
 //
 // Every (j, k) column is independent. One warp takes one column and keeps its state in its own
-// slice of shared memory (16 values and 4 flags per level): the lanes load, convert and write back
-// the levels in parallel, and run in parallel everything of a sweep that does not depend on what
-// the sweep has done before it:
+// slice of shared memory (16 values and 4 flags per level, two parcel slots): the lanes load,
+// convert and write back the levels in parallel, and run in parallel everything of a sweep that
+// does not depend on what the sweep has done before it:
 //   * at the start of each sweep every pair test (i, i+1) is evaluated, one pair per lane; while
-//     the sweep walks up the column a pair is re-tested (by lane 0) only if one of its two cells
-//     has been mixed in this sweep, which is exactly when its inputs differ from the start's (the
-//     reference's first sweep makes the same reuse with its cached test of untouched pairs);
-//   * a segment's mass-weighted means are summed by lane 0 in the reference's order, and each of
-//     its cells is then brought to equilibrium by its own lane;
-//   * the two growth tests of a segment (below and above) run on lanes 0 and 1.
-// Each test solves a cell's equilibrium by Illinois regula falsi, so the arithmetic is FP64
-// whatever the storage (FP32 storage in the mixed form is widened, T read as its FP32 pair). The
-// solve, the test, the settle, the energy balance and the enthalpy inverse are out-of-line
-// functions: inlined at each call site the kernel's code outgrew the instruction cache and most
-// issue slots went unused for want of an instruction.
+//     the sweep walks up the column a pair is re-tested only if one of its two cells has been
+//     mixed in this sweep, which is exactly when its inputs differ from the start's (the
+//     reference's first sweep makes the same reuse with its cached test of untouched pairs); the
+//     re-test's two equilibria (the parcel, the upper cell's own) are solved on two lanes at once;
+//   * a segment's mass-weighted means are summed by lane 0 in the reference's order; then one
+//     round of equilibria settles each of its cells on its own lane and, on further lanes, solves
+//     what the two growth tests (below and above) need, since none of those solves reads another's
+//     result (the lower neighbour lifted to the segment's bottom level, the mixed top cell lifted
+//     to the level above, that level's own equilibrium); the tests' decisions follow.
+// Each solve is a cell's equilibrium by Illinois regula falsi, so the arithmetic is FP64 whatever
+// the storage (FP32 storage in the mixed form is widened, T read as its FP32 pair). The solve, the
+// decision, the energy balance and the enthalpy inverse are out-of-line functions, and every round
+// reaches the solve through one call site: inlined at each call site the kernel's code outgrew the
+// instruction cache and most issue slots went unused for want of an instruction.
 // Every loop is bounded: 60 regula-falsi steps, 30 Newton steps of the enthalpy inverse, 64
 // sweeps, and a segment grows by one level per step within the column.
 #pragma once
@@ -146,20 +149,22 @@ static __device__ __noinline__ bool mca_equil(const McaConst& A, double hL, cons
 struct McaCol {
     double *T, *p, *z, *rho, *w, *hL, *qr, *Teq;   // im each
     double *qt, *ceq;                              // im * MCA_NG each
+    double *par;                                   // two parcel results: T, condensate[4], solved
     unsigned char *touched, *eq_ok, *mod, *U;      // im each: mixed ever, equilibrium cached,
                                                    // mixed in this sweep, the pair test of the sweep's start
 };
+constexpr int MCA_PAR = 6;                         // doubles per parcel slot
 // Bytes of one warp's slice for a column of im levels; a block's slices share at most MCA_SMEM_MAX.
 constexpr size_t MCA_SMEM_MAX = 227 * 1024;
 __host__ __device__ inline size_t mca_warp_bytes(int im){
-    return (size_t)(16 * im) * sizeof(double) + (((size_t)4 * im + 7) / 8) * 8;
+    return (size_t)(16 * im + 2 * MCA_PAR) * sizeof(double) + (((size_t)4 * im + 7) / 8) * 8;
 }
 __device__ inline McaCol mca_col(char* base, int im){
     McaCol C;
     double* d = reinterpret_cast<double*>(base);
     C.T = d; C.p = d + im; C.z = d + 2 * im; C.rho = d + 3 * im; C.w = d + 4 * im; C.hL = d + 5 * im;
-    C.qr = d + 6 * im; C.Teq = d + 7 * im; C.qt = d + 8 * im; C.ceq = d + 12 * im;
-    unsigned char* f = reinterpret_cast<unsigned char*>(d + 16 * im);
+    C.qr = d + 6 * im; C.Teq = d + 7 * im; C.qt = d + 8 * im; C.ceq = d + 12 * im; C.par = d + 16 * im;
+    unsigned char* f = reinterpret_cast<unsigned char*>(d + 16 * im + 2 * MCA_PAR);
     C.touched = f; C.eq_ok = f + im; C.mod = f + 2 * im; C.U = f + 3 * im;
     return C;
 }
@@ -174,16 +179,17 @@ static __device__ double mca_tv(const McaConst& A, const McaCol& C, double TT, c
     return TT * f;
 }
 
-// :627-644: is the pair (a, b = a+1) unstable? Caches b's equilibrium (written by this lane only:
-// each cell is the upper cell of one pair).
-static __device__ __noinline__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
+// The equilibrium of cell a's state (hL, qt, NH4SH) at level b's pressure and height: the parcel
+// of a pair test (a below b), or a cell's own (a = b).
+__device__ __forceinline__ bool mca_solve_at(const McaConst& A, const McaCol& C, int a, int b, double& T, double* c){
+    return mca_equil(A, C.hL[a] + mca_trE(A, C, a), &C.qt[a * MCA_NG], C.p[b], C.z[b], T, c);
+}
+
+// :627-644, the test of the pair (a, b = a+1) once both equilibria are known: the parcel (cell a at
+// b's level: Tp, pc) against cell b's cached equilibrium.
+static __device__ __noinline__ bool mca_decide(const McaConst& A, const McaCol& C, double Tp, const double* pc, int a, int b){
     const double tol_K = 1.0e-7;
-    double Tp, pc[MCA_NG], pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
-    if(!mca_equil(A, C.hL[a] + mca_trE(A, C, a), &C.qt[a * MCA_NG], C.p[b], C.z[b], Tp, pc)) return false;
-    if(!C.eq_ok[b]){
-        if(!mca_equil(A, C.hL[b] + mca_trE(A, C, b), &C.qt[b * MCA_NG], C.p[b], C.z[b], C.Teq[b], &C.ceq[b * MCA_NG])) return false;
-        C.eq_ok[b] = 1;
-    }
+    double pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
     const double Tb = C.Teq[b];
     for(int g = 0; g < MCA_NG; g++) ec[g] = C.ceq[b * MCA_NG + g];
     for(int g = 0; g < MCA_NG; g++){ pv[g] = C.qt[a * MCA_NG + g] - pc[g]; ev[g] = C.qt[b * MCA_NG + g] - ec[g]; }
@@ -191,22 +197,55 @@ static __device__ __noinline__ bool mca_unstable(const McaConst& A, McaCol& C, i
     return dTv > tol_K;
 }
 
-// :645-661, cell q to equilibrium from hL / qt; the vapour and the condensate's phase split are
-// rebuilt from qt, ceq and T at write-back (qv = qt - ceq; ceq is liquid at T >= t_0, else ice)
-static __device__ __noinline__ bool mca_settle(const McaConst& A, McaCol& C, int q){
-    double TT, pc[MCA_NG];
-    if(!mca_equil(A, C.hL[q] + mca_trE(A, C, q), &C.qt[q * MCA_NG], C.p[q], C.z[q], TT, pc)) return false;
-    C.T[q] = TT;
-    C.Teq[q] = TT; C.eq_ok[q] = 1;
-    for(int g = 0; g < MCA_NG; g++) C.ceq[q * MCA_NG + g] = pc[g];
-    C.touched[q] = 1;
-    return true;
+// The whole test of the pair (a, b) on one lane: the parcel, b's equilibrium if not cached (written
+// by this lane only: each cell is the upper cell of one pair), the decision.
+static __device__ __noinline__ bool mca_unstable(const McaConst& A, McaCol& C, int a, int b){
+    double Tp, pc[MCA_NG];
+    if(!mca_solve_at(A, C, a, b, Tp, pc)) return false;
+    if(!C.eq_ok[b]){
+        if(!mca_solve_at(A, C, b, b, C.Teq[b], &C.ceq[b * MCA_NG])) return false;
+        C.eq_ok[b] = 1;
+    }
+    return mca_decide(A, C, Tp, pc, a, b);
+}
+
+// One round of equilibria across the warp, task t on lane t mod 32, every solve through one call
+// site so that the lanes run it together. Tasks 0 .. nset-1 settle the segment cells lo .. lo+nset-1
+// at their own levels (:645-661: T, the cached equilibrium, touched); the parcel tasks (cell ca
+// lifted to level lb, result in parcel slot s) and the own-equilibrium task (cell own, if not
+// cached) follow. Returns false on the lanes whose settle failed.
+__device__ __forceinline__ bool mca_round(const McaConst& A, McaCol& C, int lane, int lo, int nset,
+                                          int ca0, int lb0, int ca1, int lb1, int own){
+    const int ntask = nset + 3;
+    bool sok = true;
+    for(int t = lane; t < ntask; t += 32){
+        int ca, lb, slot = -1;
+        if(t < nset){ ca = lb = lo + t; }
+        else if(t == nset){ if(ca0 < 0) continue; ca = ca0; lb = lb0; slot = 0; }
+        else if(t == nset + 1){ if(ca1 < 0) continue; ca = ca1; lb = lb1; slot = 1; }
+        else { if(own < 0 || C.eq_ok[own]) continue; ca = lb = own; }
+        double* To = slot < 0 ? &C.Teq[lb] : &C.par[slot * MCA_PAR];
+        double* co = slot < 0 ? &C.ceq[lb * MCA_NG] : &C.par[slot * MCA_PAR + 1];
+        const bool ok = mca_solve_at(A, C, ca, lb, *To, co);
+        if(slot >= 0) C.par[slot * MCA_PAR + 5] = ok ? 1.0 : 0.0;
+        else if(ok){ C.eq_ok[lb] = 1; if(t < nset){ C.T[lb] = C.Teq[lb]; C.touched[lb] = 1; } }
+        else if(t < nset) sok = false;
+    }
+    return sok;
+}
+// The decision of a pair whose parcel is in slot s and whose upper cell's equilibrium is cached.
+__device__ __forceinline__ bool mca_slot_unstable(const McaConst& A, const McaCol& C, int s, int a, int b){
+    return C.par[s * MCA_PAR + 5] != 0.0 && C.eq_ok[b] && mca_decide(A, C, C.par[s * MCA_PAR], &C.par[s * MCA_PAR + 1], a, b);
 }
 
 // One warp per (j, k) column (blockDim = (32, W)), k over all km stored meridians as the reference
-// loops; the warp's slice of dynamic shared memory holds the column.
+// loops; the warp's slice of dynamic shared memory holds the column. The arguments stay in the
+// constant bank (__grid_constant__): the out-of-line helpers take the constants by reference, which
+// otherwise copies the whole argument block to every thread's stack and reads it from there. Six
+// resident blocks per SM (80 registers, the sweep's bookkeeping partly spilled to L1) measured 7 %
+// faster than four at 128 registers.
 template <typename S>
-__global__ void __launch_bounds__(128) mca_warp_kernel(McaArgs<S> a){
+__global__ void __launch_bounds__(128, 6) mca_warp_kernel(const __grid_constant__ McaArgs<S> a){
     extern __shared__ __align__(16) char mca_smem[];
     const Grid& g = a.g;
     const McaConst& A = a.c;
@@ -270,8 +309,11 @@ __global__ void __launch_bounds__(128) mca_warp_kernel(McaArgs<S> a){
             bool uns;
             if(!C.mod[i] && !C.mod[i + 1]) uns = C.U[i] != 0;
             else {
+                // re-test: the parcel (lane 0) and cell i+1's own equilibrium (lane 1) in one round
+                mca_round(A, C, lane, i, 0, i, i + 1, -1, -1, i + 1);
+                __syncwarp();
                 int u = 0;
-                if(lane == 0) u = mca_unstable(A, C, i, i + 1) ? 1 : 0;
+                if(lane == 0) u = mca_slot_unstable(A, C, 0, i, i + 1) ? 1 : 0;
                 u = __shfl_sync(FULL, u, 0);
                 uns = u != 0;
                 __syncwarp();
@@ -295,21 +337,25 @@ __global__ void __launch_bounds__(128) mca_warp_kernel(McaArgs<S> a){
                 m_h = __shfl_sync(FULL, m_h, 0);
                 for(int s = 0; s < MCA_NG; s++) m_q[s] = __shfl_sync(FULL, lane == 0 ? m_q[s] : 0.0, 0);
                 m_r = __shfl_sync(FULL, m_r, 0);
-                bool sok = true;
                 for(int q = lo + lane; q <= hi; q += 32){
                     C.hL[q] = m_h;
                     for(int s = 0; s < MCA_NG; s++) C.qt[q * MCA_NG + s] = m_q[s];
                     C.qr[q] = m_r;
                     C.mod[q] = 1;
-                    if(!mca_settle(A, C, q)) sok = false;
                 }
+                __syncwarp();
+                // one round: the segment's settles and the two growth tests' solves (cell lo-1
+                // lifted to level lo, the mixed cell hi lifted to level hi+1, cell hi+1's own),
+                // none of which depends on another; the decisions follow from the results
+                const bool below = lo > i0, above = hi < i1;
+                const bool sok = mca_round(A, C, lane, lo, hi - lo + 1, below ? lo - 1 : -1, lo,
+                                           above ? hi : -1, hi + 1, above ? hi + 1 : -1);
                 fail = !__all_sync(FULL, sok);
                 __syncwarp();
                 if(fail) break;
-                // the two growth tests, below on lane 0 and above on lane 1
                 int gr = 0;
-                if(lane == 0 && lo > i0) gr = mca_unstable(A, C, lo - 1, lo) ? 1 : 0;
-                if(lane == 1 && hi < i1) gr = mca_unstable(A, C, hi, hi + 1) ? 2 : 0;
+                if(lane == 0 && below) gr = mca_slot_unstable(A, C, 0, lo - 1, lo) ? 1 : 0;
+                if(lane == 1 && above) gr = mca_slot_unstable(A, C, 1, hi, hi + 1) ? 2 : 0;
                 gr = __reduce_or_sync(FULL, (unsigned)gr);
                 __syncwarp();
                 if(gr & 1) lo--;
