@@ -155,7 +155,7 @@ int launch_turb_impl(const TurbArgs<S>& a, cudaStream_t st){
 // The precipitation (precip.cuh): one thread per column; returns the number of launches.
 template <typename S>
 int launch_precip_impl(const PrecipArgs<S>& a, cudaStream_t st){
-    precip_kernel<S><<<dim3((a.g.km + 31) / 32, a.g.jm), dim3(32, 4), 0, st>>>(a);
+    precip_kernel<S><<<dim3((a.g.km + 31) / 32, a.g.jm), 128, 0, st>>>(a);
     return 1;
 }
 // The moist convective adjustment (mca.cuh): one warp per column, W warps per block, W = 4 halved

@@ -3,16 +3,18 @@
 // (cUranusModel.h:280-297), no land cells.
 //
 // Each (j, k) column walks the levels top down (the scheme is a downward sweep: each level's
-// collection and phase-change terms read the fluxes the level above produced), one warp per
-// species over 32 adjacent columns, the species' rain / snow / graupel fluxes in registers. Per
-// cell Q_precip is written once, as the reference's sum over the species in its order (H2O, NH3,
-// CH4, H2S), with the twelve S_precip_* (or, with the coupling off, the condensate fields in
-// place); the lid row and every S field the call does not fill are written with the zeros the
-// reference's first pass puts there, so nothing is launched besides this kernel. The fluxes
-// themselves, the NH4SH settling flux and the surface maps are diagnostics and are not stored.
-// Adjacent lanes take adjacent k, so every load and store of a level is coalesced; the work is
-// per-cell FP64 arithmetic with an exp and a log per species and level (two pow where rain falls)
-// on ~16 values read and ~13 written.
+// collection and phase-change terms read the fluxes the level above produced). Four adjacent lanes
+// take the four species of one column, each with its rain / snow / graupel fluxes in registers, so
+// a warp runs 8 adjacent columns and a block of 128 threads 32, with no barrier: per level the
+// lane of H2O gathers the other three species' latent heating by shuffles and writes Q_precip once,
+// summed in the reference's order (H2O, NH3, CH4, H2S), and each lane writes its species' three
+// S_precip_* (or, with the coupling off, its condensate fields in place); the lid row and every S
+// field the call does not fill are written with the zeros the reference's first pass puts there,
+// so nothing is launched besides this kernel. The fluxes themselves, the NH4SH settling flux and
+// the surface maps are diagnostics and are not stored. The 8 lanes of one species take 8 adjacent
+// k, so every load and store of a level covers whole 32-byte sectors; the work is per-cell FP64
+// arithmetic with an exp and a log per species and level (two pow where rain falls) on ~16 values
+// read and ~13 written.
 #pragma once
 #include "common.cuh"
 
@@ -40,17 +42,13 @@ struct PrecipArgs {
 __device__ __forceinline__ double pr_max(double a, double b){ return (a < b) ? b : a; }   // std::max
 __device__ __forceinline__ double pr_min(double a, double b){ return (b < a) ? b : a; }   // std::min
 
-// One block = 32 columns (adjacent k) x the four species: warp n runs species n down the 32
-// columns, its three fluxes in registers; per level the warps of NH3, CH4 and H2S leave their
-// latent heating in shared memory (double-buffered by level) and the H2O warp adds them to its own
-// in the reference's order, and writes Q_precip.
+// Lane 4c + n of a warp: species n of the warp's column c (k = 8 * warp + c of the block's 32).
 template <typename S>
-__global__ void __launch_bounds__(128) precip_kernel(PrecipArgs<S> a){
-    __shared__ double qs[2][3][32];
-    __shared__ unsigned char qon[2][3][32];
+__global__ void __launch_bounds__(128) precip_kernel(const __grid_constant__ PrecipArgs<S> a){
     const Grid& g = a.g;
-    const int lane = threadIdx.x, n = threadIdx.y;
-    const int k = blockIdx.x * 32 + lane, j = blockIdx.y;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, n = lane & 3;
+    const int k = blockIdx.x * 32 + (threadIdx.x >> 5) * 8 + (lane >> 2), j = blockIdx.y;
     const bool kin = k < g.km;
     const size_t pl = (size_t)g.jm * g.kp;
     const size_t o = gidx(g, 0, j, kin ? k : 0);
@@ -74,7 +72,6 @@ __global__ void __launch_bounds__(128) precip_kernel(PrecipArgs<S> a){
         sv[q] = (S)0.0; sc[q] = (S)0.0; si[q] = (S)0.0;
     }
     for(int i = g.im - 2; i >= 0; i--){
-        const int b = i & 1;
         const size_t q = o + (size_t)i * pl;
         const double dz = pr_max(0.0, a.dz[i]);
         double term = 0.0;
@@ -140,13 +137,15 @@ __global__ void __launch_bounds__(128) precip_kernel(PrecipArgs<S> a){
                 Pg = pr_min(P_max_flux, pr_max(0.0, F_g));
             }
         }
-        if(n > 0){ qs[b][n - 1][lane] = term; qon[b][n - 1][lane] = added ? 1 : 0; }
-        __syncthreads();
+        // Q_precip zeroed by the first pass, then each species' += in the reference's order
+        const double t1 = __shfl_down_sync(FULL, term, 1), t2 = __shfl_down_sync(FULL, term, 2), t3 = __shfl_down_sync(FULL, term, 3);
+        const unsigned on_mask = __ballot_sync(FULL, added);
         if(n == 0 && kin){
-            // Q_precip zeroed by the first pass, then each species' += in the reference's order
             double Qc = 0.0;
             if(added) Qc += term;
-            for(int m = 0; m < 3; m++) if(qon[b][m][lane]) Qc += qs[b][m][lane];
+            if(on_mask & (1u << (lane + 1))) Qc += t1;
+            if(on_mask & (1u << (lane + 2))) Qc += t2;
+            if(on_mask & (1u << (lane + 3))) Qc += t3;
             a.Q[q] = (S)Qc;
         }
     }

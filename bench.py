@@ -427,12 +427,12 @@ def iteration_timing(api, P, S, torch, precision, pa, iters=8):
     return out
 
 
-def mca_timing(api, P, S, torch, reps=3):
-    """aturan_mca (FP64, default knobs) at 41x181x361 on a seeded synthetic state in which most
-    columns are unstable: device time of one call on the freshly uploaded state (CUDA events on the
-    context's stream, median of `reps`, after one warm-up call), and the compiled reference's same
-    call on the host cores when it is present."""
-    p = P.default_params()
+def mca_timing(api, P, S, torch, reps=3, grid=(41, 181, 361), reference=True):
+    """aturan_mca (FP64, default knobs) on a seeded synthetic state in which most columns are
+    unstable: device time of one call on the freshly uploaded state (CUDA events on the context's
+    stream, median of `reps`, after one warm-up call), and the compiled reference's same call on
+    the host cores when it is present (full grid only)."""
+    p = P.default_params(*grid)
     st = S.synthetic_state(p, seed=72)
     ctx = api.Context(p)
     s = torch.cuda.ExternalStream(ctx.stream)
@@ -449,7 +449,9 @@ def mca_timing(api, P, S, torch, reps=3):
             ms.append(e0.elapsed_time(e1))
     ctx.close()
     out = {"ms": statistics.median(ms), "columns": p.jm * p.km,
-           "what": "moist convective adjustment, FP64, 41x181x361, synthetic state (seed 72), one call per upload"}
+           "what": "moist convective adjustment, FP64, %dx%dx%d, synthetic state (seed 72), one call per upload" % grid}
+    if not reference:
+        return out
     try:
         from oracle import ref as R
         if R.available():
@@ -642,7 +644,9 @@ def main():
     from aturan_b200 import api, params as P, replicas, state as S
     if args.mca:
         if rank == 0:
-            print(json.dumps({"mca": mca_timing(api, P, S, torch)}), flush=True)
+            grid = tuple(int(x) for x in args.grid.lower().split("x"))
+            print(json.dumps({"mca": mca_timing(api, P, S, torch, grid=grid,
+                                                reference=grid == (41, 181, 361))}), flush=True)
         return
     if args.poisson:
         if rank == 0:
