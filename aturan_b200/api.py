@@ -53,6 +53,8 @@ SIGNATURES = {
     "aturan_rk4_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "aturan_rk4_adjoint_ex": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                ctypes.c_void_p], ctypes.c_int),
+    "aturan_moist_adjoint": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_void_p], ctypes.c_int),
     "aturan_set_heating": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "aturan_pressure_adjoint": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
@@ -281,8 +283,10 @@ class Context:
         return nf.value, nd.value
 
     def tape(self, on=True):
-        """aturan_tape: keep (or free) what aturan_rk4_adjoint needs from the following RK4 steps."""
-        self._check(self.L.aturan_tape(self.h, 1 if on else 0), "tape")
+        """aturan_tape: keep (or free) what the adjoint needs from the following RK4 steps; on=True
+        or 1 the dry tape (aturan_rk4_adjoint), 2 the moist tape (aturan_moist_adjoint)."""
+        mode = 0 if not on else (2 if on == 2 else 1)
+        self._check(self.L.aturan_tape(self.h, mode), "tape")
 
     def rk4_adjoint(self, ybar_ptrs, xbar_ptrs):
         """aturan_rk4_adjoint on device pointers (t, u, v, w order) to contiguous FP64 arrays."""
@@ -297,6 +301,16 @@ class Context:
         ab = (ctypes.c_void_p * 3)(*[ctypes.c_void_p(int(x)) for x in auxbar_ptrs]) if auxbar_ptrs else None
         opt = lambda x: ctypes.c_void_p(int(x)) if x else None
         self._check(self.L.aturan_rk4_adjoint_ex(self.h, yb, ab, xb, opt(pbar_ptr), opt(heatbar_ptr)), "rk4_adjoint_ex")
+
+    def moist_adjoint(self, ybar_ptrs, auxbar_ptrs, xbar_ptrs, pbar_ptr, heatbar_ptr=None):
+        """aturan_moist_adjoint: ybar_ptrs / xbar_ptrs 16 device pointers (t, u, v, w and the twelve
+        condensable species in field order); auxbar_ptrs (3, or None) in; pbar_ptr, heatbar_ptr (or
+        None) out."""
+        yb = (ctypes.c_void_p * 16)(*[ctypes.c_void_p(int(x)) for x in ybar_ptrs])
+        xb = (ctypes.c_void_p * 16)(*[ctypes.c_void_p(int(x)) for x in xbar_ptrs])
+        ab = (ctypes.c_void_p * 3)(*[ctypes.c_void_p(int(x)) for x in auxbar_ptrs]) if auxbar_ptrs else None
+        opt = lambda x: ctypes.c_void_p(int(x)) if x else None
+        self._check(self.L.aturan_moist_adjoint(self.h, yb, ab, xb, opt(pbar_ptr), opt(heatbar_ptr)), "moist_adjoint")
 
     def set_heating(self, ptr, on_device=True):
         """aturan_set_heating: a [jm][km] FP64 heating rate in K/s (device or host pointer), None removes it."""

@@ -20,7 +20,7 @@ _RESTORE = ("p_bfollow",)
 class DryStepper:
     """Holds an FP64 aturan_b200.api.Context and the fixed inputs of the step."""
 
-    def __init__(self, ctx):
+    def __init__(self, ctx, tape=True):
         if not torch.cuda.is_available():
             raise RuntimeError("DryStepper needs a CUDA device")
         self.ctx = ctx
@@ -30,7 +30,8 @@ class DryStepper:
         torch.cuda.synchronize()
         for n, t in self.saved.items():
             ctx.download_device(n, t.data_ptr())
-        ctx.tape(True)
+        if tape:
+            ctx.tape(True)
 
     def forward(self, xs):
         ctx = self.ctx
@@ -76,6 +77,7 @@ class DryRK4Step(torch.autograd.Function):
 
 
 assert all(n in F.ID for n in DRY + tuple(n + "n" for n in DRY) + _RESTORE)
+assert tuple(F.PROGNOSTIC[:4]) == DRY
 
 
 AUX = ("aux_u", "aux_v", "aux_w")
@@ -91,8 +93,8 @@ class DryFullStepper(DryStepper):
     outputs' adjoint entering at stage 3), then aturan_pressure_adjoint (p_dyn's adjoint back to
     the aux inputs'). Only the aux interior enters the next solve; boundary rows get no gradient."""
 
-    def __init__(self, ctx, kind=3, omega=1.0, max_sweeps=200, tol=1e-10):
-        super().__init__(ctx)
+    def __init__(self, ctx, kind=3, omega=1.0, max_sweeps=200, tol=1e-10, tape=True):
+        super().__init__(ctx, tape)
         self.press = (kind, omega, max_sweeps, tol)
         self.zero = torch.zeros(self.shape, dtype=torch.float64, device="cuda")
 
@@ -159,7 +161,78 @@ class DryFullStep(torch.autograd.Function):
         return (None, *xbar, *abar)
 
 
-def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn, heat=None):
+MOIST = tuple(F.PROGNOSTIC[:16])           # t, u, v, w and the twelve condensable species
+
+
+class MoistFullStepper(DryFullStepper):
+    """One full moist step in the reference's order, the saturation adjustment inside:
+    (t, u, v, w, twelve condensable species, aux_u, aux_v, aux_w) -> the same after it. The step
+    solves the pressure equation from the aux fields (from p_dyn = 0), adjusts the four gases
+    (aturan_satadj), sets the start-of-step copies to the adjusted state (aturan_sync_ncopies) and
+    runs the RK4 step. Backward: aturan_moist_adjoint (the RK4 step's adjoint over the sixteen
+    fields, then the adjustment's implicit adjoint), then aturan_pressure_adjoint. The other scalar
+    fields (NH4SH, k, epsilon), p_stat, the forcing and the hydrostatic split are held at the
+    context's values. tape=False makes a forward-only stepper, e.g. on a mixed-precision context
+    (rollout_gradient's forward_stepper)."""
+
+    def __init__(self, ctx, kind=3, omega=1.0, max_sweeps=200, tol=1e-10, tape=True):
+        super().__init__(ctx, kind, omega, max_sweeps, tol, tape=False)
+        if tape:
+            ctx.tape(2)
+        self.others = {n: torch.empty(self.shape, dtype=torch.float64, device="cuda")
+                       for n in F.PROGNOSTIC[16:]}
+        torch.cuda.synchronize()
+        for n, t in self.others.items():
+            ctx.download_device(n, t.data_ptr())
+
+    def forward(self, xs, aux, heat=None):
+        ctx = self.ctx
+        xs = [x.detach().contiguous() for x in xs]
+        aux = [a.detach().contiguous() for a in aux]
+        if heat is not None:
+            heat = heat.detach().contiguous()
+        torch.cuda.synchronize()
+        ctx.set_heating(heat.data_ptr() if heat is not None else None)
+        self.heated = heat is not None
+        for n, t in self.saved.items():
+            ctx.upload_device(n, t.data_ptr())
+        for n, t in self.others.items():
+            ctx.upload_device(n, t.data_ptr())
+        ctx.upload_device("p_dyn", self.zero.data_ptr())
+        for n, x in zip(MOIST, xs):
+            ctx.upload_device(n, x.data_ptr())
+        for n, a in zip(AUX, aux):
+            ctx.upload_device(n, a.data_ptr())
+        ctx.restore_ncopies(1.0)               # every start-of-step copy is the step's input
+        kind, omega, ms, tol = self.press
+        ctx.pressure(kind, omega=omega, max_sweeps=ms, tol=tol)
+        ctx.satadj(0xF, count=False)
+        ctx.sync_ncopies()                     # the adjusted scalars' copies (RK_SCALAR_SYNC)
+        ctx.rk4_step()
+        self.n_forward += 1
+        out = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in MOIST + AUX]
+        for n, o in zip(MOIST + AUX, out):
+            ctx.download_device(n, o.data_ptr())
+        return out[:16], out[16:]
+
+    def backward(self, ybar, auxbar):
+        z = lambda g: torch.zeros(self.shape, dtype=torch.float64, device="cuda") if g is None else g.contiguous()
+        ybar = [z(g) for g in ybar]
+        auxbar = [z(g) for g in auxbar]
+        xbar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in MOIST]
+        pbar = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        abar = [torch.empty(self.shape, dtype=torch.float64, device="cuda") for _ in AUX]
+        hbar = torch.empty(self.shape[1:], dtype=torch.float64, device="cuda") if self.heated else None
+        torch.cuda.synchronize()
+        self.ctx.moist_adjoint([g.data_ptr() for g in ybar], [g.data_ptr() for g in auxbar],
+                               [x.data_ptr() for x in xbar], pbar.data_ptr(),
+                               hbar.data_ptr() if hbar is not None else None)
+        kind, omega, ms, tol = self.press
+        self.ctx.pressure_adjoint(pbar.data_ptr(), [a.data_ptr() for a in abar], kind, omega, ms, tol)
+        return (xbar, abar) if hbar is None else (xbar, abar, hbar)
+
+
+def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn, heat=None, forward_stepper=None):
     """Loss after nsteps DryFullStepper steps from (xs0, aux0) and its gradient with respect to
     xs0 and aux0, by the hand-written adjoint with checkpointing: the forward keeps the inputs of
     every `every`-th step; the backward recomputes a segment's step inputs from its checkpoint,
@@ -167,12 +240,17 @@ def rollout_gradient(stepper, xs0, aux0, nsteps, every, loss_fn, heat=None):
     (nsteps / every + every) step inputs; cost about three forward passes plus the adjoints.
     loss_fn maps the final (t, u, v, w) to a scalar tensor (differentiated by torch.autograd).
     With heat (a [jm][km] heating rate held over the trajectory) the gradient with respect to it,
-    summed over the steps, is returned too."""
+    summed over the steps, is returned too.
+    forward_stepper (e.g. a forward-only MoistFullStepper on a mixed-precision context) runs the
+    trajectory itself: the loss and the checkpoints are its, while each segment is recomputed from
+    its checkpoint, taped and reversed by `stepper` (FP64): the adjoint of the mixed trajectory
+    linearised about FP64 steps restarted from its checkpoints."""
+    fwd = forward_stepper if forward_stepper is not None else stepper
     ck = {0: ([x.detach() for x in xs0], [a.detach() for a in aux0])}
     xs, aux = ck[0]
     with torch.no_grad():
         for n in range(nsteps):
-            xs, aux = stepper.forward(xs, aux, heat)
+            xs, aux = fwd.forward(xs, aux, heat)
             if (n + 1) % every == 0 and n + 1 < nsteps:
                 ck[n + 1] = (xs, aux)
     xf = [x.detach().requires_grad_(True) for x in xs]

@@ -20,6 +20,7 @@
 #pragma once
 #include "common.cuh"
 #include "rk4.cuh"
+#include "satadj.cuh"
 
 namespace aturan {
 
@@ -27,6 +28,14 @@ constexpr int ADJ_NF = 4;                          // t, u, v, w (state fields 0
 constexpr int ADJ_SLOT_PH = 7 * ADJ_NF;            // p_hydro tp, tm, pe, pw
 constexpr int ADJ_SLOT_PD = ADJ_SLOT_PH + 4;       // p_dyn rp, rm, tp, tm, pe, pw
 constexpr int ADJ_SLOTS = ADJ_SLOT_PD + 6;         // per field rp, rm, tp, tm, pe, pw, c; then p_hydro, p_dyn
+// The moist form: the twelve condensable species (state fields 4..15, ATURAN_CH4 .. ATURAN_NH3_ICE)
+// join the dry four, their seven slots each after the dry layout.
+constexpr int ADJ_NF_MOIST = 16;
+constexpr int ADJ_NSP = ADJ_NF_MOIST - ADJ_NF;
+constexpr int ADJ_SLOTS_MOIST = ADJ_SLOTS + 7 * ADJ_NSP;
+__host__ __device__ constexpr size_t adj_slot_base(int q){
+    return q < ADJ_NF ? (size_t)q * 7 : (size_t)ADJ_SLOTS + (size_t)(q - ADJ_NF) * 7;
+}
 
 struct AdjArgs {
     Grid g;
@@ -197,12 +206,250 @@ __global__ void __launch_bounds__(128) adj_local_kernel(const AdjArgs a){
     Q[5 * fs] = -gdp * K.inv_2dphi;           // to (k-1)
 }
 
+// The twelve condensable species' tendencies (RHS_Uran_Turb.cpp:790-850, scalar_rhs in rk4.cuh):
+// rhs_q = -(u d1r + v/r d1t + w/(r sin) d1p)(q) + D_q lap(q) + forcing, D_q = 1/(Sc_g Re) + nue_t/0.9,
+// the forcing (precipitation sources, mass fluxes) held fixed. Per interior cell and species: the
+// seven stencil contributions into the species' slots, and the transport's partials in u, v, w
+// added to the centre slots of u, v, w that adj_local_kernel wrote (same cell, same thread, the
+// next launch on the stream). a.X, a.X0, a.kbar hold ADJ_NF_MOIST fields.
+__global__ void __launch_bounds__(128) adj_species_local_kernel(const AdjArgs a){
+    const Grid& g = a.g;
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = 1 + blockIdx.y * 4 + threadIdx.y;
+    const int i = 1 + blockIdx.z;
+    if(k > g.km - 2 || j > g.jm - 2 || i > g.im - 2) return;
+    const RhsConst<double>& K = a.k;
+    const GeoIJ<double> geo = a.geo[i * g.jm + j];
+    Nbr<double> nb;
+    nb.fs  = g.fstride;
+    nb.o   = gidx(g, i, j, k);
+    nb.oim = nb.o - (size_t)g.jm * g.kp; nb.oip = nb.o + (size_t)g.jm * g.kp;
+    nb.ojm = nb.o - g.kp;                nb.ojp = nb.o + g.kp;
+    nb.okw = nb.o - k + phi_wrap(k - 1, g.km);
+    nb.oke = nb.o - k + phi_wrap(k + 1, g.km);
+    nb.X   = a.X;
+    nb.xim = (i == 1) ? a.X0 : a.X;
+    nb.xip = (i == g.im - 2) ? a.X0 : a.X;
+    nb.xjm = (j == 1) ? a.X0 : a.X;
+    nb.xjp = (j == g.jm - 2) ? a.X0 : a.X;
+    const size_t o = nb.o, fs = g.fstride;
+    const double u = a.X[1 * fs + o], v = a.X[2 * fs + o], w = a.X[3 * fs + o];
+    const double nue_c = ld(a.forc + o);
+    const double nue_t = (K.turb_coupling != 0.0 && isfinite(nue_c)) ? K.turb_coupling * cmax(0.0, nue_c) : 0.0;
+    const double nue_t_s = nue_t / 0.9;
+    const double inv_rm = geo.inv_rm, inv_rm2 = geo.inv_rm2, inv_rs = geo.inv_rmsinthe;
+    const double inv_rm2s2 = geo.inv_rm2sinthe2, cir = geo.costhe_inv_rm2sinthe, tir = geo.two_inv_rm;
+    double du = 0.0, dv = 0.0, dw = 0.0;
+    for(int n = 0; n < ADJ_NSP; n++){
+        const int q = ADJ_NF + n;
+        const D6<double> Q = diff6(K, load7<double, double>(nb, q));
+        const double aq = a.kbar[(size_t)q * fs + o];
+        const double Dq = K.inv_sc_re[n / 3] + nue_t_s;
+        G6 gq;
+        gq.d1r = aq * (-u + tir * Dq);           gq.d2r = aq * Dq;
+        gq.d1t = aq * (-v * inv_rm + cir * Dq);  gq.d2t = aq * inv_rm2 * Dq;
+        gq.d1p = aq * (-w * inv_rs);             gq.d2p = aq * inv_rm2s2 * Dq;
+        put7(a.slot + (size_t)ADJ_SLOTS * fs, fs, o, n, gq, 0.0, K);
+        du -= aq * Q.d1r;
+        dv -= aq * inv_rm * Q.d1t;
+        dw -= aq * inv_rs * Q.d1p;
+    }
+    a.slot[(1 * 7 + 6) * fs + o] += du;
+    a.slot[(2 * 7 + 6) * fs + o] += dv;
+    a.slot[(3 * 7 + 6) * fs + o] += dw;
+}
+
+// ---- the saturation adjustment's implicit adjoint ----
+// Per cell the forward (satadj_kernel, SaturationAdjustment.h:255-746) runs the four gases in the
+// loop's order H2O, H2S, NH3, CH4, the temperature carried from one to the next. For one gas every
+// step it takes -- the entry melt (:365-385) and freeze (:388-399), the Newton passes with their
+// Bergeron conversion and in-pass melt (:450-590) -- moves mass between vapour q_v, cloud q_c and
+// ice q_i and heat by the latent heats (L_f = L_s - L_v), so the total W = q_v + q_c + q_i and the
+// moist enthalpy E = h T - L_v q_c - L_s q_i (h = cp_mix rho) are invariant. The converged state
+// is the root of the closure q_v = H(T, q_c, q_i) on that invariant set, with the phases present
+// at convergence frozen (the branch of the forward):
+//   ice only      q_v = q_I(T), q_i = W - q_v              h dT = dE + L_s dW - L_s q_I'(T) dT
+//   liquid only   q_v = q_R(T), q_c = W - q_v              (L_v, q_R likewise)
+//   both          H = r q_R + (1 - r) q_I with the condensate split r = q_c / (q_c + q_i) frozen,
+//                 L = r L_v + (1 - r) L_s
+//   none          q_v = W, T = E / h (everything evaporated)
+// so dT = (dE + L dW) / (h + L H'(T)) and the rest follows; this is the derivative of the exact
+// root, which the forward approaches to its 1e-3 stopping test. A gas the forward leaves alone
+// (no adjustment needed) contributes the derivative of its entry melt / freeze, each linear on its
+// frozen branch (full, or capped at the phase temperature), and of the entry clamps.
+// The temperature entering each gas is reconstructed from the invariants: the gas's entry state
+// (the taped input, then each earlier gas's own entry and result) gives E, and its result gives
+// T = (E + L_v q_c + L_s q_i) / h. The entry logic deciding whether a gas adjusts is the forward's
+// FP64 path restated.
+struct SatEntry {
+    bool skip, go, cneg, clneg, ineg;
+    int melt, freeze;            // 0 none, 1 whole amount, 2 capped at the phase temperature,
+                                 // 3 mass only (L_f <= 0), 4 ice dropped (no conservation: melt only)
+    double t_u, c, cloud, ice;   // after the entry steps and clamps
+};
+
+__device__ __forceinline__ double sat_q_d(const GasConst& G, bool ice, double rho_c, double p_u, double T, double* dq){
+    const double C = ice ? G.C_i : G.C, L0 = ice ? G.L0_i : G.L0;
+    const double al = ice ? G.del_alf_i : G.del_alf, be = ice ? G.del_bet_i : G.del_bet;
+    const double q = rho_c * G.ep * svp(T, C, L0, G.den, al, be) / p_u;
+    if(dq) *dq = q * (L0 / (T * T) + al / T + be) / G.den;
+    return q;
+}
+
+// :358-448 on the FP64 path: the entry steps and the decision to adjust.
+__device__ SatEntry sat_entry(const SatConst& K, const GasConst& G, double rho_c, double p_u, double t_u,
+                              double c, double cloud, double ice){
+    SatEntry e;
+    e.skip = !((t_u > 0.0) && (p_u > 0.0));
+    e.go = false; e.melt = 0; e.freeze = 0; e.cneg = e.clneg = e.ineg = false;
+    e.t_u = t_u; e.c = c; e.cloud = cloud; e.ice = ice;
+    if(e.skip) return e;
+    const double t_0 = G.t_0, t_00 = G.t_00, Lf = G.Lf, hc = K.cp_mix * rho_c;
+    if(t_u > t_0){
+        if(K.conserve){
+            if(ice > 0.0){
+                double dm = ice;
+                if(Lf > 0.0){
+                    const double cap = hc * (t_u - t_0) / Lf;
+                    e.melt = 1;
+                    if(dm > cap){ dm = cap; e.melt = 2; }
+                    t_u -= Lf * dm / hc;
+                } else e.melt = 3;
+                ice -= dm;
+                cloud += dm;
+            }
+        } else { e.melt = 4; ice = 0.0; }
+    }
+    if(G.freeze_on && t_u < t_00 && cloud > 0.0){
+        double dm = cloud;
+        if(Lf > 0.0){
+            const double cap = hc * (t_00 - t_u) / Lf;
+            e.freeze = 1;
+            if(dm > cap){ dm = cap; e.freeze = 2; }
+            t_u += Lf * dm / hc;
+        } else e.freeze = 3;
+        cloud -= dm;
+        ice += dm;
+    }
+    if(c < 0.0){ c = 0.0; e.cneg = true; }
+    if(cloud < 0.0){ cloud = 0.0; e.clneg = true; }
+    if(ice < 0.0){ ice = 0.0; e.ineg = true; }
+    e.t_u = t_u; e.c = c; e.cloud = cloud; e.ice = ice;
+    const double q_Rain_0 = sat_q_d(G, false, rho_c, p_u, t_u, nullptr);
+    bool go = q_Rain_0 > 0.0;
+    if(go){
+        double q_entry = q_Rain_0;
+        if(K.ice_entry && cloud <= 0.0 && ice <= 0.0){
+            const double cnd0 = t_u <= t_00 ? 0.0 : (t_u >= t_0 ? 1.0 : (t_u - t_00) * G.t_range_inv);
+            if(cnd0 < 1.0) q_entry = cnd0 * q_Rain_0 + (1.0 - cnd0) * sat_q_d(G, true, rho_c, p_u, t_u, nullptr);
+        }
+        if(K.bergeron >= 2 && cloud <= 0.0 && ice <= 0.0 && t_u < t_0) q_entry = sat_q_d(G, true, rho_c, p_u, t_u, nullptr);
+        if(c <= q_entry){
+            if(!K.evap || !K.conserve || (cloud <= 0.0 && ice <= 0.0)) go = false;
+            else {
+                const double q_Ice_0 = sat_q_d(G, true, rho_c, p_u, t_u, nullptr);
+                double q_t0;
+                if(cloud > 0.0 && ice > 0.0) q_t0 = (cloud * q_Rain_0 + ice * q_Ice_0) / (cloud + ice);
+                else if(ice <= 0.0)          q_t0 = q_Rain_0;
+                else                         q_t0 = q_Ice_0;
+                if(fabs(c - q_t0) <= 1.0e-3 * q_t0) go = false;
+            }
+        }
+    }
+    e.go = go;
+    return e;
+}
+
+// The entry steps' adjoint: cotangents of (t_u, c, cloud, ice) after them -> before them.
+__device__ void sat_entry_adj(const GasConst& G, double hc, const SatEntry& e, double& Tb, double& cb, double& clb, double& ib){
+    const double Lf = G.Lf;
+    if(e.cneg) cb = 0.0;
+    if(e.clneg) clb = 0.0;
+    if(e.ineg) ib = 0.0;
+    if(e.freeze == 1){ clb = Tb * Lf / hc + ib; }
+    else if(e.freeze == 2){ Tb = (clb - ib) * hc / Lf; }
+    else if(e.freeze == 3){ clb = ib; }
+    if(e.melt == 1){ ib = -Tb * Lf / hc + clb; }
+    else if(e.melt == 2){ Tb = (clb - ib) * hc / Lf; }
+    else if(e.melt == 3){ ib = clb; }
+    else if(e.melt == 4){ ib = 0.0; }
+}
+
+// One cell: ybar (fields 0..15 of the step's RK4 input, i.e. after the adjustment) -> the same
+// before it. pre: the taped state before the adjustment; post: after it (ADJ_NF_MOIST fields each).
+__global__ void __launch_bounds__(128) adj_satadj_kernel(Grid g, const double* pre, const double* post, const double* ps,
+                                                         const double* rho_mix, SatConst K, double* ybar){
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if(k >= g.km) return;
+    const size_t fs = g.fstride, q = gidx(g, i, j, k);
+    const double p_u = ps[q];
+    double rho_c = K.r_mix;                               // rho_at, cUranusModel.h:526-531
+    if(K.local_rho){ const double r_ = rho_mix[q]; rho_c = (r_ > 0.0 && isfinite(r_)) ? r_ : K.r_mix; }
+    const double hc = K.cp_mix * rho_c, t_ref = K.t_ref;
+    const int base[4] = {ATURAN_H2O, ATURAN_H2S, ATURAN_NH3, ATURAN_CH4};
+    // forward replay: each gas's entry record and the temperature after it
+    SatEntry ent[4];
+    double Tout[4];
+    double T = pre[q] * t_ref;
+    for(int gi = 0; gi < 4; gi++){
+        const GasConst& G = K.gas[gi];
+        const size_t f = (size_t)base[gi] * fs + q;
+        ent[gi] = sat_entry(K, G, rho_c, p_u, T, pre[f], pre[f + fs], pre[f + 2 * fs]);
+        const SatEntry& e = ent[gi];
+        if(e.skip){ Tout[gi] = T; continue; }
+        if(e.go){
+            const double E = hc * e.t_u - G.lv * e.cloud - G.ls * e.ice;
+            T = (E + G.lv * post[f + fs] + G.ls * post[f + 2 * fs]) / hc;
+        } else T = e.t_u;
+        Tout[gi] = T;
+    }
+    // reverse
+    double Tb = ybar[q] / t_ref;
+    for(int gi = 3; gi >= 0; gi--){
+        const GasConst& G = K.gas[gi];
+        const size_t f = (size_t)base[gi] * fs + q;
+        const SatEntry& e = ent[gi];
+        if(e.skip) continue;
+        double cb = ybar[f], clb = ybar[f + fs], ib = ybar[f + 2 * fs];
+        if(e.go){
+            const double qc = post[f + fs], qi = post[f + 2 * fs], Tp = Tout[gi];
+            double Eb, Wb;
+            if(qc > 0.0 && qi > 0.0){
+                const double r = qc / (qc + qi), L = r * G.lv + (1.0 - r) * G.ls;
+                double dR, dI;
+                sat_q_d(G, false, rho_c, p_u, Tp, &dR);
+                sat_q_d(G, true, rho_c, p_u, Tp, &dI);
+                const double dH = r * dR + (1.0 - r) * dI, Cb = r * clb + (1.0 - r) * ib;
+                const double a = (Tb + (cb - Cb) * dH) / (hc + L * dH);
+                Eb = a; Wb = a * L + Cb;
+            } else if(qi > 0.0){
+                double dI;
+                sat_q_d(G, true, rho_c, p_u, Tp, &dI);
+                const double a = (Tb + (cb - ib) * dI) / (hc + G.ls * dI);
+                Eb = a; Wb = a * G.ls + ib;
+            } else if(qc > 0.0){
+                double dR;
+                sat_q_d(G, false, rho_c, p_u, Tp, &dR);
+                const double a = (Tb + (cb - clb) * dR) / (hc + G.lv * dR);
+                Eb = a; Wb = a * G.lv + clb;
+            } else {
+                Eb = Tb / hc; Wb = cb;
+            }
+            Tb = Eb * hc; cb = Wb; clb = Wb - G.lv * Eb; ib = Wb - G.ls * Eb;
+        }
+        sat_entry_adj(G, hc, e, Tb, cb, clb, ib);
+        ybar[f] = cb; ybar[f + fs] = clb; ybar[f + 2 * fs] = ib;
+    }
+    ybar[q] = Tb * t_ref;
+}
+
 // Per cell (every row, every meridian; the seam copy k = km-1 is read by no stencil and receives
 // nothing): the sum of what the cells whose stencils contain it sent, in a fixed order. Adds the
 // result into ybar and phbar; for s > 0 also forms the previous stage's kbar on the interior.
 __global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* slot, double* ybar, double* phbar,
                                                          double* pdbar, const double* g0, double* kbar, double w_prev,
-                                                         double c_prev, int has_prev){
+                                                         double c_prev, int has_prev, int nf){
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     const int i = blockIdx.z;
@@ -211,9 +458,8 @@ __global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* s
     const size_t o = gidx(g, i, j, k);
     const size_t okw = o - k + phi_wrap(k - 1, g.km), oke = o - k + phi_wrap(k + 1, g.km);
     const bool interior = i >= 1 && i <= g.im - 2 && j >= 1 && j <= g.jm - 2;
-#pragma unroll
-    for(int q = 0; q < ADJ_NF; q++){
-        const double* S = slot + (size_t)q * 7 * fs;
+    for(int q = 0; q < nf; q++){
+        const double* S = slot + adj_slot_base(q) * fs;
         double x = S[6 * fs + o];
         if(i >= 1)        x += S[0 * fs + o - si];
         if(i <= g.im - 2) x += S[1 * fs + o + si];
@@ -245,7 +491,7 @@ __global__ void __launch_bounds__(128) adj_gather_kernel(Grid g, const double* s
 // The final update's adjoint: g = ybar' (times 0 where T' was clamped), ybar = g, kbar_3 =
 // dt/6 w_3 g on the interior. ybar_in is the caller's adjoint of the step's output.
 __global__ void adj_init_kernel(Grid g, const double* ybar_in, const double* t_out, double t_min, double t_max,
-                                double w3, double* g0, double* ybar, double* kbar, double* phbar, double* pdbar){
+                                double w3, double* g0, double* ybar, double* kbar, double* phbar, double* pdbar, int nf){
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     const int i = blockIdx.z;
@@ -253,8 +499,7 @@ __global__ void adj_init_kernel(Grid g, const double* ybar_in, const double* t_o
     const size_t fs = g.fstride;
     const size_t o = gidx(g, i, j, k);
     const bool interior = i >= 1 && i <= g.im - 2 && j >= 1 && j <= g.jm - 2 && k <= g.km - 2;
-#pragma unroll
-    for(int q = 0; q < ADJ_NF; q++){
+    for(int q = 0; q < nf; q++){
         double v = ybar_in[q * fs + o];
         if(q == 0 && interior && !(t_out[o] > t_min && t_out[o] < t_max)) v = 0.0;
         g0[q * fs + o] = interior ? v : 0.0;

@@ -89,6 +89,10 @@ struct aturan_ctx {
     double *tX, *tTout, *tPd, *tSrc, *tref, *aslot, *aybar, *akbar, *ag0, *aphbar, *arbar, *apdbar, *aaux, *alev;
     bool tape_p_valid;         // a taped RB_SOR / RB_LINE pressure call has run since the tape was switched on
     double* ahacc;             // the T tendencies' adjoint summed over the stages (heating gradient)
+    int tape_nf;               // fields taped per stage: ADJ_NF (dry) or ADJ_NF_MOIST (aturan_tape(ctx, 2))
+    double* tPre;              // moist tape: the state (fields 0..15) before the saturation adjustment
+    bool tape_sat_pending;     // moist tape: an adjustment has recorded its input since the last taped RK4 step
+    bool tape_sat_valid;       // moist tape: the taped step's RK4 followed a recorded adjustment
     double* heat;              // aturan_set_heating: [jm][km] K/s, or null
     double* mca_H;             // aturan_mca: the cp table's running integral, made at the first call
     bool mca_H_ready;          // mca_H holds the integral (its kernel has launched)
@@ -337,7 +341,7 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
     if(!prelude_done){ const int rc = rk4_prelude<S>(ctx, ctx->st); if(rc) return rc; }
     if(taping<S>(ctx)){
         CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->tX, state, ADJ_NF * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->tX, state, ctx->tape_nf * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpyAsync(ctx->tPd, ctx->pdyn, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
     }
     StageArgs<S, C> a;
@@ -370,12 +374,16 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
         CK_LAUNCH("RK4 stage");
         }
         if(taping<S>(ctx)){      // the next stage's input of t, u, v, w; after stage 3 the new T
-            if(stage < 3) CK(cudaMemcpyAsync(ctx->tX + (size_t)(stage + 1) * ADJ_NF * fs, a.Y, ADJ_NF * fs * 8,
+            if(stage < 3) CK(cudaMemcpyAsync(ctx->tX + (size_t)(stage + 1) * ctx->tape_nf * fs, a.Y, ctx->tape_nf * fs * 8,
                                              cudaMemcpyDeviceToDevice, ctx->st));
             else CK(cudaMemcpyAsync(ctx->tTout, state, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
         }
     }
-    if(taping<S>(ctx)) ctx->tape_valid = true;
+    if(taping<S>(ctx)){
+        ctx->tape_valid = true;
+        ctx->tape_sat_valid = ctx->tape_sat_pending;   // this step's adjustment, if one ran before it
+        ctx->tape_sat_pending = false;
+    }
     return ATURAN_OK;
 }
 
@@ -400,6 +408,11 @@ int run_satadj(aturan_ctx* ctx, int mask, bool count, cudaStream_t st, bool with
     a.nh4sh = grp<S>(state, ATURAN_NH4SH, fs);
     a.tlo = ctx->tlo;
     a.tnlo = ctx->tlo ? ctx->tlo + fs : nullptr;
+    if(taping<S>(ctx) && ctx->tape_nf == ADJ_NF_MOIST){   // the moist tape: the adjustment's input
+        if(mask != 0xF) return fail(ctx, ATURAN_E_UNSUPPORTED, "the moist tape records the adjustment of all four gases only");
+        CK(cudaMemcpyAsync(ctx->tPre, state, (size_t)ADJ_NF_MOIST * fs * 8, cudaMemcpyDeviceToDevice, st));
+        ctx->tape_sat_pending = true;
+    }
     Region reg(ctx, ATURAN_K_SATADJ, 1, st);
     launch_satadj(a, st);
     CK_LAUNCH("saturation adjustment");
@@ -940,6 +953,7 @@ int aturan_params_default(aturan_params* p){
     p->alpha_sponge = 10.0; p->r_p_nh4sh = 1.0e-5; p->rho_cond_nh4sh = 1170.0;
     p->turb_coupling = 1.0; p->precip_coupling = 1.0; p->tmf_scale = 0.0; p->cent_mom = 0.0;
     p->pbaro_follow = 64.0; p->t_min_K = 7.5; p->t_max_K = 2000.0; p->p_dyn_cap = 0.2;
+    p->satadj_stop_tol = 1.0e-3;
     const double G[4][14] = {
         {273.15, 210.15, 8.1253, 2.5009e6, 2.8339e6, 25.096, 3148.2, 461.52, 0.0, -8.7e-3, 28.418, 3567.3, 0.0, -8.7e-3},
         {187.65, 140.0, 14.5192, 5.5e5, 7.45e5, 17.064, 747.0, 243.96, 0.0, -2.9e-3, 17.064, 747.0, 0.0, -2.9e-3},
@@ -1188,6 +1202,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
         K.freeze_on = p->satadj_freeze && p->satadj_conserve && G.t_00 > 0.0 && G.t_00 < G.t_0;
     }
     sc.cp_mix = p->cp_mix; sc.t_ref = p->t_ref; sc.r_mix = p->r_mix;
+    sc.stop_tol = p->satadj_stop_tol > 0.0 ? p->satadj_stop_tol : 1.0e-3;
     sc.conserve = p->satadj_conserve; sc.newton = p->satadj_newton; sc.evap = p->satadj_evap;
     sc.ice_entry = p->satadj_ice_entry; sc.bergeron = p->satadj_bergeron; sc.dry_exit = p->satadj_dry_exit;
     sc.local_rho = p->local_rho;
@@ -1509,13 +1524,19 @@ int aturan_tape(aturan_ctx* ctx, int on){
         ctx->tape_p_valid = false;
         return ATURAN_OK;
     }
+    if(on != 1 && on != 2) return fail(ctx, ATURAN_E_INVALID, "aturan_tape: on is 0, 1 (dry) or 2 (moist)");
     if(ctx->mixed) return fail(ctx, ATURAN_E_UNSUPPORTED, "the RK4 adjoint needs an FP64 context");
-    if(ctx->tape) return ATURAN_OK;
+    const int want = on == 2 ? ADJ_NF_MOIST : ADJ_NF;
+    if(ctx->tape && ctx->tape_nf == want) return ATURAN_OK;
+    if(ctx->tape){ CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->tape); ctx->tape = nullptr; }
     const Grid& g = ctx->g;
     const size_t fs = g.fstride;
-    // stage inputs 4 x 4, T output, p_dyn, pressure source, slots, ybar 4, kbar 4, g0 4, phbar, rbar,
-    // pdbar, aux adjoint 3, heating accumulator; level means + sums
-    const size_t nf = 4 * ADJ_NF + 3 + ADJ_SLOTS + 3 * ADJ_NF + 3 + 3 + 1;
+    const int NT = want;
+    const size_t nslot = NT == ADJ_NF ? ADJ_SLOTS : ADJ_SLOTS_MOIST;
+    // stage inputs 4 x NT, T output, p_dyn, pressure source, slots, ybar NT, kbar NT, g0 NT, phbar,
+    // rbar, pdbar, aux adjoint 3, heating accumulator, the moist tape's adjustment input NT; level
+    // means + sums
+    const size_t nf = 4 * NT + 3 + nslot + 3 * NT + 3 + 3 + 1 + (NT == ADJ_NF ? 0 : NT);
     const size_t bytes = (nf * fs + 3 * (size_t)g.im) * sizeof(double);
     void* mem = nullptr;
     if(cudaMalloc(&mem, bytes) != cudaSuccess){ cudaGetLastError(); return fail(ctx, ATURAN_E_NOMEM, "tape allocation"); }
@@ -1523,23 +1544,27 @@ int aturan_tape(aturan_ctx* ctx, int on){
     double* cur = reinterpret_cast<double*>(mem);
     auto take = [&](size_t n){ double* r = cur; cur += n; return r; };
     ctx->tape = reinterpret_cast<double*>(mem);
-    ctx->tX = take(4 * ADJ_NF * fs);
+    ctx->tape_nf = NT;
+    ctx->tX = take(4 * NT * fs);
     ctx->tTout = take(fs);
     ctx->tPd = take(fs);
     ctx->tSrc = take(fs);
-    ctx->aslot = take(ADJ_SLOTS * fs);
-    ctx->aybar = take(ADJ_NF * fs);
-    ctx->akbar = take(ADJ_NF * fs);
-    ctx->ag0 = take(ADJ_NF * fs);
+    ctx->aslot = take(nslot * fs);
+    ctx->aybar = take(NT * fs);
+    ctx->akbar = take(NT * fs);
+    ctx->ag0 = take(NT * fs);
     ctx->aphbar = take(fs);
     ctx->arbar = take(fs);
     ctx->apdbar = take(fs);
     ctx->aaux = take(3 * fs);
     ctx->ahacc = take(fs);
+    ctx->tPre = NT == ADJ_NF ? nullptr : take(NT * fs);
     ctx->tref = take(g.im);
     ctx->alev = take(2 * g.im);
     ctx->tape_valid = false;
     ctx->tape_p_valid = false;
+    ctx->tape_sat_pending = false;
+    ctx->tape_sat_valid = false;
     return ATURAN_OK;
 }
 
@@ -1547,25 +1572,35 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
     return aturan_rk4_adjoint_ex(ctx, ybar, nullptr, xbar, nullptr, nullptr);
 }
 
-int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
-                          double* const* xbar, double* pbar, double* heatbar){
+}  // extern "C"
+
+namespace {
+
+// The reverse of the taped step over its nf fields (ADJ_NF: t, u, v, w; ADJ_NF_MOIST: and the
+// twelve condensable species, then the saturation adjustment's implicit adjoint when the taped
+// step ran one).
+int rk4_adjoint_impl(aturan_ctx* ctx, int nf, const double* const* ybar, const double* const* auxbar,
+                     double* const* xbar, double* pbar, double* heatbar){
     if(!ctx || !ybar || !xbar) return ATURAN_E_INVALID;
     if(auxbar) for(int q = 0; q < 3; q++) if(!auxbar[q]) return fail(ctx, ATURAN_E_INVALID, "null aux adjoint pointer");
-    for(int q = 0; q < ADJ_NF; q++) if(!ybar[q] || !xbar[q]) return fail(ctx, ATURAN_E_INVALID, "null adjoint pointer");
+    for(int q = 0; q < nf; q++) if(!ybar[q] || !xbar[q]) return fail(ctx, ATURAN_E_INVALID, "null adjoint pointer");
     if(!ctx->tape || !ctx->tape_valid) return fail(ctx, ATURAN_E_INVALID, "no taped RK4 step (aturan_tape, then aturan_rk4_step)");
+    if(ctx->tape_nf != nf)
+        return fail(ctx, ATURAN_E_INVALID, nf == ADJ_NF ? "the tape is moist: use aturan_moist_adjoint"
+                                                        : "the tape is dry: switch it on with aturan_tape(ctx, 2)");
     const Grid g = ctx->g;
     const size_t fs = g.fstride, rows = (size_t)g.im * g.jm;
     const double dt = ctx->p.dt;
     Region reg(ctx, ATURAN_K_ADJOINT, 0);
     long nl = 0;
-    for(int q = 0; q < ADJ_NF; q++)                    // the caller's ybar' into the padded layout
+    for(int q = 0; q < nf; q++)                        // the caller's ybar' into the padded layout
         CK(cudaMemcpy2DAsync(ctx->ag0 + q * fs, g.kp * 8, ybar[q], g.km * 8, g.km * 8, rows,
                              cudaMemcpyDeviceToDevice, ctx->st));
     const RhsConst<double>& K = ctx->k64;
     const double t_min = K.t_min, t_max = K.t_max;
     const dim3 gc((g.km + 127) / 128, g.jm, g.im);
     adj_init_kernel<<<gc, 128, 0, ctx->st>>>(g, ctx->ag0, ctx->tTout, t_min, t_max, dt / 6.0 * 1.0,
-                                             ctx->ag0, ctx->aybar, ctx->akbar, ctx->aphbar, ctx->apdbar);
+                                             ctx->ag0, ctx->aybar, ctx->akbar, ctx->aphbar, ctx->apdbar, nf);
     CK_LAUNCH("adjoint init"); nl++;
     if(auxbar)                                         // the aux adjoint into the padded layout
         for(int q = 0; q < 3; q++)
@@ -1586,15 +1621,17 @@ int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const doub
     const dim3 gs((g.km - 1 + 31) / 32, (g.jm - 2 + 3) / 4, g.im - 2);
     const dim3 gg((g.km - 1 + 127) / 128, g.jm, g.im);
     for(int stage = 3; stage >= 0; stage--){
-        a.X = ctx->tX + (size_t)stage * ADJ_NF * fs;
+        a.X = ctx->tX + (size_t)stage * nf * fs;
         a.auxbar = (stage == 3 && auxbar) ? ctx->aaux : nullptr;   // aux is stage 3's output
         adj_local_kernel<<<gs, dim3(32, 4), 0, ctx->st>>>(a);
+        nl++;
+        if(nf == ADJ_NF_MOIST){ adj_species_local_kernel<<<gs, dim3(32, 4), 0, ctx->st>>>(a); nl++; }
         const int prev = stage - 1;
         const double w_prev = prev >= 0 ? dt / 6.0 * ((prev == 0 || prev == 3) ? 1.0 : 2.0) : 0.0;
         const double c_prev = prev >= 0 ? ((prev == 0 || prev == 1) ? 0.5 * dt : (prev == 2 ? dt : 0.0)) : 0.0;
         adj_gather_kernel<<<gg, 128, 0, ctx->st>>>(g, ctx->aslot, ctx->aybar, ctx->aphbar, ctx->apdbar, ctx->ag0,
-                                                  ctx->akbar, w_prev, c_prev, prev >= 0 ? 1 : 0);
-        CK_LAUNCH("adjoint stage"); nl += 2;
+                                                  ctx->akbar, w_prev, c_prev, prev >= 0 ? 1 : 0, nf);
+        CK_LAUNCH("adjoint stage"); nl++;
     }
     const double* t0 = ctx->tX;
     adj_hydro_kernel<<<(g.jm * g.km + 255) / 256, 256, 0, ctx->st>>>(
@@ -1605,8 +1642,14 @@ int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const doub
     adj_level_apply_kernel<<<gc, 128, 0, ctx->st>>>(g, t0, reinterpret_cast<const double*>(ctx->pstat), ctx->wsin,
                                                     ctx->alev, ctx->hc, ctx->aybar);
     CK_LAUNCH("adjoint hydrostatic"); nl += 3;
+    if(nf == ADJ_NF_MOIST && ctx->tape_sat_valid){     // the step's adjustment, before its RK4
+        adj_satadj_kernel<<<gc, 128, 0, ctx->st>>>(g, ctx->tPre, ctx->tX, reinterpret_cast<const double*>(ctx->pstat),
+                                                   reinterpret_cast<const double*>(ctx->forc) + (size_t)(ATURAN_RHO_MIX - ATURAN_NUE) * fs,
+                                                   ctx->sc, ctx->aybar);
+        CK_LAUNCH("adjoint saturation adjustment"); nl++;
+    }
     reg.n = nl;
-    for(int q = 0; q < ADJ_NF; q++)
+    for(int q = 0; q < nf; q++)
         CK(cudaMemcpy2DAsync(xbar[q], g.km * 8, ctx->aybar + q * fs, g.kp * 8, g.km * 8, rows,
                              cudaMemcpyDeviceToDevice, ctx->st));
     if(pbar)
@@ -1617,6 +1660,20 @@ int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const doub
     }
     CK(cudaStreamSynchronize(ctx->st));
     return ATURAN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
+                          double* const* xbar, double* pbar, double* heatbar){
+    return rk4_adjoint_impl(ctx, ADJ_NF, ybar, auxbar, xbar, pbar, heatbar);
+}
+
+int aturan_moist_adjoint(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
+                         double* const* xbar, double* pbar, double* heatbar){
+    return rk4_adjoint_impl(ctx, ADJ_NF_MOIST, ybar, auxbar, xbar, pbar, heatbar);
 }
 
 int aturan_set_heating(aturan_ctx* ctx, const double* H, int on_device){

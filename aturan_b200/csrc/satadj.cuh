@@ -27,6 +27,7 @@ struct GasConst {
 struct SatConst {
     GasConst gas[4];
     double cp_mix, t_ref, r_mix;
+    double stop_tol;                // the stopping test (:551): the reference's 1e-3 by default
     int conserve, newton, evap, ice_entry, bergeron, dry_exit, local_rho;
 };
 
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                             }
                         }
                         const double q_diff = fabs(q_v_b - q_v_hyp) / (q_v_hyp + 1e-20);
-                        if(q_diff <= 1.0e-3){ found = true; break; }
+                        if(q_diff <= K.stop_tol){ found = true; break; }
                         if(K.dry_exit && K.conserve && q_c_b <= 0.0 && q_i_b <= 0.0 && q_v_b < q_v_hyp){ dry = true; break; }
                         if(K.newton){
                             const double dT = 0.1;

@@ -134,7 +134,12 @@ typedef struct aturan_params {
     double pbaro_follow;         /* ATURAN_PBARO_FOLLOW tau [RK steps]; 0 = p_baro frozen */
     double t_min_K, t_max_K;     /* integrator temperature guards */
     double p_dyn_cap;            /* shared solver source clamp (PressureSolver.h:168) */
-    double reserved_d[8];
+    double satadj_stop_tol;      /* the adjustment's stopping test on |q_v - q_hyp| / q_hyp
+                                    (SaturationAdjustment.h:551): the reference's 1e-3 (default;
+                                    <= 0 reads as 1e-3); smaller values take the passes nearer the
+                                    root (within the 15-pass cap), as a finite-difference check of
+                                    the implicit adjoint needs */
+    double reserved_d[7];
     aturan_gas gas[4];           /* H2O, H2S, NH3, CH4: the loop's order */
 } aturan_params;
 
@@ -191,7 +196,8 @@ int aturan_rk4_step(aturan_ctx* ctx);
  * aturan_tape(ctx, 1): every later aturan_rk4_step and RB_SOR / RB_LINE aturan_pressure keeps what
  *   its adjoint needs (the stage inputs of t, u, v, w, the new T, p_dyn, the clamped pressure
  *   source and the level means: 19 fields, plus 56 fields of work arrays, of device memory);
- *   aturan_tape(ctx, 0) frees it. ATURAN_E_UNSUPPORTED on a mixed context.
+ *   aturan_tape(ctx, 2): the moist tape (aturan_moist_adjoint); aturan_tape(ctx, 0) frees either.
+ *   ATURAN_E_UNSUPPORTED on a mixed context.
  * aturan_rk4_adjoint(ctx, ybar, xbar): ybar[4] and xbar[4] are device pointers to contiguous
  *   [im][jm][km] FP64 arrays in the order t, u, v, w. Given the adjoint ybar of those fields after
  *   the last taped aturan_rk4_step, writes xbar = J^T ybar, J the step's Jacobian with respect to
@@ -210,6 +216,23 @@ int aturan_rk4_adjoint(aturan_ctx* ctx, const double* const* ybar, double* const
  * heating field of aturan_set_heating, a [jm][km] FP64 device array. */
 int aturan_rk4_adjoint_ex(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
                           double* const* xbar, double* pbar, double* heatbar);
+
+/* The moist step's adjoint (no counterpart in the reference). aturan_tape(ctx, 2) switches on the
+ * moist tape (the dry one's contents over sixteen fields -- t, u, v, w and the twelve condensable
+ * species ATURAN_CH4 .. ATURAN_NH3_ICE -- plus the state an aturan_satadj of all four gases, or
+ * aturan_step's adjustment, had on entry: 16 more fields and 84 more work fields; replaces a dry
+ * tape). Given ybar[16], the adjoint of those sixteen fields after the last taped
+ * aturan_rk4_step, writes xbar[16]: the RK4 step's adjoint over the sixteen fields (the species'
+ * transport and diffusion by the taped u, v, w, their forcing held fixed) and, when an adjustment
+ * ran between the previous taped RK4 step and this one, then the implicit adjoint of the
+ * converged saturation adjustment (SaturationAdjustment.h:255-746): per cell and gas the
+ * derivative of the root of the closure q_v = H(T, q_c, q_i) on the adjustment's invariants (total
+ * water, and the moist enthalpy cp rho T - L_v q_c - L_s q_i), the phases present at convergence
+ * frozen; a gas that was not adjusted contributes its entry melt / freeze, piecewise linear. xbar
+ * is then the adjoint with respect to the state before the adjustment. auxbar, pbar and heatbar
+ * as for aturan_rk4_adjoint_ex. FP64 contexts. Synchronous. */
+int aturan_moist_adjoint(aturan_ctx* ctx, const double* const* ybar, const double* const* auxbar,
+                         double* const* xbar, double* pbar, double* heatbar);
 
 /* A heating rate H(theta, phi) in K/s added to the temperature tendency at every interior level,
  * rhs_t += H (L_atm 1e3 / u_0) / t_ref (no counterpart in the reference, whose heating enters as

@@ -1416,6 +1416,9 @@ int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adj
     const double cp_mix = p->cp_mix, t_ref = p->t_ref;
     const int iter_prec_end = 15;
     const double q_diff_min = 1.0e-3;
+    /* the stopping test (:551), the reference's 1e-3 unless satadj_stop_tol asks for a tighter one;
+       the entry test (:446) keeps 1e-3 */
+    const double q_stop = p->satadj_stop_tol > 0.0 ? p->satadj_stop_tol : q_diff_min;
     long nadj = 0, nnc = 0;
 
     #pragma omp parallel for collapse(2) schedule(static) reduction(+:nadj,nnc)
@@ -1556,7 +1559,7 @@ int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adj
                         }
                     }
                     const double q_diff = fabs(q_v_b - q_v_hyp) / (q_v_hyp + 1e-20);
-                    if(q_diff <= q_diff_min){ cell_found = 1; break; }
+                    if(q_diff <= q_stop){ cell_found = 1; break; }
                     if(dry_exit && conserve && q_c_b <= 0.0 && q_i_b <= 0.0 && q_v_b < q_v_hyp){ cell_dry = 1; break; }
                     if(newton){
                         const double dT = 0.1;

@@ -234,3 +234,82 @@ class DryStep:
             full[1:-1, 1:-1, :N] = y
             out.append(full)
         return out
+
+
+SPECIES = ("ch4", "ch4_cloud", "ch4_ice", "h2o", "h2o_cloud", "h2o_ice",
+           "h2s", "h2s_cloud", "h2s_ice", "nh3", "nh3_cloud", "nh3_ice")
+
+
+class MoistRK4Step(DryStep):
+    """The same RK4 step over t, u, v, w and the twelve condensable species
+    (planet/RHS_Uran_Turb.cpp:790-850): each species is carried by u, v, w and diffused with
+    1/(Sc Re) + nue_t/0.9, plus its frozen forcing (the precipitation source S_precip_<species>
+    times the precipitation coupling; H2S and NH3 vapour also the mass flux times the chemical
+    reaction switch). `fixed` additionally holds S_precip_* and massflux_h2s / massflux_nh3."""
+
+    def __init__(self, p, fixed, oracle):
+        super().__init__(p, fixed, oracle)
+        T = lambda a: torch.tensor(np.array(a, dtype=np.float64))
+        N = p.km - 1
+        zero = np.zeros((p.im, p.jm, p.km))
+        self.sp_forc = []
+        for n in SPECIES:
+            f = p.precip_coupling * T(fixed.get("S_precip_" + n, zero))[1:-1, 1:-1, :N]
+            if n in ("h2s", "nh3"):
+                f = f + p.chemical_reaction * T(fixed.get("massflux_" + n, zero))[1:-1, 1:-1, :N]
+            self.sp_forc.append(f)
+        sc = {"ch4": p.sc_ch4, "h2o": p.sc_h2o, "h2s": p.sc_h2s, "nh3": p.sc_nh3}
+        self.sp_sc_re = [sc[n.split("_")[0]] * p.re for n in SPECIES]
+
+    def rhs(self, X, ph):
+        r = super().rhs(X[:4], ph)
+        p, g = self.p, self.geo
+        N = p.km - 1
+        U, V, W = X[1], X[2], X[3]
+        u, v, w = U[1:-1, 1:-1, :N], V[1:-1, 1:-1, :N], W[1:-1, 1:-1, :N]
+        v_invrm, w_invrs = v * g["inv_rm"], w * g["inv_rmsinthe"]
+        nue = self.nue[1:-1, 1:-1, :N]
+        if p.turb_coupling != 0.0:
+            nue_t = torch.where(torch.isfinite(nue), p.turb_coupling * nue.clamp(min=0.0), torch.zeros_like(nue))
+        else:
+            nue_t = torch.zeros_like(nue)
+        nue_t_s = nue_t / 0.9
+        two_inv_rm = 2.0 * g["inv_rm"]
+        for q in range(len(SPECIES)):
+            s = self._stencil(X[4 + q])
+            transport = u * s["d1r"] + v_invrm * s["d1t"] + w_invrs * s["d1p"]
+            diffusion = (s["d2r"] + s["d1r"] * two_inv_rm + s["d2t"] * g["inv_rm2"]
+                         + s["d1t"] * g["costhe_inv_rm2sinthe"] + s["d2p"] * g["inv_rm2sinthe2"])
+            r.append(-transport + diffusion / self.sp_sc_re[q] + diffusion * nue_t_s + self.sp_forc[q])
+        return r
+
+    def __call__(self, *Y):
+        p = self.p
+        N = p.km - 1
+        Y = list(Y)
+        nf = len(Y)
+        ph, _ = self.hydro(Y[0], Y[2], Y[3])
+        dt = p.dt
+        X = Y
+        acc = None
+        for stage in range(4):
+            c_in = 0.5 * dt if stage in (0, 1) else (dt if stage == 2 else 0.0)
+            wgt = 1.0 if stage in (0, 3) else 2.0
+            k = self.rhs(X, ph)
+            acc = [wgt * r for r in k] if acc is None else [a + wgt * r for a, r in zip(acc, k)]
+            if stage < 3:
+                X = []
+                for q in range(nf):
+                    full = Y[q].clone()
+                    full[1:-1, 1:-1, :N] = Y[q][1:-1, 1:-1, :N] + c_in * k[q]
+                    X.append(full)
+        out = []
+        tmin, tmax = p.t_min_K / p.t_ref, p.t_max_K / p.t_ref
+        for q in range(nf):
+            full = Y[q].clone()
+            y = Y[q][1:-1, 1:-1, :N] + dt * acc[q] / 6.0
+            if q == 0:
+                y = y.clamp(tmin, tmax)
+            full[1:-1, 1:-1, :N] = y
+            out.append(full)
+        return out

@@ -53,3 +53,28 @@ def test_dry_step_gradient_is_finite_difference_consistent(oracle_lib):
         fd = float((lp - lm) / (2 * h))
         an = float(sum((g * di).sum() for g, di in zip(grads, d)))
         assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-30), (fd, an)
+
+
+MOIST_FIXED = FIXED + tuple("S_precip_" + n for n in ("ch4", "ch4_cloud", "ch4_ice", "h2o", "h2o_cloud", "h2o_ice",
+                                                     "h2s", "h2s_cloud", "h2s_ice", "nh3", "nh3_cloud", "nh3_ice")) \
+    + ("massflux_h2s", "massflux_nh3")
+
+
+@pytest.mark.parametrize("shape,seed", [((12, 20, 33), 54), ((21, 37, 73), 55)])
+def test_moist_step_matches_oracle(oracle_lib, shape, seed):
+    """The moist restatement (t, u, v, w and the twelve condensable species) against the C
+    restatement's RK4 step."""
+    from oracle.dry_ref import MoistRK4Step, SPECIES
+    p = P.default_params(*shape)
+    st = S.synthetic_state(p, seed=seed)
+    names = ("t", "u", "v", "w") + SPECIES
+    step = MoistRK4Step(p, {n: st[n] for n in MOIST_FIXED}, oracle_lib)
+    out = step(*[torch.tensor(st[n]) for n in names])
+    ref = S.copy_state(st)
+    for n in names + ("nh4sh", "tke", "dis"):
+        ref[n + "n"][:] = ref[n]
+    oracle_lib.rk4(p, ref)
+    for n, o in zip(names, out):
+        a, b = o.numpy(), ref[n]
+        err = np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+        assert err < 1e-12, (n, err)
