@@ -352,7 +352,7 @@ __device__ SatEntry sat_entry(const SatConst& K, const GasConst& G, double rho_c
                 if(cloud > 0.0 && ice > 0.0) q_t0 = (cloud * q_Rain_0 + ice * q_Ice_0) / (cloud + ice);
                 else if(ice <= 0.0)          q_t0 = q_Rain_0;
                 else                         q_t0 = q_Ice_0;
-                if(fabs(c - q_t0) <= 1.0e-3 * q_t0) go = false;
+                if(fabs(c - q_t0) <= K.entry_tol * q_t0) go = false;
             }
         }
     }

@@ -1203,6 +1203,7 @@ int aturan_ctx_create(const aturan_params* p, aturan_ctx** out){
     }
     sc.cp_mix = p->cp_mix; sc.t_ref = p->t_ref; sc.r_mix = p->r_mix;
     sc.stop_tol = p->satadj_stop_tol > 0.0 ? p->satadj_stop_tol : 1.0e-3;
+    sc.entry_tol = p->satadj_entry_tol == 0.0 ? 1.0e-3 : (p->satadj_entry_tol < 0.0 ? 0.0 : p->satadj_entry_tol);
     sc.conserve = p->satadj_conserve; sc.newton = p->satadj_newton; sc.evap = p->satadj_evap;
     sc.ice_entry = p->satadj_ice_entry; sc.bergeron = p->satadj_bergeron; sc.dry_exit = p->satadj_dry_exit;
     sc.local_rho = p->local_rho;

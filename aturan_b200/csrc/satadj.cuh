@@ -28,6 +28,7 @@ struct SatConst {
     GasConst gas[4];
     double cp_mix, t_ref, r_mix;
     double stop_tol;                // the stopping test (:551): the reference's 1e-3 by default
+    double entry_tol;               // the entry test (:446): the reference's 1e-3 by default
     int conserve, newton, evap, ice_entry, bergeron, dry_exit, local_rho;
 };
 
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) satadj_kernel(const SatArgs<S> 
                             if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
                             else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
                             else                         q_t0 = q_Ice_0;
-                            if(fabs(c - q_t0) <= 1.0e-3 * q_t0) go = false;
+                            if(fabs(c - q_t0) <= K.entry_tol * q_t0) go = false;
                         }
                     }
                 }

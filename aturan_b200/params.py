@@ -41,14 +41,14 @@ _DBL_FIELDS = (
     "sc_ch4", "sc_h2o", "sc_h2s", "sc_nh3", "sc_nh4sh",
     "alpha_sponge", "r_p_nh4sh", "rho_cond_nh4sh",
     "turb_coupling", "precip_coupling", "tmf_scale", "cent_mom", "pbaro_follow",
-    "t_min_K", "t_max_K", "p_dyn_cap", "satadj_stop_tol")
+    "t_min_K", "t_max_K", "p_dyn_cap", "satadj_stop_tol", "satadj_entry_tol")
 
 
 class Params(ctypes.Structure):
     _fields_ = ([(n, ctypes.c_int32) for n in _INT_FIELDS]
                 + [("reserved_i", ctypes.c_int32 * 7)]
                 + [(n, ctypes.c_double) for n in _DBL_FIELDS]
-                + [("reserved_d", ctypes.c_double * 7), ("gas", Gas * 4)])
+                + [("reserved_d", ctypes.c_double * 6), ("gas", Gas * 4)])
 
     def copy(self):
         p = Params()
@@ -92,7 +92,7 @@ DEFAULTS = dict(
     sc_ch4=0.99, sc_h2o=0.61, sc_h2s=0.94, sc_nh3=0.61, sc_nh4sh=0.7,
     alpha_sponge=10.0, r_p_nh4sh=1.0e-5, rho_cond_nh4sh=1170.0,
     turb_coupling=1.0, precip_coupling=1.0, tmf_scale=0.0, cent_mom=0.0, pbaro_follow=64.0,
-    t_min_K=7.5, t_max_K=2000.0, p_dyn_cap=0.2, satadj_stop_tol=1.0e-3,
+    t_min_K=7.5, t_max_K=2000.0, p_dyn_cap=0.2, satadj_stop_tol=1.0e-3, satadj_entry_tol=0.0,
 )
 
 

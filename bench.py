@@ -622,6 +622,8 @@ def main():
                     help="only the passes after RK4 (aturan_post_step): prints the post_step object")
     ap.add_argument("--mca", action="store_true",
                     help="only the moist convective adjustment (aturan_mca): prints the mca object")
+    ap.add_argument("--iteration", action="store_true",
+                    help="only the full iteration of the model's loop (aturan_iteration): prints the iteration object")
     ap.add_argument("--poisson", action="store_true",
                     help="only the isolated Poisson solve (omega sweep, FP64 and mixed): prints the poisson object")
     args = ap.parse_args()
@@ -647,6 +649,12 @@ def main():
             grid = tuple(int(x) for x in args.grid.lower().split("x"))
             print(json.dumps({"mca": mca_timing(api, P, S, torch, grid=grid,
                                                 reference=grid == (41, 181, 361))}), flush=True)
+        return
+    if args.iteration:
+        if rank == 0:
+            print(json.dumps({"iteration": iteration_timing(api, P, S, torch, args.precision,
+                                                            press_args(args.press)[0]),
+                              "precision": args.precision}), flush=True)
         return
     if args.poisson:
         if rank == 0:

@@ -139,7 +139,12 @@ typedef struct aturan_params {
                                     <= 0 reads as 1e-3); smaller values take the passes nearer the
                                     root (within the 15-pass cap), as a finite-difference check of
                                     the implicit adjoint needs */
-    double reserved_d[7];
+    double satadj_entry_tol;     /* the entry test (SaturationAdjustment.h:446): a cell whose vapour
+                                    lies within this fraction of its entry saturation is left
+                                    alone. 0 (default): the reference's 1e-3; < 0: no band (only
+                                    exact equality is left alone), which makes the adjustment a
+                                    continuous map, as a finite-difference check needs */
+    double reserved_d[6];
     aturan_gas gas[4];           /* H2O, H2S, NH3, CH4: the loop's order */
 } aturan_params;
 

@@ -1419,6 +1419,9 @@ int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adj
     /* the stopping test (:551), the reference's 1e-3 unless satadj_stop_tol asks for a tighter one;
        the entry test (:446) keeps 1e-3 */
     const double q_stop = p->satadj_stop_tol > 0.0 ? p->satadj_stop_tol : q_diff_min;
+    /* the entry band (:446): 1e-3 unless satadj_entry_tol asks for another (< 0: none) */
+    const double q_entry_band = p->satadj_entry_tol == 0.0 ? q_diff_min
+                              : (p->satadj_entry_tol < 0.0 ? 0.0 : p->satadj_entry_tol);
     long nadj = 0, nnc = 0;
 
     #pragma omp parallel for collapse(2) schedule(static) reduction(+:nadj,nnc)
@@ -1487,7 +1490,7 @@ int oracle_satadj(const aturan_params* p, double* const* f, int gas, long* n_adj
                     if(q_c0 > 0.0 && q_i0 > 0.0) q_t0 = (q_c0 * q_Rain_0 + q_i0 * q_Ice_0) / (q_c0 + q_i0);
                     else if(q_i0 <= 0.0)         q_t0 = q_Rain_0;
                     else                         q_t0 = q_Ice_0;
-                    if(fabs(c[q] - q_t0) <= q_diff_min * q_t0) continue;
+                    if(fabs(c[q] - q_t0) <= q_entry_band * q_t0) continue;
                 }
 
                 double q_v_b = c[q], q_c_b = cloud[q], q_i_b = ice[q];

@@ -239,8 +239,8 @@ def test_config4_dry_heating_gradient():
     residual each step, checkpoints every 10 steps, a seeded heating field H(theta, phi) ~ N(0,
     1e-5 K/s) in the temperature tendency; loss = sin(theta)-weighted mean T over |lat| <= 5 deg
     minus over |lat| >= 85 deg (all interior levels and meridians) after 50 steps; its gradient
-    with respect to H against central differences in 3 seeded directions. (The moist trajectory
-    would need the saturation adjustment's adjoint, which is not built.)"""
+    with respect to H against central differences in 3 seeded directions. (The moist, mixed form
+    is tests/test_gpu_moist_adjoint.py::test_config4_moist_mixed_heating_gradient.)"""
     from aturan_b200.autograd import DryFullStepper, rollout_gradient
     p = P.default_params()
     st = S.synthetic_state(p, seed=20261207)

@@ -203,8 +203,12 @@ def test_config4_moist_mixed_heating_gradient():
     four condensables, the pressure solved to a residual each step, the adjustment of four gases,
     checkpoints every 10 steps, a seeded heating field H(theta, phi) ~ N(0, 1e-5 K/s); loss = the
     sin(theta)-weighted mean T over |lat| <= 5 deg minus over |lat| >= 85 deg after step 50.
-      * FP64 with the adjustment taken to its root (stopping test 1e-13): the adjoint gradient with
-        respect to H against central differences of the same forward in 3 seeded directions;
+      * FP64 with the adjustment a continuous map (stopping test 1e-13, so the passes reach the
+        root; no entry band, so no cell jumps between left alone and adjusted): the adjoint
+        gradient with respect to H against central differences of the same forward in 3 seeded
+        directions. With the reference's 1e-3 entry band the forward is discontinuous: over 5-50
+        steps the central differences move by 1-30 % with the step size while the adjoint stays
+        put (an FP64 run with the band, measured);
       * the reference's stopping test (1e-3): the mixed-precision trajectory (FP32 state and
         stencils, FP64 pressure refinement and adjustment; its checkpoints held as the mixed state)
         reversed by the FP64 adjoint about FP64 steps restarted from those checkpoints, against the
@@ -232,6 +236,7 @@ def test_config4_moist_mixed_heating_gradient():
     # (1) FP64 at the root: gradient against finite differences
     pr = P.default_params()
     pr.satadj_stop_tol = 1e-13
+    pr.satadj_entry_tol = -1.0
     cr = api.Context(pr)
     cr.upload_state(st)
     sr = MoistFullStepper(cr, **press)
