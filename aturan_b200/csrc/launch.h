@@ -15,8 +15,12 @@ template <typename S> struct PrecipArgs;
 template <typename S> struct McaArgs;
 struct GSW; struct RBW; struct PressConst; struct PostPlan;
 
+// launch_stage: one RK4 stage, the momentum + T launch and then the scalar launch on st; given a
+// side stream (and two events), the momentum launch runs on side beside the scalar launch on st
+// (the two read the stage input and write disjoint fields) and st waits for it.
 #define ATURAN_DECLARE_LAUNCHERS(S, C)                                                                     \
-void launch_stage(const StageArgs<S, C>& a, cudaStream_t st);                                              \
+void launch_stage(const StageArgs<S, C>& a, cudaStream_t st, cudaStream_t side = nullptr,                   \
+                  cudaEvent_t ef = nullptr, cudaEvent_t ej = nullptr);                                     \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
                  double* part_w, int nblk, double* ref, int exact, const BuoyScratch& bx, cudaStream_t st);                       \
 void launch_hydro(Grid g, const S* t, const S* ps, const S* v, const S* w, const double* ref,              \

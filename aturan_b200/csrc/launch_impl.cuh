@@ -183,11 +183,21 @@ template <> struct HydCfg<float> { static constexpr int ROWS = 16, MINB = 2; };
 }  // namespace aturan
 
 #define ATURAN_DEFINE_LAUNCHERS(S, C)                                                                     \
-void launch_stage(const StageArgs<S, C>& a, cudaStream_t st){                                             \
+void launch_stage(const StageArgs<S, C>& a, cudaStream_t st, cudaStream_t side, cudaEvent_t ef,           \
+                  cudaEvent_t ej){                                                                        \
     const Grid& g = a.g;                                                                                  \
     const dim3 grid2((g.km - 1 + 63) / 64, (g.jm - 2 + 3) / 4, g.im - 2);                                 \
-    launch_momentum(a, grid2, st);                                                                        \
+    if(!side){                                                                                            \
+        launch_momentum(a, grid2, st);                                                                    \
+        launch_scalars(a, grid2, st);                                                                     \
+        return;                                                                                           \
+    }                                                                                                     \
+    cudaEventRecord(ef, st);                                                                              \
+    cudaStreamWaitEvent(side, ef, 0);                                                                     \
+    launch_momentum(a, grid2, side);                                                                      \
     launch_scalars(a, grid2, st);                                                                         \
+    cudaEventRecord(ej, side);                                                                            \
+    cudaStreamWaitEvent(st, ej, 0);                                                                       \
 }                                                                                                         \
 void launch_buoy(Grid g, const S* t, const S* ps, const double* wsin, HydroConst h, double* part_sum,     \
                  double* part_w, int nblk, double* ref, int exact, const BuoyScratch& bx, cudaStream_t st){ \
