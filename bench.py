@@ -183,12 +183,76 @@ def adjoint_timing(api, P, S, torch, reps=5):
         e[2].synchronize()
         fwd += e[0].elapsed_time(e[1])
         adj += e[1].elapsed_time(e[2])
-    ctx.close()
-    return {"fwd_ms": fwd / reps, "adj_ms": adj / reps, "adj_over_fwd": adj / fwd, "precision": "fp64",
-            "grid": [p.im, p.jm, p.km],
-            "what": "forward = aturan_rk4_step with the tape on (level means, hydrostatic integral, 4 stages, "
-                    "tape copies); adjoint = aturan_rk4_adjoint (4 reverse stages, hydrostatic and level-mean "
-                    "adjoints, layout copies in and out)"}
+    out = {"fwd_ms": fwd / reps, "adj_ms": adj / reps, "adj_over_fwd": adj / fwd, "precision": "fp64",
+           "grid": [p.im, p.jm, p.km],
+           "what": "forward = aturan_rk4_step with the tape on (level means, hydrostatic integral, 4 stages, "
+                   "tape copies); adjoint = aturan_rk4_adjoint (4 reverse stages, hydrostatic and level-mean "
+                   "adjoints, layout copies in and out)"}
+    # the full steps the multi-step gradients chain (aturan_b200.autograd): the pressure solve to a
+    # residual and its transposed solve included, dry and moist
+    press = dict(kind=P.PRESS_RB_LINE, omega=1.0, max_sweeps=200, tol=1e-8)
+    abar_in = [torch.randn(p.shape, dtype=torch.float64, device="cuda", generator=g) for _ in range(3)]
+    abar_out = [torch.empty(p.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+    pbar = torch.empty(p.shape, dtype=torch.float64, device="cuda")
+    ai, ao = [t.data_ptr() for t in abar_in], [t.data_ptr() for t in abar_out]
+    ybar16 = [torch.randn(p.shape, dtype=torch.float64, device="cuda", generator=g) for _ in range(16)]
+    xbar16 = [torch.empty(p.shape, dtype=torch.float64, device="cuda") for _ in range(16)]
+    y16, x16 = [t.data_ptr() for t in ybar16], [t.data_ptr() for t in xbar16]
+    torch.cuda.synchronize()
+
+    def dry_fwd():
+        ctx.pressure(**press)
+        ctx.rk4_step()
+
+    def dry_adj():
+        ctx.rk4_adjoint_ex(yp, ai, xp, pbar.data_ptr())
+        ctx.pressure_adjoint(pbar.data_ptr(), ao, press["kind"], press["omega"], press["max_sweeps"], press["tol"])
+
+    def moist_fwd():
+        ctx.restore_ncopies(1.0)
+        ctx.pressure(**press)
+        ctx.satadj(0xF, count=False)
+        ctx.sync_ncopies()
+        ctx.rk4_step()
+
+    def moist_adj():
+        ctx.moist_adjoint(y16, ai, x16, pbar.data_ptr())
+        ctx.pressure_adjoint(pbar.data_ptr(), ao, press["kind"], press["omega"], press["max_sweeps"], press["tol"])
+
+    def pair(fwd_fn, adj_fn, n=3):
+        for _ in range(2):
+            fwd_fn()
+            adj_fn()
+        ctx.synchronize()
+        f_ = a_ = 0.0
+        for _ in range(n):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            fwd_fn()
+            e[1].record(stream)
+            adj_fn()
+            e[2].record(stream)
+            e[2].synchronize()
+            f_ += e[0].elapsed_time(e[1])
+            a_ += e[1].elapsed_time(e[2])
+        return f_ / n, a_ / n
+
+    try:
+        f_, a_ = pair(dry_fwd, dry_adj)
+        out["dry_full_step"] = {"fwd_ms": f_, "adj_ms": a_, "adj_over_fwd": a_ / f_,
+                                "what": "forward = aturan_pressure (RB_LINE to 1e-8, taped) + aturan_rk4_step; adjoint "
+                                        "= aturan_rk4_adjoint_ex (aux adjoint in, p_dyn adjoint out) + "
+                                        "aturan_pressure_adjoint (the transposed solve to 1e-8)"}
+        ctx.tape(2)
+        f_, a_ = pair(moist_fwd, moist_adj)
+        out["moist_full_step"] = {"fwd_ms": f_, "adj_ms": a_, "adj_over_fwd": a_ / f_,
+                                  "what": "forward = restoreVar + aturan_pressure (RB_LINE to 1e-8) + aturan_satadj "
+                                          "(4 gases) + n-copy sync + aturan_rk4_step, moist tape; adjoint = "
+                                          "aturan_moist_adjoint (RK4 over t, u, v, w and the 12 species, the "
+                                          "adjustment's implicit adjoint) + aturan_pressure_adjoint"}
+    finally:
+        ctx.close()
+    return out
 
 
 def dist_env():
@@ -894,7 +958,8 @@ def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
     per-field max |mixed - fp64| / max |fp64| over the interior after 1, 10 and 200 steps (and the
     99.99th percentile of the same ratio over cells, and the norm-wise ||mixed - fp64||_2 / ||fp64||_2),
     and both step times (CUDA events on each
-    context's stream, median over steps 2..10). A third context times the FP64 step with tree-ordered
+    context's stream, median over steps 2..10, each step timed alone and waited for; and 30 steps
+    back to back after step 200, as ms_per_step is taken). A third context times the FP64 step with tree-ordered
     level means (exact_reductions = 0): still within 1e-11 of the reference, and the fastest FP64
     step, so the fair denominator of the speed-up."""
     p64 = P.default_params(precision=P.FP64)
@@ -954,6 +1019,24 @@ def mixed_accuracy(api, P, S, F, pa, torch, steps=(1, 10, 200)):
                 tre[f] = float(d.max())
                 trq[f] = float(np.quantile(d, 0.9999))
             out["fp64_tree_vs_fp64_step10"] = {"max": tre, "p99.99": trq}
+    # the same three steps back to back (each followed by restoreVar, no host wait between
+    # steps), as ms_per_step times the bench's step: 30 steps per context after the comparison
+    def steady(ctx, stream, n=30):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            ctx.step(**pa)
+            ctx.restore_ncopies(1.0)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n
+    st64, st32, st64t = steady(c64, s64), steady(c32, s32), steady(c64t, s64t)
+    out["steady_ms_per_step"] = {"fp64": st64, "fp64_tree": st64t, "mixed": st32,
+                                 "what": "30 steps back to back per context (restoreVar after each), CUDA "
+                                         "events around all 30: the timing ms_per_step uses"}
+    out["mixed_speedup_over_fp64_steady"] = st64 / st32
+    out["mixed_speedup_over_fp64_tree_steady"] = st64t / st32
     c64.close()
     c32.close()
     c64t.close()
