@@ -331,19 +331,13 @@ int rk4_prelude(aturan_ctx* ctx, cudaStream_t st){
     return ATURAN_OK;
 }
 
-// One RK4 step; prelude_done: rk4_prelude has already run for this step (aturan_step runs it on
-// the side stream, beside the pressure solve).
+// The arguments of RK4 stage `stage` (RungeKutta_Uran_Turb.cpp:242-245: its input, output, the
+// stage coefficient and the accumulator's weight).
 template <typename S, typename C>
-int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
+StageArgs<S, C> stage_args(aturan_ctx* ctx, const RhsConst<C>& K, int stage){
     const Grid g = ctx->g;
     const size_t fs = g.fstride;
     S* state = reinterpret_cast<S*>(ctx->state);
-    if(!prelude_done){ const int rc = rk4_prelude<S>(ctx, ctx->st); if(rc) return rc; }
-    if(taping<S>(ctx)){
-        CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->tX, state, ctx->tape_nf * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
-        CK(cudaMemcpyAsync(ctx->tPd, ctx->pdyn, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
-    }
     StageArgs<S, C> a;
     a.g = g;
     a.St = state;
@@ -362,14 +356,31 @@ int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
     S* y0 = reinterpret_cast<S*>(ctx->ybuf[0]);
     S* y1 = reinterpret_cast<S*>(ctx->ybuf[1]);
     const double dt = ctx->p.dt;
+    a.stage = stage;
+    a.c_in = (C)((stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0));
+    a.wgt  = (C)((stage == 0 || stage == 3) ? 1.0 : 2.0);
+    a.X = stage == 0 ? state : (stage == 1 ? y0 : (stage == 2 ? y1 : y0));
+    a.Y = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : state));
+    return a;
+}
+
+// One RK4 step; prelude_done: rk4_prelude has already run for this step (aturan_step runs it on
+// the side stream, beside the pressure solve).
+template <typename S, typename C>
+int run_rk4(aturan_ctx* ctx, const RhsConst<C>& K, bool prelude_done = false){
+    const Grid g = ctx->g;
+    const size_t fs = g.fstride;
+    S* state = reinterpret_cast<S*>(ctx->state);
+    if(!prelude_done){ const int rc = rk4_prelude<S>(ctx, ctx->st); if(rc) return rc; }
+    if(taping<S>(ctx)){
+        CK(cudaMemcpyAsync(ctx->tref, ctx->ref_level, g.im * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->tX, state, ctx->tape_nf * fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->tPd, ctx->pdyn, fs * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    }
     for(int stage = 0; stage < 4; stage++){   // RungeKutta_Uran_Turb.cpp:242-245
-        a.stage = stage;
-        a.c_in = (C)((stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0));
-        a.wgt  = (C)((stage == 0 || stage == 3) ? 1.0 : 2.0);
-        a.X = stage == 0 ? state : (stage == 1 ? y0 : (stage == 2 ? y1 : y0));
-        a.Y = stage == 0 ? y0 : (stage == 1 ? y1 : (stage == 2 ? y0 : state));
+        const StageArgs<S, C> a = stage_args<S, C>(ctx, K, stage);
         {
-        Region reg(ctx, ATURAN_K_RK_STAGE, 1);
+        Region reg(ctx, ATURAN_K_RK_STAGE, 2);
         // mixed form: the momentum launch on the side stream beside the scalar launch (they read
         // the stage input and write disjoint fields; measured 3 % faster RK4 at 41x181x361)
         if(ctx->mixed) launch_stage(a, ctx->st, ctx->st2, ctx->ev_fork, ctx->ev_join);

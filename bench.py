@@ -786,8 +786,8 @@ def main():
         step()
         sweeps.append(ctx.pressure_last()[0])      # the step's pressure sweeps (a host-side value)
     prof = ctx.profile_read()
-    n_stage, ms_stage = prof["rk_stage"]
-    avg_stage_ms = ms_stage / max(n_stage, 1)
+    n_stage, ms_stage = prof["rk_stage"]          # 2 launches per stage
+    avg_stage_ms = ms_stage / (4 * K)
     alg = algorithmic_stage_bytes(args.precision)
     peak, peak_kind = peaks()
     achieved = alg / (avg_stage_ms / 1e3) / 1e9
