@@ -538,7 +538,7 @@ int sor_correct(aturan_ctx* ctx, T* P){
     sor_gemm_kernel<<<gi, 256, 0, ctx->st>>>(c.J, c.N, c.NM + 1, MatRef{ctx->sor_Ac, 1, c.J}, MatRef{ctx->sor_ct, c.N, 1},
                                             MatRef{ctx->sor_As, 1, c.J}, MatRef{ctx->sor_st, c.N, 1},
                                             1.0, ctx->sor_q, nullptr, c.N, 1, kci, sz_q);
-    sor_add_kernel<T, TR><<<dim3((c.N + 255) / 256, g.jm - 2, g.im - 2), 256, 0, ctx->st>>>(g, ctx->sor_q, P, SOR_KSPLIT, sz_q);
+    sor_add_kernel<T, TR><<<dim3((c.N + 127) / 128, g.jm - 2), 128, 0, ctx->st>>>(g, ctx->sor_q, P, SOR_KSPLIT, sz_q);
     CK_LAUNCH("column-uniform correction");
     return ATURAN_OK;
 }

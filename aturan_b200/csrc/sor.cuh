@@ -125,20 +125,38 @@ __global__ void __launch_bounds__(256) sor_colsum_kernel(Grid g, const T* P, con
     double R = 0.0, rr = 0.0, ss = 0.0;
     const double sh = shift ? *shift : 0.0;
     if(k < N){
-#pragma unroll 5
-        for(int i = 1 + grp; i < g.im - 1; i += 8){
-            const size_t o = gidx(g, i, j, k);
-            double diag;
-            const double acc = row_acc<TR, T>(g, P, o, i, j, k, w, &diag);
-            const double lc = acc - diag * (double)__ldg(P + o);
-            double s;
-            if(shift){ s = (double)src[o] - sh; src_w[o] = s; }      // the same subtraction as sor_shift_kernel
-            else s = (double)__ldg(src + o);
-            const double r = s - lc;
-            if(r32){ r32[o] = (float)r; e32[o] = 0.0f; }  // the mixed form's next correction solve
-            R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
-            rr += r * r;
-            ss += s * s;
+        // CH levels at a time: every load of the chunk before its stores (which the compiler must
+        // otherwise assume to alias the next level's loads); sums in level order as before
+        constexpr int CH = 5;
+        for(int i0 = 1 + grp; i0 < g.im - 1; i0 += 8 * CH){
+            double rv[CH], sv[CH];
+#pragma unroll
+            for(int c = 0; c < CH; c++){
+                const int i = i0 + 8 * c;
+                if(i < g.im - 1){
+                    const size_t o = gidx(g, i, j, k);
+                    double diag;
+                    const double acc = row_acc<TR, T>(g, P, o, i, j, k, w, &diag);
+                    const double lc = acc - diag * (double)__ldg(P + o);
+                    // the same subtraction as sor_shift_kernel
+                    const double s = shift ? (double)src[o] - sh : (double)__ldg(src + o);
+                    sv[c] = s;
+                    rv[c] = s - lc;
+                }
+            }
+#pragma unroll
+            for(int c = 0; c < CH; c++){
+                const int i = i0 + 8 * c;
+                if(i < g.im - 1){
+                    const size_t o = gidx(g, i, j, k);
+                    const double r = rv[c], s = sv[c];
+                    if(shift) src_w[o] = s;
+                    if(r32){ r32[o] = (float)r; e32[o] = 0.0f; }  // the mixed form's next correction solve
+                    R += (TR ? 1.0 : ywt(i, 1, g.im - 2)) * r;    // the radial block's left null vector
+                    rr += r * r;
+                    ss += s * s;
+                }
+            }
         }
     }
     __shared__ double sR[8][32], sr[256], sq[256];
@@ -309,16 +327,25 @@ __global__ void __launch_bounds__(128) sor_tridiag_kernel(SorConst s, ModeLU lu,
 // Onto every interior level of the column: P[i][j][k] += q(j,k).
 // (TR: y_i q, the trial functions of the transposed system's correction.)
 template <typename T, bool TR = false>
-__global__ void __launch_bounds__(256) sor_add_kernel(Grid g, const double* qbuf, T* P, int nsplit, long split_stride){
+__global__ void __launch_bounds__(128) sor_add_kernel(Grid g, const double* qbuf, T* P, int nsplit, long split_stride){
     const int N = g.km - 1;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
-    const int i = 1 + blockIdx.z;
     if(k >= N) return;
-    const size_t o = gidx(g, i, j, k);
     double q = 0.0;
     for(int z = 0; z < nsplit; z++) q += qbuf[(size_t)(j - 1) * N + k + z * split_stride];   // the partials
-    P[o] = (T)((double)P[o] + (TR ? ywt(i, 1, g.im - 2) * q : q));
+    // one thread per column: the levels' loads of a chunk before its stores
+    constexpr int CH = 8;
+    for(int i0 = 1; i0 < g.im - 1; i0 += CH){
+        T v[CH];
+#pragma unroll
+        for(int c = 0; c < CH; c++) if(i0 + c < g.im - 1) v[c] = P[gidx(g, i0 + c, j, k)];
+#pragma unroll
+        for(int c = 0; c < CH; c++){
+            const int i = i0 + c;
+            if(i < g.im - 1) P[gidx(g, i, j, k)] = (T)((double)v[c] + (TR ? ywt(i, 1, g.im - 2) * q : q));
+        }
+    }
 }
 
 // Red-black SOR colour pass of the folded operator, Lc e = r, for T = double (the FP64 solve) or
