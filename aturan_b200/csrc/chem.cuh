@@ -74,7 +74,7 @@ __device__ __forceinline__ double nh4sh_df(double x, double T0, double heat, dou
 // decreasing on the bracket (the formation heat moves T by millikelvin, against (a-x)(b-x) going
 // from ab to 0), so at a midpoint farther than `band` from the root r its sign is that of r - xm;
 // r comes from safeguarded Newton (a step that leaves the bracket is replaced by its midpoint),
-// and f itself is evaluated, as the reference does, at the ~10 midpoints inside the band instead
+// and f itself is evaluated, as the reference does, at the ~4 midpoints inside the band instead
 // of at all ~50. The final bracket is checked with f at both ends; a bracket that does not hold
 // (no single root, or Newton astray) is bisected again with f at every midpoint.
 __device__ __forceinline__ void nh4sh_bisect(double& lo, double& hi, double stop, double T0, double heat,
@@ -95,7 +95,9 @@ __device__ __forceinline__ void nh4sh_bisect(double& lo, double& hi, double stop
             if(done) break;
         }
     }
-    const double band = 1.0e3 * stop;
+    // Newton leaves r within 1e-3 stop of the root; the computed sign of f is unreliable only within
+    // rounding of it (relative ~1e-16 of the bracket, stop being 1e-15 of it), so 8 stop is ample
+    const double band = 8.0 * stop;
     for(int it = 0; it < 80; it++){
         const double xm = 0.5 * (lo + hi);
         bool pos;
