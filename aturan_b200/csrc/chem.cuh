@@ -98,16 +98,20 @@ __device__ __forceinline__ void nh4sh_bisect(double& lo, double& hi, double stop
     // Newton leaves r within 1e-3 stop of the root; the computed sign of f is unreliable only within
     // rounding of it (relative ~1e-16 of the bracket, stop being 1e-15 of it), so 8 stop is ample
     const double band = 8.0 * stop;
+    // whether the sign of f at each end was evaluated (the initial ends' signs are the caller's
+    // tests: f(lo) > 0, and f(hi) <= 0 at x = 0 or x = min(a, b), where f = -K_p) or inferred
+    bool lo_ev = true, hi_ev = true;
     for(int it = 0; it < 80; it++){
         const double xm = 0.5 * (lo + hi);
-        bool pos;
+        bool pos, ev = false;
         if(xm < r - band) pos = true;
         else if(xm > r + band) pos = false;
-        else pos = nh4sh_f(xm, T0, heat, a, b) > 0.0;
-        if(pos) lo = xm; else hi = xm;
+        else { pos = nh4sh_f(xm, T0, heat, a, b) > 0.0; ev = true; }
+        if(pos){ lo = xm; lo_ev = ev; } else { hi = xm; hi_ev = ev; }
         if(hi - lo <= stop) break;
     }
-    if(hi > lo && (nh4sh_f(lo, T0, heat, a, b) > 0.0) && !(nh4sh_f(hi, T0, heat, a, b) > 0.0)) return;
+    // the final bracket holds if f changes sign over it: only the inferred ends are evaluated
+    if(hi > lo && (lo_ev || nh4sh_f(lo, T0, heat, a, b) > 0.0) && (hi_ev || !(nh4sh_f(hi, T0, heat, a, b) > 0.0))) return;
     if(!(hi > lo)) return;
     lo = lo0; hi = hi0;                                       // the plain bisection
     for(int it = 0; it < 80; it++){
@@ -171,32 +175,6 @@ __global__ void __launch_bounds__(128) nh4sh_eq_kernel(ChemArgs<S> a){
     }
 }
 
-// ChemistryUran.h:601-686 without SeaMount cells: the central first differences of x at (i, j, k)
-template <typename S>
-__device__ __forceinline__ void chem_d1(const S* x, size_t q, size_t pl, size_t kp, int dkw, int dke,
-                                        const ChemConst& c, double& dr_, double& dt_, double& dp_){
-    dr_ = ((double)x[q + pl] - (double)x[q - pl]) / (2.0 * c.dr);
-    dt_ = ((double)x[q + kp] - (double)x[q - kp]) / (2.0 * c.dthe);
-    dp_ = ((double)x[q + dke] - (double)x[q - dkw]) / (2.0 * c.dphi);
-}
-// ChemistryUran.h:576-598 (exp_rm = 1: coord_stretching is false)
-template <typename S>
-__device__ __forceinline__ double chem_lap(const S* x, size_t q, size_t pl, size_t kp, int dkw, int dke,
-                                           double rm, double rmsinthe, double costhe, const ChemConst& c){
-    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
-    const double v = (double)x[q];
-    const double xip = (double)x[q + pl], xim = (double)x[q - pl];
-    const double xjp = (double)x[q + kp], xjm = (double)x[q - kp];
-    const double xkp = (double)x[q + dke], xkm = (double)x[q - dkw];
-    const double d2cdr2 = (xip - 2.0 * v + xim) / (c.dr * c.dr) * exp_2_rm;
-    const double d2cdthe2 = (xjp - 2.0 * v + xjm) / (c.dthe * c.dthe);
-    const double d2cdphi2 = (xkp - 2.0 * v + xkm) / (c.dphi * c.dphi);
-    const double dcdr = (xip - xim) / (2.0 * c.dr) * exp_rm;
-    const double dcdthe = (xjp - xjm) / (2.0 * c.dthe);
-    return d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) + costhe / (rm * rmsinthe) * dcdthe
-         + d2cdphi2 / (rmsinthe * rmsinthe);
-}
-
 // The phi neighbours' offsets k-1 and k+1 of k in a row: round the ring of km-1 meridians with the
 // periodic seam, else the plain neighbours (k runs over 1..km-2 then).
 __device__ __forceinline__ void chem_kn(int k, int km, int per, int& dkw, int& dke){
@@ -204,9 +182,40 @@ __device__ __forceinline__ void chem_kn(int k, int km, int per, int& dkw, int& d
     dke = per ? phi_wrap(k + 1, km) - k : 1;
 }
 
+// The seven values of x around a cell, in FP64: centre, r, theta and phi neighbours.
+struct Chem7 { double c, ip, im, jp, jm, kp, km; };
+template <typename S>
+__device__ __forceinline__ Chem7 chem_ld7(const S* x, size_t q, size_t pl, size_t kp, int dkw, int dke){
+    Chem7 v;
+    v.c = (double)x[q];
+    v.ip = (double)x[q + pl]; v.im = (double)x[q - pl];
+    v.jp = (double)x[q + kp]; v.jm = (double)x[q - kp];
+    v.kp = (double)x[q + dke]; v.km = (double)x[q - dkw];
+    return v;
+}
+// ChemistryUran.h:601-686 without SeaMount cells: the central first differences at the cell
+__device__ __forceinline__ void chem_d1v(const Chem7& x, const ChemConst& c, double& dr_, double& dt_, double& dp_){
+    dr_ = (x.ip - x.im) / (2.0 * c.dr);
+    dt_ = (x.jp - x.jm) / (2.0 * c.dthe);
+    dp_ = (x.kp - x.km) / (2.0 * c.dphi);
+}
+// ChemistryUran.h:576-598 (exp_rm = 1: coord_stretching is false)
+__device__ __forceinline__ double chem_lapv(const Chem7& x, double rm, double rmsinthe, double costhe, const ChemConst& c){
+    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
+    const double v = x.c;
+    const double d2cdr2 = (x.ip - 2.0 * v + x.im) / (c.dr * c.dr) * exp_2_rm;
+    const double d2cdthe2 = (x.jp - 2.0 * v + x.jm) / (c.dthe * c.dthe);
+    const double d2cdphi2 = (x.kp - 2.0 * v + x.km) / (c.dphi * c.dphi);
+    const double dcdr = (x.ip - x.im) / (2.0 * c.dr) * exp_rm;
+    const double dcdthe = (x.jp - x.jm) / (2.0 * c.dthe);
+    return d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) + costhe / (rm * rmsinthe) * dcdthe
+         + d2cdphi2 / (rmsinthe * rmsinthe);
+}
+
 // rho_mix on every cell (ChemistryUran.h:312-320); on the interior the thermal mass flux and the
 // diffusive tendencies difflux_x = D_x lap(c_x) (passes 1 and 2, ChemistryUran.h:322-419, with
-// j_* formed at the cell where pass 2 reads them).
+// j_* formed at the cell where pass 2 reads them). Every load of a cell comes before its first
+// store (a store could alias a later load as far as the compiler knows).
 template <typename S>
 __global__ void __launch_bounds__(128) chem_diff_kernel(ChemArgs<S> a){
     const Grid& g = a.g;
@@ -215,28 +224,34 @@ __global__ void __launch_bounds__(128) chem_diff_kernel(ChemArgs<S> a){
     const ChemConst& c = a.c;
     const size_t q = gidx(g, i, j, k);
     const double t0 = t_ld(a.t, a.tlo, q);
-    a.rho_mix[q] = (S)((double)a.ps[q] * 1e5 / (c.R_mix * t0 * c.t_ref));
+    const double rho = (double)a.ps[q] * 1e5 / (c.R_mix * t0 * c.t_ref);
     const int k_first = c.per ? 0 : 1;
-    if(i < 1 || i > g.im - 2 || j < 1 || j > g.jm - 2 || k < k_first || k > g.km - 2) return;
+    if(i < 1 || i > g.im - 2 || j < 1 || j > g.jm - 2 || k < k_first || k > g.km - 2){
+        a.rho_mix[q] = (S)rho;
+        return;
+    }
     const size_t pl = (size_t)g.jm * g.kp, kp = (size_t)g.kp;
     int dkw, dke;
     chem_kn(k, g.km, c.per, dkw, dke);
+    Chem7 T;
+    if(a.tlo){
+        T.c = t0;
+        T.ip = t_ld(a.t, a.tlo, q + pl); T.im = t_ld(a.t, a.tlo, q - pl);
+        T.jp = t_ld(a.t, a.tlo, q + kp); T.jm = t_ld(a.t, a.tlo, q - kp);
+        T.kp = t_ld(a.t, a.tlo, q + dke); T.km = t_ld(a.t, a.tlo, q - dkw);
+    } else T = chem_ld7(a.t, q, pl, kp, dkw, dke);
+    const Chem7 H = chem_ld7(a.h2s, q, pl, kp, dkw, dke);
+    const Chem7 N = chem_ld7(a.nh3, q, pl, kp, dkw, dke);
+    const Chem7 X = chem_ld7(a.nh4sh, q, pl, kp, dkw, dke);
     // pass 1's metric: the raw radius and max(sinthe_min, |sin|)
     const double rm = a.tab.rad[i];
     const double rmsinthe = rm * chem_max(c.sinthe_min, fabs(a.tab.sin[j]));
     double dtdr, dtdthe, dtdphi;
-    if(a.tlo){
-        const double tip = t_ld(a.t, a.tlo, q + pl), tim = t_ld(a.t, a.tlo, q - pl);
-        const double tjp = t_ld(a.t, a.tlo, q + kp), tjm = t_ld(a.t, a.tlo, q - kp);
-        const double tkp = t_ld(a.t, a.tlo, q + dke), tkm = t_ld(a.t, a.tlo, q - dkw);
-        dtdr = (tip - tim) / (2.0 * c.dr);
-        dtdthe = (tjp - tjm) / (2.0 * c.dthe);
-        dtdphi = (tkp - tkm) / (2.0 * c.dphi);
-    } else chem_d1(a.t, q, pl, kp, dkw, dke, c, dtdr, dtdthe, dtdphi);
+    chem_d1v(T, c, dtdr, dtdthe, dtdphi);
     double hr, ht, hp, nr, nt, np, sr, stt, sp;
-    chem_d1(a.h2s, q, pl, kp, dkw, dke, c, hr, ht, hp);
-    chem_d1(a.nh3, q, pl, kp, dkw, dke, c, nr, nt, np);
-    chem_d1(a.nh4sh, q, pl, kp, dkw, dke, c, sr, stt, sp);
+    chem_d1v(H, c, hr, ht, hp);
+    chem_d1v(N, c, nr, nt, np);
+    chem_d1v(X, c, sr, stt, sp);
     const double jT_nh3 = c.DT_nh3 / t0 * dtdr;
     const double jT_h2s = c.DT_h2s / t0 * dtdr;
     const double jT_nh4sh = c.DT_nh4sh / t0 * dtdr;
@@ -247,16 +262,21 @@ __global__ void __launch_bounds__(128) chem_diff_kernel(ChemArgs<S> a){
     const double j_h2s = c.c_mix / c.r_mix * (c.m_h2s * c.D_h2s * d_h2s - jT_h2s);
     const double j_nh4sh = c.c_mix / c.r_mix * (c.m_nh4sh * c.D_nh4sh * d_nh4sh - jT_nh4sh);
     const double w0 = 0.0;                            // w_nh3, w_h2s, w_nh4sh in the equilibrium form
-    a.tmf[q] = (S)((j_nh3 * c.cp_nh3 + j_h2s * c.cp_h2s + j_nh4sh * c.cp_nh4sh)
-                   * (dtdr + fabs(dtdthe) / rm + dtdphi / rmsinthe)
-                   + t0 * (w0 * c.k_nh3 + w0 * c.k_h2s + w0 * c.k_nh4sh));
+    const double tmf = (j_nh3 * c.cp_nh3 + j_h2s * c.cp_h2s + j_nh4sh * c.cp_nh4sh)
+                       * (dtdr + fabs(dtdthe) / rm + dtdphi / rmsinthe)
+                       + t0 * (w0 * c.k_nh3 + w0 * c.k_h2s + w0 * c.k_nh4sh);
     // the Laplacian's metric: the metric radius and max(sin, floor)
     const double rml = a.tab.rmm[i];
     const double rmsl = rml * chem_max(a.tab.sin[j], c.floor);
     const double cl = a.tab.cos[j];
-    a.df_h2s[q] = (S)(c.D_h2s * chem_lap(a.h2s, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
-    a.df_nh3[q] = (S)(c.D_nh3 * chem_lap(a.nh3, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
-    a.df_nh4sh[q] = (S)(c.D_nh4sh * chem_lap(a.nh4sh, q, pl, kp, dkw, dke, rml, rmsl, cl, c));
+    const double dfh = c.D_h2s * chem_lapv(H, rml, rmsl, cl, c);
+    const double dfn = c.D_nh3 * chem_lapv(N, rml, rmsl, cl, c);
+    const double dfx = c.D_nh4sh * chem_lapv(X, rml, rmsl, cl, c);
+    a.rho_mix[q] = (S)rho;
+    a.tmf[q] = (S)tmf;
+    a.df_h2s[q] = (S)dfh;
+    a.df_nh3[q] = (S)dfn;
+    a.df_nh4sh[q] = (S)dfx;
 }
 
 // FluxLimiter.h:68-70
@@ -274,9 +294,9 @@ __global__ void __launch_bounds__(128) chem_limit_kernel(ChemArgs<S> a){
     const int k = k_first + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y, i = 1 + blockIdx.z;
     if(k > g.km - 2) return;
     const size_t o = gidx(g, i, j, k), pl = (size_t)g.jm * g.kp, kp = (size_t)g.kp;
-    a.mf_h2s[o] = (S)(0.0 + c.dsign * (double)a.df_h2s[o]);
-    a.mf_nh3[o] = (S)(0.0 + c.dsign * (double)a.df_nh3[o]);
-    a.mf_nh4sh[o] = (S)(0.0 + c.dsign * (double)a.df_nh4sh[o]);
+    // every load of the cell before its first store (a store could alias a later load as far as
+    // the compiler knows); the far upwind values loaded whether or not the flow's sign reads them
+    const double dh = (double)a.df_h2s[o], dn = (double)a.df_nh3[o], dx = (double)a.df_nh4sh[o];
     const S* x = a.nh4sh;
     int dkw, dke;
     chem_kn(k, g.km, c.per, dkw, dke);
@@ -284,6 +304,9 @@ __global__ void __launch_bounds__(128) chem_limit_kernel(ChemArgs<S> a){
     const double q_tp = (double)x[o + kp], q_tm = (double)x[o - kp];
     const double q_pp = (double)x[o + dke], q_pm = (double)x[o - dkw];
     const double uu = (double)a.u[o], vv = (double)a.v[o], ww = (double)a.w[o];
+    const double x_r2 = (i + 2 < g.im) ? (double)x[o + 2 * pl] : q_rp;
+    const double x_t2 = (j + 2 < g.jm) ? (double)x[o + 2 * kp] : (C43 * q_tp - C13 * q);
+    const double x_p2 = c.per ? (double)x[o - k + phi_wrap(k + 2, g.km)] : ((k + 2 < g.km) ? (double)x[o + 2] : q_pp);
     const double rm = a.tab.rmm[i];
     const double sinthe = chem_max(c.floor, fabs(a.tab.sin[j]));
     const double inv_rm = 1.0 / rm, inv_rmsinthe = 1.0 / (rm * sinthe);
@@ -292,25 +315,24 @@ __global__ void __launch_bounds__(128) chem_limit_kernel(ChemArgs<S> a){
     {
         const double df = q_rp - q, db = q - q_rm;
         const double denom = df + (df >= 0.0 ? eps : -eps);
-        const double r = (uu >= 0.0) ? db / denom : ((i + 2 < g.im ? (double)x[o + 2 * pl] : q_rp) - q_rp) / denom;
+        const double r = (uu >= 0.0) ? db / denom : (x_r2 - q_rp) / denom;
         corr += (1.0 - chem_superbee(r)) * fabs(uu) * (df - db) / (2.0 * c.dr);
     }
     {
         const double df = q_tp - q, db = q - q_tm;
         const double denom = df + (df >= 0.0 ? eps : -eps);
-        const double q_far = (j + 2 < g.jm) ? (double)x[o + 2 * kp] : (C43 * q_tp - C13 * q);
-        const double r = (vv >= 0.0) ? db / denom : (q_far - q_tp) / denom;
+        const double r = (vv >= 0.0) ? db / denom : (x_t2 - q_tp) / denom;
         corr += (1.0 - chem_superbee(r)) * fabs(vv) * inv_rm * (df - db) / (2.0 * c.dthe);
     }
     {
         const double df = q_pp - q, db = q - q_pm;
         const double denom = df + (df >= 0.0 ? eps : -eps);
-        double q2;
-        if(c.per) q2 = (double)x[o - k + phi_wrap(k + 2, g.km)];
-        else q2 = (k + 2 < g.km) ? (double)x[o + 2] : q_pp;
-        const double r = (ww >= 0.0) ? db / denom : (q2 - q_pp) / denom;
+        const double r = (ww >= 0.0) ? db / denom : (x_p2 - q_pp) / denom;
         corr += (1.0 - chem_superbee(r)) * fabs(ww) * inv_rmsinthe * (df - db) / (2.0 * c.dphi);
     }
+    a.mf_h2s[o] = (S)(0.0 + c.dsign * dh);
+    a.mf_nh3[o] = (S)(0.0 + c.dsign * dn);
+    a.mf_nh4sh[o] = (S)(0.0 + c.dsign * dx);
     a.fl[o] = (S)corr;
 }
 
