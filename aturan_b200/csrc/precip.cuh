@@ -71,8 +71,25 @@ __global__ void __launch_bounds__(128) precip_kernel(const __grid_constant__ Pre
         if(n == 0) a.Q[q] = (S)0.0;
         sv[q] = (S)0.0; sc[q] = (S)0.0; si[q] = (S)0.0;
     }
+    // A level's inputs are loaded one level ahead, before the level above's stores (they are other
+    // cells; in program order after those stores the loads would wait for them, as the compiler
+    // must assume they may alias).
+    struct LevelIn { double t, p, r; S v, c, ic; };
+    auto load_level = [&](int i) -> LevelIn {
+        LevelIn L;
+        const size_t q = o + (size_t)i * pl;
+        L.t = t_ld(a.t, a.tlo, q);
+        L.p = (double)a.ps[q];
+        L.r = a.local_rho ? (double)a.rho[q] : 0.0;
+        L.v = fv[q]; L.c = fc[q]; L.ic = fi[q];
+        return L;
+    };
+    LevelIn nxt{};
+    if(kin && g.im >= 2) nxt = load_level(g.im - 2);
     for(int i = g.im - 2; i >= 0; i--){
         const size_t q = o + (size_t)i * pl;
+        const LevelIn cur = nxt;
+        if(kin && i > 0) nxt = load_level(i - 1);
         const double dz = pr_max(0.0, a.dz[i]);
         double term = 0.0;
         bool added = false;
@@ -80,13 +97,13 @@ __global__ void __launch_bounds__(128) precip_kernel(const __grid_constant__ Pre
             if(!on || dz <= 0.0){                             // dz <= 0: the fluxes pass through
                 sv[q] = (S)0.0; sc[q] = (S)0.0; si[q] = (S)0.0;
             } else {
-                const double T = t_ld(a.t, a.tlo, q) * a.t_ref;
-                const double p_u = (double)a.ps[q];
+                const double T = cur.t * a.t_ref;
+                const double p_u = cur.p;
                 double rho = a.r_mix;                          // rho_at, cUranusModel.h:526-531
-                if(a.local_rho){ const double r = (double)a.rho[q]; rho = (r > 0.0 && isfinite(r)) ? r : a.r_mix; }
-                const double q_v = pr_max(0.0, (double)fv[q]);
-                const double q_c = pr_max(0.0, (double)fc[q]);
-                const double q_i = pr_max(0.0, (double)fi[q]);
+                if(a.local_rho){ const double r = cur.r; rho = (r > 0.0 && isfinite(r)) ? r : a.r_mix; }
+                const double q_v = pr_max(0.0, (double)cur.v);
+                const double q_c = pr_max(0.0, (double)cur.c);
+                const double q_i = pr_max(0.0, (double)cur.ic);
                 const double E_r = exp(s.C + (-s.L0 / T + s.del_alf * log(T) + s.del_bet * T) / s.den);   // ATPhys.h:49-52
                 const double q_sat = (p_u > E_r) ? rho * s.ep * E_r / p_u : q_v;
                 const double F_r_in = Pr, F_s_in = Ps, F_g_in = Pg;
