@@ -169,18 +169,33 @@ __global__ void __launch_bounds__(128) turb_column_kernel(TurbArgs<S> a){
     if(k >= g.km) return;
     const size_t pl = (size_t)g.jm * g.kp, o = gidx(g, 0, j, k);
     const int kf = c.per ? 0 : 1;
+    // CH levels at a time, every load of a chunk before its stores (a store could alias the next
+    // level's load as far as the compiler knows); the same operations per cell, in the same order
+    constexpr int CH = 8;
     if(j >= 1 && j <= g.jm - 2 && k >= kf && k <= g.km - 2)
-        for(int i = 1; i < g.im - 1; i++){
-            const size_t q = o + (size_t)i * pl;
-            a.tke[q] = (S)turb_max(c.k_bg_nd, turb_max(0.0, (double)a.tke[q]));
-            a.dis[q] = (S)turb_max(c.dis_min, turb_max(c.dis_min, (double)a.dis[q]));
+        for(int i0 = 1; i0 < g.im - 1; i0 += CH){
+            S tk[CH], ds[CH];
+#pragma unroll
+            for(int u = 0; u < CH; u++)
+                if(i0 + u < g.im - 1){ const size_t q = o + (size_t)(i0 + u) * pl; tk[u] = a.tke[q]; ds[u] = a.dis[q]; }
+#pragma unroll
+            for(int u = 0; u < CH; u++)
+                if(i0 + u < g.im - 1){
+                    const size_t q = o + (size_t)(i0 + u) * pl;
+                    a.tke[q] = (S)turb_max(c.k_bg_nd, turb_max(0.0, (double)tk[u]));
+                    a.dis[q] = (S)turb_max(c.dis_min, turb_max(c.dis_min, (double)ds[u]));
+                }
         }
     a.tke[o] = a.tke[o + pl];
     a.dis[o] = a.dis[o + pl];
     a.nue[o] = a.nue[o + pl];
-    for(int i = 0; i < g.im; i++){
-        const size_t q = o + (size_t)i * pl;
-        a.nue[q] = (S)(turb_clamp3((double)a.nue[q], 0.0, c.nue_max) * 1.0);
+    for(int i0 = 0; i0 < g.im; i0 += CH){
+        S nu[CH];
+#pragma unroll
+        for(int u = 0; u < CH; u++) if(i0 + u < g.im) nu[u] = a.nue[o + (size_t)(i0 + u) * pl];
+#pragma unroll
+        for(int u = 0; u < CH; u++)
+            if(i0 + u < g.im) a.nue[o + (size_t)(i0 + u) * pl] = (S)(turb_clamp3((double)nu[u], 0.0, c.nue_max) * 1.0);
     }
 }
 
