@@ -126,22 +126,52 @@ def test_post_step(ref_model, oracle_lib, base_state):
     assert np.allclose(ra, oa, rtol=1e-12, atol=0.0)
 
 
-@pytest.mark.parametrize("knobs", ["no_geo_balance_forms", "cubic_lid_open_phi"])
-def test_post_step_knob_sets(knobs):
-    """Other knob values (forms, taper, lid, floor, filters, an open phi seam): the reference reads
-    them from its environment once per process, so each set runs in a child process with that
-    environment; the child requires bit equality as above."""
+POST_KNOBS = ["no_geo_balance_forms", "cubic_lid_open_phi"]
+PHYSICS_KNOBS = ["chem_minus_open_phi", "turb_no_curv_open_phi", "precip_uncoupled", "precip_no_h2s"]
+
+
+@pytest.fixture(scope="module")
+def knob_children():
+    """Every knob set's child process started at once, each with its share of the host's cores
+    (a child spends most of its time in the reference's serial initialisation), and waited for
+    together: {(child script, knob set): (return code, stdout, stderr)}."""
     import os
     import subprocess
     import sys
     from oracle import ref
-    from tests.post_case import KNOB_SETS
     if not ref.available():
         pytest.skip("compiled reference (oracle/_ref) not present")
-    env = dict(os.environ, **KNOB_SETS[knobs][0])
-    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_post_knobs_child.py")
-    r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    from tests.post_case import KNOB_SETS as POST_SETS
+    from _physics_knobs_child import KNOB_SETS as PHYS_SETS
+    jobs = [("_post_knobs_child.py", k, POST_SETS[k][0]) for k in POST_KNOBS]
+    jobs += [("_physics_knobs_child.py", k, PHYS_SETS[k][0]) for k in PHYSICS_KNOBS]
+    threads = str(max(1, (os.cpu_count() or 1) // len(jobs)))
+    procs = {}
+    for script, k, knob_env in jobs:
+        env = dict(os.environ, **knob_env)
+        env["OMP_NUM_THREADS"] = threads
+        procs[(script, k)] = subprocess.Popen([sys.executable, os.path.join(here, script), k], env=env,
+                                              stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    out = {}
+    for key, pr in procs.items():
+        try:
+            so, se = pr.communicate(timeout=1800)
+        except subprocess.TimeoutExpired:
+            pr.kill()
+            so, se = pr.communicate()
+        out[key] = (pr.returncode, so, se)
+    return out
+
+
+@pytest.mark.parametrize("knobs", POST_KNOBS)
+def test_post_step_knob_sets(knobs, knob_children):
+    """Other knob values (forms, taper, lid, floor, filters, an open phi seam): the reference reads
+    them from its environment once per process, so each set runs in a child process with that
+    environment; the child requires bit equality as above."""
+    rc, so, se = knob_children[("_post_knobs_child.py", knobs)]
+    assert rc == 0 and "OK" in so, so[-2000:] + se[-2000:]
 
 
 @pytest.mark.parametrize("source", ["reference_init", "synthetic"])
@@ -249,24 +279,14 @@ def test_precipitation(ref_model, oracle_lib, base_state, source):
     assert np.count_nonzero(st["Q_precip"]) > 1000
 
 
-@pytest.mark.parametrize("knobs", ["chem_minus_open_phi", "turb_no_curv_open_phi", "precip_uncoupled", "precip_no_h2s"])
-def test_physics_knob_sets(knobs):
+@pytest.mark.parametrize("knobs", PHYSICS_KNOBS)
+def test_physics_knob_sets(knobs, knob_children):
     """Other knob values of the chemistry (massflux = -difflux, the open phi seam), the turbulence
     closure (no curvature terms, the open seam) and the precipitation (the depletion written into the
     condensate fields; no H2S and another rate scale), each in a child process with that environment;
     the child requires bit equality of every written value."""
-    import os
-    import subprocess
-    import sys
-    from oracle import ref
-    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-    from _physics_knobs_child import KNOB_SETS
-    if not ref.available():
-        pytest.skip("compiled reference (oracle/_ref) not present")
-    env = dict(os.environ, **KNOB_SETS[knobs][0])
-    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_physics_knobs_child.py")
-    r = subprocess.run([sys.executable, child, knobs], env=env, capture_output=True, text=True, timeout=900)
-    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+    rc, so, se = knob_children[("_physics_knobs_child.py", knobs)]
+    assert rc == 0 and "OK" in so, so[-2000:] + se[-2000:]
 
 
 def test_reference_loop(ref_model, oracle_lib, base_state, tmp_path):
